@@ -1,0 +1,174 @@
+/*
+ * terrace_b200.h -- C ABI of the B200-native Terrace dynamic-graph hot path.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, status codes.  No CUDA
+ * or torch types appear here; a CUDA stream is passed as `void*`
+ * (cudaStream_t).  Every entry point is synchronous: it returns after the
+ * device work it launched has finished, so host buffers may be reused at
+ * once.  Unless TRC_DEVICE_PTR is set in `flags`, array arguments are HOST
+ * pointers and the library copies them to and from the device itself.
+ *
+ * Each declaration names the reference interface it replaces
+ * (PASSIONLab/terrace, paths inside that tree).  The reference is a
+ * header-only C++ library (graphstore::Graph in include/graph.h); this ABI is
+ * the flat layer a C++ facade (terrace_b200.hpp) or an FFI binds.
+ */
+#ifndef TERRACE_B200_H_
+#define TERRACE_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct trc_graph trc_graph;
+
+/* Status codes.  The reference exits or aborts on fatal errors
+ * (src/PMA.cc:2308-2316, include/io_util.h:117-131) and returns -1/0 from
+ * single-edge calls (include/graph.h:505-641, :675-791); here every call
+ * returns one of these and trc_last_error() holds a message. */
+typedef enum {
+  TRC_OK = 0,
+  TRC_ERR_INVALID = 1, /* bad argument: null pointer, vertex id >= n, ... */
+  TRC_ERR_NOMEM = 2,   /* HBM budget or device allocation exhausted */
+  TRC_ERR_CUDA = 3,    /* a CUDA call failed (message has the CUDA error) */
+  TRC_ERR_TIMEOUT = 4, /* a bounded device wait ran out (serving loop) */
+  TRC_ERR_STATE = 5,   /* call not valid in the handle's current state */
+  TRC_ERR_NOT_BUILT = 6 /* the sm_100a kernels are not available */
+} trc_status;
+
+/* flags */
+#define TRC_DEVICE_PTR 0x1u      /* array arguments are device pointers */
+#define TRC_SYMMETRIZE 0x2u      /* apply (u,v) and (v,u) for every pair */
+#define TRC_DROP_SELF_LOOPS 0x4u /* ignore pairs with u == v */
+
+#define TRC_UNREACHED 0xFFFFFFFFu /* BFS level of an unreached vertex */
+
+/* Tunables.  Defaults mirror the reference's constants where one exists. */
+typedef struct {
+  uint32_t hub_threshold;     /* degree above which a vertex moves to the
+                                 blocked tier; reference MEDIUM_DEGREE 1024
+                                 (include/graph.h:39).  Default 1024. */
+  double pma_root_density;    /* upper density bound at the PMA root;
+                                 reference 0.75 (src/PMA.cc:382-394). */
+  double pma_build_density;   /* density after a full PMA rebuild.
+                                 Default 0.6. */
+  double hub_block_fill;      /* fill of hub blocks after a rewrite.
+                                 Default 0.75. */
+  uint32_t push_pull_divisor; /* edgeMap goes dense when |F| >= n/divisor;
+                                 reference threshold 20 (include/Map.cpp:65-74).
+                                 0 = the autotuned value (default 20). */
+} trc_config;
+
+/* Fill `cfg` with the defaults listed above. */
+void trc_config_default(trc_config *cfg);
+
+const char *trc_status_string(trc_status s);
+/* Message of the last failing call on this host thread ("" if none). */
+const char *trc_last_error(void);
+
+/* ---- lifetime: replaces graphstore::Graph::Graph(uint32_t) / ~Graph
+ *      (include/graph.h:232-239).  hbm_budget_bytes caps the device memory
+ *      the handle may hold (0 = no cap beyond the device's free memory). */
+trc_status trc_graph_create(uint32_t n, uint64_t hbm_budget_bytes,
+                            const trc_config *cfg, trc_graph **out);
+trc_status trc_graph_destroy(trc_graph *g);
+/* Bind the handle to a CUDA stream (cudaStream_t); NULL = library stream. */
+trc_status trc_graph_set_stream(trc_graph *g, void *stream);
+
+/* ---- updates: replaces Graph::add_edge_batch (include/graph.h:430-502) and
+ *      the per-edge Graph::remove_edge loop of src/graph_bm.cc:375-380 (the
+ *      reference declares no remove_edge_batch, include/graph.h:143-150).
+ *      Set semantics: duplicates, already-present edges (insert) and absent
+ *      edges (remove) are ignored; input need not be sorted and is never
+ *      modified.  *applied (may be NULL) receives the number of directed
+ *      edges actually inserted / removed. */
+trc_status trc_add_edge_batch(trc_graph *g, const uint32_t *src,
+                              const uint32_t *dst, uint64_t k, uint32_t flags,
+                              uint64_t *applied);
+trc_status trc_remove_edge_batch(trc_graph *g, const uint32_t *src,
+                                 const uint32_t *dst, uint64_t k,
+                                 uint32_t flags, uint64_t *applied);
+
+/* ---- queries: replaces Graph::is_edge, Graph::degree, the NeighborIterator
+ *      and Graph::count_common (include/graph.h:643-673, :797-803, :844-899,
+ *      :1085-1255), batched over q queries. */
+trc_status trc_is_edge(trc_graph *g, const uint32_t *src, const uint32_t *dst,
+                       uint64_t q, uint8_t *out, uint32_t flags);
+trc_status trc_degree(trc_graph *g, const uint32_t *v, uint64_t q,
+                      uint32_t *out, uint32_t flags);
+/* Sorted neighbours of v into out[0..cap); *len = degree(v) (may exceed cap,
+ * in which case only cap entries are written). */
+trc_status trc_neighbors(trc_graph *g, uint32_t v, uint32_t *out, uint64_t cap,
+                         uint64_t *len, uint32_t flags);
+/* out[i] = |{w in N(s[i]) n N(d[i]) : w < min(s[i],d[i])}| */
+trc_status trc_count_common(trc_graph *g, const uint32_t *s, const uint32_t *d,
+                            uint64_t q, uint32_t *out, uint32_t flags);
+/* Graph::get_num_vertices / get_num_edges / get_size (include/graph.h:805-822) */
+trc_status trc_num_vertices(trc_graph *g, uint32_t *n);
+trc_status trc_num_edges(trc_graph *g, uint64_t *m);
+trc_status trc_get_size(trc_graph *g, uint64_t *bytes);
+/* Whole graph as sorted CSR: offsets[n+1], targets[num_edges]. */
+trc_status trc_dump_csr(trc_graph *g, uint64_t *offsets, uint32_t *targets,
+                        uint32_t flags);
+
+/* ---- analytics: replaces BFS_with_edge_map (include/BFS.h:41-84),
+ *      PR_S<double> (include/Pagerank.h:105-184), CC (include/Components.h:
+ *      92-120), BC (include/BC.h:99-157) and TC (include/TC.h:73-87). */
+/* parents: -1 unreached, parents[src]=src; levels (may be NULL):
+ * TRC_UNREACHED for unreached vertices. */
+trc_status trc_bfs(trc_graph *g, uint32_t src, int32_t *parents,
+                   uint32_t *levels, uint32_t flags);
+/* damping == 0 reproduces the reference (no damping term); 0 < damping < 1
+ * computes p' = (1-damping)/n + damping * sum. FP64. */
+trc_status trc_pagerank(trc_graph *g, uint32_t iters, double damping,
+                        double *ranks, uint32_t flags);
+/* labels[v] = smallest vertex id in v's component (symmetric graphs). */
+trc_status trc_cc(trc_graph *g, uint32_t *labels, uint32_t flags);
+/* Dependencies as the reference returns them; NaN for unreached vertices. */
+trc_status trc_bc(trc_graph *g, uint32_t src, double *dep, uint32_t flags);
+trc_status trc_tc(trc_graph *g, uint64_t *count);
+
+/* ---- generator: replaces rMat<uint32_t> (include/rmat_util.h:81-115),
+ *      bit-exact, edges first..first+count-1, on the device. */
+trc_status trc_rmat_generate(uint32_t n, uint32_t seed, double a, double b,
+                             double c, uint64_t first, uint64_t count,
+                             uint32_t *src, uint32_t *dst, uint32_t flags,
+                             void *stream);
+
+/* ---- diagnostics (no reference counterpart: the reference has only
+ *      lock-ownership checks, src/PMA.cc:29-111). */
+typedef struct {
+  uint32_t n;
+  uint64_t num_edges;
+  uint64_t inline_edges;   /* tier 1 */
+  uint64_t pma_edges;      /* tier 2 */
+  uint64_t pma_capacity;   /* tier-2 slots */
+  uint64_t hub_edges;      /* tier 3 */
+  uint32_t num_hubs;
+  uint64_t hub_blocks_used;
+  uint64_t device_bytes;   /* bytes held on the device */
+  uint64_t pma_rebuilds;   /* full tier-2 rebuilds so far */
+  uint64_t pma_window_rebalances; /* local window rebalances so far */
+} trc_stats;
+trc_status trc_get_stats(trc_graph *g, trc_stats *out);
+/* Checks every structural invariant on the device (sorted, duplicate-free
+ * lists, degree = list length, tier-2 segments inside their slots, hub
+ * blocks packed and ordered).  *violations = number of broken invariants. */
+trc_status trc_check(trc_graph *g, uint64_t *violations);
+
+/* Per-kernel device time, recorded with CUDA events on the handle's stream
+ * around every launch while enabled.  trc_profile_get returns the summed
+ * milliseconds and launch count of kernels whose name contains `name`. */
+trc_status trc_profile_enable(trc_graph *g, int on);
+trc_status trc_profile_reset(trc_graph *g);
+trc_status trc_profile_get(trc_graph *g, const char *name, double *ms,
+                           uint64_t *launches);
+/* Names of the kernels recorded so far, newline-separated, into buf. */
+trc_status trc_profile_names(trc_graph *g, char *buf, uint64_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TERRACE_B200_H_ */

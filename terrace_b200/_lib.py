@@ -1,0 +1,115 @@
+"""ctypes binding of libterrace_b200.so (the C ABI in include/terrace_b200.h).
+
+There is no CPU fallback: if the library is missing, importing the package
+raises, naming the build command.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libterrace_b200.so")
+
+TRC_OK = 0
+TRC_ERR_INVALID = 1
+TRC_ERR_NOMEM = 2
+TRC_ERR_CUDA = 3
+TRC_ERR_TIMEOUT = 4
+TRC_ERR_STATE = 5
+TRC_ERR_NOT_BUILT = 6
+
+TRC_DEVICE_PTR = 0x1
+TRC_SYMMETRIZE = 0x2
+TRC_DROP_SELF_LOOPS = 0x4
+TRC_UNREACHED = 0xFFFFFFFF
+
+
+class TrcError(RuntimeError):
+    """A non-OK trc_status; .status holds the code."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[trc status {status}] {msg}")
+        self.status = status
+
+
+class trc_config(C.Structure):
+    _fields_ = [("hub_threshold", C.c_uint32),
+                ("pma_root_density", C.c_double),
+                ("pma_build_density", C.c_double),
+                ("hub_block_fill", C.c_double),
+                ("push_pull_divisor", C.c_uint32)]
+
+
+class trc_stats(C.Structure):
+    _fields_ = [("n", C.c_uint32),
+                ("num_edges", C.c_uint64),
+                ("inline_edges", C.c_uint64),
+                ("pma_edges", C.c_uint64),
+                ("pma_capacity", C.c_uint64),
+                ("hub_edges", C.c_uint64),
+                ("num_hubs", C.c_uint32),
+                ("hub_blocks_used", C.c_uint64),
+                ("device_bytes", C.c_uint64),
+                ("pma_rebuilds", C.c_uint64),
+                ("pma_window_rebalances", C.c_uint64)]
+
+
+# (name, restype, argtypes) for every symbol the header declares
+_vp = C.c_void_p
+_u32, _u64, _i32, _int, _dbl = C.c_uint32, C.c_uint64, C.c_int32, C.c_int, C.c_double
+SIGNATURES = [
+    ("trc_config_default", None, [C.POINTER(trc_config)]),
+    ("trc_status_string", C.c_char_p, [_int]),
+    ("trc_last_error", C.c_char_p, []),
+    ("trc_graph_create", _int, [_u32, _u64, C.POINTER(trc_config), C.POINTER(_vp)]),
+    ("trc_graph_destroy", _int, [_vp]),
+    ("trc_graph_set_stream", _int, [_vp, _vp]),
+    ("trc_add_edge_batch", _int, [_vp, _vp, _vp, _u64, _u32, C.POINTER(_u64)]),
+    ("trc_remove_edge_batch", _int, [_vp, _vp, _vp, _u64, _u32, C.POINTER(_u64)]),
+    ("trc_is_edge", _int, [_vp, _vp, _vp, _u64, _vp, _u32]),
+    ("trc_degree", _int, [_vp, _vp, _u64, _vp, _u32]),
+    ("trc_neighbors", _int, [_vp, _u32, _vp, _u64, C.POINTER(_u64), _u32]),
+    ("trc_count_common", _int, [_vp, _vp, _vp, _u64, _vp, _u32]),
+    ("trc_num_vertices", _int, [_vp, C.POINTER(_u32)]),
+    ("trc_num_edges", _int, [_vp, C.POINTER(_u64)]),
+    ("trc_get_size", _int, [_vp, C.POINTER(_u64)]),
+    ("trc_dump_csr", _int, [_vp, _vp, _vp, _u32]),
+    ("trc_bfs", _int, [_vp, _u32, _vp, _vp, _u32]),
+    ("trc_pagerank", _int, [_vp, _u32, _dbl, _vp, _u32]),
+    ("trc_cc", _int, [_vp, _vp, _u32]),
+    ("trc_bc", _int, [_vp, _u32, _vp, _u32]),
+    ("trc_tc", _int, [_vp, C.POINTER(_u64)]),
+    ("trc_rmat_generate", _int, [_u32, _u32, _dbl, _dbl, _dbl, _u64, _u64, _vp, _vp, _u32, _vp]),
+    ("trc_get_stats", _int, [_vp, C.POINTER(trc_stats)]),
+    ("trc_check", _int, [_vp, C.POINTER(_u64)]),
+    ("trc_profile_enable", _int, [_vp, _int]),
+    ("trc_profile_reset", _int, [_vp]),
+    ("trc_profile_get", _int, [_vp, C.c_char_p, C.POINTER(_dbl), C.POINTER(_u64)]),
+    ("trc_profile_names", _int, [_vp, C.c_char_p, _u64]),
+]
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the library and declare every signature.  Raises if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m terrace_b200.build` "
+                          "(there is no CPU fallback)")
+    L = C.CDLL(path)
+    for name, res, args in SIGNATURES:
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status: int):
+    if status != TRC_OK:
+        msg = load().trc_last_error().decode(errors="replace")
+        raise TrcError(status, msg)

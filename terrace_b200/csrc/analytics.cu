@@ -1,0 +1,774 @@
+// analytics.cu -- edgeMap-style traversals over the three tiers.
+//
+// Replaces the Ligra layer of the reference: edgeMap / vertexMap with the
+// sparse (push) and dense (pull) directions (include/Map.cpp:7-108,
+// include/graph.h:1287-1613) and the algorithms on top of it: BFS
+// (include/BFS.h:27-84), PageRank PR_S (include/Pagerank.h:105-184), CC
+// (include/Components.h:92-120), BC (include/BC.h:99-157) and TC
+// (include/TC.h:33-87).
+//
+// Work is split by vertex class so that every lane does useful loads:
+//   S  (1..16 neighbours, all in the 64-byte inline row): 4 lanes per
+//      vertex, one 128-bit load each;
+//   M  (more than 16, PMA segment): one warp per vertex, the 16 inline
+//      neighbours then the contiguous segment in 128-byte chunks;
+//   H  (hubs, blocked tier): one CTA per hub, warps over its blocks.
+// Direction switching follows the reference rule: dense (pull) when the
+// frontier holds at least n/divisor vertices (include/Map.cpp:65-74).
+#include <vector>
+
+#include "graph.cuh"
+
+namespace trc {
+
+constexpr int AT = 256;  // threads per CTA in the analytics kernels
+
+// ---------------------------------------------------------------------------
+// Class lists
+
+struct ClassPred {
+  const uint32_t *deg;
+  const int32_t *hub_of;
+  int cls;  // 0 = S, 1 = M, 2 = H
+  __device__ bool operator()(uint64_t i) const {
+    bool hub = hub_of[i] >= 0;
+    uint32_t d = deg[i];
+    if (cls == 2) return hub;
+    if (hub) return false;
+    return cls == 0 ? (d >= 1 && d <= K_INLINE) : d > K_INLINE;
+  }
+};
+
+struct IdxVal32 {
+  __device__ uint32_t operator()(uint64_t i) const { return (uint32_t)i; }
+};
+
+void Graph::ensure_lists() {
+  if (lists.version == version) return;
+  uint64_t *cnt = s_cnt.get() + 24;
+  uint64_t *t = tmp(select_tmp_elems(n) + 4);
+  uint32_t *bufs[3] = {lists.S.ensure(n), lists.M.ensure(n), lists.Hv.ensure(H ? H : 1)};
+  uint64_t lens[3];
+  for (int c = 0; c < 3; c++) {
+    select_if(ClassPred{deg.get(), hub_of.get(), c}, IdxVal32{}, n, bufs[c], cnt + c, t, stream,
+              prof);
+  }
+  TRC_CUDA(cudaMemcpyAsync(lens, cnt, 24, cudaMemcpyDeviceToHost, stream));
+  sync();
+  lists.nS = lens[0];
+  lists.nM = lens[1];
+  lists.nH = lens[2];
+  lists.version = version;
+}
+
+// ---------------------------------------------------------------------------
+// Warp helpers
+
+__device__ __forceinline__ uint32_t warp_append(bool win, uint32_t *counter) {
+  uint32_t m = __ballot_sync(0xFFFFFFFFu, win);
+  uint32_t base = 0;
+  uint32_t lane = threadIdx.x & 31;
+  if (m) {
+    uint32_t leader = __ffs(m) - 1;
+    if (lane == leader) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  }
+  return base + __popc(m & lanemask_lt());
+}
+
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T *sh) {
+  v = warp_sum(v);
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  T r = 0;
+  if (w == 0) {
+    r = lane < (int)(blockDim.x >> 5) ? sh[lane] : T(0);
+    r = warp_sum(r);
+  }
+  __syncthreads();
+  return r;  // valid in thread 0
+}
+
+// ---------------------------------------------------------------------------
+// PageRank: per iteration p_next[u] = sum over N(u) of p[v]/deg(v)
+// (PR_Vertex then the dense PR_F pull).  The kernels read pdiv = p/deg of
+// the previous iteration and write both the new pdiv and, on the last
+// iteration, the undivided value.
+
+struct PRArgs {
+  const double *pc;
+  double *pn;
+  double *out;
+  double damping, base;
+  int last;
+};
+
+__device__ __forceinline__ void pr_store(const PRArgs &a, uint32_t u, uint32_t d, double sum) {
+  double val = a.damping > 0.0 ? a.base + a.damping * sum : sum;
+  a.pn[u] = val / (double)d;
+  if (a.last) a.out[u] = val;
+}
+
+__global__ void __launch_bounds__(AT) k_pr_S(DevView G, const uint32_t *S, uint64_t nS, PRArgs a) {
+  uint64_t gt = (uint64_t)blockIdx.x * AT + threadIdx.x;
+  uint64_t vi = gt >> 2;
+  uint32_t q = gt & 3;
+  double sum = 0.0;
+  uint32_t u = 0, d = 0;
+  if (vi < nS) {
+    u = S[vi];
+    d = G.deg[u];
+    if (q * 4 < d) {
+      uint4 v = reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE)[q];
+      sum = __ldg(a.pc + v.x);
+      if (q * 4 + 1 < d) sum += __ldg(a.pc + v.y);
+      if (q * 4 + 2 < d) sum += __ldg(a.pc + v.z);
+      if (q * 4 + 3 < d) sum += __ldg(a.pc + v.w);
+    }
+  }
+  sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 1);
+  sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 2);
+  if (vi < nS && q == 0) pr_store(a, u, d, sum);
+}
+
+__global__ void __launch_bounds__(AT) k_pr_M(DevView G, const uint32_t *M, uint64_t nM, PRArgs a) {
+  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= nM) return;
+  uint32_t u = M[w];
+  uint32_t d = G.deg[u];
+  double sum = 0.0;
+  if (lane < K_INLINE) sum = __ldg(a.pc + G.inl[(uint64_t)u * K_INLINE + lane]);
+  const uint32_t *seg = G.pma + G.pbeg[u];
+  uint32_t rest = d - K_INLINE;
+  uint32_t j = lane;
+  for (; j + 96 < rest; j += 128) {
+    uint32_t i0 = seg[j], i1 = seg[j + 32], i2 = seg[j + 64], i3 = seg[j + 96];
+    sum += __ldg(a.pc + i0) + __ldg(a.pc + i1) + __ldg(a.pc + i2) + __ldg(a.pc + i3);
+  }
+  for (; j < rest; j += 32) sum += __ldg(a.pc + seg[j]);
+  sum = warp_sum(sum);
+  if (lane == 0) pr_store(a, u, d, sum);
+}
+
+__global__ void __launch_bounds__(AT) k_pr_H(DevView G, const uint32_t *Hv, PRArgs a) {
+  __shared__ double sh[AT / 32];
+  uint32_t u = Hv[blockIdx.x];
+  int32_t h = G.hub_of[u];
+  uint32_t d = G.deg[u];
+  uint32_t ni = d < K_INLINE ? d : K_INLINE;
+  double sum = 0.0;
+  if (threadIdx.x < ni) sum = __ldg(a.pc + G.inl[(uint64_t)u * K_INLINE + threadIdx.x]);
+  uint64_t b0 = G.hub_blk0[h];
+  uint32_t nb = G.hub_nblk[h];
+  uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t b = warp; b < nb; b += AT / 32) {
+    uint32_t c = G.bcnt[b0 + b];
+    const uint32_t *blk = G.hslot + (b0 + b) * HUB_BLOCK;
+    for (uint32_t s = lane; s < c; s += 32) sum += __ldg(a.pc + blk[s]);
+  }
+  sum = block_sum(sum, sh);
+  if (threadIdx.x == 0) pr_store(a, u, d, sum);
+}
+
+__global__ void k_pr_init(const uint32_t *deg, uint32_t n, double p0, double iso, double *pdiv,
+                          double *out) {
+  uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  uint32_t d = deg[u];
+  pdiv[u] = p0 / (double)d;
+  if (d == 0) out[u] = iso;
+}
+
+void Graph::pagerank(uint32_t iters, double damping, double *ranks, uint32_t flags) {
+  if (!ranks) throw_error(TRC_ERR_INVALID, "null output");
+  if (damping < 0.0 || damping >= 1.0) throw_error(TRC_ERR_INVALID, "damping must be in [0,1)");
+  ensure_lists();
+  bool dev = flags & TRC_DEVICE_PTR;
+  DBuf<double> pa, pb, ob;
+  pa.bind(&budget);
+  pb.bind(&budget);
+  ob.bind(&budget);
+  double *p0 = pa.alloc_exact(n), *p1 = pb.alloc_exact(n);
+  double *out = dev ? ranks : ob.alloc_exact(n);
+  const double one_over_n = 1.0 / (double)n;
+  const double base = (1.0 - damping) / (double)n;
+  if (iters == 0) {
+    // the reference returns the initial vector 1/n (include/Pagerank.h:137-141)
+    std::vector<double> h(n, one_over_n);
+    TRC_CUDA(cudaMemcpyAsync(out, h.data(), (uint64_t)n * 8, cudaMemcpyHostToDevice, stream));
+    sync();
+  } else {
+    TRC_LAUNCH(prof, stream, "pr_init", ceil_div(n, AT), AT, 0, k_pr_init, deg.get(), n, one_over_n,
+               damping > 0.0 ? base : 0.0, p0, out);
+    DevView G = view();
+    for (uint32_t it = 0; it < iters; it++) {
+      PRArgs a{p0, p1, out, damping, base, it + 1 == iters};
+      TRC_LAUNCH(prof, stream, "pr_S", ceil_div(lists.nS * 4, AT), AT, 0, k_pr_S, G, lists.S.get(),
+                 lists.nS, a);
+      TRC_LAUNCH(prof, stream, "pr_M", ceil_div(lists.nM * 32, AT), AT, 0, k_pr_M, G, lists.M.get(),
+                 lists.nM, a);
+      TRC_LAUNCH(prof, stream, "pr_H", lists.nH, AT, 0, k_pr_H, G, lists.Hv.get(), a);
+      std::swap(p0, p1);
+    }
+  }
+  if (!dev) TRC_CUDA(cudaMemcpyAsync(ranks, out, (uint64_t)n * 8, cudaMemcpyDeviceToHost, stream));
+  sync();
+}
+
+// ---------------------------------------------------------------------------
+// BFS (direction-optimising).  Levels are unique; parents follow the
+// reference: push claims a vertex with CAS (any frontier parent, BFS_F::
+// updateAtomic, include/BFS.h:34-36); pull takes the first frontier
+// neighbour in sorted order (map_dense_vs_not_all breaks on cond,
+// include/graph.h:1489-1613).
+
+struct BFSState {
+  uint32_t *lv;
+  int32_t *par;
+  const uint32_t *bits;  // frontier bitmap (pull)
+  uint32_t *next;        // next-frontier queue
+  uint32_t *next_cnt;
+  uint32_t d;            // current level
+};
+
+__device__ __forceinline__ bool bit_test(const uint32_t *b, uint32_t v) {
+  return (__ldg(b + (v >> 5)) >> (v & 31)) & 1u;
+}
+
+__global__ void k_bfs_push(DevView G, const uint32_t *F, uint32_t nf, BFSState s) {
+  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= nf) return;
+  uint32_t u = F[w];
+  NbrList L = nbr_list(G, u);
+  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) {
+    uint32_t j = j0 + lane;
+    bool win = false;
+    uint32_t v = 0;
+    if (j < L.deg) {
+      v = L.at(j);
+      if (s.lv[v] == TRC_UNREACHED && atomicCAS(&s.par[v], -1, (int32_t)u) == -1) {
+        s.lv[v] = s.d + 1;
+        win = true;
+      }
+    }
+    uint32_t pos = warp_append(win, s.next_cnt);
+    if (win) s.next[pos] = v;
+  }
+}
+
+__global__ void k_set_bits(const uint32_t *F, uint32_t nf, uint32_t *bits) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nf) atomicOr(bits + (F[i] >> 5), 1u << (F[i] & 31));
+}
+
+__global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S, uint64_t nS,
+                                                   BFSState s) {
+  uint64_t gt = (uint64_t)blockIdx.x * AT + threadIdx.x;
+  uint64_t vi = gt >> 2;
+  uint32_t q = gt & 3, lane = threadIdx.x & 31;
+  uint32_t u = 0, first = 4;
+  uint4 v = make_uint4(0, 0, 0, 0);
+  if (vi < nS) {
+    u = S[vi];
+    uint32_t d = G.deg[u];
+    if (s.lv[u] == TRC_UNREACHED && q * 4 < d) {
+      v = reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE)[q];
+      if (bit_test(s.bits, v.x)) first = 0;
+      else if (q * 4 + 1 < d && bit_test(s.bits, v.y)) first = 1;
+      else if (q * 4 + 2 < d && bit_test(s.bits, v.z)) first = 2;
+      else if (q * 4 + 3 < d && bit_test(s.bits, v.w)) first = 3;
+    }
+  }
+  uint32_t m = __ballot_sync(0xFFFFFFFFu, first < 4);
+  uint32_t grp = (m >> (lane & ~3u)) & 0xFu;
+  bool win = grp && (__ffs(grp) - 1) == (int)q;
+  if (win) {
+    uint32_t p = first == 0 ? v.x : first == 1 ? v.y : first == 2 ? v.z : v.w;
+    s.par[u] = (int32_t)p;
+    s.lv[u] = s.d + 1;
+  }
+  uint32_t pos = warp_append(win, s.next_cnt);
+  if (win) s.next[pos] = u;
+}
+
+// One warp scans the neighbours of vertex u in sorted order and stops at
+// the first frontier member.  Returns that neighbour or NONE32 (warp-uniform).
+__device__ __forceinline__ uint32_t warp_first_in_frontier(const NbrList &L, const uint32_t *bits) {
+  uint32_t lane = threadIdx.x & 31;
+  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) {
+    uint32_t j = j0 + lane;
+    uint32_t v = j < L.deg ? L.at(j) : 0;
+    bool hit = j < L.deg && bit_test(bits, v);
+    uint32_t m = __ballot_sync(0xFFFFFFFFu, hit);
+    if (m) return __shfl_sync(0xFFFFFFFFu, v, __ffs(m) - 1);
+  }
+  return NONE32;
+}
+
+// Warp per vertex of a list (M or H class).
+__global__ void __launch_bounds__(AT) k_bfs_pull_W(DevView G, const uint32_t *Lst, uint64_t nL,
+                                                   BFSState s) {
+  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= nL) return;
+  uint32_t u = Lst[w];
+  bool win = false;
+  if (s.lv[u] == TRC_UNREACHED) {
+    NbrList L = nbr_list(G, u);
+    uint32_t p = warp_first_in_frontier(L, s.bits);
+    if (p != NONE32 && lane == 0) {
+      s.par[u] = (int32_t)p;
+      s.lv[u] = s.d + 1;
+      win = true;
+    }
+  }
+  uint32_t pos = warp_append(win, s.next_cnt);
+  if (win) s.next[pos] = u;
+}
+
+__global__ void k_bfs_init(uint32_t *lv, int32_t *par, uint32_t n, uint32_t src, uint32_t *q) {
+  uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  lv[u] = u == src ? 0 : TRC_UNREACHED;
+  par[u] = u == src ? (int32_t)src : -1;
+  if (u == src) q[0] = src;
+}
+
+void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags) {
+  if (src >= n) throw_error(TRC_ERR_INVALID, "source vertex out of range");
+  if (!parents) throw_error(TRC_ERR_INVALID, "null output");
+  ensure_lists();
+  bool dev = flags & TRC_DEVICE_PTR;
+  DBuf<uint32_t> lvb, qa, qb, bits, cnt;
+  DBuf<int32_t> parb;
+  for (auto *b : {&lvb, &qa, &qb, &bits, &cnt}) b->bind(&budget);
+  parb.bind(&budget);
+  uint32_t *lv = (dev && levels) ? levels : lvb.alloc_exact(n);
+  int32_t *par = dev ? parents : parb.alloc_exact(n);
+  uint32_t *F = qa.alloc_exact(n), *Nx = qb.alloc_exact(n);
+  uint64_t words = ceil_div(n, 32);
+  uint32_t *bm = bits.alloc_exact(words);
+  uint32_t *c = cnt.alloc_exact(4);
+  TRC_LAUNCH(prof, stream, "bfs_init", ceil_div(n, AT), AT, 0, k_bfs_init, lv, par, n, src, F);
+  DevView G = view();
+  uint32_t nf = 1, d = 0;
+  const uint64_t dense_at = n / push_pull_divisor();
+  while (nf > 0) {
+    TRC_CUDA(cudaMemsetAsync(c, 0, 4, stream));
+    BFSState s{lv, par, bm, Nx, c, d};
+    if ((uint64_t)nf >= dense_at && dense_at > 0) {
+      TRC_CUDA(cudaMemsetAsync(bm, 0, words * 4, stream));
+      TRC_LAUNCH(prof, stream, "bfs_bits", ceil_div(nf, AT), AT, 0, k_set_bits, F, nf, bm);
+      TRC_LAUNCH(prof, stream, "bfs_pull_S", ceil_div(lists.nS * 4, AT), AT, 0, k_bfs_pull_S, G,
+                 lists.S.get(), lists.nS, s);
+      TRC_LAUNCH(prof, stream, "bfs_pull_M", ceil_div(lists.nM * 32, AT), AT, 0, k_bfs_pull_W, G,
+                 lists.M.get(), lists.nM, s);
+      TRC_LAUNCH(prof, stream, "bfs_pull_H", ceil_div(lists.nH * 32, AT), AT, 0, k_bfs_pull_W, G,
+                 lists.Hv.get(), lists.nH, s);
+    } else {
+      TRC_LAUNCH(prof, stream, "bfs_push", ceil_div((uint64_t)nf * 32, AT), AT, 0, k_bfs_push, G, F,
+                 nf, s);
+    }
+    TRC_CUDA(cudaMemcpyAsync(&nf, c, 4, cudaMemcpyDeviceToHost, stream));
+    sync();
+    std::swap(F, Nx);
+    d++;
+  }
+  if (!dev) {
+    TRC_CUDA(cudaMemcpyAsync(parents, par, (uint64_t)n * 4, cudaMemcpyDeviceToHost, stream));
+    if (levels) TRC_CUDA(cudaMemcpyAsync(levels, lv, (uint64_t)n * 4, cudaMemcpyDeviceToHost, stream));
+  }
+  sync();
+}
+
+// ---------------------------------------------------------------------------
+// CC.  The reference propagates labels with writeMin until no label changes
+// (include/Components.h:92-120); on a symmetric graph that fixed point is the
+// smallest vertex id of each component.  The same fixed point is reached here
+// in one pass over the edges with lock-free union-find (a root is always
+// hooked under a smaller root, so the final root of a component is its
+// smallest id), then a pointer-jumping pass.
+
+__device__ __forceinline__ uint32_t uf_find(uint32_t *p, uint32_t x) {
+  uint32_t px = p[x];
+  while (px != x) {
+    uint32_t gp = p[px];
+    if (gp != px) p[x] = gp;  // path halving (monotone: ids only decrease)
+    x = px;
+    px = p[x];
+  }
+  return x;
+}
+
+__device__ __forceinline__ void uf_unite(uint32_t *p, uint32_t a, uint32_t b) {
+  while (true) {
+    a = uf_find(p, a);
+    b = uf_find(p, b);
+    if (a == b) return;
+    if (a < b) {
+      uint32_t t = a;
+      a = b;
+      b = t;
+    }
+    if (atomicCAS(p + a, a, b) == a) return;
+  }
+}
+
+__global__ void __launch_bounds__(AT) k_cc_S(DevView G, const uint32_t *S, uint64_t nS,
+                                             uint32_t *p) {
+  uint64_t gt = (uint64_t)blockIdx.x * AT + threadIdx.x;
+  uint64_t vi = gt >> 2;
+  uint32_t q = gt & 3;
+  if (vi >= nS) return;
+  uint32_t u = S[vi];
+  uint32_t d = G.deg[u];
+  if (q * 4 >= d) return;
+  uint4 v = reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE)[q];
+  uint32_t e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+    if (q * 4 + i < d && e[i] < u) uf_unite(p, u, e[i]);
+}
+
+__global__ void __launch_bounds__(AT) k_cc_W(DevView G, const uint32_t *Lst, uint64_t nL,
+                                             uint32_t *p) {
+  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= nL) return;
+  uint32_t u = Lst[w];
+  NbrList L = nbr_list(G, u);
+  for (uint32_t j = lane; j < L.deg; j += 32) {
+    uint32_t v = L.at(j);
+    if (v >= u) break;  // sorted: the rest are larger
+    uf_unite(p, u, v);
+  }
+}
+
+__global__ void k_cc_init(uint32_t *p, uint32_t n) {
+  uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < n) p[u] = (uint32_t)u;
+}
+
+__global__ void k_cc_final(uint32_t *p, uint32_t n) {
+  uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  uint32_t x = (uint32_t)u;
+  while (p[x] != x) x = p[x];
+  p[u] = x;
+}
+
+void Graph::cc(uint32_t *labels, uint32_t flags) {
+  if (!labels) throw_error(TRC_ERR_INVALID, "null output");
+  ensure_lists();
+  bool dev = flags & TRC_DEVICE_PTR;
+  DBuf<uint32_t> lb;
+  lb.bind(&budget);
+  uint32_t *p = dev ? labels : lb.alloc_exact(n);
+  DevView G = view();
+  TRC_LAUNCH(prof, stream, "cc_init", ceil_div(n, AT), AT, 0, k_cc_init, p, n);
+  TRC_LAUNCH(prof, stream, "cc_S", ceil_div(lists.nS * 4, AT), AT, 0, k_cc_S, G, lists.S.get(),
+             lists.nS, p);
+  TRC_LAUNCH(prof, stream, "cc_M", ceil_div(lists.nM * 32, AT), AT, 0, k_cc_W, G, lists.M.get(),
+             lists.nM, p);
+  TRC_LAUNCH(prof, stream, "cc_H", ceil_div(lists.nH * 32, AT), AT, 0, k_cc_W, G, lists.Hv.get(),
+             lists.nH, p);
+  TRC_LAUNCH(prof, stream, "cc_final", ceil_div(n, AT), AT, 0, k_cc_final, p, n);
+  if (!dev) TRC_CUDA(cudaMemcpyAsync(labels, p, (uint64_t)n * 4, cudaMemcpyDeviceToHost, stream));
+  sync();
+}
+
+// ---------------------------------------------------------------------------
+// BC from one source (Brandes, as the reference's BC: forward path counts
+// over BFS levels, backward dependency sums, final (Dep - 1/sigma)/(1/sigma)).
+
+struct BCFwd {
+  uint32_t *lv;
+  double *sigma;
+  uint32_t *order;      // order[base ..] receives the next level
+  uint32_t *next_cnt;
+  uint32_t d;
+};
+
+__global__ void k_bc_push(DevView G, const uint32_t *F, uint32_t nf, BCFwd s) {
+  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= nf) return;
+  uint32_t u = F[w];
+  double su = s.sigma[u];
+  NbrList L = nbr_list(G, u);
+  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) {
+    uint32_t j = j0 + lane;
+    bool win = false;
+    uint32_t v = 0;
+    if (j < L.deg) {
+      v = L.at(j);
+      uint32_t lvv = s.lv[v];
+      if (lvv == TRC_UNREACHED) {
+        uint32_t old = atomicCAS(&s.lv[v], TRC_UNREACHED, s.d + 1);
+        win = old == TRC_UNREACHED;
+        lvv = win ? s.d + 1 : old;
+      }
+      if (lvv == s.d + 1) atomicAdd(&s.sigma[v], su);
+    }
+    uint32_t pos = warp_append(win, s.next_cnt);
+    if (win) s.order[pos] = v;
+  }
+}
+
+// Pull for an unvisited vertex: sigma = sum of sigma over neighbours on level d.
+__global__ void __launch_bounds__(AT) k_bc_pull_W(DevView G, const uint32_t *Lst, uint64_t nL,
+                                                  BCFwd s) {
+  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= nL) return;
+  uint32_t u = Lst[w];
+  bool win = false;
+  if (s.lv[u] == TRC_UNREACHED) {
+    NbrList L = nbr_list(G, u);
+    double sum = 0.0;
+    for (uint32_t j = lane; j < L.deg; j += 32) {
+      uint32_t v = L.at(j);
+      if (s.lv[v] == s.d) sum += s.sigma[v];
+    }
+    sum = warp_sum(sum);
+    if (sum > 0.0 && lane == 0) {
+      s.sigma[u] = sum;
+      s.lv[u] = s.d + 1;
+      win = true;
+    }
+  }
+  uint32_t pos = warp_append(win, s.next_cnt);
+  if (win) s.order[pos] = u;
+}
+
+__global__ void __launch_bounds__(AT) k_bc_pull_S(DevView G, const uint32_t *S, uint64_t nS,
+                                                  BCFwd s) {
+  uint64_t gt = (uint64_t)blockIdx.x * AT + threadIdx.x;
+  uint64_t vi = gt >> 2;
+  uint32_t q = gt & 3;
+  double sum = 0.0;
+  uint32_t u = 0;
+  bool cand = false;
+  if (vi < nS) {
+    u = S[vi];
+    uint32_t d = G.deg[u];
+    cand = s.lv[u] == TRC_UNREACHED;
+    if (cand && q * 4 < d) {
+      uint4 v = reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE)[q];
+      uint32_t e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        if (q * 4 + i < d && s.lv[e[i]] == s.d) sum += s.sigma[e[i]];
+    }
+  }
+  sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 1);
+  sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 2);
+  bool win = cand && q == 0 && sum > 0.0;
+  if (win) {
+    s.sigma[u] = sum;
+    s.lv[u] = s.d + 1;
+  }
+  uint32_t pos = warp_append(win, s.next_cnt);
+  if (win) s.order[pos] = u;
+}
+
+// Backward, one warp per vertex of level d:
+// dep[v] = sum of dep[w] over neighbours on level d+1, plus 1/sigma[v].
+__global__ void k_bc_back(DevView G, const uint32_t *Lv, uint32_t nv, const uint32_t *lv,
+                          const double *inv, double *dep, uint32_t d) {
+  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= nv) return;
+  uint32_t u = Lv[w];
+  NbrList L = nbr_list(G, u);
+  double sum = 0.0;
+  for (uint32_t j = lane; j < L.deg; j += 32) {
+    uint32_t v = L.at(j);
+    if (lv[v] == d + 1) sum += dep[v];
+  }
+  sum = warp_sum(sum);
+  if (lane == 0) dep[u] = sum + inv[u];
+}
+
+__global__ void k_bc_init(uint32_t *lv, double *sigma, double *dep, uint32_t n, uint32_t src,
+                          uint32_t *order) {
+  uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  lv[u] = u == src ? 0 : TRC_UNREACHED;
+  sigma[u] = u == src ? 1.0 : 0.0;
+  dep[u] = 0.0;
+  if (u == src) order[0] = src;
+}
+
+__global__ void k_bc_inv(const double *sigma, double *inv, uint32_t n) {
+  uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < n) inv[u] = 1.0 / sigma[u];
+}
+
+__global__ void k_bc_final(const double *dep, const double *inv, double *out, uint32_t n) {
+  uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < n) out[u] = (dep[u] - inv[u]) / inv[u];
+}
+
+void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
+  if (src >= n) throw_error(TRC_ERR_INVALID, "source vertex out of range");
+  if (!out_user) throw_error(TRC_ERR_INVALID, "null output");
+  ensure_lists();
+  bool dev = flags & TRC_DEVICE_PTR;
+  DBuf<uint32_t> lvb, ordb, cntb;
+  DBuf<double> sig, invb, depb, outb;
+  for (auto *b : {&lvb, &ordb, &cntb}) b->bind(&budget);
+  for (auto *b : {&sig, &invb, &depb, &outb}) b->bind(&budget);
+  uint32_t *lv = lvb.alloc_exact(n), *order = ordb.alloc_exact(n), *c = cntb.alloc_exact(4);
+  double *sigma = sig.alloc_exact(n), *inv = invb.alloc_exact(n), *dep = depb.alloc_exact(n);
+  double *out = dev ? out_user : outb.alloc_exact(n);
+  TRC_LAUNCH(prof, stream, "bc_init", ceil_div(n, AT), AT, 0, k_bc_init, lv, sigma, dep, n, src,
+             order);
+  DevView G = view();
+  std::vector<uint64_t> loff = {0, 1};
+  uint32_t d = 0;
+  const uint64_t dense_at = n / push_pull_divisor();
+  while (true) {
+    uint64_t f0 = loff[d], f1 = loff[d + 1];
+    uint32_t nf = (uint32_t)(f1 - f0);
+    if (nf == 0) break;
+    TRC_CUDA(cudaMemsetAsync(c, 0, 4, stream));
+    BCFwd s{lv, sigma, order + f1, c, d};
+    if ((uint64_t)nf >= dense_at && dense_at > 0) {
+      TRC_LAUNCH(prof, stream, "bc_pull_S", ceil_div(lists.nS * 4, AT), AT, 0, k_bc_pull_S, G,
+                 lists.S.get(), lists.nS, s);
+      TRC_LAUNCH(prof, stream, "bc_pull_M", ceil_div(lists.nM * 32, AT), AT, 0, k_bc_pull_W, G,
+                 lists.M.get(), lists.nM, s);
+      TRC_LAUNCH(prof, stream, "bc_pull_H", ceil_div(lists.nH * 32, AT), AT, 0, k_bc_pull_W, G,
+                 lists.Hv.get(), lists.nH, s);
+    } else {
+      TRC_LAUNCH(prof, stream, "bc_push", ceil_div((uint64_t)nf * 32, AT), AT, 0, k_bc_push, G,
+                 order + f0, nf, s);
+    }
+    uint32_t nn = 0;
+    TRC_CUDA(cudaMemcpyAsync(&nn, c, 4, cudaMemcpyDeviceToHost, stream));
+    sync();
+    loff.push_back(f1 + nn);
+    d++;
+  }
+  // d = number of non-empty levels; the last non-empty one is d-1
+  TRC_LAUNCH(prof, stream, "bc_inv", ceil_div(n, AT), AT, 0, k_bc_inv, sigma, inv, n);
+  for (int64_t L = (int64_t)d - 1; L >= 0; L--) {
+    uint64_t a = loff[L], b = loff[L + 1];
+    TRC_LAUNCH(prof, stream, "bc_back", ceil_div((b - a) * 32, AT), AT, 0, k_bc_back, G, order + a,
+               (uint32_t)(b - a), lv, inv, dep, (uint32_t)L);
+  }
+  TRC_LAUNCH(prof, stream, "bc_final", ceil_div(n, AT), AT, 0, k_bc_final, dep, inv, out, n);
+  if (!dev) TRC_CUDA(cudaMemcpyAsync(out_user, out, (uint64_t)n * 8, cudaMemcpyDeviceToHost, stream));
+  sync();
+}
+
+// ---------------------------------------------------------------------------
+// TC.  Every triangle is counted once as w in N+(u) n N+(v) for an oriented
+// edge u->v, where N+(x) keeps the neighbours ranked above x by (degree, id).
+// The reference counts w < min(s,d) over edges s > d (id order, include/TC.h:
+// 51-87); both orders count each triangle exactly once, and the degree order
+// bounds the intersection work on skewed graphs.  N+ is materialised once as
+// an oriented CSR snapshot, then one warp per vertex intersects sorted lists
+// (lanes binary-search the shorter list's elements in the longer one).
+
+__device__ __forceinline__ bool ranked_above(const uint32_t *deg, uint32_t x, uint32_t du,
+                                             uint32_t u) {
+  uint32_t dx = deg[x];
+  return dx > du || (dx == du && x > u);
+}
+
+__global__ void k_tc_count_out(DevView G, uint32_t *outdeg) {
+  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= G.n) return;
+  uint32_t u = (uint32_t)w;
+  NbrList L = nbr_list(G, u);
+  uint32_t c = 0;
+  for (uint32_t j = lane; j < L.deg; j += 32) c += ranked_above(G.deg, L.at(j), L.deg, u);
+  c = warp_sum(c);
+  if (lane == 0) outdeg[u] = c;
+}
+
+struct LoadU32 {
+  const uint32_t *p;
+  __device__ uint64_t operator()(uint64_t i) const { return p[i]; }
+};
+
+__global__ void k_tc_fill(DevView G, const uint64_t *off, uint32_t *adj) {
+  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= G.n) return;
+  uint32_t u = (uint32_t)w;
+  NbrList L = nbr_list(G, u);
+  uint64_t o = off[u];
+  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) {
+    uint32_t j = j0 + lane;
+    uint32_t v = j < L.deg ? L.at(j) : 0;
+    bool keep = j < L.deg && ranked_above(G.deg, v, L.deg, u);
+    uint32_t m = __ballot_sync(0xFFFFFFFFu, keep);
+    if (keep) adj[o + __popc(m & lanemask_lt())] = v;
+    o += __popc(m);
+  }
+}
+
+__global__ void k_tc_intersect(uint32_t n, const uint64_t *off, const uint32_t *adj,
+                               unsigned long long *total) {
+  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= n) return;
+  uint32_t u = (uint32_t)w;
+  const uint32_t *A = adj + off[u];
+  uint32_t na = (uint32_t)(off[u + 1] - off[u]);
+  unsigned long long c = 0;
+  for (uint32_t i = 0; i < na; i++) {
+    uint32_t v = A[i];
+    const uint32_t *B = adj + off[v];
+    uint32_t nb = (uint32_t)(off[v + 1] - off[v]);
+    const uint32_t *Sm = na < nb ? A : B;
+    const uint32_t *Lg = na < nb ? B : A;
+    uint32_t ns = na < nb ? na : nb, nl = na < nb ? nb : na;
+    for (uint32_t j = lane; j < ns; j += 32) {
+      uint32_t x = Sm[j];
+      uint32_t lo = 0, hi = nl;
+      while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (Lg[mid] < x) lo = mid + 1;
+        else hi = mid;
+      }
+      c += (lo < nl && Lg[lo] == x);
+    }
+  }
+  c = warp_sum(c);
+  if (lane == 0 && c) atomicAdd(total, c);
+}
+
+uint64_t Graph::tc() {
+  DBuf<uint32_t> od, adjb;
+  DBuf<uint64_t> offb, tot;
+  od.bind(&budget);
+  adjb.bind(&budget);
+  offb.bind(&budget);
+  tot.bind(&budget);
+  uint32_t *outdeg = od.alloc_exact(n);
+  uint64_t *off = offb.alloc_exact((uint64_t)n + 1);
+  uint64_t *total = tot.alloc_exact(1);
+  DevView G = view();
+  TRC_LAUNCH(prof, stream, "tc_count", ceil_div((uint64_t)n * 32, AT), AT, 0, k_tc_count_out, G,
+             outdeg);
+  uint64_t *t = tmp(scan_tmp_elems(n) + 4);
+  exclusive_scan(LoadU32{outdeg}, n, off, t, stream, prof);
+  uint64_t mo = read_u64(off + n);
+  uint32_t *adj = adjb.alloc_exact(mo ? mo : 1);
+  TRC_LAUNCH(prof, stream, "tc_fill", ceil_div((uint64_t)n * 32, AT), AT, 0, k_tc_fill, G, off, adj);
+  TRC_CUDA(cudaMemsetAsync(total, 0, 8, stream));
+  TRC_LAUNCH(prof, stream, "tc_intersect", ceil_div((uint64_t)n * 32, AT), AT, 0, k_tc_intersect, n,
+             off, adj, (unsigned long long *)total);
+  return read_u64(total);
+}
+
+}  // namespace trc

@@ -1,0 +1,124 @@
+// graph.cuh -- the device-resident three-tier graph (host-side owner of the
+// HBM state) and the declarations of its update, query and analytics paths.
+#pragma once
+
+#include <vector>
+
+#include "prims.cuh"
+
+namespace trc {
+
+constexpr uint64_t KEY_INVALID = ~0ull;
+
+// Lookup of (u, x) in the tiers (used by the update filter and is_edge).
+__device__ __forceinline__ bool has_edge(const DevView &G, uint32_t u, uint32_t x) {
+  if (G.deg[u] == 0) return false;
+  NbrList L = nbr_list(G, u);
+  return list_has(L, x);
+}
+
+// Per-vertex class lists for the analytics kernels, rebuilt when the graph
+// version changes: S = 1..16 neighbours (inline only), M = more than 16 and
+// not a hub (inline + PMA segment), H = hubs.  hub_blocks lists every used
+// hub block (for block-parallel work on the blocked tier).
+struct ClassLists {
+  uint64_t version = ~0ull;
+  DBuf<uint32_t> S, M, Hv, hub_blocks;
+  uint64_t nS = 0, nM = 0, nH = 0, nHB = 0;
+};
+
+class Graph {
+ public:
+  Graph(uint32_t n, uint64_t budget_bytes, const trc_config &cfg);
+  ~Graph();
+
+  // ------------------------------------------------------------- state
+  uint32_t n;
+  trc_config cfg;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  Budget budget;
+  Profiler prof;
+
+  DBuf<uint32_t> deg, inl, c2, pma, err;
+  DBuf<uint64_t> pbeg;
+  DBuf<int32_t> hub_of;
+  // hub tables (device) and their host mirrors
+  DBuf<uint32_t> hub_vtx, hub_nblk, hub_per;
+  DBuf<uint64_t> hub_blk0;
+  std::vector<uint32_t> h_hub_vtx, h_hub_capb;
+  std::vector<uint64_t> h_hub_blk0;
+  uint32_t H = 0;
+  // hub block pool
+  DBuf<uint32_t> hslot, bcnt, bmin, bown;
+  uint64_t NBP = 0;       // pool capacity in blocks
+  uint64_t pool_top = 0;  // blocks handed out
+
+  uint64_t N = 0;          // tier-2 capacity (slots)
+  uint64_t m = 0;          // directed edges
+  uint64_t tier2_total = 0;
+  uint64_t version = 0;
+  uint32_t epoch = 0;
+  DBuf<uint32_t> stamp;    // per-vertex epoch marks for the rewrite set
+  uint64_t rebuilds = 0, window_rebalances = 0;
+
+  // ------------------------------------------------------------- scratch
+  DBuf<uint32_t> s_in_src, s_in_dst;
+  DBuf<uint64_t> s_A, s_B, s_C, s_tmp, s_cnt;
+  DBuf<uint32_t> s_tu, s_tdn, s_tc2, s_ovl, s_hw_u, s_hw_dn, s_hw_t, s_c2n, s_rlist;
+  DBuf<int32_t> s_hw_h;
+  DBuf<uint64_t> s_P, s_oOff, s_nOff, s_wk, s_wk2, s_mw, s_old, s_new, s_hwplan;
+  DBuf<uint8_t> s_flags;
+  DBuf<uint32_t> s_pma_next;
+  ClassLists lists;
+
+  DevView view() const;
+  uint32_t vbits() const;
+
+  // ------------------------------------------------------------- update
+  // Applies a batch; returns the number of directed edges changed.
+  uint64_t apply_batch(const uint32_t *src, const uint32_t *dst, uint64_t k, uint32_t flags,
+                       bool insert);
+
+  // ------------------------------------------------------------- queries
+  void is_edge(const uint32_t *src, const uint32_t *dst, uint64_t q, uint8_t *out, uint32_t flags);
+  void degree(const uint32_t *v, uint64_t q, uint32_t *out, uint32_t flags);
+  uint64_t neighbors(uint32_t v, uint32_t *out, uint64_t cap, uint32_t flags);
+  void count_common(const uint32_t *s, const uint32_t *d, uint64_t q, uint32_t *out,
+                    uint32_t flags);
+  void dump_csr(uint64_t *offsets, uint32_t *targets, uint32_t flags);
+  uint64_t check();
+  uint64_t size_bytes() const;
+  void stats(trc_stats *out);
+
+  // ------------------------------------------------------------- analytics
+  void ensure_lists();
+  void bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags);
+  void pagerank(uint32_t iters, double damping, double *ranks, uint32_t flags);
+  void cc(uint32_t *labels, uint32_t flags);
+  void bc(uint32_t src, double *dep, uint32_t flags);
+  uint64_t tc();
+
+  // helpers
+  uint64_t read_u64(const uint64_t *dptr);
+  void sync();
+  uint32_t push_pull_divisor() const {
+    return cfg.push_pull_divisor ? cfg.push_pull_divisor : 20u;
+  }
+
+ private:
+  void grow_hub_tables(uint32_t need);
+  void grow_pool(uint64_t need_blocks);
+  uint64_t *tmp(uint64_t elems) { return s_tmp.ensure(elems); }
+};
+
+// Copies between user buffers and device scratch, honouring TRC_DEVICE_PTR.
+template <typename T>
+const T *to_device(Graph &g, const T *p, uint64_t count, uint32_t flags, DBuf<T> &stage) {
+  if (flags & TRC_DEVICE_PTR) return p;
+  T *d = stage.ensure(count ? count : 1);
+  if (count) TRC_CUDA(cudaMemcpyAsync(d, p, count * sizeof(T), cudaMemcpyHostToDevice, g.stream));
+  return d;
+}
+
+}  // namespace trc

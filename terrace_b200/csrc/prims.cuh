@@ -1,0 +1,230 @@
+// prims.cuh -- data-parallel primitives for the update pipeline: exclusive
+// scan, order-preserving select (stream compaction), LSD radix sort of
+// 64-bit keys, merge-path merge and sorted difference.  Each primitive is a
+// few tiled kernels; tiles are sized so that a grid is many waves of the
+// 148 SMs for the batch sizes the path sees (1e1..1e9 keys).
+#pragma once
+
+#include "trc_common.cuh"
+
+namespace trc {
+
+constexpr int PT = 256;          // threads per CTA for the primitives
+constexpr int PI = 8;            // items per thread
+constexpr int PTILE = PT * PI;   // 2048 items per tile
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T v) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T t = __shfl_up_sync(0xFFFFFFFFu, v, o);
+    if ((int)lane_id() >= o) v += t;
+  }
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+  return v;
+}
+
+// Block-wide exclusive scan of one value per thread; returns the exclusive
+// prefix and sets `total`.  `ws` is shared scratch of NT/32 entries.
+template <typename T, int NT>
+__device__ __forceinline__ T block_excl_scan(T v, T *ws, T &total) {
+  T inc = warp_incl_scan(v);
+  int w = threadIdx.x >> 5;
+  if (lane_id() == 31) ws[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    T x = (lane_id() < NT / 32) ? ws[lane_id()] : T(0);
+    T xi = warp_incl_scan(x);
+    if (lane_id() < NT / 32) ws[lane_id()] = xi - x;
+    if (lane_id() == NT / 32 - 1) ws[NT / 32] = xi;
+  }
+  __syncthreads();
+  T r = inc - v + ws[w];
+  total = ws[NT / 32];
+  __syncthreads();
+  return r;
+}
+
+// ------------------------------------------------------------------- scan
+// Exclusive scan of f(i), i < n, into out[0..n] (out[n] = total).  The
+// functor returns uint64_t.  Three phases: tile sums, scan of tile sums
+// (recursive), tile scan with the tile offset.
+
+template <typename F>
+__global__ void k_tile_sum(F f, uint64_t n, uint64_t *tile_sums) {
+  __shared__ uint64_t ws[PT / 32 + 1];
+  uint64_t base = (uint64_t)blockIdx.x * PTILE;
+  uint64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < PI; i++) {
+    uint64_t idx = base + (uint64_t)i * PT + threadIdx.x;
+    if (idx < n) s += f(idx);
+  }
+  uint64_t tot;
+  block_excl_scan<uint64_t, PT>(s, ws, tot);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+template <typename F>
+__global__ void k_tile_scan(F f, uint64_t n, const uint64_t *tile_off, uint64_t *out) {
+  __shared__ uint64_t ws[PT / 32 + 1];
+  // each thread owns PI consecutive items
+  uint64_t base = (uint64_t)blockIdx.x * PTILE + (uint64_t)threadIdx.x * PI;
+  uint64_t v[PI];
+  uint64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < PI; i++) {
+    uint64_t idx = base + i;
+    v[i] = idx < n ? f(idx) : 0;
+    s += v[i];
+  }
+  uint64_t tot;
+  uint64_t ex = block_excl_scan<uint64_t, PT>(s, ws, tot);
+  ex += tile_off[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < PI; i++) {
+    uint64_t idx = base + i;
+    if (idx < n) out[idx] = ex;
+    ex += v[i];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == PT - 1) out[n] = ex;
+}
+
+struct LoadU64 {
+  const uint64_t *p;
+  __device__ uint64_t operator()(uint64_t i) const { return p[i]; }
+};
+
+class Scratch;
+
+// Exclusive scan into out[0..n]; tmp needs scan_tmp_elems(n) entries.
+inline uint64_t scan_tmp_elems(uint64_t n) {
+  uint64_t t = ceil_div(n, PTILE);
+  if (t <= 1) return 2;
+  return 2 * t + 1 + scan_tmp_elems(t);
+}
+
+template <typename F>
+void exclusive_scan(F f, uint64_t n, uint64_t *out, uint64_t *tmp, cudaStream_t s, Profiler &prof) {
+  if (n == 0) {
+    TRC_CUDA(cudaMemsetAsync(out, 0, sizeof(uint64_t), s));
+    return;
+  }
+  uint64_t tiles = ceil_div(n, PTILE);
+  if (tiles == 1) {
+    TRC_CUDA(cudaMemsetAsync(tmp, 0, sizeof(uint64_t), s));
+    TRC_LAUNCH(prof, s, "scan_tile", 1, PT, 0, k_tile_scan<F>, f, n, tmp, out);
+    return;
+  }
+  uint64_t *sums = tmp;              // tiles entries
+  uint64_t *offs = tmp + tiles;      // tiles+1 entries
+  TRC_LAUNCH(prof, s, "scan_sum", tiles, PT, 0, k_tile_sum<F>, f, n, sums);
+  exclusive_scan(LoadU64{sums}, tiles, offs, offs + tiles + 1, s, prof);
+  TRC_LAUNCH(prof, s, "scan_tile", tiles, PT, 0, k_tile_scan<F>, f, n, offs, out);
+}
+
+// ----------------------------------------------------------------- select
+// Order-preserving compaction: out[j] = val(i) for the j-th i < n with
+// pred(i).  *count (device) receives the number selected.
+
+template <typename P>
+struct PredCount {
+  P p;
+  __device__ uint64_t operator()(uint64_t i) const { return p(i) ? 1 : 0; }
+};
+
+template <typename P, typename V, typename T>
+__global__ void k_select_scatter(P pred, V val, uint64_t n, const uint64_t *tile_off, T *out,
+                                 uint64_t *count) {
+  __shared__ uint64_t ws[PT / 32 + 1];
+  uint64_t base = (uint64_t)blockIdx.x * PTILE + (uint64_t)threadIdx.x * PI;
+  bool f[PI];
+  uint64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < PI; i++) {
+    uint64_t idx = base + i;
+    f[i] = idx < n && pred(idx);
+    s += f[i];
+  }
+  uint64_t tot;
+  uint64_t ex = block_excl_scan<uint64_t, PT>(s, ws, tot);
+  ex += tile_off[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < PI; i++) {
+    if (f[i]) out[ex++] = val(base + i);
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *count = tile_off[gridDim.x];
+}
+
+template <typename P, typename V, typename T>
+void select_if(P pred, V val, uint64_t n, T *out, uint64_t *count, uint64_t *tmp, cudaStream_t s,
+               Profiler &prof) {
+  if (n == 0) {
+    TRC_CUDA(cudaMemsetAsync(count, 0, sizeof(uint64_t), s));
+    return;
+  }
+  uint64_t tiles = ceil_div(n, PTILE);
+  uint64_t *sums = tmp;
+  uint64_t *offs = tmp + tiles;
+  TRC_LAUNCH(prof, s, "select_count", tiles, PT, 0, k_tile_sum<PredCount<P>>, PredCount<P>{pred}, n,
+             sums);
+  exclusive_scan(LoadU64{sums}, tiles, offs, offs + tiles + 1, s, prof);
+  auto kscatter = k_select_scatter<P, V, T>;
+  TRC_LAUNCH(prof, s, "select_scatter", tiles, PT, 0, kscatter, pred, val, n, offs, out, count);
+}
+
+inline uint64_t select_tmp_elems(uint64_t n) {
+  uint64_t t = ceil_div(n, PTILE);
+  return 2 * t + 1 + scan_tmp_elems(t) + 2;
+}
+
+// ------------------------------------------------------------- radix sort
+// LSD radix sort of 64-bit keys, 8-bit digits, stable.  Only the digit
+// positions listed are sorted (keys are (src<<32)|dst with src,dst < 2^b,
+// so the digits at shifts 0,8,..<b and 32,40,..<32+b suffice).
+constexpr int RS_T = 256;
+constexpr int RS_I = 16;
+constexpr int RS_TILE = RS_T * RS_I;  // 4096 keys
+constexpr int RS_W = RS_T / 32;
+
+__global__ void k_rs_hist(const uint64_t *in, uint64_t n, int shift, uint32_t ntiles,
+                          uint64_t *hist);
+__global__ void k_rs_scatter(const uint64_t *in, uint64_t *out, uint64_t n, int shift,
+                             uint32_t ntiles, const uint64_t *offs);
+
+// Sorts keys[0..n) using alt as the ping-pong buffer; returns the buffer that
+// holds the result (keys or alt).  tmp needs radix_tmp_elems(n) entries.
+uint64_t *radix_sort_u64(uint64_t *keys, uint64_t *alt, uint64_t n, uint32_t vbits,
+                         uint64_t *tmp, cudaStream_t s, Profiler &prof);
+// Same, over an explicit list of 8-bit digit shifts (least significant first).
+uint64_t *radix_sort_u64_shifts(uint64_t *keys, uint64_t *alt, uint64_t n, const int *shifts,
+                                int ns, uint64_t *tmp, cudaStream_t s, Profiler &prof);
+uint64_t radix_tmp_elems(uint64_t n);
+
+// ------------------------------------------------------------ merge path
+// Merge of two sorted u64 arrays without common elements (A first on ties).
+__global__ void k_merge(const uint64_t *A, uint64_t na, const uint64_t *B, uint64_t nb,
+                        uint64_t *out);
+void merge_u64(const uint64_t *A, uint64_t na, const uint64_t *B, uint64_t nb, uint64_t *out,
+               cudaStream_t s, Profiler &prof);
+
+// out = A \ B for sorted unique A and sorted B that is a subset of A.
+// flags: na bytes; tmp: select_tmp_elems(na).
+void difference_u64(const uint64_t *A, uint64_t na, const uint64_t *B, uint64_t nb,
+                    uint64_t *out, uint64_t *count, uint8_t *flags, uint64_t *tmp,
+                    cudaStream_t s, Profiler &prof);
+
+}  // namespace trc

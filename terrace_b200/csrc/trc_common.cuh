@@ -1,0 +1,252 @@
+// trc_common.cuh -- shared definitions of the sm_100a Terrace hot path:
+// the device view of the three degree tiers, error handling, device
+// allocation under an HBM budget, and per-kernel CUDA-event profiling.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "terrace_b200.h"
+
+namespace trc {
+
+// ---------------------------------------------------------------------------
+// Tier constants.
+//
+// Tier 1: the first K_INLINE neighbours of every vertex live in a 64-byte
+// row (one 128-bit load per 4 neighbours).  The reference keeps 13 in-place
+// neighbours because its 64-byte block also holds the degree and a pointer
+// (include/graph.h:34-38, :216-224); here degree and tier pointers live in
+// separate arrays, so the row holds 16.
+constexpr uint32_t K_INLINE = 16;
+// Tier 3: hub neighbours are kept in blocks of HUB_BLOCK slots.
+constexpr uint32_t HUB_BLOCK = 256;
+constexpr uint32_t NONE32 = 0xFFFFFFFFu;
+
+// Device error word bits.
+constexpr uint32_t ERR_BAD_VERTEX = 1u;
+constexpr uint32_t ERR_BOUNDS = 2u;
+constexpr uint32_t ERR_TIMEOUT = 4u;
+
+// ---------------------------------------------------------------------------
+// Device view of the graph, passed to kernels by value.
+//
+//   deg[n]        total degree of every vertex
+//   inl[n*16]     tier 1: sorted neighbours 0..min(deg,16)-1
+//   pbeg[n+1]     tier 2 (packed-memory array over vertex segments): vertex
+//                 u's neighbours 16..deg-1 sit in pma[pbeg[u] .. pbeg[u]+c2[u])
+//                 with slack up to pbeg[u+1]; pbeg[n] = capacity
+//   c2[n]         tier-2 element count (0 for hubs and low-degree vertices)
+//   hub_of[n]     hub index or -1
+//   hub tables    per hub: vertex, first block, blocks used, capacity in
+//                 blocks, elements per block ("per": blocks are filled
+//                 uniformly, so rank r of the hub part is at block r/per,
+//                 slot r%per)
+//   hslot/bcnt/bmin/bown   block pool: slots, count, first key, owner vertex
+struct DevView {
+  uint32_t n;
+  uint32_t hub_T;
+  uint32_t *deg;
+  uint32_t *inl;
+  uint64_t *pbeg;
+  uint32_t *c2;
+  uint32_t *pma;
+  uint64_t N;
+  int32_t *hub_of;
+  uint32_t *hub_vtx;
+  uint64_t *hub_blk0;
+  uint32_t *hub_nblk;
+  uint32_t *hub_per;
+  uint32_t *hslot;
+  uint32_t *bcnt;
+  uint32_t *bmin;
+  uint32_t *bown;
+  uint32_t *err;  // device error word
+};
+
+// Read-only accessor for one vertex's sorted neighbour list by rank.
+struct NbrList {
+  const uint32_t *inl;   // row
+  const uint32_t *seg;   // tier-2 segment (non-hub) or hub slot base
+  uint32_t ni;           // inline count
+  uint32_t rest;         // elements after the inline ones
+  uint32_t per;          // hub: elements per block; 0 = tier-2 segment
+  uint32_t deg;
+
+  __device__ __forceinline__ uint32_t at(uint32_t r) const {
+    if (r < ni) return inl[r];
+    r -= ni;
+    if (per == 0) return seg[r];
+    return seg[(r / per) * HUB_BLOCK + (r % per)];
+  }
+};
+
+__device__ __forceinline__ NbrList nbr_list(const DevView &G, uint32_t u) {
+  NbrList L;
+  uint32_t d = G.deg[u];
+  L.deg = d;
+  L.inl = G.inl + (uint64_t)u * K_INLINE;
+  L.ni = d < K_INLINE ? d : K_INLINE;
+  L.rest = d - L.ni;
+  int32_t h = G.hub_of[u];
+  if (h < 0) {
+    L.seg = G.pma + G.pbeg[u];
+    L.per = 0;
+  } else {
+    L.seg = G.hslot + G.hub_blk0[h] * HUB_BLOCK;
+    L.per = G.hub_per[h] ? G.hub_per[h] : 1;
+  }
+  return L;
+}
+
+// Binary search for x in the neighbour list (lists are sorted, unique).
+__device__ __forceinline__ bool list_has(const NbrList &L, uint32_t x) {
+  uint32_t lo = 0, hi = L.deg;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    uint32_t v = L.at(mid);
+    if (v < x) lo = mid + 1;
+    else if (v > x) hi = mid;
+    else return true;
+  }
+  return false;
+}
+
+// Number of list elements < x.
+__device__ __forceinline__ uint32_t list_lower_bound(const NbrList &L, uint32_t x) {
+  uint32_t lo = 0, hi = L.deg;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (L.at(mid) < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// ---------------------------------------------------------------------------
+// Host-side error handling: internal code throws Error; the C ABI layer
+// converts it into a trc_status plus a thread-local message.
+struct Error {
+  trc_status status;
+  std::string msg;
+};
+
+[[noreturn]] void throw_error(trc_status s, const std::string &msg);
+void cuda_check(cudaError_t e, const char *what, const char *file, int line);
+#define TRC_CUDA(call) ::trc::cuda_check((call), #call, __FILE__, __LINE__)
+
+// ---------------------------------------------------------------------------
+// Device memory under a per-graph HBM budget.
+class Budget {
+ public:
+  uint64_t limit = 0;  // 0 = device free memory is the only limit
+  uint64_t used = 0;
+  void *alloc(uint64_t bytes);
+  void release(void *p, uint64_t bytes);
+};
+
+template <typename T>
+class DBuf {
+ public:
+  DBuf() = default;
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  ~DBuf() { reset(); }
+  void bind(Budget *b) { budget_ = b; }
+  // Ensures capacity for `count` elements; contents are NOT preserved.
+  T *ensure(uint64_t count) {
+    if (count > cap_) {
+      reset();
+      uint64_t c = count < 16 ? 16 : count;
+      ptr_ = static_cast<T *>(budget_->alloc(c * sizeof(T)));
+      cap_ = c;
+    }
+    return ptr_;
+  }
+  // Exactly `count` elements, contents NOT preserved.
+  T *alloc_exact(uint64_t count) {
+    reset();
+    uint64_t c = count < 1 ? 1 : count;
+    ptr_ = static_cast<T *>(budget_->alloc(c * sizeof(T)));
+    cap_ = c;
+    return ptr_;
+  }
+  // Grows to at least `count`, preserving the first `keep` elements.
+  T *grow(uint64_t count, uint64_t keep, cudaStream_t s) {
+    if (count <= cap_) return ptr_;
+    uint64_t c = count < 16 ? 16 : count;
+    T *np = static_cast<T *>(budget_->alloc(c * sizeof(T)));
+    if (keep) TRC_CUDA(cudaMemcpyAsync(np, ptr_, keep * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    TRC_CUDA(cudaStreamSynchronize(s));
+    reset();
+    ptr_ = np;
+    cap_ = c;
+    return ptr_;
+  }
+  void swap(DBuf &o) {
+    std::swap(ptr_, o.ptr_);
+    std::swap(cap_, o.cap_);
+    std::swap(budget_, o.budget_);
+  }
+  void reset() {
+    if (ptr_) budget_->release(ptr_, cap_ * sizeof(T));
+    ptr_ = nullptr;
+    cap_ = 0;
+  }
+  T *get() const { return ptr_; }
+  uint64_t capacity() const { return cap_; }
+  uint64_t bytes() const { return cap_ * sizeof(T); }
+
+ private:
+  T *ptr_ = nullptr;
+  uint64_t cap_ = 0;
+  Budget *budget_ = nullptr;
+};
+
+// ---------------------------------------------------------------------------
+// Per-kernel profiling with CUDA events on the launching stream.
+class Profiler {
+ public:
+  bool on = false;
+  struct Rec {
+    cudaEvent_t a, b;
+    std::string name;
+  };
+  std::vector<Rec> pending;
+  std::map<std::string, std::pair<double, uint64_t>> totals;
+
+  int begin(const char *name, cudaStream_t s);
+  void end(int idx, cudaStream_t s);
+  void resolve();
+  void reset();
+  ~Profiler();
+
+ private:
+  std::vector<cudaEvent_t> pool_;
+  cudaEvent_t get_event();
+};
+
+// Launch wrapper: skips empty grids, records events when profiling, checks
+// the launch error.
+#define TRC_LAUNCH(prof, stream, name, grid, block, smem, kern, ...)          \
+  do {                                                                       \
+    uint64_t _g = (uint64_t)(grid);                                          \
+    if (_g > 0) {                                                            \
+      int _pi = (prof).begin(name, stream);                                  \
+      kern<<<(unsigned)_g, (block), (smem), (stream)>>>(__VA_ARGS__);        \
+      (prof).end(_pi, stream);                                               \
+      TRC_CUDA(cudaGetLastError());                                          \
+    }                                                                        \
+  } while (0)
+
+inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+
+// Number of SMs on the current device (cached).
+int num_sms();
+
+}  // namespace trc

@@ -1,0 +1,707 @@
+// update.cu -- the graph's HBM state and the batch update pipeline.
+//
+// Replaces Graph::add_edge_batch (include/graph.h:430-502, with add_inplace
+// :251-372, add_btree :375-426 and the per-edge PMA inserts of
+// src/PMA.cc:2050-2108, :1253-1513) and the per-edge remove loop
+// (include/graph.h:675-791, src/PMA.cc:2800-2873).  Instead of per-edge
+// inserts under spin locks, a whole batch goes through one device pipeline:
+//
+//   1  keys (src<<32|dst), symmetrized on request; ids validated
+//   2  LSD radix sort + adjacent unique
+//   3  existence filter against the tiers (insert keeps new edges, remove
+//      keeps present ones) -> the batch B, sorted
+//   4  touched vertices (runs of B by source), new degree and tier of each:
+//      deg <= 16 inline only, > hub_threshold (or already a hub) blocked
+//      tier, otherwise inline + PMA segment
+//   5  PMA planning: a vertex whose new segment does not fit its slots
+//      triggers the packed-memory-array rule -- climb the implicit tree of
+//      aligned vertex ranges until a window's density is within the bound of
+//      its level (1.0 at a single vertex down to pma_root_density at the
+//      root), rebalance the maximal such windows, or rebuild the whole PMA
+//      at pma_build_density when the root overflows (the reference's
+//      density bounds, src/PMA.cc:382-394, redistribute :419-655,
+//      double_list :659-720)
+//   6  rewrite set R = touched vertices + vertices of rebalanced windows
+//      (+ every PMA vertex on a rebuild); their old lists are gathered as
+//      sorted 64-bit keys, merged with B (insert) or stripped of B (remove)
+//      by merge path, and scattered back: first 16 to the inline row, the
+//      rest to the PMA segment at its (possibly new) offset or to the hub's
+//      blocks (uniformly filled, hub_block_fill).
+//
+// Set semantics throughout: the reference's duplicate leak (include/graph.h:
+// 269-289) and absent-edge remove (include/graph.h:695-716) do not occur.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "graph.cuh"
+
+namespace trc {
+
+// ---------------------------------------------------------------------------
+// Lifetime
+
+Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_), cfg(cfg_) {
+  budget.limit = budget_bytes;
+  TRC_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+  stream = own_stream;
+  for (auto *b : {&deg, &inl, &c2, &pma, &err, &hub_vtx, &hub_nblk, &hub_per, &hslot, &bcnt, &bmin,
+                  &bown, &stamp, &s_in_src, &s_in_dst, &s_tu, &s_tdn, &s_tc2, &s_ovl, &s_hw_u,
+                  &s_hw_dn, &s_hw_t, &s_c2n, &s_rlist, &s_pma_next, &lists.S, &lists.M, &lists.Hv,
+                  &lists.hub_blocks})
+    b->bind(&budget);
+  for (auto *b : {&pbeg, &hub_blk0, &s_A, &s_B, &s_C, &s_tmp, &s_cnt, &s_P, &s_oOff, &s_nOff,
+                  &s_wk, &s_wk2, &s_mw, &s_old, &s_new, &s_hwplan})
+    b->bind(&budget);
+  hub_of.bind(&budget);
+  s_hw_h.bind(&budget);
+  s_flags.bind(&budget);
+
+  uint64_t nn = n ? n : 1;
+  deg.alloc_exact(nn);
+  inl.alloc_exact(nn * K_INLINE);
+  c2.alloc_exact(nn);
+  pbeg.alloc_exact(nn + 1);
+  hub_of.alloc_exact(nn);
+  stamp.alloc_exact(nn);
+  err.alloc_exact(4);
+  s_cnt.alloc_exact(32);
+  pma.alloc_exact(1);
+  N = 0;
+  TRC_CUDA(cudaMemsetAsync(deg.get(), 0, nn * 4, stream));
+  TRC_CUDA(cudaMemsetAsync(inl.get(), 0, nn * K_INLINE * 4, stream));
+  TRC_CUDA(cudaMemsetAsync(c2.get(), 0, nn * 4, stream));
+  TRC_CUDA(cudaMemsetAsync(pbeg.get(), 0, (nn + 1) * 8, stream));
+  TRC_CUDA(cudaMemsetAsync(hub_of.get(), 0xFF, nn * 4, stream));
+  TRC_CUDA(cudaMemsetAsync(stamp.get(), 0, nn * 4, stream));
+  TRC_CUDA(cudaMemsetAsync(err.get(), 0, 16, stream));
+  grow_hub_tables(64);
+  grow_pool(64);
+  sync();
+}
+
+Graph::~Graph() {
+  if (own_stream) cudaStreamSynchronize(own_stream);
+  if (stream && stream != own_stream) cudaStreamSynchronize(stream);
+  prof.reset();
+  if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+DevView Graph::view() const {
+  DevView v;
+  v.n = n;
+  v.hub_T = cfg.hub_threshold;
+  v.deg = deg.get();
+  v.inl = inl.get();
+  v.pbeg = pbeg.get();
+  v.c2 = c2.get();
+  v.pma = pma.get();
+  v.N = N;
+  v.hub_of = hub_of.get();
+  v.hub_vtx = hub_vtx.get();
+  v.hub_blk0 = hub_blk0.get();
+  v.hub_nblk = hub_nblk.get();
+  v.hub_per = hub_per.get();
+  v.hslot = hslot.get();
+  v.bcnt = bcnt.get();
+  v.bmin = bmin.get();
+  v.bown = bown.get();
+  v.err = err.get();
+  return v;
+}
+
+uint32_t Graph::vbits() const {
+  uint32_t b = 1;
+  while (b < 32 && (1ull << b) < (uint64_t)n) b++;
+  return b;
+}
+
+void Graph::sync() { TRC_CUDA(cudaStreamSynchronize(stream)); }
+
+uint64_t Graph::read_u64(const uint64_t *dptr) {
+  uint64_t v = 0;
+  TRC_CUDA(cudaMemcpyAsync(&v, dptr, 8, cudaMemcpyDeviceToHost, stream));
+  sync();
+  return v;
+}
+
+void Graph::grow_hub_tables(uint32_t need) {
+  uint64_t cap = hub_vtx.capacity();
+  if (need <= cap && cap) return;
+  uint64_t nc = std::max<uint64_t>(need, cap * 2);
+  hub_vtx.grow(nc, H, stream);
+  hub_nblk.grow(nc, H, stream);
+  hub_per.grow(nc, H, stream);
+  hub_blk0.grow(nc, H, stream);
+}
+
+void Graph::grow_pool(uint64_t need_blocks) {
+  if (need_blocks <= NBP) return;
+  uint64_t nc = std::max<uint64_t>(need_blocks, NBP * 2);
+  hslot.grow(nc * HUB_BLOCK, pool_top * HUB_BLOCK, stream);
+  bcnt.grow(nc, pool_top, stream);
+  bmin.grow(nc, pool_top, stream);
+  bown.grow(nc, pool_top, stream);
+  NBP = nc;
+}
+
+// ---------------------------------------------------------------------------
+// Kernels of the pipeline
+
+__global__ void k_make_keys(const uint32_t *src, const uint32_t *dst, uint64_t k, uint32_t n,
+                            int sym, int drop_self, uint64_t *keys, uint32_t *err) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= k) return;
+  uint32_t s = src[i], d = dst[i];
+  uint64_t a = KEY_INVALID, b = KEY_INVALID;
+  if (s >= n || d >= n) {
+    atomicOr(err, ERR_BAD_VERTEX);
+  } else if (!(drop_self && s == d)) {
+    a = ((uint64_t)s << 32) | d;
+    b = ((uint64_t)d << 32) | s;
+  }
+  if (sym) {
+    keys[2 * i] = a;
+    keys[2 * i + 1] = b;
+  } else {
+    keys[i] = a;
+  }
+}
+
+struct UniquePred {
+  const uint64_t *k;
+  __device__ bool operator()(uint64_t i) const {
+    uint64_t x = k[i];
+    return x != KEY_INVALID && (i == 0 || k[i - 1] != x);
+  }
+};
+
+struct ExistPred {
+  DevView G;
+  const uint64_t *keys;
+  const uint64_t *count;
+  int insert;
+  __device__ bool operator()(uint64_t i) const {
+    if (i >= *count) return false;
+    uint64_t x = keys[i];
+    bool has = has_edge(G, (uint32_t)(x >> 32), (uint32_t)x);
+    return insert ? !has : has;
+  }
+};
+
+struct RunStartPred {
+  const uint64_t *keys;
+  const uint64_t *count;
+  __device__ bool operator()(uint64_t i) const {
+    if (i >= *count) return false;
+    return i == 0 || (keys[i] >> 32) != (keys[i - 1] >> 32);
+  }
+};
+
+struct IndexVal {
+  __device__ uint64_t operator()(uint64_t i) const { return i; }
+};
+
+// Counters in s_cnt (device u64 array)
+enum {
+  C_KU = 0,
+  C_KB,
+  C_NT,
+  C_NOV,
+  C_NH,
+  C_ROOT,
+  C_NW,
+  C_NMW,
+  C_NR,
+  C_T2DELTA,
+  C_COUNT
+};
+
+// Classify touched vertices (step 4).
+__global__ void k_classify(DevView G, const uint64_t *bkeys, const uint64_t *tpos, uint64_t nt,
+                           uint64_t kb, int insert, uint32_t *tu, uint32_t *tdn, uint32_t *tc2,
+                           uint32_t *ovl, uint32_t *hw_u, uint32_t *hw_dn, uint32_t *hw_t,
+                           int32_t *hw_h, uint64_t *cnt) {
+  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  uint64_t p0 = tpos[t];
+  uint64_t p1 = t + 1 < nt ? tpos[t + 1] : kb;
+  uint32_t u = (uint32_t)(bkeys[p0] >> 32);
+  uint32_t c = (uint32_t)(p1 - p0);
+  uint32_t d = G.deg[u];
+  uint32_t dn = insert ? d + c : d - c;
+  int32_t h = G.hub_of[u];
+  bool hub = h >= 0 || dn > G.hub_T;
+  uint32_t nc2 = (!hub && dn > K_INLINE) ? dn - K_INLINE : 0;
+  tu[t] = u;
+  tdn[t] = dn;
+  tc2[t] = nc2;
+  int64_t delta = (int64_t)nc2 - (int64_t)G.c2[u];
+  if (delta) atomicAdd((unsigned long long *)&cnt[C_T2DELTA], (unsigned long long)delta);
+  if (!hub && (uint64_t)nc2 > G.pbeg[u + 1] - G.pbeg[u]) {
+    uint64_t j = atomicAdd((unsigned long long *)&cnt[C_NOV], 1ull);
+    ovl[j] = u;
+  }
+  if (hub) {
+    uint64_t j = atomicAdd((unsigned long long *)&cnt[C_NH], 1ull);
+    hw_u[j] = u;
+    hw_dn[j] = dn;
+    hw_t[j] = (uint32_t)t;
+    hw_h[j] = h;
+  }
+}
+
+__global__ void k_scatter_c2(const uint32_t *tu, const uint32_t *tc2, uint64_t nt, uint32_t *c2n) {
+  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nt) c2n[tu[t]] = tc2[t];
+}
+
+struct LoadC2 {
+  const uint32_t *c;
+  __device__ uint64_t operator()(uint64_t i) const { return c[i]; }
+};
+
+// Window search (step 5): lowest level whose aligned vertex range has
+// density within its bound.  Keys sort by (start asc, level desc).
+__global__ void k_find_windows(const uint32_t *ovl, uint64_t nov, const uint64_t *P,
+                               const uint64_t *pbeg, uint32_t n, uint32_t levels, double root_dens,
+                               uint64_t *wkeys, uint64_t *cnt) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nov) return;
+  uint32_t u = ovl[i];
+  for (uint32_t h = 1; h <= levels; h++) {
+    uint64_t a = ((uint64_t)u >> h) << h;
+    uint64_t b = a + (1ull << h);
+    if (b > n) b = n;
+    uint64_t E = P[b] - P[a];
+    uint64_t S = pbeg[b] - pbeg[a];
+    double tau = 1.0 - (1.0 - root_dens) * (double)h / (double)levels;
+    if ((double)E <= tau * (double)S) {
+      wkeys[i] = (a << 6) | (uint64_t)(63 - h);
+      return;
+    }
+  }
+  wkeys[i] = KEY_INVALID;
+  atomicOr((unsigned long long *)&cnt[C_ROOT], 1ull);
+}
+
+// A sorted unique window is maximal when no enclosing window (same range
+// at a higher level) was also chosen.
+struct MaximalWindowPred {
+  const uint64_t *w;
+  uint64_t nw;
+  uint32_t levels;
+  __device__ bool operator()(uint64_t i) const {
+    uint64_t x = w[i];
+    if (i > 0 && w[i - 1] == x) return false;  // duplicate
+    uint64_t a = x >> 6;
+    uint32_t h = 63 - (uint32_t)(x & 63);
+    for (uint32_t hh = h + 1; hh <= levels; hh++) {
+      uint64_t aa = (a >> hh) << hh;
+      uint64_t key = (aa << 6) | (uint64_t)(63 - hh);
+      uint64_t lo = 0, hi = nw;
+      while (lo < hi) {
+        uint64_t mid = (lo + hi) >> 1;
+        if (w[mid] < key) lo = mid + 1;
+        else hi = mid;
+      }
+      if (lo < nw && w[lo] == key) return false;
+    }
+    return true;
+  }
+};
+
+struct LoadU64Val {
+  const uint64_t *p;
+  __device__ uint64_t operator()(uint64_t i) const { return p[i]; }
+};
+
+__global__ void k_mark_touched(const uint32_t *tu, uint64_t nt, uint32_t *stamp, uint32_t epoch) {
+  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nt) stamp[tu[t]] = epoch;
+}
+
+__device__ __forceinline__ void window_range(uint64_t x, uint32_t n, uint64_t &a, uint64_t &b) {
+  a = x >> 6;
+  uint32_t h = 63 - (uint32_t)(x & 63);
+  b = a + (1ull << h);
+  if (b > n) b = n;
+}
+
+// One CTA per maximal window: put its vertices in the rewrite set.
+__global__ void k_window_mark(const uint64_t *mw, uint32_t n, uint32_t *stamp, uint32_t epoch) {
+  uint64_t a, b;
+  window_range(mw[blockIdx.x], n, a, b);
+  for (uint64_t u = a + threadIdx.x; u < b; u += blockDim.x) stamp[u] = epoch;
+}
+
+// One CTA per maximal window: new segment offsets of its vertices,
+// pbeg'[u] = pbeg[a] + (P[u]-P[a]) + floor(gap*(P[u]-P[a])/E); the window's
+// slot range [pbeg[a], pbeg[b]) is unchanged.
+__global__ void k_window_layout(const uint64_t *mw, uint32_t n, const uint64_t *P, uint64_t *pbeg) {
+  uint64_t a, b;
+  window_range(mw[blockIdx.x], n, a, b);
+  uint64_t base = pbeg[a];
+  uint64_t S = pbeg[b] - base;
+  uint64_t E = P[b] - P[a];
+  uint64_t gap = S - E;
+  __syncthreads();  // every thread has read pbeg[a], pbeg[b] before any write
+  for (uint64_t u = a + 1 + threadIdx.x; u < b; u += blockDim.x) {
+    uint64_t e = P[u] - P[a];
+    unsigned __int128 q = (unsigned __int128)gap * e;
+    pbeg[u] = base + e + (uint64_t)(q / E);
+  }
+}
+
+// Rebuild layout: every vertex, target density; pbeg'[n] = N'.
+__global__ void k_rebuild_layout(const uint64_t *P, uint32_t n, uint64_t Nn, uint64_t *pbeg) {
+  uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u > n) return;
+  uint64_t tot = P[n];
+  uint64_t gap = Nn - tot;
+  uint64_t e = P[u];
+  uint64_t extra = tot ? (uint64_t)(((unsigned __int128)gap * e) / tot) : 0;
+  pbeg[u] = (u == n) ? Nn : e + extra;
+}
+
+__global__ void k_mark_pma_vertices(const uint32_t *c2n, uint32_t n, uint32_t *stamp, uint32_t epoch) {
+  uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < n && c2n[u] > 0) stamp[u] = epoch;
+}
+
+struct StampPred {
+  const uint32_t *stamp;
+  uint32_t epoch;
+  __device__ bool operator()(uint64_t i) const { return stamp[i] == epoch; }
+};
+
+struct IndexVal32 {
+  __device__ uint32_t operator()(uint64_t i) const { return (uint32_t)i; }
+};
+
+struct OldDeg {
+  const uint32_t *rlist, *deg;
+  __device__ uint64_t operator()(uint64_t i) const { return deg[rlist[i]]; }
+};
+
+// New degree of a rewrite-set vertex: from the touched table when touched.
+struct NewDeg {
+  const uint32_t *rlist, *deg, *tu, *tdn;
+  uint64_t nt;
+  __device__ uint64_t operator()(uint64_t i) const {
+    uint32_t u = rlist[i];
+    uint64_t lo = 0, hi = nt;
+    while (lo < hi) {
+      uint64_t mid = (lo + hi) >> 1;
+      if (tu[mid] < u) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo < nt && tu[lo] == u) return tdn[lo];
+    return deg[u];
+  }
+};
+
+// Gather old lists of the rewrite set as sorted 64-bit keys (warp/vertex).
+__global__ void k_gather_old(DevView G, const uint32_t *rlist, uint64_t nr, const uint64_t *oOff,
+                             uint64_t *out) {
+  uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= nr) return;
+  uint32_t u = rlist[w];
+  NbrList L = nbr_list(G, u);
+  uint64_t base = oOff[w];
+  uint64_t hi = (uint64_t)u << 32;
+  for (uint32_t j = lane; j < L.deg; j += 32) out[base + j] = hi | L.at(j);
+}
+
+// Hub table update from the host plan.  plan rows: {h, u, blk0, nb, per, capb}.
+__global__ void k_apply_hub_plan(DevView G, const uint64_t *plan, uint64_t nh) {
+  uint64_t i = blockIdx.x;
+  if (i >= nh) return;
+  const uint64_t *p = plan + 6 * i;
+  uint32_t h = (uint32_t)p[0], u = (uint32_t)p[1];
+  uint64_t blk0 = p[2];
+  uint32_t nb = (uint32_t)p[3], per = (uint32_t)p[4], capb = (uint32_t)p[5];
+  if (threadIdx.x == 0) {
+    G.hub_vtx[h] = u;
+    G.hub_blk0[h] = blk0;
+    G.hub_nblk[h] = nb;
+    G.hub_per[h] = per;
+    G.hub_of[u] = (int32_t)h;
+  }
+  for (uint32_t b = nb + threadIdx.x; b < capb; b += blockDim.x) {
+    G.bcnt[blk0 + b] = 0;
+    G.bown[blk0 + b] = NONE32;
+  }
+}
+
+// Scatter new lists of the rewrite set into the tiers (warp/vertex).
+__global__ void k_scatter_new(DevView G, const uint32_t *rlist, uint64_t nr, const uint64_t *nOff,
+                              const uint64_t *src) {
+  uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= nr) return;
+  uint32_t u = rlist[w];
+  uint64_t base = nOff[w];
+  uint32_t dn = (uint32_t)(nOff[w + 1] - base);
+  uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
+  uint32_t ni = dn < K_INLINE ? dn : K_INLINE;
+  if (lane < ni) row[lane] = (uint32_t)src[base + lane];
+  if (dn > K_INLINE) {
+    uint32_t rest = dn - K_INLINE;
+    int32_t h = G.hub_of[u];
+    if (h < 0) {
+      uint32_t *dst = G.pma + G.pbeg[u];
+      for (uint32_t j = lane; j < rest; j += 32) dst[j] = (uint32_t)src[base + K_INLINE + j];
+    } else {
+      uint64_t blk0 = G.hub_blk0[h];
+      uint32_t per = G.hub_per[h];
+      for (uint32_t j = lane; j < rest; j += 32) {
+        uint32_t b = j / per, s = j - b * per;
+        uint32_t v = (uint32_t)src[base + K_INLINE + j];
+        G.hslot[(blk0 + b) * HUB_BLOCK + s] = v;
+        if (s == 0) {
+          uint32_t c = rest - b * per;
+          G.bcnt[blk0 + b] = c < per ? c : per;
+          G.bmin[blk0 + b] = v;
+          G.bown[blk0 + b] = u;
+        }
+      }
+    }
+  }
+  if (lane == 0) G.deg[u] = dn;
+}
+
+__global__ void k_scatter_c2_final(const uint32_t *tu, const uint32_t *tc2, uint64_t nt,
+                                   uint32_t *c2) {
+  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nt) c2[tu[t]] = tc2[t];
+}
+
+// ---------------------------------------------------------------------------
+// The pipeline
+
+uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint64_t k,
+                            uint32_t flags, bool insert) {
+  if (k == 0) return 0;
+  if (!src_in || !dst_in) throw_error(TRC_ERR_INVALID, "null edge array");
+  const int sym = (flags & TRC_SYMMETRIZE) ? 1 : 0;
+  const int drop = (flags & TRC_DROP_SELF_LOOPS) ? 1 : 0;
+  const uint32_t *src = to_device(*this, src_in, k, flags, s_in_src);
+  const uint32_t *dst = to_device(*this, dst_in, k, flags, s_in_dst);
+  const uint64_t k2 = sym ? 2 * k : k;
+  DevView G = view();
+  uint64_t *cnt = s_cnt.get();
+  TRC_CUDA(cudaMemsetAsync(cnt, 0, 32 * 8, stream));
+  TRC_CUDA(cudaMemsetAsync(err.get(), 0, 4, stream));
+
+  // 1-2: keys, sort, unique
+  uint64_t *A = s_A.ensure(k2), *B = s_B.ensure(k2);
+  TRC_LAUNCH(prof, stream, "upd_make_keys", ceil_div(k, 256), 256, 0, k_make_keys, src, dst, k, n,
+             sym, drop, A, err.get());
+  uint64_t *t = tmp(std::max(radix_tmp_elems(k2), select_tmp_elems(k2)));
+  uint64_t *sorted = radix_sort_u64(A, B, k2, vbits(), t, stream, prof);
+  uint64_t *other = sorted == A ? B : A;
+  select_if(UniquePred{sorted}, LoadU64Val{sorted}, k2, other, cnt + C_KU, t, stream, prof);
+  uint64_t *ukeys = other;
+  uint64_t *bkeys = sorted;  // sorted buffer is free now
+  // 3: existence filter
+  select_if(ExistPred{G, ukeys, cnt + C_KU, insert ? 1 : 0}, LoadU64Val{ukeys}, k2, bkeys,
+            cnt + C_KB, t, stream, prof);
+  // 4: runs by source
+  uint64_t *tpos = s_C.ensure(k2);
+  select_if(RunStartPred{bkeys, cnt + C_KB}, IndexVal{}, k2, tpos, cnt + C_NT, t, stream, prof);
+  uint64_t hc[C_COUNT];
+  uint32_t herr = 0;
+  TRC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, stream));
+  TRC_CUDA(cudaMemcpyAsync(&herr, err.get(), 4, cudaMemcpyDeviceToHost, stream));
+  sync();
+  if (herr & ERR_BAD_VERTEX) throw_error(TRC_ERR_INVALID, "vertex id out of range [0, n)");
+  const uint64_t kb = hc[C_KB], nt = hc[C_NT];
+  if (kb == 0) return 0;
+
+  uint32_t *tu = s_tu.ensure(nt), *tdn = s_tdn.ensure(nt), *tc2 = s_tc2.ensure(nt);
+  uint32_t *ovl = s_ovl.ensure(nt);
+  uint32_t *hw_u = s_hw_u.ensure(nt), *hw_dn = s_hw_dn.ensure(nt), *hw_t = s_hw_t.ensure(nt);
+  int32_t *hw_h = s_hw_h.ensure(nt);
+  TRC_LAUNCH(prof, stream, "upd_classify", ceil_div(nt, 256), 256, 0, k_classify, G, bkeys, tpos,
+             nt, kb, insert ? 1 : 0, tu, tdn, tc2, ovl, hw_u, hw_dn, hw_t, hw_h, cnt);
+  TRC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, stream));
+  sync();
+  const uint64_t nov = hc[C_NOV], nh = hc[C_NH];
+  const int64_t t2delta = (int64_t)hc[C_T2DELTA];
+  const uint64_t t2new = (uint64_t)((int64_t)tier2_total + t2delta);
+
+  // ---- hub plan (host): indices for new hubs, regions for grown ones.
+  std::vector<uint64_t> plan;
+  if (nh) {
+    std::vector<uint32_t> hu(nh), hdn(nh);
+    std::vector<int32_t> hh(nh);
+    TRC_CUDA(cudaMemcpyAsync(hu.data(), hw_u, nh * 4, cudaMemcpyDeviceToHost, stream));
+    TRC_CUDA(cudaMemcpyAsync(hdn.data(), hw_dn, nh * 4, cudaMemcpyDeviceToHost, stream));
+    TRC_CUDA(cudaMemcpyAsync(hh.data(), hw_h, nh * 4, cudaMemcpyDeviceToHost, stream));
+    sync();
+    plan.resize(6 * nh);
+    const double fill = cfg.hub_block_fill > 0 && cfg.hub_block_fill <= 1 ? cfg.hub_block_fill : 0.75;
+    const uint64_t blk_target = std::max<uint64_t>(1, (uint64_t)(HUB_BLOCK * fill));
+    uint64_t need_top = pool_top;
+    for (uint64_t i = 0; i < nh; i++) {
+      int32_t h = hh[i];
+      if (h < 0) {
+        h = (int32_t)H++;
+        h_hub_vtx.push_back(hu[i]);
+        h_hub_blk0.push_back(0);
+        h_hub_capb.push_back(0);
+      }
+      uint64_t rest = hdn[i] > K_INLINE ? hdn[i] - K_INLINE : 0;
+      uint64_t nb = rest ? ceil_div(rest, blk_target) : 0;
+      uint64_t per = nb ? ceil_div(rest, nb) : 0;
+      if (nb > h_hub_capb[h]) {
+        uint64_t capb = std::max<uint64_t>(nb + nb / 2, 2);
+        h_hub_blk0[h] = need_top;
+        h_hub_capb[h] = (uint32_t)capb;
+        need_top += capb;
+      }
+      uint64_t *p = &plan[6 * i];
+      p[0] = (uint64_t)h;
+      p[1] = hu[i];
+      p[2] = h_hub_blk0[h];
+      p[3] = nb;
+      p[4] = per;
+      p[5] = h_hub_capb[h];
+    }
+    grow_hub_tables(H);
+    grow_pool(need_top);
+    pool_top = need_top;
+    G = view();
+  }
+
+  // ---- PMA planning
+  bool rebuild = false;
+  uint64_t nmw = 0;
+  uint64_t Nn = N;
+  uint32_t *c2n = nullptr;
+  uint64_t *P = nullptr;
+  const double root_d = (cfg.pma_root_density > 0 && cfg.pma_root_density < 1) ? cfg.pma_root_density : 0.75;
+  const double build_d = (cfg.pma_build_density > 0 && cfg.pma_build_density < 1) ? cfg.pma_build_density : 0.5;
+  uint32_t levels = 1;
+  while (levels < 32 && (1ull << levels) < (uint64_t)n) levels++;
+  bool shrink = !insert && N > (1ull << 20) && (double)t2new < 0.125 * (double)N;
+  if (nov > 0 || shrink) {
+    c2n = s_c2n.ensure(n);
+    TRC_CUDA(cudaMemcpyAsync(c2n, c2.get(), (uint64_t)n * 4, cudaMemcpyDeviceToDevice, stream));
+    TRC_LAUNCH(prof, stream, "upd_scatter_c2", ceil_div(nt, 256), 256, 0, k_scatter_c2, tu, tc2, nt,
+               c2n);
+    P = s_P.ensure((uint64_t)n + 1);
+    uint64_t *st = tmp(scan_tmp_elems(n) + 4);
+    exclusive_scan(LoadC2{c2n}, n, P, st, stream, prof);
+    if (shrink || (double)t2new > root_d * (double)N) {
+      rebuild = true;
+    } else {
+      uint64_t *wk = s_wk.ensure(nov), *wk2 = s_wk2.ensure(nov);
+      TRC_LAUNCH(prof, stream, "upd_find_windows", ceil_div(nov, 256), 256, 0, k_find_windows, ovl,
+                 nov, P, pbeg.get(), n, levels, root_d, wk, cnt);
+      uint64_t root = read_u64(cnt + C_ROOT);
+      if (root) {
+        rebuild = true;
+      } else {
+        uint64_t *t2 = tmp(radix_tmp_elems(nov) + 4);
+        // window keys: start (< 2^32) << 6 | level code -> the low 38 bits
+        const int wshifts[5] = {0, 8, 16, 24, 32};
+        uint64_t *ws = radix_sort_u64_shifts(wk, wk2, nov, wshifts, 5, t2, stream, prof);
+        uint64_t *mw = s_mw.ensure(nov);
+        uint64_t *t3 = tmp(select_tmp_elems(nov) + 4);
+        select_if(MaximalWindowPred{ws, nov, levels}, LoadU64Val{ws}, nov, mw, cnt + C_NMW, t3,
+                  stream, prof);
+        nmw = read_u64(cnt + C_NMW);
+      }
+    }
+  }
+
+  // ---- rewrite set R
+  epoch++;
+  if (epoch == 0) {  // wrapped: clear stamps
+    TRC_CUDA(cudaMemsetAsync(stamp.get(), 0, (uint64_t)n * 4, stream));
+    epoch = 1;
+  }
+  TRC_LAUNCH(prof, stream, "upd_mark", ceil_div(nt, 256), 256, 0, k_mark_touched, tu, nt,
+             stamp.get(), epoch);
+  if (nmw)
+    TRC_LAUNCH(prof, stream, "upd_window_mark", nmw, 256, 0, k_window_mark, s_mw.get(), n,
+               stamp.get(), epoch);
+  uint64_t Ptot = 0;
+  if (rebuild) {
+    Ptot = read_u64(P + n);  // the layout kernel spreads exactly this many
+    Nn = std::max<uint64_t>((uint64_t)std::ceil((double)Ptot / build_d), Ptot + 1);
+    TRC_LAUNCH(prof, stream, "upd_mark_pma", ceil_div(n, 256), 256, 0, k_mark_pma_vertices, c2n, n,
+               stamp.get(), epoch);
+  }
+  uint32_t *rlist = s_rlist.ensure(n);
+  {
+    uint64_t *t4 = tmp(select_tmp_elems(n) + 4);
+    select_if(StampPred{stamp.get(), epoch}, IndexVal32{}, n, rlist, cnt + C_NR, t4, stream, prof);
+  }
+  const uint64_t nr = read_u64(cnt + C_NR);
+  uint64_t *oOff = s_oOff.ensure(nr + 1), *nOff = s_nOff.ensure(nr + 1);
+  {
+    uint64_t *t5 = tmp(scan_tmp_elems(nr) + 4);
+    exclusive_scan(OldDeg{rlist, deg.get()}, nr, oOff, t5, stream, prof);
+    exclusive_scan(NewDeg{rlist, deg.get(), tu, tdn, nt}, nr, nOff, t5, stream, prof);
+  }
+  uint64_t SO = 0, SN = 0;
+  TRC_CUDA(cudaMemcpyAsync(&SO, oOff + nr, 8, cudaMemcpyDeviceToHost, stream));
+  TRC_CUDA(cudaMemcpyAsync(&SN, nOff + nr, 8, cudaMemcpyDeviceToHost, stream));
+  sync();
+
+  // ---- gather, merge / difference
+  uint64_t *oldk = s_old.ensure(SO + 1);
+  uint64_t *newk = s_new.ensure((SN > SO ? SN : SO) + 1);
+  TRC_LAUNCH(prof, stream, "upd_gather", ceil_div(nr * 32, 256), 256, 0, k_gather_old, G, rlist, nr,
+             oOff, oldk);
+  if (insert) {
+    merge_u64(oldk, SO, bkeys, kb, newk, stream, prof);
+  } else {
+    uint8_t *fl = s_flags.ensure(SO + 1);
+    uint64_t *t6 = tmp(select_tmp_elems(SO) + 4);
+    difference_u64(oldk, SO, bkeys, kb, newk, cnt + C_KU, fl, t6, stream, prof);
+  }
+
+  // ---- new tier-2 layout
+  if (rebuild) {
+    uint32_t *np = s_pma_next.alloc_exact(Nn);
+    TRC_LAUNCH(prof, stream, "upd_rebuild_layout", ceil_div((uint64_t)n + 1, 256), 256, 0,
+               k_rebuild_layout, P, n, Nn, pbeg.get());
+    (void)np;
+    rebuilds++;
+  } else if (nmw) {
+    TRC_LAUNCH(prof, stream, "upd_window_layout", nmw, 256, 0, k_window_layout, s_mw.get(), n, P,
+               pbeg.get());
+    window_rebalances += nmw;
+  }
+  if (!plan.empty()) {
+    uint64_t *dplan = s_hwplan.ensure(plan.size());
+    TRC_CUDA(cudaMemcpyAsync(dplan, plan.data(), plan.size() * 8, cudaMemcpyHostToDevice, stream));
+    TRC_LAUNCH(prof, stream, "upd_hub_plan", nh, 128, 0, k_apply_hub_plan, G, dplan, nh);
+  }
+  DevView GN = view();
+  if (rebuild) {
+    GN.pma = s_pma_next.get();
+    GN.N = Nn;
+  }
+  TRC_LAUNCH(prof, stream, "upd_scatter", ceil_div(nr * 32, 256), 256, 0, k_scatter_new, GN, rlist,
+             nr, nOff, newk);
+  TRC_LAUNCH(prof, stream, "upd_c2", ceil_div(nt, 256), 256, 0, k_scatter_c2_final, tu, tc2, nt,
+             c2.get());
+  if (rebuild) {
+    pma.swap(s_pma_next);
+    s_pma_next.reset();
+    N = Nn;
+  }
+  if (!plan.empty()) sync();  // the host plan vector must outlive its copy
+  m = insert ? m + kb : m - kb;
+  tier2_total = rebuild ? Ptot : t2new;
+  version++;
+  return kb;
+}
+
+}  // namespace trc

@@ -1,0 +1,272 @@
+"""GPU parity of the sm_100a library (through the C ABI) against the golden
+fixtures recorded from the reference and against the CPU oracle.
+
+Tolerances: lists, levels, labels and counts are compared exactly; PageRank
+and BC are FP64 sums whose order differs (warp reductions here, atomics /
+sequential sums in the reference), compared at relative 1e-9 (REL_TOL)."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+REL_TOL = 1e-9
+SYM = dict(symmetrize=True, drop_self_loops=True)
+
+
+def load(name):
+    return np.load(os.path.join(GOLD, name))
+
+
+def rel_close(a, b, tol=REL_TOL):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    if not np.array_equal(np.isnan(a), np.isnan(b)):
+        return False
+    f = ~np.isnan(a)
+    scale = np.maximum(np.abs(a[f]), np.abs(b[f]))
+    return bool(np.all(np.abs(a[f] - b[f]) <= tol * np.maximum(scale, 1e-300)))
+
+
+def csr_sha(off, tgt):
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(off, "<u8").tobytes())
+    h.update(np.ascontiguousarray(tgt, "<u4").tobytes())
+    return h.hexdigest()
+
+
+@pytest.fixture(scope="module")
+def T():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    import terrace_b200
+    return terrace_b200
+
+
+def graph_from_csr(T, off, tgt, **kw):
+    n = len(off) - 1
+    g = T.Graph(n, **kw)
+    src = np.repeat(np.arange(n, dtype=np.uint32), np.diff(off.astype(np.int64)))
+    g.add_edge_batch(src, tgt)
+    return g
+
+
+def assert_same_csr(g, off, tgt):
+    goff, gtgt = g.dump_csr()
+    assert np.array_equal(goff, off)
+    assert np.array_equal(gtgt, tgt)
+    assert g.check() == 0
+
+
+def check_algorithms(g, off, tgt, rec=None, prefix=""):
+    """BFS levels/parents, PR(5,10), CC, BC, TC against oracle (+ fixture)."""
+    deg = np.diff(off.astype(np.int64))
+    src = int(rec[prefix + "bfs_src"]) if rec is not None else int(deg.argmax())
+    par, lv = g.bfs(src)
+    want_lv = O.bfs_levels(off, tgt, src)
+    assert np.array_equal(lv, want_lv)
+    if rec is not None:
+        assert np.array_equal(lv, rec[prefix + "bfs_levels"])
+    assert O.bfs_check_parents(off, tgt, src, lv, par) == 0
+    for it in (5, 10):
+        pr = g.pagerank(it)
+        assert rel_close(pr, O.pagerank(off, tgt, it))
+        if rec is not None:
+            assert rel_close(pr, rec[prefix + f"pr{it}"])
+    assert rel_close(g.pagerank(7, damping=0.85), O.pagerank(off, tgt, 7, 0.85))
+    cc = g.cc()
+    assert np.array_equal(cc, O.cc(off, tgt))
+    if rec is not None:
+        assert np.array_equal(cc, rec[prefix + "cc"])
+    bc = g.bc(src)
+    assert rel_close(bc, O.bc(off, tgt, src))
+    if rec is not None:
+        assert rel_close(bc, rec[prefix + "bc"])
+    assert g.tc() == O.tc(off, tgt)
+
+
+def test_rmat_device_generator_bitexact(T):
+    z = load("rmat_pin.npz")
+    for i in range(3):
+        n, seed, a, b, c = z[f"p{i}_params"]
+        s, d = T.rmat_generate(int(n), int(seed), a, b, c, 4096, first=1000)
+        assert np.array_equal(s, z[f"p{i}_src"]) and np.array_equal(d, z[f"p{i}_dst"])
+    s, d = T.rmat_generate(1 << 20, 77, .57, .19, .19, 200000, first=123456789)
+    os_, od = O.rmat(1 << 20, 77, .57, .19, .19, 200000, first=123456789)
+    assert np.array_equal(s, os_) and np.array_equal(d, od)
+
+
+@pytest.mark.parametrize("name", ["s12_updates.npz", "s12_skew.npz"])
+@pytest.mark.parametrize("hub_threshold", [1024, 64])
+def test_update_sequence_matches_reference(T, name, hub_threshold):
+    """Bulk load, then every insert/delete batch of the fixture; the sorted
+    adjacency must equal the reference's after each step."""
+    z = load(name)
+    n = int(z["n"])
+    g = graph_from_csr(T, z["s0_off"], z["s0_tgt"], hub_threshold=hub_threshold)
+    assert_same_csr(g, z["s0_off"], z["s0_tgt"])
+    step, j = 1, 0
+    while f"batch{j}_src" in z.files:
+        bs, bd = z[f"batch{j}_src"], z[f"batch{j}_dst"]
+        g.add_edge_batch(bs, bd, **SYM)
+        assert_same_csr(g, z[f"s{step}_off"], z[f"s{step}_tgt"])
+        g.remove_edge_batch(bs, bd, **SYM)
+        assert_same_csr(g, z[f"s{step + 1}_off"], z[f"s{step + 1}_tgt"])
+        step += 2
+        j += 1
+    assert g.get_num_vertices() == n
+
+
+@pytest.mark.parametrize("name", ["s12_updates.npz", "s12_skew.npz"])
+def test_algorithms_match_reference(T, name):
+    z = load(name)
+    g = graph_from_csr(T, z["s0_off"], z["s0_tgt"])
+    check_algorithms(g, z["s0_off"], z["s0_tgt"], z, "s0_")
+    last = int(z["steps"]) - 1
+    g2 = graph_from_csr(T, z[f"s{last}_off"], z[f"s{last}_tgt"], hub_threshold=64)
+    check_algorithms(g2, z[f"s{last}_off"], z[f"s{last}_tgt"], z, "final_")
+
+
+def test_tc_matches_reference_exact_path(T):
+    z = load("low_degree_tc.npz")
+    off, tgt = O.csr_from_keys(int(z["n"]), z["keys"])
+    g = graph_from_csr(T, off, tgt)
+    assert g.tc() == int(z["ref_tc"]) == 12000
+
+
+def test_static_workload_rmat17(T):
+    """RMAT scale 17 ef 8 seed 0 (bulk load + BFS from 9 and from the
+    max-degree vertex, PR 5, CC, BC, TC) against the reference summary."""
+    with open(os.path.join(GOLD, "config1_summary.json")) as f:
+        s = json.load(f)
+    n = 1 << 17
+    src, dst = T.rmat_generate(n, 0, .5, .1, .1, 8 * n)
+    g = T.Graph(n)
+    g.add_edge_batch(src, dst, **SYM)
+    assert g.get_num_edges() == s["m"]
+    off, tgt = g.dump_csr()
+    assert csr_sha(off, tgt) == s["csr_sha256"]
+    assert g.check() == 0
+    for v in (9, s["argmax_degree"]):
+        par, lv = g.bfs(v)
+        assert hashlib.sha256(lv.astype("<u4").tobytes()).hexdigest() == s[f"bfs{v}_levels_sha256"]
+        assert O.bfs_check_parents(off, tgt, v, lv, par) == 0
+    sample = np.array(s["sample"])
+    pr = g.pagerank(5)
+    assert rel_close(pr[sample], np.array(s["pr5_sample"]))
+    assert abs(pr.sum() - s["pr5_sum"]) <= 1e-9 * s["pr5_sum"]
+    cc = g.cc()
+    assert hashlib.sha256(cc.astype("<u4").tobytes()).hexdigest() == s["cc_sha256"]
+    bc = g.bc(s["bc_src"])
+    ref = np.array([np.nan if x is None else x for x in s["bc_sample"]])
+    assert rel_close(bc[sample], ref)
+    assert g.tc() == s["tc_exact_published_in_survey"] == 758730
+
+
+def test_set_semantics_edge_cases(T):
+    g = T.Graph(100, hub_threshold=20)
+    assert g.add_edge_batch(np.array([], np.uint32), np.array([], np.uint32)) == 0
+    # duplicates and both directions
+    assert g.add_edge_batch([1, 1, 2, 1], [5, 5, 1, 5]) == 2
+    assert g.degree(1) == 1 and g.degree(2) == 1
+    assert list(g.neighbors(1)) == [5]
+    assert g.add_edge(1, 5) == -1 and g.add_edge(5, 1) == 0
+    # self loops kept unless dropped
+    assert g.add_edge_batch([7], [7]) == 1
+    assert g.add_edge_batch([8], [8], drop_self_loops=True) == 0
+    # removing absent edges is a no-op (the reference would drop a neighbour)
+    assert g.remove_edge_batch([1, 3], [6, 4]) == 0
+    assert g.remove_edge(1, 5) == 0 and g.remove_edge(1, 5) == -1
+    # out-of-range ids fail with TRC_ERR_INVALID and leave the graph unchanged
+    m = g.get_num_edges()
+    with pytest.raises(T.TrcError) as e:
+        g.add_edge_batch([1, 200], [2, 3])
+    assert e.value.status == 1
+    assert g.get_num_edges() == m
+    with pytest.raises(T.TrcError):
+        g.degree(100)
+    # grow a vertex through every tier: inline -> PMA -> hub, then shrink
+    nb = np.arange(30, 100, dtype=np.uint32)
+    g.add_edge_batch(np.full(len(nb), 0, np.uint32), nb, symmetrize=True)
+    assert list(g.neighbors(0)) == list(nb)
+    assert g.stats()["num_hubs"] >= 1
+    assert g.check() == 0
+    g.remove_edge_batch(np.full(60, 0, np.uint32), nb[:60], symmetrize=True)
+    assert list(g.neighbors(0)) == list(nb[60:])
+    assert g.check() == 0
+    assert g.is_edge(0, 99) == 1 and g.is_edge(0, 30) == 0
+    assert g.count_common(0, 95) == 0
+
+
+def test_random_updates_against_set_model(T):
+    """Random inserts/deletes with small tier thresholds, checked against the
+    oracle's set model after every batch (exercises window rebalances, PMA
+    rebuilds, hub promotion and hub region growth)."""
+    rng = np.random.default_rng(1)
+    n = 3000
+    g = T.Graph(n, hub_threshold=48)
+    cur = np.zeros(0, np.uint64)
+    for step in range(14):
+        k = int(rng.integers(1, 20000))
+        s = rng.integers(0, n, k).astype(np.uint32)
+        # skew: a few vertices get many edges
+        s[: k // 3] = rng.integers(0, 20, k // 3).astype(np.uint32)
+        d = rng.integers(0, n, k).astype(np.uint32)
+        bk = O.make_keys(s, d, True, True)
+        if step % 3 == 2:
+            g.remove_edge_batch(s, d, **SYM)
+            cur = O.key_difference(cur, bk)
+        else:
+            g.add_edge_batch(s, d, **SYM)
+            cur = O.key_union(cur, bk)
+        off, tgt = O.csr_from_keys(n, cur)
+        assert_same_csr(g, off, tgt)
+    st = g.stats()
+    assert st["num_hubs"] > 0 and st["pma_rebuilds"] >= 1
+    check_algorithms(g, off, tgt)
+    # queries
+    qs = rng.integers(0, n, 5000).astype(np.uint32)
+    qd = rng.integers(0, n, 5000).astype(np.uint32)
+    want = np.isin((qs.astype(np.uint64) << np.uint64(32)) | qd.astype(np.uint64), cur)
+    assert np.array_equal(g.is_edge(qs, qd).astype(bool), want)
+    assert np.array_equal(g.degree(qs), np.diff(off.astype(np.int64))[qs].astype(np.uint32))
+    cc_q = g.count_common(qs[:500], qd[:500])
+    for a, b, c in zip(qs[:500], qd[:500], cc_q):
+        na = set(tgt[off[a]:off[a + 1]].tolist())
+        nb = set(tgt[off[b]:off[b + 1]].tolist())
+        assert c == sum(1 for w in na & nb if w < min(a, b))
+
+
+def test_streaming_rmat22_roundtrip_and_parity(T):
+    """LiveJournal-shaped RMAT scale 22 ef 16: bulk load and one 1e6-pair
+    insert + delete batch.  Parity with the oracle's set model by CSR hash,
+    plus the size-independent round trip (insert then delete of a fresh
+    batch restores the original hash)."""
+    n = 1 << 22
+    s, d = T.rmat_generate(n, 0, .5, .1, .1, 16 * n)
+    g = T.Graph(n)
+    g.add_edge_batch(s, d, **SYM)
+    n_, keys = O.rmat_graph_keys(22, 16, .5, .1, .1, 0)
+    off, tgt = g.dump_csr()
+    woff, wtgt = O.csr_from_keys(n, keys)
+    assert np.array_equal(off, woff) and np.array_equal(tgt, wtgt)
+    h0 = csr_sha(off, tgt)
+    bs, bd = T.rmat_generate(n, O.batch_seed(1, 0), .5, .1, .1, 1000000)
+    bk = O.make_keys(bs, bd, True, True)
+    fresh = O.key_difference(bk, keys)
+    fs, fd = O.keys_to_pairs(fresh)
+    assert g.add_edge_batch(fs, fd) == len(fresh)
+    off1, tgt1 = g.dump_csr()
+    w1off, w1tgt = O.csr_from_keys(n, O.key_union(keys, bk))
+    assert np.array_equal(off1, w1off) and np.array_equal(tgt1, w1tgt)
+    assert g.check() == 0
+    assert g.remove_edge_batch(fs, fd) == len(fresh)
+    assert csr_sha(*g.dump_csr()) == h0
+    assert g.check() == 0
