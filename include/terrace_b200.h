@@ -167,6 +167,8 @@ trc_status trc_profile_get(trc_graph *g, const char *name, double *ms,
                            uint64_t *launches);
 /* Names of the kernels recorded so far, newline-separated, into buf. */
 trc_status trc_profile_names(trc_graph *g, char *buf, uint64_t cap);
+/* Kernels this handle has launched since it was created (always counted). */
+trc_status trc_launch_count(trc_graph *g, uint64_t *launches);
 
 #ifdef __cplusplus
 }

@@ -87,6 +87,7 @@ SIGNATURES = [
     ("trc_profile_reset", _int, [_vp]),
     ("trc_profile_get", _int, [_vp, C.c_char_p, C.POINTER(_dbl), C.POINTER(_u64)]),
     ("trc_profile_names", _int, [_vp, C.c_char_p, _u64]),
+    ("trc_launch_count", _int, [_vp, C.POINTER(_u64)]),
 ]
 
 _lib = None

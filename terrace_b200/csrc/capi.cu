@@ -285,4 +285,11 @@ trc_status trc_profile_names(trc_graph *g, char *buf, uint64_t cap) {
   });
 }
 
+trc_status trc_launch_count(trc_graph *g, uint64_t *launches) {
+  return guard([&] {
+    if (!launches) trc::throw_error(TRC_ERR_INVALID, "null output");
+    *launches = G(g).prof.launches;
+  });
+}
+
 }  // extern "C"

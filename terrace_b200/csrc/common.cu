@@ -57,6 +57,7 @@ cudaEvent_t Profiler::get_event() {
 }
 
 int Profiler::begin(const char *name, cudaStream_t s) {
+  launches++;
   if (!on) return -1;
   Rec r;
   r.a = get_event();

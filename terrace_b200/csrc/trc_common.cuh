@@ -176,9 +176,11 @@ class DBuf {
     cap_ = c;
     return ptr_;
   }
-  // Grows to at least `count`, preserving the first `keep` elements.
+  // Grows to at least `count`, preserving the first `keep` elements (at
+  // most the old capacity).
   T *grow(uint64_t count, uint64_t keep, cudaStream_t s) {
     if (count <= cap_) return ptr_;
+    if (keep > cap_) keep = cap_;
     uint64_t c = count < 16 ? 16 : count;
     T *np = static_cast<T *>(budget_->alloc(c * sizeof(T)));
     if (keep) TRC_CUDA(cudaMemcpyAsync(np, ptr_, keep * sizeof(T), cudaMemcpyDeviceToDevice, s));
@@ -213,6 +215,7 @@ class DBuf {
 class Profiler {
  public:
   bool on = false;
+  uint64_t launches = 0;  // every kernel launch, profiled or not
   struct Rec {
     cudaEvent_t a, b;
     std::string name;

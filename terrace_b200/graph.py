@@ -242,6 +242,11 @@ class Graph:
                                         C.byref(ms), C.byref(cnt)))
         return ms.value, int(cnt.value)
 
+    def launch_count(self) -> int:
+        x = C.c_uint64()
+        L.check(self._L.trc_launch_count(self._h, C.byref(x)))
+        return int(x.value)
+
     def profile_names(self):
         buf = C.create_string_buffer(1 << 16)
         L.check(self._L.trc_profile_names(self._h, buf, len(buf)))
