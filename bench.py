@@ -173,8 +173,6 @@ def run_ours(args, rank, world):
     # ---- warm-up inserts (W), then K timed inserts, then deletes of all
     for j in range(args.warmup):
         g.add_edge_batch(*batches[j], symmetrize=True, drop_self_loops=True)
-    g.profile(True)
-    g.profile_reset()
     l0 = g.launch_count()
     clk = ClockSampler(dev.index)
     clk.start()
@@ -182,21 +180,27 @@ def run_ours(args, rank, world):
                                                    drop_self_loops=True), args.steps)
     clocks = clk.stop()
     launches = g.launch_count() - l0
-    kernel_ms = {}
-    for name in g.profile_names():
-        ms, cnt = g.profile_get(name)
-        kernel_ms[name] = (ms, cnt)
-    g.profile(False)
     inserted = sum(ins)
     value = inserted * world / (ins_ms / 1e3)
     pairs_per_s = BATCH * args.steps * world / (ins_ms / 1e3)
-
     del_ms, dels = timed(lambda i: g.remove_edge_batch(*batches[args.warmup + i], symmetrize=True,
                                                        drop_self_loops=True), args.steps)
     deleted = sum(dels)
+
+    # ---- profiled pass (separate from the timed region): the same K inserts
+    # again with CUDA events around every kernel, plus the per-batch sizes
+    g.profile(True)
+    g.profile_reset()
+    sizes = []
+    for i in range(args.steps):
+        g.add_edge_batch(*batches[args.warmup + i], symmetrize=True, drop_self_loops=True)
+        sizes.append(g.stats())
+    kernel_ms = {name: g.profile_get(name) for name in g.profile_names()}
+    g.profile(False)
+    for i in range(args.steps):
+        g.remove_edge_batch(*batches[args.warmup + i], symmetrize=True, drop_self_loops=True)
     for j in range(args.warmup):
         g.remove_edge_batch(*batches[j], symmetrize=True, drop_self_loops=True)
-    assert g.get_num_edges() == m0, "insert+delete round trip changed the edge count"
 
     # ---- e2e: same metric through the public API with pinned HOST buffers
     host = []
@@ -251,7 +255,7 @@ def run_ours(args, rank, world):
 
     # ---- roofline of the dominant kernel of the timed insert steps
     dom = max(kernel_ms.items(), key=lambda kv: kv[1][0])
-    roof = roofline_for(dom[0], dom[1], st, args, hbm_gbs, peak_kind, n)
+    roof = roofline_for(dom[0], dom[1], sizes, hbm_gbs, peak_kind)
     total_kernel_ms = sum(v[0] for v in kernel_ms.values())
 
     g.close()
@@ -290,24 +294,36 @@ def run_ours(args, rank, world):
     return res
 
 
-def roofline_for(name, ms_cnt, st, args, hbm_gbs, peak_kind, n):
-    """Algorithmic bytes per launch of the dominant insert kernel (formulas
-    in DESIGN.md), divided by its mean CUDA-event duration."""
+def kernel_bytes(name, sz):
+    """Algorithmic bytes of one launch of an update-pipeline kernel for a
+    batch with sizes `sz` (trc_stats last_*): the bytes the kernel must move
+    (DESIGN.md lists the formulas)."""
+    k2, kb, nr = sz["last_keys"], sz["last_applied"], sz["last_rewritten"]
+    so, sn = sz["last_gathered"], sz["last_written"]
+    if name == "upd_gather":      # old lists (4 B) -> 64-bit keys; per-vertex metadata
+        return 12 * so + 28 * nr
+    if name == "merge":           # two sorted key streams in, one out
+        return 8 * (so + kb) + 8 * sn
+    if name == "upd_scatter":     # keys in, 4-byte lists out; per-vertex metadata
+        return 12 * sn + 28 * nr
+    if name == "radix_scatter":   # read + write one key per pass
+        return 16 * k2
+    if name == "radix_hist":
+        return 8 * k2
+    return None
+
+
+def roofline_for(name, ms_cnt, sizes, hbm_gbs, peak_kind):
+    """Algorithmic bytes per launch of the dominant insert kernel divided by
+    its mean CUDA-event duration (profiled pass of the same batches)."""
     ms, cnt = ms_cnt
     per_launch_ms = ms / max(cnt, 1)
-    k2 = 2 * BATCH
-    # average sizes per batch step are not returned by the library; the
-    # formula uses the batch geometry the kernels process
-    if name.startswith("radix_scatter"):
-        bytes_per = 16 * k2          # read + write one 8-byte key
-        unit = "keys"
-    elif name.startswith("radix_hist"):
-        bytes_per = 8 * k2
-        unit = "keys"
-    else:
+    per = [kernel_bytes(name, sz) for sz in sizes]
+    if any(b is None for b in per):
         return {"bound": "hbm", "kernel": name, "achieved": None, "peak": hbm_gbs, "unit": "GB/s",
                 "frac": None, "traffic": None, "peak_kind": peak_kind,
                 "note": "no byte formula for this kernel", "launch_ms": per_launch_ms}
+    bytes_per = sum(per) / len(per)
     achieved = bytes_per / (per_launch_ms / 1e3) / 1e9
     return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm_gbs, "unit": "GB/s",
             "frac": achieved / hbm_gbs, "traffic": None, "peak_kind": peak_kind,

@@ -151,6 +151,15 @@ typedef struct {
   uint64_t device_bytes;   /* bytes held on the device */
   uint64_t pma_rebuilds;   /* full tier-2 rebuilds so far */
   uint64_t pma_window_rebalances; /* local window rebalances so far */
+  /* sizes inside the last update batch */
+  uint64_t last_keys;      /* keys after symmetrize */
+  uint64_t last_applied;   /* edges inserted / removed */
+  uint64_t last_touched;   /* source vertices with changes */
+  uint64_t last_rewritten; /* vertices whose lists were rewritten */
+  uint64_t last_gathered;  /* list elements read (old lists) */
+  uint64_t last_written;   /* list elements written (new lists) */
+  uint64_t last_windows;   /* PMA windows rebalanced */
+  uint64_t last_rebuild;   /* 1 if the PMA was rebuilt */
 } trc_stats;
 trc_status trc_get_stats(trc_graph *g, trc_stats *out);
 /* Checks every structural invariant on the device (sorted, duplicate-free

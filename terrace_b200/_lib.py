@@ -52,7 +52,15 @@ class trc_stats(C.Structure):
                 ("hub_blocks_used", C.c_uint64),
                 ("device_bytes", C.c_uint64),
                 ("pma_rebuilds", C.c_uint64),
-                ("pma_window_rebalances", C.c_uint64)]
+                ("pma_window_rebalances", C.c_uint64),
+                ("last_keys", C.c_uint64),
+                ("last_applied", C.c_uint64),
+                ("last_touched", C.c_uint64),
+                ("last_rewritten", C.c_uint64),
+                ("last_gathered", C.c_uint64),
+                ("last_written", C.c_uint64),
+                ("last_windows", C.c_uint64),
+                ("last_rebuild", C.c_uint64)]
 
 
 # (name, restype, argtypes) for every symbol the header declares

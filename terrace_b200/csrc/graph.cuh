@@ -61,6 +61,7 @@ class Graph {
   uint32_t epoch = 0;
   DBuf<uint32_t> stamp;    // per-vertex epoch marks for the rewrite set
   uint64_t rebuilds = 0, window_rebalances = 0;
+  uint64_t last[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // sizes of the last batch
 
   // ------------------------------------------------------------- scratch
   DBuf<uint32_t> s_in_src, s_in_dst;

@@ -257,6 +257,14 @@ void Graph::stats(trc_stats *o) {
   o->device_bytes = budget.used;
   o->pma_rebuilds = rebuilds;
   o->pma_window_rebalances = window_rebalances;
+  o->last_keys = last[0];
+  o->last_applied = last[1];
+  o->last_touched = last[2];
+  o->last_rewritten = last[3];
+  o->last_gathered = last[4];
+  o->last_written = last[5];
+  o->last_windows = last[6];
+  o->last_rebuild = last[7];
   // inline = sum(min(deg,16)); hub = m - inline - tier2
   uint64_t *t = tmp(scan_tmp_elems(n) + 4);
   uint64_t *off = s_oOff.ensure((uint64_t)n + 1);

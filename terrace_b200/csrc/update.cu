@@ -217,33 +217,55 @@ enum {
   C_COUNT
 };
 
+// Warp-aggregated append: one atomic per warp, returns this lane's slot.
+__device__ __forceinline__ uint64_t warp_append64(bool take, unsigned long long *counter) {
+  uint32_t m = __ballot_sync(0xFFFFFFFFu, take);
+  uint64_t base = 0;
+  if (m) {
+    uint32_t leader = __ffs(m) - 1;
+    if ((threadIdx.x & 31) == leader) base = atomicAdd(counter, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  }
+  return base + __popc(m & lanemask_lt());
+}
+
 // Classify touched vertices (step 4).
 __global__ void k_classify(DevView G, const uint64_t *bkeys, const uint64_t *tpos, uint64_t nt,
                            uint64_t kb, int insert, uint32_t *tu, uint32_t *tdn, uint32_t *tc2,
                            uint32_t *ovl, uint32_t *hw_u, uint32_t *hw_dn, uint32_t *hw_t,
                            int32_t *hw_h, uint64_t *cnt) {
   uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nt) return;
-  uint64_t p0 = tpos[t];
-  uint64_t p1 = t + 1 < nt ? tpos[t + 1] : kb;
-  uint32_t u = (uint32_t)(bkeys[p0] >> 32);
-  uint32_t c = (uint32_t)(p1 - p0);
-  uint32_t d = G.deg[u];
-  uint32_t dn = insert ? d + c : d - c;
-  int32_t h = G.hub_of[u];
-  bool hub = h >= 0 || dn > G.hub_T;
-  uint32_t nc2 = (!hub && dn > K_INLINE) ? dn - K_INLINE : 0;
-  tu[t] = u;
-  tdn[t] = dn;
-  tc2[t] = nc2;
-  int64_t delta = (int64_t)nc2 - (int64_t)G.c2[u];
-  if (delta) atomicAdd((unsigned long long *)&cnt[C_T2DELTA], (unsigned long long)delta);
-  if (!hub && (uint64_t)nc2 > G.pbeg[u + 1] - G.pbeg[u]) {
-    uint64_t j = atomicAdd((unsigned long long *)&cnt[C_NOV], 1ull);
-    ovl[j] = u;
+  bool valid = t < nt;
+  uint32_t u = 0, dn = 0;
+  int32_t h = -1;
+  bool hub = false, over = false;
+  long long delta = 0;
+  if (valid) {
+    uint64_t p0 = tpos[t];
+    uint64_t p1 = t + 1 < nt ? tpos[t + 1] : kb;
+    u = (uint32_t)(bkeys[p0] >> 32);
+    uint32_t c = (uint32_t)(p1 - p0);
+    uint32_t d = G.deg[u];
+    dn = insert ? d + c : d - c;
+    h = G.hub_of[u];
+    hub = h >= 0 || dn > G.hub_T;
+    uint32_t nc2 = (!hub && dn > K_INLINE) ? dn - K_INLINE : 0;
+    tu[t] = u;
+    tdn[t] = dn;
+    tc2[t] = nc2;
+    delta = (long long)nc2 - (long long)G.c2[u];
+    over = !hub && (uint64_t)nc2 > G.pbeg[u + 1] - G.pbeg[u];
   }
-  if (hub) {
-    uint64_t j = atomicAdd((unsigned long long *)&cnt[C_NH], 1ull);
+  // per-warp delta sum, one atomic per warp
+  long long wd = delta;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) wd += __shfl_xor_sync(0xFFFFFFFFu, wd, o);
+  if ((threadIdx.x & 31) == 0 && wd)
+    atomicAdd((unsigned long long *)&cnt[C_T2DELTA], (unsigned long long)wd);
+  uint64_t j = warp_append64(over, (unsigned long long *)&cnt[C_NOV]);
+  if (over) ovl[j] = u;
+  j = warp_append64(valid && hub, (unsigned long long *)&cnt[C_NH]);
+  if (valid && hub) {
     hw_u[j] = u;
     hw_dn[j] = dn;
     hw_t[j] = (uint32_t)t;
@@ -518,7 +540,11 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   sync();
   if (herr & ERR_BAD_VERTEX) throw_error(TRC_ERR_INVALID, "vertex id out of range [0, n)");
   const uint64_t kb = hc[C_KB], nt = hc[C_NT];
-  if (kb == 0) return 0;
+  if (kb == 0) {
+    for (auto &x : last) x = 0;
+    last[0] = k2;
+    return 0;
+  }
 
   uint32_t *tu = s_tu.ensure(nt), *tdn = s_tdn.ensure(nt), *tc2 = s_tc2.ensure(nt);
   uint32_t *ovl = s_ovl.ensure(nt);
@@ -700,6 +726,14 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   if (!plan.empty()) sync();  // the host plan vector must outlive its copy
   m = insert ? m + kb : m - kb;
   tier2_total = rebuild ? Ptot : t2new;
+  last[0] = k2;
+  last[1] = kb;
+  last[2] = nt;
+  last[3] = nr;
+  last[4] = SO;
+  last[5] = SN;
+  last[6] = nmw;
+  last[7] = rebuild ? 1 : 0;
   version++;
   return kb;
 }
