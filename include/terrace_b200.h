@@ -49,7 +49,9 @@ typedef enum {
 typedef struct {
   uint32_t hub_threshold;     /* degree above which a vertex moves to the
                                  blocked tier; reference MEDIUM_DEGREE 1024
-                                 (include/graph.h:39).  Default 1024. */
+                                 (include/graph.h:39).  Default 1024; at
+                                 most 12288 (a PMA vertex's list is staged
+                                 in 48 KB of shared memory when merged). */
   double pma_root_density;    /* upper density bound at the PMA root;
                                  reference 0.75 (src/PMA.cc:382-394). */
   double pma_build_density;   /* density after a full PMA rebuild.

@@ -78,7 +78,8 @@ trc_status trc_graph_create(uint32_t n, uint64_t hbm_budget_bytes, const trc_con
     trc_config c;
     trc_config_default(&c);
     if (cfg) c = *cfg;
-    if (c.hub_threshold < trc::K_INLINE) trc::throw_error(TRC_ERR_INVALID, "hub_threshold < 16");
+    if (c.hub_threshold < trc::K_INLINE || c.hub_threshold > 12288)
+      trc::throw_error(TRC_ERR_INVALID, "hub_threshold must be in [16, 12288]");
     *out = nullptr;
     trc_graph *h = new trc_graph{nullptr};
     try {

@@ -60,6 +60,8 @@ class Graph {
   uint64_t version = 0;
   uint32_t epoch = 0;
   DBuf<uint32_t> stamp;    // per-vertex epoch marks for the rewrite set
+  DBuf<uint32_t> wstamp;   // per-vertex epoch marks for rebalanced windows
+  DBuf<uint64_t> pbeg_alt; // next tier-2 layout while a batch is applied
   uint64_t rebuilds = 0, window_rebalances = 0;
   uint64_t last[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // sizes of the last batch
 

@@ -54,6 +54,8 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
                   &s_wk, &s_wk2, &s_mw, &s_old, &s_new, &s_hwplan})
     b->bind(&budget);
   hub_of.bind(&budget);
+  wstamp.bind(&budget);
+  pbeg_alt.bind(&budget);
   s_hw_h.bind(&budget);
   s_flags.bind(&budget);
 
@@ -64,6 +66,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   pbeg.alloc_exact(nn + 1);
   hub_of.alloc_exact(nn);
   stamp.alloc_exact(nn);
+  wstamp.alloc_exact(nn);
   err.alloc_exact(4);
   s_cnt.alloc_exact(32);
   pma.alloc_exact(1);
@@ -74,6 +77,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   TRC_CUDA(cudaMemsetAsync(pbeg.get(), 0, (nn + 1) * 8, stream));
   TRC_CUDA(cudaMemsetAsync(hub_of.get(), 0xFF, nn * 4, stream));
   TRC_CUDA(cudaMemsetAsync(stamp.get(), 0, nn * 4, stream));
+  TRC_CUDA(cudaMemsetAsync(wstamp.get(), 0, nn * 4, stream));
   TRC_CUDA(cudaMemsetAsync(err.get(), 0, 16, stream));
   grow_hub_tables(64);
   grow_pool(64);
@@ -501,6 +505,169 @@ __global__ void k_scatter_c2_final(const uint32_t *tu, const uint32_t *tc2, uint
 }
 
 // ---------------------------------------------------------------------------
+// Fused per-vertex merge for vertices that stay in tiers 1-2 (degree <= the
+// hub threshold before and after).  One warp per vertex: the old list is
+// staged in shared memory, every old element's output rank is its index plus
+// the number of batch keys below it (binary search in the vertex's slice of
+// the sorted batch), every inserted key's rank is its index plus the number
+// of old elements below it; outputs go straight to the inline row and the
+// PMA segment (in place, or to the layout's new position).  About 8 bytes of
+// HBM traffic per list element instead of a gather / global merge / scatter.
+
+// Position of vertex u in the sorted touched list, or nt.
+__device__ __forceinline__ uint64_t touched_index(const uint32_t *tu, uint64_t nt, uint32_t u) {
+  uint64_t lo = 0, hi = nt;
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) >> 1;
+    if (tu[mid] < u) lo = mid + 1;
+    else hi = mid;
+  }
+  return (lo < nt && tu[lo] == u) ? lo : nt;
+}
+
+// Rewrite-set members handled by the fused merge: non-hubs that stay <= T.
+struct SmallPred {
+  const uint32_t *stamp;
+  uint32_t epoch;
+  const int32_t *hub_of;
+  const uint32_t *deg, *tu, *tdn;
+  uint64_t nt;
+  uint32_t T;
+  __device__ bool operator()(uint64_t i) const {
+    if (stamp[i] != epoch || hub_of[i] >= 0) return false;
+    uint64_t t = touched_index(tu, nt, (uint32_t)i);
+    uint32_t dn = t < nt ? tdn[t] : deg[i];
+    return dn <= T;
+  }
+};
+
+struct MergeArgs {
+  const uint32_t *rs;
+  uint64_t nrs;
+  const uint32_t *tu;
+  const uint64_t *tpos;
+  uint64_t nt, kb;
+  const uint64_t *bkeys;
+  int insert;
+  const uint64_t *pbeg_new;  // segment offsets after this batch
+  uint32_t *dst_pma;         // destination of vertices that do not move
+  uint32_t *mov_pma;         // destination of vertices inside a rebalanced window
+  const uint32_t *wstamp;    // window marks (null: no window moves)
+  uint32_t epoch;
+  uint32_t T;
+};
+
+__device__ __forceinline__ uint32_t lower_bound_keys(const uint64_t *B, uint32_t nb, uint32_t x) {
+  uint32_t lo = 0, hi = nb;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if ((uint32_t)B[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *A, uint32_t na, uint32_t x) {
+  uint32_t lo = 0, hi = na;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (A[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_merge_small(DevView G, MergeArgs a) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint64_t w = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+  if (w >= a.nrs) return;
+  uint32_t *A = smem + (uint64_t)wib * a.T;
+  const uint32_t u = a.rs[w];
+  NbrList L = nbr_list(G, u);
+  const uint32_t d = L.deg;
+  for (uint32_t j = lane; j < d; j += 32) A[j] = L.at(j);
+  uint64_t t = touched_index(a.tu, a.nt, u);
+  uint64_t b0 = 0, b1 = 0;
+  if (t < a.nt) {
+    b0 = a.tpos[t];
+    b1 = t + 1 < a.nt ? a.tpos[t + 1] : a.kb;
+  }
+  const uint32_t nb = (uint32_t)(b1 - b0);
+  const uint64_t *B = a.bkeys + b0;
+  const uint32_t dn = a.insert ? d + nb : d - nb;
+  __syncwarp();
+  uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
+  bool moved = a.wstamp && a.wstamp[u] == a.epoch;
+  uint32_t *seg = (moved ? a.mov_pma : a.dst_pma) + a.pbeg_new[u];
+  if (a.insert) {
+    for (uint32_t i = lane; i < d; i += 32) {
+      uint32_t x = A[i];
+      uint32_t r = i + lower_bound_keys(B, nb, x);
+      if (r < K_INLINE) row[r] = x;
+      else seg[r - K_INLINE] = x;
+    }
+    for (uint32_t j = lane; j < nb; j += 32) {
+      uint32_t x = (uint32_t)B[j];
+      uint32_t r = j + lower_bound_u32(A, d, x);
+      if (r < K_INLINE) row[r] = x;
+      else seg[r - K_INLINE] = x;
+    }
+  } else {
+    for (uint32_t i = lane; i < d; i += 32) {
+      uint32_t x = A[i];
+      uint32_t c = lower_bound_keys(B, nb, x);
+      if (c < nb && (uint32_t)B[c] == x) continue;
+      uint32_t r = i - c;
+      if (r < K_INLINE) row[r] = x;
+      else seg[r - K_INLINE] = x;
+    }
+  }
+  if (lane == 0) G.deg[u] = dn;
+}
+
+// Moves the segments written to the window buffer to their final slots.
+__global__ void k_window_copy(DevView G, const uint32_t *rs, uint64_t nrs, const uint32_t *mov,
+                              const uint64_t *pbeg_new, const uint32_t *wstamp, uint32_t epoch) {
+  uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= nrs) return;
+  uint32_t u = rs[w];
+  if (wstamp[u] != epoch) return;
+  uint32_t dn = G.deg[u];
+  if (dn <= K_INLINE) return;
+  uint64_t o = pbeg_new[u];
+  for (uint32_t j = lane; j < dn - K_INLINE; j += 32) G.pma[o + j] = mov[o + j];
+}
+
+__global__ void k_window_mark2(const uint64_t *mw, uint32_t n, uint32_t *stamp, uint32_t *wstamp,
+                               uint32_t epoch) {
+  uint64_t a, b;
+  window_range(mw[blockIdx.x], n, a, b);
+  for (uint64_t u = a + threadIdx.x; u < b; u += blockDim.x) {
+    stamp[u] = epoch;
+    wstamp[u] = epoch;
+  }
+}
+
+// Keys of the batch whose source is in the sorted vertex list V.
+struct KeyInListPred {
+  const uint64_t *keys;
+  const uint32_t *V;
+  uint64_t nv;
+  __device__ bool operator()(uint64_t i) const {
+    uint32_t u = (uint32_t)(keys[i] >> 32);
+    uint64_t lo = 0, hi = nv;
+    while (lo < hi) {
+      uint64_t mid = (lo + hi) >> 1;
+      if (V[mid] < u) lo = mid + 1;
+      else hi = mid;
+    }
+    return lo < nv && V[lo] == u;
+  }
+};
+
+// ---------------------------------------------------------------------------
 // The pipeline
 
 uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint64_t k,
@@ -644,17 +811,18 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     }
   }
 
-  // ---- rewrite set R
+  // ---- rewrite set: touched vertices, window members, (rebuild) all PMA vertices
   epoch++;
-  if (epoch == 0) {  // wrapped: clear stamps
+  if (epoch == 0) {  // wrapped: clear the marks
     TRC_CUDA(cudaMemsetAsync(stamp.get(), 0, (uint64_t)n * 4, stream));
+    TRC_CUDA(cudaMemsetAsync(wstamp.get(), 0, (uint64_t)n * 4, stream));
     epoch = 1;
   }
   TRC_LAUNCH(prof, stream, "upd_mark", ceil_div(nt, 256), 256, 0, k_mark_touched, tu, nt,
              stamp.get(), epoch);
   if (nmw)
-    TRC_LAUNCH(prof, stream, "upd_window_mark", nmw, 256, 0, k_window_mark, s_mw.get(), n,
-               stamp.get(), epoch);
+    TRC_LAUNCH(prof, stream, "upd_window_mark", nmw, 256, 0, k_window_mark2, s_mw.get(), n,
+               stamp.get(), wstamp.get(), epoch);
   uint64_t Ptot = 0;
   if (rebuild) {
     Ptot = read_u64(P + n);  // the layout kernel spreads exactly this many
@@ -662,68 +830,113 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     TRC_LAUNCH(prof, stream, "upd_mark_pma", ceil_div(n, 256), 256, 0, k_mark_pma_vertices, c2n, n,
                stamp.get(), epoch);
   }
-  uint32_t *rlist = s_rlist.ensure(n);
+
+  // ---- new tier-2 layout (into pbeg_alt; pbeg keeps the old one until the end)
+  const bool relayout = rebuild || nmw;
+  uint64_t *pbeg_new = pbeg.get();
+  uint32_t *dst_pma = pma.get();
+  uint32_t *mov_pma = nullptr;
+  if (relayout) {
+    pbeg_new = pbeg_alt.ensure((uint64_t)n + 1);
+    if (rebuild) {
+      dst_pma = s_pma_next.alloc_exact(Nn);
+      TRC_LAUNCH(prof, stream, "upd_rebuild_layout", ceil_div((uint64_t)n + 1, 256), 256, 0,
+                 k_rebuild_layout, P, n, Nn, pbeg_new);
+      rebuilds++;
+    } else {
+      TRC_CUDA(cudaMemcpyAsync(pbeg_new, pbeg.get(), ((uint64_t)n + 1) * 8,
+                               cudaMemcpyDeviceToDevice, stream));
+      TRC_LAUNCH(prof, stream, "upd_window_layout", nmw, 256, 0, k_window_layout, s_mw.get(), n, P,
+                 pbeg_new);
+      mov_pma = s_pma_next.ensure(N ? N : 1);
+      window_rebalances += nmw;
+    }
+  }
+
+  // ---- fused merge for every rewrite vertex that stays in tiers 1-2
+  const uint32_t T = cfg.hub_threshold;
+  uint32_t *rs = s_rlist.ensure(n);
   {
     uint64_t *t4 = tmp(select_tmp_elems(n) + 4);
-    select_if(StampPred{stamp.get(), epoch}, IndexVal32{}, n, rlist, cnt + C_NR, t4, stream, prof);
+    select_if(SmallPred{stamp.get(), epoch, hub_of.get(), deg.get(), tu, tdn, nt, T}, IndexVal32{},
+              n, rs, cnt + C_NR, t4, stream, prof);
   }
-  const uint64_t nr = read_u64(cnt + C_NR);
-  uint64_t *oOff = s_oOff.ensure(nr + 1), *nOff = s_nOff.ensure(nr + 1);
-  {
-    uint64_t *t5 = tmp(scan_tmp_elems(nr) + 4);
-    exclusive_scan(OldDeg{rlist, deg.get()}, nr, oOff, t5, stream, prof);
-    exclusive_scan(NewDeg{rlist, deg.get(), tu, tdn, nt}, nr, nOff, t5, stream, prof);
-  }
+  const uint64_t nrs = read_u64(cnt + C_NR);
   uint64_t SO = 0, SN = 0;
-  TRC_CUDA(cudaMemcpyAsync(&SO, oOff + nr, 8, cudaMemcpyDeviceToHost, stream));
-  TRC_CUDA(cudaMemcpyAsync(&SN, nOff + nr, 8, cudaMemcpyDeviceToHost, stream));
-  sync();
-
-  // ---- gather, merge / difference
-  uint64_t *oldk = s_old.ensure(SO + 1);
-  uint64_t *newk = s_new.ensure((SN > SO ? SN : SO) + 1);
-  TRC_LAUNCH(prof, stream, "upd_gather", ceil_div(nr * 32, 256), 256, 0, k_gather_old, G, rlist, nr,
-             oOff, oldk);
-  if (insert) {
-    merge_u64(oldk, SO, bkeys, kb, newk, stream, prof);
-  } else {
-    uint8_t *fl = s_flags.ensure(SO + 1);
-    uint64_t *t6 = tmp(select_tmp_elems(SO) + 4);
-    difference_u64(oldk, SO, bkeys, kb, newk, cnt + C_KU, fl, t6, stream, prof);
+  if (prof.on && nrs) {  // element counts for the profiler's byte accounting
+    uint64_t *oo = s_oOff.ensure(nrs + 1);
+    uint64_t *t5 = tmp(scan_tmp_elems(nrs) + 4);
+    exclusive_scan(OldDeg{rs, deg.get()}, nrs, oo, t5, stream, prof);
+    SO = read_u64(oo + nrs);
+    exclusive_scan(NewDeg{rs, deg.get(), tu, tdn, nt}, nrs, oo, t5, stream, prof);
+    SN = read_u64(oo + nrs);
+  }
+  if (nrs) {
+    uint32_t wpc = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(8, (48u << 10) / (4ull * T)));
+    size_t smem = (size_t)wpc * T * 4;
+    MergeArgs ma{rs, nrs, tu, tpos, nt, kb, bkeys, insert ? 1 : 0, pbeg_new, dst_pma, mov_pma,
+                 nmw ? wstamp.get() : nullptr, epoch, T};
+    TRC_LAUNCH(prof, stream, "upd_merge_small", ceil_div(nrs, wpc), wpc * 32, smem, k_merge_small, G,
+               ma);
   }
 
-  // ---- new tier-2 layout
-  if (rebuild) {
-    uint32_t *np = s_pma_next.alloc_exact(Nn);
-    TRC_LAUNCH(prof, stream, "upd_rebuild_layout", ceil_div((uint64_t)n + 1, 256), 256, 0,
-               k_rebuild_layout, P, n, Nn, pbeg.get());
-    (void)np;
-    rebuilds++;
-  } else if (nmw) {
-    TRC_LAUNCH(prof, stream, "upd_window_layout", nmw, 256, 0, k_window_layout, s_mw.get(), n, P,
-               pbeg.get());
-    window_rebalances += nmw;
-  }
-  if (!plan.empty()) {
+  // ---- hub path: gather / merge / scatter over the touched hubs (few)
+  uint64_t SOh = 0, SNh = 0;
+  if (nh) {
+    std::vector<uint32_t> rh(nh);
+    for (uint64_t i = 0; i < nh; i++) rh[i] = (uint32_t)plan[6 * i + 1];
+    std::sort(rh.begin(), rh.end());
+    uint32_t *drh = s_hw_t.ensure(nh);
+    TRC_CUDA(cudaMemcpyAsync(drh, rh.data(), nh * 4, cudaMemcpyHostToDevice, stream));
+    uint64_t *bkh = s_wk2.ensure(kb);
+    uint64_t *t6 = tmp(select_tmp_elems(kb) + scan_tmp_elems(nh) + 8);
+    select_if(KeyInListPred{bkeys, drh, nh}, LoadU64Val{bkeys}, kb, bkh, cnt + C_NW, t6, stream,
+              prof);
+    uint64_t *oOff = s_oOff.ensure(nh + 1), *nOff = s_nOff.ensure(nh + 1);
+    exclusive_scan(OldDeg{drh, deg.get()}, nh, oOff, t6, stream, prof);
+    exclusive_scan(NewDeg{drh, deg.get(), tu, tdn, nt}, nh, nOff, t6, stream, prof);
+    uint64_t hcnt[1];
+    TRC_CUDA(cudaMemcpyAsync(&SOh, oOff + nh, 8, cudaMemcpyDeviceToHost, stream));
+    TRC_CUDA(cudaMemcpyAsync(&SNh, nOff + nh, 8, cudaMemcpyDeviceToHost, stream));
+    TRC_CUDA(cudaMemcpyAsync(hcnt, cnt + C_NW, 8, cudaMemcpyDeviceToHost, stream));
+    sync();
+    const uint64_t kbh = hcnt[0];
+    uint64_t *oldk = s_old.ensure(SOh + 1);
+    uint64_t *newk = s_new.ensure((SNh > SOh ? SNh : SOh) + 1);
+    TRC_LAUNCH(prof, stream, "upd_gather", ceil_div(nh * 32, 256), 256, 0, k_gather_old, G, drh, nh,
+               oOff, oldk);
+    if (insert) {
+      merge_u64(oldk, SOh, bkh, kbh, newk, stream, prof);
+    } else {
+      uint8_t *fl = s_flags.ensure(SOh + 1);
+      uint64_t *t7 = tmp(select_tmp_elems(SOh) + 4);
+      difference_u64(oldk, SOh, bkh, kbh, newk, cnt + C_KU, fl, t7, stream, prof);
+    }
     uint64_t *dplan = s_hwplan.ensure(plan.size());
     TRC_CUDA(cudaMemcpyAsync(dplan, plan.data(), plan.size() * 8, cudaMemcpyHostToDevice, stream));
     TRC_LAUNCH(prof, stream, "upd_hub_plan", nh, 128, 0, k_apply_hub_plan, G, dplan, nh);
+    TRC_LAUNCH(prof, stream, "upd_scatter", ceil_div(nh * 32, 256), 256, 0, k_scatter_new, view(),
+               drh, nh, nOff, newk);
   }
-  DevView GN = view();
-  if (rebuild) {
-    GN.pma = s_pma_next.get();
-    GN.N = Nn;
+
+  // ---- window moves land after every reader of the old segments is done
+  if (nmw && nrs) {
+    DevView GC = view();
+    TRC_LAUNCH(prof, stream, "upd_window_copy", ceil_div(nrs * 32, 256), 256, 0, k_window_copy, GC,
+               rs, nrs, mov_pma, pbeg_new, wstamp.get(), epoch);
   }
-  TRC_LAUNCH(prof, stream, "upd_scatter", ceil_div(nr * 32, 256), 256, 0, k_scatter_new, GN, rlist,
-             nr, nOff, newk);
   TRC_LAUNCH(prof, stream, "upd_c2", ceil_div(nt, 256), 256, 0, k_scatter_c2_final, tu, tc2, nt,
              c2.get());
+  if (relayout) pbeg.swap(pbeg_alt);
   if (rebuild) {
     pma.swap(s_pma_next);
     s_pma_next.reset();
     N = Nn;
   }
-  if (!plan.empty()) sync();  // the host plan vector must outlive its copy
+  sync();  // host vectors (plan, rh) outlive their copies
+  const uint64_t nr = nrs + nh;
+  SO += SOh;
+  SN += SNh;
   m = insert ? m + kb : m - kb;
   tier2_total = rebuild ? Ptot : t2new;
   last[0] = k2;
