@@ -300,6 +300,8 @@ def kernel_bytes(name, sz):
     (DESIGN.md lists the formulas)."""
     k2, kb, nr = sz["last_keys"], sz["last_applied"], sz["last_rewritten"]
     so, sn = sz["last_gathered"], sz["last_written"]
+    if name == "upd_merge_small":  # old list in (4 B), batch keys in (8 B), new list out (4 B)
+        return 4 * so + 8 * kb + 4 * sn + 40 * nr
     if name == "upd_gather":      # old lists (4 B) -> 64-bit keys; per-vertex metadata
         return 12 * so + 28 * nr
     if name == "merge":           # two sorted key streams in, one out

@@ -171,7 +171,9 @@ trc_status trc_check(trc_graph *g, uint64_t *violations);
 
 /* Per-kernel device time, recorded with CUDA events on the handle's stream
  * around every launch while enabled.  trc_profile_get returns the summed
- * milliseconds and launch count of kernels whose name contains `name`. */
+ * milliseconds and launch count of the kernel called `name` (of every kernel
+ * whose name starts with the prefix when `name` ends in '*'; all kernels
+ * when `name` is NULL). */
 trc_status trc_profile_enable(trc_graph *g, int on);
 trc_status trc_profile_reset(trc_graph *g);
 trc_status trc_profile_get(trc_graph *g, const char *name, double *ms,

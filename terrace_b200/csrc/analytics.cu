@@ -29,12 +29,13 @@ constexpr int AT = 256;  // threads per CTA in the analytics kernels
 struct ClassPred {
   const uint32_t *deg;
   const int32_t *hub_of;
-  int cls;  // 0 = S, 1 = M, 2 = H
+  int cls;  // 0 = S, 1 = M, 2 = H, 3 = S and M (non-hub, degree >= 1)
   __device__ bool operator()(uint64_t i) const {
     bool hub = hub_of[i] >= 0;
     uint32_t d = deg[i];
     if (cls == 2) return hub;
     if (hub) return false;
+    if (cls == 3) return d >= 1;
     return cls == 0 ? (d >= 1 && d <= K_INLINE) : d > K_INLINE;
   }
 };
@@ -47,17 +48,19 @@ void Graph::ensure_lists() {
   if (lists.version == version) return;
   uint64_t *cnt = s_cnt.get() + 24;
   uint64_t *t = tmp(select_tmp_elems(n) + 4);
-  uint32_t *bufs[3] = {lists.S.ensure(n), lists.M.ensure(n), lists.Hv.ensure(H ? H : 1)};
-  uint64_t lens[3];
-  for (int c = 0; c < 3; c++) {
+  uint32_t *bufs[4] = {lists.S.ensure(n), lists.M.ensure(n), lists.Hv.ensure(H ? H : 1),
+                       lists.SM.ensure(n)};
+  uint64_t lens[4];
+  for (int c = 0; c < 4; c++) {
     select_if(ClassPred{deg.get(), hub_of.get(), c}, IdxVal32{}, n, bufs[c], cnt + c, t, stream,
               prof);
   }
-  TRC_CUDA(cudaMemcpyAsync(lens, cnt, 24, cudaMemcpyDeviceToHost, stream));
+  TRC_CUDA(cudaMemcpyAsync(lens, cnt, 32, cudaMemcpyDeviceToHost, stream));
   sync();
   lists.nS = lens[0];
   lists.nM = lens[1];
   lists.nH = lens[2];
+  lists.nSM = lens[3];
   lists.version = version;
 }
 
@@ -153,6 +156,125 @@ __global__ void __launch_bounds__(AT) k_pr_M(DevView G, const uint32_t *M, uint6
   if (lane == 0) pr_store(a, u, d, sum);
 }
 
+// Load-balanced pull.  Warp w takes list entries [32w, 32w+32); their
+// neighbour lists (inline row, then PMA segment or hub blocks) are flattened
+// and walked 64 elements per step: each lane finds the owner of its element
+// with a shuffle binary search over the lanes' start offsets, loads the
+// neighbour id and applies Op::gather; a segmented warp scan sums per owner
+// and the segment's last lane adds into the owner's slot in shared memory.
+// Every load of a step is independent of the others, so a warp keeps 64
+// index loads and 64 gathers in flight instead of one vertex's chain.
+struct FlatWarp {
+  uint32_t u, d, start, total, per;
+  const uint32_t *seg;
+  bool valid;
+};
+
+template <class Op>
+__device__ __forceinline__ FlatWarp flat_setup(const DevView &G, const uint32_t *V, uint64_t nV,
+                                               uint64_t base, const Op &op) {
+  FlatWarp f;
+  uint32_t lane = threadIdx.x & 31;
+  uint64_t idx = base + lane;
+  f.valid = idx < nV;
+  f.u = f.valid ? V[idx] : 0;
+  f.d = 0;
+  f.per = 0;
+  f.seg = G.pma;
+  if (f.valid && !op.skip(f.u)) {
+    f.d = G.deg[f.u];
+    if (f.d > K_INLINE) {
+      int32_t h = G.hub_of[f.u];
+      if (h < 0) {
+        f.seg = G.pma + G.pbeg[f.u];
+      } else {
+        f.seg = G.hslot + G.hub_blk0[h] * HUB_BLOCK;
+        f.per = G.hub_per[h];
+      }
+    }
+  }
+  uint32_t incl = warp_incl_scan(f.d);
+  f.start = incl - f.d;
+  f.total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  return f;
+}
+
+// owner lane of flattened element e (largest lane v with start_v <= e)
+__device__ __forceinline__ int flat_owner(const FlatWarp &f, uint32_t e) {
+  int v = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1) {
+    uint32_t sv = __shfl_sync(0xFFFFFFFFu, f.start, v + step);
+    if (sv <= e) v += step;
+  }
+  return v;
+}
+
+// element of flattened index e (owner v): its rank r = e - start_v
+__device__ __forceinline__ uint32_t flat_fetch(const DevView &G, const FlatWarp &f, int v,
+                                               uint32_t e, bool act) {
+  uint32_t uo = __shfl_sync(0xFFFFFFFFu, f.u, v);
+  uint32_t so = __shfl_sync(0xFFFFFFFFu, f.start, v);
+  uint32_t po = __shfl_sync(0xFFFFFFFFu, f.per, v);
+  const uint32_t *sg = (const uint32_t *)__shfl_sync(0xFFFFFFFFu, (unsigned long long)f.seg, v);
+  if (!act) return 0;
+  uint32_t r = e - so;
+  if (r < K_INLINE) return __ldg(G.inl + (uint64_t)uo * K_INLINE + r);
+  r -= K_INLINE;
+  if (po == 0) return __ldg(sg + r);
+  return __ldg(sg + (r / po) * HUB_BLOCK + (r % po));
+}
+
+// segmented inclusive sum over lanes (segments = equal owner), tail lanes
+// add the segment total into acc[owner]
+__device__ __forceinline__ void flat_seg_add(double val, int v, double *acc) {
+  uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    double t = __shfl_up_sync(0xFFFFFFFFu, val, o);
+    int vo = __shfl_up_sync(0xFFFFFFFFu, v, o);
+    if ((int)lane >= o && vo == v) val += t;
+  }
+  int vn = __shfl_down_sync(0xFFFFFFFFu, v, 1);
+  if (lane == 31 || vn != v) acc[v] += val;
+}
+
+template <class Op>
+__global__ void __launch_bounds__(AT) k_flat(DevView G, const uint32_t *V, uint64_t nV, Op op) {
+  __shared__ double acc_all[AT];
+  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint64_t base = ((uint64_t)blockIdx.x * (AT / 32) + wib) * 32;
+  if (base >= nV) return;
+  double *acc = acc_all + wib * 32;
+  FlatWarp f = flat_setup(G, V, nV, base, op);
+  acc[lane] = 0.0;
+  __syncwarp();
+  for (uint32_t e0 = 0; e0 < f.total; e0 += 64) {
+    uint32_t e1 = e0 + lane, e2 = e0 + 32 + lane;
+    bool a1 = e1 < f.total, a2 = e2 < f.total;
+    int v1 = flat_owner(f, a1 ? e1 : f.total - 1);
+    int v2 = flat_owner(f, a2 ? e2 : f.total - 1);
+    uint32_t x1 = flat_fetch(G, f, v1, e1, a1);
+    uint32_t x2 = flat_fetch(G, f, v2, e2, a2);
+    double g1 = a1 ? op.gather(x1) : 0.0;
+    double g2 = a2 ? op.gather(x2) : 0.0;
+    flat_seg_add(g1, v1, acc);
+    __syncwarp();
+    flat_seg_add(g2, v2, acc);
+    __syncwarp();
+  }
+  op.store(f.valid && f.d > 0, f.u, f.d, acc[lane]);
+}
+
+struct PROp {
+  PRArgs a;
+  __device__ bool skip(uint32_t) const { return false; }
+  __device__ double gather(uint32_t x) const { return __ldg(a.pc + x); }
+  __device__ void store(bool ok, uint32_t u, uint32_t d, double sum) const {
+    if (ok) pr_store(a, u, d, sum);
+  }
+};
+
 __global__ void __launch_bounds__(AT) k_pr_H(DevView G, const uint32_t *Hv, PRArgs a) {
   __shared__ double sh[AT / 32];
   uint32_t u = Hv[blockIdx.x];
@@ -206,10 +328,8 @@ void Graph::pagerank(uint32_t iters, double damping, double *ranks, uint32_t fla
     DevView G = view();
     for (uint32_t it = 0; it < iters; it++) {
       PRArgs a{p0, p1, out, damping, base, it + 1 == iters};
-      TRC_LAUNCH(prof, stream, "pr_S", ceil_div(lists.nS * 4, AT), AT, 0, k_pr_S, G, lists.S.get(),
-                 lists.nS, a);
-      TRC_LAUNCH(prof, stream, "pr_M", ceil_div(lists.nM * 32, AT), AT, 0, k_pr_M, G, lists.M.get(),
-                 lists.nM, a);
+      TRC_LAUNCH(prof, stream, "pr_flat", ceil_div(lists.nSM, AT), AT, 0, k_flat<PROp>, G,
+                 lists.SM.get(), lists.nSM, PROp{a});
       TRC_LAUNCH(prof, stream, "pr_H", lists.nH, AT, 0, k_pr_H, G, lists.Hv.get(), a);
       std::swap(p0, p1);
     }
@@ -295,11 +415,13 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
   if (win) s.next[pos] = u;
 }
 
-// One warp scans the neighbours of vertex u in sorted order and stops at
-// the first frontier member.  Returns that neighbour or NONE32 (warp-uniform).
-__device__ __forceinline__ uint32_t warp_first_in_frontier(const NbrList &L, const uint32_t *bits) {
+// One warp scans the neighbours of vertex u in sorted order from rank j_first
+// and stops at the first frontier member.  Returns that neighbour or NONE32
+// (warp-uniform).
+__device__ __forceinline__ uint32_t warp_first_in_frontier(const NbrList &L, const uint32_t *bits,
+                                                           uint32_t j_first) {
   uint32_t lane = threadIdx.x & 31;
-  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) {
+  for (uint32_t j0 = j_first; j0 < L.deg; j0 += 32) {
     uint32_t j = j0 + lane;
     uint32_t v = j < L.deg ? L.at(j) : 0;
     bool hit = j < L.deg && bit_test(bits, v);
@@ -309,9 +431,10 @@ __device__ __forceinline__ uint32_t warp_first_in_frontier(const NbrList &L, con
   return NONE32;
 }
 
-// Warp per vertex of a list (M or H class).
+// Warp per vertex of a list (M or H class), scanning from rank j_first (the
+// inline pass has already checked ranks below it for M vertices).
 __global__ void __launch_bounds__(AT) k_bfs_pull_W(DevView G, const uint32_t *Lst, uint64_t nL,
-                                                   BFSState s) {
+                                                   BFSState s, uint32_t j_first) {
   uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
   uint32_t lane = threadIdx.x & 31;
   if (w >= nL) return;
@@ -319,7 +442,7 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_W(DevView G, const uint32_t *Ls
   bool win = false;
   if (s.lv[u] == TRC_UNREACHED) {
     NbrList L = nbr_list(G, u);
-    uint32_t p = warp_first_in_frontier(L, s.bits);
+    uint32_t p = warp_first_in_frontier(L, s.bits, j_first);
     if (p != NONE32 && lane == 0) {
       s.par[u] = (int32_t)p;
       s.lv[u] = s.d + 1;
@@ -363,12 +486,14 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
     if ((uint64_t)nf >= dense_at && dense_at > 0) {
       TRC_CUDA(cudaMemsetAsync(bm, 0, words * 4, stream));
       TRC_LAUNCH(prof, stream, "bfs_bits", ceil_div(nf, AT), AT, 0, k_set_bits, F, nf, bm);
-      TRC_LAUNCH(prof, stream, "bfs_pull_S", ceil_div(lists.nS * 4, AT), AT, 0, k_bfs_pull_S, G,
-                 lists.S.get(), lists.nS, s);
+      // pass A: the 16 inline neighbours of every unvisited non-hub vertex
+      TRC_LAUNCH(prof, stream, "bfs_pull_inline", ceil_div(lists.nSM * 4, AT), AT, 0, k_bfs_pull_S,
+                 G, lists.SM.get(), lists.nSM, s);
+      // pass B: the PMA segments of those still unvisited; hubs from rank 0
       TRC_LAUNCH(prof, stream, "bfs_pull_M", ceil_div(lists.nM * 32, AT), AT, 0, k_bfs_pull_W, G,
-                 lists.M.get(), lists.nM, s);
+                 lists.M.get(), lists.nM, s, K_INLINE);
       TRC_LAUNCH(prof, stream, "bfs_pull_H", ceil_div(lists.nH * 32, AT), AT, 0, k_bfs_pull_W, G,
-                 lists.Hv.get(), lists.nH, s);
+                 lists.Hv.get(), lists.nH, s, 0u);
     } else {
       TRC_LAUNCH(prof, stream, "bfs_push", ceil_div((uint64_t)nf * 32, AT), AT, 0, k_bfs_push, G, F,
                  nf, s);
@@ -576,6 +701,39 @@ __global__ void __launch_bounds__(AT) k_bc_pull_S(DevView G, const uint32_t *S, 
   if (win) s.order[pos] = u;
 }
 
+// Dense forward step with the load-balanced pull: an unvisited vertex sums
+// sigma over its neighbours on level d; a positive sum puts it on level d+1.
+struct BCPullOp {
+  BCFwd s;
+  __device__ bool skip(uint32_t u) const { return s.lv[u] != TRC_UNREACHED; }
+  __device__ double gather(uint32_t x) const {
+    return __ldg(s.lv + x) == s.d ? __ldg(s.sigma + x) : 0.0;
+  }
+  __device__ void store(bool ok, uint32_t u, uint32_t, double sum) const {
+    bool win = ok && sum > 0.0;
+    if (win) {
+      s.sigma[u] = sum;
+      s.lv[u] = s.d + 1;
+    }
+    uint32_t pos = warp_append(win, s.next_cnt);
+    if (win) s.order[pos] = u;
+  }
+};
+
+// Backward step with the load-balanced pull over the vertices of level d:
+// dep[v] = sum of dep[w] over neighbours on level d+1, plus 1/sigma[v].
+struct BCBackOp {
+  const uint32_t *lv;
+  const double *inv;
+  double *dep;
+  uint32_t d;
+  __device__ bool skip(uint32_t) const { return false; }
+  __device__ double gather(uint32_t x) const { return __ldg(lv + x) == d + 1 ? dep[x] : 0.0; }
+  __device__ void store(bool ok, uint32_t u, uint32_t, double sum) const {
+    if (ok) dep[u] = sum + inv[u];
+  }
+};
+
 // Backward, one warp per vertex of level d:
 // dep[v] = sum of dep[w] over neighbours on level d+1, plus 1/sigma[v].
 __global__ void k_bc_back(DevView G, const uint32_t *Lv, uint32_t nv, const uint32_t *lv,
@@ -639,10 +797,8 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
     TRC_CUDA(cudaMemsetAsync(c, 0, 4, stream));
     BCFwd s{lv, sigma, order + f1, c, d};
     if ((uint64_t)nf >= dense_at && dense_at > 0) {
-      TRC_LAUNCH(prof, stream, "bc_pull_S", ceil_div(lists.nS * 4, AT), AT, 0, k_bc_pull_S, G,
-                 lists.S.get(), lists.nS, s);
-      TRC_LAUNCH(prof, stream, "bc_pull_M", ceil_div(lists.nM * 32, AT), AT, 0, k_bc_pull_W, G,
-                 lists.M.get(), lists.nM, s);
+      TRC_LAUNCH(prof, stream, "bc_pull_flat", ceil_div(lists.nSM, AT), AT, 0, k_flat<BCPullOp>,
+                 G, lists.SM.get(), lists.nSM, BCPullOp{s});
       TRC_LAUNCH(prof, stream, "bc_pull_H", ceil_div(lists.nH * 32, AT), AT, 0, k_bc_pull_W, G,
                  lists.Hv.get(), lists.nH, s);
     } else {
@@ -659,8 +815,8 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
   TRC_LAUNCH(prof, stream, "bc_inv", ceil_div(n, AT), AT, 0, k_bc_inv, sigma, inv, n);
   for (int64_t L = (int64_t)d - 1; L >= 0; L--) {
     uint64_t a = loff[L], b = loff[L + 1];
-    TRC_LAUNCH(prof, stream, "bc_back", ceil_div((b - a) * 32, AT), AT, 0, k_bc_back, G, order + a,
-               (uint32_t)(b - a), lv, inv, dep, (uint32_t)L);
+    TRC_LAUNCH(prof, stream, "bc_back_flat", ceil_div(b - a, AT), AT, 0, k_flat<BCBackOp>, G,
+               order + a, b - a, BCBackOp{lv, inv, dep, (uint32_t)L});
   }
   TRC_LAUNCH(prof, stream, "bc_final", ceil_div(n, AT), AT, 0, k_bc_final, dep, inv, out, n);
   if (!dev) TRC_CUDA(cudaMemcpyAsync(out_user, out, (uint64_t)n * 8, cudaMemcpyDeviceToHost, stream));

@@ -258,8 +258,11 @@ trc_status trc_profile_get(trc_graph *g, const char *name, double *ms, uint64_t 
     gr.prof.resolve();
     double t = 0;
     uint64_t c = 0;
+    std::string want = name ? name : "";
+    bool prefix = !want.empty() && want.back() == '*';
+    if (prefix) want.pop_back();
     for (auto &kv : gr.prof.totals) {
-      if (!name || kv.first.find(name) != std::string::npos) {
+      if (!name || (prefix ? kv.first.compare(0, want.size(), want) == 0 : kv.first == want)) {
         t += kv.second.first;
         c += kv.second.second;
       }

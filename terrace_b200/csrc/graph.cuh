@@ -23,8 +23,8 @@ __device__ __forceinline__ bool has_edge(const DevView &G, uint32_t u, uint32_t 
 // hub block (for block-parallel work on the blocked tier).
 struct ClassLists {
   uint64_t version = ~0ull;
-  DBuf<uint32_t> S, M, Hv, hub_blocks;
-  uint64_t nS = 0, nM = 0, nH = 0, nHB = 0;
+  DBuf<uint32_t> S, M, Hv, SM, hub_blocks;
+  uint64_t nS = 0, nM = 0, nH = 0, nSM = 0, nHB = 0;
 };
 
 class Graph {
@@ -73,6 +73,7 @@ class Graph {
   DBuf<uint64_t> s_P, s_oOff, s_nOff, s_wk, s_wk2, s_mw, s_old, s_new, s_hwplan;
   DBuf<uint8_t> s_flags;
   DBuf<uint32_t> s_pma_next;
+  DBuf<uint32_t> s_tix;  // vertex -> index in the touched list (this batch)
   ClassLists lists;
 
   DevView view() const;

@@ -48,7 +48,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   for (auto *b : {&deg, &inl, &c2, &pma, &err, &hub_vtx, &hub_nblk, &hub_per, &hslot, &bcnt, &bmin,
                   &bown, &stamp, &s_in_src, &s_in_dst, &s_tu, &s_tdn, &s_tc2, &s_ovl, &s_hw_u,
                   &s_hw_dn, &s_hw_t, &s_c2n, &s_rlist, &s_pma_next, &lists.S, &lists.M, &lists.Hv,
-                  &lists.hub_blocks})
+                  &lists.SM, &lists.hub_blocks})
     b->bind(&budget);
   for (auto *b : {&pbeg, &hub_blk0, &s_A, &s_B, &s_C, &s_tmp, &s_cnt, &s_P, &s_oOff, &s_nOff,
                   &s_wk, &s_wk2, &s_mw, &s_old, &s_new, &s_hwplan})
@@ -56,6 +56,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   hub_of.bind(&budget);
   wstamp.bind(&budget);
   pbeg_alt.bind(&budget);
+  s_tix.bind(&budget);
   s_hw_h.bind(&budget);
   s_flags.bind(&budget);
 
@@ -342,10 +343,22 @@ struct LoadU64Val {
   __device__ uint64_t operator()(uint64_t i) const { return p[i]; }
 };
 
-__global__ void k_mark_touched(const uint32_t *tu, uint64_t nt, uint32_t *stamp, uint32_t epoch) {
+// Marks the touched vertices and records u -> touched index (tix), so the
+// merge finds a vertex's slice of the batch without a search.  Runs after the
+// window / rebuild marking, which resets tix to NONE32 for its vertices.
+__global__ void k_mark_touched(const uint32_t *tu, uint64_t nt, uint32_t *stamp, uint32_t *tix,
+                               uint32_t epoch) {
   uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < nt) stamp[tu[t]] = epoch;
+  if (t < nt) {
+    stamp[tu[t]] = epoch;
+    tix[tu[t]] = (uint32_t)t;
+  }
 }
+
+// Slack of a layout is spread in proportion to (elements + PMA_VWEIGHT), so a
+// vertex with few or no PMA elements still gets a few free slots: a vertex
+// crossing the inline limit then usually fits without a window rebalance.
+constexpr uint64_t PMA_VWEIGHT = 4;
 
 __device__ __forceinline__ void window_range(uint64_t x, uint32_t n, uint64_t &a, uint64_t &b) {
   a = x >> 6;
@@ -362,8 +375,9 @@ __global__ void k_window_mark(const uint64_t *mw, uint32_t n, uint32_t *stamp, u
 }
 
 // One CTA per maximal window: new segment offsets of its vertices,
-// pbeg'[u] = pbeg[a] + (P[u]-P[a]) + floor(gap*(P[u]-P[a])/E); the window's
-// slot range [pbeg[a], pbeg[b]) is unchanged.
+// pbeg'[u] = pbeg[a] + (P[u]-P[a]) + floor(gap*Q(u)/Q(b)) with
+// Q(u) = (P[u]-P[a]) + PMA_VWEIGHT*(u-a); the window's slot range
+// [pbeg[a], pbeg[b]) is unchanged and every vertex keeps >= its elements.
 __global__ void k_window_layout(const uint64_t *mw, uint32_t n, const uint64_t *P, uint64_t *pbeg) {
   uint64_t a, b;
   window_range(mw[blockIdx.x], n, a, b);
@@ -371,11 +385,12 @@ __global__ void k_window_layout(const uint64_t *mw, uint32_t n, const uint64_t *
   uint64_t S = pbeg[b] - base;
   uint64_t E = P[b] - P[a];
   uint64_t gap = S - E;
+  uint64_t QW = E + PMA_VWEIGHT * (b - a);
   __syncthreads();  // every thread has read pbeg[a], pbeg[b] before any write
   for (uint64_t u = a + 1 + threadIdx.x; u < b; u += blockDim.x) {
     uint64_t e = P[u] - P[a];
-    unsigned __int128 q = (unsigned __int128)gap * e;
-    pbeg[u] = base + e + (uint64_t)(q / E);
+    uint64_t q = e + PMA_VWEIGHT * (u - a);
+    pbeg[u] = base + e + (uint64_t)(((unsigned __int128)gap * q) / QW);
   }
 }
 
@@ -384,15 +399,21 @@ __global__ void k_rebuild_layout(const uint64_t *P, uint32_t n, uint64_t Nn, uin
   uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (u > n) return;
   uint64_t tot = P[n];
-  uint64_t gap = Nn - tot;
+  uint64_t gap = Nn > tot ? Nn - tot : 0;
+  uint64_t QW = tot + PMA_VWEIGHT * (uint64_t)n;
   uint64_t e = P[u];
-  uint64_t extra = tot ? (uint64_t)(((unsigned __int128)gap * e) / tot) : 0;
+  uint64_t q = e + PMA_VWEIGHT * u;
+  uint64_t extra = QW ? (uint64_t)(((unsigned __int128)gap * q) / QW) : 0;
   pbeg[u] = (u == n) ? Nn : e + extra;
 }
 
-__global__ void k_mark_pma_vertices(const uint32_t *c2n, uint32_t n, uint32_t *stamp, uint32_t epoch) {
+__global__ void k_mark_pma_vertices(const uint32_t *c2n, uint32_t n, uint32_t *stamp,
+                                    uint32_t *tix, uint32_t epoch) {
   uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (u < n && c2n[u] > 0) stamp[u] = epoch;
+  if (u < n && c2n[u] > 0) {
+    stamp[u] = epoch;
+    tix[u] = NONE32;
+  }
 }
 
 struct StampPred {
@@ -412,18 +433,11 @@ struct OldDeg {
 
 // New degree of a rewrite-set vertex: from the touched table when touched.
 struct NewDeg {
-  const uint32_t *rlist, *deg, *tu, *tdn;
-  uint64_t nt;
+  const uint32_t *rlist, *deg, *tix, *tdn;
   __device__ uint64_t operator()(uint64_t i) const {
     uint32_t u = rlist[i];
-    uint64_t lo = 0, hi = nt;
-    while (lo < hi) {
-      uint64_t mid = (lo + hi) >> 1;
-      if (tu[mid] < u) lo = mid + 1;
-      else hi = mid;
-    }
-    if (lo < nt && tu[lo] == u) return tdn[lo];
-    return deg[u];
+    uint32_t t = tix[u];
+    return t != NONE32 ? tdn[t] : deg[u];
   }
 };
 
@@ -514,29 +528,17 @@ __global__ void k_scatter_c2_final(const uint32_t *tu, const uint32_t *tc2, uint
 // PMA segment (in place, or to the layout's new position).  About 8 bytes of
 // HBM traffic per list element instead of a gather / global merge / scatter.
 
-// Position of vertex u in the sorted touched list, or nt.
-__device__ __forceinline__ uint64_t touched_index(const uint32_t *tu, uint64_t nt, uint32_t u) {
-  uint64_t lo = 0, hi = nt;
-  while (lo < hi) {
-    uint64_t mid = (lo + hi) >> 1;
-    if (tu[mid] < u) lo = mid + 1;
-    else hi = mid;
-  }
-  return (lo < nt && tu[lo] == u) ? lo : nt;
-}
-
 // Rewrite-set members handled by the fused merge: non-hubs that stay <= T.
 struct SmallPred {
   const uint32_t *stamp;
   uint32_t epoch;
   const int32_t *hub_of;
-  const uint32_t *deg, *tu, *tdn;
-  uint64_t nt;
+  const uint32_t *deg, *tix, *tdn;
   uint32_t T;
   __device__ bool operator()(uint64_t i) const {
     if (stamp[i] != epoch || hub_of[i] >= 0) return false;
-    uint64_t t = touched_index(tu, nt, (uint32_t)i);
-    uint32_t dn = t < nt ? tdn[t] : deg[i];
+    uint32_t t = tix[i];
+    uint32_t dn = t != NONE32 ? tdn[t] : deg[i];
     return dn <= T;
   }
 };
@@ -544,7 +546,7 @@ struct SmallPred {
 struct MergeArgs {
   const uint32_t *rs;
   uint64_t nrs;
-  const uint32_t *tu;
+  const uint32_t *tix;
   const uint64_t *tpos;
   uint64_t nt, kb;
   const uint64_t *bkeys;
@@ -587,9 +589,9 @@ __global__ void k_merge_small(DevView G, MergeArgs a) {
   NbrList L = nbr_list(G, u);
   const uint32_t d = L.deg;
   for (uint32_t j = lane; j < d; j += 32) A[j] = L.at(j);
-  uint64_t t = touched_index(a.tu, a.nt, u);
+  uint64_t t = a.tix[u];
   uint64_t b0 = 0, b1 = 0;
-  if (t < a.nt) {
+  if (t != NONE32) {
     b0 = a.tpos[t];
     b1 = t + 1 < a.nt ? a.tpos[t + 1] : a.kb;
   }
@@ -641,12 +643,13 @@ __global__ void k_window_copy(DevView G, const uint32_t *rs, uint64_t nrs, const
 }
 
 __global__ void k_window_mark2(const uint64_t *mw, uint32_t n, uint32_t *stamp, uint32_t *wstamp,
-                               uint32_t epoch) {
+                               uint32_t *tix, uint32_t epoch) {
   uint64_t a, b;
   window_range(mw[blockIdx.x], n, a, b);
   for (uint64_t u = a + threadIdx.x; u < b; u += blockDim.x) {
     stamp[u] = epoch;
     wstamp[u] = epoch;
+    tix[u] = NONE32;
   }
 }
 
@@ -818,18 +821,19 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     TRC_CUDA(cudaMemsetAsync(wstamp.get(), 0, (uint64_t)n * 4, stream));
     epoch = 1;
   }
-  TRC_LAUNCH(prof, stream, "upd_mark", ceil_div(nt, 256), 256, 0, k_mark_touched, tu, nt,
-             stamp.get(), epoch);
+  uint32_t *tix = s_tix.ensure(n);
   if (nmw)
     TRC_LAUNCH(prof, stream, "upd_window_mark", nmw, 256, 0, k_window_mark2, s_mw.get(), n,
-               stamp.get(), wstamp.get(), epoch);
+               stamp.get(), wstamp.get(), tix, epoch);
   uint64_t Ptot = 0;
   if (rebuild) {
     Ptot = read_u64(P + n);  // the layout kernel spreads exactly this many
     Nn = std::max<uint64_t>((uint64_t)std::ceil((double)Ptot / build_d), Ptot + 1);
     TRC_LAUNCH(prof, stream, "upd_mark_pma", ceil_div(n, 256), 256, 0, k_mark_pma_vertices, c2n, n,
-               stamp.get(), epoch);
+               stamp.get(), tix, epoch);
   }
+  TRC_LAUNCH(prof, stream, "upd_mark", ceil_div(nt, 256), 256, 0, k_mark_touched, tu, nt,
+             stamp.get(), tix, epoch);
 
   // ---- new tier-2 layout (into pbeg_alt; pbeg keeps the old one until the end)
   const bool relayout = rebuild || nmw;
@@ -858,7 +862,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   uint32_t *rs = s_rlist.ensure(n);
   {
     uint64_t *t4 = tmp(select_tmp_elems(n) + 4);
-    select_if(SmallPred{stamp.get(), epoch, hub_of.get(), deg.get(), tu, tdn, nt, T}, IndexVal32{},
+    select_if(SmallPred{stamp.get(), epoch, hub_of.get(), deg.get(), tix, tdn, T}, IndexVal32{},
               n, rs, cnt + C_NR, t4, stream, prof);
   }
   const uint64_t nrs = read_u64(cnt + C_NR);
@@ -868,13 +872,13 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     uint64_t *t5 = tmp(scan_tmp_elems(nrs) + 4);
     exclusive_scan(OldDeg{rs, deg.get()}, nrs, oo, t5, stream, prof);
     SO = read_u64(oo + nrs);
-    exclusive_scan(NewDeg{rs, deg.get(), tu, tdn, nt}, nrs, oo, t5, stream, prof);
+    exclusive_scan(NewDeg{rs, deg.get(), tix, tdn}, nrs, oo, t5, stream, prof);
     SN = read_u64(oo + nrs);
   }
   if (nrs) {
     uint32_t wpc = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(8, (48u << 10) / (4ull * T)));
     size_t smem = (size_t)wpc * T * 4;
-    MergeArgs ma{rs, nrs, tu, tpos, nt, kb, bkeys, insert ? 1 : 0, pbeg_new, dst_pma, mov_pma,
+    MergeArgs ma{rs, nrs, tix, tpos, nt, kb, bkeys, insert ? 1 : 0, pbeg_new, dst_pma, mov_pma,
                  nmw ? wstamp.get() : nullptr, epoch, T};
     TRC_LAUNCH(prof, stream, "upd_merge_small", ceil_div(nrs, wpc), wpc * 32, smem, k_merge_small, G,
                ma);
@@ -894,7 +898,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
               prof);
     uint64_t *oOff = s_oOff.ensure(nh + 1), *nOff = s_nOff.ensure(nh + 1);
     exclusive_scan(OldDeg{drh, deg.get()}, nh, oOff, t6, stream, prof);
-    exclusive_scan(NewDeg{drh, deg.get(), tu, tdn, nt}, nh, nOff, t6, stream, prof);
+    exclusive_scan(NewDeg{drh, deg.get(), tix, tdn}, nh, nOff, t6, stream, prof);
     uint64_t hcnt[1];
     TRC_CUDA(cudaMemcpyAsync(&SOh, oOff + nh, 8, cudaMemcpyDeviceToHost, stream));
     TRC_CUDA(cudaMemcpyAsync(&SNh, nOff + nh, 8, cudaMemcpyDeviceToHost, stream));
