@@ -29,13 +29,16 @@ constexpr int AT = 256;  // threads per CTA in the analytics kernels
 struct ClassPred {
   const uint32_t *deg;
   const int32_t *hub_of;
-  int cls;  // 0 = S, 1 = M, 2 = H, 3 = S and M (non-hub, degree >= 1)
+  int cls;  // 0 = S, 1 = M, 2 = H, 3 = S and M (non-hub, degree >= 1),
+            // 4 = M with 17..64 neighbours, 5 = M with more than 64
   __device__ bool operator()(uint64_t i) const {
     bool hub = hub_of[i] >= 0;
     uint32_t d = deg[i];
     if (cls == 2) return hub;
     if (hub) return false;
     if (cls == 3) return d >= 1;
+    if (cls == 4) return d > K_INLINE && d <= 64;
+    if (cls == 5) return d > 64;
     return cls == 0 ? (d >= 1 && d <= K_INLINE) : d > K_INLINE;
   }
 };
@@ -48,19 +51,21 @@ void Graph::ensure_lists() {
   if (lists.version == version) return;
   uint64_t *cnt = s_cnt.get() + 24;
   uint64_t *t = tmp(select_tmp_elems(n) + 4);
-  uint32_t *bufs[4] = {lists.S.ensure(n), lists.M.ensure(n), lists.Hv.ensure(H ? H : 1),
-                       lists.SM.ensure(n)};
-  uint64_t lens[4];
-  for (int c = 0; c < 4; c++) {
+  uint32_t *bufs[6] = {lists.S.ensure(n), lists.M.ensure(n), lists.Hv.ensure(H ? H : 1),
+                       lists.SM.ensure(n), lists.M1.ensure(n), lists.M2.ensure(n)};
+  uint64_t lens[6];
+  for (int c = 0; c < 6; c++) {
     select_if(ClassPred{deg.get(), hub_of.get(), c}, IdxVal32{}, n, bufs[c], cnt + c, t, stream,
               prof);
   }
-  TRC_CUDA(cudaMemcpyAsync(lens, cnt, 32, cudaMemcpyDeviceToHost, stream));
+  TRC_CUDA(cudaMemcpyAsync(lens, cnt, 48, cudaMemcpyDeviceToHost, stream));
   sync();
   lists.nS = lens[0];
   lists.nM = lens[1];
   lists.nH = lens[2];
   lists.nSM = lens[3];
+  lists.nM1 = lens[4];
+  lists.nM2 = lens[5];
   lists.version = version;
 }
 
@@ -275,6 +280,41 @@ struct PROp {
   }
 };
 
+// Group pull for PMA vertices: GS lanes per vertex (8 for 17..64 neighbours,
+// 32 above), each lane issuing up to 8 independent index loads and then 8
+// gathers before using any of them; a shuffle reduction within the group.
+template <int GS>
+__global__ void __launch_bounds__(AT) k_pr_group(DevView G, const uint32_t *V, uint64_t nV, PRArgs a) {
+  constexpr int U = 8;
+  uint64_t gt = (uint64_t)blockIdx.x * AT + threadIdx.x;
+  uint64_t vi = gt / GS;
+  uint32_t q = gt % GS;
+  double sum = 0.0;
+  uint32_t u = 0, d = 0;
+  if (vi < nV) {
+    u = V[vi];
+    d = G.deg[u];
+    const uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
+    const uint32_t *seg = G.pma + G.pbeg[u] - K_INLINE;  // index by rank
+    for (uint32_t j0 = q; j0 < d; j0 += GS * U) {
+      uint32_t x[U];
+#pragma unroll
+      for (int k = 0; k < U; k++) {
+        uint32_t j = j0 + k * GS;
+        x[k] = j < d ? (j < K_INLINE ? __ldg(row + j) : __ldg(seg + j)) : 0u;
+      }
+#pragma unroll
+      for (int k = 0; k < U; k++) {
+        uint32_t j = j0 + k * GS;
+        if (j < d) sum += __ldg(a.pc + x[k]);
+      }
+    }
+  }
+#pragma unroll
+  for (int o = GS / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+  if (vi < nV && q == 0) pr_store(a, u, d, sum);
+}
+
 __global__ void __launch_bounds__(AT) k_pr_H(DevView G, const uint32_t *Hv, PRArgs a) {
   __shared__ double sh[AT / 32];
   uint32_t u = Hv[blockIdx.x];
@@ -328,8 +368,12 @@ void Graph::pagerank(uint32_t iters, double damping, double *ranks, uint32_t fla
     DevView G = view();
     for (uint32_t it = 0; it < iters; it++) {
       PRArgs a{p0, p1, out, damping, base, it + 1 == iters};
-      TRC_LAUNCH(prof, stream, "pr_flat", ceil_div(lists.nSM, AT), AT, 0, k_flat<PROp>, G,
-                 lists.SM.get(), lists.nSM, PROp{a});
+      TRC_LAUNCH(prof, stream, "pr_S", ceil_div(lists.nS * 4, AT), AT, 0, k_pr_S, G, lists.S.get(),
+                 lists.nS, a);
+      TRC_LAUNCH(prof, stream, "pr_M8", ceil_div(lists.nM1 * 8, AT), AT, 0, k_pr_group<8>, G,
+                 lists.M1.get(), lists.nM1, a);
+      TRC_LAUNCH(prof, stream, "pr_M32", ceil_div(lists.nM2 * 32, AT), AT, 0, k_pr_group<32>, G,
+                 lists.M2.get(), lists.nM2, a);
       TRC_LAUNCH(prof, stream, "pr_H", lists.nH, AT, 0, k_pr_H, G, lists.Hv.get(), a);
       std::swap(p0, p1);
     }

@@ -23,8 +23,8 @@ __device__ __forceinline__ bool has_edge(const DevView &G, uint32_t u, uint32_t 
 // hub block (for block-parallel work on the blocked tier).
 struct ClassLists {
   uint64_t version = ~0ull;
-  DBuf<uint32_t> S, M, Hv, SM, hub_blocks;
-  uint64_t nS = 0, nM = 0, nH = 0, nSM = 0, nHB = 0;
+  DBuf<uint32_t> S, M, Hv, SM, M1, M2, hub_blocks;
+  uint64_t nS = 0, nM = 0, nH = 0, nSM = 0, nM1 = 0, nM2 = 0, nHB = 0;
 };
 
 class Graph {
@@ -104,6 +104,10 @@ class Graph {
   uint64_t tc();
 
   // helpers
+  // Host wall time since the previous phase mark, accumulated under
+  // "host:<name>" while profiling (shows syncs and host work per phase).
+  void phase(const char *name);
+  double phase_t0 = 0.0;
   uint64_t read_u64(const uint64_t *dptr);
   void sync();
   uint32_t push_pull_divisor() const {

@@ -31,6 +31,7 @@
 // Set semantics throughout: the reference's duplicate leak (include/graph.h:
 // 269-289) and absent-edge remove (include/graph.h:695-716) do not occur.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 
@@ -48,7 +49,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   for (auto *b : {&deg, &inl, &c2, &pma, &err, &hub_vtx, &hub_nblk, &hub_per, &hslot, &bcnt, &bmin,
                   &bown, &stamp, &s_in_src, &s_in_dst, &s_tu, &s_tdn, &s_tc2, &s_ovl, &s_hw_u,
                   &s_hw_dn, &s_hw_t, &s_c2n, &s_rlist, &s_pma_next, &lists.S, &lists.M, &lists.Hv,
-                  &lists.SM, &lists.hub_blocks})
+                  &lists.SM, &lists.M1, &lists.M2, &lists.hub_blocks})
     b->bind(&budget);
   for (auto *b : {&pbeg, &hub_blk0, &s_A, &s_B, &s_C, &s_tmp, &s_cnt, &s_P, &s_oOff, &s_nOff,
                   &s_wk, &s_wk2, &s_mw, &s_old, &s_new, &s_hwplan})
@@ -122,6 +123,19 @@ uint32_t Graph::vbits() const {
 }
 
 void Graph::sync() { TRC_CUDA(cudaStreamSynchronize(stream)); }
+
+void Graph::phase(const char *name) {
+  if (!prof.on) return;
+  double now = std::chrono::duration<double, std::milli>(
+                   std::chrono::steady_clock::now().time_since_epoch())
+                   .count();
+  if (name) {
+    auto &t = prof.totals[std::string("host:") + name];
+    t.first += now - phase_t0;
+    t.second += 1;
+  }
+  phase_t0 = now;
+}
 
 uint64_t Graph::read_u64(const uint64_t *dptr) {
   uint64_t v = 0;
@@ -679,6 +693,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   if (!src_in || !dst_in) throw_error(TRC_ERR_INVALID, "null edge array");
   const int sym = (flags & TRC_SYMMETRIZE) ? 1 : 0;
   const int drop = (flags & TRC_DROP_SELF_LOOPS) ? 1 : 0;
+  phase(nullptr);
   const uint32_t *src = to_device(*this, src_in, k, flags, s_in_src);
   const uint32_t *dst = to_device(*this, dst_in, k, flags, s_in_dst);
   const uint64_t k2 = sym ? 2 * k : k;
@@ -709,6 +724,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   TRC_CUDA(cudaMemcpyAsync(&herr, err.get(), 4, cudaMemcpyDeviceToHost, stream));
   sync();
   if (herr & ERR_BAD_VERTEX) throw_error(TRC_ERR_INVALID, "vertex id out of range [0, n)");
+  phase("sort_filter");
   const uint64_t kb = hc[C_KB], nt = hc[C_NT];
   if (kb == 0) {
     for (auto &x : last) x = 0;
@@ -728,6 +744,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   const int64_t t2delta = (int64_t)hc[C_T2DELTA];
   const uint64_t t2new = (uint64_t)((int64_t)tier2_total + t2delta);
 
+  phase("classify");
   // ---- hub plan (host): indices for new hubs, regions for grown ones.
   std::vector<uint64_t> plan;
   if (nh) {
@@ -772,6 +789,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     G = view();
   }
 
+  phase("hub_plan");
   // ---- PMA planning
   bool rebuild = false;
   uint64_t nmw = 0;
@@ -814,6 +832,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     }
   }
 
+  phase("pma_plan");
   // ---- rewrite set: touched vertices, window members, (rebuild) all PMA vertices
   epoch++;
   if (epoch == 0) {  // wrapped: clear the marks
@@ -857,6 +876,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     }
   }
 
+  phase("layout");
   // ---- fused merge for every rewrite vertex that stays in tiers 1-2
   const uint32_t T = cfg.hub_threshold;
   uint32_t *rs = s_rlist.ensure(n);
@@ -884,6 +904,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
                ma);
   }
 
+  phase("merge_small");
   // ---- hub path: gather / merge / scatter over the touched hubs (few)
   uint64_t SOh = 0, SNh = 0;
   if (nh) {
@@ -923,6 +944,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
                drh, nh, nOff, newk);
   }
 
+  phase("hub_path");
   // ---- window moves land after every reader of the old segments is done
   if (nmw && nrs) {
     DevView GC = view();
@@ -938,6 +960,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     N = Nn;
   }
   sync();  // host vectors (plan, rh) outlive their copies
+  phase("finish");
   const uint64_t nr = nrs + nh;
   SO += SOh;
   SN += SNh;
