@@ -61,6 +61,10 @@ typedef struct {
   uint32_t push_pull_divisor; /* edgeMap goes dense when |F| >= n/divisor;
                                  reference threshold 20 (include/Map.cpp:65-74).
                                  0 = the autotuned value (default 20). */
+  uint32_t hub_stage_limit;   /* largest hub list (elements) merged by the
+                                 shared-memory hub kernel; larger hubs take
+                                 the gather/merge/scatter path.  Default and
+                                 maximum 49152. */
 } trc_config;
 
 /* Fill `cfg` with the defaults listed above. */

@@ -38,7 +38,8 @@ class trc_config(C.Structure):
                 ("pma_root_density", C.c_double),
                 ("pma_build_density", C.c_double),
                 ("hub_block_fill", C.c_double),
-                ("push_pull_divisor", C.c_uint32)]
+                ("push_pull_divisor", C.c_uint32),
+                ("hub_stage_limit", C.c_uint32)]
 
 
 class trc_stats(C.Structure):

@@ -51,6 +51,7 @@ void trc_config_default(trc_config *cfg) {
   cfg->pma_build_density = 0.5;
   cfg->hub_block_fill = 0.75;
   cfg->push_pull_divisor = 20;
+  cfg->hub_stage_limit = 49152;
 }
 
 const char *trc_status_string(trc_status s) {
@@ -80,6 +81,7 @@ trc_status trc_graph_create(uint32_t n, uint64_t hbm_budget_bytes, const trc_con
     if (cfg) c = *cfg;
     if (c.hub_threshold < trc::K_INLINE || c.hub_threshold > 12288)
       trc::throw_error(TRC_ERR_INVALID, "hub_threshold must be in [16, 12288]");
+    if (c.hub_stage_limit > 49152 || c.hub_stage_limit == 0) c.hub_stage_limit = 49152;
     *out = nullptr;
     trc_graph *h = new trc_graph{nullptr};
     try {

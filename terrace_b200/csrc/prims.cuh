@@ -118,22 +118,24 @@ inline uint64_t scan_tmp_elems(uint64_t n) {
 }
 
 template <typename F>
-void exclusive_scan(F f, uint64_t n, uint64_t *out, uint64_t *tmp, cudaStream_t s, Profiler &prof) {
+void exclusive_scan(F f, uint64_t n, uint64_t *out, uint64_t *tmp, cudaStream_t s, Profiler &prof,
+                    const char *tag = "scan") {
   if (n == 0) {
     TRC_CUDA(cudaMemsetAsync(out, 0, sizeof(uint64_t), s));
     return;
   }
+  const std::string t_sum = std::string(tag) + ".sum", t_tile = std::string(tag) + ".tile";
   uint64_t tiles = ceil_div(n, PTILE);
   if (tiles == 1) {
     TRC_CUDA(cudaMemsetAsync(tmp, 0, sizeof(uint64_t), s));
-    TRC_LAUNCH(prof, s, "scan_tile", 1, PT, 0, k_tile_scan<F>, f, n, tmp, out);
+    TRC_LAUNCH(prof, s, t_tile.c_str(), 1, PT, 0, k_tile_scan<F>, f, n, tmp, out);
     return;
   }
   uint64_t *sums = tmp;              // tiles entries
   uint64_t *offs = tmp + tiles;      // tiles+1 entries
-  TRC_LAUNCH(prof, s, "scan_sum", tiles, PT, 0, k_tile_sum<F>, f, n, sums);
-  exclusive_scan(LoadU64{sums}, tiles, offs, offs + tiles + 1, s, prof);
-  TRC_LAUNCH(prof, s, "scan_tile", tiles, PT, 0, k_tile_scan<F>, f, n, offs, out);
+  TRC_LAUNCH(prof, s, t_sum.c_str(), tiles, PT, 0, k_tile_sum<F>, f, n, sums);
+  exclusive_scan(LoadU64{sums}, tiles, offs, offs + tiles + 1, s, prof, "scan_tiles");
+  TRC_LAUNCH(prof, s, t_tile.c_str(), tiles, PT, 0, k_tile_scan<F>, f, n, offs, out);
 }
 
 // ----------------------------------------------------------------- select
@@ -171,19 +173,20 @@ __global__ void k_select_scatter(P pred, V val, uint64_t n, const uint64_t *tile
 
 template <typename P, typename V, typename T>
 void select_if(P pred, V val, uint64_t n, T *out, uint64_t *count, uint64_t *tmp, cudaStream_t s,
-               Profiler &prof) {
+               Profiler &prof, const char *tag = "select") {
   if (n == 0) {
     TRC_CUDA(cudaMemsetAsync(count, 0, sizeof(uint64_t), s));
     return;
   }
+  const std::string t_cnt = std::string(tag) + ".count", t_sc = std::string(tag) + ".scatter";
   uint64_t tiles = ceil_div(n, PTILE);
   uint64_t *sums = tmp;
   uint64_t *offs = tmp + tiles;
-  TRC_LAUNCH(prof, s, "select_count", tiles, PT, 0, k_tile_sum<PredCount<P>>, PredCount<P>{pred}, n,
+  TRC_LAUNCH(prof, s, t_cnt.c_str(), tiles, PT, 0, k_tile_sum<PredCount<P>>, PredCount<P>{pred}, n,
              sums);
-  exclusive_scan(LoadU64{sums}, tiles, offs, offs + tiles + 1, s, prof);
+  exclusive_scan(LoadU64{sums}, tiles, offs, offs + tiles + 1, s, prof, "scan_tiles");
   auto kscatter = k_select_scatter<P, V, T>;
-  TRC_LAUNCH(prof, s, "select_scatter", tiles, PT, 0, kscatter, pred, val, n, offs, out, count);
+  TRC_LAUNCH(prof, s, t_sc.c_str(), tiles, PT, 0, kscatter, pred, val, n, offs, out, count);
 }
 
 inline uint64_t select_tmp_elems(uint64_t n) {

@@ -58,6 +58,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   wstamp.bind(&budget);
   pbeg_alt.bind(&budget);
   s_tix.bind(&budget);
+  s_hw_do.bind(&budget);
   s_hw_h.bind(&budget);
   s_flags.bind(&budget);
 
@@ -187,25 +188,25 @@ __global__ void k_make_keys(const uint32_t *src, const uint32_t *dst, uint64_t k
   }
 }
 
-struct UniquePred {
-  const uint64_t *k;
-  __device__ bool operator()(uint64_t i) const {
-    uint64_t x = k[i];
-    return x != KEY_INVALID && (i == 0 || k[i - 1] != x);
-  }
-};
-
-struct ExistPred {
-  DevView G;
-  const uint64_t *keys;
-  const uint64_t *count;
-  int insert;
-  __device__ bool operator()(uint64_t i) const {
-    if (i >= *count) return false;
-    uint64_t x = keys[i];
+// Unique test and existence filter in one pass, one tier lookup per key:
+// flag[i] = key i is the first of its run and (insert: absent / remove:
+// present) in the graph.
+__global__ void k_filter_flags(DevView G, const uint64_t *keys, uint64_t k2, int insert,
+                               uint8_t *flags) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= k2) return;
+  uint64_t x = keys[i];
+  bool keep = x != KEY_INVALID && (i == 0 || keys[i - 1] != x);
+  if (keep) {
     bool has = has_edge(G, (uint32_t)(x >> 32), (uint32_t)x);
-    return insert ? !has : has;
+    keep = insert ? !has : has;
   }
+  flags[i] = keep ? 1 : 0;
+}
+
+struct FlagPred {
+  const uint8_t *f;
+  __device__ bool operator()(uint64_t i) const { return f[i] != 0; }
 };
 
 struct RunStartPred {
@@ -252,10 +253,10 @@ __device__ __forceinline__ uint64_t warp_append64(bool take, unsigned long long 
 __global__ void k_classify(DevView G, const uint64_t *bkeys, const uint64_t *tpos, uint64_t nt,
                            uint64_t kb, int insert, uint32_t *tu, uint32_t *tdn, uint32_t *tc2,
                            uint32_t *ovl, uint32_t *hw_u, uint32_t *hw_dn, uint32_t *hw_t,
-                           int32_t *hw_h, uint64_t *cnt) {
+                           int32_t *hw_h, uint32_t *hw_do, uint64_t *cnt) {
   uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   bool valid = t < nt;
-  uint32_t u = 0, dn = 0;
+  uint32_t u = 0, dn = 0, d = 0;
   int32_t h = -1;
   bool hub = false, over = false;
   long long delta = 0;
@@ -264,7 +265,7 @@ __global__ void k_classify(DevView G, const uint64_t *bkeys, const uint64_t *tpo
     uint64_t p1 = t + 1 < nt ? tpos[t + 1] : kb;
     u = (uint32_t)(bkeys[p0] >> 32);
     uint32_t c = (uint32_t)(p1 - p0);
-    uint32_t d = G.deg[u];
+    d = G.deg[u];
     dn = insert ? d + c : d - c;
     h = G.hub_of[u];
     hub = h >= 0 || dn > G.hub_T;
@@ -289,6 +290,7 @@ __global__ void k_classify(DevView G, const uint64_t *bkeys, const uint64_t *tpo
     hw_dn[j] = dn;
     hw_t[j] = (uint32_t)t;
     hw_h[j] = h;
+    hw_do[j] = d;
   }
 }
 
@@ -667,6 +669,85 @@ __global__ void k_window_mark2(const uint64_t *mw, uint32_t n, uint32_t *stamp, 
   }
 }
 
+// Fused merge for touched hubs, one CTA per hub: the old list (inline row +
+// blocks, or inline row + PMA segment for a vertex promoted now) is staged in
+// shared memory, output ranks come from binary searches as in k_merge_small,
+// and the new list is written to the hub's region (from the host plan) with
+// uniform block fill; thread 0 then updates the hub tables.
+struct HubMergeArgs {
+  const uint64_t *plan;  // rows {h, u, blk0, nb, per, capb}
+  uint64_t nh;
+  const uint32_t *tix;
+  const uint64_t *tpos;
+  uint64_t nt, kb;
+  const uint64_t *bkeys;
+  int insert;
+};
+
+__global__ void __launch_bounds__(256) k_merge_hub(DevView G, HubMergeArgs a) {
+  extern __shared__ uint32_t A[];
+  const uint64_t *p = a.plan + 6 * (uint64_t)blockIdx.x;
+  const uint32_t h = (uint32_t)p[0], u = (uint32_t)p[1];
+  const uint64_t blk0 = p[2];
+  const uint32_t nbn = (uint32_t)p[3], per = (uint32_t)p[4], capb = (uint32_t)p[5];
+  NbrList L = nbr_list(G, u);  // old tier pointers
+  const uint32_t d = L.deg;
+  for (uint32_t j = threadIdx.x; j < d; j += blockDim.x) A[j] = L.at(j);
+  const uint32_t t = a.tix[u];
+  const uint64_t b0 = a.tpos[t];
+  const uint64_t b1 = t + 1 < a.nt ? a.tpos[t + 1] : a.kb;
+  const uint32_t nb = (uint32_t)(b1 - b0);
+  const uint64_t *B = a.bkeys + b0;
+  const uint32_t dn = a.insert ? d + nb : d - nb;
+  const uint32_t rest = dn > K_INLINE ? dn - K_INLINE : 0;
+  __syncthreads();
+  uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
+  auto put = [&](uint32_t r, uint32_t x) {
+    if (r < K_INLINE) {
+      row[r] = x;
+      return;
+    }
+    uint32_t rr = r - K_INLINE;
+    uint32_t bi = rr / per, si = rr - bi * per;
+    G.hslot[(blk0 + bi) * HUB_BLOCK + si] = x;
+    if (si == 0) {
+      uint32_t c = rest - bi * per;
+      G.bcnt[blk0 + bi] = c < per ? c : per;
+      G.bmin[blk0 + bi] = x;
+      G.bown[blk0 + bi] = u;
+    }
+  };
+  if (a.insert) {
+    for (uint32_t i = threadIdx.x; i < d; i += blockDim.x) {
+      uint32_t x = A[i];
+      put(i + lower_bound_keys(B, nb, x), x);
+    }
+    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
+      uint32_t x = (uint32_t)B[j];
+      put(j + lower_bound_u32(A, d, x), x);
+    }
+  } else {
+    for (uint32_t i = threadIdx.x; i < d; i += blockDim.x) {
+      uint32_t x = A[i];
+      uint32_t c = lower_bound_keys(B, nb, x);
+      if (c < nb && (uint32_t)B[c] == x) continue;
+      put(i - c, x);
+    }
+  }
+  for (uint32_t b = nbn + threadIdx.x; b < capb; b += blockDim.x) {
+    G.bcnt[blk0 + b] = 0;
+    G.bown[blk0 + b] = NONE32;
+  }
+  if (threadIdx.x == 0) {
+    G.hub_vtx[h] = u;
+    G.hub_blk0[h] = blk0;
+    G.hub_nblk[h] = nbn;
+    G.hub_per[h] = per;
+    G.hub_of[u] = (int32_t)h;
+    G.deg[u] = dn;
+  }
+}
+
 // Keys of the batch whose source is in the sorted vertex list V.
 struct KeyInListPred {
   const uint64_t *keys;
@@ -683,6 +764,9 @@ struct KeyInListPred {
     return lo < nv && V[lo] == u;
   }
 };
+
+// Largest old hub list the fused hub merge stages in shared memory (~192 KB).
+constexpr uint32_t HUB_SMEM_ELEMS = 48 * 1024;
 
 // ---------------------------------------------------------------------------
 // The pipeline
@@ -708,16 +792,17 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
              sym, drop, A, err.get());
   uint64_t *t = tmp(std::max(radix_tmp_elems(k2), select_tmp_elems(k2)));
   uint64_t *sorted = radix_sort_u64(A, B, k2, vbits(), t, stream, prof);
-  uint64_t *other = sorted == A ? B : A;
-  select_if(UniquePred{sorted}, LoadU64Val{sorted}, k2, other, cnt + C_KU, t, stream, prof);
-  uint64_t *ukeys = other;
-  uint64_t *bkeys = sorted;  // sorted buffer is free now
-  // 3: existence filter
-  select_if(ExistPred{G, ukeys, cnt + C_KU, insert ? 1 : 0}, LoadU64Val{ukeys}, k2, bkeys,
-            cnt + C_KB, t, stream, prof);
+  uint64_t *bkeys = sorted == A ? B : A;
+  // 3: unique + existence filter (one lookup per key), compacted
+  uint8_t *kflags = s_flags.ensure(k2);
+  TRC_LAUNCH(prof, stream, "upd_filter", ceil_div(k2, 256), 256, 0, k_filter_flags, G, sorted, k2,
+             insert ? 1 : 0, kflags);
+  select_if(FlagPred{kflags}, LoadU64Val{sorted}, k2, bkeys, cnt + C_KB, t, stream, prof,
+            "sel_filter");
   // 4: runs by source
   uint64_t *tpos = s_C.ensure(k2);
-  select_if(RunStartPred{bkeys, cnt + C_KB}, IndexVal{}, k2, tpos, cnt + C_NT, t, stream, prof);
+  select_if(RunStartPred{bkeys, cnt + C_KB}, IndexVal{}, k2, tpos, cnt + C_NT, t, stream, prof,
+            "sel_runs");
   uint64_t hc[C_COUNT];
   uint32_t herr = 0;
   TRC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, stream));
@@ -737,7 +822,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   uint32_t *hw_u = s_hw_u.ensure(nt), *hw_dn = s_hw_dn.ensure(nt), *hw_t = s_hw_t.ensure(nt);
   int32_t *hw_h = s_hw_h.ensure(nt);
   TRC_LAUNCH(prof, stream, "upd_classify", ceil_div(nt, 256), 256, 0, k_classify, G, bkeys, tpos,
-             nt, kb, insert ? 1 : 0, tu, tdn, tc2, ovl, hw_u, hw_dn, hw_t, hw_h, cnt);
+             nt, kb, insert ? 1 : 0, tu, tdn, tc2, ovl, hw_u, hw_dn, hw_t, hw_h, s_hw_do.ensure(nt), cnt);
   TRC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, stream));
   sync();
   const uint64_t nov = hc[C_NOV], nh = hc[C_NH];
@@ -747,13 +832,21 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   phase("classify");
   // ---- hub plan (host): indices for new hubs, regions for grown ones.
   std::vector<uint64_t> plan;
+  uint32_t hub_max_old = 0;
+  uint64_t hub_old_total = 0, hub_new_total = 0;
   if (nh) {
-    std::vector<uint32_t> hu(nh), hdn(nh);
+    std::vector<uint32_t> hu(nh), hdn(nh), hdo(nh);
     std::vector<int32_t> hh(nh);
     TRC_CUDA(cudaMemcpyAsync(hu.data(), hw_u, nh * 4, cudaMemcpyDeviceToHost, stream));
     TRC_CUDA(cudaMemcpyAsync(hdn.data(), hw_dn, nh * 4, cudaMemcpyDeviceToHost, stream));
     TRC_CUDA(cudaMemcpyAsync(hh.data(), hw_h, nh * 4, cudaMemcpyDeviceToHost, stream));
+    TRC_CUDA(cudaMemcpyAsync(hdo.data(), s_hw_do.get(), nh * 4, cudaMemcpyDeviceToHost, stream));
     sync();
+    for (uint64_t i = 0; i < nh; i++) {
+      hub_max_old = std::max(hub_max_old, hdo[i]);
+      hub_old_total += hdo[i];
+      hub_new_total += hdn[i];
+    }
     plan.resize(6 * nh);
     const double fill = cfg.hub_block_fill > 0 && cfg.hub_block_fill <= 1 ? cfg.hub_block_fill : 0.75;
     const uint64_t blk_target = std::max<uint64_t>(1, (uint64_t)(HUB_BLOCK * fill));
@@ -808,7 +901,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
                c2n);
     P = s_P.ensure((uint64_t)n + 1);
     uint64_t *st = tmp(scan_tmp_elems(n) + 4);
-    exclusive_scan(LoadC2{c2n}, n, P, st, stream, prof);
+    exclusive_scan(LoadC2{c2n}, n, P, st, stream, prof, "scan_c2");
     if (shrink || (double)t2new > root_d * (double)N) {
       rebuild = true;
     } else {
@@ -826,7 +919,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
         uint64_t *mw = s_mw.ensure(nov);
         uint64_t *t3 = tmp(select_tmp_elems(nov) + 4);
         select_if(MaximalWindowPred{ws, nov, levels}, LoadU64Val{ws}, nov, mw, cnt + C_NMW, t3,
-                  stream, prof);
+                  stream, prof, "sel_windows");
         nmw = read_u64(cnt + C_NMW);
       }
     }
@@ -883,7 +976,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   {
     uint64_t *t4 = tmp(select_tmp_elems(n) + 4);
     select_if(SmallPred{stamp.get(), epoch, hub_of.get(), deg.get(), tix, tdn, T}, IndexVal32{},
-              n, rs, cnt + C_NR, t4, stream, prof);
+              n, rs, cnt + C_NR, t4, stream, prof, "sel_rewrite");
   }
   const uint64_t nrs = read_u64(cnt + C_NR);
   uint64_t SO = 0, SN = 0;
@@ -905,9 +998,27 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   }
 
   phase("merge_small");
-  // ---- hub path: gather / merge / scatter over the touched hubs (few)
+  // ---- hub path: fused CTA-per-hub merge (old lists staged in shared
+  // memory); hubs too large for shared memory take the general
+  // gather / merge / scatter path
   uint64_t SOh = 0, SNh = 0;
-  if (nh) {
+  bool hub_general = nh && hub_max_old > std::min<uint32_t>(HUB_SMEM_ELEMS, cfg.hub_stage_limit);
+  if (nh && !hub_general) {
+    static bool attr_set = false;
+    if (!attr_set) {
+      TRC_CUDA(cudaFuncSetAttribute(k_merge_hub, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(HUB_SMEM_ELEMS * 4)));
+      attr_set = true;
+    }
+    uint64_t *dplan = s_hwplan.ensure(plan.size());
+    TRC_CUDA(cudaMemcpyAsync(dplan, plan.data(), plan.size() * 8, cudaMemcpyHostToDevice, stream));
+    HubMergeArgs ha{dplan, nh, tix, tpos, nt, kb, bkeys, insert ? 1 : 0};
+    size_t smem = (size_t)std::max<uint32_t>(hub_max_old, 1) * 4;
+    TRC_LAUNCH(prof, stream, "upd_merge_hub", nh, 256, smem, k_merge_hub, G, ha);
+    SOh = hub_old_total;
+    SNh = hub_new_total;
+  }
+  if (hub_general) {
     std::vector<uint32_t> rh(nh);
     for (uint64_t i = 0; i < nh; i++) rh[i] = (uint32_t)plan[6 * i + 1];
     std::sort(rh.begin(), rh.end());

@@ -37,7 +37,8 @@ class Graph:
 
     def __init__(self, n: int, hbm_budget: int = 0, hub_threshold: int = 1024,
                  pma_root_density: float = 0.75, pma_build_density: float = 0.5,
-                 hub_block_fill: float = 0.75, push_pull_divisor: int = 20):
+                 hub_block_fill: float = 0.75, push_pull_divisor: int = 20,
+                 hub_stage_limit: int = 49152):
         self._L = L.load()
         cfg = L.trc_config()
         self._L.trc_config_default(C.byref(cfg))
@@ -46,6 +47,7 @@ class Graph:
         cfg.pma_build_density = pma_build_density
         cfg.hub_block_fill = hub_block_fill
         cfg.push_pull_divisor = push_pull_divisor
+        cfg.hub_stage_limit = hub_stage_limit
         h = C.c_void_p()
         L.check(self._L.trc_graph_create(n, hbm_budget, C.byref(cfg), C.byref(h)))
         self._h = h

@@ -104,13 +104,15 @@ def test_rmat_device_generator_bitexact(T):
 
 
 @pytest.mark.parametrize("name", ["s12_updates.npz", "s12_skew.npz"])
-@pytest.mark.parametrize("hub_threshold", [1024, 64])
-def test_update_sequence_matches_reference(T, name, hub_threshold):
+@pytest.mark.parametrize("hub_threshold,stage", [(1024, 49152), (64, 49152), (64, 100)])
+def test_update_sequence_matches_reference(T, name, hub_threshold, stage):
     """Bulk load, then every insert/delete batch of the fixture; the sorted
-    adjacency must equal the reference's after each step."""
+    adjacency must equal the reference's after each step.  stage=100 sends
+    hubs through the general gather/merge/scatter path."""
     z = load(name)
     n = int(z["n"])
-    g = graph_from_csr(T, z["s0_off"], z["s0_tgt"], hub_threshold=hub_threshold)
+    g = graph_from_csr(T, z["s0_off"], z["s0_tgt"], hub_threshold=hub_threshold,
+                       hub_stage_limit=stage)
     assert_same_csr(g, z["s0_off"], z["s0_tgt"])
     step, j = 1, 0
     while f"batch{j}_src" in z.files:
@@ -211,7 +213,7 @@ def test_random_updates_against_set_model(T):
     rebuilds, hub promotion and hub region growth)."""
     rng = np.random.default_rng(1)
     n = 3000
-    g = T.Graph(n, hub_threshold=48)
+    g = T.Graph(n, hub_threshold=48, hub_stage_limit=400)
     cur = np.zeros(0, np.uint64)
     for step in range(14):
         k = int(rng.integers(1, 20000))
