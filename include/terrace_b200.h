@@ -136,6 +136,23 @@ trc_status trc_cc(trc_graph *g, uint32_t *labels, uint32_t flags);
 trc_status trc_bc(trc_graph *g, uint32_t src, double *dep, uint32_t flags);
 trc_status trc_tc(trc_graph *g, uint64_t *count);
 
+/* ---- BFS without device allocation.  No counterpart in the reference.
+ *      For callers that cannot call cudaMalloc when they traverse: a service
+ *      whose device memory is fixed at start-up, an embedding whose
+ *      allocator belongs to another component, or a request path that must
+ *      not allocate.  Same results as trc_bfs (levels exact, parents a valid
+ *      BFS tree), computed with push steps only.  Its scratch (two frontier
+ *      queues and a counter, 8 MiB + 256 B) is a static array every GPU that
+ *      loads the library holds until exit; the first call on a device looks
+ *      up the array's device address, so make that first call before any
+ *      stream capture.  Outputs must be device arrays (TRC_DEVICE_PTR); the
+ *      graph may have at most TRC_NOALLOC_MAX_VERTICES vertices
+ *      (TRC_ERR_INVALID otherwise).  All calls share the scratch: calls that
+ *      overlap on the GPU race. */
+#define TRC_NOALLOC_MAX_VERTICES 1048576u
+trc_status trc_bfs_noalloc(trc_graph *g, uint32_t src, int32_t *parents,
+                           uint32_t *levels, uint32_t flags);
+
 /* ---- generator: replaces rMat<uint32_t> (include/rmat_util.h:81-115),
  *      bit-exact, edges first..first+count-1, on the device. */
 trc_status trc_rmat_generate(uint32_t n, uint32_t seed, double a, double b,

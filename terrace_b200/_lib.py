@@ -23,6 +23,7 @@ TRC_DEVICE_PTR = 0x1
 TRC_SYMMETRIZE = 0x2
 TRC_DROP_SELF_LOOPS = 0x4
 TRC_UNREACHED = 0xFFFFFFFF
+TRC_NOALLOC_MAX_VERTICES = 1048576
 
 
 class TrcError(RuntimeError):
@@ -85,6 +86,7 @@ SIGNATURES = [
     ("trc_get_size", _int, [_vp, C.POINTER(_u64)]),
     ("trc_dump_csr", _int, [_vp, _vp, _vp, _u32]),
     ("trc_bfs", _int, [_vp, _u32, _vp, _vp, _u32]),
+    ("trc_bfs_noalloc", _int, [_vp, _u32, _vp, _vp, _u32]),
     ("trc_pagerank", _int, [_vp, _u32, _dbl, _vp, _u32]),
     ("trc_cc", _int, [_vp, _vp, _u32]),
     ("trc_bc", _int, [_vp, _u32, _vp, _u32]),

@@ -99,6 +99,9 @@ class Graph {
   // ------------------------------------------------------------- analytics
   void ensure_lists();
   void bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags);
+  // BFS with scratch in a static device array (no allocation), noalloc.cu
+  void bfs_noalloc(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags);
+  int device = 0;  // device the graph was created on
   void pagerank(uint32_t iters, double damping, double *ranks, uint32_t flags);
   void cc(uint32_t *labels, uint32_t flags);
   void bc(uint32_t src, double *dep, uint32_t flags);

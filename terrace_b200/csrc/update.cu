@@ -44,6 +44,7 @@ namespace trc {
 
 Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_), cfg(cfg_) {
   budget.limit = budget_bytes;
+  TRC_CUDA(cudaGetDevice(&device));
   TRC_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
   stream = own_stream;
   for (auto *b : {&deg, &inl, &c2, &pma, &err, &hub_vtx, &hub_nblk, &hub_per, &hslot, &bcnt, &bmin,
