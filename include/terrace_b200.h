@@ -83,6 +83,12 @@ trc_status trc_graph_destroy(trc_graph *g);
 /* Bind the handle to a CUDA stream (cudaStream_t); NULL = library stream. */
 trc_status trc_graph_set_stream(trc_graph *g, void *stream);
 
+/* Frees the temporary device buffers kept between calls (sort buffers,
+ * merge staging, frontier lists); the next call that needs them allocates
+ * them again.  Useful after a bulk load.  No reference counterpart (the
+ * reference frees its temporaries per call). */
+trc_status trc_release_scratch(trc_graph *g);
+
 /* ---- updates: replaces Graph::add_edge_batch (include/graph.h:430-502) and
  *      the per-edge Graph::remove_edge loop of src/graph_bm.cc:375-380 (the
  *      reference declares no remove_edge_batch, include/graph.h:143-150).

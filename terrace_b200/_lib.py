@@ -75,6 +75,7 @@ SIGNATURES = [
     ("trc_graph_create", _int, [_u32, _u64, C.POINTER(trc_config), C.POINTER(_vp)]),
     ("trc_graph_destroy", _int, [_vp]),
     ("trc_graph_set_stream", _int, [_vp, _vp]),
+    ("trc_release_scratch", _int, [_vp]),
     ("trc_add_edge_batch", _int, [_vp, _vp, _vp, _u64, _u32, C.POINTER(_u64)]),
     ("trc_remove_edge_batch", _int, [_vp, _vp, _vp, _u64, _u32, C.POINTER(_u64)]),
     ("trc_is_edge", _int, [_vp, _vp, _vp, _u64, _vp, _u32]),

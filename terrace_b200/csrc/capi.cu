@@ -110,6 +110,10 @@ trc_status trc_graph_set_stream(trc_graph *g, void *stream) {
   });
 }
 
+trc_status trc_release_scratch(trc_graph *g) {
+  return guard([&] { G(g).release_scratch(); });
+}
+
 trc_status trc_add_edge_batch(trc_graph *g, const uint32_t *src, const uint32_t *dst, uint64_t k,
                               uint32_t flags, uint64_t *applied) {
   return guard([&] {

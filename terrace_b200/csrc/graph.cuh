@@ -79,6 +79,7 @@ class Graph {
 
   DevView view() const;
   uint32_t vbits() const;
+  void release_scratch();
 
   // ------------------------------------------------------------- update
   // Applies a batch; returns the number of directed edges changed.

@@ -118,6 +118,21 @@ DevView Graph::view() const {
   return v;
 }
 
+void Graph::release_scratch() {
+  sync();
+  for (auto *b : {&s_in_src, &s_in_dst, &s_tu, &s_tdn, &s_tc2, &s_ovl, &s_hw_u, &s_hw_dn, &s_hw_t,
+                  &s_c2n, &s_rlist, &s_pma_next, &s_tix, &s_hw_do})
+    b->reset();
+  for (auto *b : {&s_A, &s_B, &s_C, &s_tmp, &s_P, &s_oOff, &s_nOff, &s_wk, &s_wk2, &s_mw, &s_old,
+                  &s_new, &s_hwplan, &pbeg_alt})
+    b->reset();
+  s_hw_h.reset();
+  s_flags.reset();
+  lists.version = ~0ull;
+  for (auto *b : {&lists.S, &lists.M, &lists.Hv, &lists.SM, &lists.M1, &lists.M2, &lists.hub_blocks})
+    b->reset();
+}
+
 uint32_t Graph::vbits() const {
   uint32_t b = 1;
   while (b < 32 && (1ull << b) < (uint64_t)n) b++;

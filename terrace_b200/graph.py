@@ -76,6 +76,10 @@ class Graph:
         ptr = getattr(stream, "cuda_stream", stream)
         L.check(self._L.trc_graph_set_stream(self._h, C.c_void_p(ptr or 0)))
 
+    def release_scratch(self):
+        """Free temporary device buffers kept between calls."""
+        L.check(self._L.trc_release_scratch(self._h))
+
     # ---------------------------------------------------------------- updates
     def add_edge_batch(self, srcs, dests, symmetrize: bool = False,
                        drop_self_loops: bool = False) -> int:
