@@ -22,6 +22,9 @@
 namespace trc {
 
 constexpr int AT = 256;  // threads per CTA in the analytics kernels
+// PageRank runs two passes per iteration when its rank vector is larger than
+// this (half of it then stays in the 126 MB L2 beside the streamed lists).
+constexpr uint64_t PR_SPLIT_BYTES = 48ull << 20;
 
 // ---------------------------------------------------------------------------
 // Class lists
@@ -105,15 +108,42 @@ __device__ __forceinline__ T block_sum(T v, T *sh) {
 // the previous iteration and write both the new pdiv and, on the last
 // iteration, the undivided value.
 
+// When the rank vector is larger than L2 can keep beside the streaming
+// adjacency, an iteration runs as two passes over halves of the id space:
+// pass 0 sums the neighbours below `half` (ranks [0, split[u]) of the sorted
+// list) into acc[u], pass 1 adds the rest and stores.  Each pass gathers
+// from a half of the vector that stays L2-resident; every neighbour id is
+// still read once per iteration.
 struct PRArgs {
   const double *pc;
   double *pn;
   double *out;
   double damping, base;
   int last;
+  const uint32_t *split;  // null: single pass
+  double *acc;
+  int pass;  // 0 or 1 when split
 };
 
+__device__ __forceinline__ void pr_range(const PRArgs &a, uint32_t u, uint32_t d, uint32_t &lo,
+                                         uint32_t &hi) {
+  lo = 0;
+  hi = d;
+  if (a.split) {
+    uint32_t sp = a.split[u];
+    if (a.pass == 0) hi = sp;
+    else lo = sp;
+  }
+}
+
 __device__ __forceinline__ void pr_store(const PRArgs &a, uint32_t u, uint32_t d, double sum) {
+  if (a.split) {
+    if (a.pass == 0) {
+      a.acc[u] = sum;
+      return;
+    }
+    sum = a.acc[u] + sum;
+  }
   double val = a.damping > 0.0 ? a.base + a.damping * sum : sum;
   a.pn[u] = val / (double)d;
   if (a.last) a.out[u] = val;
@@ -128,12 +158,15 @@ __global__ void __launch_bounds__(AT) k_pr_S(DevView G, const uint32_t *S, uint6
   if (vi < nS) {
     u = S[vi];
     d = G.deg[u];
-    if (q * 4 < d) {
-      uint4 v = reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE)[q];
-      sum = __ldg(a.pc + v.x);
-      if (q * 4 + 1 < d) sum += __ldg(a.pc + v.y);
-      if (q * 4 + 2 < d) sum += __ldg(a.pc + v.z);
-      if (q * 4 + 3 < d) sum += __ldg(a.pc + v.w);
+    uint32_t lo, hi;
+    pr_range(a, u, d, lo, hi);
+    uint32_t e = q * 4;
+    if (e < hi && e + 4 > lo) {
+      uint4 v = __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE) + q);
+      if (e >= lo && e < hi) sum += __ldg(a.pc + v.x);
+      if (e + 1 >= lo && e + 1 < hi) sum += __ldg(a.pc + v.y);
+      if (e + 2 >= lo && e + 2 < hi) sum += __ldg(a.pc + v.z);
+      if (e + 3 >= lo && e + 3 < hi) sum += __ldg(a.pc + v.w);
     }
   }
   sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 1);
@@ -294,19 +327,21 @@ __global__ void __launch_bounds__(AT) k_pr_group(DevView G, const uint32_t *V, u
   if (vi < nV) {
     u = V[vi];
     d = G.deg[u];
+    uint32_t lo, hi;
+    pr_range(a, u, d, lo, hi);
     const uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
     const uint32_t *seg = G.pma + G.pbeg[u] - K_INLINE;  // index by rank
-    for (uint32_t j0 = q; j0 < d; j0 += GS * U) {
+    for (uint32_t j0 = lo + q; j0 < hi; j0 += GS * U) {
       uint32_t x[U];
 #pragma unroll
       for (int k = 0; k < U; k++) {
         uint32_t j = j0 + k * GS;
-        x[k] = j < d ? (j < K_INLINE ? __ldg(row + j) : __ldg(seg + j)) : 0u;
+        x[k] = j < hi ? (j < K_INLINE ? __ldcs(row + j) : __ldcs(seg + j)) : 0u;
       }
 #pragma unroll
       for (int k = 0; k < U; k++) {
         uint32_t j = j0 + k * GS;
-        if (j < d) sum += __ldg(a.pc + x[k]);
+        if (j < hi) sum += __ldg(a.pc + x[k]);
       }
     }
   }
@@ -333,6 +368,15 @@ __global__ void __launch_bounds__(AT) k_pr_H(DevView G, const uint32_t *Hv, PRAr
   }
   sum = block_sum(sum, sh);
   if (threadIdx.x == 0) pr_store(a, u, d, sum);
+}
+
+// split[u] = number of u's neighbours below `half` (binary search).
+__global__ void k_pr_split(DevView G, const uint32_t *V, uint64_t nV, uint32_t half,
+                           uint32_t *split) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nV) return;
+  uint32_t u = V[i];
+  split[u] = list_lower_bound(nbr_list(G, u), half);
 }
 
 __global__ void k_pr_init(const uint32_t *deg, uint32_t n, double p0, double iso, double *pdiv,
@@ -366,15 +410,37 @@ void Graph::pagerank(uint32_t iters, double damping, double *ranks, uint32_t fla
     TRC_LAUNCH(prof, stream, "pr_init", ceil_div(n, AT), AT, 0, k_pr_init, deg.get(), n, one_over_n,
                damping > 0.0 ? base : 0.0, p0, out);
     DevView G = view();
+    // two passes when the rank vector exceeds PR_SPLIT_BYTES (see PRArgs)
+    const bool two = (uint64_t)n * 8 > PR_SPLIT_BYTES;
+    uint32_t *split = nullptr;
+    DBuf<double> accb;
+    accb.bind(&budget);
+    double *acc = nullptr;
+    if (two) {
+      split = pr_split.ensure(n);
+      if (pr_split_version != version) {
+        const uint32_t half = n / 2;
+        TRC_LAUNCH(prof, stream, "pr_split", ceil_div(lists.nSM, AT), AT, 0, k_pr_split, G,
+                   lists.SM.get(), lists.nSM, half, split);
+        pr_split_version = version;
+      }
+      acc = accb.alloc_exact(n);
+    }
     for (uint32_t it = 0; it < iters; it++) {
-      PRArgs a{p0, p1, out, damping, base, it + 1 == iters};
-      TRC_LAUNCH(prof, stream, "pr_S", ceil_div(lists.nS * 4, AT), AT, 0, k_pr_S, G, lists.S.get(),
-                 lists.nS, a);
-      TRC_LAUNCH(prof, stream, "pr_M8", ceil_div(lists.nM1 * 8, AT), AT, 0, k_pr_group<8>, G,
-                 lists.M1.get(), lists.nM1, a);
-      TRC_LAUNCH(prof, stream, "pr_M32", ceil_div(lists.nM2 * 32, AT), AT, 0, k_pr_group<32>, G,
-                 lists.M2.get(), lists.nM2, a);
-      TRC_LAUNCH(prof, stream, "pr_H", lists.nH, AT, 0, k_pr_H, G, lists.Hv.get(), a);
+      for (int pass = two ? 0 : 1; pass < 2; pass++) {
+        PRArgs a{p0, p1, out, damping, base, it + 1 == iters, split, acc, pass};
+        TRC_LAUNCH(prof, stream, "pr_S", ceil_div(lists.nS * 4, AT), AT, 0, k_pr_S, G,
+                   lists.S.get(), lists.nS, a);
+        TRC_LAUNCH(prof, stream, "pr_M8", ceil_div(lists.nM1 * 8, AT), AT, 0, k_pr_group<8>, G,
+                   lists.M1.get(), lists.nM1, a);
+        TRC_LAUNCH(prof, stream, "pr_M32", ceil_div(lists.nM2 * 32, AT), AT, 0, k_pr_group<32>, G,
+                   lists.M2.get(), lists.nM2, a);
+        if (pass == 1) {
+          PRArgs ah = a;
+          ah.split = nullptr;
+          TRC_LAUNCH(prof, stream, "pr_H", lists.nH, AT, 0, k_pr_H, G, lists.Hv.get(), ah);
+        }
+      }
       std::swap(p0, p1);
     }
   }
@@ -424,6 +490,22 @@ __global__ void k_bfs_push(DevView G, const uint32_t *F, uint32_t nf, BFSState s
   }
 }
 
+// List entries that are still unvisited (and have more than min_deg
+// neighbours).
+struct UnvisitedPred {
+  const uint32_t *L, *lv, *deg;
+  uint32_t min_deg;
+  __device__ bool operator()(uint64_t i) const {
+    uint32_t u = L[i];
+    return lv[u] == TRC_UNREACHED && deg[u] > min_deg;
+  }
+};
+
+struct ListVal {
+  const uint32_t *L;
+  __device__ uint32_t operator()(uint64_t i) const { return L[i]; }
+};
+
 __global__ void k_set_bits(const uint32_t *F, uint32_t nf, uint32_t *bits) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nf) atomicOr(bits + (F[i] >> 5), 1u << (F[i] & 31));
@@ -440,7 +522,7 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
     u = S[vi];
     uint32_t d = G.deg[u];
     if (s.lv[u] == TRC_UNREACHED && q * 4 < d) {
-      v = reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE)[q];
+      v = __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE) + q);
       if (bit_test(s.bits, v.x)) first = 0;
       else if (q * 4 + 1 < d && bit_test(s.bits, v.y)) first = 1;
       else if (q * 4 + 2 < d && bit_test(s.bits, v.z)) first = 2;
@@ -524,6 +606,16 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
   DevView G = view();
   uint32_t nf = 1, d = 0;
   const uint64_t dense_at = n / push_pull_divisor();
+  // candidates of the dense steps: non-hub vertices not yet visited,
+  // compacted after every dense step
+  DBuf<uint32_t> cbuf[2], segb;  // candidate ping-pong, segment-pass list
+  cbuf[0].bind(&budget);
+  cbuf[1].bind(&budget);
+  segb.bind(&budget);
+  const uint32_t *cand = lists.SM.get();
+  uint64_t ncand = lists.nSM;
+  int cnext = 0;
+  uint64_t *sc = s_cnt.get() + 28;
   while (nf > 0) {
     TRC_CUDA(cudaMemsetAsync(c, 0, 4, stream));
     BFSState s{lv, par, bm, Nx, c, d};
@@ -531,13 +623,26 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
       TRC_CUDA(cudaMemsetAsync(bm, 0, words * 4, stream));
       TRC_LAUNCH(prof, stream, "bfs_bits", ceil_div(nf, AT), AT, 0, k_set_bits, F, nf, bm);
       // pass A: the 16 inline neighbours of every unvisited non-hub vertex
-      TRC_LAUNCH(prof, stream, "bfs_pull_inline", ceil_div(lists.nSM * 4, AT), AT, 0, k_bfs_pull_S,
-                 G, lists.SM.get(), lists.nSM, s);
-      // pass B: the PMA segments of those still unvisited; hubs from rank 0
-      TRC_LAUNCH(prof, stream, "bfs_pull_M", ceil_div(lists.nM * 32, AT), AT, 0, k_bfs_pull_W, G,
-                 lists.M.get(), lists.nM, s, K_INLINE);
+      TRC_LAUNCH(prof, stream, "bfs_pull_inline", ceil_div(ncand * 4, AT), AT, 0, k_bfs_pull_S,
+                 G, cand, ncand, s);
+      // pass B: the PMA segments of those still unvisited (compacted); hubs
+      // from rank 0
+      uint32_t *pb = segb.ensure(ncand ? ncand : 1);
+      uint64_t *t = tmp(select_tmp_elems(ncand) + 4);
+      select_if(UnvisitedPred{cand, lv, deg.get(), K_INLINE}, ListVal{cand}, ncand, pb, sc, t,
+                stream, prof, "sel_bfs_segment");
+      uint64_t nb = read_u64(sc);
+      TRC_LAUNCH(prof, stream, "bfs_pull_M", ceil_div(nb * 32, AT), AT, 0, k_bfs_pull_W, G, pb, nb,
+                 s, K_INLINE);
       TRC_LAUNCH(prof, stream, "bfs_pull_H", ceil_div(lists.nH * 32, AT), AT, 0, k_bfs_pull_W, G,
                  lists.Hv.get(), lists.nH, s, 0u);
+      // candidates left for the next dense step
+      uint32_t *pa = cbuf[cnext].ensure(ncand ? ncand : 1);  // never the list being read
+      select_if(UnvisitedPred{cand, lv, deg.get(), 0}, ListVal{cand}, ncand, pa, sc, t, stream,
+                prof, "sel_bfs_cand");
+      ncand = read_u64(sc);
+      cand = pa;
+      cnext ^= 1;
     } else {
       TRC_LAUNCH(prof, stream, "bfs_push", ceil_div((uint64_t)nf * 32, AT), AT, 0, k_bfs_push, G, F,
                  nf, s);

@@ -272,3 +272,24 @@ def test_streaming_rmat22_roundtrip_and_parity(T):
     assert g.remove_edge_batch(fs, fd) == len(fresh)
     assert csr_sha(*g.dump_csr()) == h0
     assert g.check() == 0
+
+
+def test_large_graph_two_pass_pagerank_and_bfs(T):
+    """RMAT scale 23 (8.4M vertices): the rank vector (67 MB) is above the
+    single-pass limit, so PageRank runs its two-pass L2-resident form; BFS
+    runs several dense steps with candidate compaction."""
+    n = 1 << 23
+    s, d = T.rmat_generate(n, 5, .57, .19, .19, 4 * n)
+    g = T.Graph(n)
+    g.add_edge_batch(s, d, **SYM)
+    keys = O.make_keys(s, d, True, True)
+    off, tgt = O.csr_from_keys(n, keys)
+    goff, gtgt = g.dump_csr()
+    assert np.array_equal(goff, off) and np.array_equal(gtgt, tgt)
+    assert rel_close(g.pagerank(3), O.pagerank(off, tgt, 3))
+    assert rel_close(g.pagerank(2, damping=0.85), O.pagerank(off, tgt, 2, 0.85))
+    src = int(np.diff(off.astype(np.int64)).argmax())
+    par, lv = g.bfs(src)
+    assert np.array_equal(lv, O.bfs_levels(off, tgt, src))
+    assert O.bfs_check_parents(off, tgt, src, lv, par) == 0
+    assert np.array_equal(g.cc(), O.cc(off, tgt))
