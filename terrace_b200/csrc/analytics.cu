@@ -22,9 +22,6 @@
 namespace trc {
 
 constexpr int AT = 256;  // threads per CTA in the analytics kernels
-// PageRank runs two passes per iteration when its rank vector is larger than
-// this (half of it then stays in the 126 MB L2 beside the streamed lists).
-constexpr uint64_t PR_SPLIT_BYTES = 48ull << 20;
 
 // ---------------------------------------------------------------------------
 // Class lists
@@ -108,42 +105,23 @@ __device__ __forceinline__ T block_sum(T v, T *sh) {
 // the previous iteration and write both the new pdiv and, on the last
 // iteration, the undivided value.
 
-// When the rank vector is larger than L2 can keep beside the streaming
-// adjacency, an iteration runs as two passes over halves of the id space:
-// pass 0 sums the neighbours below `half` (ranks [0, split[u]) of the sorted
-// list) into acc[u], pass 1 adds the rest and stores.  Each pass gathers
-// from a half of the vector that stays L2-resident; every neighbour id is
-// still read once per iteration.
+// Neighbour ids are read with streaming (evict-first) loads so the list
+// stream does not push the gathered rank vector out of L2.
 struct PRArgs {
   const double *pc;
   double *pn;
   double *out;
   double damping, base;
   int last;
-  const uint32_t *split;  // null: single pass
-  double *acc;
-  int pass;  // 0 or 1 when split
 };
 
-__device__ __forceinline__ void pr_range(const PRArgs &a, uint32_t u, uint32_t d, uint32_t &lo,
+__device__ __forceinline__ void pr_range(const PRArgs &, uint32_t, uint32_t d, uint32_t &lo,
                                          uint32_t &hi) {
   lo = 0;
   hi = d;
-  if (a.split) {
-    uint32_t sp = a.split[u];
-    if (a.pass == 0) hi = sp;
-    else lo = sp;
-  }
 }
 
 __device__ __forceinline__ void pr_store(const PRArgs &a, uint32_t u, uint32_t d, double sum) {
-  if (a.split) {
-    if (a.pass == 0) {
-      a.acc[u] = sum;
-      return;
-    }
-    sum = a.acc[u] + sum;
-  }
   double val = a.damping > 0.0 ? a.base + a.damping * sum : sum;
   a.pn[u] = val / (double)d;
   if (a.last) a.out[u] = val;
@@ -370,15 +348,6 @@ __global__ void __launch_bounds__(AT) k_pr_H(DevView G, const uint32_t *Hv, PRAr
   if (threadIdx.x == 0) pr_store(a, u, d, sum);
 }
 
-// split[u] = number of u's neighbours below `half` (binary search).
-__global__ void k_pr_split(DevView G, const uint32_t *V, uint64_t nV, uint32_t half,
-                           uint32_t *split) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nV) return;
-  uint32_t u = V[i];
-  split[u] = list_lower_bound(nbr_list(G, u), half);
-}
-
 __global__ void k_pr_init(const uint32_t *deg, uint32_t n, double p0, double iso, double *pdiv,
                           double *out) {
   uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -410,37 +379,15 @@ void Graph::pagerank(uint32_t iters, double damping, double *ranks, uint32_t fla
     TRC_LAUNCH(prof, stream, "pr_init", ceil_div(n, AT), AT, 0, k_pr_init, deg.get(), n, one_over_n,
                damping > 0.0 ? base : 0.0, p0, out);
     DevView G = view();
-    // two passes when the rank vector exceeds PR_SPLIT_BYTES (see PRArgs)
-    const bool two = (uint64_t)n * 8 > PR_SPLIT_BYTES;
-    uint32_t *split = nullptr;
-    DBuf<double> accb;
-    accb.bind(&budget);
-    double *acc = nullptr;
-    if (two) {
-      split = pr_split.ensure(n);
-      if (pr_split_version != version) {
-        const uint32_t half = n / 2;
-        TRC_LAUNCH(prof, stream, "pr_split", ceil_div(lists.nSM, AT), AT, 0, k_pr_split, G,
-                   lists.SM.get(), lists.nSM, half, split);
-        pr_split_version = version;
-      }
-      acc = accb.alloc_exact(n);
-    }
     for (uint32_t it = 0; it < iters; it++) {
-      for (int pass = two ? 0 : 1; pass < 2; pass++) {
-        PRArgs a{p0, p1, out, damping, base, it + 1 == iters, split, acc, pass};
-        TRC_LAUNCH(prof, stream, "pr_S", ceil_div(lists.nS * 4, AT), AT, 0, k_pr_S, G,
-                   lists.S.get(), lists.nS, a);
-        TRC_LAUNCH(prof, stream, "pr_M8", ceil_div(lists.nM1 * 8, AT), AT, 0, k_pr_group<8>, G,
-                   lists.M1.get(), lists.nM1, a);
-        TRC_LAUNCH(prof, stream, "pr_M32", ceil_div(lists.nM2 * 32, AT), AT, 0, k_pr_group<32>, G,
-                   lists.M2.get(), lists.nM2, a);
-        if (pass == 1) {
-          PRArgs ah = a;
-          ah.split = nullptr;
-          TRC_LAUNCH(prof, stream, "pr_H", lists.nH, AT, 0, k_pr_H, G, lists.Hv.get(), ah);
-        }
-      }
+      PRArgs a{p0, p1, out, damping, base, it + 1 == iters};
+      TRC_LAUNCH(prof, stream, "pr_S", ceil_div(lists.nS * 4, AT), AT, 0, k_pr_S, G, lists.S.get(),
+                 lists.nS, a);
+      TRC_LAUNCH(prof, stream, "pr_M8", ceil_div(lists.nM1 * 8, AT), AT, 0, k_pr_group<8>, G,
+                 lists.M1.get(), lists.nM1, a);
+      TRC_LAUNCH(prof, stream, "pr_M32", ceil_div(lists.nM2 * 32, AT), AT, 0, k_pr_group<32>, G,
+                 lists.M2.get(), lists.nM2, a);
+      TRC_LAUNCH(prof, stream, "pr_H", lists.nH, AT, 0, k_pr_H, G, lists.Hv.get(), a);
       std::swap(p0, p1);
     }
   }

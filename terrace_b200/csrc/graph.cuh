@@ -76,8 +76,6 @@ class Graph {
   DBuf<uint32_t> s_tix;  // vertex -> index in the touched list (this batch)
   DBuf<uint32_t> s_hw_do;  // old degree of each touched hub
   ClassLists lists;
-  DBuf<uint32_t> pr_split;  // per-vertex split rank for two-pass PageRank
-  uint64_t pr_split_version = ~0ull;
 
   DevView view() const;
   uint32_t vbits() const;

@@ -60,7 +60,6 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   pbeg_alt.bind(&budget);
   s_tix.bind(&budget);
   s_hw_do.bind(&budget);
-  pr_split.bind(&budget);
   s_hw_h.bind(&budget);
   s_flags.bind(&budget);
 
@@ -129,8 +128,6 @@ void Graph::release_scratch() {
     b->reset();
   s_hw_h.reset();
   s_flags.reset();
-  pr_split.reset();
-  pr_split_version = ~0ull;
   lists.version = ~0ull;
   for (auto *b : {&lists.S, &lists.M, &lists.Hv, &lists.SM, &lists.M1, &lists.M2, &lists.hub_blocks})
     b->reset();

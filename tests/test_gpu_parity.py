@@ -274,10 +274,9 @@ def test_streaming_rmat22_roundtrip_and_parity(T):
     assert g.check() == 0
 
 
-def test_large_graph_two_pass_pagerank_and_bfs(T):
-    """RMAT scale 23 (8.4M vertices): the rank vector (67 MB) is above the
-    single-pass limit, so PageRank runs its two-pass L2-resident form; BFS
-    runs several dense steps with candidate compaction."""
+def test_large_graph_pagerank_bfs_cc(T):
+    """RMAT scale 23 (8.4M vertices, rank vector 67 MB): PageRank, CC, and
+    BFS through several dense steps with candidate compaction."""
     n = 1 << 23
     s, d = T.rmat_generate(n, 5, .57, .19, .19, 4 * n)
     g = T.Graph(n)
