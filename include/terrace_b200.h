@@ -159,6 +159,29 @@ trc_status trc_tc(trc_graph *g, uint64_t *count);
 trc_status trc_bfs_noalloc(trc_graph *g, uint32_t src, int32_t *parents,
                            uint32_t *levels, uint32_t flags);
 
+/* ---- device view for user kernels (terrace_b200_edge_map.cuh): raw device
+ *      pointers of the tiers, valid until the next update of the graph.  No
+ *      reference counterpart (the reference's functors run inside
+ *      Graph::map_* on the host, include/graph.h:1287-1613).  Neighbour r of
+ *      u: r < min(deg,16): inl[16u + r]; otherwise r' = r - 16 and, when
+ *      hub_of[u] < 0, pma[pbeg[u] + r'], else with h = hub_of[u], per =
+ *      hub_per[h]: hslot[(hub_blk0[h] + r'/per) * hub_block + r'%per]. */
+typedef struct {
+  uint32_t n;
+  uint32_t inline_slots; /* 16 */
+  uint32_t hub_block;    /* 256 */
+  const uint32_t *deg;
+  const uint32_t *inl;
+  const uint64_t *pbeg;
+  const uint32_t *pma;
+  const int32_t *hub_of;
+  const uint64_t *hub_blk0;
+  const uint32_t *hub_per;
+  const uint32_t *hslot;
+  void *stream; /* the handle's cudaStream_t */
+} trc_device_view;
+trc_status trc_get_device_view(trc_graph *g, trc_device_view *out);
+
 /* ---- generator: replaces rMat<uint32_t> (include/rmat_util.h:81-115),
  *      bit-exact, edges first..first+count-1, on the device. */
 trc_status trc_rmat_generate(uint32_t n, uint32_t seed, double a, double b,

@@ -43,6 +43,13 @@ class trc_config(C.Structure):
                 ("hub_stage_limit", C.c_uint32)]
 
 
+class trc_device_view(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("inline_slots", C.c_uint32), ("hub_block", C.c_uint32),
+                ("deg", C.c_void_p), ("inl", C.c_void_p), ("pbeg", C.c_void_p), ("pma", C.c_void_p),
+                ("hub_of", C.c_void_p), ("hub_blk0", C.c_void_p), ("hub_per", C.c_void_p),
+                ("hslot", C.c_void_p), ("stream", C.c_void_p)]
+
+
 class trc_stats(C.Structure):
     _fields_ = [("n", C.c_uint32),
                 ("num_edges", C.c_uint64),
@@ -94,6 +101,7 @@ SIGNATURES = [
     ("trc_tc", _int, [_vp, C.POINTER(_u64)]),
     ("trc_rmat_generate", _int, [_u32, _u32, _dbl, _dbl, _dbl, _u64, _u64, _vp, _vp, _u32, _vp]),
     ("trc_get_stats", _int, [_vp, C.POINTER(trc_stats)]),
+    ("trc_get_device_view", _int, [_vp, C.POINTER(trc_device_view)]),
     ("trc_check", _int, [_vp, C.POINTER(_u64)]),
     ("trc_profile_enable", _int, [_vp, _int]),
     ("trc_profile_reset", _int, [_vp]),

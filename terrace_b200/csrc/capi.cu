@@ -241,6 +241,27 @@ trc_status trc_rmat_generate(uint32_t n, uint32_t seed, double a, double b, doub
   });
 }
 
+trc_status trc_get_device_view(trc_graph *g, trc_device_view *out) {
+  return guard([&] {
+    if (!out) trc::throw_error(TRC_ERR_INVALID, "null output");
+    trc::Graph &gr = G(g);
+    gr.sync();
+    trc::DevView v = gr.view();
+    out->n = v.n;
+    out->inline_slots = trc::K_INLINE;
+    out->hub_block = trc::HUB_BLOCK;
+    out->deg = v.deg;
+    out->inl = v.inl;
+    out->pbeg = v.pbeg;
+    out->pma = v.pma;
+    out->hub_of = v.hub_of;
+    out->hub_blk0 = v.hub_blk0;
+    out->hub_per = v.hub_per;
+    out->hslot = v.hslot;
+    out->stream = gr.stream;
+  });
+}
+
 trc_status trc_get_stats(trc_graph *g, trc_stats *out) {
   return guard([&] {
     if (!out) trc::throw_error(TRC_ERR_INVALID, "null output");
