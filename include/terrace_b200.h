@@ -132,6 +132,12 @@ trc_status trc_dump_csr(trc_graph *g, uint64_t *offsets, uint32_t *targets,
  * TRC_UNREACHED for unreached vertices. */
 trc_status trc_bfs(trc_graph *g, uint32_t src, int32_t *parents,
                    uint32_t *levels, uint32_t flags);
+/* Multi-source BFS: k <= 64 sources traversed together, one bit per source
+ * in a 64-bit mask per vertex (the reference runs BFS_with_edge_map once per
+ * source).  levels[i*n + v] = BFS level of v from sources[i], TRC_UNREACHED
+ * if unreached; identical to trc_bfs's levels for each source. */
+trc_status trc_msbfs(trc_graph *g, const uint32_t *sources, uint32_t k,
+                     uint32_t *levels, uint32_t flags);
 /* damping == 0 reproduces the reference (no damping term); 0 < damping < 1
  * computes p' = (1-damping)/n + damping * sum. FP64. */
 trc_status trc_pagerank(trc_graph *g, uint32_t iters, double damping,

@@ -95,6 +95,7 @@ SIGNATURES = [
     ("trc_dump_csr", _int, [_vp, _vp, _vp, _u32]),
     ("trc_bfs", _int, [_vp, _u32, _vp, _vp, _u32]),
     ("trc_bfs_noalloc", _int, [_vp, _u32, _vp, _vp, _u32]),
+    ("trc_msbfs", _int, [_vp, _vp, _u32, _vp, _u32]),
     ("trc_pagerank", _int, [_vp, _u32, _dbl, _vp, _u32]),
     ("trc_cc", _int, [_vp, _vp, _u32]),
     ("trc_bc", _int, [_vp, _u32, _vp, _u32]),

@@ -181,6 +181,11 @@ trc_status trc_bfs(trc_graph *g, uint32_t src, int32_t *parents, uint32_t *level
   return guard([&] { G(g).bfs(src, parents, levels, flags); });
 }
 
+trc_status trc_msbfs(trc_graph *g, const uint32_t *sources, uint32_t k, uint32_t *levels,
+                     uint32_t flags) {
+  return guard([&] { G(g).msbfs(sources, k, levels, flags); });
+}
+
 trc_status trc_bfs_noalloc(trc_graph *g, uint32_t src, int32_t *parents, uint32_t *levels,
                            uint32_t flags) {
   return guard([&] { G(g).bfs_noalloc(src, parents, levels, flags); });

@@ -100,6 +100,8 @@ class Graph {
   // ------------------------------------------------------------- analytics
   void ensure_lists();
   void bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags);
+  // up to 64 BFS at once, levels[i*n + v] (msbfs.cu)
+  void msbfs(const uint32_t *sources, uint32_t k, uint32_t *levels, uint32_t flags);
   // BFS with scratch in a static device array (no allocation), noalloc.cu
   void bfs_noalloc(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags);
   int device = 0;  // device the graph was created on

@@ -1,0 +1,265 @@
+// msbfs.cu -- multi-source BFS: up to 64 sources at once as one bit per
+// source in a 64-bit mask per vertex (the batching layer; the reference runs
+// BFS_with_edge_map once per source, include/BFS.h:41-84).
+//
+// Per vertex: seen[v] (sources that reached v), front[v] (sources whose
+// frontier holds v at this level).  A level computes, for every vertex,
+// reach = OR of front over its neighbours; new = reach & ~seen[v] gives the
+// sources discovering v at level L+1.  Two directions, as in the single-
+// source BFS:
+//   pull  -- every vertex not yet seen by all sources ORs its neighbours'
+//            front masks, stopping once nothing more can be added
+//            (4 lanes per inline-only vertex, a warp per larger vertex);
+//   push  -- when few vertices are in any frontier, each active vertex ORs
+//            its mask into its neighbours' next masks (64-bit atomicOr).
+// Levels are written vertex-major (one 256-byte row per vertex, contiguous
+// writes) and transposed to one row per source at the end.
+#include <algorithm>
+#include <vector>
+
+#include "graph.cuh"
+
+namespace trc {
+
+namespace {
+constexpr int MT = 256;
+
+__device__ __forceinline__ uint64_t shfl_or64(uint64_t x, int o) {
+  uint32_t lo = (uint32_t)x, hi = (uint32_t)(x >> 32);
+  lo |= __shfl_xor_sync(0xFFFFFFFFu, lo, o);
+  hi |= __shfl_xor_sync(0xFFFFFFFFu, hi, o);
+  return ((uint64_t)hi << 32) | lo;
+}
+
+struct MSState {
+  uint64_t *seen;
+  const uint64_t *front;
+  uint64_t *next;   // pull: written per vertex; push: OR-accumulated
+  uint32_t *lvrow;  // n x k levels, vertex-major
+  uint32_t k;
+  uint64_t all;     // mask of the k sources
+  uint32_t level;   // the level being discovered (L+1)
+  uint32_t *active; // count of vertices with new bits
+};
+
+__device__ __forceinline__ void ms_commit(const MSState &s, uint32_t v, uint64_t reach) {
+  uint64_t sv = s.seen[v];
+  uint64_t nw = reach & ~sv;
+  s.next[v] = nw;
+  if (nw) {
+    s.seen[v] = sv | nw;
+    atomicAdd(s.active, 1u);
+    uint64_t m = nw;
+    while (m) {
+      int i = __ffsll((long long)m) - 1;
+      m &= m - 1;
+      s.lvrow[(uint64_t)v * s.k + i] = s.level;
+    }
+  }
+}
+
+// pull, 4 lanes per inline-only vertex
+__global__ void __launch_bounds__(MT) k_ms_pull_S(DevView G, const uint32_t *V, uint64_t nV,
+                                                  MSState s) {
+  uint64_t gt = (uint64_t)blockIdx.x * MT + threadIdx.x;
+  uint64_t vi = gt >> 2;
+  uint32_t q = gt & 3;
+  uint64_t reach = 0;
+  uint32_t v = 0;
+  bool live = false;
+  if (vi < nV) {
+    v = V[vi];
+    live = s.seen[v] != s.all;
+    uint32_t d = G.deg[v];
+    if (live && q * 4 < d) {
+      uint4 r = __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)v * K_INLINE) + q);
+      reach = s.front[r.x];
+      if (q * 4 + 1 < d) reach |= s.front[r.y];
+      if (q * 4 + 2 < d) reach |= s.front[r.z];
+      if (q * 4 + 3 < d) reach |= s.front[r.w];
+    }
+  }
+  reach = shfl_or64(reach, 1);
+  reach = shfl_or64(reach, 2);
+  if (vi < nV && q == 0) {
+    if (live) ms_commit(s, v, reach);
+    else s.next[v] = 0;
+  }
+}
+
+// pull, one warp per vertex, stopping once seen | reach covers every source
+__global__ void __launch_bounds__(MT) k_ms_pull_W(DevView G, const uint32_t *V, uint64_t nV,
+                                                  MSState s) {
+  uint64_t w = ((uint64_t)blockIdx.x * MT + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= nV) return;
+  uint32_t v = V[w];
+  uint64_t sv = s.seen[v];
+  if (sv == s.all) {
+    if (lane == 0) s.next[v] = 0;
+    return;
+  }
+  NbrList L = nbr_list(G, v);
+  uint64_t reach = 0;
+  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) {
+    uint32_t j = j0 + lane;
+    if (j < L.deg) reach |= s.front[L.at(j)];
+    uint64_t r = reach;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r = shfl_or64(r, o);
+    reach = r;
+    if ((reach | sv) == s.all) break;
+  }
+  if (lane == 0) ms_commit(s, v, reach);
+}
+
+// push: every vertex with a non-empty front mask ORs it into its
+// neighbours' accumulators (warp per active vertex)
+__global__ void k_ms_push(DevView G, const uint32_t *F, uint32_t nf, const uint64_t *front,
+                          unsigned long long *acc) {
+  uint64_t w = ((uint64_t)blockIdx.x * MT + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= nf) return;
+  uint32_t u = F[w];
+  uint64_t m = front[u];
+  NbrList L = nbr_list(G, u);
+  for (uint32_t j = lane; j < L.deg; j += 32) atomicOr(acc + L.at(j), (unsigned long long)m);
+}
+
+// after a push: commit acc into seen / next for every vertex, collect the
+// next active list
+__global__ void k_ms_commit_all(uint32_t n, MSState s, unsigned long long *acc, uint32_t *list,
+                                uint32_t *list_cnt) {
+  uint64_t v = (uint64_t)blockIdx.x * MT + threadIdx.x;
+  if (v >= n) return;
+  uint64_t a = acc[v];
+  if (a) acc[v] = 0;
+  uint64_t sv = s.seen[v];
+  uint64_t nw = a & ~sv;
+  s.next[v] = nw;
+  if (nw) {
+    s.seen[v] = sv | nw;
+    list[atomicAdd(list_cnt, 1u)] = (uint32_t)v;
+    uint64_t m = nw;
+    while (m) {
+      int i = __ffsll((long long)m) - 1;
+      m &= m - 1;
+      s.lvrow[v * s.k + i] = s.level;
+    }
+  }
+}
+
+// active list after a pull step
+__global__ void k_ms_collect(uint32_t n, const uint64_t *front, uint32_t *list, uint32_t *cnt) {
+  uint64_t v = (uint64_t)blockIdx.x * MT + threadIdx.x;
+  if (v < n && front[v]) list[atomicAdd(cnt, 1u)] = (uint32_t)v;
+}
+
+__global__ void k_ms_init(uint32_t n, uint32_t k, const uint32_t *src, uint64_t *seen,
+                          uint64_t *front, uint32_t *lvrow, unsigned long long *acc) {
+  uint64_t v = (uint64_t)blockIdx.x * MT + threadIdx.x;
+  if (v >= n) return;
+  uint64_t m = 0;
+  for (uint32_t i = 0; i < k; i++)
+    if (src[i] == v) m |= 1ull << i;
+  seen[v] = m;
+  front[v] = m;
+  acc[v] = 0;
+  for (uint32_t i = 0; i < k; i++) lvrow[v * k + i] = (m >> i) & 1 ? 0u : TRC_UNREACHED;
+}
+
+// levels (vertex-major n x k) -> out (source-major k x n), 32x32 tiles
+__global__ void k_ms_transpose(const uint32_t *lvrow, uint32_t n, uint32_t k, uint32_t *out) {
+  __shared__ uint32_t t[32][33];
+  uint64_t v0 = (uint64_t)blockIdx.x * 32;
+  uint32_t i0 = blockIdx.y * 32;
+  for (uint32_t r = threadIdx.y; r < 32; r += blockDim.y) {
+    uint64_t v = v0 + r;
+    uint32_t i = i0 + threadIdx.x;
+    if (v < n && i < k) t[r][threadIdx.x] = lvrow[v * k + i];
+  }
+  __syncthreads();
+  for (uint32_t r = threadIdx.y; r < 32; r += blockDim.y) {
+    uint32_t i = i0 + r;
+    uint64_t v = v0 + threadIdx.x;
+    if (v < n && i < k) out[(uint64_t)i * n + v] = t[threadIdx.x][r];
+  }
+}
+}  // namespace
+
+void Graph::msbfs(const uint32_t *sources, uint32_t k, uint32_t *levels, uint32_t flags) {
+  if (k == 0) return;
+  if (k > 64) throw_error(TRC_ERR_INVALID, "at most 64 sources per multi-source BFS");
+  if (!sources || !levels) throw_error(TRC_ERR_INVALID, "null pointer");
+  std::vector<uint32_t> hsrc(k);
+  if (flags & TRC_DEVICE_PTR) {
+    TRC_CUDA(cudaMemcpyAsync(hsrc.data(), sources, k * 4, cudaMemcpyDeviceToHost, stream));
+    sync();
+  } else {
+    std::copy(sources, sources + k, hsrc.begin());
+  }
+  for (uint32_t x : hsrc)
+    if (x >= n) throw_error(TRC_ERR_INVALID, "source vertex out of range");
+  ensure_lists();
+  DBuf<uint64_t> seenb, fa, fb, accb;
+  DBuf<uint32_t> lvb, outb, srcb, lst, cnt;
+  for (auto *b : {&seenb, &fa, &fb, &accb}) b->bind(&budget);
+  for (auto *b : {&lvb, &outb, &srcb, &lst, &cnt}) b->bind(&budget);
+  uint64_t *seen = seenb.alloc_exact(n), *front = fa.alloc_exact(n), *next = fb.alloc_exact(n);
+  unsigned long long *acc = (unsigned long long *)accb.alloc_exact(n);
+  uint32_t *lvrow = lvb.alloc_exact((uint64_t)n * k);
+  uint32_t *dsrc = srcb.alloc_exact(k);
+  uint32_t *list = lst.alloc_exact(n), *c = cnt.alloc_exact(2);
+  TRC_CUDA(cudaMemcpyAsync(dsrc, hsrc.data(), k * 4, cudaMemcpyHostToDevice, stream));
+  TRC_LAUNCH(prof, stream, "ms_init", ceil_div(n, MT), MT, 0, k_ms_init, n, k, dsrc, seen, front,
+             lvrow, acc);
+  // initial active list = the distinct sources
+  std::vector<uint32_t> act(hsrc);
+  std::sort(act.begin(), act.end());
+  act.erase(std::unique(act.begin(), act.end()), act.end());
+  TRC_CUDA(cudaMemcpyAsync(list, act.data(), act.size() * 4, cudaMemcpyHostToDevice, stream));
+  uint32_t nact = (uint32_t)act.size();
+  const uint64_t all = k == 64 ? ~0ull : ((1ull << k) - 1);
+  const uint64_t dense_at = n / push_pull_divisor();
+  DevView G = view();
+  uint32_t level = 0;
+  while (nact > 0) {
+    level++;
+    TRC_CUDA(cudaMemsetAsync(c, 0, 8, stream));
+    MSState s{seen, front, next, lvrow, k, all, level, c};
+    if ((uint64_t)nact >= dense_at && dense_at > 0) {
+      // vertices in no class list (isolated) keep an empty next mask
+      TRC_CUDA(cudaMemsetAsync(next, 0, (uint64_t)n * 8, stream));
+      TRC_LAUNCH(prof, stream, "ms_pull_S", ceil_div(lists.nS * 4, MT), MT, 0, k_ms_pull_S, G,
+                 lists.S.get(), lists.nS, s);
+      TRC_LAUNCH(prof, stream, "ms_pull_M", ceil_div(lists.nM * 32, MT), MT, 0, k_ms_pull_W, G,
+                 lists.M.get(), lists.nM, s);
+      TRC_LAUNCH(prof, stream, "ms_pull_H", ceil_div(lists.nH * 32, MT), MT, 0, k_ms_pull_W, G,
+                 lists.Hv.get(), lists.nH, s);
+      // isolated vertices are never in a frontier; their next mask stays 0
+      TRC_LAUNCH(prof, stream, "ms_collect", ceil_div(n, MT), MT, 0, k_ms_collect, n, next, list,
+                 c + 1);
+    } else {
+      TRC_LAUNCH(prof, stream, "ms_push", ceil_div((uint64_t)nact * 32, MT), MT, 0, k_ms_push, G,
+                 list, nact, front, acc);
+      TRC_LAUNCH(prof, stream, "ms_commit", ceil_div(n, MT), MT, 0, k_ms_commit_all, n, s, acc,
+                 list, c + 1);
+    }
+    uint32_t hc[2];
+    TRC_CUDA(cudaMemcpyAsync(hc, c, 8, cudaMemcpyDeviceToHost, stream));
+    sync();
+    nact = hc[1];
+    std::swap(front, next);
+  }
+  bool dev = flags & TRC_DEVICE_PTR;
+  uint32_t *out = dev ? levels : outb.alloc_exact((uint64_t)n * k);
+  dim3 grid((unsigned)ceil_div(n, 32), (unsigned)ceil_div(k, 32));
+  dim3 block(32, 8);
+  k_ms_transpose<<<grid, block, 0, stream>>>(lvrow, n, k, out);
+  prof.launches++;
+  TRC_CUDA(cudaGetLastError());
+  if (!dev) TRC_CUDA(cudaMemcpyAsync(levels, out, (uint64_t)n * k * 4, cudaMemcpyDeviceToHost, stream));
+  sync();
+}
+
+}  // namespace trc

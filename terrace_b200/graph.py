@@ -203,6 +203,15 @@ class Graph:
         L.check(self._L.trc_bfs(self._h, src, C.c_void_p(pp), C.c_void_p(pl), f))
         return par, lv
 
+    def msbfs(self, sources, device: bool = False):
+        """Levels of up to 64 BFS at once: array (k, n), TRC_UNREACHED if
+        unreached (one traversal, one bit per source per vertex)."""
+        src = np.ascontiguousarray(sources, np.uint32)
+        k = len(src)
+        out, po, f = self._out(device, np.uint32, k * self.n)
+        L.check(self._L.trc_msbfs(self._h, C.c_void_p(src.ctypes.data), k, C.c_void_p(po), f))
+        return out.reshape(k, self.n)
+
     def pagerank(self, iters: int, damping: float = 0.0, device: bool = False):
         """PR_S<double>; damping 0 = the reference's undamped iteration."""
         out, po, f = self._out(device, np.float64, self.n)

@@ -292,3 +292,24 @@ def test_large_graph_pagerank_bfs_cc(T):
     assert np.array_equal(lv, O.bfs_levels(off, tgt, src))
     assert O.bfs_check_parents(off, tgt, src, lv, par) == 0
     assert np.array_equal(g.cc(), O.cc(off, tgt))
+
+
+@pytest.mark.parametrize("n_log,k", [(10, 5), (16, 64), (20, 33)])
+def test_msbfs_equals_single_source_bfs(T, n_log, k):
+    """Multi-source BFS (k sources as bits of one 64-bit mask per vertex)
+    gives, for every source, exactly the levels of a single-source BFS;
+    the small graph exercises pull steps, the large ones push then pull."""
+    n = 1 << n_log
+    s, d = T.rmat_generate(n, 11, .57, .19, .19, 8 * n)
+    g = T.Graph(n, hub_threshold=64)
+    g.add_edge_batch(s, d, **SYM)
+    off, tgt = g.dump_csr()
+    rng = np.random.default_rng(n_log)
+    deg = np.diff(off.astype(np.int64))
+    cand = np.nonzero(deg > 0)[0]
+    srcs = rng.choice(cand, k, replace=False).astype(np.uint32)
+    srcs[0] = 0 if deg[0] == 0 else srcs[0]   # an isolated source when vertex 0 is isolated
+    lv = g.msbfs(srcs)
+    assert lv.shape == (k, n)
+    for i in range(k):
+        assert np.array_equal(lv[i], O.bfs_levels(off, tgt, int(srcs[i]))), i
