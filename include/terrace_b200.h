@@ -195,6 +195,71 @@ trc_status trc_rmat_generate(uint32_t n, uint32_t seed, double a, double b,
                              uint32_t *src, uint32_t *dst, uint32_t flags,
                              void *stream);
 
+/* ---- serving layer (no reference counterpart: the reference has no serving
+ *      mode and forbids updates concurrent with analytics, include/graph.h:
+ *      73-230).  A persistent worker thread serves requests on the graph in
+ *      rounds.  TRC_SERVE_BATCHED (continuous batching): a round takes every
+ *      pending request, runs its queries on the current snapshot (BFS packed
+ *      64 per multi-source launch, degree lookups in one launch, PageRank
+ *      shared per iteration count), then applies all its updates as one net
+ *      change (the last request touching an edge decides).  Requests that
+ *      arrive meanwhile join the next round.  TRC_SERVE_FIFO: one request per
+ *      round in arrival order (the plain path).  Each request records the
+ *      snapshot version it observed (queries) or produced (updates).  While a
+ *      server runs, the graph must not be used directly. */
+typedef struct trc_server trc_server;
+typedef enum {
+  TRC_REQ_INSERT = 0,    /* a = src, b = dst, k pairs; result: u64 directed
+                            edges inserted by the request's round (FIFO:
+                            by the request) */
+  TRC_REQ_DELETE = 1,    /* same, removed */
+  TRC_REQ_BFS = 2,       /* param = source; result: u32 levels[n] (FULL) or
+                            {reached, eccentricity} (SUMMARY) */
+  TRC_REQ_DEGREE = 3,    /* a = vertices, k; result: u32 degrees[k] */
+  TRC_REQ_NEIGHBORS = 4, /* param = vertex; result: sorted u32 neighbours */
+  TRC_REQ_PAGERANK = 5   /* param = iterations; result: f64 ranks[n] (FULL)
+                            or {sum, max} (SUMMARY); undamped as PR_S */
+} trc_request_kind;
+#define TRC_SERVE_FIFO 0u
+#define TRC_SERVE_BATCHED 1u
+#define TRC_RESULT_FULL 0u
+#define TRC_RESULT_SUMMARY 1u
+typedef struct {
+  uint32_t mode;            /* TRC_SERVE_BATCHED or TRC_SERVE_FIFO */
+  uint32_t result_mode;     /* TRC_RESULT_FULL or TRC_RESULT_SUMMARY */
+  uint32_t symmetrize;      /* updates apply (u,v) and (v,u) */
+  uint32_t max_bfs_group;   /* sources per multi-source BFS launch (<= 64) */
+  uint64_t max_round_edges; /* update admission per round (directed keys) */
+} trc_server_config;
+typedef struct {
+  uint64_t completed;
+  double elapsed_s;     /* first submit (or reset) to last completion */
+  double p50_ms, p99_ms, mean_ms, max_ms; /* completion - arrival */
+  uint64_t rounds;
+  uint64_t device_calls;
+  uint64_t rejected;    /* updates refused by the HBM budget */
+  uint64_t version;     /* snapshots produced so far */
+} trc_server_stats;
+void trc_server_config_default(trc_server_config *cfg);
+trc_status trc_server_create(trc_graph *g, const trc_server_config *cfg, trc_server **out);
+/* Drains every pending request, then stops the worker. */
+trc_status trc_server_destroy(trc_server *s);
+/* Copies the inputs; the arrival time is the call time. */
+trc_status trc_server_submit(trc_server *s, trc_request_kind kind, const uint32_t *a,
+                             const uint32_t *b, uint64_t k, uint32_t param, uint64_t *id);
+/* TRC_ERR_TIMEOUT if the request is not done within timeout_ms (< 0: wait). */
+trc_status trc_server_wait(trc_server *s, uint64_t id, int64_t timeout_ms);
+/* Copies up to cap bytes of the result; *bytes = full size; *latency_ms =
+ * completion - arrival; *version = snapshot; *status = the request's own
+ * status (e.g. TRC_ERR_INVALID for a bad vertex id). */
+trc_status trc_server_result(trc_server *s, uint64_t id, void *out, uint64_t cap,
+                             uint64_t *bytes, double *latency_ms, uint64_t *version,
+                             trc_status *status);
+trc_status trc_server_release(trc_server *s, uint64_t id);
+/* kind < 0: every request; otherwise one trc_request_kind. */
+trc_status trc_server_get_stats(trc_server *s, int kind, trc_server_stats *out);
+trc_status trc_server_reset_stats(trc_server *s);
+
 /* ---- diagnostics (no reference counterpart: the reference has only
  *      lock-ownership checks, src/PMA.cc:29-111). */
 typedef struct {

@@ -8,5 +8,6 @@ the library was not built (there is no CPU fallback).
 from ._lib import (TRC_DEVICE_PTR, TRC_DROP_SELF_LOOPS, TRC_SYMMETRIZE, TRC_UNREACHED,  # noqa: F401
                    TrcError, LIB_PATH)
 from .graph import Graph, rmat_generate  # noqa: F401
+from .server import Server  # noqa: F401
 
-__all__ = ["Graph", "rmat_generate", "TrcError", "TRC_UNREACHED", "LIB_PATH"]
+__all__ = ["Graph", "Server", "rmat_generate", "TrcError", "TRC_UNREACHED", "LIB_PATH"]

@@ -24,6 +24,9 @@ TRC_SYMMETRIZE = 0x2
 TRC_DROP_SELF_LOOPS = 0x4
 TRC_UNREACHED = 0xFFFFFFFF
 TRC_NOALLOC_MAX_VERTICES = 1048576
+REQ_INSERT, REQ_DELETE, REQ_BFS, REQ_DEGREE, REQ_NEIGHBORS, REQ_PAGERANK = range(6)
+SERVE_FIFO, SERVE_BATCHED = 0, 1
+RESULT_FULL, RESULT_SUMMARY = 0, 1
 
 
 class TrcError(RuntimeError):
@@ -48,6 +51,18 @@ class trc_device_view(C.Structure):
                 ("deg", C.c_void_p), ("inl", C.c_void_p), ("pbeg", C.c_void_p), ("pma", C.c_void_p),
                 ("hub_of", C.c_void_p), ("hub_blk0", C.c_void_p), ("hub_per", C.c_void_p),
                 ("hslot", C.c_void_p), ("stream", C.c_void_p)]
+
+
+class trc_server_config(C.Structure):
+    _fields_ = [("mode", C.c_uint32), ("result_mode", C.c_uint32), ("symmetrize", C.c_uint32),
+                ("max_bfs_group", C.c_uint32), ("max_round_edges", C.c_uint64)]
+
+
+class trc_server_stats(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("elapsed_s", C.c_double), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double),
+                ("rounds", C.c_uint64), ("device_calls", C.c_uint64), ("rejected", C.c_uint64),
+                ("version", C.c_uint64)]
 
 
 class trc_stats(C.Structure):
@@ -109,6 +124,16 @@ SIGNATURES = [
     ("trc_profile_get", _int, [_vp, C.c_char_p, C.POINTER(_dbl), C.POINTER(_u64)]),
     ("trc_profile_names", _int, [_vp, C.c_char_p, _u64]),
     ("trc_launch_count", _int, [_vp, C.POINTER(_u64)]),
+    ("trc_server_config_default", None, [C.POINTER(trc_server_config)]),
+    ("trc_server_create", _int, [_vp, C.POINTER(trc_server_config), C.POINTER(_vp)]),
+    ("trc_server_destroy", _int, [_vp]),
+    ("trc_server_submit", _int, [_vp, _int, _vp, _vp, _u64, _u32, C.POINTER(_u64)]),
+    ("trc_server_wait", _int, [_vp, _u64, C.c_int64]),
+    ("trc_server_result", _int, [_vp, _u64, _vp, _u64, C.POINTER(_u64), C.POINTER(_dbl),
+                                 C.POINTER(_u64), C.POINTER(_int)]),
+    ("trc_server_release", _int, [_vp, _u64]),
+    ("trc_server_get_stats", _int, [_vp, _int, C.POINTER(trc_server_stats)]),
+    ("trc_server_reset_stats", _int, [_vp]),
 ]
 
 _lib = None

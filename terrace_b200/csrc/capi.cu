@@ -42,6 +42,13 @@ trc::Graph &G(trc_graph *g) {
 }
 }  // namespace
 
+// Shared with server.cu: the graph behind a handle, and the error slot.
+trc::Graph &trc_internal_graph(trc_graph *g) { return G(g); }
+extern "C" trc_status trc_internal_set_error(trc_status st, const char *msg) {
+  g_last_error = msg ? msg : "";
+  return st;
+}
+
 extern "C" {
 
 void trc_config_default(trc_config *cfg) {
@@ -107,6 +114,7 @@ trc_status trc_graph_set_stream(trc_graph *g, void *stream) {
     trc::Graph &gr = G(g);
     gr.sync();
     gr.stream = stream ? static_cast<cudaStream_t>(stream) : gr.own_stream;
+    gr.budget.stream = gr.stream;
   });
 }
 

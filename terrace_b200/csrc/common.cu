@@ -17,6 +17,26 @@ void cuda_check(cudaError_t e, const char *what, const char *file, int line) {
   throw Error{TRC_ERR_CUDA, buf};
 }
 
+void Budget::open_pool(int device) {
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  TRC_CUDA(cudaMemPoolCreate(&pool, &props));
+  uint64_t keep = ~0ull;  // never release at synchronisation points
+  TRC_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+}
+
+void Budget::trim() {
+  if (pool) cudaMemPoolTrimTo(pool, 0);
+}
+
+// Outstanding frees complete before the pool's memory is returned (the
+// runtime defers the destruction until then).
+Budget::~Budget() {
+  if (pool) cudaMemPoolDestroy(pool);
+}
+
 void *Budget::alloc(uint64_t bytes) {
   if (bytes == 0) bytes = 16;
   if (limit && used + bytes > limit) {
@@ -26,7 +46,7 @@ void *Budget::alloc(uint64_t bytes) {
     throw Error{TRC_ERR_NOMEM, buf};
   }
   void *p = nullptr;
-  cudaError_t e = cudaMalloc(&p, bytes);
+  cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, stream) : cudaMalloc(&p, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
     char buf[256];
@@ -40,7 +60,8 @@ void *Budget::alloc(uint64_t bytes) {
 
 void Budget::release(void *p, uint64_t bytes) {
   if (!p) return;
-  cudaFree(p);
+  if (pool) cudaFreeAsync(p, stream);
+  else cudaFree(p);
   if (bytes == 0) bytes = 16;
   used -= bytes;
 }

@@ -102,6 +102,10 @@ class Graph {
   void bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags);
   // up to 64 BFS at once, levels[i*n + v] (msbfs.cu)
   void msbfs(const uint32_t *sources, uint32_t k, uint32_t *levels, uint32_t flags);
+  // per source: vertices reached and deepest level, without level arrays
+  void msbfs_summary(const uint32_t *sources, uint32_t k, uint64_t *reached, uint32_t *ecc);
+  void msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uint32_t flags,
+                 uint64_t *reached, uint32_t *ecc);
   // BFS with scratch in a static device array (no allocation), noalloc.cu
   void bfs_noalloc(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags);
   int device = 0;  // device the graph was created on

@@ -35,12 +35,28 @@ struct MSState {
   uint64_t *seen;
   const uint64_t *front;
   uint64_t *next;   // pull: written per vertex; push: OR-accumulated
-  uint32_t *lvrow;  // n x k levels, vertex-major
+  uint32_t *lvrow;  // n x k levels, vertex-major; null: summary only
   uint32_t k;
   uint64_t all;     // mask of the k sources
   uint32_t level;   // the level being discovered (L+1)
   uint32_t *active; // count of vertices with new bits
 };
+
+__device__ __forceinline__ void write_levels(const MSState &s, uint64_t v, uint64_t nw) {
+  while (nw) {
+    int i = __ffsll((long long)nw) - 1;
+    nw &= nw - 1;
+    s.lvrow[v * s.k + i] = s.level;
+  }
+}
+
+// OR of x over the warp into *dst (one atomic per warp); every lane calls
+__device__ __forceinline__ void warp_or_into(uint64_t x, unsigned long long *dst) {
+  uint32_t lo = __reduce_or_sync(0xFFFFFFFFu, (uint32_t)x);
+  uint32_t hi = __reduce_or_sync(0xFFFFFFFFu, (uint32_t)(x >> 32));
+  uint64_t r = ((uint64_t)hi << 32) | lo;
+  if ((threadIdx.x & 31) == 0 && r) atomicOr(dst, (unsigned long long)r);
+}
 
 __device__ __forceinline__ void ms_commit(const MSState &s, uint32_t v, uint64_t reach) {
   uint64_t sv = s.seen[v];
@@ -49,12 +65,7 @@ __device__ __forceinline__ void ms_commit(const MSState &s, uint32_t v, uint64_t
   if (nw) {
     s.seen[v] = sv | nw;
     atomicAdd(s.active, 1u);
-    uint64_t m = nw;
-    while (m) {
-      int i = __ffsll((long long)m) - 1;
-      m &= m - 1;
-      s.lvrow[(uint64_t)v * s.k + i] = s.level;
-    }
+    if (s.lvrow) write_levels(s, v, nw);
   }
 }
 
@@ -129,30 +140,57 @@ __global__ void k_ms_push(DevView G, const uint32_t *F, uint32_t nf, const uint6
 // after a push: commit acc into seen / next for every vertex, collect the
 // next active list
 __global__ void k_ms_commit_all(uint32_t n, MSState s, unsigned long long *acc, uint32_t *list,
-                                uint32_t *list_cnt) {
+                                uint32_t *list_cnt, unsigned long long *any) {
   uint64_t v = (uint64_t)blockIdx.x * MT + threadIdx.x;
-  if (v >= n) return;
-  uint64_t a = acc[v];
-  if (a) acc[v] = 0;
-  uint64_t sv = s.seen[v];
-  uint64_t nw = a & ~sv;
-  s.next[v] = nw;
-  if (nw) {
-    s.seen[v] = sv | nw;
-    list[atomicAdd(list_cnt, 1u)] = (uint32_t)v;
-    uint64_t m = nw;
-    while (m) {
-      int i = __ffsll((long long)m) - 1;
-      m &= m - 1;
-      s.lvrow[v * s.k + i] = s.level;
+  uint64_t nw = 0;
+  if (v < n) {
+    uint64_t a = acc[v];
+    if (a) acc[v] = 0;
+    uint64_t sv = s.seen[v];
+    nw = a & ~sv;
+    s.next[v] = nw;
+    if (nw) {
+      s.seen[v] = sv | nw;
+      list[atomicAdd(list_cnt, 1u)] = (uint32_t)v;
+      if (s.lvrow) write_levels(s, v, nw);
     }
   }
+  if (any) warp_or_into(nw, any);
 }
 
-// active list after a pull step
-__global__ void k_ms_collect(uint32_t n, const uint64_t *front, uint32_t *list, uint32_t *cnt) {
+// active list after a pull step; `any` (optional) collects the sources
+// that discovered a vertex at this level
+__global__ void k_ms_collect(uint32_t n, const uint64_t *front, uint32_t *list, uint32_t *cnt,
+                             unsigned long long *any) {
   uint64_t v = (uint64_t)blockIdx.x * MT + threadIdx.x;
-  if (v < n && front[v]) list[atomicAdd(cnt, 1u)] = (uint32_t)v;
+  uint64_t f = v < n ? front[v] : 0;
+  if (f) list[atomicAdd(cnt, 1u)] = (uint32_t)v;
+  if (any) warp_or_into(f, any);
+}
+
+// per source: vertices reached (popcount of each bit of seen over all
+// vertices), one ballot per bit per 32 vertices
+__global__ void k_ms_count(uint32_t n, const uint64_t *seen, unsigned long long *cnt) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t warps = (uint64_t)gridDim.x * (MT / 32);
+  uint32_t c0 = 0, c1 = 0;
+  for (uint64_t base = ((uint64_t)blockIdx.x * MT + threadIdx.x - lane); base < n;
+       base += warps * 32) {
+    uint64_t v = base + lane;
+    uint64_t x = v < n ? seen[v] : 0;
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+      uint32_t b = __popc(__ballot_sync(0xFFFFFFFFu, (x >> i) & 1));
+      if (lane == i) c0 += b;
+    }
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+      uint32_t b = __popc(__ballot_sync(0xFFFFFFFFu, (x >> (32 + i)) & 1));
+      if (lane == i) c1 += b;
+    }
+  }
+  if (c0) atomicAdd(cnt + lane, (unsigned long long)c0);
+  if (c1) atomicAdd(cnt + 32 + lane, (unsigned long long)c1);
 }
 
 __global__ void k_ms_init(uint32_t n, uint32_t k, const uint32_t *src, uint64_t *seen,
@@ -165,7 +203,8 @@ __global__ void k_ms_init(uint32_t n, uint32_t k, const uint32_t *src, uint64_t 
   seen[v] = m;
   front[v] = m;
   acc[v] = 0;
-  for (uint32_t i = 0; i < k; i++) lvrow[v * k + i] = (m >> i) & 1 ? 0u : TRC_UNREACHED;
+  if (lvrow)
+    for (uint32_t i = 0; i < k; i++) lvrow[v * k + i] = (m >> i) & 1 ? 0u : TRC_UNREACHED;
 }
 
 // levels (vertex-major n x k) -> out (source-major k x n), 32x32 tiles
@@ -188,9 +227,23 @@ __global__ void k_ms_transpose(const uint32_t *lvrow, uint32_t n, uint32_t k, ui
 }  // namespace
 
 void Graph::msbfs(const uint32_t *sources, uint32_t k, uint32_t *levels, uint32_t flags) {
+  if (!levels) throw_error(TRC_ERR_INVALID, "null pointer");
+  msbfs_run(sources, k, levels, flags, nullptr, nullptr);
+}
+
+void Graph::msbfs_summary(const uint32_t *sources, uint32_t k, uint64_t *reached, uint32_t *ecc) {
+  if (!reached || !ecc) throw_error(TRC_ERR_INVALID, "null pointer");
+  msbfs_run(sources, k, nullptr, 0, reached, ecc);
+}
+
+// levels != null: per-source levels; otherwise reached / ecc (host arrays
+// of k) get the number of vertices each source reaches and its deepest level
+void Graph::msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uint32_t flags,
+                      uint64_t *reached, uint32_t *ecc) {
   if (k == 0) return;
   if (k > 64) throw_error(TRC_ERR_INVALID, "at most 64 sources per multi-source BFS");
-  if (!sources || !levels) throw_error(TRC_ERR_INVALID, "null pointer");
+  if (!sources) throw_error(TRC_ERR_INVALID, "null pointer");
+  const bool summary = levels == nullptr;
   std::vector<uint32_t> hsrc(k);
   if (flags & TRC_DEVICE_PTR) {
     TRC_CUDA(cudaMemcpyAsync(hsrc.data(), sources, k * 4, cudaMemcpyDeviceToHost, stream));
@@ -207,8 +260,13 @@ void Graph::msbfs(const uint32_t *sources, uint32_t k, uint32_t *levels, uint32_
   for (auto *b : {&lvb, &outb, &srcb, &lst, &cnt}) b->bind(&budget);
   uint64_t *seen = seenb.alloc_exact(n), *front = fa.alloc_exact(n), *next = fb.alloc_exact(n);
   unsigned long long *acc = (unsigned long long *)accb.alloc_exact(n);
-  uint32_t *lvrow = lvb.alloc_exact((uint64_t)n * k);
+  uint32_t *lvrow = summary ? nullptr : lvb.alloc_exact((uint64_t)n * k);
   uint32_t *dsrc = srcb.alloc_exact(k);
+  DBuf<uint64_t> anyb;
+  anyb.bind(&budget);
+  // [0] sources that discovered a vertex this level, [1..64] reach counts
+  unsigned long long *any = summary ? (unsigned long long *)anyb.alloc_exact(65) : nullptr;
+  std::vector<uint32_t> depth(k, 0);
   uint32_t *list = lst.alloc_exact(n), *c = cnt.alloc_exact(2);
   TRC_CUDA(cudaMemcpyAsync(dsrc, hsrc.data(), k * 4, cudaMemcpyHostToDevice, stream));
   TRC_LAUNCH(prof, stream, "ms_init", ceil_div(n, MT), MT, 0, k_ms_init, n, k, dsrc, seen, front,
@@ -226,6 +284,7 @@ void Graph::msbfs(const uint32_t *sources, uint32_t k, uint32_t *levels, uint32_
   while (nact > 0) {
     level++;
     TRC_CUDA(cudaMemsetAsync(c, 0, 8, stream));
+    if (any) TRC_CUDA(cudaMemsetAsync(any, 0, 8, stream));
     MSState s{seen, front, next, lvrow, k, all, level, c};
     if ((uint64_t)nact >= dense_at && dense_at > 0) {
       // vertices in no class list (isolated) keep an empty next mask
@@ -238,18 +297,36 @@ void Graph::msbfs(const uint32_t *sources, uint32_t k, uint32_t *levels, uint32_
                  lists.Hv.get(), lists.nH, s);
       // isolated vertices are never in a frontier; their next mask stays 0
       TRC_LAUNCH(prof, stream, "ms_collect", ceil_div(n, MT), MT, 0, k_ms_collect, n, next, list,
-                 c + 1);
+                 c + 1, any);
     } else {
       TRC_LAUNCH(prof, stream, "ms_push", ceil_div((uint64_t)nact * 32, MT), MT, 0, k_ms_push, G,
                  list, nact, front, acc);
       TRC_LAUNCH(prof, stream, "ms_commit", ceil_div(n, MT), MT, 0, k_ms_commit_all, n, s, acc,
-                 list, c + 1);
+                 list, c + 1, any);
     }
     uint32_t hc[2];
+    uint64_t hany = 0;
     TRC_CUDA(cudaMemcpyAsync(hc, c, 8, cudaMemcpyDeviceToHost, stream));
+    if (any) TRC_CUDA(cudaMemcpyAsync(&hany, any, 8, cudaMemcpyDeviceToHost, stream));
     sync();
     nact = hc[1];
+    for (uint32_t i = 0; i < k; i++)
+      if ((hany >> i) & 1) depth[i] = level;
     std::swap(front, next);
+  }
+  if (summary) {
+    TRC_CUDA(cudaMemsetAsync(any + 1, 0, 64 * 8, stream));
+    TRC_LAUNCH(prof, stream, "ms_count", (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(
+                                             ceil_div(n, MT), (uint64_t)num_sms() * 8)),
+               MT, 0, k_ms_count, n, seen, any + 1);
+    uint64_t cnts[64];
+    TRC_CUDA(cudaMemcpyAsync(cnts, any + 1, 64 * 8, cudaMemcpyDeviceToHost, stream));
+    sync();
+    for (uint32_t i = 0; i < k; i++) {
+      reached[i] = cnts[i];
+      ecc[i] = depth[i];
+    }
+    return;
   }
   bool dev = flags & TRC_DEVICE_PTR;
   uint32_t *out = dev ? levels : outb.alloc_exact((uint64_t)n * k);

@@ -141,11 +141,19 @@ void cuda_check(cudaError_t e, const char *what, const char *file, int line);
 #define TRC_CUDA(call) ::trc::cuda_check((call), #call, __FILE__, __LINE__)
 
 // ---------------------------------------------------------------------------
-// Device memory under a per-graph HBM budget.
+// Device memory under a per-graph HBM budget.  Allocations are
+// stream-ordered (cudaMallocFromPoolAsync / cudaFreeAsync on the graph's
+// stream) from a pool owned by the graph that keeps freed memory for reuse,
+// so per-call scratch of the analytics costs no device synchronisation.
 class Budget {
  public:
   uint64_t limit = 0;  // 0 = device free memory is the only limit
   uint64_t used = 0;
+  cudaStream_t stream = nullptr;  // allocation / free order
+  cudaMemPool_t pool = nullptr;
+  void open_pool(int device);
+  void trim();  // returns cached free memory to the device
+  ~Budget();
   void *alloc(uint64_t bytes);
   void release(void *p, uint64_t bytes);
 };

@@ -47,6 +47,8 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   TRC_CUDA(cudaGetDevice(&device));
   TRC_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
   stream = own_stream;
+  budget.stream = stream;
+  budget.open_pool(device);
   for (auto *b : {&deg, &inl, &c2, &pma, &err, &hub_vtx, &hub_nblk, &hub_per, &hslot, &bcnt, &bmin,
                   &bown, &stamp, &s_in_src, &s_in_dst, &s_tu, &s_tdn, &s_tc2, &s_ovl, &s_hw_u,
                   &s_hw_dn, &s_hw_t, &s_c2n, &s_rlist, &s_pma_next, &lists.S, &lists.M, &lists.Hv,
@@ -92,6 +94,9 @@ Graph::~Graph() {
   if (own_stream) cudaStreamSynchronize(own_stream);
   if (stream && stream != own_stream) cudaStreamSynchronize(stream);
   prof.reset();
+  // the members free after this body, on the legacy stream (the work on
+  // the graph's streams has finished)
+  budget.stream = nullptr;
   if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -131,6 +136,8 @@ void Graph::release_scratch() {
   lists.version = ~0ull;
   for (auto *b : {&lists.S, &lists.M, &lists.Hv, &lists.SM, &lists.M1, &lists.M2, &lists.hub_blocks})
     b->reset();
+  sync();
+  budget.trim();
 }
 
 uint32_t Graph::vbits() const {

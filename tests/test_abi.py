@@ -81,3 +81,21 @@ def test_no_cpu_fallback_without_gpu():
     with pytest.raises(T.TrcError) as e:
         T.Graph(16)
     assert e.value.status == 3  # TRC_ERR_CUDA
+
+
+def test_server_abi_without_gpu(lib):
+    """Server entry points validate their handles before any device work."""
+    from terrace_b200 import _lib
+    L = _lib.load()
+    cfg = _lib.trc_server_config()
+    L.trc_server_config_default(ctypes.byref(cfg))
+    assert cfg.mode == _lib.SERVE_BATCHED and cfg.result_mode == _lib.RESULT_FULL
+    assert cfg.max_bfs_group == 64 and cfg.symmetrize == 1
+    h = ctypes.c_void_p()
+    assert L.trc_server_create(None, ctypes.byref(cfg), ctypes.byref(h)) == _lib.TRC_ERR_INVALID
+    rid = ctypes.c_uint64()
+    assert L.trc_server_submit(None, _lib.REQ_BFS, None, None, 0, 0,
+                               ctypes.byref(rid)) == _lib.TRC_ERR_INVALID
+    assert L.trc_server_wait(None, 1, 0) == _lib.TRC_ERR_INVALID
+    st = _lib.trc_server_stats()
+    assert L.trc_server_get_stats(None, -1, ctypes.byref(st)) == _lib.TRC_ERR_INVALID
