@@ -9,8 +9,11 @@ symmetrized) inserted through the library.  value = directed edges inserted
 per second over the K timed steps, batches already resident in HBM.
 
 Also measured (extra keys): deletes of the same batches, BFS / PageRank /
-CC / BC / TC on the scale-22 graph, and BFS / PageRank GTEPS with their HBM
-roofline on the scale-24 RMAT graph (ef 32, a=.57 b=.19 c=.19).
+CC / BC / TC on the scale-22 graph, BFS / PageRank GTEPS with their HBM
+roofline on the scale-24 RMAT graph (ef 32, a=.57 b=.19 c=.19), and the
+serving mix on the scale-25 graph ("serving": p50 / p99 latency and
+throughput of the plain one-request-at-a-time path and of continuous
+batching at increasing Poisson arrival rates).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -34,25 +37,17 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from terrace_b200.workload import batch_seed, hash32  # noqa: E402
+
 SCALE, EF, A, B, C = 22, 16, 0.5, 0.1, 0.1
 BATCH = 1_000_000
 BATCH_STREAM = 1
 S24 = (24, 32, 0.57, 0.19, 0.19)
-
-
-def hash32(a: int) -> int:
-    a &= 0xFFFFFFFF
-    a = ((a + 0x7ED55D16) + (a << 12)) & 0xFFFFFFFF
-    a = ((a ^ 0xC761C23C) ^ (a >> 19)) & 0xFFFFFFFF
-    a = ((a + 0x165667B1) + (a << 5)) & 0xFFFFFFFF
-    a = ((a + 0xD3A2646C) ^ (a << 9)) & 0xFFFFFFFF
-    a = ((a + 0xFD7046C5) + (a << 3)) & 0xFFFFFFFF
-    a = ((a ^ 0xB55A4F09) ^ (a >> 16)) & 0xFFFFFFFF
-    return a
-
-
-def batch_seed(stream: int, j: int) -> int:
-    return hash32(stream) ^ j
+# serving mix: RMAT scale 25 ef 16, Poisson arrivals (seed 3); 60% update
+# batches (log-uniform size in [1, 1e6], half inserts, half deletes), 25%
+# single-source BFS, 10% degree / neighbour-list lookups, 5% PageRank (10 it)
+SERVE = dict(scale=25, ef=16, seed=3, rates=(25, 50, 100, 200, 400, 800, 1600),
+             seconds=3.0, min_reqs=120, max_reqs=2400, hbm_budget=96 << 30)
 
 
 def load_peaks():
@@ -320,6 +315,24 @@ def kernel_bytes(name, sz):
     return None
 
 
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# dominant kernels, from the committed ncu summaries of the same workload
+NCU_TRAFFIC = {"upd_merge_small": ("insert_rmat22_batch1e6.md", "traffic (read + write)")}
+
+
+def ncu_traffic(name):
+    if name not in NCU_TRAFFIC:
+        return None, None
+    fn, row = NCU_TRAFFIC[name]
+    try:
+        for line in open(os.path.join(ROOT, "profiles", fn)):
+            if line.startswith("| " + row + " |"):
+                return int(line.split("|")[2].strip().split()[0].replace(",", "")), "profiles/" + fn
+    except OSError:
+        pass
+    return None, None
+
+
 def roofline_for(name, ms_cnt, sizes, hbm_gbs, peak_kind):
     """Algorithmic bytes per launch of the dominant insert kernel divided by
     its mean CUDA-event duration (profiled pass of the same batches)."""
@@ -332,9 +345,10 @@ def roofline_for(name, ms_cnt, sizes, hbm_gbs, peak_kind):
                 "note": "no byte formula for this kernel", "launch_ms": per_launch_ms}
     bytes_per = sum(per) / len(per)
     achieved = bytes_per / (per_launch_ms / 1e3) / 1e9
+    traffic, src = ncu_traffic(name)
     return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm_gbs, "unit": "GB/s",
-            "frac": achieved / hbm_gbs, "traffic": None, "peak_kind": peak_kind,
-            "bytes_per_launch": bytes_per, "launch_ms": per_launch_ms}
+            "frac": achieved / hbm_gbs, "traffic": traffic, "traffic_source": src,
+            "peak_kind": peak_kind, "bytes_per_launch": bytes_per, "launch_ms": per_launch_ms}
 
 
 def scale24(T, torch, stream, hbm_gbs, peak_kind):
@@ -398,6 +412,127 @@ def scale24(T, torch, stream, hbm_gbs, peak_kind):
         "bfs_kernels": {k: v for k, v in bfs_prof.items()},
         "tiers": {k: st[k] for k in ("inline_edges", "pma_edges", "hub_edges", "num_hubs")},
     }
+
+
+# ------------------------------------------------------------ serving
+def serving_stream(n, count, rng, pool_len, sources):
+    """The request mix: (kind, payload) with payload an offset/length into the
+    update pair pool, a vertex, a vertex array or an iteration count.  BFS
+    sources are drawn from the non-isolated vertices of the initial graph."""
+    out = []
+    for _ in range(count):
+        x = rng.random()
+        if x < 0.60:
+            k = int(np.exp(rng.uniform(0.0, np.log(1e6))))
+            off = int(rng.integers(0, pool_len - k))
+            out.append(("ins" if rng.random() < 0.5 else "del", (off, k)))
+        elif x < 0.85:
+            out.append(("bfs", int(sources[rng.integers(0, len(sources))])))
+        elif x < 0.95:
+            if rng.random() < 0.5:
+                out.append(("deg", rng.integers(0, n, int(rng.integers(1, 1025)), dtype=np.uint32)))
+            else:
+                out.append(("nbr", int(rng.integers(0, n))))
+        else:
+            out.append(("pr", 10))
+    return out
+
+
+def serving_run(T, g, batched, reqs, gaps, rate, ps, pd):
+    """Submits reqs at Poisson times (gaps / rate seconds apart), waits for
+    all; returns offered / achieved rate and latency percentiles."""
+    srv = T.Server(g, batched=batched, summary=True)
+    ids, kinds = [], []
+    t0 = time.perf_counter()
+    t_next = t0
+    for (kind, x), gap in zip(reqs, gaps):
+        t_next += gap / rate
+        while True:
+            dt = t_next - time.perf_counter()
+            if dt <= 0:
+                break
+            time.sleep(min(dt, 0.002))
+        if kind == "ins":
+            ids.append(srv.insert(ps[x[0]:x[0] + x[1]], pd[x[0]:x[0] + x[1]]))
+        elif kind == "del":
+            ids.append(srv.delete(ps[x[0]:x[0] + x[1]], pd[x[0]:x[0] + x[1]]))
+        elif kind == "bfs":
+            ids.append(srv.bfs(x))
+        elif kind == "deg":
+            ids.append(srv.degree(x))
+        elif kind == "nbr":
+            ids.append(srv.neighbors(x))
+        else:
+            ids.append(srv.pagerank(x))
+        kinds.append(kind)
+    t_sub = time.perf_counter() - t0
+    bad = 0
+    for rid in ids:
+        srv.wait(rid, 600_000)
+        _, _, _, st = srv.result(rid)
+        bad += st != 0
+        srv.release(rid)
+    st = srv.stats()
+    per = {}
+    for k, code in (("update", None), ("bfs", 2), ("pagerank", 5)):
+        if code is None:
+            a = srv.stats(0)
+            b = srv.stats(1)
+            c = a["completed"] + b["completed"]
+            per[k] = {"p99_ms": max(a["p99_ms"], b["p99_ms"]), "completed": c}
+        else:
+            x = srv.stats(code)
+            per[k] = {"p50_ms": x["p50_ms"], "p99_ms": x["p99_ms"], "completed": x["completed"]}
+    srv.close()
+    return {"offered_rps": len(reqs) / t_sub, "target_rps": rate, "requests": len(reqs),
+            "throughput_rps": st["completed"] / st["elapsed_s"], "p50_ms": st["p50_ms"],
+            "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
+            "rounds": st["rounds"], "device_calls": st["device_calls"],
+            "rejected": st["rejected"], "failed": bad, "per_kind": per}
+
+
+def serving(T, torch):
+    """Serving mix on the scale-25 graph: the plain path (FIFO, one request
+    at a time) against continuous batching, at increasing offered rates."""
+    cfg = SERVE
+    n = 1 << cfg["scale"]
+    s, d = T.rmat_generate(n, 0, A, B, C, cfg["ef"] * n, device=True)
+    g = T.Graph(n, hbm_budget=cfg["hbm_budget"])
+    m0 = g.add_edge_batch(s, d, symmetrize=True, drop_self_loops=True)
+    del s, d
+    torch.cuda.empty_cache()
+    # update pairs: RMAT pairs of seed stream 3 (same distribution as the graph)
+    pool_len = 1 << 23
+    ps, pd = T.rmat_generate(n, hash32(cfg["seed"]), A, B, C, pool_len)
+    sources = np.flatnonzero(g.degree(np.arange(n, dtype=np.uint32))).astype(np.uint32)
+    out = {"graph": f"rmat{cfg['scale']} ef{cfg['ef']} a={A} b={B} c={C} symmetrized",
+           "n": n, "m0": m0, "hbm_budget_bytes": cfg["hbm_budget"],
+           "mix": "60% updates (log-uniform 1..1e6 pairs, half insert / half delete), 25% BFS, "
+                  "10% degree/neighbour lookups, 5% PageRank 10 it; Poisson arrivals seed 3",
+           "results": "summaries computed on the device (BFS: reached, depth; PageRank: sum, max)",
+           "latency": "host clock, submit to completion", "fifo": [], "batched": []}
+    for mode in ("fifo", "batched"):
+        for rate in cfg["rates"]:
+            cnt = int(min(max(rate * cfg["seconds"], cfg["min_reqs"]), cfg["max_reqs"]))
+            rng = np.random.default_rng(cfg["seed"])
+            reqs = serving_stream(n, cnt, rng, pool_len, sources)
+            gaps = rng.exponential(1.0, cnt)
+            r = serving_run(T, g, mode == "batched", reqs, gaps, rate, ps, pd)
+            out[mode].append(r)
+            # stop once the mode no longer keeps up with the offered load
+            if r["throughput_rps"] < 0.7 * r["offered_rps"] or r["p99_ms"] > 20_000:
+                break
+    # throughput at equal p99: the SLO is the largest p99 the plain path shows
+    # while it keeps up (throughput >= 90% of offered)
+    keep = [r for r in out["fifo"] if r["throughput_rps"] >= 0.9 * r["offered_rps"]]
+    slo = max((r["p99_ms"] for r in keep), default=None)
+    if slo is not None:
+        fb = max((r["throughput_rps"] for r in keep), default=0.0)
+        bb = max((r["throughput_rps"] for r in out["batched"] if r["p99_ms"] <= slo), default=0.0)
+        out["at_equal_p99"] = {"p99_slo_ms": slo, "fifo_rps": fb, "batched_rps": bb,
+                               "batched_over_fifo": bb / fb if fb else None}
+    g.close()
+    return out
 
 
 # ------------------------------------------------------------ CPU baselines
@@ -485,6 +620,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-scale24", action="store_true")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--serving-only", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -500,7 +637,16 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.serving_only:
+        import torch
+        import terrace_b200 as T
+        print(json.dumps({"serving": serving(T, torch)}), flush=True)
+        return
     res = run_ours(args, rank, world)
+    if world == 1 and not args.skip_serving:
+        import torch
+        import terrace_b200 as T
+        res["serving"] = serving(T, torch)
     if rank == 0:
         if not args.skip_cpu_baseline:
             res["cpu_baseline"] = cpu_baseline_for_ours()
