@@ -488,7 +488,11 @@ def serving_run(T, g, batched, reqs, gaps, rate, ps, pd):
             "throughput_rps": st["completed"] / st["elapsed_s"], "p50_ms": st["p50_ms"],
             "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
             "rounds": st["rounds"], "device_calls": st["device_calls"],
-            "rejected": st["rejected"], "failed": bad, "per_kind": per}
+            "rejected": st["rejected"], "failed": bad, "per_kind": per,
+            "pma_rebuilds": st["pma_rebuilds"],
+            "worst_round": {k: st["worst_" + k] for k in
+                            ("round_ms", "update_ms", "bfs_ms", "pagerank_ms", "round_requests",
+                             "round_rebuilds")}}
 
 
 def serving(T, torch):

@@ -55,7 +55,7 @@ typedef struct {
   double pma_root_density;    /* upper density bound at the PMA root;
                                  reference 0.75 (src/PMA.cc:382-394). */
   double pma_build_density;   /* density after a full PMA rebuild.
-                                 Default 0.6. */
+                                 Default 0.5. */
   double hub_block_fill;      /* fill of hub blocks after a rewrite.
                                  Default 0.75. */
   uint32_t push_pull_divisor; /* edgeMap goes dense when |F| >= n/divisor;
@@ -65,6 +65,9 @@ typedef struct {
                                  shared-memory hub kernel; larger hubs take
                                  the gather/merge/scatter path.  Default and
                                  maximum 49152. */
+  uint32_t cuda_graphs;       /* 1: iteration loops (PageRank) are replayed
+                                 from captured CUDA graphs; 0: launched one
+                                 by one.  Default 1. */
 } trc_config;
 
 /* Fill `cfg` with the defaults listed above. */
@@ -239,6 +242,10 @@ typedef struct {
   uint64_t device_calls;
   uint64_t rejected;    /* updates refused by the HBM budget */
   uint64_t version;     /* snapshots produced so far */
+  /* the slowest round: duration, its parts, requests, full PMA rebuilds */
+  double worst_round_ms, worst_update_ms, worst_bfs_ms, worst_pagerank_ms;
+  uint64_t worst_round_requests, worst_round_rebuilds;
+  uint64_t pma_rebuilds; /* full tier-2 rebuilds caused by served updates */
 } trc_server_stats;
 void trc_server_config_default(trc_server_config *cfg);
 trc_status trc_server_create(trc_graph *g, const trc_server_config *cfg, trc_server **out);

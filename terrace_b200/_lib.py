@@ -43,7 +43,8 @@ class trc_config(C.Structure):
                 ("pma_build_density", C.c_double),
                 ("hub_block_fill", C.c_double),
                 ("push_pull_divisor", C.c_uint32),
-                ("hub_stage_limit", C.c_uint32)]
+                ("hub_stage_limit", C.c_uint32),
+                ("cuda_graphs", C.c_uint32)]
 
 
 class trc_device_view(C.Structure):
@@ -62,7 +63,10 @@ class trc_server_stats(C.Structure):
     _fields_ = [("completed", C.c_uint64), ("elapsed_s", C.c_double), ("p50_ms", C.c_double),
                 ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double),
                 ("rounds", C.c_uint64), ("device_calls", C.c_uint64), ("rejected", C.c_uint64),
-                ("version", C.c_uint64)]
+                ("version", C.c_uint64), ("worst_round_ms", C.c_double),
+                ("worst_update_ms", C.c_double), ("worst_bfs_ms", C.c_double),
+                ("worst_pagerank_ms", C.c_double), ("worst_round_requests", C.c_uint64),
+                ("worst_round_rebuilds", C.c_uint64), ("pma_rebuilds", C.c_uint64)]
 
 
 class trc_stats(C.Structure):

@@ -15,6 +15,7 @@
 //   H  (hubs, blocked tier): one CTA per hub, warps over its blocks.
 // Direction switching follows the reference rule: dense (pull) when the
 // frontier holds at least n/divisor vertices (include/Map.cpp:65-74).
+#include <cstring>
 #include <vector>
 
 #include "graph.cuh"
@@ -368,31 +369,97 @@ void Graph::pagerank(uint32_t iters, double damping, double *ranks, uint32_t fla
   ob.bind(&budget);
   double *p0 = pa.alloc_exact(n), *p1 = pb.alloc_exact(n);
   double *out = dev ? ranks : ob.alloc_exact(n);
-  const double one_over_n = 1.0 / (double)n;
-  const double base = (1.0 - damping) / (double)n;
   if (iters == 0) {
     // the reference returns the initial vector 1/n (include/Pagerank.h:137-141)
-    std::vector<double> h(n, one_over_n);
+    std::vector<double> h(n, 1.0 / (double)n);
     TRC_CUDA(cudaMemcpyAsync(out, h.data(), (uint64_t)n * 8, cudaMemcpyHostToDevice, stream));
     sync();
   } else {
-    TRC_LAUNCH(prof, stream, "pr_init", ceil_div(n, AT), AT, 0, k_pr_init, deg.get(), n, one_over_n,
-               damping > 0.0 ? base : 0.0, p0, out);
-    DevView G = view();
-    for (uint32_t it = 0; it < iters; it++) {
-      PRArgs a{p0, p1, out, damping, base, it + 1 == iters};
-      TRC_LAUNCH(prof, stream, "pr_S", ceil_div(lists.nS * 4, AT), AT, 0, k_pr_S, G, lists.S.get(),
-                 lists.nS, a);
-      TRC_LAUNCH(prof, stream, "pr_M8", ceil_div(lists.nM1 * 8, AT), AT, 0, k_pr_group<8>, G,
-                 lists.M1.get(), lists.nM1, a);
-      TRC_LAUNCH(prof, stream, "pr_M32", ceil_div(lists.nM2 * 32, AT), AT, 0, k_pr_group<32>, G,
-                 lists.M2.get(), lists.nM2, a);
-      TRC_LAUNCH(prof, stream, "pr_H", lists.nH, AT, 0, k_pr_H, G, lists.Hv.get(), a);
-      std::swap(p0, p1);
-    }
+    pagerank_launch(iters, damping, p0, p1, out, stream);
   }
   if (!dev) TRC_CUDA(cudaMemcpyAsync(ranks, out, (uint64_t)n * 8, cudaMemcpyDeviceToHost, stream));
   sync();
+}
+
+void Graph::pr_kernels(uint32_t iters, double damping, double *p0, double *p1, double *out,
+                       cudaStream_t s) {
+  const double one_over_n = 1.0 / (double)n;
+  const double base = (1.0 - damping) / (double)n;
+  TRC_LAUNCH(prof, s, "pr_init", ceil_div(n, AT), AT, 0, k_pr_init, deg.get(), n, one_over_n,
+             damping > 0.0 ? base : 0.0, p0, out);
+  DevView G = view();
+  for (uint32_t it = 0; it < iters; it++) {
+    PRArgs a{p0, p1, out, damping, base, it + 1 == iters};
+    TRC_LAUNCH(prof, s, "pr_S", ceil_div(lists.nS * 4, AT), AT, 0, k_pr_S, G, lists.S.get(),
+               lists.nS, a);
+    TRC_LAUNCH(prof, s, "pr_M8", ceil_div(lists.nM1 * 8, AT), AT, 0, k_pr_group<8>, G,
+               lists.M1.get(), lists.nM1, a);
+    TRC_LAUNCH(prof, s, "pr_M32", ceil_div(lists.nM2 * 32, AT), AT, 0, k_pr_group<32>, G,
+               lists.M2.get(), lists.nM2, a);
+    TRC_LAUNCH(prof, s, "pr_H", lists.nH, AT, 0, k_pr_H, G, lists.Hv.get(), a);
+    std::swap(p0, p1);
+  }
+}
+
+// The iteration loop (iters x 4 launches) is replayed from a CUDA graph:
+// captured once per (iteration count, buffers, class lists) and patched with
+// cudaGraphExecUpdate when only kernel arguments changed.  With the
+// per-kernel profiler on, kernels are launched directly so that each gets
+// its own events.  Requires the class lists (ensure_lists) and iters >= 1;
+// nothing is allocated or synchronised, so it may run on a second stream.
+void Graph::pagerank_launch(uint32_t iters, double damping, double *p0, double *p1, double *out,
+                            cudaStream_t s) {
+  if (prof.on || !use_graphs || iters < 2) {
+    pr_kernels(iters, damping, p0, p1, out, s);
+    return;
+  }
+  uint64_t dbits;
+  memcpy(&dbits, &damping, 8);
+  const uint64_t key[PRGraphCache::KEY] = {iters, dbits, (uint64_t)p0, (uint64_t)p1, (uint64_t)out,
+                                           lists.version, (uint64_t)lists.S.get(), lists.nS,
+                                           lists.nM1, lists.nM2, lists.nH, (uint64_t)s};
+  bool same = prg.exec != nullptr;
+  for (int i = 0; same && i < PRGraphCache::KEY; i++) same = prg.key[i] == key[i];
+  if (!same) {
+    const uint64_t before = prof.launches;
+    cudaGraph_t gr = nullptr;
+    TRC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      pr_kernels(iters, damping, p0, p1, out, s);
+    } catch (...) {
+      cudaStreamEndCapture(s, &gr);
+      if (gr) cudaGraphDestroy(gr);
+      prof.launches = before;
+      throw;
+    }
+    TRC_CUDA(cudaStreamEndCapture(s, &gr));
+    prg.kernels = prof.launches - before;
+    prof.launches = before;
+    bool updated = false;
+    if (prg.exec) {
+      cudaGraphExecUpdateResultInfo info;
+      updated = cudaGraphExecUpdate(prg.exec, gr, &info) == cudaSuccess;
+      if (!updated) {
+        cudaGetLastError();
+        cudaGraphExecDestroy(prg.exec);
+        prg.exec = nullptr;
+      }
+    }
+    if (!updated) {
+      cudaError_t e = cudaGraphInstantiate(&prg.exec, gr, 0);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(gr);
+        prg.exec = nullptr;
+        TRC_CUDA(e);
+      }
+    }
+    cudaGraphDestroy(gr);
+    memcpy(prg.key, key, sizeof(key));
+    prg.replays_built++;
+  }
+  TRC_CUDA(cudaGraphLaunch(prg.exec, s));
+  prof.launches += prg.kernels;
+  prg.replays++;
 }
 
 // ---------------------------------------------------------------------------

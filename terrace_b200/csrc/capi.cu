@@ -59,6 +59,7 @@ void trc_config_default(trc_config *cfg) {
   cfg->hub_block_fill = 0.75;
   cfg->push_pull_divisor = 20;
   cfg->hub_stage_limit = 49152;
+  cfg->cuda_graphs = 1;
 }
 
 const char *trc_status_string(trc_status s) {

@@ -110,6 +110,20 @@ class Graph {
   void bfs_noalloc(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags);
   int device = 0;  // device the graph was created on
   void pagerank(uint32_t iters, double damping, double *ranks, uint32_t flags);
+  // the iterations on stream s into caller buffers (n each); class lists
+  // must be current; no allocation or synchronisation
+  void pagerank_launch(uint32_t iters, double damping, double *p0, double *p1, double *out,
+                       cudaStream_t s);
+  void pr_kernels(uint32_t iters, double damping, double *p0, double *p1, double *out,
+                  cudaStream_t s);
+  struct PRGraphCache {
+    static constexpr int KEY = 12;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t key[KEY] = {};
+    uint64_t kernels = 0;       // kernel nodes per replay
+    uint64_t replays = 0, replays_built = 0;
+  } prg;
+  bool use_graphs = true;     // CUDA-graph replay of iteration loops
   void cc(uint32_t *labels, uint32_t flags);
   void bc(uint32_t src, double *dep, uint32_t flags);
   uint64_t tc();

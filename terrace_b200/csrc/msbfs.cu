@@ -7,8 +7,9 @@
 // reach = OR of front over its neighbours; new = reach & ~seen[v] gives the
 // sources discovering v at level L+1.  Two directions, as in the single-
 // source BFS:
-//   pull  -- every vertex not yet seen by all sources ORs its neighbours'
-//            front masks, stopping once nothing more can be added
+//   pull  -- every vertex not yet seen by every live source (one whose
+//            frontier is not empty) ORs its neighbours' front masks,
+//            stopping once nothing more can be added
 //            (4 lanes per inline-only vertex, a warp per larger vertex);
 //   push  -- when few vertices are in any frontier, each active vertex ORs
 //            its mask into its neighbours' next masks (64-bit atomicOr).
@@ -37,7 +38,8 @@ struct MSState {
   uint64_t *next;   // pull: written per vertex; push: OR-accumulated
   uint32_t *lvrow;  // n x k levels, vertex-major; null: summary only
   uint32_t k;
-  uint64_t all;     // mask of the k sources
+  uint64_t live;    // sources whose frontier is not empty at this level:
+                    // only their bits can still be discovered
   uint32_t level;   // the level being discovered (L+1)
   uint32_t *active; // count of vertices with new bits
 };
@@ -80,7 +82,7 @@ __global__ void __launch_bounds__(MT) k_ms_pull_S(DevView G, const uint32_t *V, 
   bool live = false;
   if (vi < nV) {
     v = V[vi];
-    live = s.seen[v] != s.all;
+    live = (s.seen[v] & s.live) != s.live;
     uint32_t d = G.deg[v];
     if (live && q * 4 < d) {
       uint4 r = __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)v * K_INLINE) + q);
@@ -98,7 +100,8 @@ __global__ void __launch_bounds__(MT) k_ms_pull_S(DevView G, const uint32_t *V, 
   }
 }
 
-// pull, one warp per vertex, stopping once seen | reach covers every source
+// pull, one warp per vertex, stopping once seen | reach covers every live
+// source
 __global__ void __launch_bounds__(MT) k_ms_pull_W(DevView G, const uint32_t *V, uint64_t nV,
                                                   MSState s) {
   uint64_t w = ((uint64_t)blockIdx.x * MT + threadIdx.x) >> 5;
@@ -106,7 +109,7 @@ __global__ void __launch_bounds__(MT) k_ms_pull_W(DevView G, const uint32_t *V, 
   if (w >= nV) return;
   uint32_t v = V[w];
   uint64_t sv = s.seen[v];
-  if (sv == s.all) {
+  if ((sv & s.live) == s.live) {
     if (lane == 0) s.next[v] = 0;
     return;
   }
@@ -119,43 +122,68 @@ __global__ void __launch_bounds__(MT) k_ms_pull_W(DevView G, const uint32_t *V, 
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) r = shfl_or64(r, o);
     reach = r;
-    if ((reach | sv) == s.all) break;
+    if (((reach | sv) & s.live) == s.live) break;
   }
   if (lane == 0) ms_commit(s, v, reach);
 }
 
-// push: every vertex with a non-empty front mask ORs it into its
-// neighbours' accumulators (warp per active vertex)
-__global__ void k_ms_push(DevView G, const uint32_t *F, uint32_t nf, const uint64_t *front,
-                          unsigned long long *acc) {
+// push: every vertex of the active list ORs its front mask into its
+// neighbours' accumulators (warp per active vertex), skipping neighbours
+// that every source in the mask has already seen.  The first OR into an
+// accumulator appends the neighbour to the touched list T.  The warp clears
+// front[u] after reading it (nothing else reads front in a push level), so
+// that front is all-zero when the level ends.
+__global__ void k_ms_push(DevView G, const uint32_t *F, uint32_t nf, uint64_t *front,
+                          const uint64_t *seen, unsigned long long *acc, uint32_t *T,
+                          uint32_t *tcnt) {
   uint64_t w = ((uint64_t)blockIdx.x * MT + threadIdx.x) >> 5;
   uint32_t lane = threadIdx.x & 31;
   if (w >= nf) return;
   uint32_t u = F[w];
   uint64_t m = front[u];
+  __syncwarp();
+  if (lane == 0) front[u] = 0;
   NbrList L = nbr_list(G, u);
-  for (uint32_t j = lane; j < L.deg; j += 32) atomicOr(acc + L.at(j), (unsigned long long)m);
+  for (uint32_t j = lane; j < L.deg; j += 32) {
+    uint32_t x = L.at(j);
+    if ((m & ~seen[x]) == 0) continue;
+    if (atomicOr(acc + x, (unsigned long long)m) == 0) T[atomicAdd(tcnt, 1u)] = x;
+  }
 }
 
-// after a push: commit acc into seen / next for every vertex, collect the
-// next active list
-__global__ void k_ms_commit_all(uint32_t n, MSState s, unsigned long long *acc, uint32_t *list,
-                                uint32_t *list_cnt, unsigned long long *any) {
-  uint64_t v = (uint64_t)blockIdx.x * MT + threadIdx.x;
-  uint64_t nw = 0;
-  if (v < n) {
-    uint64_t a = acc[v];
-    if (a) acc[v] = 0;
-    uint64_t sv = s.seen[v];
-    nw = a & ~sv;
-    s.next[v] = nw;
-    if (nw) {
-      s.seen[v] = sv | nw;
-      list[atomicAdd(list_cnt, 1u)] = (uint32_t)v;
-      if (s.lvrow) write_levels(s, v, nw);
+// after a push: commit the touched accumulators into seen / next and append
+// the vertices with new sources to the next active list (grid-stride over
+// the device-side count of T)
+__global__ void k_ms_commit_list(MSState s, const uint32_t *T, const uint32_t *tcnt,
+                                 unsigned long long *acc, uint32_t *list, uint32_t *list_cnt,
+                                 unsigned long long *any) {
+  const uint32_t nt = *tcnt;
+  const uint64_t stride = (uint64_t)gridDim.x * MT;
+  for (uint64_t base = (uint64_t)blockIdx.x * MT; base < nt; base += stride) {
+    uint64_t i = base + threadIdx.x;
+    uint64_t nw = 0;
+    if (i < nt) {
+      uint32_t v = T[i];
+      uint64_t a = acc[v];
+      acc[v] = 0;
+      uint64_t sv = s.seen[v];
+      nw = a & ~sv;
+      if (nw) {
+        s.seen[v] = sv | nw;
+        s.next[v] = nw;
+        list[atomicAdd(list_cnt, 1u)] = v;
+        if (s.lvrow) write_levels(s, v, nw);
+      }
     }
+    warp_or_into(nw, any);
   }
-  if (any) warp_or_into(nw, any);
+}
+
+// clears front[v] for the vertices of the old active list (after a pull
+// level, so that the array is all-zero when it becomes `next`)
+__global__ void k_ms_clear(uint64_t *front, const uint32_t *F, uint32_t nf) {
+  uint64_t i = (uint64_t)blockIdx.x * MT + threadIdx.x;
+  if (i < nf) front[F[i]] = 0;
 }
 
 // active list after a pull step; `any` (optional) collects the sources
@@ -194,7 +222,8 @@ __global__ void k_ms_count(uint32_t n, const uint64_t *seen, unsigned long long 
 }
 
 __global__ void k_ms_init(uint32_t n, uint32_t k, const uint32_t *src, uint64_t *seen,
-                          uint64_t *front, uint32_t *lvrow, unsigned long long *acc) {
+                          uint64_t *front, uint64_t *next, uint32_t *lvrow,
+                          unsigned long long *acc) {
   uint64_t v = (uint64_t)blockIdx.x * MT + threadIdx.x;
   if (v >= n) return;
   uint64_t m = 0;
@@ -202,6 +231,7 @@ __global__ void k_ms_init(uint32_t n, uint32_t k, const uint32_t *src, uint64_t 
     if (src[i] == v) m |= 1ull << i;
   seen[v] = m;
   front[v] = m;
+  next[v] = 0;
   acc[v] = 0;
   if (lvrow)
     for (uint32_t i = 0; i < k; i++) lvrow[v * k + i] = (m >> i) & 1 ? 0u : TRC_UNREACHED;
@@ -264,55 +294,69 @@ void Graph::msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uin
   uint32_t *dsrc = srcb.alloc_exact(k);
   DBuf<uint64_t> anyb;
   anyb.bind(&budget);
-  // [0] sources that discovered a vertex this level, [1..64] reach counts
-  unsigned long long *any = summary ? (unsigned long long *)anyb.alloc_exact(65) : nullptr;
+  // [0] sources that discovered a vertex this level (the next level's live
+  // sources), [1..64] reach counts
+  unsigned long long *any = (unsigned long long *)anyb.alloc_exact(65);
   std::vector<uint32_t> depth(k, 0);
-  uint32_t *list = lst.alloc_exact(n), *c = cnt.alloc_exact(2);
+  // active lists (double-buffered) and the touched list of push levels
+  DBuf<uint32_t> lst2, tl;
+  lst2.bind(&budget);
+  tl.bind(&budget);
+  uint32_t *L[2] = {lst.alloc_exact(n), lst2.alloc_exact(n)};
+  uint32_t *T = tl.alloc_exact(n);
+  uint32_t *c = cnt.alloc_exact(4);  // [0] pull commits, [1] next active, [2] touched
   TRC_CUDA(cudaMemcpyAsync(dsrc, hsrc.data(), k * 4, cudaMemcpyHostToDevice, stream));
   TRC_LAUNCH(prof, stream, "ms_init", ceil_div(n, MT), MT, 0, k_ms_init, n, k, dsrc, seen, front,
-             lvrow, acc);
+             next, lvrow, acc);
   // initial active list = the distinct sources
   std::vector<uint32_t> act(hsrc);
   std::sort(act.begin(), act.end());
   act.erase(std::unique(act.begin(), act.end()), act.end());
-  TRC_CUDA(cudaMemcpyAsync(list, act.data(), act.size() * 4, cudaMemcpyHostToDevice, stream));
+  int cur = 0;
+  TRC_CUDA(cudaMemcpyAsync(L[cur], act.data(), act.size() * 4, cudaMemcpyHostToDevice, stream));
   uint32_t nact = (uint32_t)act.size();
-  const uint64_t all = k == 64 ? ~0ull : ((1ull << k) - 1);
+  uint64_t live = k == 64 ? ~0ull : ((1ull << k) - 1);
   const uint64_t dense_at = n / push_pull_divisor();
+  const unsigned commit_grid = (unsigned)std::max(1, num_sms() * 8);
   DevView G = view();
   uint32_t level = 0;
+  // invariants at the start of a level: front is non-zero exactly on
+  // L[cur] (nact vertices), next and acc are all-zero
   while (nact > 0) {
     level++;
-    TRC_CUDA(cudaMemsetAsync(c, 0, 8, stream));
-    if (any) TRC_CUDA(cudaMemsetAsync(any, 0, 8, stream));
-    MSState s{seen, front, next, lvrow, k, all, level, c};
+    TRC_CUDA(cudaMemsetAsync(c, 0, 16, stream));
+    TRC_CUDA(cudaMemsetAsync(any, 0, 8, stream));
+    MSState s{seen, front, next, lvrow, k, live, level, c};
+    uint32_t *nl = L[cur ^ 1];
     if ((uint64_t)nact >= dense_at && dense_at > 0) {
-      // vertices in no class list (isolated) keep an empty next mask
-      TRC_CUDA(cudaMemsetAsync(next, 0, (uint64_t)n * 8, stream));
       TRC_LAUNCH(prof, stream, "ms_pull_S", ceil_div(lists.nS * 4, MT), MT, 0, k_ms_pull_S, G,
                  lists.S.get(), lists.nS, s);
       TRC_LAUNCH(prof, stream, "ms_pull_M", ceil_div(lists.nM * 32, MT), MT, 0, k_ms_pull_W, G,
                  lists.M.get(), lists.nM, s);
       TRC_LAUNCH(prof, stream, "ms_pull_H", ceil_div(lists.nH * 32, MT), MT, 0, k_ms_pull_W, G,
                  lists.Hv.get(), lists.nH, s);
-      // isolated vertices are never in a frontier; their next mask stays 0
-      TRC_LAUNCH(prof, stream, "ms_collect", ceil_div(n, MT), MT, 0, k_ms_collect, n, next, list,
+      // isolated vertices are in no class list; their next mask stays 0
+      TRC_LAUNCH(prof, stream, "ms_collect", ceil_div(n, MT), MT, 0, k_ms_collect, n, next, nl,
                  c + 1, any);
+      TRC_LAUNCH(prof, stream, "ms_clear", ceil_div(nact, MT), MT, 0, k_ms_clear, front, L[cur],
+                 nact);
     } else {
       TRC_LAUNCH(prof, stream, "ms_push", ceil_div((uint64_t)nact * 32, MT), MT, 0, k_ms_push, G,
-                 list, nact, front, acc);
-      TRC_LAUNCH(prof, stream, "ms_commit", ceil_div(n, MT), MT, 0, k_ms_commit_all, n, s, acc,
-                 list, c + 1, any);
+                 L[cur], nact, front, seen, acc, T, c + 2);
+      TRC_LAUNCH(prof, stream, "ms_commit", commit_grid, MT, 0, k_ms_commit_list, s, T, c + 2,
+                 acc, nl, c + 1, any);
     }
     uint32_t hc[2];
     uint64_t hany = 0;
     TRC_CUDA(cudaMemcpyAsync(hc, c, 8, cudaMemcpyDeviceToHost, stream));
-    if (any) TRC_CUDA(cudaMemcpyAsync(&hany, any, 8, cudaMemcpyDeviceToHost, stream));
+    TRC_CUDA(cudaMemcpyAsync(&hany, any, 8, cudaMemcpyDeviceToHost, stream));
     sync();
     nact = hc[1];
+    live = hany;
     for (uint32_t i = 0; i < k; i++)
       if ((hany >> i) & 1) depth[i] = level;
     std::swap(front, next);
+    cur ^= 1;
   }
   if (summary) {
     TRC_CUDA(cudaMemsetAsync(any + 1, 0, 64 * 8, stream));

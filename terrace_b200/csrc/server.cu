@@ -58,6 +58,8 @@ struct Request {
   uint64_t out_count = 0;
   trc_status status = TRC_OK;
   bool done = false;
+  bool in_round = false;  // taken by the worker; deleted by it if released meanwhile
+  bool released = false;
 };
 
 // reached count and deepest level of one level array (summary of a BFS)
@@ -78,6 +80,11 @@ __global__ void k_level_summary(const uint32_t *lv, uint32_t n, unsigned long lo
     if (c) atomicAdd(reached, (unsigned long long)c);
     atomicMax(depth, d);
   }
+}
+
+__global__ void k_fill_f64(double *x, uint32_t n, double v) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = v;
 }
 
 // per-block partial sum and max of a rank vector; the host adds the
@@ -248,9 +255,11 @@ class Server {
     std::lock_guard<std::mutex> lk(mu_);
     auto it = all_.find(id);
     if (it == all_.end()) return;
-    if (!it->second->done) throw_error(TRC_ERR_STATE, "request not finished");
-    delete it->second;
+    Request *r = it->second;
+    if (!r->done) throw_error(TRC_ERR_STATE, "request not finished");
     all_.erase(it);
+    if (r->in_round) r->released = true;  // the worker still holds it
+    else delete r;
   }
 
   void stats(int kind, trc_server_stats *o) {
@@ -274,6 +283,13 @@ class Server {
     o->device_calls = calls_;
     o->rejected = rejected_;
     o->version = version_;
+    o->worst_round_ms = worst_.ms;
+    o->worst_update_ms = worst_.upd_ms;
+    o->worst_bfs_ms = worst_.bfs_ms;
+    o->worst_pagerank_ms = worst_.pr_ms;
+    o->worst_round_requests = worst_.requests;
+    o->worst_round_rebuilds = worst_.rebuilds;
+    o->pma_rebuilds = rebuilds_;
   }
 
   void reset_stats() {
@@ -282,6 +298,8 @@ class Server {
     t0_ = now_ms();
     last_done_ = 0;
     rounds_ = calls_ = rejected_ = 0;
+    worst_ = RoundInfo();
+    rebuilds_ = 0;
   }
 
  private:
@@ -300,9 +318,18 @@ class Server {
   DBuf<uint64_t> keys_[2], roff_;
   DBuf<uint32_t> ins_s_, ins_d_, del_s_, del_d_, up_s_, up_d_, rop_, lvl_;
   DBuf<int32_t> par_;
-  DBuf<double> ranks_;
+  DBuf<double> ranks_, pr0_, pr1_, pr_part_;
   DBuf<uint64_t> red_;
   bool bufs_bound_ = false;
+  cudaStream_t s2_ = nullptr;  // PageRank overlapping the BFS groups
+  double *pin_ = nullptr;      // pinned PageRank partial sums
+  unsigned pin_cap_ = 0;
+  std::vector<std::pair<size_t, size_t>> pr_groups_;
+  struct RoundInfo {
+    double ms = 0, upd_ms = 0, bfs_ms = 0, pr_ms = 0;
+    uint64_t requests = 0, rebuilds = 0;
+  } worst_;                    // guarded by mu_
+  uint64_t rebuilds_ = 0;      // guarded by mu_
 
   void bind_bufs() {
     if (bufs_bound_) return;
@@ -310,7 +337,7 @@ class Server {
     for (auto *b : {&ins_s_, &ins_d_, &del_s_, &del_d_, &up_s_, &up_d_, &rop_, &lvl_})
       b->bind(&g_.budget);
     par_.bind(&g_.budget);
-    ranks_.bind(&g_.budget);
+    for (auto *b : {&ranks_, &pr0_, &pr1_, &pr_part_}) b->bind(&g_.budget);
     bufs_bound_ = true;
   }
 
@@ -360,16 +387,18 @@ class Server {
 
   static bool is_update(trc_request_kind k) { return k == TRC_REQ_INSERT || k == TRC_REQ_DELETE; }
 
+  // completes requests (each part of a round completes as soon as it is done)
   void finish(std::vector<Request *> &rs) {
+    if (rs.empty()) return;
     double t = now_ms();
     std::lock_guard<std::mutex> lk(mu_);
     for (Request *r : rs) {
+      if (r->done) continue;
       r->t_done = t;
       r->done = true;
       lat_.push_back({(int)r->kind, r->t_done - r->t_arrive});
     }
     last_done_ = t;
-    rounds_++;
     done_cv_.notify_all();
   }
 
@@ -383,15 +412,17 @@ class Server {
 
   void loop() {
     cudaSetDevice(g_.device);
+    if (cudaStreamCreateWithFlags(&s2_, cudaStreamNonBlocking) != cudaSuccess) s2_ = nullptr;
     while (true) {
       std::vector<Request *> round;
       {
         std::unique_lock<std::mutex> lk(mu_);
         cv_.wait(lk, [&] { return stop_ || !pending_.empty(); });
-        if (pending_.empty() && stop_) return;
+        if (pending_.empty() && stop_) break;
         if (cfg_.mode == TRC_SERVE_FIFO) {
           round.push_back(pending_.front());
           pending_.pop_front();
+          round.back()->in_round = true;
         } else {
           // all pending queries, and updates up to the admission limits
           std::deque<Request *> keep;
@@ -399,12 +430,14 @@ class Server {
           bool blocked = false;
           for (Request *r : pending_) {
             if (!is_update(r->kind)) {
+              r->in_round = true;
               round.push_back(r);
               continue;
             }
             uint64_t e = r->a.size() * (cfg_.symmetrize ? 2 : 1);
             bool first = edges == 0;
             if (!blocked && (first || (edges + e <= cfg_.max_round_edges && fits(edges + e)))) {
+              r->in_round = true;
               round.push_back(r);
               edges += e;
             } else {
@@ -416,89 +449,167 @@ class Server {
         }
       }
       run_round(round);
-      finish(round);
+      rounds_++;
+      std::lock_guard<std::mutex> lk(mu_);
+      for (Request *r : round) {
+        r->in_round = false;
+        if (r->released) delete r;
+      }
+    }
+    if (s2_) {
+      cudaStreamSynchronize(s2_);
+      cudaStreamDestroy(s2_);
+    }
+    if (pin_) cudaFreeHost(pin_);
+  }
+
+  template <typename F>
+  void guarded(std::vector<Request *> &rs, F &&f) {
+    try {
+      f();
+    } catch (const Error &e) {
+      if (e.status == TRC_ERR_NOMEM && !rs.empty() && is_update(rs[0]->kind)) rejected_ += rs.size();
+      for (Request *r : rs)
+        if (!r->done) r->status = e.status;
+    } catch (const std::exception &) {
+      for (Request *r : rs)
+        if (!r->done) r->status = TRC_ERR_STATE;
     }
   }
 
+  // One round, cheapest parts first; every part completes its requests as
+  // soon as it is done:
+  //   1. degree / neighbour lookups on snapshot v;
+  //   2. the updates as one net change -> v+1;
+  //   3. PageRank (shared per iteration count) launched on a second stream
+  //      and overlapping with
+  //   4. the BFS groups (64 sources per multi-source launch) on v+1;
+  //   5. PageRank results.
+  // Nothing modifies the graph while 3-5 read it.
   void run_round(std::vector<Request *> &round) {
-    std::vector<Request *> q, u;
-    for (Request *r : round) (is_update(r->kind) ? u : q).push_back(r);
-    try {
-      run_queries(q);
-    } catch (const Error &e) {
-      for (Request *r : q) r->status = e.status;
-    } catch (const std::exception &) {
-      for (Request *r : q) r->status = TRC_ERR_STATE;
-    }
-    if (u.empty()) return;
-    try {
-      if (cfg_.mode == TRC_SERVE_FIFO || u.size() == 1) {
-        for (Request *r : u) apply_one(r);
-      } else {
-        apply_net(u);
-      }
-    } catch (const Error &e) {
-      if (e.status == TRC_ERR_NOMEM) rejected_ += u.size();
-      for (Request *r : u) r->status = e.status;
-    } catch (const std::exception &) {
-      for (Request *r : u) r->status = TRC_ERR_STATE;
-    }
-  }
-
-  void run_queries(std::vector<Request *> &q) {
-    if (q.empty()) return;
-    const uint32_t n = g_.n;
-    const bool full = cfg_.result_mode == TRC_RESULT_FULL;
-    // BFS: groups of up to max_bfs_group sources per multi-source launch
-    std::vector<Request *> bfs, deg, pr;
-    for (Request *r : q) {
-      r->version = version_;
-      if (r->kind == TRC_REQ_BFS) bfs.push_back(r);
-      else if (r->kind == TRC_REQ_DEGREE) deg.push_back(r);
+    std::vector<Request *> look, upd, bfs, pr;
+    for (Request *r : round) {
+      if (is_update(r->kind)) upd.push_back(r);
+      else if (r->kind == TRC_REQ_BFS) bfs.push_back(r);
       else if (r->kind == TRC_REQ_PAGERANK) pr.push_back(r);
-      else if (r->kind == TRC_REQ_NEIGHBORS) {
-        if (r->param >= n) {
-          r->status = TRC_ERR_INVALID;
-          continue;
-        }
-        uint32_t d = 0;
-        g_.degree(&r->param, 1, &d, 0);
-        r->out_u32.resize(d ? d : 1);
-        g_.neighbors(r->param, r->out_u32.data(), d, 0);
-        r->out_u32.resize(d);
-        r->out_count = d;
-        calls_ += 2;
-      }
+      else look.push_back(r);
     }
     bind_bufs();
+    RoundInfo info;
+    info.requests = round.size();
+    const uint64_t rb0 = g_.rebuilds;
+    const double t0 = now_ms();
+    guarded(look, [&] { run_lookups(look); });
+    finish(look);
+    const double t1 = now_ms();
+    if (!upd.empty()) {
+      guarded(upd, [&] {
+        if (cfg_.mode == TRC_SERVE_FIFO || upd.size() == 1) {
+          for (Request *r : upd) apply_one(r);
+        } else {
+          apply_net(upd);
+        }
+      });
+      finish(upd);
+    }
+    const double t2 = now_ms();
+    for (Request *r : bfs) r->version = version_;
+    for (Request *r : pr) r->version = version_;
+    bool pr_async = false;
+    guarded(pr, [&] { pr_async = start_pagerank(pr); });
+    if (!pr_async) finish(pr);  // computed synchronously (or failed)
+    const double t3 = now_ms();
+    guarded(bfs, [&] { run_bfs(bfs); });
+    finish(bfs);  // groups that completed were finished already
+    const double t4 = now_ms();
+    if (pr_async) {
+      guarded(pr, [&] { end_pagerank(pr); });
+      finish(pr);
+    }
+    const double t5 = now_ms();
+    info.ms = t5 - t0;
+    info.upd_ms = t2 - t1;
+    info.bfs_ms = t4 - t3;
+    info.pr_ms = (t3 - t2) + (t5 - t4);  // synchronous part + wait after the BFS groups
+    info.rebuilds = g_.rebuilds - rb0;
+    std::lock_guard<std::mutex> lk(mu_);
+    rebuilds_ += info.rebuilds;
+    if (info.ms > worst_.ms) worst_ = info;
+  }
+
+  void run_lookups(std::vector<Request *> &q) {
+    const uint32_t n = g_.n;
+    std::vector<Request *> deg;
+    for (Request *r : q) {
+      r->version = version_;
+      if (r->kind == TRC_REQ_DEGREE) {
+        deg.push_back(r);
+        continue;
+      }
+      if (r->param >= n) {  // neighbours
+        r->status = TRC_ERR_INVALID;
+        continue;
+      }
+      uint32_t d = 0;
+      g_.degree(&r->param, 1, &d, 0);
+      r->out_u32.resize(d ? d : 1);
+      g_.neighbors(r->param, r->out_u32.data(), d, 0);
+      r->out_u32.resize(d);
+      r->out_count = d;
+      calls_ += 2;
+    }
+    if (deg.empty()) return;
+    std::vector<uint32_t> all;  // one lookup launch for every degree request
+    for (Request *r : deg) all.insert(all.end(), r->a.begin(), r->a.end());
+    std::vector<uint32_t> out(all.size());
+    bool ok = true;
+    for (uint32_t v : all) ok &= v < n;
+    if (ok && !all.empty()) {
+      g_.degree(all.data(), all.size(), out.data(), 0);
+      calls_++;
+    }
+    size_t o = 0;
+    for (Request *r : deg) {
+      if (!ok) r->status = TRC_ERR_INVALID;
+      else r->out_u32.assign(out.begin() + o, out.begin() + o + r->a.size());
+      o += r->a.size();
+      r->out_count = r->a.size();
+    }
+  }
+
+  // smallest BFS group run as one multi-source launch: up to three
+  // single-source BFS (direction-optimising, compacted candidates) beat a
+  // multi-source launch on RMAT scale 25 (3 sources: 27-30 ms one by one vs
+  // 34-42 ms together); from 4-8 sources the shared traversal wins
+  static constexpr size_t kMinGroup = 4;
+
+  void run_bfs(std::vector<Request *> &bfs) {
+    const uint32_t n = g_.n;
+    const bool full = cfg_.result_mode == TRC_RESULT_FULL;
     for (size_t i = 0; i < bfs.size();) {
       size_t k = cfg_.mode == TRC_SERVE_FIFO ? 1 : std::min<size_t>(cfg_.max_bfs_group, bfs.size() - i);
+      std::vector<Request *> grp(bfs.begin() + i, bfs.begin() + i + k);
       std::vector<uint32_t> src(k);
       bool bad = false;
       for (size_t j = 0; j < k; j++) {
-        src[j] = bfs[i + j]->param;
+        src[j] = grp[j]->param;
         bad |= src[j] >= n;
       }
       if (bad) {  // the group's valid sources run one by one
-        for (size_t j = 0; j < k; j++) {
-          Request *r = bfs[i + j];
+        for (Request *r : grp) {
           if (r->param >= n) r->status = TRC_ERR_INVALID;
           else bfs_one(r, full);
         }
-        i += k;
-        continue;
-      }
-      if (k == 1) {
-        bfs_one(bfs[i], full);
+      } else if (k < kMinGroup) {  // below this, single-source BFS is faster
+        for (Request *r : grp) bfs_one(r, full);
       } else if (full) {
         std::vector<uint32_t> lv((uint64_t)k * n);
         g_.msbfs(src.data(), (uint32_t)k, lv.data(), 0);
         calls_++;
         for (size_t j = 0; j < k; j++) {
-          Request *r = bfs[i + j];
           const uint32_t *row = lv.data() + (uint64_t)j * n;
-          r->out_u32.assign(row, row + n);
-          r->out_count = n;
+          grp[j]->out_u32.assign(row, row + n);
+          grp[j]->out_count = n;
         }
       } else {
         std::vector<uint64_t> reached(k);
@@ -506,53 +617,86 @@ class Server {
         g_.msbfs_summary(src.data(), (uint32_t)k, reached.data(), ecc.data());
         calls_++;
         for (size_t j = 0; j < k; j++) {
-          Request *r = bfs[i + j];
-          r->out_u32 = {(uint32_t)reached[j], ecc[j]};
-          r->out_count = reached[j];
+          grp[j]->out_u32 = {(uint32_t)reached[j], ecc[j]};
+          grp[j]->out_count = reached[j];
         }
       }
+      finish(grp);
       i += k;
     }
-    if (!deg.empty()) {
-      std::vector<uint32_t> all;
-      for (Request *r : deg) all.insert(all.end(), r->a.begin(), r->a.end());
-      std::vector<uint32_t> out(all.size());
-      bool ok = true;
-      for (uint32_t v : all) ok &= v < n;
-      if (ok && !all.empty()) {
-        g_.degree(all.data(), all.size(), out.data(), 0);
-        calls_++;
-      }
-      size_t o = 0;
-      for (Request *r : deg) {
-        if (!ok) r->status = TRC_ERR_INVALID;
-        else r->out_u32.assign(out.begin() + o, out.begin() + o + r->a.size());
-        o += r->a.size();
-        r->out_count = r->a.size();
-      }
-    }
-    // PageRank: one computation per distinct iteration count
+  }
+
+  // PageRank groups (one computation per distinct iteration count).  In
+  // summary mode they run on the second stream and the call returns true;
+  // end_pagerank collects them.  Full results are copied synchronously.
+  bool start_pagerank(std::vector<Request *> &pr) {
+    pr_groups_.clear();
+    if (pr.empty()) return false;
+    const uint32_t n = g_.n;
     std::sort(pr.begin(), pr.end(), [](Request *x, Request *y) { return x->param < y->param; });
     for (size_t i = 0; i < pr.size();) {
       size_t j = i;
-      while (j < pr.size() && pr[j]->param == pr[i]->param &&
-             (cfg_.mode != TRC_SERVE_FIFO || j == i))
+      while (j < pr.size() && pr[j]->param == pr[i]->param && (cfg_.mode != TRC_SERVE_FIFO || j == i))
         j++;
-      std::vector<double> ranks;
-      double sum = 0, mx = 0;
-      if (full) {
-        ranks.resize(n);
-        g_.pagerank(pr[i]->param, 0.0, ranks.data(), 0);
-      } else {
-        pagerank_summary(pr[i]->param, &sum, &mx);
-      }
-      calls_++;
-      for (size_t t = i; t < j; t++) {
-        if (full) pr[t]->out_f64 = ranks;
-        else pr[t]->out_f64 = {sum, mx};
-        pr[t]->out_count = n;
-      }
+      pr_groups_.push_back({i, j});
       i = j;
+    }
+    const bool full = cfg_.result_mode == TRC_RESULT_FULL;
+    if (full || !s2_) {
+      for (auto &gr : pr_groups_) {
+        std::vector<double> ranks(full ? n : 0);
+        double sum = 0, mx = 0;
+        if (full) g_.pagerank(pr[gr.first]->param, 0.0, ranks.data(), 0);
+        else pagerank_summary(pr[gr.first]->param, &sum, &mx);
+        calls_++;
+        for (size_t t = gr.first; t < gr.second; t++) {
+          pr[t]->out_f64 = full ? ranks : std::vector<double>{sum, mx};
+          pr[t]->out_count = n;
+        }
+      }
+      return false;
+    }
+    // async: class lists current, buffers sized, then everything on s2_
+    g_.ensure_lists();
+    const unsigned nb = reduce_grid();
+    double *p0 = pr0_.ensure(n), *p1 = pr1_.ensure(n), *x = ranks_.ensure(n);
+    double *part = pr_part_.ensure(2 * (uint64_t)nb * pr_groups_.size());
+    if (pin_cap_ < 2 * nb * pr_groups_.size()) {
+      if (pin_) cudaFreeHost(pin_);
+      pin_cap_ = 2 * nb * (unsigned)pr_groups_.size();
+      TRC_CUDA(cudaMallocHost(&pin_, pin_cap_ * sizeof(double)));
+    }
+    g_.sync();  // allocations and lists complete before s2_ reads them
+    for (size_t gi = 0; gi < pr_groups_.size(); gi++) {
+      const uint32_t iters = pr[pr_groups_[gi].first]->param;
+      double *out = part + 2 * nb * gi;
+      if (iters == 0) {
+        TRC_LAUNCH(g_.prof, s2_, "srv_pr_uniform", ceil_div(n, 256), 256, 0, k_fill_f64, x, n,
+                   1.0 / (double)n);
+      } else {
+        g_.pagerank_launch(iters, 0.0, p0, p1, x, s2_);
+      }
+      TRC_LAUNCH(g_.prof, s2_, "srv_pr_summary", nb, 256, 0, k_rank_summary, x, n, out);
+      TRC_CUDA(cudaMemcpyAsync(pin_ + 2 * nb * gi, out, 16 * nb, cudaMemcpyDeviceToHost, s2_));
+      calls_++;
+    }
+    return true;
+  }
+
+  void end_pagerank(std::vector<Request *> &pr) {
+    TRC_CUDA(cudaStreamSynchronize(s2_));
+    const unsigned nb = reduce_grid();
+    for (size_t gi = 0; gi < pr_groups_.size(); gi++) {
+      double s = 0, m = 0;
+      const double *h = pin_ + 2 * nb * gi;
+      for (unsigned b = 0; b < nb; b++) {
+        s += h[2 * b];
+        m = std::max(m, h[2 * b + 1]);
+      }
+      for (size_t t = pr_groups_[gi].first; t < pr_groups_[gi].second; t++) {
+        pr[t]->out_f64 = {s, m};
+        pr[t]->out_count = g_.n;
+      }
     }
   }
 
@@ -596,6 +740,7 @@ class Server {
       return;
     }
     bind_bufs();
+    g_.phase(nullptr);
     const int sym = cfg_.symmetrize ? 1 : 0;
     uint64_t total = 0;
     for (Request *r : u) total += r->a.size() * (sym ? 2 : 1);
@@ -616,6 +761,7 @@ class Server {
       std::copy(r->b.begin(), r->b.end(), hd.begin() + off);
       off += r->a.size();
     }
+    g_.phase("srv_concat");
     uint32_t *ps = up_s_.ensure(np), *pd = up_d_.ensure(np), *dop = rop_.ensure(R);
     uint64_t *doff = roff_.ensure(R);
     TRC_CUDA(cudaMemcpyAsync(ps, hs.data(), np * 4, cudaMemcpyHostToDevice, s));
@@ -631,6 +777,7 @@ class Server {
     TRC_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, s));
     TRC_CUDA(cudaStreamSynchronize(s));
     if (herr) throw_error(TRC_ERR_INVALID, "vertex id out of range in an update");
+    g_.phase("srv_tag");
     // sort by (edge, arrival rank): every bit below the top spare bits
     uint32_t rb = 1;  // bits of (rank << 1 | op)
     while ((1ull << rb) < ((uint64_t)R << 1)) rb++;
@@ -653,6 +800,7 @@ class Server {
     select_if(LastOpPred{sorted, total, tagbits, 1}, KeyDst{sorted, tagbits, vb}, total, id, cnt, t,
               s, g_.prof, "srv_net_ins");
     uint64_t ni = g_.read_u64(cnt);
+    g_.phase("srv_net");
     uint64_t removed = nd ? g_.apply_batch(ds, dd, nd, TRC_DEVICE_PTR, false) : 0;
     uint64_t added = ni ? g_.apply_batch(is, id, ni, TRC_DEVICE_PTR, true) : 0;
     calls_ += 2;

@@ -49,6 +49,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   stream = own_stream;
   budget.stream = stream;
   budget.open_pool(device);
+  use_graphs = cfg.cuda_graphs != 0;
   for (auto *b : {&deg, &inl, &c2, &pma, &err, &hub_vtx, &hub_nblk, &hub_per, &hslot, &bcnt, &bmin,
                   &bown, &stamp, &s_in_src, &s_in_dst, &s_tu, &s_tdn, &s_tc2, &s_ovl, &s_hw_u,
                   &s_hw_dn, &s_hw_t, &s_c2n, &s_rlist, &s_pma_next, &lists.S, &lists.M, &lists.Hv,
@@ -94,6 +95,7 @@ Graph::~Graph() {
   if (own_stream) cudaStreamSynchronize(own_stream);
   if (stream && stream != own_stream) cudaStreamSynchronize(stream);
   prof.reset();
+  if (prg.exec) cudaGraphExecDestroy(prg.exec);
   // the members free after this body, on the legacy stream (the work on
   // the graph's streams has finished)
   budget.stream = nullptr;

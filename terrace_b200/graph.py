@@ -38,7 +38,7 @@ class Graph:
     def __init__(self, n: int, hbm_budget: int = 0, hub_threshold: int = 1024,
                  pma_root_density: float = 0.75, pma_build_density: float = 0.5,
                  hub_block_fill: float = 0.75, push_pull_divisor: int = 20,
-                 hub_stage_limit: int = 49152):
+                 hub_stage_limit: int = 49152, cuda_graphs: bool = True):
         self._L = L.load()
         cfg = L.trc_config()
         self._L.trc_config_default(C.byref(cfg))
@@ -48,6 +48,7 @@ class Graph:
         cfg.hub_block_fill = hub_block_fill
         cfg.push_pull_divisor = push_pull_divisor
         cfg.hub_stage_limit = hub_stage_limit
+        cfg.cuda_graphs = int(cuda_graphs)
         h = C.c_void_p()
         L.check(self._L.trc_graph_create(n, hbm_budget, C.byref(cfg), C.byref(h)))
         self._h = h
