@@ -198,6 +198,34 @@ trc_status trc_rmat_generate(uint32_t n, uint32_t seed, double a, double b,
                              uint32_t *src, uint32_t *dst, uint32_t flags,
                              void *stream);
 
+/* ---- autotuner (no reference counterpart: the reference fixes these at
+ *      compile time or as constants: the edgeMap threshold 20,
+ *      include/Map.cpp:65-74; PMA leaf sizing, src/PMA.cc:2961-2962).
+ *      trc_autotune times candidates on this graph and keeps the fastest;
+ *      later calls use them.  BFS levels and adjacency stay exact; PageRank
+ *      stays within FP64 reordering (1e-9 relative). */
+#define TRC_TUNE_PUSH_PULL 1u /* direction threshold: BFS from 4 sources */
+#define TRC_TUNE_PAGERANK 2u  /* PageRank lanes per vertex and degree cut */
+#define TRC_TUNE_PMA 4u       /* PMA leaf: insert + remove of the sample's
+                                 absent edges (the edge set is unchanged) */
+typedef struct {
+  uint32_t push_pull_divisor; /* dense when |F| >= n / divisor */
+  uint32_t pr_group_cut;      /* PageRank: degrees 17..cut use a lane group */
+  uint32_t pr_group_lanes;    /* lanes per vertex in that group: 4, 8, 16 */
+  uint32_t pma_leaf_log;      /* smallest PMA window: 2^x vertex segments */
+  double bfs_ms;              /* best time per BFS (0 if not tuned) */
+  double pagerank_iter_ms;    /* best time per PageRank iteration */
+  double pma_insert_ms;       /* best insert time of the sample */
+} trc_tuning;
+/* `what`: TRC_TUNE_* bits.  The sample (src, dst, k; flags TRC_DEVICE_PTR
+ * and TRC_SYMMETRIZE apply) is needed by TRC_TUNE_PMA only. */
+trc_status trc_autotune(trc_graph *g, uint32_t what, const uint32_t *src, const uint32_t *dst,
+                        uint64_t k, uint32_t flags, trc_tuning *out);
+trc_status trc_get_tuning(trc_graph *g, trc_tuning *out);
+/* Applies saved choices (validated: divisor >= 1, lanes 4/8/16, cut 17..4096,
+ * leaf 1..20). */
+trc_status trc_set_tuning(trc_graph *g, const trc_tuning *in);
+
 /* ---- serving layer (no reference counterpart: the reference has no serving
  *      mode and forbids updates concurrent with analytics, include/graph.h:
  *      73-230).  A persistent worker thread serves requests on the graph in

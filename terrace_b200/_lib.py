@@ -24,6 +24,7 @@ TRC_SYMMETRIZE = 0x2
 TRC_DROP_SELF_LOOPS = 0x4
 TRC_UNREACHED = 0xFFFFFFFF
 TRC_NOALLOC_MAX_VERTICES = 1048576
+TUNE_PUSH_PULL, TUNE_PAGERANK, TUNE_PMA = 1, 2, 4
 REQ_INSERT, REQ_DELETE, REQ_BFS, REQ_DEGREE, REQ_NEIGHBORS, REQ_PAGERANK = range(6)
 SERVE_FIFO, SERVE_BATCHED = 0, 1
 RESULT_FULL, RESULT_SUMMARY = 0, 1
@@ -52,6 +53,13 @@ class trc_device_view(C.Structure):
                 ("deg", C.c_void_p), ("inl", C.c_void_p), ("pbeg", C.c_void_p), ("pma", C.c_void_p),
                 ("hub_of", C.c_void_p), ("hub_blk0", C.c_void_p), ("hub_per", C.c_void_p),
                 ("hslot", C.c_void_p), ("stream", C.c_void_p)]
+
+
+class trc_tuning(C.Structure):
+    _fields_ = [("push_pull_divisor", C.c_uint32), ("pr_group_cut", C.c_uint32),
+                ("pr_group_lanes", C.c_uint32), ("pma_leaf_log", C.c_uint32),
+                ("bfs_ms", C.c_double), ("pagerank_iter_ms", C.c_double),
+                ("pma_insert_ms", C.c_double)]
 
 
 class trc_server_config(C.Structure):
@@ -128,6 +136,9 @@ SIGNATURES = [
     ("trc_profile_get", _int, [_vp, C.c_char_p, C.POINTER(_dbl), C.POINTER(_u64)]),
     ("trc_profile_names", _int, [_vp, C.c_char_p, _u64]),
     ("trc_launch_count", _int, [_vp, C.POINTER(_u64)]),
+    ("trc_autotune", _int, [_vp, _u32, _vp, _vp, _u64, _u32, C.POINTER(trc_tuning)]),
+    ("trc_get_tuning", _int, [_vp, C.POINTER(trc_tuning)]),
+    ("trc_set_tuning", _int, [_vp, C.POINTER(trc_tuning)]),
     ("trc_server_config_default", None, [C.POINTER(trc_server_config)]),
     ("trc_server_create", _int, [_vp, C.POINTER(trc_server_config), C.POINTER(_vp)]),
     ("trc_server_destroy", _int, [_vp]),

@@ -31,15 +31,16 @@ struct ClassPred {
   const uint32_t *deg;
   const int32_t *hub_of;
   int cls;  // 0 = S, 1 = M, 2 = H, 3 = S and M (non-hub, degree >= 1),
-            // 4 = M with 17..64 neighbours, 5 = M with more than 64
+            // 4 = M with 17..cut neighbours, 5 = M with more than cut
+  uint32_t cut;
   __device__ bool operator()(uint64_t i) const {
     bool hub = hub_of[i] >= 0;
     uint32_t d = deg[i];
     if (cls == 2) return hub;
     if (hub) return false;
     if (cls == 3) return d >= 1;
-    if (cls == 4) return d > K_INLINE && d <= 64;
-    if (cls == 5) return d > 64;
+    if (cls == 4) return d > K_INLINE && d <= cut;
+    if (cls == 5) return d > cut;
     return cls == 0 ? (d >= 1 && d <= K_INLINE) : d > K_INLINE;
   }
 };
@@ -56,7 +57,8 @@ void Graph::ensure_lists() {
                        lists.SM.ensure(n), lists.M1.ensure(n), lists.M2.ensure(n)};
   uint64_t lens[6];
   for (int c = 0; c < 6; c++) {
-    select_if(ClassPred{deg.get(), hub_of.get(), c}, IdxVal32{}, n, bufs[c], cnt + c, t, stream,
+    select_if(ClassPred{deg.get(), hub_of.get(), c, tuned.pr_group_cut}, IdxVal32{}, n, bufs[c],
+              cnt + c, t, stream,
               prof);
   }
   TRC_CUDA(cudaMemcpyAsync(lens, cnt, 48, cudaMemcpyDeviceToHost, stream));
@@ -392,8 +394,19 @@ void Graph::pr_kernels(uint32_t iters, double damping, double *p0, double *p1, d
     PRArgs a{p0, p1, out, damping, base, it + 1 == iters};
     TRC_LAUNCH(prof, s, "pr_S", ceil_div(lists.nS * 4, AT), AT, 0, k_pr_S, G, lists.S.get(),
                lists.nS, a);
-    TRC_LAUNCH(prof, s, "pr_M8", ceil_div(lists.nM1 * 8, AT), AT, 0, k_pr_group<8>, G,
-               lists.M1.get(), lists.nM1, a);
+    switch (tuned.pr_group_lanes) {
+      case 4:
+        TRC_LAUNCH(prof, s, "pr_M4", ceil_div(lists.nM1 * 4, AT), AT, 0, k_pr_group<4>, G,
+                   lists.M1.get(), lists.nM1, a);
+        break;
+      case 16:
+        TRC_LAUNCH(prof, s, "pr_M16", ceil_div(lists.nM1 * 16, AT), AT, 0, k_pr_group<16>, G,
+                   lists.M1.get(), lists.nM1, a);
+        break;
+      default:
+        TRC_LAUNCH(prof, s, "pr_M8", ceil_div(lists.nM1 * 8, AT), AT, 0, k_pr_group<8>, G,
+                   lists.M1.get(), lists.nM1, a);
+    }
     TRC_LAUNCH(prof, s, "pr_M32", ceil_div(lists.nM2 * 32, AT), AT, 0, k_pr_group<32>, G,
                lists.M2.get(), lists.nM2, a);
     TRC_LAUNCH(prof, s, "pr_H", lists.nH, AT, 0, k_pr_H, G, lists.Hv.get(), a);
@@ -417,7 +430,8 @@ void Graph::pagerank_launch(uint32_t iters, double damping, double *p0, double *
   memcpy(&dbits, &damping, 8);
   const uint64_t key[PRGraphCache::KEY] = {iters, dbits, (uint64_t)p0, (uint64_t)p1, (uint64_t)out,
                                            lists.version, (uint64_t)lists.S.get(), lists.nS,
-                                           lists.nM1, lists.nM2, lists.nH, (uint64_t)s};
+                                           lists.nM1, lists.nM2, lists.nH, (uint64_t)s,
+                                           tuned.pr_group_lanes};
   bool same = prg.exec != nullptr;
   for (int i = 0; same && i < PRGraphCache::KEY; i++) same = prg.key[i] == key[i];
   if (!same) {

@@ -110,6 +110,59 @@ trc_status trc_graph_destroy(trc_graph *g) {
   });
 }
 
+static void fill_tuning(const trc::Graph &g, trc_tuning *o) {
+  o->push_pull_divisor = g.tuned.push_pull_divisor;
+  o->pr_group_cut = g.tuned.pr_group_cut;
+  o->pr_group_lanes = g.tuned.pr_group_lanes;
+  o->pma_leaf_log = g.tuned.pma_leaf_log;
+}
+
+trc_status trc_autotune(trc_graph *g, uint32_t what, const uint32_t *src, const uint32_t *dst,
+                        uint64_t k, uint32_t flags, trc_tuning *out) {
+  return guard([&] {
+    trc::Graph &gr = G(g);
+    if (what & ~(TRC_TUNE_PUSH_PULL | TRC_TUNE_PAGERANK | TRC_TUNE_PMA))
+      trc::throw_error(TRC_ERR_INVALID, "unknown TRC_TUNE_* bit");
+    double ms[3];
+    gr.autotune(what, src, dst, k, flags, ms);
+    if (out) {
+      memset(out, 0, sizeof(*out));
+      fill_tuning(gr, out);
+      out->bfs_ms = ms[0];
+      out->pagerank_iter_ms = ms[1];
+      out->pma_insert_ms = ms[2];
+    }
+  });
+}
+
+trc_status trc_get_tuning(trc_graph *g, trc_tuning *out) {
+  return guard([&] {
+    if (!out) trc::throw_error(TRC_ERR_INVALID, "null output");
+    memset(out, 0, sizeof(*out));
+    fill_tuning(G(g), out);
+  });
+}
+
+trc_status trc_set_tuning(trc_graph *g, const trc_tuning *in) {
+  return guard([&] {
+    trc::Graph &gr = G(g);
+    if (!in) trc::throw_error(TRC_ERR_INVALID, "null input");
+    if (in->push_pull_divisor < 1) trc::throw_error(TRC_ERR_INVALID, "push_pull_divisor >= 1");
+    if (in->pr_group_lanes != 4 && in->pr_group_lanes != 8 && in->pr_group_lanes != 16)
+      trc::throw_error(TRC_ERR_INVALID, "pr_group_lanes must be 4, 8 or 16");
+    if (in->pr_group_cut <= trc::K_INLINE || in->pr_group_cut > 4096)
+      trc::throw_error(TRC_ERR_INVALID, "pr_group_cut must be in 17..4096");
+    if (in->pma_leaf_log < 1 || in->pma_leaf_log > 20)
+      trc::throw_error(TRC_ERR_INVALID, "pma_leaf_log must be in 1..20");
+    gr.sync();
+    if (in->pr_group_cut != gr.tuned.pr_group_cut) gr.lists.version = ~0ull;
+    gr.tuned.push_pull_divisor = in->push_pull_divisor;
+    gr.tuned.pr_group_cut = in->pr_group_cut;
+    gr.tuned.pr_group_lanes = in->pr_group_lanes;
+    gr.tuned.pma_leaf_log = in->pma_leaf_log;
+  });
+}
+
 trc_status trc_graph_set_stream(trc_graph *g, void *stream) {
   return guard([&] {
     trc::Graph &gr = G(g);

@@ -117,7 +117,7 @@ class Graph {
   void pr_kernels(uint32_t iters, double damping, double *p0, double *p1, double *out,
                   cudaStream_t s);
   struct PRGraphCache {
-    static constexpr int KEY = 12;
+    static constexpr int KEY = 13;
     cudaGraphExec_t exec = nullptr;
     uint64_t key[KEY] = {};
     uint64_t kernels = 0;       // kernel nodes per replay
@@ -135,9 +135,17 @@ class Graph {
   double phase_t0 = 0.0;
   uint64_t read_u64(const uint64_t *dptr);
   void sync();
-  uint32_t push_pull_divisor() const {
-    return cfg.push_pull_divisor ? cfg.push_pull_divisor : 20u;
-  }
+  uint32_t push_pull_divisor() const { return tuned.push_pull_divisor; }
+
+  // per-graph choices (config defaults, changed by trc_autotune / trc_set_tuning)
+  struct Tuning {
+    uint32_t push_pull_divisor = 20;  // dense traversal when |F| >= n / divisor
+    uint32_t pr_group_cut = 64;       // PageRank: degree 17..cut use a lane group
+    uint32_t pr_group_lanes = 8;      // ... of this many lanes (4, 8 or 16); above: a warp
+    uint32_t pma_leaf_log = 1;        // smallest PMA window: 2^x vertex segments
+  } tuned;
+  void autotune(uint32_t what, const uint32_t *src, const uint32_t *dst, uint64_t k,
+                uint32_t flags, double *ms_out);
 
  private:
   void grow_hub_tables(uint32_t need);

@@ -50,6 +50,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   budget.stream = stream;
   budget.open_pool(device);
   use_graphs = cfg.cuda_graphs != 0;
+  if (cfg.push_pull_divisor) tuned.push_pull_divisor = cfg.push_pull_divisor;
   for (auto *b : {&deg, &inl, &c2, &pma, &err, &hub_vtx, &hub_nblk, &hub_per, &hslot, &bcnt, &bmin,
                   &bown, &stamp, &s_in_src, &s_in_dst, &s_tu, &s_tdn, &s_tc2, &s_ovl, &s_hw_u,
                   &s_hw_dn, &s_hw_t, &s_c2n, &s_rlist, &s_pma_next, &lists.S, &lists.M, &lists.Hv,
@@ -329,15 +330,15 @@ struct LoadC2 {
   __device__ uint64_t operator()(uint64_t i) const { return c[i]; }
 };
 
-// Window search (step 5): lowest level whose aligned vertex range has
-// density within its bound.  Keys sort by (start asc, level desc).
+// Window search (step 5): lowest level (from the leaf level, 2^leaf vertex
+// segments) whose aligned vertex range has density within its bound.  Keys sort by (start asc, level desc).
 __global__ void k_find_windows(const uint32_t *ovl, uint64_t nov, const uint64_t *P,
-                               const uint64_t *pbeg, uint32_t n, uint32_t levels, double root_dens,
-                               uint64_t *wkeys, uint64_t *cnt) {
+                               const uint64_t *pbeg, uint32_t n, uint32_t levels, uint32_t leaf,
+                               double root_dens, uint64_t *wkeys, uint64_t *cnt) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nov) return;
   uint32_t u = ovl[i];
-  for (uint32_t h = 1; h <= levels; h++) {
+  for (uint32_t h = leaf; h <= levels; h++) {
     uint64_t a = ((uint64_t)u >> h) << h;
     uint64_t b = a + (1ull << h);
     if (b > n) b = n;
@@ -932,7 +933,8 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     } else {
       uint64_t *wk = s_wk.ensure(nov), *wk2 = s_wk2.ensure(nov);
       TRC_LAUNCH(prof, stream, "upd_find_windows", ceil_div(nov, 256), 256, 0, k_find_windows, ovl,
-                 nov, P, pbeg.get(), n, levels, root_d, wk, cnt);
+                 nov, P, pbeg.get(), n, levels, std::min(std::max(tuned.pma_leaf_log, 1u), levels),
+                 root_d, wk, cnt);
       uint64_t root = read_u64(cnt + C_ROOT);
       if (root) {
         rebuild = true;

@@ -235,6 +235,42 @@ class Graph:
         return int(x.value)
 
     # ---------------------------------------------------------------- diagnostics
+    # ---------------------------------------------------------------- tuning
+    def autotune(self, push_pull: bool = True, pagerank: bool = True, sample=None,
+                 symmetrize: bool = True) -> dict:
+        """trc_autotune: times candidate choices on this graph and keeps the
+        fastest.  `sample` = (srcs, dests) tunes the PMA leaf (inserted and
+        removed again; the edge set is unchanged)."""
+        what = (L.TUNE_PUSH_PULL if push_pull else 0) | (L.TUNE_PAGERANK if pagerank else 0)
+        ps = pd = None
+        k = 0
+        flags = L.TRC_SYMMETRIZE if symmetrize else 0
+        keep = ()
+        if sample is not None:
+            what |= L.TUNE_PMA
+            a, na, fa, ka = _arr(sample[0], np.uint32)
+            b, nb, fb, kb = _arr(sample[1], np.uint32)
+            if na != nb or fa != fb:
+                raise ValueError("sample arrays differ in length or location")
+            ps, pd, k, keep = C.c_void_p(a), C.c_void_p(b), na, (ka, kb)
+            flags |= fa
+        t = L.trc_tuning()
+        L.check(self._L.trc_autotune(self._h, what, ps, pd, k, flags, C.byref(t)))
+        del keep
+        return {k: getattr(t, k) for k, _ in L.trc_tuning._fields_}
+
+    def get_tuning(self) -> dict:
+        t = L.trc_tuning()
+        L.check(self._L.trc_get_tuning(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in L.trc_tuning._fields_}
+
+    def set_tuning(self, **kw):
+        t = L.trc_tuning()
+        L.check(self._L.trc_get_tuning(self._h, C.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, v)
+        L.check(self._L.trc_set_tuning(self._h, C.byref(t)))
+
     def stats(self) -> dict:
         s = L.trc_stats()
         L.check(self._L.trc_get_stats(self._h, C.byref(s)))

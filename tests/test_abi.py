@@ -85,6 +85,15 @@ def test_no_cpu_fallback_without_gpu():
     assert e.value.status == 3  # TRC_ERR_CUDA
 
 
+def test_tuning_abi_without_gpu(lib):
+    from terrace_b200 import _lib
+    L = _lib.load()
+    t = _lib.trc_tuning()
+    assert L.trc_get_tuning(None, ctypes.byref(t)) == _lib.TRC_ERR_INVALID
+    assert L.trc_set_tuning(None, ctypes.byref(t)) == _lib.TRC_ERR_INVALID
+    assert L.trc_autotune(None, 1, None, None, 0, 0, ctypes.byref(t)) == _lib.TRC_ERR_INVALID
+
+
 def test_server_abi_without_gpu(lib):
     """Server entry points validate their handles before any device work."""
     from terrace_b200 import _lib
