@@ -140,7 +140,8 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     bulk_s = time.perf_counter() - t0
     del s, d
-    nb = args.warmup + 2 * args.steps
+    # batches: W warm-up, K timed, K profiled, K end-to-end (each used once)
+    nb = args.warmup + 3 * args.steps
     batches = [T.rmat_generate(n, batch_seed(BATCH_STREAM, j), A, B, C, BATCH, device=True)
                for j in range(nb)]
     torch.cuda.synchronize()
@@ -187,7 +188,7 @@ def run_ours(args, rank, world):
     g.profile(True)
     g.profile_reset()
     sizes = []
-    pb = batches[args.warmup + args.steps:]
+    pb = batches[args.warmup + args.steps:args.warmup + 2 * args.steps]
     for bs_, bd_ in pb:
         g.add_edge_batch(bs_, bd_, symmetrize=True, drop_self_loops=True)
         sizes.append(g.stats())
@@ -205,8 +206,8 @@ def run_ours(args, rank, world):
     for j in range(args.steps):
         hs = torch.empty(BATCH, dtype=torch.int32, pin_memory=True)
         hd = torch.empty(BATCH, dtype=torch.int32, pin_memory=True)
-        hs.copy_(batches[args.warmup + j][0].cpu())
-        hd.copy_(batches[args.warmup + j][1].cpu())
+        hs.copy_(batches[args.warmup + 2 * args.steps + j][0].cpu())
+        hd.copy_(batches[args.warmup + 2 * args.steps + j][1].cpu())
         host.append((hs.numpy().view(np.uint32), hd.numpy().view(np.uint32)))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
