@@ -179,9 +179,26 @@ def run_ours(args, rank, world):
     inserted = sum(ins)
     value = inserted * world / (ins_ms / 1e3)
     pairs_per_s = BATCH * args.steps * world / (ins_ms / 1e3)
+    # ---- e2e: same metric through the public API with pinned HOST buffers,
+    # K fresh batches right after the timed ones (same graph state)
+    host = []
+    for j in range(args.steps):
+        hs = torch.empty(BATCH, dtype=torch.int32, pin_memory=True)
+        hd = torch.empty(BATCH, dtype=torch.int32, pin_memory=True)
+        hs.copy_(batches[args.warmup + 2 * args.steps + j][0].cpu())
+        hd.copy_(batches[args.warmup + 2 * args.steps + j][1].cpu())
+        host.append((hs.numpy().view(np.uint32), hd.numpy().view(np.uint32)))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_cnt = [g.add_edge_batch(hs, hd, symmetrize=True, drop_self_loops=True) for hs, hd in host]
+    e2e_s = time.perf_counter() - t0
+    e2e_val = sum(e2e_cnt) * world / e2e_s
+
     del_ms, dels = timed(lambda i: g.remove_edge_batch(*batches[args.warmup + i], symmetrize=True,
                                                        drop_self_loops=True), args.steps)
     deleted = sum(dels)
+    for hs, hd in host:
+        g.remove_edge_batch(hs, hd, symmetrize=True, drop_self_loops=True)
 
     # ---- profiled pass (separate from the timed region): K fresh batches of
     # the same stream, CUDA events around every kernel, per-batch sizes
@@ -200,22 +217,6 @@ def run_ours(args, rank, world):
         g.remove_edge_batch(bs_, bd_, symmetrize=True, drop_self_loops=True)
     for j in range(args.warmup):
         g.remove_edge_batch(*batches[j], symmetrize=True, drop_self_loops=True)
-
-    # ---- e2e: same metric through the public API with pinned HOST buffers
-    host = []
-    for j in range(args.steps):
-        hs = torch.empty(BATCH, dtype=torch.int32, pin_memory=True)
-        hd = torch.empty(BATCH, dtype=torch.int32, pin_memory=True)
-        hs.copy_(batches[args.warmup + 2 * args.steps + j][0].cpu())
-        hd.copy_(batches[args.warmup + 2 * args.steps + j][1].cpu())
-        host.append((hs.numpy().view(np.uint32), hd.numpy().view(np.uint32)))
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e2e_cnt = [g.add_edge_batch(hs, hd, symmetrize=True, drop_self_loops=True) for hs, hd in host]
-    e2e_s = time.perf_counter() - t0
-    for hs, hd in host:
-        g.remove_edge_batch(hs, hd, symmetrize=True, drop_self_loops=True)
-    e2e_val = sum(e2e_cnt) * world / e2e_s
 
     # ---- analytics on the scale-22 graph (device outputs)
     st = g.stats()
