@@ -355,32 +355,6 @@ __global__ void k_find_windows(const uint32_t *ovl, uint64_t nov, const uint64_t
   atomicOr((unsigned long long *)&cnt[C_ROOT], 1ull);
 }
 
-// A sorted unique window is maximal when no enclosing window (same range
-// at a higher level) was also chosen.
-struct MaximalWindowPred {
-  const uint64_t *w;
-  uint64_t nw;
-  uint32_t levels;
-  __device__ bool operator()(uint64_t i) const {
-    uint64_t x = w[i];
-    if (i > 0 && w[i - 1] == x) return false;  // duplicate
-    uint64_t a = x >> 6;
-    uint32_t h = 63 - (uint32_t)(x & 63);
-    for (uint32_t hh = h + 1; hh <= levels; hh++) {
-      uint64_t aa = (a >> hh) << hh;
-      uint64_t key = (aa << 6) | (uint64_t)(63 - hh);
-      uint64_t lo = 0, hi = nw;
-      while (lo < hi) {
-        uint64_t mid = (lo + hi) >> 1;
-        if (w[mid] < key) lo = mid + 1;
-        else hi = mid;
-      }
-      if (lo < nw && w[lo] == key) return false;
-    }
-    return true;
-  }
-};
-
 struct LoadU64Val {
   const uint64_t *p;
   __device__ uint64_t operator()(uint64_t i) const { return p[i]; }
@@ -409,6 +383,92 @@ __device__ __forceinline__ void window_range(uint64_t x, uint32_t n, uint64_t &a
   b = a + (1ull << h);
   if (b > n) b = n;
 }
+
+// Maximal windows by a prefix maximum instead of per-level searches.
+// Aligned windows are nested or disjoint, and the key order (start
+// ascending, larger window first) puts every enclosing window before the
+// windows it contains, so window i is maximal exactly when its start is at
+// or above the largest end among windows 0..i-1 (a duplicate key fails the
+// test against its twin).  Pass 1: largest end per tile; pass 2 (one CTA):
+// exclusive running maximum over the tiles; pass 3: the running maximum
+// inside each tile and the flag.
+constexpr int WT = 256;  // threads per tile, one key each
+
+__device__ __forceinline__ uint64_t window_end(uint64_t x, uint32_t n) {
+  uint64_t a, b;
+  window_range(x, n, a, b);
+  return b;
+}
+
+__global__ void k_win_tilemax(const uint64_t *w, uint64_t nw, uint32_t n, uint64_t *tmax) {
+  __shared__ uint64_t sh[WT / 32];
+  uint64_t i = (uint64_t)blockIdx.x * WT + threadIdx.x;
+  uint64_t e = i < nw ? window_end(w[i], n) : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e = max(e, __shfl_xor_sync(0xFFFFFFFFu, e, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t m = 0;
+    for (int k = 0; k < WT / 32; k++) m = max(m, sh[k]);
+    tmax[blockIdx.x] = m;
+  }
+}
+
+// one CTA: tmax[t] <- max(tmax[0..t-1]) (0 for t = 0), in chunks of WT
+__global__ void k_win_tilescan(uint64_t *tmax, uint64_t nt) {
+  __shared__ uint64_t sh[WT / 32];
+  uint64_t carry = 0;
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (uint64_t base = 0; base < nt; base += WT) {
+    uint64_t i = base + threadIdx.x;
+    uint64_t v = i < nt ? tmax[i] : 0;
+    uint64_t inc = v;  // inclusive warp max
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint64_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+      if ((int)lane >= o) inc = max(inc, t);
+    }
+    if (lane == 31) sh[wid] = inc;
+    __syncthreads();
+    uint64_t before = carry;  // max of earlier warps in this chunk and earlier chunks
+    for (uint32_t k = 0; k < wid; k++) before = max(before, sh[k]);
+    uint64_t excl = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
+    excl = lane ? max(before, excl) : before;
+    uint64_t chunk_max = carry;
+    for (int k = 0; k < WT / 32; k++) chunk_max = max(chunk_max, sh[k]);
+    __syncthreads();
+    if (i < nt) tmax[i] = excl;
+    carry = chunk_max;
+  }
+}
+
+__global__ void k_win_flag(const uint64_t *w, uint64_t nw, uint32_t n, const uint64_t *tprefix,
+                           uint8_t *flag) {
+  __shared__ uint64_t sh[WT / 32];
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint64_t i = (uint64_t)blockIdx.x * WT + threadIdx.x;
+  uint64_t x = i < nw ? w[i] : 0;
+  uint64_t e = i < nw ? window_end(x, n) : 0;
+  uint64_t inc = e;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint64_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+    if ((int)lane >= o) inc = max(inc, t);
+  }
+  if (lane == 31) sh[wid] = inc;
+  __syncthreads();
+  uint64_t before = tprefix[blockIdx.x];
+  for (uint32_t k = 0; k < wid; k++) before = max(before, sh[k]);
+  uint64_t excl = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
+  excl = lane ? max(before, excl) : before;
+  if (i < nw) flag[i] = (x >> 6) >= excl ? 1 : 0;
+}
+
+struct ByteFlagPred {
+  const uint8_t *f;
+  __device__ bool operator()(uint64_t i) const { return f[i] != 0; }
+};
 
 // One CTA per maximal window: put its vertices in the rewrite set.
 __global__ void k_window_mark(const uint64_t *mw, uint32_t n, uint32_t *stamp, uint32_t epoch) {
@@ -1081,9 +1141,15 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
         const int wshifts[5] = {0, 8, 16, 24, 32};
         uint64_t *ws = radix_sort_u64_shifts(wk, wk2, nov, wshifts, 5, t2, stream, prof);
         uint64_t *mw = s_mw.ensure(nov);
-        uint64_t *t3 = tmp(select_tmp_elems(nov) + 4);
-        select_if(MaximalWindowPred{ws, nov, levels}, LoadU64Val{ws}, nov, mw, cnt + C_NMW, t3,
-                  stream, prof, "sel_windows");
+        const uint64_t wtiles = ceil_div(nov, WT);
+        uint64_t *t3 = tmp(select_tmp_elems(nov) + wtiles + 4);
+        uint64_t *tmx = t3 + select_tmp_elems(nov) + 2;
+        uint8_t *wflag = s_flags.ensure(nov);
+        TRC_LAUNCH(prof, stream, "upd_win_tilemax", wtiles, WT, 0, k_win_tilemax, ws, nov, n, tmx);
+        TRC_LAUNCH(prof, stream, "upd_win_tilescan", 1, WT, 0, k_win_tilescan, tmx, wtiles);
+        TRC_LAUNCH(prof, stream, "upd_win_flag", wtiles, WT, 0, k_win_flag, ws, nov, n, tmx, wflag);
+        select_if(ByteFlagPred{wflag}, LoadU64Val{ws}, nov, mw, cnt + C_NMW, t3, stream, prof,
+                  "sel_windows");
         nmw = read_u64(cnt + C_NMW);
       }
     }
