@@ -1,45 +1,78 @@
 // prims.cu -- radix sort, merge-path merge and sorted difference of 64-bit
 // keys (declarations and the scan/select templates are in prims.cuh).
+#include <algorithm>
+
 #include "prims.cuh"
 
 namespace trc {
 
 // ---------------------------------------------------------------------------
-// Radix sort.  Per 8-bit digit: (1) per-tile digit histogram, written
-// digit-major so that (2) one exclusive scan gives every (digit, tile) its
-// global output offset, then (3) a stable scatter: each warp ranks its keys
-// with __match_any_sync, warps are combined with a per-digit prefix in
-// shared memory.
+// Radix sort, one sweep per 8-bit digit.  (1) One pass over the keys counts
+// every digit position at once (per-CTA shared histograms, then global
+// atomics), (2) one CTA turns the counts into each digit value's global
+// start, (3) per digit, one scatter kernel: each tile ranks its keys (warp
+// __match_any_sync ranking, warps combined by a per-digit prefix in shared
+// memory), publishes its per-digit counts, and finds the counts of all
+// earlier tiles by decoupled look-back over a status word per (tile, digit)
+// (flag in the top bits, running count below; tiles take ids in launch
+// order from an atomic counter, so a tile only waits on tiles that started
+// before it).  The wait is bounded: after OS_SPIN_LIMIT polls the tile sets
+// ERR_TIMEOUT in the error word and proceeds (its output is then garbage and
+// the caller fails the call).
 
-__global__ void k_rs_hist(const uint64_t *in, uint64_t n, int shift, uint32_t ntiles,
-                          uint64_t *hist) {
-  __shared__ uint32_t h[256];
-  h[threadIdx.x] = 0;
+constexpr uint64_t OS_AGG = 1ull << 62;   // tile count published
+constexpr uint64_t OS_INC = 2ull << 62;   // count of this tile and all before it
+constexpr uint64_t OS_VAL = (1ull << 62) - 1;
+constexpr uint32_t OS_SPIN_LIMIT = 1u << 22;
+constexpr int OS_MAXD = 8;
+
+struct OsShifts {
+  int s[OS_MAXD];
+  int n;
+};
+
+__global__ void __launch_bounds__(RS_T) k_os_hist(const uint64_t *in, uint64_t n, OsShifts sh,
+                                                  unsigned long long *ghist) {
+  __shared__ uint32_t h[OS_MAXD][256];
+  for (int i = threadIdx.x; i < OS_MAXD * 256; i += RS_T) (&h[0][0])[i] = 0;
   __syncthreads();
-  uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
-#pragma unroll 4
-  for (int i = 0; i < RS_I; i++) {
-    uint64_t idx = base + (uint64_t)i * RS_T + threadIdx.x;
-    if (idx < n) atomicAdd(&h[(uint32_t)(in[idx] >> shift) & 255u], 1u);
+  const uint64_t stride = (uint64_t)gridDim.x * RS_T;
+  for (uint64_t i = (uint64_t)blockIdx.x * RS_T + threadIdx.x; i < n; i += stride) {
+    uint64_t k = in[i];
+    for (int d = 0; d < sh.n; d++) atomicAdd(&h[d][(uint32_t)(k >> sh.s[d]) & 255u], 1u);
   }
   __syncthreads();
-  hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+  for (int d = 0; d < sh.n; d++)
+    if (h[d][threadIdx.x]) atomicAdd(&ghist[d * 256 + threadIdx.x], (unsigned long long)h[d][threadIdx.x]);
 }
 
-__global__ void __launch_bounds__(RS_T) k_rs_scatter(const uint64_t *in, uint64_t *out, uint64_t n,
-                                                     int shift, uint32_t ntiles,
-                                                     const uint64_t *offs) {
+// one CTA of 256 threads: exclusive prefix of every digit position's counts
+__global__ void k_os_prefix(const unsigned long long *ghist, int nd, uint64_t *goff) {
+  __shared__ uint64_t ws[RS_T / 32 + 1];
+  for (int d = 0; d < nd; d++) {
+    uint64_t tot;
+    uint64_t ex = block_excl_scan<uint64_t, RS_T>(ghist[d * 256 + threadIdx.x], ws, tot);
+    goff[d * 256 + threadIdx.x] = ex;
+  }
+}
+
+__global__ void __launch_bounds__(RS_T) k_os_scatter(const uint64_t *in, uint64_t *out, uint64_t n,
+                                                     int shift, const uint64_t *goff,
+                                                     uint64_t *status, uint32_t *tile_ctr,
+                                                     uint32_t *err) {
   __shared__ uint32_t wh[RS_W][256];
   __shared__ uint64_t tbase[256];
+  __shared__ uint32_t tile_s;
   for (int i = threadIdx.x; i < RS_W * 256; i += RS_T) (&wh[0][0])[i] = 0;
-  tbase[threadIdx.x] = offs[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
+  if (threadIdx.x == 0) tile_s = atomicAdd(tile_ctr, 1u);
   __syncthreads();
+  const uint32_t tile = tile_s;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // warp w owns keys [base, base + RS_I*32) of the tile, slot-major
-  uint64_t base = (uint64_t)blockIdx.x * RS_TILE + (uint64_t)warp * (RS_I * 32);
+  const uint64_t base = (uint64_t)tile * RS_TILE + (uint64_t)warp * (RS_I * 32);
   uint64_t k[RS_I];
   uint32_t rank[RS_I];
-  uint32_t lt = lanemask_lt();
+  const uint32_t lt = lanemask_lt();
 #pragma unroll
   for (int s = 0; s < RS_I; s++) {
     uint64_t idx = base + (uint64_t)s * 32 + lane;
@@ -58,13 +91,41 @@ __global__ void __launch_bounds__(RS_T) k_rs_scatter(const uint64_t *in, uint64_
   }
   __syncthreads();
   {
-    uint32_t d = threadIdx.x, run = 0;
+    // thread d: offsets of digit d inside the tile (per warp) and the tile's count
+    const uint32_t d = threadIdx.x;
+    uint32_t run = 0;
 #pragma unroll
     for (int w = 0; w < RS_W; w++) {
       uint32_t c = wh[w][d];
       wh[w][d] = run;
       run += c;
     }
+    volatile uint64_t *st = status;
+    uint64_t excl = 0;
+    if (tile == 0) {
+      st[d] = OS_INC | run;
+    } else {
+      st[(uint64_t)tile * 256 + d] = OS_AGG | run;
+      int64_t t = (int64_t)tile - 1;
+      uint32_t spins = 0;
+      while (t >= 0) {
+        uint64_t v = st[(uint64_t)t * 256 + d];
+        uint64_t f = v & ~OS_VAL;
+        if (f == 0) {
+          if (++spins > OS_SPIN_LIMIT) {
+            atomicOr(err, ERR_TIMEOUT);
+            break;
+          }
+          if (spins > 64) __nanosleep(64);
+          continue;
+        }
+        excl += v & OS_VAL;
+        if (f == OS_INC) break;
+        t--;
+      }
+      st[(uint64_t)tile * 256 + d] = OS_INC | (excl + run);
+    }
+    tbase[d] = goff[d] + excl;
   }
   __syncthreads();
 #pragma unroll
@@ -79,32 +140,45 @@ __global__ void __launch_bounds__(RS_T) k_rs_scatter(const uint64_t *in, uint64_
 
 uint64_t radix_tmp_elems(uint64_t n) {
   uint64_t tiles = ceil_div(n, RS_TILE);
-  return tiles * 256 + scan_tmp_elems(tiles * 256) + tiles * 256 + 2;
+  // histograms + digit starts (OS_MAXD x 256 each), status (tiles x 256),
+  // tile counters (one word per digit position)
+  return 2 * OS_MAXD * 256 + tiles * 256 + OS_MAXD + 2;
 }
 
 uint64_t *radix_sort_u64(uint64_t *keys, uint64_t *alt, uint64_t n, uint32_t vbits,
-                         uint64_t *tmp, cudaStream_t s, Profiler &prof) {
+                         uint64_t *tmp, cudaStream_t s, Profiler &prof, uint32_t *err) {
   // digit shifts: dst bits [0,vbits) and src bits [32,32+vbits)
   int shifts[16];
   int ns = 0;
   for (int sh = 0; sh < (int)vbits; sh += 8) shifts[ns++] = sh;
   for (int sh = 32; sh < 32 + (int)vbits; sh += 8) shifts[ns++] = sh;
-  return radix_sort_u64_shifts(keys, alt, n, shifts, ns, tmp, s, prof);
+  return radix_sort_u64_shifts(keys, alt, n, shifts, ns, tmp, s, prof, err);
 }
 
 uint64_t *radix_sort_u64_shifts(uint64_t *keys, uint64_t *alt, uint64_t n, const int *shifts,
-                                int ns, uint64_t *tmp, cudaStream_t s, Profiler &prof) {
-  if (n <= 1) return keys;
-  uint32_t ntiles = (uint32_t)ceil_div(n, RS_TILE);
-  uint64_t *hist = tmp;
-  uint64_t *offs = tmp + (uint64_t)ntiles * 256;
-  uint64_t *stmp = offs + (uint64_t)ntiles * 256 + 1;
+                                int ns, uint64_t *tmp, cudaStream_t s, Profiler &prof,
+                                uint32_t *err) {
+  if (n <= 1 || ns == 0) return keys;
+  if (ns > OS_MAXD) throw_error(TRC_ERR_INVALID, "too many radix digits");
+  const uint64_t ntiles = ceil_div(n, RS_TILE);
+  if (ntiles > 0xFFFFFFFFull) throw_error(TRC_ERR_INVALID, "sort too large");
+  unsigned long long *ghist = (unsigned long long *)tmp;
+  uint64_t *goff = tmp + OS_MAXD * 256;
+  uint64_t *status = goff + OS_MAXD * 256;
+  uint32_t *ctr = (uint32_t *)(status + ntiles * 256);
+  OsShifts sh;
+  sh.n = ns;
+  for (int i = 0; i < OS_MAXD; i++) sh.s[i] = i < ns ? shifts[i] : 0;
+  TRC_CUDA(cudaMemsetAsync(ghist, 0, (size_t)OS_MAXD * 256 * 8, s));
+  TRC_CUDA(cudaMemsetAsync(ctr, 0, (size_t)OS_MAXD * 4, s));
+  const unsigned hgrid = (unsigned)std::min<uint64_t>(ceil_div(n, RS_T * 8), (uint64_t)num_sms() * 8);
+  TRC_LAUNCH(prof, s, "radix_hist", hgrid, RS_T, 0, k_os_hist, keys, n, sh, ghist);
+  TRC_LAUNCH(prof, s, "radix_prefix", 1, RS_T, 0, k_os_prefix, ghist, ns, goff);
   uint64_t *cur = keys, *nxt = alt;
   for (int i = 0; i < ns; i++) {
-    TRC_LAUNCH(prof, s, "radix_hist", ntiles, RS_T, 0, k_rs_hist, cur, n, shifts[i], ntiles, hist);
-    exclusive_scan(LoadU64{hist}, (uint64_t)ntiles * 256, offs, stmp, s, prof);
-    TRC_LAUNCH(prof, s, "radix_scatter", ntiles, RS_T, 0, k_rs_scatter, cur, nxt, n, shifts[i],
-               ntiles, offs);
+    TRC_CUDA(cudaMemsetAsync(status, 0, ntiles * 256 * 8, s));
+    TRC_LAUNCH(prof, s, "radix_scatter", ntiles, RS_T, 0, k_os_scatter, cur, nxt, n, shifts[i],
+               goff + i * 256, status, ctr + i, err);
     uint64_t *t = cur;
     cur = nxt;
     nxt = t;

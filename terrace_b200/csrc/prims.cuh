@@ -195,26 +195,26 @@ inline uint64_t select_tmp_elems(uint64_t n) {
 }
 
 // ------------------------------------------------------------- radix sort
-// LSD radix sort of 64-bit keys, 8-bit digits, stable.  Only the digit
-// positions listed are sorted (keys are (src<<32)|dst with src,dst < 2^b,
-// so the digits at shifts 0,8,..<b and 32,40,..<32+b suffice).
+// LSD radix sort of 64-bit keys, 8-bit digits, stable, one sweep per digit
+// (prims.cu).  Only the digit positions listed are sorted (keys are
+// (src<<32)|dst with src,dst < 2^b, so the digits at shifts 0,8,..<b and
+// 32,40,..<32+b suffice).
 constexpr int RS_T = 256;
 constexpr int RS_I = 16;
 constexpr int RS_TILE = RS_T * RS_I;  // 4096 keys
 constexpr int RS_W = RS_T / 32;
 
-__global__ void k_rs_hist(const uint64_t *in, uint64_t n, int shift, uint32_t ntiles,
-                          uint64_t *hist);
-__global__ void k_rs_scatter(const uint64_t *in, uint64_t *out, uint64_t n, int shift,
-                             uint32_t ntiles, const uint64_t *offs);
-
 // Sorts keys[0..n) using alt as the ping-pong buffer; returns the buffer that
 // holds the result (keys or alt).  tmp needs radix_tmp_elems(n) entries.
+// err: device error word; ERR_TIMEOUT is or-ed in if a look-back wait gave
+// up (the caller must then fail the call).
 uint64_t *radix_sort_u64(uint64_t *keys, uint64_t *alt, uint64_t n, uint32_t vbits,
-                         uint64_t *tmp, cudaStream_t s, Profiler &prof);
-// Same, over an explicit list of 8-bit digit shifts (least significant first).
+                         uint64_t *tmp, cudaStream_t s, Profiler &prof, uint32_t *err);
+// Same, over an explicit list of at most 8 digit shifts (least significant
+// first).
 uint64_t *radix_sort_u64_shifts(uint64_t *keys, uint64_t *alt, uint64_t n, const int *shifts,
-                                int ns, uint64_t *tmp, cudaStream_t s, Profiler &prof);
+                                int ns, uint64_t *tmp, cudaStream_t s, Profiler &prof,
+                                uint32_t *err);
 uint64_t radix_tmp_elems(uint64_t n);
 
 // ------------------------------------------------------------ merge path

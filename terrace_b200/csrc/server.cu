@@ -786,7 +786,7 @@ class Server {
     for (uint32_t sh = 0; sh < rb; sh += 8) shifts[ns++] = (int)sh;
     for (uint32_t sh = tagbits; sh < 64; sh += 8) shifts[ns++] = (int)sh;
     uint64_t *t = g_.s_tmp.ensure(radix_tmp_elems(total) + 2 * select_tmp_elems(total) + 8);
-    uint64_t *sorted = radix_sort_u64_shifts(K, K2, total, shifts, ns, t, s, g_.prof);
+    uint64_t *sorted = radix_sort_u64_shifts(K, K2, total, shifts, ns, t, s, g_.prof, err);
     uint64_t *cnt = g_.s_cnt.get() + 30;
     uint32_t *ds = del_s_.ensure(total), *dd = del_d_.ensure(total);
     uint32_t *is = ins_s_.ensure(total), *id = ins_d_.ensure(total);
@@ -800,6 +800,10 @@ class Server {
     select_if(LastOpPred{sorted, total, tagbits, 1}, KeyDst{sorted, tagbits, vb}, total, id, cnt, t,
               s, g_.prof, "srv_net_ins");
     uint64_t ni = g_.read_u64(cnt);
+    uint32_t herr2 = 0;
+    TRC_CUDA(cudaMemcpyAsync(&herr2, err, 4, cudaMemcpyDeviceToHost, s));
+    TRC_CUDA(cudaStreamSynchronize(s));
+    if (herr2 & ERR_TIMEOUT) throw_error(TRC_ERR_TIMEOUT, "radix sort look-back wait gave up");
     g_.phase("srv_net");
     uint64_t removed = nd ? g_.apply_batch(ds, dd, nd, TRC_DEVICE_PTR, false) : 0;
     uint64_t added = ni ? g_.apply_batch(is, id, ni, TRC_DEVICE_PTR, true) : 0;

@@ -1014,7 +1014,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   TRC_LAUNCH(prof, stream, "upd_make_keys", ceil_div(k, 256), 256, 0, k_make_keys, src, dst, k, n,
              sym, drop, A, err.get());
   uint64_t *t = tmp(std::max(radix_tmp_elems(k2), select_tmp_elems(k2)));
-  uint64_t *sorted = radix_sort_u64(A, B, k2, vbits(), t, stream, prof);
+  uint64_t *sorted = radix_sort_u64(A, B, k2, vbits(), t, stream, prof, err.get());
   uint64_t *bkeys = sorted == A ? B : A;
   // 3: unique + existence filter (one lookup per key), compacted
   uint8_t *kflags = s_flags.ensure(k2);
@@ -1032,6 +1032,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   TRC_CUDA(cudaMemcpyAsync(&herr, err.get(), 4, cudaMemcpyDeviceToHost, stream));
   sync();
   if (herr & ERR_BAD_VERTEX) throw_error(TRC_ERR_INVALID, "vertex id out of range [0, n)");
+  if (herr & ERR_TIMEOUT) throw_error(TRC_ERR_TIMEOUT, "radix sort look-back wait gave up");
   phase("sort_filter");
   const uint64_t kb = hc[C_KB], nt = hc[C_NT];
   if (kb == 0) {
@@ -1139,7 +1140,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
         uint64_t *t2 = tmp(radix_tmp_elems(nov) + 4);
         // window keys: start (< 2^32) << 6 | level code -> the low 38 bits
         const int wshifts[5] = {0, 8, 16, 24, 32};
-        uint64_t *ws = radix_sort_u64_shifts(wk, wk2, nov, wshifts, 5, t2, stream, prof);
+        uint64_t *ws = radix_sort_u64_shifts(wk, wk2, nov, wshifts, 5, t2, stream, prof, err.get());
         uint64_t *mw = s_mw.ensure(nov);
         const uint64_t wtiles = ceil_div(nov, WT);
         uint64_t *t3 = tmp(select_tmp_elems(nov) + wtiles + 4);
@@ -1151,6 +1152,10 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
         select_if(ByteFlagPred{wflag}, LoadU64Val{ws}, nov, mw, cnt + C_NMW, t3, stream, prof,
                   "sel_windows");
         nmw = read_u64(cnt + C_NMW);
+        uint32_t werr = 0;
+        TRC_CUDA(cudaMemcpyAsync(&werr, err.get(), 4, cudaMemcpyDeviceToHost, stream));
+        sync();
+        if (werr & ERR_TIMEOUT) throw_error(TRC_ERR_TIMEOUT, "radix sort look-back wait gave up");
       }
     }
   }
