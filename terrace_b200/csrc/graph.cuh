@@ -75,7 +75,6 @@ class Graph {
   DBuf<uint32_t> s_pma_next;
   DBuf<uint32_t> s_tix;  // vertex -> index in the touched list (this batch)
   DBuf<uint32_t> s_hw_do;  // old degree of each touched hub
-  DBuf<uint32_t> s_ovf;    // vertices the register merge leaves to the staged one
   ClassLists lists;
 
   DevView view() const;

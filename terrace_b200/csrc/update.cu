@@ -63,7 +63,6 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   wstamp.bind(&budget);
   pbeg_alt.bind(&budget);
   s_tix.bind(&budget);
-  s_ovf.bind(&budget);
   s_hw_do.bind(&budget);
   s_hw_h.bind(&budget);
   s_flags.bind(&budget);
@@ -130,7 +129,7 @@ DevView Graph::view() const {
 void Graph::release_scratch() {
   sync();
   for (auto *b : {&s_in_src, &s_in_dst, &s_tu, &s_tdn, &s_tc2, &s_ovl, &s_hw_u, &s_hw_dn, &s_hw_t,
-                  &s_c2n, &s_rlist, &s_pma_next, &s_tix, &s_hw_do, &s_ovf})
+                  &s_c2n, &s_rlist, &s_pma_next, &s_tix, &s_hw_do})
     b->reset();
   for (auto *b : {&s_A, &s_B, &s_C, &s_tmp, &s_P, &s_oOff, &s_nOff, &s_wk, &s_wk2, &s_mw, &s_old,
                   &s_new, &s_hwplan, &pbeg_alt})
@@ -704,98 +703,25 @@ __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *A, uint32_t 
   return lo;
 }
 
-// Staged variant: the old list's tail is copied to shared memory first.
-// Used (persistent, over a device-side list) for insertions that add more
-// than MF_KEYS keys to one vertex.
-__device__ __forceinline__ void merge_staged(const DevView &G, const MergeArgs &a, uint32_t u,
-                                             uint32_t lane, uint32_t *A) {
-  NbrList L = nbr_list(G, u);
-  const uint32_t d = L.deg;
-  uint64_t t = a.tix[u];
-  uint64_t b0 = 0, b1 = 0;
-  if (t != NONE32) {
-    b0 = a.tpos[t];
-    b1 = t + 1 < a.nt ? a.tpos[t + 1] : a.kb;
-  }
-  const uint32_t nb = (uint32_t)(b1 - b0);
-  const uint64_t *B = a.bkeys + b0;
-  const uint32_t dn = a.insert ? d + nb : d - nb;
-  uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
-  const bool moved = a.wstamp && a.wstamp[u] == a.epoch;
-  uint32_t *seg = (moved ? a.mov_pma : a.dst_pma) + a.pbeg_new[u];
-  // A list that stays where it is keeps the elements below the batch's
-  // first key (they neither move nor change): only the tail from p on is
-  // staged and rewritten.
-  uint32_t p = 0;
-  if (a.inplace && !moved && nb > 0) p = warp_list_lower_bound(L, d, (uint32_t)B[0], lane);
-  const uint32_t dt = d - p;
-  for (uint32_t j = lane; j < dt; j += 32) A[j] = L.at(p + j);
-  __syncwarp();
-  if (a.insert) {
-    for (uint32_t i = lane; i < dt; i += 32) {
-      uint32_t x = A[i];
-      uint32_t r = p + i + lower_bound_keys(B, nb, x);
-      if (r < K_INLINE) row[r] = x;
-      else seg[r - K_INLINE] = x;
-    }
-    for (uint32_t j = lane; j < nb; j += 32) {
-      uint32_t x = (uint32_t)B[j];
-      uint32_t r = p + j + lower_bound_u32(A, dt, x);
-      if (r < K_INLINE) row[r] = x;
-      else seg[r - K_INLINE] = x;
-    }
-  } else {
-    for (uint32_t i = lane; i < dt; i += 32) {
-      uint32_t x = A[i];
-      uint32_t c = lower_bound_keys(B, nb, x);
-      if (c < nb && (uint32_t)B[c] == x) continue;
-      uint32_t r = p + i - c;
-      if (r < K_INLINE) row[r] = x;
-      else seg[r - K_INLINE] = x;
-    }
-  }
-  if (lane == 0) G.deg[u] = dn;
-}
-
-// persistent: every warp loops over the device-side list
-__global__ void k_merge_staged(DevView G, MergeArgs a, const uint32_t *lst, const uint32_t *cnt) {
-  extern __shared__ uint32_t smem[];
-  const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t nw = *cnt;
-  const uint64_t stride = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t w = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib; w < nw; w += stride)
-    merge_staged(G, a, lst[w], lane, smem + (uint64_t)wib * a.T);
-}
-
 // Register variant (no shared memory, so occupancy is set by registers):
 // the list is moved in chunks of MF_CH elements held in registers, which is
 // safe in place because an insertion only moves elements up (chunks are
 // taken from the top down) and a deletion only moves them down (bottom up);
-// the loads of a chunk complete (__syncwarp) before its stores.  The ranks
-// of the inserted keys are computed from the intact list before anything
-// moves, one key per lane, so an insertion of more than MF_KEYS keys into
-// one vertex goes to the staged variant instead (appended to `ovf`).
+// the loads of a chunk complete (__syncwarp) before its stores.
+// Insertion ranks without searching the old list: with c(i) = number of
+// batch keys below old element i (c(p-1) = 0, c(d) = nb), key j lands at
+// j + i for the i with c(i-1) <= j < c(i); the lane holding element i writes
+// those keys while the chunk is in registers, at positions >= i >= the
+// chunk's start, so no unread element is overwritten.
 constexpr uint32_t MF_R = 4;
 constexpr uint32_t MF_CH = 32 * MF_R;
-constexpr uint32_t MF_KEYS = 32;
 
 __device__ __forceinline__ void put_rank(uint32_t *row, uint32_t *seg, uint32_t r, uint32_t x) {
   if (r < K_INLINE) row[r] = x;
   else seg[r - K_INLINE] = x;
 }
 
-__device__ __forceinline__ uint32_t list_lower_bound_from(const NbrList &L, uint32_t lo,
-                                                          uint32_t hi, uint32_t x) {
-  while (lo < hi) {
-    uint32_t mid = (lo + hi) >> 1;
-    if (L.at(mid) < x) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
-}
-
-__global__ void __launch_bounds__(256, 8) k_merge_small(DevView G, MergeArgs a, uint32_t *ovf,
-                                                     uint32_t *novf) {
+__global__ void __launch_bounds__(256, 8) k_merge_small(DevView G, MergeArgs a) {
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= a.nrs) return;
@@ -807,42 +733,53 @@ __global__ void __launch_bounds__(256, 8) k_merge_small(DevView G, MergeArgs a, 
     b1 = t + 1 < a.nt ? a.tpos[t + 1] : a.kb;
   }
   const uint32_t nb = (uint32_t)(b1 - b0);
-  if (a.insert && nb > MF_KEYS) {
-    if (lane == 0) ovf[atomicAdd(novf, 1u)] = u;
-    return;
-  }
   NbrList L = nbr_list(G, u);
   const uint32_t d = L.deg;
   const uint64_t *B = a.bkeys + b0;
   uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
   const bool moved = a.wstamp && a.wstamp[u] == a.epoch;
   uint32_t *seg = (moved ? a.mov_pma : a.dst_pma) + a.pbeg_new[u];
-  uint32_t p = 0;  // elements below the first key keep their place (in place only)
-  if (a.inplace && !moved && nb > 0) p = warp_list_lower_bound(L, d, (uint32_t)B[0], lane);
+  // elements below the first key keep their place (in place, long lists)
+  uint32_t p = 0;
+  if (a.inplace && !moved && nb > 0 && d > MF_CH)
+    p = warp_list_lower_bound(L, d, (uint32_t)B[0], lane);
   if (a.insert) {
-    uint32_t kx = 0, kr = 0;
-    if (lane < nb) {
-      kx = (uint32_t)B[lane];
-      kr = lane + list_lower_bound_from(L, p, d, kx);
-    }
+    // keys above every old element: ranks j + d
+    uint32_t ctop = 0;
+    if (d > p) ctop = lower_bound_keys(B, nb, L.at(d - 1));
+    for (uint32_t j = ctop + lane; j < nb; j += 32) put_rank(row, seg, j + d, (uint32_t)B[j]);
     for (uint32_t e = d; e > p;) {
       const uint32_t s0 = e - p > MF_CH ? e - MF_CH : p;
-      uint32_t x[MF_R];
+      uint32_t x[MF_R], c[MF_R];
 #pragma unroll
       for (uint32_t k = 0; k < MF_R; k++) {
         uint32_t i = s0 + k * 32 + lane;
         x[k] = i < e ? L.at(i) : 0u;
       }
+      // keys below the chunk's first element (from the element under it)
+      uint32_t cbelow = 0;
+      if (s0 > p) cbelow = lower_bound_keys(B, nb, L.at(s0 - 1));
+#pragma unroll
+      for (uint32_t k = 0; k < MF_R; k++) {
+        uint32_t i = s0 + k * 32 + lane;
+        c[k] = i < e ? lower_bound_keys(B, nb, x[k]) : 0u;
+      }
       __syncwarp();
 #pragma unroll
       for (uint32_t k = 0; k < MF_R; k++) {
         uint32_t i = s0 + k * 32 + lane;
-        if (i < e) put_rank(row, seg, i + lower_bound_keys(B, nb, x[k]), x[k]);
+        uint32_t cp = __shfl_up_sync(0xFFFFFFFFu, c[k], 1);
+        uint32_t last = k > 0 ? __shfl_sync(0xFFFFFFFFu, c[k > 0 ? k - 1 : 0], 31) : cbelow;
+        if (lane == 0) cp = last;
+        if (i < e) {
+          put_rank(row, seg, i + c[k], x[k]);
+          for (uint32_t j = cp; j < c[k]; j++) put_rank(row, seg, j + i, (uint32_t)B[j]);
+        }
       }
       __syncwarp();
       e = s0;
     }
-    if (lane < nb) put_rank(row, seg, kr, kx);
+    // list empty above p (d == p): the keys all went above
   } else {
     for (uint32_t s0 = p; s0 < d; s0 += MF_CH) {
       const uint32_t e = d - s0 > MF_CH ? s0 + MF_CH : d;
@@ -857,8 +794,8 @@ __global__ void __launch_bounds__(256, 8) k_merge_small(DevView G, MergeArgs a, 
       for (uint32_t k = 0; k < MF_R; k++) {
         uint32_t i = s0 + k * 32 + lane;
         if (i < e) {
-          uint32_t c = lower_bound_keys(B, nb, x[k]);
-          if (!(c < nb && (uint32_t)B[c] == x[k])) put_rank(row, seg, i - c, x[k]);
+          uint32_t cc = lower_bound_keys(B, nb, x[k]);
+          if (!(cc < nb && (uint32_t)B[cc] == x[k])) put_rank(row, seg, i - cc, x[k]);
         }
       }
       __syncwarp();
@@ -1226,17 +1163,8 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   if (nrs) {
     MergeArgs ma{rs, nrs, tix, tpos, nt, kb, bkeys, insert ? 1 : 0, pbeg_new, dst_pma, mov_pma,
                  nmw ? wstamp.get() : nullptr, epoch, T, dst_pma == pma.get() ? 1 : 0};
-    uint32_t *ovf = s_ovf.ensure(nrs);
-    uint32_t *novf = err.get() + 1;  // err[1]: overflow count of this batch
-    TRC_CUDA(cudaMemsetAsync(novf, 0, 4, stream));
     TRC_LAUNCH(prof, stream, "upd_merge_small", ceil_div(nrs * 32, 256), 256, 0, k_merge_small, G,
-               ma, ovf, novf);
-    if (insert) {  // insertions of more than MF_KEYS keys into one vertex
-      uint32_t wpc = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(8, (48u << 10) / (4ull * T)));
-      size_t smem = (size_t)wpc * T * 4;
-      TRC_LAUNCH(prof, stream, "upd_merge_staged", (unsigned)num_sms() * 4, wpc * 32, smem,
-                 k_merge_staged, G, ma, ovf, novf);
-    }
+               ma);
   }
 
   phase("merge_small");
