@@ -61,15 +61,19 @@ __global__ void __launch_bounds__(RS_T) k_os_scatter(const uint64_t *in, uint64_
                                                      uint64_t *status, uint32_t *tile_ctr,
                                                      uint32_t *err) {
   __shared__ uint32_t wh[RS_W][256];
-  __shared__ uint64_t tbase[256];
+  __shared__ uint64_t tbase[256];    // global start of digit d for this tile, minus its tile start
+  __shared__ uint32_t dstart[256];   // start of digit d inside the tile (tile-sorted order)
+  __shared__ uint64_t stage[RS_TILE];
   __shared__ uint32_t tile_s;
+  __shared__ uint32_t ws[RS_W + 1];
   for (int i = threadIdx.x; i < RS_W * 256; i += RS_T) (&wh[0][0])[i] = 0;
   if (threadIdx.x == 0) tile_s = atomicAdd(tile_ctr, 1u);
   __syncthreads();
   const uint32_t tile = tile_s;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // warp w owns keys [base, base + RS_I*32) of the tile, slot-major
-  const uint64_t base = (uint64_t)tile * RS_TILE + (uint64_t)warp * (RS_I * 32);
+  const uint64_t tile0 = (uint64_t)tile * RS_TILE;
+  const uint64_t base = tile0 + (uint64_t)warp * (RS_I * 32);
   uint64_t k[RS_I];
   uint32_t rank[RS_I];
   const uint32_t lt = lanemask_lt();
@@ -100,6 +104,10 @@ __global__ void __launch_bounds__(RS_T) k_os_scatter(const uint64_t *in, uint64_
       wh[w][d] = run;
       run += c;
     }
+    // start of digit d in the tile-sorted order
+    uint32_t tot;
+    uint32_t ex = block_excl_scan<uint32_t, RS_T>(run, ws, tot);
+    dstart[d] = ex;
     volatile uint64_t *st = status;
     uint64_t excl = 0;
     if (tile == 0) {
@@ -125,16 +133,25 @@ __global__ void __launch_bounds__(RS_T) k_os_scatter(const uint64_t *in, uint64_
       }
       st[(uint64_t)tile * 256 + d] = OS_INC | (excl + run);
     }
-    tbase[d] = goff[d] + excl;
+    tbase[d] = goff[d] + excl - ex;  // + tile-sorted position = output position
   }
   __syncthreads();
+  // stage the tile in digit order, then write it out: consecutive threads
+  // write consecutive keys of one digit to consecutive output slots
 #pragma unroll
   for (int s = 0; s < RS_I; s++) {
     uint64_t idx = base + (uint64_t)s * 32 + lane;
     if (idx < n) {
       uint32_t d = (uint32_t)(k[s] >> shift) & 255u;
-      out[tbase[d] + wh[warp][d] + rank[s]] = k[s];
+      stage[dstart[d] + wh[warp][d] + rank[s]] = k[s];
     }
+  }
+  __syncthreads();
+  const uint32_t valid = n - tile0 < (uint64_t)RS_TILE ? (uint32_t)(n - tile0) : (uint32_t)RS_TILE;
+  for (uint32_t j = threadIdx.x; j < valid; j += RS_T) {
+    uint64_t x = stage[j];
+    uint32_t d = (uint32_t)(x >> shift) & 255u;
+    out[tbase[d] + j] = x;
   }
 }
 

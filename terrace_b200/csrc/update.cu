@@ -721,10 +721,8 @@ __device__ __forceinline__ void put_rank(uint32_t *row, uint32_t *seg, uint32_t 
   else seg[r - K_INLINE] = x;
 }
 
-__global__ void __launch_bounds__(256, 8) k_merge_small(DevView G, MergeArgs a) {
-  const uint32_t lane = threadIdx.x & 31;
-  const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= a.nrs) return;
+__device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a, uint64_t w,
+                                          uint32_t lane) {
   const uint32_t u = a.rs[w];
   uint64_t t = a.tix[u];
   uint64_t b0 = 0, b1 = 0;
@@ -804,18 +802,32 @@ __global__ void __launch_bounds__(256, 8) k_merge_small(DevView G, MergeArgs a) 
   if (lane == 0) G.deg[u] = a.insert ? d + nb : d - nb;
 }
 
-// Moves the segments written to the window buffer to their final slots.
-__global__ void k_window_copy(DevView G, const uint32_t *rs, uint64_t nrs, const uint32_t *mov,
-                              const uint64_t *pbeg_new, const uint32_t *wstamp, uint32_t epoch) {
-  uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  uint32_t lane = threadIdx.x & 31;
-  if (w >= nrs) return;
-  uint32_t u = rs[w];
-  if (wstamp[u] != epoch) return;
-  uint32_t dn = G.deg[u];
-  if (dn <= K_INLINE) return;
-  uint64_t o = pbeg_new[u];
-  for (uint32_t j = lane; j < dn - K_INLINE; j += 32) G.pma[o + j] = mov[o + j];
+// persistent over the rewrite list, whose length is read on the device
+__global__ void __launch_bounds__(256, 8) k_merge_small(DevView G, MergeArgs a,
+                                                        const uint64_t *nrs) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t nw = *nrs;
+  const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nw; w += stride)
+    merge_one(G, a, w, lane);
+}
+
+// Moves the segments written to the window buffer to their final slots
+// (persistent over the rewrite list, length read on the device).
+__global__ void k_window_copy(DevView G, const uint32_t *rs, const uint64_t *nrs,
+                              const uint32_t *mov, const uint64_t *pbeg_new, const uint32_t *wstamp,
+                              uint32_t epoch) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t nw = *nrs;
+  const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nw; w += stride) {
+    uint32_t u = rs[w];
+    if (wstamp[u] != epoch) continue;
+    uint32_t dn = G.deg[u];
+    if (dn <= K_INLINE) continue;
+    uint64_t o = pbeg_new[u];
+    for (uint32_t j = lane; j < dn - K_INLINE; j += 32) G.pma[o + j] = mov[o + j];
+  }
 }
 
 __global__ void k_window_mark2(const uint64_t *mw, uint32_t n, uint32_t *stamp, uint32_t *wstamp,
@@ -1070,30 +1082,32 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
       TRC_LAUNCH(prof, stream, "upd_find_windows", ceil_div(nov, 256), 256, 0, k_find_windows, ovl,
                  nov, P, pbeg.get(), n, levels, std::min(std::max(tuned.pma_leaf_log, 1u), levels),
                  root_d, wk, cnt);
-      uint64_t root = read_u64(cnt + C_ROOT);
-      if (root) {
-        rebuild = true;
-      } else {
-        uint64_t *t2 = tmp(radix_tmp_elems(nov) + 4);
-        // window keys: start (< 2^32) << 6 | level code -> the low 38 bits
-        const int wshifts[5] = {0, 8, 16, 24, 32};
-        uint64_t *ws = radix_sort_u64_shifts(wk, wk2, nov, wshifts, 5, t2, stream, prof, err.get());
-        uint64_t *mw = s_mw.ensure(nov);
-        const uint64_t wtiles = ceil_div(nov, WT);
-        uint64_t *t3 = tmp(select_tmp_elems(nov) + wtiles + 4);
-        uint64_t *tmx = t3 + select_tmp_elems(nov) + 2;
-        uint8_t *wflag = s_flags.ensure(nov);
-        TRC_LAUNCH(prof, stream, "upd_win_tilemax", wtiles, WT, 0, k_win_tilemax, ws, nov, n, tmx);
-        TRC_LAUNCH(prof, stream, "upd_win_tilescan", 1, WT, 0, k_win_tilescan, tmx, wtiles);
-        TRC_LAUNCH(prof, stream, "upd_win_flag", wtiles, WT, 0, k_win_flag, ws, nov, n, tmx, wflag);
-        select_if(ByteFlagPred{wflag}, LoadU64Val{ws}, nov, mw, cnt + C_NMW, t3, stream, prof,
-                  "sel_windows");
-        nmw = read_u64(cnt + C_NMW);
-        uint32_t werr = 0;
-        TRC_CUDA(cudaMemcpyAsync(&werr, err.get(), 4, cudaMemcpyDeviceToHost, stream));
-        sync();
-        if (werr & ERR_TIMEOUT) throw_error(TRC_ERR_TIMEOUT, "radix sort look-back wait gave up");
-      }
+      // windows are selected before the root flag is read (one sync for
+      // both); a root overflow discards them and rebuilds
+      uint64_t *t2 = tmp(radix_tmp_elems(nov) + 4);
+      // window keys: start << 6 | level code, start < 2^vbits
+      int wshifts[8];
+      int nws = 0;
+      for (uint32_t sh = 0; sh < 6 + vbits(); sh += 8) wshifts[nws++] = (int)sh;
+      uint64_t *ws = radix_sort_u64_shifts(wk, wk2, nov, wshifts, nws, t2, stream, prof, err.get());
+      uint64_t *mw = s_mw.ensure(nov);
+      const uint64_t wtiles = ceil_div(nov, WT);
+      uint64_t *t3 = tmp(select_tmp_elems(nov) + wtiles + 4);
+      uint64_t *tmx = t3 + select_tmp_elems(nov) + 2;
+      uint8_t *wflag = s_flags.ensure(nov);
+      TRC_LAUNCH(prof, stream, "upd_win_tilemax", wtiles, WT, 0, k_win_tilemax, ws, nov, n, tmx);
+      TRC_LAUNCH(prof, stream, "upd_win_tilescan", 1, WT, 0, k_win_tilescan, tmx, wtiles);
+      TRC_LAUNCH(prof, stream, "upd_win_flag", wtiles, WT, 0, k_win_flag, ws, nov, n, tmx, wflag);
+      select_if(ByteFlagPred{wflag}, LoadU64Val{ws}, nov, mw, cnt + C_NMW, t3, stream, prof,
+                "sel_windows");
+      uint64_t wc[C_COUNT];
+      uint32_t werr = 0;
+      TRC_CUDA(cudaMemcpyAsync(wc, cnt, sizeof(wc), cudaMemcpyDeviceToHost, stream));
+      TRC_CUDA(cudaMemcpyAsync(&werr, err.get(), 4, cudaMemcpyDeviceToHost, stream));
+      sync();
+      if (werr & ERR_TIMEOUT) throw_error(TRC_ERR_TIMEOUT, "radix sort look-back wait gave up");
+      if (wc[C_ROOT]) rebuild = true;
+      else nmw = wc[C_NMW];
     }
   }
 
@@ -1150,8 +1164,12 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     select_if(SmallPred{stamp.get(), epoch, hub_of.get(), deg.get(), tix, tdn, T}, IndexVal32{},
               n, rs, cnt + C_NR, t4, stream, prof, "sel_rewrite");
   }
-  const uint64_t nrs = read_u64(cnt + C_NR);
+  // the rewrite list's length stays on the device (read with the final sync)
+  const uint64_t *nrs_dev = cnt + C_NR;
+  const unsigned pgrid = (unsigned)num_sms() * 8;  // persistent kernels, 64 warps per SM
+  uint64_t nrs = 0;
   uint64_t SO = 0, SN = 0;
+  if (prof.on) nrs = read_u64(cnt + C_NR);
   if (prof.on && nrs) {  // element counts for the profiler's byte accounting
     uint64_t *oo = s_oOff.ensure(nrs + 1);
     uint64_t *t5 = tmp(scan_tmp_elems(nrs) + 4);
@@ -1160,11 +1178,10 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     exclusive_scan(NewDeg{rs, deg.get(), tix, tdn}, nrs, oo, t5, stream, prof);
     SN = read_u64(oo + nrs);
   }
-  if (nrs) {
-    MergeArgs ma{rs, nrs, tix, tpos, nt, kb, bkeys, insert ? 1 : 0, pbeg_new, dst_pma, mov_pma,
+  {
+    MergeArgs ma{rs, 0, tix, tpos, nt, kb, bkeys, insert ? 1 : 0, pbeg_new, dst_pma, mov_pma,
                  nmw ? wstamp.get() : nullptr, epoch, T, dst_pma == pma.get() ? 1 : 0};
-    TRC_LAUNCH(prof, stream, "upd_merge_small", ceil_div(nrs * 32, 256), 256, 0, k_merge_small, G,
-               ma);
+    TRC_LAUNCH(prof, stream, "upd_merge_small", pgrid, 256, 0, k_merge_small, G, ma, nrs_dev);
   }
 
   phase("merge_small");
@@ -1227,10 +1244,10 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
 
   phase("hub_path");
   // ---- window moves land after every reader of the old segments is done
-  if (nmw && nrs) {
+  if (nmw) {
     DevView GC = view();
-    TRC_LAUNCH(prof, stream, "upd_window_copy", ceil_div(nrs * 32, 256), 256, 0, k_window_copy, GC,
-               rs, nrs, mov_pma, pbeg_new, wstamp.get(), epoch);
+    TRC_LAUNCH(prof, stream, "upd_window_copy", pgrid, 256, 0, k_window_copy, GC, rs, nrs_dev,
+               mov_pma, pbeg_new, wstamp.get(), epoch);
   }
   TRC_LAUNCH(prof, stream, "upd_c2", ceil_div(nt, 256), 256, 0, k_scatter_c2_final, tu, tc2, nt,
              c2.get());
@@ -1240,6 +1257,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     s_pma_next.reset();
     N = Nn;
   }
+  TRC_CUDA(cudaMemcpyAsync(&nrs, nrs_dev, 8, cudaMemcpyDeviceToHost, stream));
   sync();  // host vectors (plan, rh) outlive their copies
   phase("finish");
   const uint64_t nr = nrs + nh;
