@@ -294,6 +294,10 @@ trc_status trc_server_release(trc_server *s, uint64_t id);
 /* kind < 0: every request; otherwise one trc_request_kind. */
 trc_status trc_server_get_stats(trc_server *s, int kind, trc_server_stats *out);
 trc_status trc_server_reset_stats(trc_server *s);
+/* hold != 0: start no new round (requests queue up); hold = 0: the next round
+ * takes every pending request, subject to the admission limits.  Lets a
+ * caller gather a burst into one round.  Destroy drains a held server. */
+trc_status trc_server_hold(trc_server *s, int hold);
 
 /* ---- diagnostics (no reference counterpart: the reference has only
  *      lock-ownership checks, src/PMA.cc:29-111). */

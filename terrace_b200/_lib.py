@@ -149,6 +149,7 @@ SIGNATURES = [
     ("trc_server_release", _int, [_vp, _u64]),
     ("trc_server_get_stats", _int, [_vp, _int, C.POINTER(trc_server_stats)]),
     ("trc_server_reset_stats", _int, [_vp]),
+    ("trc_server_hold", _int, [_vp, _int]),
 ]
 
 _lib = None

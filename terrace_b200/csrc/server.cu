@@ -211,6 +211,15 @@ class Server {
     return r->id;
   }
 
+  // While held, the worker starts no new round and requests queue up; on
+  // release the next round takes every pending request (subject to the
+  // admission limits).  Destroying a held server still drains it.
+  void hold(bool on) {
+    std::lock_guard<std::mutex> lk(mu_);
+    hold_ = on;
+    cv_.notify_all();
+  }
+
   trc_status wait(uint64_t id, int64_t timeout_ms) {
     std::unique_lock<std::mutex> lk(mu_);
     auto it = all_.find(id);
@@ -312,6 +321,7 @@ class Server {
   std::unordered_map<uint64_t, Request *> all_;
   uint64_t next_id_ = 1;
   bool stop_ = false;
+  bool hold_ = false;
   std::vector<std::pair<int, double>> lat_;
   double t0_ = 0, last_done_ = 0;
   std::atomic<uint64_t> rounds_{0}, calls_{0}, rejected_{0}, version_{0};
@@ -417,7 +427,7 @@ class Server {
       std::vector<Request *> round;
       {
         std::unique_lock<std::mutex> lk(mu_);
-        cv_.wait(lk, [&] { return stop_ || !pending_.empty(); });
+        cv_.wait(lk, [&] { return stop_ || (!hold_ && !pending_.empty()); });
         if (pending_.empty() && stop_) break;
         if (cfg_.mode == TRC_SERVE_FIFO) {
           round.push_back(pending_.front());
@@ -732,10 +742,12 @@ class Server {
   // decides), applied as one delete batch then one insert batch.
   void apply_net(std::vector<Request *> &u) {
     const uint32_t vb = g_.vbits();
-    const uint32_t tagbits = 64 - 2 * vb;
-    // arrival rank must fit the tag (1 bit for the op); otherwise apply the
-    // updates one by one
-    if (tagbits < 2 || u.size() >= (1ull << (tagbits - 1))) {
+    // key = (src, dst, arrival rank, op), the tag directly below the edge so
+    // that the sorted bits are contiguous: ceil((2 vb + tagbits) / 8) <= 8
+    // radix digits.  If the tag does not fit, apply the updates one by one.
+    uint32_t tagbits = 1;  // bits of (rank << 1 | op)
+    while ((1ull << tagbits) < ((uint64_t)u.size() << 1)) tagbits++;
+    if (2 * vb + tagbits > 64) {
       for (Request *r : u) apply_one(r);
       return;
     }
@@ -778,13 +790,10 @@ class Server {
     TRC_CUDA(cudaStreamSynchronize(s));
     if (herr) throw_error(TRC_ERR_INVALID, "vertex id out of range in an update");
     g_.phase("srv_tag");
-    // sort by (edge, arrival rank): every bit below the top spare bits
-    uint32_t rb = 1;  // bits of (rank << 1 | op)
-    while ((1ull << rb) < ((uint64_t)R << 1)) rb++;
+    // sort by (edge, arrival rank): the 2 vb + tagbits low bits
     int shifts[16];
     int ns = 0;
-    for (uint32_t sh = 0; sh < rb; sh += 8) shifts[ns++] = (int)sh;
-    for (uint32_t sh = tagbits; sh < 64; sh += 8) shifts[ns++] = (int)sh;
+    for (uint32_t sh = 0; sh < 2 * vb + tagbits; sh += 8) shifts[ns++] = (int)sh;
     uint64_t *t = g_.s_tmp.ensure(radix_tmp_elems(total) + 2 * select_tmp_elems(total) + 8);
     uint64_t *sorted = radix_sort_u64_shifts(K, K2, total, shifts, ns, t, s, g_.prof, err);
     uint64_t *cnt = g_.s_cnt.get() + 30;
@@ -914,6 +923,10 @@ trc_status trc_server_get_stats(trc_server *s, int kind, trc_server_stats *out) 
 
 trc_status trc_server_reset_stats(trc_server *s) {
   return sguard([&] { S(s).reset_stats(); });
+}
+
+trc_status trc_server_hold(trc_server *s, int hold) {
+  return sguard([&] { S(s).hold(hold != 0); });
 }
 
 }  // extern "C"

@@ -100,3 +100,8 @@ class Server:
 
     def reset_stats(self):
         L.check(self._L.trc_server_reset_stats(self._h))
+
+    def hold(self, on: bool = True):
+        """While held no new round starts; release (hold(False)) to serve
+        everything queued meanwhile as one round."""
+        L.check(self._L.trc_server_hold(self._h, 1 if on else 0))

@@ -174,3 +174,45 @@ def test_server_admission_and_errors():
     srv.close()
     assert g.get_num_edges() == m0
     assert np.array_equal(deg, g.degree(np.arange(16, dtype=np.uint32)))
+
+
+def test_large_round_wide_vertex_ids():
+    """A round of 300 update requests on a graph with 25-bit vertex ids: the
+    round's tagged sort key (src, dst, arrival rank, op) needs all of its
+    bits; the net change must equal the requests applied one by one."""
+    _gpu()
+    import terrace_b200 as T
+    n = 1 << 25
+    g = T.Graph(n)
+    rng = np.random.default_rng(7)
+    srv = T.Server(g, batched=True)
+    srv.hold(True)
+    reqs, ids = [], []
+    for i in range(300):
+        k = int(rng.integers(1, 40))
+        # overlapping endpoints across requests (low ids), plus high ids
+        a = rng.integers(0, 4096, k, dtype=np.uint32)
+        b = np.where(rng.random(k) < .5, rng.integers(0, 4096, k), rng.integers(n - 4096, n, k))
+        b = b.astype(np.uint32)
+        op = "ins" if (i < 20 or rng.random() < .6) else "del"
+        reqs.append((op, a, b))
+        ids.append(srv.insert(a, b) if op == "ins" else srv.delete(a, b))
+    srv.hold(False)
+    for rid in ids:
+        srv.wait(rid, 120000)
+        _, _, ver, st = srv.result(rid)
+        assert st == 0
+        assert ver == 1  # one round, one net change
+        srv.release(rid)
+    assert srv.stats()["rounds"] == 1
+    srv.close()
+    keys = np.zeros(0, np.uint64)
+    for op, a, b in reqs:
+        kk = O.make_keys(a, b, True, True)
+        keys = O.key_union(keys, kk) if op == "ins" else O.key_difference(keys, kk)
+    assert g.get_num_edges() == len(keys)
+    us = np.unique((keys >> np.uint64(32)).astype(np.uint32))
+    for u in us[:: max(1, len(us) // 200)]:
+        want = (keys[(keys >> np.uint64(32)) == u] & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+        assert np.array_equal(g.neighbors(int(u)), want), u
+    g.close()
