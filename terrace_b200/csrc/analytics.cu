@@ -539,53 +539,92 @@ __global__ void k_set_bits(const uint32_t *F, uint32_t nf, uint32_t *bits) {
   if (i < nf) atomicOr(bits + (F[i] >> 5), 1u << (F[i] & 31));
 }
 
+// Inline pass of a dense step: 4 lanes per vertex (one 128-bit quarter of
+// the 64-byte row each), BP_V vertices per quad.  A quad's vertices are
+// list entries q0 + i * 8 (i < BP_V; the 8 quads of a warp take consecutive
+// entries), and every load of a step is issued for all of them before any
+// is used: list entries, then degree and level, then the row quarters, then
+// the 4 * BP_V frontier-bitmap words.  The first frontier neighbour in
+// sorted order wins (lowest lane of the quad with a hit, then its lowest
+// element).
+constexpr uint32_t BP_V = 4;
+
 __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S, uint64_t nS,
                                                    BFSState s) {
-  uint64_t gt = (uint64_t)blockIdx.x * AT + threadIdx.x;
-  uint64_t vi = gt >> 2;
-  uint32_t q = gt & 3, lane = threadIdx.x & 31;
-  uint32_t u = 0, first = 4;
-  uint4 v = make_uint4(0, 0, 0, 0);
-  if (vi < nS) {
-    u = S[vi];
-    uint32_t d = G.deg[u];
-    if (s.lv[u] == TRC_UNREACHED && q * 4 < d) {
-      v = __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE) + q);
-      if (bit_test(s.bits, v.x)) first = 0;
-      else if (q * 4 + 1 < d && bit_test(s.bits, v.y)) first = 1;
-      else if (q * 4 + 2 < d && bit_test(s.bits, v.z)) first = 2;
-      else if (q * 4 + 3 < d && bit_test(s.bits, v.w)) first = 3;
+  const uint32_t lane = threadIdx.x & 31, q = lane & 3, qw = lane >> 2;
+  const uint64_t wbase = (((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5) * (8 * BP_V);
+  uint32_t u[BP_V], d[BP_V];
+  bool act[BP_V];
+#pragma unroll
+  for (uint32_t i = 0; i < BP_V; i++) {
+    const uint64_t vi = wbase + i * 8 + qw;
+    u[i] = vi < nS ? S[vi] : 0u;
+    act[i] = vi < nS;
+  }
+#pragma unroll
+  for (uint32_t i = 0; i < BP_V; i++) {
+    d[i] = act[i] ? G.deg[u[i]] : 0u;
+    act[i] = act[i] && s.lv[u[i]] == TRC_UNREACHED && q * 4 < d[i];
+  }
+  uint4 v[BP_V];
+#pragma unroll
+  for (uint32_t i = 0; i < BP_V; i++)
+    v[i] = act[i] ? __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u[i] * K_INLINE) + q)
+                  : make_uint4(0, 0, 0, 0);
+  uint32_t wx[BP_V], wy[BP_V], wz[BP_V], ww[BP_V];
+#pragma unroll
+  for (uint32_t i = 0; i < BP_V; i++) {
+    const uint32_t e = q * 4;
+    wx[i] = act[i] ? __ldg(s.bits + (v[i].x >> 5)) : 0u;
+    wy[i] = act[i] && e + 1 < d[i] ? __ldg(s.bits + (v[i].y >> 5)) : 0u;
+    wz[i] = act[i] && e + 2 < d[i] ? __ldg(s.bits + (v[i].z >> 5)) : 0u;
+    ww[i] = act[i] && e + 3 < d[i] ? __ldg(s.bits + (v[i].w >> 5)) : 0u;
+  }
+#pragma unroll
+  for (uint32_t i = 0; i < BP_V; i++) {
+    uint32_t first = 4;
+    if ((wx[i] >> (v[i].x & 31)) & 1u) first = 0;
+    else if ((wy[i] >> (v[i].y & 31)) & 1u) first = 1;
+    else if ((wz[i] >> (v[i].z & 31)) & 1u) first = 2;
+    else if ((ww[i] >> (v[i].w & 31)) & 1u) first = 3;
+    uint32_t m = __ballot_sync(0xFFFFFFFFu, first < 4);
+    uint32_t grp = (m >> (lane & ~3u)) & 0xFu;
+    bool win = grp && (__ffs(grp) - 1) == (int)q;
+    if (win) {
+      uint32_t p = first == 0 ? v[i].x : first == 1 ? v[i].y : first == 2 ? v[i].z : v[i].w;
+      s.par[u[i]] = (int32_t)p;
+      s.lv[u[i]] = s.d + 1;
     }
+    uint32_t pos = warp_append(win, s.next_cnt);
+    if (win) s.next[pos] = u[i];
   }
-  uint32_t m = __ballot_sync(0xFFFFFFFFu, first < 4);
-  uint32_t grp = (m >> (lane & ~3u)) & 0xFu;
-  bool win = grp && (__ffs(grp) - 1) == (int)q;
-  if (win) {
-    uint32_t p = first == 0 ? v.x : first == 1 ? v.y : first == 2 ? v.z : v.w;
-    s.par[u] = (int32_t)p;
-    s.lv[u] = s.d + 1;
-  }
-  uint32_t pos = warp_append(win, s.next_cnt);
-  if (win) s.next[pos] = u;
 }
 
-// One warp scans the neighbours of vertex u in sorted order from rank j_first
-// and stops at the first frontier member.  Returns that neighbour or NONE32
-// (warp-uniform).
-__device__ __forceinline__ uint32_t warp_first_in_frontier(const NbrList &L, const uint32_t *bits,
-                                                           uint32_t j_first) {
-  uint32_t lane = threadIdx.x & 31;
-  for (uint32_t j0 = j_first; j0 < L.deg; j0 += 32) {
-    uint32_t j = j0 + lane;
-    uint32_t v = j < L.deg ? L.at(j) : 0;
-    bool hit = j < L.deg && bit_test(bits, v);
-    uint32_t m = __ballot_sync(0xFFFFFFFFu, hit);
-    if (m) return __shfl_sync(0xFFFFFFFFu, v, __ffs(m) - 1);
+// One warp scans the neighbours of vertex u of rank >= j_first for a
+// frontier member, 64 per step from the largest id down (two independent
+// loads per lane), and returns the smallest frontier neighbour of the first
+// step that has one, or NONE32 (warp-uniform).  Any frontier neighbour is a
+// valid parent (the levels do not depend on the choice); scanning from the
+// top finds one sooner on graphs whose high-degree vertices have large ids
+// (RMAT with its d quadrant heaviest).
+__device__ __forceinline__ uint32_t warp_any_in_frontier(const NbrList &L, const uint32_t *bits,
+                                                         uint32_t j_first) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t e = L.deg; e > j_first;) {
+    const uint32_t s0 = e - j_first > 64 ? e - 64 : j_first;
+    const uint32_t ja = s0 + lane, jb = s0 + 32 + lane;
+    const bool va = ja < e, vb = jb < e;
+    const uint32_t xa = va ? L.at(ja) : 0u, xb = vb ? L.at(jb) : 0u;
+    const bool ha = va && bit_test(bits, xa), hb = vb && bit_test(bits, xb);
+    const uint32_t ma = __ballot_sync(0xFFFFFFFFu, ha), mb = __ballot_sync(0xFFFFFFFFu, hb);
+    if (ma) return __shfl_sync(0xFFFFFFFFu, xa, __ffs(ma) - 1);
+    if (mb) return __shfl_sync(0xFFFFFFFFu, xb, __ffs(mb) - 1);
+    e = s0;
   }
   return NONE32;
 }
 
-// Warp per vertex of a list (M or H class), scanning from rank j_first (the
+// Warp per vertex of a list (M or H class), scanning ranks >= j_first (the
 // inline pass has already checked ranks below it for M vertices).
 __global__ void __launch_bounds__(AT) k_bfs_pull_W(DevView G, const uint32_t *Lst, uint64_t nL,
                                                    BFSState s, uint32_t j_first) {
@@ -596,7 +635,7 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_W(DevView G, const uint32_t *Ls
   bool win = false;
   if (s.lv[u] == TRC_UNREACHED) {
     NbrList L = nbr_list(G, u);
-    uint32_t p = warp_first_in_frontier(L, s.bits, j_first);
+    uint32_t p = warp_any_in_frontier(L, s.bits, j_first);
     if (p != NONE32 && lane == 0) {
       s.par[u] = (int32_t)p;
       s.lv[u] = s.d + 1;
@@ -651,8 +690,8 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
       TRC_CUDA(cudaMemsetAsync(bm, 0, words * 4, stream));
       TRC_LAUNCH(prof, stream, "bfs_bits", ceil_div(nf, AT), AT, 0, k_set_bits, F, nf, bm);
       // pass A: the 16 inline neighbours of every unvisited non-hub vertex
-      TRC_LAUNCH(prof, stream, "bfs_pull_inline", ceil_div(ncand * 4, AT), AT, 0, k_bfs_pull_S,
-                 G, cand, ncand, s);
+      TRC_LAUNCH(prof, stream, "bfs_pull_inline", ceil_div(ncand * 4, (uint64_t)AT * BP_V), AT, 0,
+                 k_bfs_pull_S, G, cand, ncand, s);
       // pass B: the PMA segments of those still unvisited (compacted); hubs
       // from rank 0
       uint32_t *pb = segb.ensure(ncand ? ncand : 1);

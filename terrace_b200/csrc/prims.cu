@@ -157,9 +157,10 @@ __global__ void __launch_bounds__(RS_T) k_os_scatter(const uint64_t *in, uint64_
 
 uint64_t radix_tmp_elems(uint64_t n) {
   uint64_t tiles = ceil_div(n, RS_TILE);
-  // histograms + digit starts (OS_MAXD x 256 each), status (tiles x 256),
-  // tile counters (one word per digit position)
-  return 2 * OS_MAXD * 256 + tiles * 256 + OS_MAXD + 2;
+  // histograms + digit starts (OS_MAXD x 256 each), status (tiles x 256 per
+  // digit position, cleared once per sort), tile counters (one word per
+  // digit position)
+  return 2 * OS_MAXD * 256 + (uint64_t)OS_MAXD * tiles * 256 + OS_MAXD + 2;
 }
 
 uint64_t *radix_sort_u64(uint64_t *keys, uint64_t *alt, uint64_t n, uint32_t vbits,
@@ -182,20 +183,20 @@ uint64_t *radix_sort_u64_shifts(uint64_t *keys, uint64_t *alt, uint64_t n, const
   unsigned long long *ghist = (unsigned long long *)tmp;
   uint64_t *goff = tmp + OS_MAXD * 256;
   uint64_t *status = goff + OS_MAXD * 256;
-  uint32_t *ctr = (uint32_t *)(status + ntiles * 256);
+  uint32_t *ctr = (uint32_t *)(status + (uint64_t)ns * ntiles * 256);
   OsShifts sh;
   sh.n = ns;
   for (int i = 0; i < OS_MAXD; i++) sh.s[i] = i < ns ? shifts[i] : 0;
   TRC_CUDA(cudaMemsetAsync(ghist, 0, (size_t)OS_MAXD * 256 * 8, s));
   TRC_CUDA(cudaMemsetAsync(ctr, 0, (size_t)OS_MAXD * 4, s));
+  TRC_CUDA(cudaMemsetAsync(status, 0, (size_t)ns * ntiles * 256 * 8, s));
   const unsigned hgrid = (unsigned)std::min<uint64_t>(ceil_div(n, RS_T * 8), (uint64_t)num_sms() * 8);
   TRC_LAUNCH(prof, s, "radix_hist", hgrid, RS_T, 0, k_os_hist, keys, n, sh, ghist);
   TRC_LAUNCH(prof, s, "radix_prefix", 1, RS_T, 0, k_os_prefix, ghist, ns, goff);
   uint64_t *cur = keys, *nxt = alt;
   for (int i = 0; i < ns; i++) {
-    TRC_CUDA(cudaMemsetAsync(status, 0, ntiles * 256 * 8, s));
     TRC_LAUNCH(prof, s, "radix_scatter", ntiles, RS_T, 0, k_os_scatter, cur, nxt, n, shifts[i],
-               goff + i * 256, status, ctr + i, err);
+               goff + i * 256, status + (uint64_t)i * ntiles * 256, ctr + i, err);
     uint64_t *t = cur;
     cur = nxt;
     nxt = t;
