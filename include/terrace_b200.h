@@ -149,6 +149,13 @@ trc_status trc_pagerank(trc_graph *g, uint32_t iters, double damping,
 trc_status trc_cc(trc_graph *g, uint32_t *labels, uint32_t flags);
 /* Dependencies as the reference returns them; NaN for unreached vertices. */
 trc_status trc_bc(trc_graph *g, uint32_t src, double *dep, uint32_t flags);
+/* Multi-source BC: k <= 64 sources in one traversal (one bit per source in a
+ * 64-bit mask per vertex; the reference runs BC once per source,
+ * include/BC.h:99-157).  dep[i*n + v] = trc_bc(sources[i])'s value for v
+ * (FP64 sums in the reference's neighbour order; NaN where unreached).
+ * Device memory: 16 * k * n bytes for path counts and dependencies. */
+trc_status trc_msbc(trc_graph *g, const uint32_t *sources, uint32_t k, double *dep,
+                    uint32_t flags);
 trc_status trc_tc(trc_graph *g, uint64_t *count);
 
 /* ---- BFS without device allocation.  No counterpart in the reference.

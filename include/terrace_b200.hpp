@@ -188,6 +188,16 @@ inline double *BC(Graph &G, const uint32_t &start) {
   return d;
 }
 
+// BC of up to 64 sources in one traversal: row i (n doubles) = BC(G, starts[i]).
+inline double *BC_multi(Graph &G, const uint32_t *starts, uint32_t k) {
+  double *d = (double *)malloc(sizeof(double) * (size_t)k * G.get_num_vertices());
+  if (!d) throw std::bad_alloc();
+  trc_status s = trc_msbc(G.handle(), starts, k, d, 0);
+  if (s != TRC_OK) free(d);
+  check(s);
+  return d;
+}
+
 // TC (include/TC.h:73-87): exact triangle count.
 inline uint64_t TC(Graph &G) {
   uint64_t c = 0;

@@ -123,6 +123,7 @@ SIGNATURES = [
     ("trc_bfs", _int, [_vp, _u32, _vp, _vp, _u32]),
     ("trc_bfs_noalloc", _int, [_vp, _u32, _vp, _vp, _u32]),
     ("trc_msbfs", _int, [_vp, _vp, _u32, _vp, _u32]),
+    ("trc_msbc", _int, [_vp, _vp, _u32, _vp, _u32]),
     ("trc_pagerank", _int, [_vp, _u32, _dbl, _vp, _u32]),
     ("trc_cc", _int, [_vp, _vp, _u32]),
     ("trc_bc", _int, [_vp, _u32, _vp, _u32]),

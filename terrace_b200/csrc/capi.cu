@@ -248,6 +248,11 @@ trc_status trc_msbfs(trc_graph *g, const uint32_t *sources, uint32_t k, uint32_t
   return guard([&] { G(g).msbfs(sources, k, levels, flags); });
 }
 
+trc_status trc_msbc(trc_graph *g, const uint32_t *sources, uint32_t k, double *dep,
+                    uint32_t flags) {
+  return guard([&] { G(g).msbc(sources, k, dep, flags); });
+}
+
 trc_status trc_bfs_noalloc(trc_graph *g, uint32_t src, int32_t *parents, uint32_t *levels,
                            uint32_t flags) {
   return guard([&] { G(g).bfs_noalloc(src, parents, levels, flags); });

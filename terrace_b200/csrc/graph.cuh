@@ -106,6 +106,8 @@ class Graph {
   void msbfs_summary(const uint32_t *sources, uint32_t k, uint64_t *reached, uint32_t *ecc);
   void msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uint32_t flags,
                  uint64_t *reached, uint32_t *ecc);
+  // up to 64 BC at once, out[i*n + v] (msbfs.cu)
+  void msbc(const uint32_t *sources, uint32_t k, double *out, uint32_t flags);
   // BFS with scratch in a static device array (no allocation), noalloc.cu
   void bfs_noalloc(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags);
   int device = 0;  // device the graph was created on

@@ -254,6 +254,128 @@ __global__ void k_ms_transpose(const uint32_t *lvrow, uint32_t n, uint32_t k, ui
     if (v < n && i < k) out[(uint64_t)i * n + v] = t[threadIdx.x][r];
   }
 }
+
+// ---------------------------------------------------------------------------
+// Multi-source BC (Brandes per source, as the reference's BC, include/BC.h:
+// 99-157, for up to 64 sources at once).  The forward levels come from the
+// multi-source BFS above; per level L+1 the vertices discovered (active list,
+// new-source mask next[v]) get, for each new source s,
+//   sigma[v][s] = sum of sigma[u][s] over neighbours u with s in front[u]
+// (front = level-L masks).  Each level's (vertex, mask) pairs are kept in
+// compact form; the backward pass walks them from the deepest level:
+//   dep[v][s] = sum of dep[w][s] over neighbours w at level L+1 for s,
+//               plus 1/sigma[v][s];
+// and the result is (dep - 1/sigma) / (1/sigma) (NaN where s does not reach
+// v), source-major.  sigma and dep are vertex-major (k doubles per vertex);
+// lane l of a warp owns sources l and l + 32, neighbours are visited in
+// sorted order, so every sum runs in the reference's order.
+
+__device__ __forceinline__ uint64_t shfl64(uint64_t x, int src) {
+  uint32_t lo = __shfl_sync(0xFFFFFFFFu, (uint32_t)x, src);
+  uint32_t hi = __shfl_sync(0xFFFFFFFFu, (uint32_t)(x >> 32), src);
+  return ((uint64_t)hi << 32) | lo;
+}
+
+// Sums val[u][s] over the neighbours u of v with s in (mask[u] & want), for
+// lane l's sources l and l + 32 (warp-uniform v).
+__device__ __forceinline__ void mbc_gather(const DevView &G, uint32_t v, uint64_t want,
+                                           const uint64_t *mask, const double *val, uint32_t k,
+                                           uint32_t lane, double &a0, double &a1) {
+  NbrList L = nbr_list(G, v);
+  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) {
+    const uint32_t j = j0 + lane;
+    const uint32_t u = j < L.deg ? L.at(j) : 0u;
+    const uint64_t mu = j < L.deg ? (mask[u] & want) : 0ull;
+    uint32_t ball = __ballot_sync(0xFFFFFFFFu, mu != 0);
+    while (ball) {
+      const int b = __ffs(ball) - 1;
+      ball &= ball - 1;
+      const uint32_t uu = __shfl_sync(0xFFFFFFFFu, u, b);
+      const uint64_t mm = shfl64(mu, b);
+      const double *row = val + (uint64_t)uu * k;
+      if (lane < k && ((mm >> lane) & 1)) a0 += row[lane];
+      if (lane + 32 < k && ((mm >> (lane + 32)) & 1)) a1 += row[lane + 32];
+    }
+  }
+}
+
+// sigma of the vertices discovered this level (grid-stride over the device
+// count of the active list)
+__global__ void k_mbc_sigma(DevView G, const uint32_t *A, const uint32_t *cnt, const uint64_t *front,
+                            const uint64_t *next, double *sigma, uint32_t k) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t na = *cnt;
+  const uint64_t stride = ((uint64_t)gridDim.x * MT) >> 5;
+  for (uint64_t w = ((uint64_t)blockIdx.x * MT + threadIdx.x) >> 5; w < na; w += stride) {
+    const uint32_t v = A[w];
+    const uint64_t nm = next[v];
+    double a0 = 0.0, a1 = 0.0;
+    mbc_gather(G, v, nm, front, sigma, k, lane, a0, a1);
+    double *row = sigma + (uint64_t)v * k;
+    if (lane < k && ((nm >> lane) & 1)) row[lane] = a0;
+    if (lane + 32 < k && ((nm >> (lane + 32)) & 1)) row[lane + 32] = a1;
+  }
+}
+
+// compact copy of a level: ord[i] = A[i], om[i] = mask[A[i]]
+__global__ void k_mbc_store(const uint32_t *A, const uint32_t *cnt, const uint64_t *mask,
+                            uint32_t *ord, uint64_t *om) {
+  const uint32_t na = *cnt;
+  const uint64_t stride = (uint64_t)gridDim.x * MT;
+  for (uint64_t i = (uint64_t)blockIdx.x * MT + threadIdx.x; i < na; i += stride) {
+    const uint32_t v = A[i];
+    ord[i] = v;
+    om[i] = mask[v];
+  }
+}
+
+__global__ void k_mbc_scatter(const uint32_t *ord, const uint64_t *om, uint32_t cnt,
+                              uint64_t *dense) {
+  const uint64_t i = (uint64_t)blockIdx.x * MT + threadIdx.x;
+  if (i < cnt) dense[ord[i]] = om[i];
+}
+
+__global__ void k_mbc_back(DevView G, const uint32_t *ord, const uint64_t *om, uint32_t cnt,
+                           const uint64_t *fnext, const double *sigma, double *dep, uint32_t k) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t w = ((uint64_t)blockIdx.x * MT + threadIdx.x) >> 5;
+  if (w >= cnt) return;
+  const uint32_t v = ord[w];
+  const uint64_t fm = om[w];
+  double a0 = 0.0, a1 = 0.0;
+  mbc_gather(G, v, fm, fnext, dep, k, lane, a0, a1);
+  const double *sg = sigma + (uint64_t)v * k;
+  double *row = dep + (uint64_t)v * k;
+  if (lane < k && ((fm >> lane) & 1)) row[lane] = a0 + 1.0 / sg[lane];
+  if (lane + 32 < k && ((fm >> (lane + 32)) & 1)) row[lane + 32] = a1 + 1.0 / sg[lane + 32];
+}
+
+__global__ void k_mbc_seed(const uint32_t *src, uint32_t k, double *sigma) {
+  const uint32_t i = threadIdx.x;
+  if (i < k) sigma[(uint64_t)src[i] * k + i] = 1.0;
+}
+
+// out[s * n + v] = (dep - 1/sigma) / (1/sigma), through 32 x 32 tiles
+__global__ void k_mbc_final(const double *dep, const double *sigma, uint32_t n, uint32_t k,
+                            double *out) {
+  __shared__ double t[32][33];
+  const uint64_t v0 = (uint64_t)blockIdx.x * 32;
+  const uint32_t i0 = blockIdx.y * 32;
+  for (uint32_t r = threadIdx.y; r < 32; r += blockDim.y) {
+    const uint64_t v = v0 + r;
+    const uint32_t i = i0 + threadIdx.x;
+    if (v < n && i < k) {
+      const double inv = 1.0 / sigma[v * k + i];
+      t[r][threadIdx.x] = (dep[v * k + i] - inv) / inv;
+    }
+  }
+  __syncthreads();
+  for (uint32_t r = threadIdx.y; r < 32; r += blockDim.y) {
+    const uint32_t i = i0 + r;
+    const uint64_t v = v0 + threadIdx.x;
+    if (v < n && i < k) out[(uint64_t)i * n + v] = t[threadIdx.x][r];
+  }
+}
 }  // namespace
 
 void Graph::msbfs(const uint32_t *sources, uint32_t k, uint32_t *levels, uint32_t flags) {
@@ -380,6 +502,166 @@ void Graph::msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uin
   prof.launches++;
   TRC_CUDA(cudaGetLastError());
   if (!dev) TRC_CUDA(cudaMemcpyAsync(levels, out, (uint64_t)n * k * 4, cudaMemcpyDeviceToHost, stream));
+  sync();
+}
+
+
+// Compact per-level storage that grows by copying (device order preserved).
+struct LevelStore {
+  DBuf<uint32_t> ord[2];
+  DBuf<uint64_t> om[2];
+  int cur = 0;
+  uint64_t cap = 0;
+  void bind(Budget *b) {
+    for (int i = 0; i < 2; i++) {
+      ord[i].bind(b);
+      om[i].bind(b);
+    }
+  }
+  // room for `need` entries, keeping the first `used`
+  void reserve(uint64_t need, uint64_t used, cudaStream_t s) {
+    if (need <= cap) return;
+    uint64_t nc = std::max<uint64_t>(need, cap * 2);
+    int o = cur ^ 1;
+    ord[o].alloc_exact(nc);
+    om[o].alloc_exact(nc);
+    if (used) {
+      TRC_CUDA(cudaMemcpyAsync(ord[o].get(), ord[cur].get(), used * 4, cudaMemcpyDeviceToDevice, s));
+      TRC_CUDA(cudaMemcpyAsync(om[o].get(), om[cur].get(), used * 8, cudaMemcpyDeviceToDevice, s));
+    }
+    ord[cur].reset();
+    om[cur].reset();
+    cur = o;
+    cap = nc;
+  }
+  uint32_t *o32() { return ord[cur].get(); }
+  uint64_t *o64() { return om[cur].get(); }
+};
+
+void Graph::msbc(const uint32_t *sources, uint32_t k, double *out_user, uint32_t flags) {
+  if (k == 0) return;
+  if (k > 64) throw_error(TRC_ERR_INVALID, "at most 64 sources per multi-source BC");
+  if (!sources || !out_user) throw_error(TRC_ERR_INVALID, "null pointer");
+  std::vector<uint32_t> hsrc(k);
+  if (flags & TRC_DEVICE_PTR) {
+    TRC_CUDA(cudaMemcpyAsync(hsrc.data(), sources, k * 4, cudaMemcpyDeviceToHost, stream));
+    sync();
+  } else {
+    std::copy(sources, sources + k, hsrc.begin());
+  }
+  for (uint32_t x : hsrc)
+    if (x >= n) throw_error(TRC_ERR_INVALID, "source vertex out of range");
+  ensure_lists();
+  DBuf<uint64_t> seenb, fa, fb, accb;
+  DBuf<uint32_t> srcb, lst, lst2, tl, cnt;
+  DBuf<double> sigb, depb, outb;
+  for (auto *b : {&seenb, &fa, &fb, &accb}) b->bind(&budget);
+  for (auto *b : {&srcb, &lst, &lst2, &tl, &cnt}) b->bind(&budget);
+  for (auto *b : {&sigb, &depb, &outb}) b->bind(&budget);
+  uint64_t *seen = seenb.alloc_exact(n), *front = fa.alloc_exact(n), *next = fb.alloc_exact(n);
+  unsigned long long *acc = (unsigned long long *)accb.alloc_exact(n);
+  double *sigma = sigb.alloc_exact((uint64_t)n * k), *dep = depb.alloc_exact((uint64_t)n * k);
+  uint32_t *dsrc = srcb.alloc_exact(k);
+  uint32_t *L[2] = {lst.alloc_exact(n), lst2.alloc_exact(n)};
+  uint32_t *T = tl.alloc_exact(n);
+  uint32_t *c = cnt.alloc_exact(4);  // [0] pull commits, [1] next active, [2] touched
+  DBuf<uint64_t> anyb;
+  anyb.bind(&budget);
+  unsigned long long *any = (unsigned long long *)anyb.alloc_exact(1);
+  LevelStore lv;
+  lv.bind(&budget);
+  TRC_CUDA(cudaMemcpyAsync(dsrc, hsrc.data(), k * 4, cudaMemcpyHostToDevice, stream));
+  TRC_CUDA(cudaMemsetAsync(sigma, 0, (uint64_t)n * k * 8, stream));
+  TRC_CUDA(cudaMemsetAsync(dep, 0, (uint64_t)n * k * 8, stream));
+  TRC_LAUNCH(prof, stream, "ms_init", ceil_div(n, MT), MT, 0, k_ms_init, n, k, dsrc, seen, front,
+             next, (uint32_t *)nullptr, acc);
+  TRC_LAUNCH(prof, stream, "mbc_seed", 1, 64, 0, k_mbc_seed, dsrc, k, sigma);
+  std::vector<uint32_t> act(hsrc);
+  std::sort(act.begin(), act.end());
+  act.erase(std::unique(act.begin(), act.end()), act.end());
+  int cur = 0;
+  uint32_t nact = (uint32_t)act.size();
+  TRC_CUDA(cudaMemcpyAsync(L[cur], act.data(), nact * 4, cudaMemcpyHostToDevice, stream));
+  // level 0 in compact form
+  std::vector<uint64_t> loff = {0};
+  lv.reserve(std::max<uint64_t>(2 * (uint64_t)n, 1024), 0, stream);
+  TRC_CUDA(cudaMemcpyAsync(c + 1, &nact, 4, cudaMemcpyHostToDevice, stream));
+  TRC_LAUNCH(prof, stream, "mbc_store", ceil_div(nact, MT), MT, 0, k_mbc_store, L[cur], c + 1,
+             front, lv.o32(), lv.o64());
+  loff.push_back(nact);
+  uint64_t live = k == 64 ? ~0ull : ((1ull << k) - 1);
+  const uint64_t dense_at = n / push_pull_divisor();
+  const unsigned pgrid = (unsigned)std::max(1, num_sms() * 8);
+  DevView G = view();
+  uint32_t level = 0;
+  while (nact > 0) {
+    level++;
+    TRC_CUDA(cudaMemsetAsync(c, 0, 16, stream));
+    TRC_CUDA(cudaMemsetAsync(any, 0, 8, stream));
+    MSState s{seen, front, next, nullptr, k, live, level, c};
+    uint32_t *nl = L[cur ^ 1];
+    const uint64_t base = loff.back();
+    lv.reserve(base + n, base, stream);
+    if ((uint64_t)nact >= dense_at && dense_at > 0) {
+      TRC_LAUNCH(prof, stream, "ms_pull_S", ceil_div(lists.nS * 4, MT), MT, 0, k_ms_pull_S, G,
+                 lists.S.get(), lists.nS, s);
+      TRC_LAUNCH(prof, stream, "ms_pull_M", ceil_div(lists.nM * 32, MT), MT, 0, k_ms_pull_W, G,
+                 lists.M.get(), lists.nM, s);
+      TRC_LAUNCH(prof, stream, "ms_pull_H", ceil_div(lists.nH * 32, MT), MT, 0, k_ms_pull_W, G,
+                 lists.Hv.get(), lists.nH, s);
+      TRC_LAUNCH(prof, stream, "ms_collect", ceil_div(n, MT), MT, 0, k_ms_collect, n, next, nl,
+                 c + 1, any);
+    } else {
+      TRC_LAUNCH(prof, stream, "ms_push", ceil_div((uint64_t)nact * 32, MT), MT, 0, k_ms_push, G,
+                 L[cur], nact, front, seen, acc, T, c + 2);
+      TRC_LAUNCH(prof, stream, "ms_commit", pgrid, MT, 0, k_ms_commit_list, s, T, c + 2, acc, nl,
+                 c + 1, any);
+      // the push cleared front; restore this level's masks for sigma
+      const uint64_t b0 = loff[loff.size() - 2];
+      TRC_LAUNCH(prof, stream, "mbc_restore", ceil_div(nact, MT), MT, 0, k_mbc_scatter,
+                 lv.o32() + b0, lv.o64() + b0, nact, front);
+    }
+    TRC_LAUNCH(prof, stream, "mbc_sigma", pgrid, MT, 0, k_mbc_sigma, G, nl, c + 1, front, next,
+               sigma, k);
+    TRC_LAUNCH(prof, stream, "mbc_store", pgrid, MT, 0, k_mbc_store, nl, c + 1, next,
+               lv.o32() + base, lv.o64() + base);
+    TRC_LAUNCH(prof, stream, "ms_clear", ceil_div(nact, MT), MT, 0, k_ms_clear, front, L[cur], nact);
+    uint32_t hc[2];
+    uint64_t hany = 0;
+    TRC_CUDA(cudaMemcpyAsync(hc, c, 8, cudaMemcpyDeviceToHost, stream));
+    TRC_CUDA(cudaMemcpyAsync(&hany, any, 8, cudaMemcpyDeviceToHost, stream));
+    sync();
+    nact = hc[1];
+    live = hany;
+    loff.push_back(base + nact);
+    std::swap(front, next);
+    cur ^= 1;
+  }
+  // levels 0..D with entries; loff has D + 2 offsets (the last level empty)
+  const int64_t D = (int64_t)loff.size() - 3;
+  // dense masks of level L+1 for the backward step (front is all-zero now)
+  uint64_t *fnext = front;
+  for (int64_t Lv = D; Lv >= 0; Lv--) {
+    const uint64_t a = loff[Lv], b = loff[Lv + 1];
+    const uint64_t a1 = loff[Lv + 1], b1 = loff[Lv + 2];
+    if (b1 > a1)
+      TRC_LAUNCH(prof, stream, "mbc_scatter", ceil_div(b1 - a1, MT), MT, 0, k_mbc_scatter,
+                 lv.o32() + a1, lv.o64() + a1, (uint32_t)(b1 - a1), fnext);
+    TRC_LAUNCH(prof, stream, "mbc_back", ceil_div((b - a) * 32, MT), MT, 0, k_mbc_back, G,
+               lv.o32() + a, lv.o64() + a, (uint32_t)(b - a), fnext, sigma, dep, k);
+    if (b1 > a1)
+      TRC_LAUNCH(prof, stream, "mbc_clear", ceil_div(b1 - a1, MT), MT, 0, k_ms_clear, fnext,
+                 lv.o32() + a1, (uint32_t)(b1 - a1));
+  }
+  bool dev = flags & TRC_DEVICE_PTR;
+  double *out = dev ? out_user : outb.alloc_exact((uint64_t)n * k);
+  dim3 grid((unsigned)ceil_div(n, 32), (unsigned)ceil_div(k, 32));
+  dim3 block(32, 8);
+  k_mbc_final<<<grid, block, 0, stream>>>(dep, sigma, n, k, out);
+  prof.launches++;
+  TRC_CUDA(cudaGetLastError());
+  if (!dev)
+    TRC_CUDA(cudaMemcpyAsync(out_user, out, (uint64_t)n * k * 8, cudaMemcpyDeviceToHost, stream));
   sync();
 }
 

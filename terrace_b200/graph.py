@@ -213,6 +213,15 @@ class Graph:
         L.check(self._L.trc_msbfs(self._h, C.c_void_p(src.ctypes.data), k, C.c_void_p(po), f))
         return out.reshape(k, self.n)
 
+    def msbc(self, sources, device: bool = False):
+        """BC of up to 64 sources at once: array (k, n), row i = bc(sources[i])
+        (one traversal, one bit per source per vertex)."""
+        src = np.ascontiguousarray(sources, np.uint32)
+        k = len(src)
+        out, po, f = self._out(device, np.float64, k * self.n)
+        L.check(self._L.trc_msbc(self._h, C.c_void_p(src.ctypes.data), k, C.c_void_p(po), f))
+        return out.reshape(k, self.n)
+
     def pagerank(self, iters: int, damping: float = 0.0, device: bool = False):
         """PR_S<double>; damping 0 = the reference's undamped iteration."""
         out, po, f = self._out(device, np.float64, self.n)
