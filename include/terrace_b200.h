@@ -35,7 +35,8 @@ typedef enum {
   TRC_ERR_CUDA = 3,    /* a CUDA call failed (message has the CUDA error) */
   TRC_ERR_TIMEOUT = 4, /* a bounded device wait ran out (serving loop) */
   TRC_ERR_STATE = 5,   /* call not valid in the handle's current state */
-  TRC_ERR_NOT_BUILT = 6 /* the sm_100a kernels are not available */
+  TRC_ERR_NOT_BUILT = 6, /* the sm_100a kernels are not available */
+  TRC_ERR_IO = 7         /* a file could not be opened, read or written */
 } trc_status;
 
 /* flags */
@@ -127,6 +128,26 @@ trc_status trc_get_size(trc_graph *g, uint64_t *bytes);
 /* Whole graph as sorted CSR: offsets[n+1], targets[num_edges]. */
 trc_status trc_dump_csr(trc_graph *g, uint64_t *offsets, uint32_t *targets,
                         uint32_t flags);
+
+/* ---- graph files: replaces get_edges_from_file_adj_sym (include/io_util.h:
+ *      112-145) and the load in src/graph_bm.cc:262-266.  The AdjacencyGraph
+ *      text file ("AdjacencyGraph", n, m, n offsets, m targets; vertex i's
+ *      edges are targets [offsets[i], offsets[i+1]), the last ending at m) is
+ *      parsed on the GPU and its edges inserted as one batch (flags:
+ *      TRC_SYMMETRIZE / TRC_DROP_SELF_LOOPS apply to them; the reference
+ *      inserts them as given).  TRC_ERR_INVALID for a malformed file
+ *      (missing header, wrong word count, a non-number, offsets that do not
+ *      rise from 0, a target >= n), TRC_ERR_IO if it cannot be read.
+ *      The binary CSR file: "TRCCSR01", n and m (u64), offsets[n+1] (u64),
+ *      targets[m] (u32), little-endian. */
+trc_status trc_graph_load_adj(const char *path, uint64_t hbm_budget_bytes,
+                              const trc_config *cfg, uint32_t flags, trc_graph **out);
+/* Writes the graph as an AdjacencyGraph file (sorted lists), formatted on
+ * the GPU. */
+trc_status trc_graph_save_adj(trc_graph *g, const char *path);
+trc_status trc_graph_load_csr(const char *path, uint64_t hbm_budget_bytes,
+                              const trc_config *cfg, uint32_t flags, trc_graph **out);
+trc_status trc_graph_save_csr(trc_graph *g, const char *path);
 
 /* ---- analytics: replaces BFS_with_edge_map (include/BFS.h:41-84),
  *      PR_S<double> (include/Pagerank.h:105-184), CC (include/Components.h:

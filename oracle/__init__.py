@@ -259,6 +259,8 @@ def ref_lib():
         L.ref_rmat.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double,
                                C.c_uint64, C.c_uint64, _u32p, _u32p]
         L.ref_rmat.restype = None
+        L.ref_read_adj.argtypes = [C.c_char_p, C.POINTER(C.c_uint32), _u32p, _u32p, C.c_uint64]
+        L.ref_read_adj.restype = C.c_uint64
         _ref = L
     return _ref
 
@@ -269,6 +271,62 @@ def ref_rmat(n: int, seed: int, a: float, b: float, c: float, count: int, first:
     dst = np.empty(count, np.uint32)
     ref_lib().ref_rmat(n, seed & 0xFFFFFFFF, a, b, c, first, count, src, dst)
     return src, dst
+
+
+def ref_read_adj(path: str):
+    """The reference's AdjacencyGraph reader on a well-formed file:
+    (n, src, dst) in file order."""
+    n = C.c_uint32()
+    probe = np.empty(1, np.uint32)
+    m = ref_lib().ref_read_adj(path.encode(), C.byref(n), probe, probe, 0)
+    src = np.empty(max(m, 1), np.uint32)
+    dst = np.empty(max(m, 1), np.uint32)
+    ref_lib().ref_read_adj(path.encode(), C.byref(n), src, dst, m)
+    return int(n.value), src[:m], dst[:m]
+
+
+# --------------------------------------------------------------------------
+# AdjacencyGraph text (include/io_util.h:112-145): words separated by space,
+# tab, newline, carriage return or NUL (isSpace, include/io_util.h:27-36);
+# "AdjacencyGraph", n, m, n offsets, m targets; vertex i's edges are
+# targets [off[i], off[i+1]), the last vertex's ending at m.
+
+_ADJ_SPACE = b" \t\n\r\0"
+
+
+def parse_adj(data: bytes):
+    """(n, src, dst) of an AdjacencyGraph text, edges in file order; raises
+    ValueError where the reference would stop (missing header, word count
+    other than n + m + 2) and on words that are not decimal numbers or
+    offsets that do not rise from 0 (the reference's atol accepts those
+    silently)."""
+    import re
+    words = re.split(b"[ \t\n\r\x00]+", data.strip(_ADJ_SPACE))
+    if not words or words[0] != b"AdjacencyGraph":
+        raise ValueError("missing header AdjacencyGraph")
+    nums = words[1:]
+    if any(not w.isdigit() for w in nums):
+        raise ValueError("a word is not a number")
+    vals = np.array([int(w) for w in nums], dtype=np.uint64)
+    if len(vals) < 2:
+        raise ValueError("missing n and m")
+    n, m = int(vals[0]), int(vals[1])
+    if len(vals) != n + m + 2:
+        raise ValueError("length != n + m + 2")
+    off = vals[2:2 + n]
+    if n and (off[0] != 0 or np.any(np.diff(off.astype(np.int64)) < 0) or np.any(off > m)):
+        raise ValueError("offsets not monotone from 0")
+    ends = np.append(off[1:], np.uint64(m)) if n else off
+    src = np.repeat(np.arange(n, dtype=np.uint32), (ends - off).astype(np.int64))
+    dst = vals[2 + n:].astype(np.uint32)
+    return n, src, dst
+
+
+def format_adj(off, tgt) -> bytes:
+    """AdjacencyGraph text of a CSR: one number per line after the header."""
+    n = len(off) - 1
+    nums = [n, int(off[n])] + [int(x) for x in off[:n]] + [int(x) for x in tgt]
+    return b"AdjacencyGraph\n" + b"".join(b"%d\n" % x for x in nums)
 
 
 class RefGraph:

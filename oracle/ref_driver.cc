@@ -35,6 +35,7 @@
 #include "BC.h"
 #include "TC.h"
 #include "rmat_util.h"
+#include "io_util.h"
 
 namespace {
 
@@ -168,6 +169,27 @@ void ref_rmat(uint32_t n, uint32_t seed, double a, double b, double c,
     src[i] = e.first;
     dst[i] = e.second;
   }
+}
+
+// The reference's AdjacencyGraph reader (get_edges_from_file_adj_sym,
+// include/io_util.h:112-145) on a well-formed file: returns m and sets *n;
+// with src/dst given (capacity cap) copies the edge pairs in file order.
+uint64_t ref_read_adj(const char *path, uint32_t *n, uint32_t *src, uint32_t *dst, uint64_t cap) {
+  uint64_t m = 0;
+  uint32_t nn = 0;
+  pair_uint *e = nullptr;
+  {
+    QuietStdout q;
+    e = get_edges_from_file_adj_sym(path, &m, &nn, false);
+  }
+  *n = nn;
+  if (src && dst)
+    for (uint64_t i = 0; i < m && i < cap; i++) {
+      src[i] = e[i].x;
+      dst[i] = e[i].y;
+    }
+  free(e);
+  return m;
 }
 
 }  // extern "C"

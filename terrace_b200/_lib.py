@@ -18,6 +18,7 @@ TRC_ERR_CUDA = 3
 TRC_ERR_TIMEOUT = 4
 TRC_ERR_STATE = 5
 TRC_ERR_NOT_BUILT = 6
+TRC_ERR_IO = 7
 
 TRC_DEVICE_PTR = 0x1
 TRC_SYMMETRIZE = 0x2
@@ -120,6 +121,10 @@ SIGNATURES = [
     ("trc_num_edges", _int, [_vp, C.POINTER(_u64)]),
     ("trc_get_size", _int, [_vp, C.POINTER(_u64)]),
     ("trc_dump_csr", _int, [_vp, _vp, _vp, _u32]),
+    ("trc_graph_load_adj", _int, [C.c_char_p, _u64, C.POINTER(trc_config), _u32, C.POINTER(_vp)]),
+    ("trc_graph_save_adj", _int, [_vp, C.c_char_p]),
+    ("trc_graph_load_csr", _int, [C.c_char_p, _u64, C.POINTER(trc_config), _u32, C.POINTER(_vp)]),
+    ("trc_graph_save_csr", _int, [_vp, C.c_char_p]),
     ("trc_bfs", _int, [_vp, _u32, _vp, _vp, _u32]),
     ("trc_bfs_noalloc", _int, [_vp, _u32, _vp, _vp, _u32]),
     ("trc_msbfs", _int, [_vp, _vp, _u32, _vp, _u32]),

@@ -71,6 +71,7 @@ const char *trc_status_string(trc_status s) {
     case TRC_ERR_TIMEOUT: return "device wait timed out";
     case TRC_ERR_STATE: return "invalid state";
     case TRC_ERR_NOT_BUILT: return "kernels not available";
+    case TRC_ERR_IO: return "file input/output failed";
   }
   return "unknown status";
 }

@@ -93,6 +93,11 @@ class Graph {
   void count_common(const uint32_t *s, const uint32_t *d, uint64_t q, uint32_t *out,
                     uint32_t flags);
   void dump_csr(uint64_t *offsets, uint32_t *targets, uint32_t flags);
+  // graph files (io.cu): parse AdjacencyGraph text with m edges and insert
+  // them; insert a host CSR; the graph as AdjacencyGraph text
+  void load_adj(const uint8_t *bytes, uint64_t len, uint64_t m_file, uint32_t flags);
+  void load_csr(const uint64_t *offsets, const uint32_t *targets, uint64_t m_file, uint32_t flags);
+  std::vector<uint8_t> format_adj();
   uint64_t check();
   uint64_t size_bytes() const;
   void stats(trc_stats *out);

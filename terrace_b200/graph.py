@@ -32,27 +32,68 @@ def _arr(x, dtype):
     return a.ctypes.data, a.size, 0, a
 
 
+def _config(hub_threshold: int = 1024, pma_root_density: float = 0.75,
+            pma_build_density: float = 0.5, hub_block_fill: float = 0.75,
+            push_pull_divisor: int = 20, hub_stage_limit: int = 49152,
+            cuda_graphs: bool = True):
+    lib = L.load()
+    cfg = L.trc_config()
+    lib.trc_config_default(C.byref(cfg))
+    cfg.hub_threshold = hub_threshold
+    cfg.pma_root_density = pma_root_density
+    cfg.pma_build_density = pma_build_density
+    cfg.hub_block_fill = hub_block_fill
+    cfg.push_pull_divisor = push_pull_divisor
+    cfg.hub_stage_limit = hub_stage_limit
+    cfg.cuda_graphs = int(cuda_graphs)
+    return cfg
+
+
 class Graph:
     """B200-resident Terrace graph: inline rows, PMA segments, hub blocks."""
 
-    def __init__(self, n: int, hbm_budget: int = 0, hub_threshold: int = 1024,
-                 pma_root_density: float = 0.75, pma_build_density: float = 0.5,
-                 hub_block_fill: float = 0.75, push_pull_divisor: int = 20,
-                 hub_stage_limit: int = 49152, cuda_graphs: bool = True):
+    def __init__(self, n: int, hbm_budget: int = 0, *, _handle=None, **config):
         self._L = L.load()
-        cfg = L.trc_config()
-        self._L.trc_config_default(C.byref(cfg))
-        cfg.hub_threshold = hub_threshold
-        cfg.pma_root_density = pma_root_density
-        cfg.pma_build_density = pma_build_density
-        cfg.hub_block_fill = hub_block_fill
-        cfg.push_pull_divisor = push_pull_divisor
-        cfg.hub_stage_limit = hub_stage_limit
-        cfg.cuda_graphs = int(cuda_graphs)
-        h = C.c_void_p()
-        L.check(self._L.trc_graph_create(n, hbm_budget, C.byref(cfg), C.byref(h)))
-        self._h = h
+        if _handle is None:
+            cfg = _config(**config)
+            h = C.c_void_p()
+            L.check(self._L.trc_graph_create(n, hbm_budget, C.byref(cfg), C.byref(h)))
+            _handle = h
+        self._h = _handle
         self.n = n
+
+    @classmethod
+    def load_adj(cls, path: str, hbm_budget: int = 0, symmetrize: bool = False,
+                 drop_self_loops: bool = False, **config) -> "Graph":
+        """A graph from an AdjacencyGraph text file (the reference's input
+        format, include/io_util.h:112-145), parsed on the GPU."""
+        return cls._load(L.load().trc_graph_load_adj, path, hbm_budget, symmetrize,
+                         drop_self_loops, config)
+
+    @classmethod
+    def load_csr(cls, path: str, hbm_budget: int = 0, symmetrize: bool = False,
+                 drop_self_loops: bool = False, **config) -> "Graph":
+        """A graph from a binary CSR file written by save_csr."""
+        return cls._load(L.load().trc_graph_load_csr, path, hbm_budget, symmetrize,
+                         drop_self_loops, config)
+
+    @classmethod
+    def _load(cls, fn, path, hbm_budget, sym, drop, config):
+        cfg = _config(**config)
+        flags = (L.TRC_SYMMETRIZE if sym else 0) | (L.TRC_DROP_SELF_LOOPS if drop else 0)
+        h = C.c_void_p()
+        L.check(fn(str(path).encode(), hbm_budget, C.byref(cfg), flags, C.byref(h)))
+        n = C.c_uint32()
+        L.check(L.load().trc_num_vertices(h, C.byref(n)))
+        return cls(int(n.value), _handle=h)
+
+    def save_adj(self, path: str):
+        """Writes the graph as an AdjacencyGraph text file (formatted on the GPU)."""
+        L.check(self._L.trc_graph_save_adj(self._h, str(path).encode()))
+
+    def save_csr(self, path: str):
+        """Writes the graph as a binary CSR file ("TRCCSR01", n, m, offsets, targets)."""
+        L.check(self._L.trc_graph_save_csr(self._h, str(path).encode()))
 
     # ---------------------------------------------------------------- lifetime
     def close(self):

@@ -23,6 +23,9 @@ Fixtures:
                        runs only its in-place intersection and is exact
   config1_summary.json RMAT scale 17 ef 8 seed 0 (the static workload):
                        hashes and samples of every output
+  adj_pin.npz          AdjacencyGraph texts and the reference reader's
+                       (n, edges) for each (python tests/golden/make_golden.py
+                       --adj-only regenerates only this one)
 """
 from __future__ import annotations
 
@@ -156,10 +159,41 @@ def run_sequence(name, n, keys, batches, params):
     print(name, "n", n, "m0", len(keys), "steps", step, "maxdeg", int(deg.max()))
 
 
+def adj_texts():
+    """AdjacencyGraph texts for the reader pins: mixed white space (tabs,
+    carriage returns, runs of blanks, a NUL), empty lists, a last vertex with
+    edges, a directed graph, and a seeded RMAT graph one number per line."""
+    yield (b"AdjacencyGraph\n5\n7\n0\n2\n2\n5\n6\n1\n4\n0\n3\n4\n0\n1\n")
+    yield (b"  AdjacencyGraph\r\n4 \t 5\r\n0  1\t1 3\r\n\r\n3 0 2\x00 1\t\t0 ")
+    yield b"AdjacencyGraph 3 0 0 0 0"
+    n, keys = O.rmat_graph_keys(10, 4, .57, .19, .19, 3)
+    off, tgt = O.csr_from_keys(n, keys)
+    yield O.format_adj(off, tgt)
+
+
+def adj_pin():
+    """adj_pin.npz: each text and the reference reader's (n, src, dst)."""
+    rec = {}
+    path = os.path.join(OUT, "_adj_tmp.adj")
+    for i, text in enumerate(adj_texts()):
+        with open(path, "wb") as f:
+            f.write(text)
+        n, src, dst = O.ref_read_adj(path)
+        rec[f"t{i}_text"] = np.frombuffer(text, np.uint8)
+        rec[f"t{i}_n"] = np.uint32(n)
+        rec[f"t{i}_src"], rec[f"t{i}_dst"] = src, dst
+        print("adj text", i, "n", n, "m", len(src))
+    os.remove(path)
+    np.savez_compressed(os.path.join(OUT, "adj_pin.npz"), **rec)
+
+
 def main():
     if not O.ref_available():
         raise SystemExit("build oracle/_ref first: oracle/build_ref.sh")
     O.ref_lib().ref_set_threads(1)
+    adj_pin()
+    if "--adj-only" in sys.argv:
+        return
 
     pins = {}
     for i, (n, seed, a, b, c) in enumerate([(1 << 17, 0, .5, .1, .1),

@@ -124,3 +124,27 @@ def test_config1_summary():
     ref = np.array([np.nan if x is None else x for x in s["bc_sample"]])
     assert rel_close(bc[sample], ref)
     assert O.tc(off, tgt) == s["tc_exact_published_in_survey"] == 758730
+
+
+def test_adj_reader_pinned_to_reference():
+    """The oracle's AdjacencyGraph parser gives exactly the reference
+    reader's (n, edges) on every pinned text (mixed white space, empty
+    lists, a NUL separator, a one-number-per-line RMAT graph), and the
+    oracle's formatter writes text that parses back to the same CSR."""
+    z = np.load(os.path.join(GOLD, "adj_pin.npz"))
+    i = 0
+    while f"t{i}_text" in z:
+        n, s, d = O.parse_adj(z[f"t{i}_text"].tobytes())
+        assert n == int(z[f"t{i}_n"])
+        assert np.array_equal(s, z[f"t{i}_src"]) and np.array_equal(d, z[f"t{i}_dst"])
+        i += 1
+    assert i >= 4
+    n, keys = O.rmat_graph_keys(9, 4, .5, .1, .1, 1)
+    off, tgt = O.csr_from_keys(n, keys)
+    n2, s2, d2 = O.parse_adj(O.format_adj(off, tgt))
+    off2, tgt2 = O.csr_from_keys(n2, O.make_keys(s2, d2, False, False))
+    assert n2 == n and np.array_equal(off2, off) and np.array_equal(tgt2, tgt)
+    for bad in (b"AdjGraph 1 0 0", b"AdjacencyGraph 2 1 0 1", b"AdjacencyGraph 2 1 0 x 1",
+                b"AdjacencyGraph 2 1 1 0 1"):
+        with pytest.raises(ValueError):
+            O.parse_adj(bad)
