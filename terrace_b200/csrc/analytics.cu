@@ -87,6 +87,30 @@ __device__ __forceinline__ uint32_t warp_append(bool win, uint32_t *counter) {
   return base + __popc(m & lanemask_lt());
 }
 
+// Appends each thread's `cnt` items to a global list with ONE atomic per
+// CTA (a per-level frontier counter is one address: a warp-level atomic per
+// warp serialises there).  Every thread of the CTA must call it; returns the
+// thread's first slot.  sh: AT/32 + 2 words of shared memory.
+__device__ __forceinline__ uint32_t block_append(uint32_t cnt, uint32_t *counter, uint32_t *sh) {
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t incl = warp_incl_scan(cnt);
+  if (lane == 31) sh[w] = incl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (uint32_t k = 0; k < (blockDim.x >> 5); k++) {
+      const uint32_t c = sh[k];
+      sh[k] = t;
+      t += c;
+    }
+    sh[AT / 32] = t ? atomicAdd(counter, t) : 0u;
+  }
+  __syncthreads();
+  const uint32_t pos = sh[AT / 32] + sh[w] + incl - cnt;
+  __syncthreads();
+  return pos;
+}
+
 template <typename T>
 __device__ __forceinline__ T block_sum(T v, T *sh) {
   v = warp_sum(v);
@@ -496,27 +520,68 @@ __device__ __forceinline__ bool bit_test(const uint32_t *b, uint32_t v) {
   return (__ldg(b + (v >> 5)) >> (v & 31)) & 1u;
 }
 
+// One 32-neighbour chunk of u's list (ranks j0..j0+31): claim unvisited
+// neighbours by CAS on the parent (any frontier parent, as BFS_F::
+// updateAtomic).
+__device__ __forceinline__ void bfs_push_chunk(const NbrList &L, uint32_t u, uint32_t j0,
+                                               const BFSState &s, uint32_t lane) {
+  const uint32_t j = j0 + lane;
+  bool win = false;
+  uint32_t v = 0;
+  if (j < L.deg) {
+    v = L.at(j);
+    if (s.lv[v] == TRC_UNREACHED && atomicCAS(&s.par[v], -1, (int32_t)u) == -1) {
+      s.lv[v] = s.d + 1;
+      win = true;
+    }
+  }
+  uint32_t pos = warp_append(win, s.next_cnt);
+  if (win) s.next[pos] = v;
+}
+
+// Warp per frontier vertex; hubs are left to k_bfs_push_hubs.
 __global__ void k_bfs_push(DevView G, const uint32_t *F, uint32_t nf, BFSState s) {
   uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
   uint32_t lane = threadIdx.x & 31;
   if (w >= nf) return;
   uint32_t u = F[w];
+  if (G.hub_of[u] >= 0) return;
   NbrList L = nbr_list(G, u);
-  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) {
-    uint32_t j = j0 + lane;
-    bool win = false;
-    uint32_t v = 0;
-    if (j < L.deg) {
-      v = L.at(j);
-      if (s.lv[v] == TRC_UNREACHED && atomicCAS(&s.par[v], -1, (int32_t)u) == -1) {
-        s.lv[v] = s.d + 1;
-        win = true;
-      }
-    }
-    uint32_t pos = warp_append(win, s.next_cnt);
-    if (win) s.next[pos] = v;
+  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) bfs_push_chunk(L, u, j0, s, lane);
+}
+
+// The frontier's hubs (list and device count from a compaction).  The first
+// PUSH_WIDE hubs are spread over the whole grid (every warp takes their
+// 32-neighbour chunks round-robin), so one vertex of 1e5-1e6 neighbours
+// uses the whole GPU; the rest get a CTA each (grid-stride), its warps
+// taking the chunks round-robin.
+constexpr uint64_t PUSH_WIDE = 64;
+
+__global__ void k_bfs_push_hubs(DevView G, const uint32_t *FH, const uint64_t *nfh, BFSState s) {
+  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint64_t gw = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * AT) >> 5;
+  const uint64_t nh = *nfh;
+  const uint64_t nwide = nh < PUSH_WIDE ? nh : PUSH_WIDE;
+  for (uint64_t i = 0; i < nwide; i++) {
+    const uint32_t u = FH[i];
+    NbrList L = nbr_list(G, u);
+    const uint64_t nch = (L.deg + 31) >> 5;
+    for (uint64_t c = gw; c < nch; c += nwarps) bfs_push_chunk(L, u, (uint32_t)(c << 5), s, lane);
+  }
+  for (uint64_t i = nwide + blockIdx.x; i < nh; i += gridDim.x) {
+    const uint32_t u = FH[i];
+    NbrList L = nbr_list(G, u);
+    const uint32_t nch = (L.deg + 31) >> 5;
+    for (uint32_t c = wib; c < nch; c += AT / 32) bfs_push_chunk(L, u, c << 5, s, lane);
   }
 }
+
+struct HubPred {
+  const uint32_t *F;
+  const int32_t *hub_of;
+  __device__ bool operator()(uint64_t i) const { return hub_of[F[i]] >= 0; }
+};
 
 // List entries that are still unvisited (and have more than min_deg
 // neighbours).
@@ -580,6 +645,7 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
     wz[i] = act[i] && e + 2 < d[i] ? __ldg(s.bits + (v[i].z >> 5)) : 0u;
     ww[i] = act[i] && e + 3 < d[i] ? __ldg(s.bits + (v[i].w >> 5)) : 0u;
   }
+  uint32_t wins = 0;  // bit i: this lane claimed vertex i
 #pragma unroll
   for (uint32_t i = 0; i < BP_V; i++) {
     uint32_t first = 4;
@@ -594,10 +660,14 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
       uint32_t p = first == 0 ? v[i].x : first == 1 ? v[i].y : first == 2 ? v[i].z : v[i].w;
       s.par[u[i]] = (int32_t)p;
       s.lv[u[i]] = s.d + 1;
+      wins |= 1u << i;
     }
-    uint32_t pos = warp_append(win, s.next_cnt);
-    if (win) s.next[pos] = u[i];
   }
+  __shared__ uint32_t sh[AT / 32 + 2];
+  uint32_t pos = block_append(__popc(wins), s.next_cnt, sh);
+#pragma unroll
+  for (uint32_t i = 0; i < BP_V; i++)
+    if ((wins >> i) & 1u) s.next[pos++] = u[i];
 }
 
 // One warp scans the neighbours of vertex u of rank >= j_first for a
@@ -630,19 +700,22 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_W(DevView G, const uint32_t *Ls
                                                    BFSState s, uint32_t j_first) {
   uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
   uint32_t lane = threadIdx.x & 31;
-  if (w >= nL) return;
-  uint32_t u = Lst[w];
+  uint32_t u = 0;
   bool win = false;
-  if (s.lv[u] == TRC_UNREACHED) {
-    NbrList L = nbr_list(G, u);
-    uint32_t p = warp_any_in_frontier(L, s.bits, j_first);
-    if (p != NONE32 && lane == 0) {
-      s.par[u] = (int32_t)p;
-      s.lv[u] = s.d + 1;
-      win = true;
+  if (w < nL) {
+    u = Lst[w];
+    if (s.lv[u] == TRC_UNREACHED) {
+      NbrList L = nbr_list(G, u);
+      uint32_t p = warp_any_in_frontier(L, s.bits, j_first);
+      if (p != NONE32 && lane == 0) {
+        s.par[u] = (int32_t)p;
+        s.lv[u] = s.d + 1;
+        win = true;
+      }
     }
   }
-  uint32_t pos = warp_append(win, s.next_cnt);
+  __shared__ uint32_t sh[AT / 32 + 2];
+  uint32_t pos = block_append(win ? 1u : 0u, s.next_cnt, sh);
   if (win) s.next[pos] = u;
 }
 
@@ -713,6 +786,15 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
     } else {
       TRC_LAUNCH(prof, stream, "bfs_push", ceil_div((uint64_t)nf * 32, AT), AT, 0, k_bfs_push, G, F,
                  nf, s);
+      if (H) {
+        // frontier hubs, spread over the grid
+        uint32_t *fh = segb.ensure(nf);
+        uint64_t *t = tmp(select_tmp_elems(nf) + 4);
+        select_if(HubPred{F, hub_of.get()}, ListVal{F}, nf, fh, sc + 1, t, stream, prof,
+                  "sel_bfs_hubs");
+        TRC_LAUNCH(prof, stream, "bfs_push_hubs", (unsigned)num_sms() * 8, AT, 0, k_bfs_push_hubs, G,
+                   fh, sc + 1, s);
+      }
     }
     TRC_CUDA(cudaMemcpyAsync(&nf, c, 4, cudaMemcpyDeviceToHost, stream));
     sync();
