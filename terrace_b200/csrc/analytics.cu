@@ -514,6 +514,11 @@ struct BFSState {
   uint32_t *next;        // next-frontier queue
   uint32_t *next_cnt;
   uint32_t d;            // current level
+  // dense steps: vertices left unvisited by the inline pass that have a
+  // PMA segment (seg), and vertices left unvisited by the step (cand, the
+  // next dense step's candidates); push steps: the frontier's hubs (seg)
+  uint32_t *seg, *seg_cnt;
+  uint32_t *cand, *cand_cnt;
 };
 
 __device__ __forceinline__ bool bit_test(const uint32_t *b, uint32_t v) {
@@ -539,13 +544,16 @@ __device__ __forceinline__ void bfs_push_chunk(const NbrList &L, uint32_t u, uin
   if (win) s.next[pos] = v;
 }
 
-// Warp per frontier vertex; hubs are left to k_bfs_push_hubs.
+// Warp per frontier vertex; hubs are listed for k_bfs_push_hubs.
 __global__ void k_bfs_push(DevView G, const uint32_t *F, uint32_t nf, BFSState s) {
   uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
   uint32_t lane = threadIdx.x & 31;
   if (w >= nf) return;
   uint32_t u = F[w];
-  if (G.hub_of[u] >= 0) return;
+  if (G.hub_of[u] >= 0) {
+    if (lane == 0) s.seg[atomicAdd(s.seg_cnt, 1u)] = u;
+    return;
+  }
   NbrList L = nbr_list(G, u);
   for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) bfs_push_chunk(L, u, j0, s, lane);
 }
@@ -557,11 +565,12 @@ __global__ void k_bfs_push(DevView G, const uint32_t *F, uint32_t nf, BFSState s
 // taking the chunks round-robin.
 constexpr uint64_t PUSH_WIDE = 64;
 
-__global__ void k_bfs_push_hubs(DevView G, const uint32_t *FH, const uint64_t *nfh, BFSState s) {
+__global__ void k_bfs_push_hubs(DevView G, BFSState s) {
   const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint64_t gw = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * AT) >> 5;
-  const uint64_t nh = *nfh;
+  const uint32_t *FH = s.seg;
+  const uint64_t nh = *s.seg_cnt;
   const uint64_t nwide = nh < PUSH_WIDE ? nh : PUSH_WIDE;
   for (uint64_t i = 0; i < nwide; i++) {
     const uint32_t u = FH[i];
@@ -577,11 +586,7 @@ __global__ void k_bfs_push_hubs(DevView G, const uint32_t *FH, const uint64_t *n
   }
 }
 
-struct HubPred {
-  const uint32_t *F;
-  const int32_t *hub_of;
-  __device__ bool operator()(uint64_t i) const { return hub_of[F[i]] >= 0; }
-};
+
 
 // List entries that are still unvisited (and have more than min_deg
 // neighbours).
@@ -599,9 +604,12 @@ struct ListVal {
   __device__ uint32_t operator()(uint64_t i) const { return L[i]; }
 };
 
-__global__ void k_set_bits(const uint32_t *F, uint32_t nf, uint32_t *bits) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nf) atomicOr(bits + (F[i] >> 5), 1u << (F[i] & 31));
+// frontier bitmap of level d from the levels: one ballot per 32 vertices
+// (no atomics, no clearing pass)
+__global__ void k_level_bits(const uint32_t *lv, uint32_t n, uint32_t d, uint32_t *bits) {
+  const uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t b = __ballot_sync(0xFFFFFFFFu, v < n && lv[v] == d);
+  if ((threadIdx.x & 31) == 0 && v < n) bits[v >> 5] = b;
 }
 
 // Inline pass of a dense step: 4 lanes per vertex (one 128-bit quarter of
@@ -646,8 +654,10 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
     ww[i] = act[i] && e + 3 < d[i] ? __ldg(s.bits + (v[i].w >> 5)) : 0u;
   }
   uint32_t wins = 0;  // bit i: this lane claimed vertex i
+  uint32_t tosg = 0, tocand = 0;  // bit i (lane q == 0): vertex i stays unvisited
 #pragma unroll
   for (uint32_t i = 0; i < BP_V; i++) {
+    const bool uv = d[i] > 0 && s.lv[u[i]] == TRC_UNREACHED;  // cached: loaded above
     uint32_t first = 4;
     if ((wx[i] >> (v[i].x & 31)) & 1u) first = 0;
     else if ((wy[i] >> (v[i].y & 31)) & 1u) first = 1;
@@ -662,12 +672,24 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
       s.lv[u[i]] = s.d + 1;
       wins |= 1u << i;
     }
+    if (q == 0 && uv && grp == 0) {
+      if (d[i] > K_INLINE) tosg |= 1u << i;
+      else tocand |= 1u << i;
+    }
   }
   __shared__ uint32_t sh[AT / 32 + 2];
   uint32_t pos = block_append(__popc(wins), s.next_cnt, sh);
 #pragma unroll
   for (uint32_t i = 0; i < BP_V; i++)
     if ((wins >> i) & 1u) s.next[pos++] = u[i];
+  pos = block_append(__popc(tosg), s.seg_cnt, sh);
+#pragma unroll
+  for (uint32_t i = 0; i < BP_V; i++)
+    if ((tosg >> i) & 1u) s.seg[pos++] = u[i];
+  pos = block_append(__popc(tocand), s.cand_cnt, sh);
+#pragma unroll
+  for (uint32_t i = 0; i < BP_V; i++)
+    if ((tocand >> i) & 1u) s.cand[pos++] = u[i];
 }
 
 // One warp scans the neighbours of vertex u of rank >= j_first for a
@@ -696,27 +718,57 @@ __device__ __forceinline__ uint32_t warp_any_in_frontier(const NbrList &L, const
 
 // Warp per vertex of a list (M or H class), scanning ranks >= j_first (the
 // inline pass has already checked ranks below it for M vertices).
+// Per-warp staging of list appends: entries collect in 32 shared slots and
+// go out 32 at a time with one atomic (no CTA-wide synchronisation, so the
+// warps of a CTA never wait for each other's scans).
+struct WarpBuf {
+  uint32_t *slot;  // 32 shared words of this warp
+  uint32_t cnt = 0;
+  __device__ void push(bool has, uint32_t v, uint32_t *list, uint32_t *counter, uint32_t lane) {
+    if (!has) return;  // warp-uniform
+    if (lane == 0) slot[cnt] = v;
+    if (++cnt == 32) flush(list, counter, lane);
+  }
+  __device__ void flush(uint32_t *list, uint32_t *counter, uint32_t lane) {
+    __syncwarp();
+    if (cnt) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(counter, cnt);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (lane < cnt) list[base + lane] = slot[lane];
+    }
+    __syncwarp();
+    cnt = 0;
+  }
+};
+
+// Warp per list entry (nL_dev: count on the device, else nL), grid-stride;
+// with `keep`, entries left unvisited join the candidates.
 __global__ void __launch_bounds__(AT) k_bfs_pull_W(DevView G, const uint32_t *Lst, uint64_t nL,
-                                                   BFSState s, uint32_t j_first) {
-  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
-  uint32_t lane = threadIdx.x & 31;
-  uint32_t u = 0;
-  bool win = false;
-  if (w < nL) {
-    u = Lst[w];
-    if (s.lv[u] == TRC_UNREACHED) {
+                                                   const uint32_t *nL_dev, BFSState s,
+                                                   uint32_t j_first, int keep) {
+  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint64_t n_l = nL_dev ? *nL_dev : nL;
+  __shared__ uint32_t sw[AT / 32][32], sl[AT / 32][32];
+  WarpBuf bw{sw[wib]}, bl{sl[wib]};
+  const uint64_t stride = ((uint64_t)gridDim.x * AT) >> 5;
+  for (uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5; w < n_l; w += stride) {
+    const uint32_t u = Lst[w];
+    uint32_t p = NONE32;
+    const bool unvisited = s.lv[u] == TRC_UNREACHED;
+    if (unvisited) {
       NbrList L = nbr_list(G, u);
-      uint32_t p = warp_any_in_frontier(L, s.bits, j_first);
+      p = warp_any_in_frontier(L, s.bits, j_first);
       if (p != NONE32 && lane == 0) {
         s.par[u] = (int32_t)p;
         s.lv[u] = s.d + 1;
-        win = true;
       }
     }
+    bw.push(unvisited && p != NONE32, u, s.next, s.next_cnt, lane);
+    if (keep) bl.push(unvisited && p == NONE32, u, s.cand, s.cand_cnt, lane);
   }
-  __shared__ uint32_t sh[AT / 32 + 2];
-  uint32_t pos = block_append(win ? 1u : 0u, s.next_cnt, sh);
-  if (win) s.next[pos] = u;
+  bw.flush(s.next, s.next_cnt, lane);
+  if (keep) bl.flush(s.cand, s.cand_cnt, lane);
 }
 
 __global__ void k_bfs_init(uint32_t *lv, int32_t *par, uint32_t n, uint32_t src, uint32_t *q) {
@@ -755,49 +807,42 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
   const uint32_t *cand = lists.SM.get();
   uint64_t ncand = lists.nSM;
   int cnext = 0;
-  uint64_t *sc = s_cnt.get() + 28;
+  uint32_t *sg = segb.ensure(n);
+  const unsigned pgrid = (unsigned)num_sms() * 8;
   while (nf > 0) {
-    TRC_CUDA(cudaMemsetAsync(c, 0, 4, stream));
-    BFSState s{lv, par, bm, Nx, c, d};
+    TRC_CUDA(cudaMemsetAsync(c, 0, 16, stream));  // next, seg, cand counts
+    BFSState s{lv, par, bm, Nx, c, d, sg, c + 1, nullptr, c + 2};
+    uint32_t hc[3] = {0, 0, 0};
     if ((uint64_t)nf >= dense_at && dense_at > 0) {
-      TRC_CUDA(cudaMemsetAsync(bm, 0, words * 4, stream));
-      TRC_LAUNCH(prof, stream, "bfs_bits", ceil_div(nf, AT), AT, 0, k_set_bits, F, nf, bm);
-      // pass A: the 16 inline neighbours of every unvisited non-hub vertex
+      TRC_LAUNCH(prof, stream, "bfs_bits", ceil_div(n, AT), AT, 0, k_level_bits, lv, n, d, bm);
+      // candidates left for the next dense step (never the list being read)
+      s.cand = cbuf[cnext].ensure(ncand ? ncand : 1);
+      // pass A: the 16 inline neighbours of every unvisited non-hub vertex;
+      // those left unvisited go to the segment list (PMA vertices) or the
+      // next candidates
       TRC_LAUNCH(prof, stream, "bfs_pull_inline", ceil_div(ncand * 4, (uint64_t)AT * BP_V), AT, 0,
                  k_bfs_pull_S, G, cand, ncand, s);
-      // pass B: the PMA segments of those still unvisited (compacted); hubs
-      // from rank 0
-      uint32_t *pb = segb.ensure(ncand ? ncand : 1);
-      uint64_t *t = tmp(select_tmp_elems(ncand) + 4);
-      select_if(UnvisitedPred{cand, lv, deg.get(), K_INLINE}, ListVal{cand}, ncand, pb, sc, t,
-                stream, prof, "sel_bfs_segment");
-      uint64_t nb = read_u64(sc);
-      TRC_LAUNCH(prof, stream, "bfs_pull_M", ceil_div(nb * 32, AT), AT, 0, k_bfs_pull_W, G, pb, nb,
-                 s, K_INLINE);
+      // pass B: the PMA segments of the segment list (count on the device);
+      // hubs from rank 0
+      TRC_LAUNCH(prof, stream, "bfs_pull_M", pgrid, AT, 0, k_bfs_pull_W, G, sg, 0, c + 1, s,
+                 K_INLINE, 1);
       TRC_LAUNCH(prof, stream, "bfs_pull_H", ceil_div(lists.nH * 32, AT), AT, 0, k_bfs_pull_W, G,
-                 lists.Hv.get(), lists.nH, s, 0u);
-      // candidates left for the next dense step
-      uint32_t *pa = cbuf[cnext].ensure(ncand ? ncand : 1);  // never the list being read
-      select_if(UnvisitedPred{cand, lv, deg.get(), 0}, ListVal{cand}, ncand, pa, sc, t, stream,
-                prof, "sel_bfs_cand");
-      ncand = read_u64(sc);
-      cand = pa;
+                 lists.Hv.get(), lists.nH, (const uint32_t *)nullptr, s, 0u, 0);
+      TRC_CUDA(cudaMemcpyAsync(hc, c, 12, cudaMemcpyDeviceToHost, stream));
+      sync();
+      ncand = hc[2];
+      cand = s.cand;
       cnext ^= 1;
     } else {
       TRC_LAUNCH(prof, stream, "bfs_push", ceil_div((uint64_t)nf * 32, AT), AT, 0, k_bfs_push, G, F,
                  nf, s);
-      if (H) {
-        // frontier hubs, spread over the grid
-        uint32_t *fh = segb.ensure(nf);
-        uint64_t *t = tmp(select_tmp_elems(nf) + 4);
-        select_if(HubPred{F, hub_of.get()}, ListVal{F}, nf, fh, sc + 1, t, stream, prof,
-                  "sel_bfs_hubs");
-        TRC_LAUNCH(prof, stream, "bfs_push_hubs", (unsigned)num_sms() * 8, AT, 0, k_bfs_push_hubs, G,
-                   fh, sc + 1, s);
-      }
+      // the frontier's hubs (listed by bfs_push), spread over the grid
+      if (H)
+        TRC_LAUNCH(prof, stream, "bfs_push_hubs", pgrid, AT, 0, k_bfs_push_hubs, G, s);
+      TRC_CUDA(cudaMemcpyAsync(hc, c, 4, cudaMemcpyDeviceToHost, stream));
+      sync();
     }
-    TRC_CUDA(cudaMemcpyAsync(&nf, c, 4, cudaMemcpyDeviceToHost, stream));
-    sync();
+    nf = hc[0];
     std::swap(F, Nx);
     d++;
   }
