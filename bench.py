@@ -253,6 +253,8 @@ def run_ours(args, rank, world):
         "cc_ms": cc_ms, "bc_ms": bc_ms, "tc_ms": tc_ms, "triangles": tcount,
     }
 
+    batched22 = {} if args.skip_batched else batched(T, torch, g, stream, n, t_call)
+
     # ---- roofline of the dominant kernel of the timed insert steps
     dom = max(kernel_ms.items(), key=lambda kv: kv[1][0])
     roof = roofline_for(dom[0], dom[1], sizes, hbm_gbs, peak_kind)
@@ -289,11 +291,69 @@ def run_ours(args, rank, world):
         "kernel_share": {k: round(v[0] / total_kernel_ms, 4) for k, v in
                          sorted(kernel_ms.items(), key=lambda kv: -kv[1][0])[:12]},
         "analytics_rmat22": analytics22,
+        "batched_rmat22": batched22,
         "analytics_rmat24": s24,
         "tiers": {k: st[k] for k in ("inline_edges", "pma_edges", "hub_edges", "num_hubs",
                                      "pma_capacity", "pma_rebuilds", "pma_window_rebalances")},
     }
     return res
+
+
+def batched(T, torch, g, stream, n, t_call):
+    """Batched multi-instance analytics on the scale-22 graph: 64 BFS and 64
+    BC sources (uniform over non-isolated vertices, seed 2) as per-vertex
+    source masks in one traversal, against the same sources one by one; 256
+    insert batches of log-uniform size in [10, 1e5] pairs (seed 2) applied
+    as one coalesced sort + merge against one call per batch (both from HBM;
+    the edges are removed again afterwards, untimed)."""
+    rng = np.random.default_rng(2)
+    deg = g.degree(np.arange(n, dtype=np.uint32))
+    src = rng.choice(np.flatnonzero(deg), 64, replace=False).astype(np.uint32)
+    ms_bfs, _ = t_call(lambda: g.msbfs(src, device=True), reps=2)
+    one_bfs = 0.0
+    for v in src:
+        t, _ = t_call(lambda: g.bfs(int(v), device=True), reps=1)
+        one_bfs += t
+    ms_bc, _ = t_call(lambda: g.msbc(src, device=True), reps=1)
+    torch.cuda.empty_cache()
+    one_bc = 0.0
+    for v in src:
+        t, _ = t_call(lambda: g.bc(int(v), device=True), reps=1)
+        one_bc += t
+    sizes = np.exp(rng.uniform(np.log(10), np.log(1e5), 256)).astype(np.int64)
+    bs, bd = T.rmat_generate(n, hash32(2), A, B, C, int(sizes.sum()), device=True)
+    # pairs of edges not in the graph (and no self-loops), so that removing
+    # the batches afterwards restores the graph and both runs insert the
+    # same edge set
+    keep = (g.is_edge(bs, bd) == 0) & (bs != bd)
+    cuts = np.concatenate([[0], np.cumsum(sizes)])
+    kc = torch.cumsum(keep.to(torch.int64), 0).cpu().numpy()
+    cuts = np.concatenate([[0], kc[cuts[1:] - 1]])
+    bs, bd = bs[keep].contiguous(), bd[keep].contiguous()
+
+    def one_by_one():
+        return sum(g.add_edge_batch(bs[cuts[i]:cuts[i + 1]], bd[cuts[i]:cuts[i + 1]],
+                                    symmetrize=True, drop_self_loops=True) for i in range(256))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    added = one_by_one()
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    g.remove_edge_batch(bs, bd, symmetrize=True, drop_self_loops=True)
+    torch.cuda.synchronize()
+    ev[2].record(stream)
+    added2 = g.add_edge_batch(bs, bd, symmetrize=True, drop_self_loops=True)
+    ev[3].record(stream)
+    torch.cuda.synchronize()
+    g.remove_edge_batch(bs, bd, symmetrize=True, drop_self_loops=True)
+    t_sep, t_co = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
+    return {"sources": 64, "msbfs_ms": ms_bfs, "bfs_64_one_by_one_ms": one_bfs,
+            "msbc_ms": ms_bc, "bc_64_one_by_one_ms": one_bc,
+            "update_batches": 256, "update_pairs": int(cuts[-1]),
+            "separate_ms": t_sep, "separate_edges_per_s": added / (t_sep / 1e3),
+            "coalesced_ms": t_co, "coalesced_edges_per_s": added2 / (t_co / 1e3),
+            "same_edges": added == added2}
 
 
 def kernel_bytes(name, sz):
@@ -642,6 +702,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-scale24", action="store_true")
+    ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--serving-only", action="store_true")

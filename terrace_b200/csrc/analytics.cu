@@ -287,7 +287,8 @@ __global__ void __launch_bounds__(AT) k_flat(DevView G, const uint32_t *V, uint6
   __shared__ double acc_all[AT];
   const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint64_t base = ((uint64_t)blockIdx.x * (AT / 32) + wib) * 32;
-  if (base >= nV) return;
+  // warps past the end keep going with no entries: Op::store may be
+  // CTA-collective
   double *acc = acc_all + wib * 32;
   FlatWarp f = flat_setup(G, V, nV, base, op);
   acc[lane] = 0.0;
@@ -959,31 +960,67 @@ struct BCFwd {
   uint32_t *order;      // order[base ..] receives the next level
   uint32_t *next_cnt;
   uint32_t d;
+  uint32_t *hubs, *hub_cnt;  // push steps: the frontier's hubs
 };
 
+// One 32-neighbour chunk of a frontier vertex u (sigma su): claim
+// unvisited neighbours for level d+1 and add su to the path count of every
+// neighbour on level d+1 (BC_F::updateAtomic's CAS-add, include/BC.h:44-58).
+__device__ __forceinline__ void bc_push_chunk(const NbrList &L, double su, uint32_t j0,
+                                              const BCFwd &s, uint32_t lane) {
+  const uint32_t j = j0 + lane;
+  bool win = false;
+  uint32_t v = 0;
+  if (j < L.deg) {
+    v = L.at(j);
+    uint32_t lvv = s.lv[v];
+    if (lvv == TRC_UNREACHED) {
+      uint32_t old = atomicCAS(&s.lv[v], TRC_UNREACHED, s.d + 1);
+      win = old == TRC_UNREACHED;
+      lvv = win ? s.d + 1 : old;
+    }
+    if (lvv == s.d + 1) atomicAdd(&s.sigma[v], su);
+  }
+  uint32_t pos = warp_append(win, s.next_cnt);
+  if (win) s.order[pos] = v;
+}
+
+// Warp per frontier vertex; hubs are listed for k_bc_push_hubs.
 __global__ void k_bc_push(DevView G, const uint32_t *F, uint32_t nf, BCFwd s) {
   uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
   uint32_t lane = threadIdx.x & 31;
   if (w >= nf) return;
   uint32_t u = F[w];
+  if (G.hub_of[u] >= 0) {
+    if (lane == 0) s.hubs[atomicAdd(s.hub_cnt, 1u)] = u;
+    return;
+  }
   double su = s.sigma[u];
   NbrList L = nbr_list(G, u);
-  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) {
-    uint32_t j = j0 + lane;
-    bool win = false;
-    uint32_t v = 0;
-    if (j < L.deg) {
-      v = L.at(j);
-      uint32_t lvv = s.lv[v];
-      if (lvv == TRC_UNREACHED) {
-        uint32_t old = atomicCAS(&s.lv[v], TRC_UNREACHED, s.d + 1);
-        win = old == TRC_UNREACHED;
-        lvv = win ? s.d + 1 : old;
-      }
-      if (lvv == s.d + 1) atomicAdd(&s.sigma[v], su);
-    }
-    uint32_t pos = warp_append(win, s.next_cnt);
-    if (win) s.order[pos] = v;
+  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) bc_push_chunk(L, su, j0, s, lane);
+}
+
+// The frontier's hubs: the first PUSH_WIDE spread over the grid, the rest a
+// CTA each (as k_bfs_push_hubs).
+__global__ void k_bc_push_hubs(DevView G, BCFwd s) {
+  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint64_t gw = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * AT) >> 5;
+  const uint64_t nh = *s.hub_cnt;
+  const uint64_t nwide = nh < PUSH_WIDE ? nh : PUSH_WIDE;
+  for (uint64_t i = 0; i < nwide; i++) {
+    const uint32_t u = s.hubs[i];
+    const double su = s.sigma[u];
+    NbrList L = nbr_list(G, u);
+    const uint64_t nch = (L.deg + 31) >> 5;
+    for (uint64_t c = gw; c < nch; c += nwarps) bc_push_chunk(L, su, (uint32_t)(c << 5), s, lane);
+  }
+  for (uint64_t i = nwide + blockIdx.x; i < nh; i += gridDim.x) {
+    const uint32_t u = s.hubs[i];
+    const double su = s.sigma[u];
+    NbrList L = nbr_list(G, u);
+    const uint32_t nch = (L.deg + 31) >> 5;
+    for (uint32_t c = wib; c < nch; c += AT / 32) bc_push_chunk(L, su, c << 5, s, lane);
   }
 }
 
@@ -1058,7 +1095,8 @@ struct BCPullOp {
       s.sigma[u] = sum;
       s.lv[u] = s.d + 1;
     }
-    uint32_t pos = warp_append(win, s.next_cnt);
+    __shared__ uint32_t sh[AT / 32 + 2];
+    uint32_t pos = block_append(win ? 1u : 0u, s.next_cnt, sh);  // every thread of the CTA
     if (win) s.order[pos] = u;
   }
 };
@@ -1125,6 +1163,9 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
   for (auto *b : {&lvb, &ordb, &cntb}) b->bind(&budget);
   for (auto *b : {&sig, &invb, &depb, &outb}) b->bind(&budget);
   uint32_t *lv = lvb.alloc_exact(n), *order = ordb.alloc_exact(n), *c = cntb.alloc_exact(4);
+  DBuf<uint32_t> hubb;
+  hubb.bind(&budget);
+  uint32_t *hubl = hubb.alloc_exact(H ? H : 1);  // frontier hubs of a push step
   double *sigma = sig.alloc_exact(n), *inv = invb.alloc_exact(n), *dep = depb.alloc_exact(n);
   double *out = dev ? out_user : outb.alloc_exact(n);
   TRC_LAUNCH(prof, stream, "bc_init", ceil_div(n, AT), AT, 0, k_bc_init, lv, sigma, dep, n, src,
@@ -1137,8 +1178,8 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
     uint64_t f0 = loff[d], f1 = loff[d + 1];
     uint32_t nf = (uint32_t)(f1 - f0);
     if (nf == 0) break;
-    TRC_CUDA(cudaMemsetAsync(c, 0, 4, stream));
-    BCFwd s{lv, sigma, order + f1, c, d};
+    TRC_CUDA(cudaMemsetAsync(c, 0, 8, stream));
+    BCFwd s{lv, sigma, order + f1, c, d, hubl, c + 1};
     if ((uint64_t)nf >= dense_at && dense_at > 0) {
       TRC_LAUNCH(prof, stream, "bc_pull_flat", ceil_div(lists.nSM, AT), AT, 0, k_flat<BCPullOp>,
                  G, lists.SM.get(), lists.nSM, BCPullOp{s});
@@ -1147,6 +1188,9 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
     } else {
       TRC_LAUNCH(prof, stream, "bc_push", ceil_div((uint64_t)nf * 32, AT), AT, 0, k_bc_push, G,
                  order + f0, nf, s);
+      if (H)
+        TRC_LAUNCH(prof, stream, "bc_push_hubs", (unsigned)num_sms() * 8, AT, 0, k_bc_push_hubs, G,
+                   s);
     }
     uint32_t nn = 0;
     TRC_CUDA(cudaMemcpyAsync(&nn, c, 4, cudaMemcpyDeviceToHost, stream));

@@ -248,19 +248,30 @@ class Graph:
     def msbfs(self, sources, device: bool = False):
         """Levels of up to 64 BFS at once: array (k, n), TRC_UNREACHED if
         unreached (one traversal, one bit per source per vertex)."""
-        src = np.ascontiguousarray(sources, np.uint32)
+        src, ps, keep = self._sources(sources, device)
         k = len(src)
         out, po, f = self._out(device, np.uint32, k * self.n)
-        L.check(self._L.trc_msbfs(self._h, C.c_void_p(src.ctypes.data), k, C.c_void_p(po), f))
+        L.check(self._L.trc_msbfs(self._h, C.c_void_p(ps), k, C.c_void_p(po), f))
         return out.reshape(k, self.n)
+
+    @staticmethod
+    def _sources(sources, device):
+        """Host sources as (array, pointer, keepalive); on the device when the
+        outputs are (one flag covers every array argument)."""
+        src = np.ascontiguousarray(sources, np.uint32)
+        if not device:
+            return src, src.ctypes.data, src
+        import torch
+        t = torch.as_tensor(src.view(np.int32)).to("cuda")
+        return src, t.data_ptr(), t
 
     def msbc(self, sources, device: bool = False):
         """BC of up to 64 sources at once: array (k, n), row i = bc(sources[i])
         (one traversal, one bit per source per vertex)."""
-        src = np.ascontiguousarray(sources, np.uint32)
+        src, ps, keep = self._sources(sources, device)
         k = len(src)
         out, po, f = self._out(device, np.float64, k * self.n)
-        L.check(self._L.trc_msbc(self._h, C.c_void_p(src.ctypes.data), k, C.c_void_p(po), f))
+        L.check(self._L.trc_msbc(self._h, C.c_void_p(ps), k, C.c_void_p(po), f))
         return out.reshape(k, self.n)
 
     def pagerank(self, iters: int, damping: float = 0.0, device: bool = False):
