@@ -63,6 +63,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   wstamp.bind(&budget);
   pbeg_alt.bind(&budget);
   s_tix.bind(&budget);
+  s_wbits.bind(&budget);
   s_hw_do.bind(&budget);
   s_hw_h.bind(&budget);
   s_flags.bind(&budget);
@@ -129,7 +130,7 @@ DevView Graph::view() const {
 void Graph::release_scratch() {
   sync();
   for (auto *b : {&s_in_src, &s_in_dst, &s_tu, &s_tdn, &s_tc2, &s_ovl, &s_hw_u, &s_hw_dn, &s_hw_t,
-                  &s_c2n, &s_rlist, &s_pma_next, &s_tix, &s_hw_do})
+                  &s_c2n, &s_rlist, &s_pma_next, &s_tix, &s_hw_do, &s_wbits})
     b->reset();
   for (auto *b : {&s_A, &s_B, &s_C, &s_tmp, &s_P, &s_oOff, &s_nOff, &s_wk, &s_wk2, &s_mw, &s_old,
                   &s_new, &s_hwplan, &pbeg_alt})
@@ -330,11 +331,25 @@ struct LoadC2 {
   __device__ uint64_t operator()(uint64_t i) const { return c[i]; }
 };
 
+// Per-level bitmaps of the chosen windows: level h has one bit per aligned
+// range of 2^h vertices, starting at word base[h].
+struct WinBits {
+  uint32_t *mark;  // windows chosen by some overflow vertex
+  uint32_t *emit;  // maximal windows already listed
+  uint64_t base[34];
+};
+
+__device__ __forceinline__ bool win_bit(const uint32_t *bits, const WinBits &wb, uint32_t h,
+                                        uint64_t idx) {
+  return (bits[wb.base[h] + (idx >> 5)] >> (idx & 31)) & 1u;
+}
+
 // Window search (step 5): lowest level (from the leaf level, 2^leaf vertex
-// segments) whose aligned vertex range has density within its bound.  Keys sort by (start asc, level desc).
+// segments) whose aligned vertex range has density within its bound; its
+// key is (start << 6 | 63 - level) and its bit is set in the level bitmap.
 __global__ void k_find_windows(const uint32_t *ovl, uint64_t nov, const uint64_t *P,
                                const uint64_t *pbeg, uint32_t n, uint32_t levels, uint32_t leaf,
-                               double root_dens, uint64_t *wkeys, uint64_t *cnt) {
+                               double root_dens, uint64_t *wkeys, uint64_t *cnt, WinBits wb) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nov) return;
   uint32_t u = ovl[i];
@@ -347,11 +362,33 @@ __global__ void k_find_windows(const uint32_t *ovl, uint64_t nov, const uint64_t
     double tau = 1.0 - (1.0 - root_dens) * (double)h / (double)levels;
     if ((double)E <= tau * (double)S) {
       wkeys[i] = (a << 6) | (uint64_t)(63 - h);
+      const uint64_t idx = a >> h;
+      atomicOr(wb.mark + wb.base[h] + (idx >> 5), 1u << (idx & 31));
       return;
     }
   }
   wkeys[i] = KEY_INVALID;
   atomicOr((unsigned long long *)&cnt[C_ROOT], 1ull);
+}
+
+// Maximal windows without sorting: aligned windows are nested or disjoint,
+// so a chosen window is maximal exactly when no enclosing range (the same
+// start shifted to every higher level) is chosen; the first overflow vertex
+// to claim a maximal window's emit bit lists it (order is irrelevant: the
+// windows are laid out independently).
+__global__ void k_win_select(const uint64_t *wkeys, uint64_t nov, uint32_t levels, WinBits wb,
+                             uint64_t *mw, unsigned long long *nmw) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nov) return;
+  const uint64_t x = wkeys[i];
+  if (x == KEY_INVALID) return;
+  const uint64_t a = x >> 6;
+  const uint32_t h = 63 - (uint32_t)(x & 63);
+  for (uint32_t h2 = h + 1; h2 <= levels; h2++)
+    if (win_bit(wb.mark, wb, h2, a >> h2)) return;
+  const uint64_t idx = a >> h;
+  const uint32_t bit = 1u << (idx & 31);
+  if (!(atomicOr(wb.emit + wb.base[h] + (idx >> 5), bit) & bit)) mw[atomicAdd(nmw, 1ull)] = x;
 }
 
 struct LoadU64Val {
@@ -382,92 +419,6 @@ __device__ __forceinline__ void window_range(uint64_t x, uint32_t n, uint64_t &a
   b = a + (1ull << h);
   if (b > n) b = n;
 }
-
-// Maximal windows by a prefix maximum instead of per-level searches.
-// Aligned windows are nested or disjoint, and the key order (start
-// ascending, larger window first) puts every enclosing window before the
-// windows it contains, so window i is maximal exactly when its start is at
-// or above the largest end among windows 0..i-1 (a duplicate key fails the
-// test against its twin).  Pass 1: largest end per tile; pass 2 (one CTA):
-// exclusive running maximum over the tiles; pass 3: the running maximum
-// inside each tile and the flag.
-constexpr int WT = 256;  // threads per tile, one key each
-
-__device__ __forceinline__ uint64_t window_end(uint64_t x, uint32_t n) {
-  uint64_t a, b;
-  window_range(x, n, a, b);
-  return b;
-}
-
-__global__ void k_win_tilemax(const uint64_t *w, uint64_t nw, uint32_t n, uint64_t *tmax) {
-  __shared__ uint64_t sh[WT / 32];
-  uint64_t i = (uint64_t)blockIdx.x * WT + threadIdx.x;
-  uint64_t e = i < nw ? window_end(w[i], n) : 0;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) e = max(e, __shfl_xor_sync(0xFFFFFFFFu, e, o));
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = e;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint64_t m = 0;
-    for (int k = 0; k < WT / 32; k++) m = max(m, sh[k]);
-    tmax[blockIdx.x] = m;
-  }
-}
-
-// one CTA: tmax[t] <- max(tmax[0..t-1]) (0 for t = 0), in chunks of WT
-__global__ void k_win_tilescan(uint64_t *tmax, uint64_t nt) {
-  __shared__ uint64_t sh[WT / 32];
-  uint64_t carry = 0;
-  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (uint64_t base = 0; base < nt; base += WT) {
-    uint64_t i = base + threadIdx.x;
-    uint64_t v = i < nt ? tmax[i] : 0;
-    uint64_t inc = v;  // inclusive warp max
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint64_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
-      if ((int)lane >= o) inc = max(inc, t);
-    }
-    if (lane == 31) sh[wid] = inc;
-    __syncthreads();
-    uint64_t before = carry;  // max of earlier warps in this chunk and earlier chunks
-    for (uint32_t k = 0; k < wid; k++) before = max(before, sh[k]);
-    uint64_t excl = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
-    excl = lane ? max(before, excl) : before;
-    uint64_t chunk_max = carry;
-    for (int k = 0; k < WT / 32; k++) chunk_max = max(chunk_max, sh[k]);
-    __syncthreads();
-    if (i < nt) tmax[i] = excl;
-    carry = chunk_max;
-  }
-}
-
-__global__ void k_win_flag(const uint64_t *w, uint64_t nw, uint32_t n, const uint64_t *tprefix,
-                           uint8_t *flag) {
-  __shared__ uint64_t sh[WT / 32];
-  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  uint64_t i = (uint64_t)blockIdx.x * WT + threadIdx.x;
-  uint64_t x = i < nw ? w[i] : 0;
-  uint64_t e = i < nw ? window_end(x, n) : 0;
-  uint64_t inc = e;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint64_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
-    if ((int)lane >= o) inc = max(inc, t);
-  }
-  if (lane == 31) sh[wid] = inc;
-  __syncthreads();
-  uint64_t before = tprefix[blockIdx.x];
-  for (uint32_t k = 0; k < wid; k++) before = max(before, sh[k]);
-  uint64_t excl = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
-  excl = lane ? max(before, excl) : before;
-  if (i < nw) flag[i] = (x >> 6) >= excl ? 1 : 0;
-}
-
-struct ByteFlagPred {
-  const uint8_t *f;
-  __device__ bool operator()(uint64_t i) const { return f[i] != 0; }
-};
 
 // One CTA per maximal window: put its vertices in the rewrite set.
 __global__ void k_window_mark(const uint64_t *mw, uint32_t n, uint32_t *stamp, uint32_t epoch) {
@@ -1078,34 +1029,29 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     if (shrink || (double)t2new > root_d * (double)N) {
       rebuild = true;
     } else {
-      uint64_t *wk = s_wk.ensure(nov), *wk2 = s_wk2.ensure(nov);
+      uint64_t *wk = s_wk.ensure(nov);
+      // level bitmaps (mark, emit), cleared per batch
+      WinBits wb;
+      uint64_t words = 0;
+      for (uint32_t h = 0; h <= levels && h < 34; h++) {
+        wb.base[h] = words;
+        words += ceil_div(ceil_div((uint64_t)n, 1ull << h), 32);
+      }
+      uint32_t *wbits = s_wbits.ensure(2 * words);
+      wb.mark = wbits;
+      wb.emit = wbits + words;
+      TRC_CUDA(cudaMemsetAsync(wbits, 0, 2 * words * 4, stream));
       TRC_LAUNCH(prof, stream, "upd_find_windows", ceil_div(nov, 256), 256, 0, k_find_windows, ovl,
                  nov, P, pbeg.get(), n, levels, std::min(std::max(tuned.pma_leaf_log, 1u), levels),
-                 root_d, wk, cnt);
+                 root_d, wk, cnt, wb);
       // windows are selected before the root flag is read (one sync for
       // both); a root overflow discards them and rebuilds
-      uint64_t *t2 = tmp(radix_tmp_elems(nov) + 4);
-      // window keys: start << 6 | level code, start < 2^vbits
-      int wshifts[8];
-      int nws = 0;
-      for (uint32_t sh = 0; sh < 6 + vbits(); sh += 8) wshifts[nws++] = (int)sh;
-      uint64_t *ws = radix_sort_u64_shifts(wk, wk2, nov, wshifts, nws, t2, stream, prof, err.get());
       uint64_t *mw = s_mw.ensure(nov);
-      const uint64_t wtiles = ceil_div(nov, WT);
-      uint64_t *t3 = tmp(select_tmp_elems(nov) + wtiles + 4);
-      uint64_t *tmx = t3 + select_tmp_elems(nov) + 2;
-      uint8_t *wflag = s_flags.ensure(nov);
-      TRC_LAUNCH(prof, stream, "upd_win_tilemax", wtiles, WT, 0, k_win_tilemax, ws, nov, n, tmx);
-      TRC_LAUNCH(prof, stream, "upd_win_tilescan", 1, WT, 0, k_win_tilescan, tmx, wtiles);
-      TRC_LAUNCH(prof, stream, "upd_win_flag", wtiles, WT, 0, k_win_flag, ws, nov, n, tmx, wflag);
-      select_if(ByteFlagPred{wflag}, LoadU64Val{ws}, nov, mw, cnt + C_NMW, t3, stream, prof,
-                "sel_windows");
+      TRC_LAUNCH(prof, stream, "upd_win_select", ceil_div(nov, 256), 256, 0, k_win_select, wk, nov,
+                 levels, wb, mw, (unsigned long long *)(cnt + C_NMW));
       uint64_t wc[C_COUNT];
-      uint32_t werr = 0;
       TRC_CUDA(cudaMemcpyAsync(wc, cnt, sizeof(wc), cudaMemcpyDeviceToHost, stream));
-      TRC_CUDA(cudaMemcpyAsync(&werr, err.get(), 4, cudaMemcpyDeviceToHost, stream));
       sync();
-      if (werr & ERR_TIMEOUT) throw_error(TRC_ERR_TIMEOUT, "radix sort look-back wait gave up");
       if (wc[C_ROOT]) rebuild = true;
       else nmw = wc[C_NMW];
     }
