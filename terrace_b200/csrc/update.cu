@@ -581,6 +581,51 @@ __global__ void k_scatter_c2_final(const uint32_t *tu, const uint32_t *tc2, uint
 // PMA segment (in place, or to the layout's new position).  About 8 bytes of
 // HBM traffic per list element instead of a gather / global merge / scatter.
 
+// Touched vertices handled by the fused merge: non-hubs that stay <= T.
+struct TouchedSmallPred {
+  const uint32_t *tu, *tdn;
+  const int32_t *hub_of;
+  uint32_t T;
+  __device__ bool operator()(uint64_t t) const { return hub_of[tu[t]] < 0 && tdn[t] <= T; }
+};
+
+struct TouchedVal {
+  const uint32_t *tu;
+  __device__ uint32_t operator()(uint64_t t) const { return tu[t]; }
+};
+
+// One CTA per maximal window: appends the window's members that are not
+// touched but have PMA elements (their segments move) to the rewrite list
+// after the touched ones (count on the device).
+__global__ void k_window_members(const uint64_t *mw, uint32_t n, const uint32_t *tix,
+                                 const int32_t *hub_of, const uint32_t *c2, uint32_t *rs,
+                                 unsigned long long *nrs) {
+  __shared__ uint32_t sh[256 / 32 + 2];
+  uint64_t a, b;
+  window_range(mw[blockIdx.x], n, a, b);
+  for (uint64_t base = a; base < b; base += blockDim.x) {
+    const uint64_t u = base + threadIdx.x;
+    const bool take = u < b && tix[u] == NONE32 && hub_of[u] < 0 && c2[u] > 0;
+    // per-CTA append (every thread of the CTA runs the same iterations)
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, take);
+    if (lane == 0) sh[w] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t t = 0;
+      for (uint32_t k = 0; k < (blockDim.x >> 5); k++) {
+        const uint32_t c = sh[k];
+        sh[k] = t;
+        t += c;
+      }
+      sh[8] = t ? (uint32_t)atomicAdd(nrs, (unsigned long long)t) : 0u;
+    }
+    __syncthreads();
+    if (take) rs[sh[8] + sh[w] + __popc(m & lanemask_lt())] = (uint32_t)u;
+    __syncthreads();
+  }
+}
+
 // Rewrite-set members handled by the fused merge: non-hubs that stay <= T.
 struct SmallPred {
   const uint32_t *stamp;
@@ -1105,10 +1150,17 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   // ---- fused merge for every rewrite vertex that stays in tiers 1-2
   const uint32_t T = cfg.hub_threshold;
   uint32_t *rs = s_rlist.ensure(n);
-  {
+  if (rebuild) {  // every PMA vertex moves: one pass over all vertices
     uint64_t *t4 = tmp(select_tmp_elems(n) + 4);
     select_if(SmallPred{stamp.get(), epoch, hub_of.get(), deg.get(), tix, tdn, T}, IndexVal32{},
               n, rs, cnt + C_NR, t4, stream, prof, "sel_rewrite");
+  } else {  // touched vertices (in vertex order), then untouched window members
+    uint64_t *t4 = tmp(select_tmp_elems(nt) + 4);
+    select_if(TouchedSmallPred{tu, tdn, hub_of.get(), T}, TouchedVal{tu}, nt, rs, cnt + C_NR, t4,
+              stream, prof, "sel_rewrite");
+    if (nmw)
+      TRC_LAUNCH(prof, stream, "upd_window_members", nmw, 256, 0, k_window_members, s_mw.get(), n,
+                 tix, hub_of.get(), c2.get(), rs, (unsigned long long *)(cnt + C_NR));
   }
   // the rewrite list's length stays on the device (read with the final sync)
   const uint64_t *nrs_dev = cnt + C_NR;
