@@ -288,6 +288,10 @@ def run_ours(args, rank, world):
         "roofline": roof,
         "host_phase_ms_per_batch": {k: round(v, 3) for k, v in host_ms.items()},
         "kernel_ms_per_batch": round(total_kernel_ms / args.steps, 3),
+        "batch_sizes_last": {k: sizes[-1][k] for k in ("last_keys", "last_applied", "last_touched",
+                                                       "last_rewritten", "last_gathered",
+                                                       "last_written", "last_windows",
+                                                       "last_rebuild")} if sizes else {},
         "kernel_share": {k: round(v[0] / total_kernel_ms, 4) for k, v in
                          sorted(kernel_ms.items(), key=lambda kv: -kv[1][0])[:12]},
         "analytics_rmat22": analytics22,

@@ -733,7 +733,9 @@ __device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a, 
   uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
   const bool moved = a.wstamp && a.wstamp[u] == a.epoch;
   uint32_t *seg = (moved ? a.mov_pma : a.dst_pma) + a.pbeg_new[u];
-  // elements below the first key keep their place (in place, long lists)
+  // elements below the first key keep their place (in place, long lists);
+  // in place, an element whose rank does not change is not rewritten
+  const bool stay = a.inplace && !moved;
   uint32_t p = 0;
   if (a.inplace && !moved && nb > 0 && d > MF_CH)
     p = warp_list_lower_bound(L, d, (uint32_t)B[0], lane);
@@ -766,7 +768,7 @@ __device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a, 
         uint32_t last = k > 0 ? __shfl_sync(0xFFFFFFFFu, c[k > 0 ? k - 1 : 0], 31) : cbelow;
         if (lane == 0) cp = last;
         if (i < e) {
-          put_rank(row, seg, i + c[k], x[k]);
+          if (c[k] || !stay) put_rank(row, seg, i + c[k], x[k]);
           for (uint32_t j = cp; j < c[k]; j++) put_rank(row, seg, j + i, (uint32_t)B[j]);
         }
       }
@@ -789,7 +791,7 @@ __device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a, 
         uint32_t i = s0 + k * 32 + lane;
         if (i < e) {
           uint32_t cc = lower_bound_keys(B, nb, x[k]);
-          if (!(cc < nb && (uint32_t)B[cc] == x[k])) put_rank(row, seg, i - cc, x[k]);
+          if (!(cc < nb && (uint32_t)B[cc] == x[k]) && (cc || !stay)) put_rank(row, seg, i - cc, x[k]);
         }
       }
       __syncwarp();
