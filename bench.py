@@ -318,7 +318,7 @@ def batched(T, torch, g, stream, n, t_call):
     for v in src:
         t, _ = t_call(lambda: g.bfs(int(v), device=True), reps=1)
         one_bfs += t
-    ms_bc, _ = t_call(lambda: g.msbc(src, device=True), reps=1)
+    ms_bc, _ = t_call(lambda: g.msbc(src, device=True), reps=2)
     torch.cuda.empty_cache()
     one_bc = 0.0
     for v in src:
@@ -521,6 +521,33 @@ def serving_stream(n, count, rng, pool_len, sources):
     return out
 
 
+def serving_submit(srv, kind, x, ps, pd):
+    if kind == "ins":
+        return srv.insert(ps[x[0]:x[0] + x[1]], pd[x[0]:x[0] + x[1]])
+    if kind == "del":
+        return srv.delete(ps[x[0]:x[0] + x[1]], pd[x[0]:x[0] + x[1]])
+    if kind == "bfs":
+        return srv.bfs(x)
+    if kind == "deg":
+        return srv.degree(x)
+    if kind == "nbr":
+        return srv.neighbors(x)
+    return srv.pagerank(x)
+
+
+def serving_warmup(T, g, batched, reqs, ps, pd):
+    """Untimed: the requests as one held burst, then one by one, so buffers
+    grow to a full round and every kernel path has run once."""
+    srv = T.Server(g, batched=batched, summary=True)
+    srv.hold(True)
+    ids = [serving_submit(srv, k, x, ps, pd) for k, x in reqs]
+    srv.hold(False)
+    for rid in ids:
+        srv.wait(rid, 600_000)
+        srv.release(rid)
+    srv.close()
+
+
 def serving_run(T, g, batched, reqs, gaps, rate, ps, pd):
     """Submits reqs at Poisson times (gaps / rate seconds apart), waits for
     all; returns offered / achieved rate and latency percentiles."""
@@ -535,18 +562,7 @@ def serving_run(T, g, batched, reqs, gaps, rate, ps, pd):
             if dt <= 0:
                 break
             time.sleep(min(dt, 0.002))
-        if kind == "ins":
-            ids.append(srv.insert(ps[x[0]:x[0] + x[1]], pd[x[0]:x[0] + x[1]]))
-        elif kind == "del":
-            ids.append(srv.delete(ps[x[0]:x[0] + x[1]], pd[x[0]:x[0] + x[1]]))
-        elif kind == "bfs":
-            ids.append(srv.bfs(x))
-        elif kind == "deg":
-            ids.append(srv.degree(x))
-        elif kind == "nbr":
-            ids.append(srv.neighbors(x))
-        else:
-            ids.append(srv.pagerank(x))
+        ids.append(serving_submit(srv, kind, x, ps, pd))
         kinds.append(kind)
     t_sub = time.perf_counter() - t0
     bad = 0
@@ -584,6 +600,7 @@ def serving(T, torch):
     cfg = SERVE
     n = 1 << cfg["scale"]
     s, d = T.rmat_generate(n, 0, A, B, C, cfg["ef"] * n, device=True)
+
     g = T.Graph(n, hbm_budget=cfg["hbm_budget"])
     m0 = g.add_edge_batch(s, d, symmetrize=True, drop_self_loops=True)
     del s, d
@@ -598,8 +615,19 @@ def serving(T, torch):
                   "10% degree/neighbour lookups, 5% PageRank 10 it; Poisson arrivals seed 3",
            "results": "summaries computed on the device (BFS: reached, depth; PageRank: sum, max)",
            "latency": "host clock, submit to completion", "fifo": [], "batched": []}
+    # warm-up (untimed): a short stream in each mode grows the memory pools
+    # and builds the class lists and CUDA graphs; updates draw from one pool
+    # of 8M pairs, so the graph's growth over the runs stays bounded
+    wrng = np.random.default_rng(cfg["seed"] + 100)
+    wreqs = serving_stream(n, 200, wrng, pool_len, sources)
     for mode in ("fifo", "batched"):
-        for rate in cfg["rates"]:
+        serving_warmup(T, g, mode == "batched", wreqs, ps, pd)
+    # modes interleaved per rate, so both meet the same graph state
+    live = {"fifo": True, "batched": True}
+    for rate in cfg["rates"]:
+        for mode in ("fifo", "batched"):
+            if not live[mode]:
+                continue
             cnt = int(min(max(rate * cfg["seconds"], cfg["min_reqs"]), cfg["max_reqs"]))
             rng = np.random.default_rng(cfg["seed"])
             reqs = serving_stream(n, cnt, rng, pool_len, sources)
@@ -608,7 +636,9 @@ def serving(T, torch):
             out[mode].append(r)
             # stop once the mode no longer keeps up with the offered load
             if r["throughput_rps"] < 0.7 * r["offered_rps"] or r["p99_ms"] > 20_000:
-                break
+                live[mode] = False
+    out["runs"] = ("one graph; untimed warm-up stream per mode; modes interleaved per rate; "
+                   "update pairs from one 8M-pair pool")
     # throughput at equal p99: the SLO is the largest p99 the plain path shows
     # while it keeps up (throughput >= 90% of offered)
     keep = [r for r in out["fifo"] if r["throughput_rps"] >= 0.9 * r["offered_rps"]]
@@ -618,6 +648,17 @@ def serving(T, torch):
         bb = max((r["throughput_rps"] for r in out["batched"] if r["p99_ms"] <= slo), default=0.0)
         out["at_equal_p99"] = {"p99_slo_ms": slo, "fifo_rps": fb, "batched_rps": bb,
                                "batched_over_fifo": bb / fb if fb else None}
+    # the same comparison at fixed p99 targets: the largest throughput each
+    # mode sustains (>= 90 % of offered) with p99 under the target
+    def best(runs, t):
+        ok = [r["throughput_rps"] for r in runs
+              if r["p99_ms"] <= t and r["throughput_rps"] >= 0.9 * r["offered_rps"]]
+        return max(ok, default=0.0)
+    out["at_p99_targets"] = []
+    for t in (100, 150, 200, 250, 500):
+        fb, bb = best(out["fifo"], t), best(out["batched"], t)
+        out["at_p99_targets"].append({"p99_ms": t, "fifo_rps": fb, "batched_rps": bb,
+                                      "batched_over_fifo": bb / fb if fb else None})
     g.close()
     return out
 

@@ -41,7 +41,6 @@ struct MSState {
   uint64_t live;    // sources whose frontier is not empty at this level:
                     // only their bits can still be discovered
   uint32_t level;   // the level being discovered (L+1)
-  uint32_t *active; // count of vertices with new bits
 };
 
 __device__ __forceinline__ void write_levels(const MSState &s, uint64_t v, uint64_t nw) {
@@ -66,9 +65,31 @@ __device__ __forceinline__ void ms_commit(const MSState &s, uint32_t v, uint64_t
   s.next[v] = nw;
   if (nw) {
     s.seen[v] = sv | nw;
-    atomicAdd(s.active, 1u);
     if (s.lvrow) write_levels(s, v, nw);
   }
+}
+
+// List appends with one atomic per CTA (a list counter is one address:
+// per-item or per-warp atomics on it serialise).  Every thread of the CTA
+// must call; returns the thread's slot.
+__device__ __forceinline__ uint32_t cta_append(bool take, uint32_t *counter, uint32_t *sh) {
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t m = __ballot_sync(0xFFFFFFFFu, take);
+  if (lane == 0) sh[w] = __popc(m);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (uint32_t k = 0; k < (blockDim.x >> 5); k++) {
+      const uint32_t c = sh[k];
+      sh[k] = t;
+      t += c;
+    }
+    sh[MT / 32] = t ? atomicAdd(counter, t) : 0u;
+  }
+  __syncthreads();
+  const uint32_t pos = sh[MT / 32] + sh[w] + __popc(m & lanemask_lt());
+  __syncthreads();
+  return pos;
 }
 
 // pull, 4 lanes per inline-only vertex
@@ -133,9 +154,31 @@ __global__ void __launch_bounds__(MT) k_ms_pull_W(DevView G, const uint32_t *V, 
 // accumulator appends the neighbour to the touched list T.  The warp clears
 // front[u] after reading it (nothing else reads front in a push level), so
 // that front is all-zero when the level ends.
+// One 32-neighbour chunk of a pushing vertex with source mask m.
+__device__ __forceinline__ void ms_push_chunk(const NbrList &L, uint64_t m, uint32_t j0,
+                                              const uint64_t *seen, unsigned long long *acc,
+                                              uint32_t *T, uint32_t *tcnt, uint32_t lane) {
+  const uint32_t j = j0 + lane;
+  uint32_t x = 0;
+  bool first = false;
+  if (j < L.deg) {
+    x = L.at(j);
+    if ((m & ~seen[x]) != 0) first = atomicOr(acc + x, (unsigned long long)m) == 0;
+  }
+  const uint32_t b = __ballot_sync(0xFFFFFFFFu, first);
+  uint32_t base = 0;
+  if (b) {
+    if (lane == 0) base = atomicAdd(tcnt, __popc(b));
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+  }
+  if (first) T[base + __popc(b & lanemask_lt())] = x;
+}
+
+// Warp per active vertex; hubs are listed (with their masks) for
+// k_ms_push_hubs.
 __global__ void k_ms_push(DevView G, const uint32_t *F, uint32_t nf, uint64_t *front,
                           const uint64_t *seen, unsigned long long *acc, uint32_t *T,
-                          uint32_t *tcnt) {
+                          uint32_t *tcnt, uint32_t *hu, uint64_t *hm, uint32_t *hcnt) {
   uint64_t w = ((uint64_t)blockIdx.x * MT + threadIdx.x) >> 5;
   uint32_t lane = threadIdx.x & 31;
   if (w >= nf) return;
@@ -143,11 +186,38 @@ __global__ void k_ms_push(DevView G, const uint32_t *F, uint32_t nf, uint64_t *f
   uint64_t m = front[u];
   __syncwarp();
   if (lane == 0) front[u] = 0;
+  if (G.hub_of[u] >= 0) {
+    if (lane == 0) {
+      const uint32_t i = atomicAdd(hcnt, 1u);
+      hu[i] = u;
+      hm[i] = m;
+    }
+    return;
+  }
   NbrList L = nbr_list(G, u);
-  for (uint32_t j = lane; j < L.deg; j += 32) {
-    uint32_t x = L.at(j);
-    if ((m & ~seen[x]) == 0) continue;
-    if (atomicOr(acc + x, (unsigned long long)m) == 0) T[atomicAdd(tcnt, 1u)] = x;
+  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) ms_push_chunk(L, m, j0, seen, acc, T, tcnt, lane);
+}
+
+// The listed hubs: the first 64 spread over the grid, the rest a CTA each.
+__global__ void k_ms_push_hubs(DevView G, const uint32_t *hu, const uint64_t *hm,
+                               const uint32_t *hcnt, const uint64_t *seen,
+                               unsigned long long *acc, uint32_t *T, uint32_t *tcnt) {
+  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint64_t gw = ((uint64_t)blockIdx.x * MT + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * MT) >> 5;
+  const uint64_t nh = *hcnt;
+  const uint64_t nwide = nh < 64 ? nh : 64;
+  for (uint64_t i = 0; i < nwide; i++) {
+    NbrList L = nbr_list(G, hu[i]);
+    const uint64_t nch = (L.deg + 31) >> 5;
+    for (uint64_t c = gw; c < nch; c += nwarps)
+      ms_push_chunk(L, hm[i], (uint32_t)(c << 5), seen, acc, T, tcnt, lane);
+  }
+  for (uint64_t i = nwide + blockIdx.x; i < nh; i += gridDim.x) {
+    NbrList L = nbr_list(G, hu[i]);
+    const uint32_t nch = (L.deg + 31) >> 5;
+    for (uint32_t c = wib; c < nch; c += MT / 32)
+      ms_push_chunk(L, hm[i], c << 5, seen, acc, T, tcnt, lane);
   }
 }
 
@@ -157,13 +227,15 @@ __global__ void k_ms_push(DevView G, const uint32_t *F, uint32_t nf, uint64_t *f
 __global__ void k_ms_commit_list(MSState s, const uint32_t *T, const uint32_t *tcnt,
                                  unsigned long long *acc, uint32_t *list, uint32_t *list_cnt,
                                  unsigned long long *any) {
+  __shared__ uint32_t sh[MT / 32 + 2];
   const uint32_t nt = *tcnt;
   const uint64_t stride = (uint64_t)gridDim.x * MT;
   for (uint64_t base = (uint64_t)blockIdx.x * MT; base < nt; base += stride) {
     uint64_t i = base + threadIdx.x;
     uint64_t nw = 0;
+    uint32_t v = 0;
     if (i < nt) {
-      uint32_t v = T[i];
+      v = T[i];
       uint64_t a = acc[v];
       acc[v] = 0;
       uint64_t sv = s.seen[v];
@@ -171,10 +243,11 @@ __global__ void k_ms_commit_list(MSState s, const uint32_t *T, const uint32_t *t
       if (nw) {
         s.seen[v] = sv | nw;
         s.next[v] = nw;
-        list[atomicAdd(list_cnt, 1u)] = v;
         if (s.lvrow) write_levels(s, v, nw);
       }
     }
+    const uint32_t pos = cta_append(nw != 0, list_cnt, sh);
+    if (nw) list[pos] = v;
     warp_or_into(nw, any);
   }
 }
@@ -190,9 +263,11 @@ __global__ void k_ms_clear(uint64_t *front, const uint32_t *F, uint32_t nf) {
 // that discovered a vertex at this level
 __global__ void k_ms_collect(uint32_t n, const uint64_t *front, uint32_t *list, uint32_t *cnt,
                              unsigned long long *any) {
+  __shared__ uint32_t sh[MT / 32 + 2];
   uint64_t v = (uint64_t)blockIdx.x * MT + threadIdx.x;
   uint64_t f = v < n ? front[v] : 0;
-  if (f) list[atomicAdd(cnt, 1u)] = (uint32_t)v;
+  const uint32_t pos = cta_append(f != 0, cnt, sh);
+  if (f) list[pos] = (uint32_t)v;
   if (any) warp_or_into(f, any);
 }
 
@@ -426,7 +501,13 @@ void Graph::msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uin
   tl.bind(&budget);
   uint32_t *L[2] = {lst.alloc_exact(n), lst2.alloc_exact(n)};
   uint32_t *T = tl.alloc_exact(n);
-  uint32_t *c = cnt.alloc_exact(4);  // [0] pull commits, [1] next active, [2] touched
+  uint32_t *c = cnt.alloc_exact(4);  // [1] next active, [2] touched, [3] pushing hubs
+  DBuf<uint32_t> hub_u;
+  DBuf<uint64_t> hub_m;
+  hub_u.bind(&budget);
+  hub_m.bind(&budget);
+  uint32_t *hu = hub_u.alloc_exact(H ? H : 1);  // hubs of a push level and their masks
+  uint64_t *hm = hub_m.alloc_exact(H ? H : 1);
   TRC_CUDA(cudaMemcpyAsync(dsrc, hsrc.data(), k * 4, cudaMemcpyHostToDevice, stream));
   TRC_LAUNCH(prof, stream, "ms_init", ceil_div(n, MT), MT, 0, k_ms_init, n, k, dsrc, seen, front,
              next, lvrow, acc);
@@ -448,7 +529,7 @@ void Graph::msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uin
     level++;
     TRC_CUDA(cudaMemsetAsync(c, 0, 16, stream));
     TRC_CUDA(cudaMemsetAsync(any, 0, 8, stream));
-    MSState s{seen, front, next, lvrow, k, live, level, c};
+    MSState s{seen, front, next, lvrow, k, live, level};
     uint32_t *nl = L[cur ^ 1];
     if ((uint64_t)nact >= dense_at && dense_at > 0) {
       TRC_LAUNCH(prof, stream, "ms_pull_S", ceil_div(lists.nS * 4, MT), MT, 0, k_ms_pull_S, G,
@@ -464,7 +545,10 @@ void Graph::msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uin
                  nact);
     } else {
       TRC_LAUNCH(prof, stream, "ms_push", ceil_div((uint64_t)nact * 32, MT), MT, 0, k_ms_push, G,
-                 L[cur], nact, front, seen, acc, T, c + 2);
+                 L[cur], nact, front, seen, acc, T, c + 2, hu, hm, c + 3);
+      if (H)
+        TRC_LAUNCH(prof, stream, "ms_push_hubs", (unsigned)num_sms() * 8, MT, 0, k_ms_push_hubs, G,
+                   hu, hm, c + 3, seen, acc, T, c + 2);
       TRC_LAUNCH(prof, stream, "ms_commit", commit_grid, MT, 0, k_ms_commit_list, s, T, c + 2,
                  acc, nl, c + 1, any);
     }
@@ -564,7 +648,13 @@ void Graph::msbc(const uint32_t *sources, uint32_t k, double *out_user, uint32_t
   uint32_t *dsrc = srcb.alloc_exact(k);
   uint32_t *L[2] = {lst.alloc_exact(n), lst2.alloc_exact(n)};
   uint32_t *T = tl.alloc_exact(n);
-  uint32_t *c = cnt.alloc_exact(4);  // [0] pull commits, [1] next active, [2] touched
+  uint32_t *c = cnt.alloc_exact(4);  // [1] next active, [2] touched, [3] pushing hubs
+  DBuf<uint32_t> hub_u;
+  DBuf<uint64_t> hub_m;
+  hub_u.bind(&budget);
+  hub_m.bind(&budget);
+  uint32_t *hu = hub_u.alloc_exact(H ? H : 1);  // hubs of a push level and their masks
+  uint64_t *hm = hub_m.alloc_exact(H ? H : 1);
   DBuf<uint64_t> anyb;
   anyb.bind(&budget);
   unsigned long long *any = (unsigned long long *)anyb.alloc_exact(1);
@@ -598,7 +688,7 @@ void Graph::msbc(const uint32_t *sources, uint32_t k, double *out_user, uint32_t
     level++;
     TRC_CUDA(cudaMemsetAsync(c, 0, 16, stream));
     TRC_CUDA(cudaMemsetAsync(any, 0, 8, stream));
-    MSState s{seen, front, next, nullptr, k, live, level, c};
+    MSState s{seen, front, next, nullptr, k, live, level};
     uint32_t *nl = L[cur ^ 1];
     const uint64_t base = loff.back();
     lv.reserve(base + n, base, stream);
@@ -613,7 +703,10 @@ void Graph::msbc(const uint32_t *sources, uint32_t k, double *out_user, uint32_t
                  c + 1, any);
     } else {
       TRC_LAUNCH(prof, stream, "ms_push", ceil_div((uint64_t)nact * 32, MT), MT, 0, k_ms_push, G,
-                 L[cur], nact, front, seen, acc, T, c + 2);
+                 L[cur], nact, front, seen, acc, T, c + 2, hu, hm, c + 3);
+      if (H)
+        TRC_LAUNCH(prof, stream, "ms_push_hubs", (unsigned)num_sms() * 8, MT, 0, k_ms_push_hubs, G,
+                   hu, hm, c + 3, seen, acc, T, c + 2);
       TRC_LAUNCH(prof, stream, "ms_commit", pgrid, MT, 0, k_ms_commit_list, s, T, c + 2, acc, nl,
                  c + 1, any);
       // the push cleared front; restore this level's masks for sigma
