@@ -179,8 +179,12 @@ def run_ours(args, rank, world):
     inserted = sum(ins)
     value = inserted * world / (ins_ms / 1e3)
     pairs_per_s = BATCH * args.steps * world / (ins_ms / 1e3)
+    del_ms, dels = timed(lambda i: g.remove_edge_batch(*batches[args.warmup + i], symmetrize=True,
+                                                       drop_self_loops=True), args.steps)
+    deleted = sum(dels)
     # ---- e2e: same metric through the public API with pinned HOST buffers,
-    # K fresh batches right after the timed ones (same graph state)
+    # K fresh batches on the graph the timed inserts started from (their
+    # deletion restored it), so both meet the same PMA fill
     host = []
     for j in range(args.steps):
         hs = torch.empty(BATCH, dtype=torch.int32, pin_memory=True)
@@ -193,10 +197,6 @@ def run_ours(args, rank, world):
     e2e_cnt = [g.add_edge_batch(hs, hd, symmetrize=True, drop_self_loops=True) for hs, hd in host]
     e2e_s = time.perf_counter() - t0
     e2e_val = sum(e2e_cnt) * world / e2e_s
-
-    del_ms, dels = timed(lambda i: g.remove_edge_batch(*batches[args.warmup + i], symmetrize=True,
-                                                       drop_self_loops=True), args.steps)
-    deleted = sum(dels)
     for hs, hd in host:
         g.remove_edge_batch(hs, hd, symmetrize=True, drop_self_loops=True)
 
