@@ -55,8 +55,10 @@ typedef struct {
                                  in 48 KB of shared memory when merged). */
   double pma_root_density;    /* upper density bound at the PMA root;
                                  reference 0.75 (src/PMA.cc:382-394). */
-  double pma_build_density;   /* density after a full PMA rebuild.
-                                 Default 0.5. */
+  double pma_build_density;   /* density after a full PMA rebuild.  Default
+                                 0.375: the reference doubles its array when
+                                 the root passes 0.75 (double_list,
+                                 src/PMA.cc:659-720). */
   double hub_block_fill;      /* fill of hub blocks after a rewrite.
                                  Default 0.75. */
   uint32_t push_pull_divisor; /* edgeMap goes dense when |F| >= n/divisor;

@@ -55,7 +55,7 @@ void trc_config_default(trc_config *cfg) {
   if (!cfg) return;
   cfg->hub_threshold = 1024;
   cfg->pma_root_density = 0.75;
-  cfg->pma_build_density = 0.5;
+  cfg->pma_build_density = 0.375;
   cfg->hub_block_fill = 0.75;
   cfg->push_pull_divisor = 20;
   cfg->hub_stage_limit = 49152;

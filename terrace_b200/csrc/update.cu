@@ -1061,7 +1061,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   uint32_t *c2n = nullptr;
   uint64_t *P = nullptr;
   const double root_d = (cfg.pma_root_density > 0 && cfg.pma_root_density < 1) ? cfg.pma_root_density : 0.75;
-  const double build_d = (cfg.pma_build_density > 0 && cfg.pma_build_density < 1) ? cfg.pma_build_density : 0.5;
+  const double build_d = (cfg.pma_build_density > 0 && cfg.pma_build_density < 1) ? cfg.pma_build_density : 0.375;
   uint32_t levels = 1;
   while (levels < 32 && (1ull << levels) < (uint64_t)n) levels++;
   bool shrink = !insert && N > (1ull << 20) && (double)t2new < 0.125 * (double)N;

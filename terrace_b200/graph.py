@@ -33,7 +33,7 @@ def _arr(x, dtype):
 
 
 def _config(hub_threshold: int = 1024, pma_root_density: float = 0.75,
-            pma_build_density: float = 0.5, hub_block_fill: float = 0.75,
+            pma_build_density: float = 0.375, hub_block_fill: float = 0.75,
             push_pull_divisor: int = 20, hub_stage_limit: int = 49152,
             cuda_graphs: bool = True):
     lib = L.load()

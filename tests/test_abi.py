@@ -56,7 +56,7 @@ def test_config_defaults_match_reference_constants(lib):
     assert cfg.hub_threshold == 1024          # MEDIUM_DEGREE, include/graph.h:39
     assert cfg.push_pull_divisor == 20        # edgeMap threshold, include/Map.cpp:65-74
     assert abs(cfg.pma_root_density - 0.75) < 1e-12
-    assert abs(cfg.pma_build_density - 0.5) < 1e-12
+    assert abs(cfg.pma_build_density - 0.375) < 1e-12
     assert cfg.cuda_graphs == 1
 
 
