@@ -157,6 +157,9 @@ class Graph {
 
  private:
   void grow_hub_tables(uint32_t need);
+  // pinned staging for the classify counts and the touched hubs' records
+  static constexpr uint64_t HUB_SPEC = 4096;
+  uint32_t *hub_stage_ = nullptr;
   void grow_pool(uint64_t need_blocks);
   uint64_t *tmp(uint64_t elems) { return s_tmp.ensure(elems); }
 };

@@ -91,6 +91,8 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   grow_hub_tables(64);
   grow_pool(64);
   sync();
+  // last, so that nothing after it can throw out of the constructor
+  TRC_CUDA(cudaMallocHost(&hub_stage_, 256 + 4 * 4 * HUB_SPEC));  // 32 counters, 4 hub arrays
 }
 
 Graph::~Graph() {
@@ -101,6 +103,7 @@ Graph::~Graph() {
   // the members free after this body, on the legacy stream (the work on
   // the graph's streams has finished)
   budget.stream = nullptr;
+  if (hub_stage_) cudaFreeHost(hub_stage_);
   if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -994,8 +997,22 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   int32_t *hw_h = s_hw_h.ensure(nt);
   TRC_LAUNCH(prof, stream, "upd_classify", ceil_div(nt, 256), 256, 0, k_classify, G, bkeys, tpos,
              nt, kb, insert ? 1 : 0, tu, tdn, tc2, ovl, hw_u, hw_dn, hw_t, hw_h, s_hw_do.ensure(nt), cnt);
-  TRC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, stream));
+  // the counts and (speculatively) the first HUB_SPEC touched-hub records in
+  // one copy to pinned staging and one synchronisation; more hubs than that
+  // take a second copy
+  const uint64_t spec = std::min<uint64_t>(nt, HUB_SPEC);
+  uint32_t *sp = hub_stage_ + 64;  // after the 32 counters
+  static_assert(C_COUNT <= 32, "counter staging");
+  TRC_CUDA(cudaMemcpyAsync(hub_stage_, cnt, sizeof(hc), cudaMemcpyDeviceToHost, stream));
+  {
+    const uint32_t *src4[4] = {hw_u, hw_dn, (const uint32_t *)hw_h, s_hw_do.get()};
+    for (int a = 0; a < 4; a++)
+      if (spec)
+        TRC_CUDA(cudaMemcpyAsync(sp + a * HUB_SPEC, src4[a], spec * 4, cudaMemcpyDeviceToHost,
+                                 stream));
+  }
   sync();
+  memcpy(hc, hub_stage_, sizeof(hc));
   const uint64_t nov = hc[C_NOV], nh = hc[C_NH];
   const int64_t t2delta = (int64_t)hc[C_T2DELTA];
   const uint64_t t2new = (uint64_t)((int64_t)tier2_total + t2delta);
@@ -1008,11 +1025,18 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   if (nh) {
     std::vector<uint32_t> hu(nh), hdn(nh), hdo(nh);
     std::vector<int32_t> hh(nh);
-    TRC_CUDA(cudaMemcpyAsync(hu.data(), hw_u, nh * 4, cudaMemcpyDeviceToHost, stream));
-    TRC_CUDA(cudaMemcpyAsync(hdn.data(), hw_dn, nh * 4, cudaMemcpyDeviceToHost, stream));
-    TRC_CUDA(cudaMemcpyAsync(hh.data(), hw_h, nh * 4, cudaMemcpyDeviceToHost, stream));
-    TRC_CUDA(cudaMemcpyAsync(hdo.data(), s_hw_do.get(), nh * 4, cudaMemcpyDeviceToHost, stream));
-    sync();
+    if (nh <= spec) {
+      memcpy(hu.data(), sp, nh * 4);
+      memcpy(hdn.data(), sp + HUB_SPEC, nh * 4);
+      memcpy(hh.data(), sp + 2 * HUB_SPEC, nh * 4);
+      memcpy(hdo.data(), sp + 3 * HUB_SPEC, nh * 4);
+    } else {
+      TRC_CUDA(cudaMemcpyAsync(hu.data(), hw_u, nh * 4, cudaMemcpyDeviceToHost, stream));
+      TRC_CUDA(cudaMemcpyAsync(hdn.data(), hw_dn, nh * 4, cudaMemcpyDeviceToHost, stream));
+      TRC_CUDA(cudaMemcpyAsync(hh.data(), hw_h, nh * 4, cudaMemcpyDeviceToHost, stream));
+      TRC_CUDA(cudaMemcpyAsync(hdo.data(), s_hw_do.get(), nh * 4, cudaMemcpyDeviceToHost, stream));
+      sync();
+    }
     for (uint64_t i = 0; i < nh; i++) {
       hub_max_old = std::max(hub_max_old, hdo[i]);
       hub_old_total += hdo[i];
