@@ -350,11 +350,11 @@ __device__ __forceinline__ bool win_bit(const uint32_t *bits, const WinBits &wb,
 // Window search (step 5): lowest level (from the leaf level, 2^leaf vertex
 // segments) whose aligned vertex range has density within its bound; its
 // key is (start << 6 | 63 - level) and its bit is set in the level bitmap.
-__global__ void k_find_windows(const uint32_t *ovl, uint64_t nov, const uint64_t *P,
+__global__ void k_find_windows(const uint32_t *ovl, const uint64_t *nov, const uint64_t *P,
                                const uint64_t *pbeg, uint32_t n, uint32_t levels, uint32_t leaf,
                                double root_dens, uint64_t *wkeys, uint64_t *cnt, WinBits wb) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nov) return;
+  if (i >= *nov) return;
   uint32_t u = ovl[i];
   for (uint32_t h = leaf; h <= levels; h++) {
     uint64_t a = ((uint64_t)u >> h) << h;
@@ -379,10 +379,10 @@ __global__ void k_find_windows(const uint32_t *ovl, uint64_t nov, const uint64_t
 // start shifted to every higher level) is chosen; the first overflow vertex
 // to claim a maximal window's emit bit lists it (order is irrelevant: the
 // windows are laid out independently).
-__global__ void k_win_select(const uint64_t *wkeys, uint64_t nov, uint32_t levels, WinBits wb,
+__global__ void k_win_select(const uint64_t *wkeys, const uint64_t *nov, uint32_t levels, WinBits wb,
                              uint64_t *mw, unsigned long long *nmw) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nov) return;
+  if (i >= *nov) return;
   const uint64_t x = wkeys[i];
   if (x == KEY_INVALID) return;
   const uint64_t a = x >> 6;
@@ -938,6 +938,11 @@ struct KeyInListPred {
   }
 };
 
+// Batches touching at least this many vertices search PMA windows before
+// the classify counts are read (one synchronisation less; the O(n) prefix of
+// the tier-2 counts is then computed even when no vertex overflows).
+constexpr uint64_t PLAN_SPECULATE = 1u << 16;
+
 // Largest old hub list the fused hub merge stages in shared memory (~192 KB).
 constexpr uint32_t HUB_SMEM_ELEMS = 48 * 1024;
 
@@ -997,6 +1002,53 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   int32_t *hw_h = s_hw_h.ensure(nt);
   TRC_LAUNCH(prof, stream, "upd_classify", ceil_div(nt, 256), 256, 0, k_classify, G, bkeys, tpos,
              nt, kb, insert ? 1 : 0, tu, tdn, tc2, ovl, hw_u, hw_dn, hw_t, hw_h, s_hw_do.ensure(nt), cnt);
+  // ---- PMA planning inputs: the new tier-2 counts c2n, their prefix P, and
+  // (large batches) the window search on the device-side overflow count,
+  // before the synchronisation that reads the counts; a rebuild decided
+  // after it discards the windows
+  const uint32_t T_levels = [&] {
+    uint32_t l = 1;
+    while (l < 32 && (1ull << l) < (uint64_t)n) l++;
+    return l;
+  }();
+  const double root_d = (cfg.pma_root_density > 0 && cfg.pma_root_density < 1) ? cfg.pma_root_density : 0.75;
+  uint32_t *c2n = nullptr;
+  uint64_t *P = nullptr;
+  auto plan_prefix = [&] {
+    c2n = s_c2n.ensure(n);
+    TRC_CUDA(cudaMemcpyAsync(c2n, c2.get(), (uint64_t)n * 4, cudaMemcpyDeviceToDevice, stream));
+    TRC_LAUNCH(prof, stream, "upd_scatter_c2", ceil_div(nt, 256), 256, 0, k_scatter_c2, tu, tc2, nt,
+               c2n);
+    P = s_P.ensure((uint64_t)n + 1);
+    uint64_t *st = tmp(scan_tmp_elems(n) + 4);
+    exclusive_scan(LoadC2{c2n}, n, P, st, stream, prof, "scan_c2");
+  };
+  auto plan_windows = [&](uint64_t cap) {  // cap >= the overflow count on the device
+    uint64_t *wk = s_wk.ensure(cap);
+    // level bitmaps (mark, emit), cleared per batch
+    WinBits wb;
+    uint64_t words = 0;
+    for (uint32_t h = 0; h <= T_levels && h < 34; h++) {
+      wb.base[h] = words;
+      words += ceil_div(ceil_div((uint64_t)n, 1ull << h), 32);
+    }
+    uint32_t *wbits = s_wbits.ensure(2 * words);
+    wb.mark = wbits;
+    wb.emit = wbits + words;
+    TRC_CUDA(cudaMemsetAsync(wbits, 0, 2 * words * 4, stream));
+    TRC_LAUNCH(prof, stream, "upd_find_windows", ceil_div(cap, 256), 256, 0, k_find_windows, ovl,
+               cnt + C_NOV, P, pbeg.get(), n, T_levels,
+               std::min(std::max(tuned.pma_leaf_log, 1u), T_levels), root_d, wk, cnt, wb);
+    uint64_t *mw = s_mw.ensure(cap);
+    TRC_LAUNCH(prof, stream, "upd_win_select", ceil_div(cap, 256), 256, 0, k_win_select, wk,
+               cnt + C_NOV, T_levels, wb, mw, (unsigned long long *)(cnt + C_NMW));
+  };
+  const bool speculate = nt >= PLAN_SPECULATE;
+  if (speculate) {
+    plan_prefix();
+    plan_windows(nt);
+  }
+
   // the counts and (speculatively) the first HUB_SPEC touched-hub records in
   // one copy to pinned staging and one synchronisation; more hubs than that
   // take a second copy
@@ -1082,44 +1134,19 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   bool rebuild = false;
   uint64_t nmw = 0;
   uint64_t Nn = N;
-  uint32_t *c2n = nullptr;
-  uint64_t *P = nullptr;
-  const double root_d = (cfg.pma_root_density > 0 && cfg.pma_root_density < 1) ? cfg.pma_root_density : 0.75;
   const double build_d = (cfg.pma_build_density > 0 && cfg.pma_build_density < 1) ? cfg.pma_build_density : 0.375;
-  uint32_t levels = 1;
-  while (levels < 32 && (1ull << levels) < (uint64_t)n) levels++;
   bool shrink = !insert && N > (1ull << 20) && (double)t2new < 0.125 * (double)N;
   if (nov > 0 || shrink) {
-    c2n = s_c2n.ensure(n);
-    TRC_CUDA(cudaMemcpyAsync(c2n, c2.get(), (uint64_t)n * 4, cudaMemcpyDeviceToDevice, stream));
-    TRC_LAUNCH(prof, stream, "upd_scatter_c2", ceil_div(nt, 256), 256, 0, k_scatter_c2, tu, tc2, nt,
-               c2n);
-    P = s_P.ensure((uint64_t)n + 1);
-    uint64_t *st = tmp(scan_tmp_elems(n) + 4);
-    exclusive_scan(LoadC2{c2n}, n, P, st, stream, prof, "scan_c2");
+    if (!speculate) plan_prefix();
     if (shrink || (double)t2new > root_d * (double)N) {
       rebuild = true;
+    } else if (speculate) {  // windows already searched; their counts came with hc
+      if (hc[C_ROOT]) rebuild = true;
+      else nmw = hc[C_NMW];
     } else {
-      uint64_t *wk = s_wk.ensure(nov);
-      // level bitmaps (mark, emit), cleared per batch
-      WinBits wb;
-      uint64_t words = 0;
-      for (uint32_t h = 0; h <= levels && h < 34; h++) {
-        wb.base[h] = words;
-        words += ceil_div(ceil_div((uint64_t)n, 1ull << h), 32);
-      }
-      uint32_t *wbits = s_wbits.ensure(2 * words);
-      wb.mark = wbits;
-      wb.emit = wbits + words;
-      TRC_CUDA(cudaMemsetAsync(wbits, 0, 2 * words * 4, stream));
-      TRC_LAUNCH(prof, stream, "upd_find_windows", ceil_div(nov, 256), 256, 0, k_find_windows, ovl,
-                 nov, P, pbeg.get(), n, levels, std::min(std::max(tuned.pma_leaf_log, 1u), levels),
-                 root_d, wk, cnt, wb);
       // windows are selected before the root flag is read (one sync for
       // both); a root overflow discards them and rebuilds
-      uint64_t *mw = s_mw.ensure(nov);
-      TRC_LAUNCH(prof, stream, "upd_win_select", ceil_div(nov, 256), 256, 0, k_win_select, wk, nov,
-                 levels, wb, mw, (unsigned long long *)(cnt + C_NMW));
+      plan_windows(nov);
       uint64_t wc[C_COUNT];
       TRC_CUDA(cudaMemcpyAsync(wc, cnt, sizeof(wc), cudaMemcpyDeviceToHost, stream));
       sync();
