@@ -226,7 +226,10 @@ __global__ void k_filter_flags(DevView G, const uint64_t *keys, uint64_t k2, int
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= k2) return;
   uint64_t x = keys[i];
-  bool keep = x != KEY_INVALID && (i == 0 || keys[i - 1] != x);
+  // (ids checked against n too: a key that is not a valid edge never passes,
+  // whatever an upstream failure left in the buffer)
+  bool keep = x != KEY_INVALID && (x >> 32) < G.n && (uint32_t)x < G.n &&
+              (i == 0 || keys[i - 1] != x);
   if (keep) {
     bool has = has_edge(G, (uint32_t)(x >> 32), (uint32_t)x);
     keep = insert ? !has : has;
@@ -280,10 +283,11 @@ __device__ __forceinline__ uint64_t warp_append64(bool take, unsigned long long 
 }
 
 // Classify touched vertices (step 4).
-__global__ void k_classify(DevView G, const uint64_t *bkeys, const uint64_t *tpos, uint64_t nt,
-                           uint64_t kb, int insert, uint32_t *tu, uint32_t *tdn, uint32_t *tc2,
-                           uint32_t *ovl, uint32_t *hw_u, uint32_t *hw_dn, uint32_t *hw_t,
-                           int32_t *hw_h, uint32_t *hw_do, uint64_t *cnt) {
+__global__ void k_classify(DevView G, const uint64_t *bkeys, const uint64_t *tpos, int insert,
+                           uint32_t *tu, uint32_t *tdn, uint32_t *tc2, uint32_t *ovl,
+                           uint32_t *hw_u, uint32_t *hw_dn, uint32_t *hw_t, int32_t *hw_h,
+                           uint32_t *hw_do, uint64_t *cnt) {
+  const uint64_t nt = cnt[C_NT], kb = cnt[C_KB];  // on the device: no synchronisation before
   uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   bool valid = t < nt;
   uint32_t u = 0, dn = 0, d = 0;
@@ -324,9 +328,10 @@ __global__ void k_classify(DevView G, const uint64_t *bkeys, const uint64_t *tpo
   }
 }
 
-__global__ void k_scatter_c2(const uint32_t *tu, const uint32_t *tc2, uint64_t nt, uint32_t *c2n) {
+__global__ void k_scatter_c2(const uint32_t *tu, const uint32_t *tc2, const uint64_t *nt,
+                             uint32_t *c2n) {
   uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < nt) c2n[tu[t]] = tc2[t];
+  if (t < *nt) c2n[tu[t]] = tc2[t];
 }
 
 struct LoadC2 {
@@ -981,27 +986,18 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   uint64_t *tpos = s_C.ensure(k2);
   select_if(RunStartPred{bkeys, cnt + C_KB}, IndexVal{}, k2, tpos, cnt + C_NT, t, stream, prof,
             "sel_runs");
-  uint64_t hc[C_COUNT];
-  uint32_t herr = 0;
-  TRC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, stream));
-  TRC_CUDA(cudaMemcpyAsync(&herr, err.get(), 4, cudaMemcpyDeviceToHost, stream));
-  sync();
-  if (herr & ERR_BAD_VERTEX) throw_error(TRC_ERR_INVALID, "vertex id out of range [0, n)");
-  if (herr & ERR_TIMEOUT) throw_error(TRC_ERR_TIMEOUT, "radix sort look-back wait gave up");
   phase("sort_filter");
-  const uint64_t kb = hc[C_KB], nt = hc[C_NT];
-  if (kb == 0) {
-    for (auto &x : last) x = 0;
-    last[0] = k2;
-    return 0;
-  }
-
-  uint32_t *tu = s_tu.ensure(nt), *tdn = s_tdn.ensure(nt), *tc2 = s_tc2.ensure(nt);
-  uint32_t *ovl = s_ovl.ensure(nt);
-  uint32_t *hw_u = s_hw_u.ensure(nt), *hw_dn = s_hw_dn.ensure(nt), *hw_t = s_hw_t.ensure(nt);
-  int32_t *hw_h = s_hw_h.ensure(nt);
-  TRC_LAUNCH(prof, stream, "upd_classify", ceil_div(nt, 256), 256, 0, k_classify, G, bkeys, tpos,
-             nt, kb, insert ? 1 : 0, tu, tdn, tc2, ovl, hw_u, hw_dn, hw_t, hw_h, s_hw_do.ensure(nt), cnt);
+  // ---- classify on the device-side counts (no synchronisation here: the
+  // batch's counts, the error word and the plan inputs are read together
+  // after it; nothing modifies the graph before that read)
+  uint64_t hc[C_COUNT];
+  const uint64_t cap = std::min<uint64_t>(k2, n);  // touched vertices <= both
+  uint32_t *tu = s_tu.ensure(cap), *tdn = s_tdn.ensure(cap), *tc2 = s_tc2.ensure(cap);
+  uint32_t *ovl = s_ovl.ensure(cap);
+  uint32_t *hw_u = s_hw_u.ensure(cap), *hw_dn = s_hw_dn.ensure(cap), *hw_t = s_hw_t.ensure(cap);
+  int32_t *hw_h = s_hw_h.ensure(cap);
+  TRC_LAUNCH(prof, stream, "upd_classify", ceil_div(cap, 256), 256, 0, k_classify, G, bkeys, tpos,
+             insert ? 1 : 0, tu, tdn, tc2, ovl, hw_u, hw_dn, hw_t, hw_h, s_hw_do.ensure(cap), cnt);
   // ---- PMA planning inputs: the new tier-2 counts c2n, their prefix P, and
   // (large batches) the window search on the device-side overflow count,
   // before the synchronisation that reads the counts; a rebuild decided
@@ -1017,8 +1013,8 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   auto plan_prefix = [&] {
     c2n = s_c2n.ensure(n);
     TRC_CUDA(cudaMemcpyAsync(c2n, c2.get(), (uint64_t)n * 4, cudaMemcpyDeviceToDevice, stream));
-    TRC_LAUNCH(prof, stream, "upd_scatter_c2", ceil_div(nt, 256), 256, 0, k_scatter_c2, tu, tc2, nt,
-               c2n);
+    TRC_LAUNCH(prof, stream, "upd_scatter_c2", ceil_div(cap, 256), 256, 0, k_scatter_c2, tu, tc2,
+               cnt + C_NT, c2n);
     P = s_P.ensure((uint64_t)n + 1);
     uint64_t *st = tmp(scan_tmp_elems(n) + 4);
     exclusive_scan(LoadC2{c2n}, n, P, st, stream, prof, "scan_c2");
@@ -1043,19 +1039,20 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     TRC_LAUNCH(prof, stream, "upd_win_select", ceil_div(cap, 256), 256, 0, k_win_select, wk,
                cnt + C_NOV, T_levels, wb, mw, (unsigned long long *)(cnt + C_NMW));
   };
-  const bool speculate = nt >= PLAN_SPECULATE;
+  const bool speculate = k2 >= 2 * PLAN_SPECULATE;
   if (speculate) {
     plan_prefix();
-    plan_windows(nt);
+    plan_windows(cap);
   }
 
   // the counts and (speculatively) the first HUB_SPEC touched-hub records in
   // one copy to pinned staging and one synchronisation; more hubs than that
   // take a second copy
-  const uint64_t spec = std::min<uint64_t>(nt, HUB_SPEC);
+  const uint64_t spec = std::min<uint64_t>(cap, HUB_SPEC);
   uint32_t *sp = hub_stage_ + 64;  // after the 32 counters
   static_assert(C_COUNT <= 32, "counter staging");
   TRC_CUDA(cudaMemcpyAsync(hub_stage_, cnt, sizeof(hc), cudaMemcpyDeviceToHost, stream));
+  TRC_CUDA(cudaMemcpyAsync(hub_stage_ + 60, err.get(), 4, cudaMemcpyDeviceToHost, stream));
   {
     const uint32_t *src4[4] = {hw_u, hw_dn, (const uint32_t *)hw_h, s_hw_do.get()};
     for (int a = 0; a < 4; a++)
@@ -1065,6 +1062,15 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   }
   sync();
   memcpy(hc, hub_stage_, sizeof(hc));
+  const uint32_t herr = hub_stage_[60];
+  if (herr & ERR_BAD_VERTEX) throw_error(TRC_ERR_INVALID, "vertex id out of range [0, n)");
+  if (herr & ERR_TIMEOUT) throw_error(TRC_ERR_TIMEOUT, "radix sort look-back wait gave up");
+  const uint64_t kb = hc[C_KB], nt = hc[C_NT];
+  if (kb == 0) {
+    for (auto &x : last) x = 0;
+    last[0] = k2;
+    return 0;
+  }
   const uint64_t nov = hc[C_NOV], nh = hc[C_NH];
   const int64_t t2delta = (int64_t)hc[C_T2DELTA];
   const uint64_t t2new = (uint64_t)((int64_t)tier2_total + t2delta);
