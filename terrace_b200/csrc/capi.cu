@@ -88,7 +88,7 @@ trc_status trc_graph_create(uint32_t n, uint64_t hbm_budget_bytes, const trc_con
     trc_config c;
     trc_config_default(&c);
     if (cfg) c = *cfg;
-    if (c.hub_threshold < trc::K_INLINE || c.hub_threshold > 12288)
+    if (c.hub_threshold < trc::K_INLINE || c.hub_threshold > trc::HUB_THRESHOLD_MAX)
       trc::throw_error(TRC_ERR_INVALID, "hub_threshold must be in [16, 12288]");
     if (c.hub_stage_limit > 49152 || c.hub_stage_limit == 0) c.hub_stage_limit = 49152;
     *out = nullptr;

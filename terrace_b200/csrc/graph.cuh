@@ -68,6 +68,7 @@ class Graph {
   // ------------------------------------------------------------- scratch
   DBuf<uint32_t> s_in_src, s_in_dst;
   DBuf<uint64_t> s_A, s_B, s_C, s_tmp, s_cnt;
+  DBuf<uint64_t> s_mrec;  // merge records, two words per rewrite entry
   DBuf<uint32_t> s_tu, s_tdn, s_tc2, s_ovl, s_hw_u, s_hw_dn, s_hw_t, s_c2n, s_rlist;
   DBuf<int32_t> s_hw_h;
   DBuf<uint64_t> s_P, s_oOff, s_nOff, s_wk, s_wk2, s_mw, s_old, s_new, s_hwplan;

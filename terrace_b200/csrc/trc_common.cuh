@@ -24,6 +24,7 @@ namespace trc {
 // (include/graph.h:34-38, :216-224); here degree and tier pointers live in
 // separate arrays, so the row holds 16.
 constexpr uint32_t K_INLINE = 16;
+constexpr uint32_t HUB_THRESHOLD_MAX = 12288;  // largest configurable hub threshold
 // Tier 3: hub neighbours are kept in blocks of HUB_BLOCK slots.
 constexpr uint32_t HUB_BLOCK = 256;
 constexpr uint32_t NONE32 = 0xFFFFFFFFu;

@@ -57,7 +57,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
                   &lists.SM, &lists.M1, &lists.M2, &lists.hub_blocks})
     b->bind(&budget);
   for (auto *b : {&pbeg, &hub_blk0, &s_A, &s_B, &s_C, &s_tmp, &s_cnt, &s_P, &s_oOff, &s_nOff,
-                  &s_wk, &s_wk2, &s_mw, &s_old, &s_new, &s_hwplan})
+                  &s_wk, &s_wk2, &s_mw, &s_old, &s_new, &s_hwplan, &s_mrec})
     b->bind(&budget);
   hub_of.bind(&budget);
   wstamp.bind(&budget);
@@ -136,7 +136,7 @@ void Graph::release_scratch() {
                   &s_c2n, &s_rlist, &s_pma_next, &s_tix, &s_hw_do, &s_wbits})
     b->reset();
   for (auto *b : {&s_A, &s_B, &s_C, &s_tmp, &s_P, &s_oOff, &s_nOff, &s_wk, &s_wk2, &s_mw, &s_old,
-                  &s_new, &s_hwplan, &pbeg_alt})
+                  &s_new, &s_hwplan, &pbeg_alt, &s_mrec})
     b->reset();
   s_hw_h.reset();
   s_flags.reset();
@@ -725,17 +725,45 @@ __device__ __forceinline__ void put_rank(uint32_t *row, uint32_t *seg, uint32_t 
   else seg[r - K_INLINE] = x;
 }
 
-__device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a, uint64_t w,
-                                          uint32_t lane) {
-  const uint32_t u = a.rs[w];
-  uint64_t t = a.tix[u];
-  uint64_t b0 = 0, b1 = 0;
-  if (t != NONE32) {
-    b0 = a.tpos[t];
-    b1 = t + 1 < a.nt ? a.tpos[t + 1] : a.kb;
+// Per rewrite entry, packed by k_merge_prep (one thread per entry, all its
+// loads independent across threads): x = batch slice start << MR_BITS | key
+// count, y = old segment offset << MR_BITS | old degree.  The merge's warp
+// then reads it next to rs[w] instead of the dependent chains
+// rs -> tix -> tpos and rs -> hub_of -> pbeg (about 5 % of the merge's time
+// at RMAT scale 22, batch 1e6).  Both counts are at most the hub threshold
+// (<= HUB_THRESHOLD_MAX by the configuration check); slice starts and segment offsets
+// stay below 2^40 (an 8 TB batch or PMA).
+constexpr uint32_t MR_BITS = 24;
+constexpr uint64_t MR_MASK = (1ull << MR_BITS) - 1;
+
+__global__ void k_merge_prep(DevView G, MergeArgs a, const uint64_t *nrs, ulonglong2 *rec) {
+  const uint64_t nw = *nrs;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += stride) {
+    const uint32_t u = a.rs[w];
+    const uint32_t t = a.tix[u];
+    uint64_t b0 = 0, b1 = 0;
+    if (t != NONE32) {
+      b0 = a.tpos[t];
+      b1 = t + 1 < a.nt ? a.tpos[t + 1] : a.kb;
+    }
+    rec[w] = make_ulonglong2((b0 << MR_BITS) | (b1 - b0), (G.pbeg[u] << MR_BITS) | G.deg[u]);
   }
-  const uint32_t nb = (uint32_t)(b1 - b0);
-  NbrList L = nbr_list(G, u);
+}
+
+__device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a,
+                                          const ulonglong2 *rec, uint64_t w, uint32_t lane) {
+  const uint32_t u = a.rs[w];
+  const ulonglong2 r = rec[w];
+  const uint64_t b0 = r.x >> MR_BITS;
+  const uint32_t nb = (uint32_t)(r.x & MR_MASK);
+  NbrList L;  // (merge vertices are never hubs)
+  L.deg = (uint32_t)(r.y & MR_MASK);
+  L.inl = G.inl + (uint64_t)u * K_INLINE;
+  L.ni = L.deg < K_INLINE ? L.deg : K_INLINE;
+  L.rest = L.deg - L.ni;
+  L.seg = G.pma + (r.y >> MR_BITS);
+  L.per = 0;
   const uint32_t d = L.deg;
   const uint64_t *B = a.bkeys + b0;
   uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
@@ -810,12 +838,13 @@ __device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a, 
 
 // persistent over the rewrite list, whose length is read on the device
 __global__ void __launch_bounds__(256, 8) k_merge_small(DevView G, MergeArgs a,
-                                                        const uint64_t *nrs) {
+                                                        const uint64_t *nrs,
+                                                        const ulonglong2 *rec) {
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t nw = *nrs;
   const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nw; w += stride)
-    merge_one(G, a, w, lane);
+    merge_one(G, a, rec, w, lane);
 }
 
 // Moves the segments written to the window buffer to their final slots
@@ -1238,7 +1267,11 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   {
     MergeArgs ma{rs, 0, tix, tpos, nt, kb, bkeys, insert ? 1 : 0, pbeg_new, dst_pma, mov_pma,
                  nmw ? wstamp.get() : nullptr, epoch, T, dst_pma == pma.get() ? 1 : 0};
-    TRC_LAUNCH(prof, stream, "upd_merge_small", pgrid, 256, 0, k_merge_small, G, ma, nrs_dev);
+    static_assert(HUB_THRESHOLD_MAX <= MR_MASK, "merge record counts");
+    ulonglong2 *rec = reinterpret_cast<ulonglong2 *>(s_mrec.ensure(2 * (uint64_t)n));
+    TRC_LAUNCH(prof, stream, "upd_merge_prep", pgrid, 256, 0, k_merge_prep, G, ma, nrs_dev, rec);
+    TRC_LAUNCH(prof, stream, "upd_merge_small", pgrid, 256, 0, k_merge_small, G, ma, nrs_dev,
+               (const ulonglong2 *)rec);
   }
 
   phase("merge_small");
