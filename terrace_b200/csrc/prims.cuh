@@ -78,17 +78,28 @@ __global__ void k_tile_sum(F f, uint64_t n, uint64_t *tile_sums) {
   if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
 }
 
+// The tile goes through shared memory so that global loads and stores are
+// coalesced (item i*PT + t by thread t) while each thread scans PI
+// consecutive items; a pad word after every 16 keeps both access patterns
+// free of bank conflicts.
+__device__ __forceinline__ uint32_t pad16(uint32_t j) { return j + (j >> 4); }
+
 template <typename F>
 __global__ void k_tile_scan(F f, uint64_t n, const uint64_t *tile_off, uint64_t *out) {
+  __shared__ uint64_t sv[PTILE + PTILE / 16];
   __shared__ uint64_t ws[PT / 32 + 1];
-  // each thread owns PI consecutive items
-  uint64_t base = (uint64_t)blockIdx.x * PTILE + (uint64_t)threadIdx.x * PI;
+  const uint64_t base = (uint64_t)blockIdx.x * PTILE;
+#pragma unroll
+  for (int i = 0; i < PI; i++) {
+    const uint32_t j = i * PT + threadIdx.x;
+    sv[pad16(j)] = base + j < n ? f(base + j) : 0;
+  }
+  __syncthreads();
   uint64_t v[PI];
   uint64_t s = 0;
 #pragma unroll
   for (int i = 0; i < PI; i++) {
-    uint64_t idx = base + i;
-    v[i] = idx < n ? f(idx) : 0;
+    v[i] = sv[pad16(threadIdx.x * PI + i)];
     s += v[i];
   }
   uint64_t tot;
@@ -96,9 +107,14 @@ __global__ void k_tile_scan(F f, uint64_t n, const uint64_t *tile_off, uint64_t 
   ex += tile_off[blockIdx.x];
 #pragma unroll
   for (int i = 0; i < PI; i++) {
-    uint64_t idx = base + i;
-    if (idx < n) out[idx] = ex;
+    sv[pad16(threadIdx.x * PI + i)] = ex;
     ex += v[i];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < PI; i++) {
+    const uint32_t j = i * PT + threadIdx.x;
+    if (base + j < n) out[base + j] = sv[pad16(j)];
   }
   if (blockIdx.x == gridDim.x - 1 && threadIdx.x == PT - 1) out[n] = ex;
 }
@@ -148,25 +164,39 @@ struct PredCount {
   __device__ uint64_t operator()(uint64_t i) const { return p(i) ? 1 : 0; }
 };
 
+// Round i of a tile covers items i*PT + t (coalesced predicate and value
+// reads); an item's rank in the tile is the selected count of earlier
+// rounds, then of earlier warps of its round, then of earlier lanes, so
+// consecutive selected items go to consecutive slots from consecutive lanes.
 template <typename P, typename V, typename T>
 __global__ void k_select_scatter(P pred, V val, uint64_t n, const uint64_t *tile_off, T *out,
                                  uint64_t *count) {
-  __shared__ uint64_t ws[PT / 32 + 1];
-  uint64_t base = (uint64_t)blockIdx.x * PTILE + (uint64_t)threadIdx.x * PI;
-  bool f[PI];
-  uint64_t s = 0;
+  constexpr int NW = PT / 32;
+  static_assert(PI * NW == 64, "one warp scans the tile's (round, warp) counts, two per lane");
+  __shared__ uint32_t wc[PI * NW];
+  const uint64_t base = (uint64_t)blockIdx.x * PTILE;
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t m[PI];
 #pragma unroll
   for (int i = 0; i < PI; i++) {
-    uint64_t idx = base + i;
-    f[i] = idx < n && pred(idx);
-    s += f[i];
+    const uint64_t idx = base + (uint64_t)i * PT + threadIdx.x;
+    m[i] = __ballot_sync(0xFFFFFFFFu, idx < n && pred(idx));
+    if (lane == 0) wc[i * NW + w] = __popc(m[i]);
   }
-  uint64_t tot;
-  uint64_t ex = block_excl_scan<uint64_t, PT>(s, ws, tot);
-  ex += tile_off[blockIdx.x];
+  __syncthreads();
+  if (w == 0) {
+    const uint32_t a = wc[2 * lane], b = wc[2 * lane + 1];
+    const uint32_t ex = warp_incl_scan(a + b) - (a + b);
+    wc[2 * lane] = ex;
+    wc[2 * lane + 1] = ex + a;
+  }
+  __syncthreads();
+  const uint64_t off = tile_off[blockIdx.x];
+  const uint32_t lt = lanemask_lt();
 #pragma unroll
   for (int i = 0; i < PI; i++) {
-    if (f[i]) out[ex++] = val(base + i);
+    if ((m[i] >> lane) & 1u)
+      out[off + wc[i * NW + w] + __popc(m[i] & lt)] = val(base + (uint64_t)i * PT + threadIdx.x);
   }
   if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *count = tile_off[gridDim.x];
 }
