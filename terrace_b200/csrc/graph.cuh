@@ -37,6 +37,8 @@ class Graph {
   trc_config cfg;
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
+  cudaStream_t side_stream = nullptr;  // hub merge, concurrent with the small-vertex merge
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   Budget budget;
   Profiler prof;
 

@@ -46,6 +46,9 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   budget.limit = budget_bytes;
   TRC_CUDA(cudaGetDevice(&device));
   TRC_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+  TRC_CUDA(cudaStreamCreateWithFlags(&side_stream, cudaStreamNonBlocking));
+  TRC_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+  TRC_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
   stream = own_stream;
   budget.stream = stream;
   budget.open_pool(device);
@@ -98,12 +101,16 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
 Graph::~Graph() {
   if (own_stream) cudaStreamSynchronize(own_stream);
   if (stream && stream != own_stream) cudaStreamSynchronize(stream);
+  if (side_stream) cudaStreamSynchronize(side_stream);
   prof.reset();
   if (prg.exec) cudaGraphExecDestroy(prg.exec);
   // the members free after this body, on the legacy stream (the work on
   // the graph's streams has finished)
   budget.stream = nullptr;
   if (hub_stage_) cudaFreeHost(hub_stage_);
+  if (ev_fork) cudaEventDestroy(ev_fork);
+  if (ev_join) cudaEventDestroy(ev_join);
+  if (side_stream) cudaStreamDestroy(side_stream);
   if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -267,6 +274,7 @@ enum {
   C_NMW,
   C_NR,
   C_T2DELTA,
+  C_MWORK,  // rewrite entries handed out to k_merge_small's warps
   C_COUNT
 };
 
@@ -836,15 +844,25 @@ __device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a,
   if (lane == 0) G.deg[u] = a.insert ? d + nb : d - nb;
 }
 
-// persistent over the rewrite list, whose length is read on the device
+// Persistent over the rewrite list, whose length is read on the device;
+// warps take MS_CHUNK entries at a time from a counter, so CTAs that start
+// late (behind the hub merge on the side stream) take fewer.
+constexpr uint32_t MS_CHUNK = 8;
+
 __global__ void __launch_bounds__(256, 8) k_merge_small(DevView G, MergeArgs a,
                                                         const uint64_t *nrs,
-                                                        const ulonglong2 *rec) {
+                                                        const ulonglong2 *rec,
+                                                        unsigned long long *work) {
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t nw = *nrs;
-  const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nw; w += stride)
-    merge_one(G, a, rec, w, lane);
+  for (;;) {
+    uint64_t w0 = 0;
+    if (lane == 0) w0 = atomicAdd(work, (unsigned long long)MS_CHUNK);
+    w0 = __shfl_sync(0xFFFFFFFFu, w0, 0);
+    if (w0 >= nw) break;
+    const uint64_t w1 = w0 + MS_CHUNK < nw ? w0 + MS_CHUNK : nw;
+    for (uint64_t w = w0; w < w1; w++) merge_one(G, a, rec, w, lane);
+  }
 }
 
 // Moves the segments written to the window buffer to their final slots
@@ -1264,37 +1282,46 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     exclusive_scan(NewDeg{rs, deg.get(), tix, tdn}, nrs, oo, t5, stream, prof);
     SN = read_u64(oo + nrs);
   }
+  uint64_t SOh = 0, SNh = 0;
+  const bool hub_general =
+      nh && hub_max_old > std::min<uint32_t>(HUB_SMEM_ELEMS, cfg.hub_stage_limit);
   {
     MergeArgs ma{rs, 0, tix, tpos, nt, kb, bkeys, insert ? 1 : 0, pbeg_new, dst_pma, mov_pma,
                  nmw ? wstamp.get() : nullptr, epoch, T, dst_pma == pma.get() ? 1 : 0};
     static_assert(HUB_THRESHOLD_MAX <= MR_MASK, "merge record counts");
     ulonglong2 *rec = reinterpret_cast<ulonglong2 *>(s_mrec.ensure(2 * (uint64_t)n));
     TRC_LAUNCH(prof, stream, "upd_merge_prep", pgrid, 256, 0, k_merge_prep, G, ma, nrs_dev, rec);
+    // ---- hub path: fused CTA-per-hub merge (old lists staged in shared
+    // memory) on the side stream, concurrent with the small-vertex merge:
+    // the two touch disjoint vertices (hubs and vertices promoted now versus
+    // the rewrite list), nothing is allocated or freed on the graph's stream
+    // until the join, and window moves land after it.  Hubs too large for
+    // shared memory take the general gather / merge / scatter path below.
+    if (nh && !hub_general) {
+      static bool attr_set = false;
+      if (!attr_set) {
+        TRC_CUDA(cudaFuncSetAttribute(k_merge_hub, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(HUB_SMEM_ELEMS * 4)));
+        attr_set = true;
+      }
+      uint64_t *dplan = s_hwplan.ensure(plan.size());
+      TRC_CUDA(
+          cudaMemcpyAsync(dplan, plan.data(), plan.size() * 8, cudaMemcpyHostToDevice, stream));
+      HubMergeArgs ha{dplan, nh, tix, tpos, nt, kb, bkeys, insert ? 1 : 0};
+      size_t smem = (size_t)std::max<uint32_t>(hub_max_old, 1) * 4;
+      TRC_CUDA(cudaEventRecord(ev_fork, stream));
+      TRC_CUDA(cudaStreamWaitEvent(side_stream, ev_fork, 0));
+      TRC_LAUNCH(prof, side_stream, "upd_merge_hub", nh, 256, smem, k_merge_hub, G, ha);
+      TRC_CUDA(cudaEventRecord(ev_join, side_stream));
+      SOh = hub_old_total;
+      SNh = hub_new_total;
+    }
     TRC_LAUNCH(prof, stream, "upd_merge_small", pgrid, 256, 0, k_merge_small, G, ma, nrs_dev,
-               (const ulonglong2 *)rec);
+               (const ulonglong2 *)rec, (unsigned long long *)(cnt + C_MWORK));
+    if (nh && !hub_general) TRC_CUDA(cudaStreamWaitEvent(stream, ev_join, 0));
   }
 
   phase("merge_small");
-  // ---- hub path: fused CTA-per-hub merge (old lists staged in shared
-  // memory); hubs too large for shared memory take the general
-  // gather / merge / scatter path
-  uint64_t SOh = 0, SNh = 0;
-  bool hub_general = nh && hub_max_old > std::min<uint32_t>(HUB_SMEM_ELEMS, cfg.hub_stage_limit);
-  if (nh && !hub_general) {
-    static bool attr_set = false;
-    if (!attr_set) {
-      TRC_CUDA(cudaFuncSetAttribute(k_merge_hub, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(HUB_SMEM_ELEMS * 4)));
-      attr_set = true;
-    }
-    uint64_t *dplan = s_hwplan.ensure(plan.size());
-    TRC_CUDA(cudaMemcpyAsync(dplan, plan.data(), plan.size() * 8, cudaMemcpyHostToDevice, stream));
-    HubMergeArgs ha{dplan, nh, tix, tpos, nt, kb, bkeys, insert ? 1 : 0};
-    size_t smem = (size_t)std::max<uint32_t>(hub_max_old, 1) * 4;
-    TRC_LAUNCH(prof, stream, "upd_merge_hub", nh, 256, smem, k_merge_hub, G, ha);
-    SOh = hub_old_total;
-    SNh = hub_new_total;
-  }
   if (hub_general) {
     std::vector<uint32_t> rh(nh);
     for (uint64_t i = 0; i < nh; i++) rh[i] = (uint32_t)plan[6 * i + 1];
