@@ -245,7 +245,7 @@ def main():
     summ = {"n": n, "m": int(len(keys)), "max_degree": int(deg.max()),
             "argmax_degree": int(deg.argmax()), "isolated": int((deg == 0).sum()),
             "csr_sha256": csr_sha(off, tgt), "sample": sample.tolist(),
-            "tc_exact_published_in_survey": 758730}
+            "tc_exact_rmat17": 758730}
     for src in (9, int(deg.argmax())):
         p = R.bfs(src)
         lv = O.levels_from_parents(p, src)

@@ -169,7 +169,7 @@ def test_static_workload_rmat17(T):
     bc = g.bc(s["bc_src"])
     ref = np.array([np.nan if x is None else x for x in s["bc_sample"]])
     assert rel_close(bc[sample], ref)
-    assert g.tc() == s["tc_exact_published_in_survey"] == 758730
+    assert g.tc() == s["tc_exact_rmat17"] == 758730
 
 
 def test_set_semantics_edge_cases(T):

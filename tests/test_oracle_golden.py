@@ -123,7 +123,7 @@ def test_config1_summary():
     bc = O.bc(off, tgt, s["bc_src"])
     ref = np.array([np.nan if x is None else x for x in s["bc_sample"]])
     assert rel_close(bc[sample], ref)
-    assert O.tc(off, tgt) == s["tc_exact_published_in_survey"] == 758730
+    assert O.tc(off, tgt) == s["tc_exact_rmat17"] == 758730
 
 
 def test_adj_reader_pinned_to_reference():
