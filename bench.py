@@ -665,11 +665,12 @@ def serving(T, torch):
 
 
 # ------------------------------------------------------------ CPU baselines
-def reference_insert_run(steps, warmup, threads, scale=SCALE, sample_note=None):
+def reference_insert_run(steps, warmup, threads, scale=SCALE, sample_note=None, single=0):
     """Reference Terrace (oracle/_ref) on the host: bulk load (untimed), then
     `steps` timed add_edge_batch calls of 1e6-pair batches (sorted, deduped,
     only new edges -- the reference's preconditions, prepared untimed as
-    src/graph_bm.cc:343-355 does)."""
+    src/graph_bm.cc:343-355 does).  With single > 0, that many further
+    batches are timed on one thread (returned as a fourth value, edges/s)."""
     import oracle as O
     O.ref_lib().ref_set_threads(threads)
     n = 1 << scale
@@ -678,7 +679,10 @@ def reference_insert_run(steps, warmup, threads, scale=SCALE, sample_note=None):
     R.add_keys(keys, 0)
     cur = keys
     times, counts = [], []
-    for j in range(warmup + steps):
+    t1, c1 = 0.0, 0
+    for j in range(warmup + steps + single):
+        if j == warmup + steps:
+            O.ref_lib().ref_set_threads(1)
         bs, bd = O.rmat(n, batch_seed(BATCH_STREAM, j), A, B, C, BATCH)
         bk = O.make_keys(bs, bd, True, True)
         new = O.key_difference(bk, cur)
@@ -686,10 +690,16 @@ def reference_insert_run(steps, warmup, threads, scale=SCALE, sample_note=None):
         t0 = time.perf_counter()
         R.add_keys(new, perm_seed=j + 1)
         dt = time.perf_counter() - t0
-        if j >= warmup:
+        if j >= warmup + steps:
+            t1 += dt
+            c1 += len(new)
+        elif j >= warmup:
             times.append(dt)
             counts.append(len(new))
     R.close()
+    O.ref_lib().ref_set_threads(threads)
+    if single:
+        return sum(counts) / sum(times), sum(times), len(keys), c1 / t1
     return sum(counts) / sum(times), sum(times), len(keys)
 
 
@@ -735,10 +745,12 @@ def cpu_baseline_for_ours():
         return {"value": len(new) / dt, "unit": "edges/s", "cores": 1, "kind": "port",
                 "sample": "one 1e6-pair batch merged into the scale-22 edge set (oracle set model)"}
     threads = os.cpu_count() or 1
-    val, tsum, m = reference_insert_run(3, 0, threads)
+    val, tsum, m, val1 = reference_insert_run(3, 0, threads, single=1)
     return {"value": val, "unit": "edges/s", "cores": threads, "kind": "reference",
             "sample": f"3 add_edge_batch calls of 1e6-pair batches into the scale-22 graph "
-                      f"({m} edges, bulk load untimed), {tsum:.2f} s timed"}
+                      f"({m} edges, bulk load untimed), {tsum:.2f} s timed",
+            "single_thread": {"value": val1, "unit": "edges/s", "cores": 1,
+                              "sample": "a fourth 1e6-pair batch into the same graph on one thread"}}
 
 
 def main():
