@@ -86,7 +86,10 @@ const char *trc_last_error(void);
 trc_status trc_graph_create(uint32_t n, uint64_t hbm_budget_bytes,
                             const trc_config *cfg, trc_graph **out);
 trc_status trc_graph_destroy(trc_graph *g);
-/* Bind the handle to a CUDA stream (cudaStream_t); NULL = library stream. */
+/* Bind the handle to a CUDA stream (cudaStream_t); NULL = library stream.
+ * Batch updates also run their hub merge on a second stream owned by the
+ * handle, forked from and joined back to the bound stream with events, so
+ * every call's work stays ordered after earlier work on the bound stream. */
 trc_status trc_graph_set_stream(trc_graph *g, void *stream);
 
 /* Frees the temporary device buffers kept between calls (sort buffers,
