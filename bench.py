@@ -120,6 +120,29 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- our GPU arm
+# ------------------------------------------------------------ replicas
+# Whole-job figures over N independent replicas (one process per GPU): units
+# are summed over ranks and times are the slowest rank's.  With one rank
+# both return their argument; otherwise every rank must call them in the same
+# order (they are all-reduces on `device`: cuda under NCCL, cpu under gloo).
+def sum_over_ranks(x, device, world):
+    if world == 1:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+    return type(x)(t.item())
+
+
+def max_over_ranks(x, device, world):
+    if world == 1:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, rank, world):
     import torch
     import terrace_b200 as T
@@ -148,7 +171,7 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
 
     def timed(fn, K, flush=False):
-        """Max over ranks of device time of K calls of fn(i) (ms/step)."""
+        """Max over ranks of the device time (ms) of K calls of fn(i)."""
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
@@ -160,12 +183,7 @@ def run_ours(args, rank, world):
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
-        ms = ev0.elapsed_time(ev1)
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms, out
+        return max_over_ranks(ev0.elapsed_time(ev1), dev, world), out
 
     # ---- warm-up inserts (W), then K timed inserts, then deletes of all
     for j in range(args.warmup):
@@ -177,12 +195,12 @@ def run_ours(args, rank, world):
                                                    drop_self_loops=True), args.steps)
     clocks = clk.stop()
     launches = g.launch_count() - l0
-    inserted = sum(ins)
-    value = inserted * world / (ins_ms / 1e3)
+    inserted = sum_over_ranks(sum(ins), dev, world)
+    value = inserted / (ins_ms / 1e3)
     pairs_per_s = BATCH * args.steps * world / (ins_ms / 1e3)
     del_ms, dels = timed(lambda i: g.remove_edge_batch(*batches[args.warmup + i], symmetrize=True,
                                                        drop_self_loops=True), args.steps)
-    deleted = sum(dels)
+    deleted = sum_over_ranks(sum(dels), dev, world)
     # ---- e2e: same metric through the public API with pinned HOST buffers,
     # K fresh batches on the graph the timed inserts started from (their
     # deletion restored it), so both meet the same PMA fill
@@ -196,8 +214,8 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_cnt = [g.add_edge_batch(hs, hd, symmetrize=True, drop_self_loops=True) for hs, hd in host]
-    e2e_s = time.perf_counter() - t0
-    e2e_val = sum(e2e_cnt) * world / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dev, world)
+    e2e_val = sum_over_ranks(sum(e2e_cnt), dev, world) / e2e_s
     for hs, hd in host:
         g.remove_edge_batch(hs, hd, symmetrize=True, drop_self_loops=True)
 
@@ -280,7 +298,7 @@ def run_ours(args, rank, world):
                    "batch_pairs": BATCH, "graph_edges": m0, "l2": "working set > L2 (graph ~0.9 GB)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "pairs_per_s": pairs_per_s,
-        "delete_edges_per_s": deleted * world / (del_ms / 1e3),
+        "delete_edges_per_s": deleted / (del_ms / 1e3),
         "bulk_load_edges_per_s": m0 / bulk_s,
         "e2e": {"value": e2e_val, "unit": "edges/s", "h2d_bytes_per_step": 8 * BATCH,
                 "d2h_bytes_per_step": 8},
