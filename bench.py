@@ -61,13 +61,25 @@ def load_peaks():
 
 
 # --------------------------------------------------------------------- clocks
+def smi_id(cuda_index: int) -> str:
+    """nvidia-smi's name for a CUDA device: its PCI bus id.  CUDA ordinals
+    are relative to CUDA_VISIBLE_DEVICES while nvidia-smi -i takes physical
+    indices, so the ordinal could name another GPU."""
+    try:
+        import torch
+        p = torch.cuda.get_device_properties(cuda_index)
+        return "%08X:%02X:%02X.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+    except Exception:
+        return str(cuda_index)
+
+
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
-        self.idx = gpu_index
+        self.idx = smi_id(gpu_index)
         self.proc = None
         self.path = os.path.join(tempfile.gettempdir(), f"trc_clocks_{os.getpid()}.csv")
 
@@ -283,6 +295,20 @@ def run_ours(args, rank, world):
     del batches
     torch.cuda.empty_cache()
 
+    # ---- the update sweep of the streaming workload (1e1..1e6 pairs, insert
+    # then delete, analytics after each) on a freshly loaded copy
+    sweep = []
+    if not args.skip_sweep:
+        s, d = T.rmat_generate(n, 0, A, B, C, EF * n, device=True)
+        g2 = T.Graph(n)
+        g2.set_stream(stream)
+        g2.add_edge_batch(s, d, symmetrize=True, drop_self_loops=True)
+        del s, d
+        sweep = sweep_rmat22(T, torch, g2, stream, n, src)
+        g2.close()
+        torch.cuda.empty_cache()
+    coalesced = {} if args.skip_batched else coalesced_updates(T, torch, n)
+
     # ---- scale-24 static analytics (BFS / PageRank roofline target)
     s24 = {} if args.skip_scale24 else scale24(T, torch, stream, hbm_gbs, peak_kind)
 
@@ -314,7 +340,9 @@ def run_ours(args, rank, world):
         "kernel_share": {k: round(v[0] / total_kernel_ms, 4) for k, v in
                          sorted(kernel_ms.items(), key=lambda kv: -kv[1][0])[:12]},
         "analytics_rmat22": analytics22,
+        "sweep_rmat22": sweep,
         "batched_rmat22": batched22,
+        "coalesced_updates_rmat22": coalesced,
         "analytics_rmat24": s24,
         "tiers": {k: st[k] for k in ("inline_edges", "pma_edges", "hub_edges", "num_hubs",
                                      "pma_capacity", "pma_rebuilds", "pma_window_rebalances")},
@@ -325,10 +353,9 @@ def run_ours(args, rank, world):
 def batched(T, torch, g, stream, n, t_call):
     """Batched multi-instance analytics on the scale-22 graph: 64 BFS and 64
     BC sources (uniform over non-isolated vertices, seed 2) as per-vertex
-    source masks in one traversal, against the same sources one by one; 256
-    insert batches of log-uniform size in [10, 1e5] pairs (seed 2) applied
-    as one coalesced sort + merge against one call per batch (both from HBM;
-    the edges are removed again afterwards, untimed)."""
+    source masks in one traversal, against the same sources one by one.  (The
+    256 coalesced update batches are measured through the server by
+    coalesced_updates.)"""
     rng = np.random.default_rng(2)
     deg = g.degree(np.arange(n, dtype=np.uint32))
     src = rng.choice(np.flatnonzero(deg), 64, replace=False).astype(np.uint32)
@@ -343,46 +370,145 @@ def batched(T, torch, g, stream, n, t_call):
     for v in src:
         t, _ = t_call(lambda: g.bc(int(v), device=True), reps=1)
         one_bc += t
-    sizes = np.exp(rng.uniform(np.log(10), np.log(1e5), 256)).astype(np.int64)
-    bs, bd = T.rmat_generate(n, hash32(2), A, B, C, int(sizes.sum()), device=True)
-    # pairs of edges not in the graph (and no self-loops), so that removing
-    # the batches afterwards restores the graph and both runs insert the
-    # same edge set
-    keep = (g.is_edge(bs, bd) == 0) & (bs != bd)
-    cuts = np.concatenate([[0], np.cumsum(sizes)])
-    kc = torch.cumsum(keep.to(torch.int64), 0).cpu().numpy()
-    cuts = np.concatenate([[0], kc[cuts[1:] - 1]])
-    bs, bd = bs[keep].contiguous(), bd[keep].contiguous()
-
-    def one_by_one():
-        return sum(g.add_edge_batch(bs[cuts[i]:cuts[i + 1]], bd[cuts[i]:cuts[i + 1]],
-                                    symmetrize=True, drop_self_loops=True) for i in range(256))
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    torch.cuda.synchronize()
-    ev[0].record(stream)
-    added = one_by_one()
-    ev[1].record(stream)
-    torch.cuda.synchronize()
-    g.remove_edge_batch(bs, bd, symmetrize=True, drop_self_loops=True)
-    torch.cuda.synchronize()
-    ev[2].record(stream)
-    added2 = g.add_edge_batch(bs, bd, symmetrize=True, drop_self_loops=True)
-    ev[3].record(stream)
-    torch.cuda.synchronize()
-    g.remove_edge_batch(bs, bd, symmetrize=True, drop_self_loops=True)
-    t_sep, t_co = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
     return {"sources": 64, "msbfs_ms": ms_bfs, "bfs_64_one_by_one_ms": one_bfs,
-            "msbc_ms": ms_bc, "bc_64_one_by_one_ms": one_bc,
-            "update_batches": 256, "update_pairs": int(cuts[-1]),
-            "separate_ms": t_sep, "separate_edges_per_s": added / (t_sep / 1e3),
-            "coalesced_ms": t_co, "coalesced_edges_per_s": added2 / (t_co / 1e3),
-            "same_edges": added == added2}
+            "msbc_ms": ms_bc, "bc_64_one_by_one_ms": one_bc}
+
+
+SWEEP_SIZES = (10, 1000, 100000, 1000000)
+
+
+def sweep_trials(k):
+    """Trials per batch size of the sweep (the reference's graph_bm runs 20
+    per size, src/graph_bm.cc:322-327; the large sizes take fewer here so the
+    CPU arm stays within its time bound)."""
+    return 20 if k <= 1000 else (5 if k <= 100000 else 3)
+
+
+def sweep_seed(i, ts):
+    """Seed of trial ts of sweep size i: batch 1000 + 100 i + ts of stream 1."""
+    return batch_seed(BATCH_STREAM, 1000 + 100 * i + ts)
+
+
+def sweep_rmat22(T, torch, g, stream, n, src):
+    """The streaming workload as the reference's update benchmark runs it
+    (src/graph_bm.cc:316-390): for each batch size 1e1, 1e3, 1e5 and 1e6
+    pairs, trials of insert-then-delete of a fresh RMAT batch (seed stream
+    1, symmetrized), each call timed on the device; after the first trial's
+    insert and again after its delete, BFS (from the maximum-degree vertex),
+    CC, PageRank 10 and TC on the updated graph.  Batches are resident in
+    HBM; `wall` is the host clock around the same synchronous calls."""
+    out = []
+    for i, k in enumerate(SWEEP_SIZES):
+        trials = sweep_trials(k)
+        ins_ms = del_ms = 0.0
+        ins_wall = del_wall = 0.0
+        ins_e = del_e = 0
+        after = {}
+        for ts in range(trials):
+            bs, bd = T.rmat_generate(n, sweep_seed(i, ts), A, B, C, k, device=True)
+            torch.cuda.synchronize()
+            for op in ("insert", "delete"):
+                fn = g.add_edge_batch if op == "insert" else g.remove_edge_batch
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                w0 = time.perf_counter()
+                e0.record(stream)
+                c = fn(bs, bd, symmetrize=True, drop_self_loops=True)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                w = time.perf_counter() - w0
+                ms = e0.elapsed_time(e1)
+                if op == "insert":
+                    ins_ms, ins_wall, ins_e = ins_ms + ms, ins_wall + w, ins_e + c
+                else:
+                    del_ms, del_wall, del_e = del_ms + ms, del_wall + w, del_e + c
+                if ts == 0:
+                    after[op] = analytics_ms(g, torch, stream, src)
+        out.append({"batch_pairs": k, "trials": trials,
+                    "insert_edges_per_s": ins_e / (ins_ms / 1e3),
+                    "insert_pairs_per_s": k * trials / (ins_ms / 1e3),
+                    "insert_ms": ins_ms / trials, "insert_wall_ms": 1e3 * ins_wall / trials,
+                    "delete_edges_per_s": del_e / (del_ms / 1e3),
+                    "delete_pairs_per_s": k * trials / (del_ms / 1e3),
+                    "delete_ms": del_ms / trials, "delete_wall_ms": 1e3 * del_wall / trials,
+                    "after_insert": after["insert"], "after_delete": after["delete"]})
+    return out
+
+
+def analytics_ms(g, torch, stream, src):
+    """BFS / CC / PageRank 10 / TC once each on the current graph (device
+    time, CUDA events on the graph's stream)."""
+    res = {}
+    for name, fn in (("bfs_ms", lambda: g.bfs(src, device=True)), ("cc_ms", lambda: g.cc(device=True)),
+                     ("pagerank10_ms", lambda: g.pagerank(10, device=True)), ("tc_ms", g.tc)):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[name] = round(e0.elapsed_time(e1), 3)
+        if name == "tc_ms":
+            res["triangles"] = r
+    return res
+
+
+def coalesced_updates(T, torch, n):
+    """The batching layer's coalescer: 256 update requests (sizes
+    log-uniform in [10, 1e5] pairs, seed 2, alternating insert / delete)
+    submitted to a held server and released at once, so the continuous-
+    batching server applies them as one round (one tagged radix sort of all
+    requests, then one delete batch and one insert batch), against the same
+    requests through the plain one-request-at-a-time server.  Each mode runs
+    on its own freshly loaded copy of the scale-22 graph; both must end with
+    the same CSR.  Host buffers; time = host clock from release to the last
+    completion."""
+    import hashlib
+    rng = np.random.default_rng(2)
+    sizes = np.exp(rng.uniform(np.log(10), np.log(1e5), 256)).astype(np.int64)
+    ps, pd = T.rmat_generate(n, hash32(2), A, B, C, int(sizes.sum()))
+    cuts = np.concatenate([[0], np.cumsum(sizes)])
+    res = {"requests": 256, "pairs": int(cuts[-1])}
+    hashes = {}
+    for mode in ("fifo", "batched"):
+        s, d = T.rmat_generate(n, 0, A, B, C, EF * n, device=True)
+        g = T.Graph(n)
+        g.add_edge_batch(s, d, symmetrize=True, drop_self_loops=True)
+        del s, d
+        m0 = g.get_num_edges()
+        torch.cuda.synchronize()
+        srv = T.Server(g, batched=mode == "batched", summary=True)
+        srv.hold(True)
+        ids = []
+        for i in range(256):
+            a, b = ps[cuts[i]:cuts[i + 1]], pd[cuts[i]:cuts[i + 1]]
+            ids.append(srv.insert(a, b) if i % 2 == 0 else srv.delete(a, b))
+        t0 = time.perf_counter()
+        srv.hold(False)
+        for rid in ids:
+            srv.wait(rid, 600_000)
+            srv.release(rid)
+        dt = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        off, tgt = g.dump_csr()
+        h = hashlib.sha256()
+        h.update(np.ascontiguousarray(off, "<u8").tobytes())
+        h.update(np.ascontiguousarray(tgt, "<u4").tobytes())
+        hashes[mode] = h.hexdigest()
+        res[mode] = {"ms": 1e3 * dt, "pairs_per_s": cuts[-1] / dt, "rounds": st["rounds"],
+                     "device_calls": st["device_calls"],
+                     "net_edge_change": int(g.get_num_edges()) - int(m0)}
+        g.close()
+        torch.cuda.empty_cache()
+    res["same_final_csr"] = hashes["fifo"] == hashes["batched"]
+    res["batched_over_fifo"] = res["fifo"]["ms"] / res["batched"]["ms"]
+    return res
 
 
 def kernel_bytes(name, sz):
     """Algorithmic bytes of one launch of an update-pipeline kernel for a
-    batch with sizes `sz` (trc_stats last_*): the bytes the kernel must move
-    (DESIGN.md lists the formulas)."""
+    batch with sizes `sz` (trc_stats last_*): the bytes the kernel must move."""
     k2, kb, nr = sz["last_keys"], sz["last_applied"], sz["last_rewritten"]
     so, sn = sz["last_gathered"], sz["last_written"]
     if name == "upd_merge_small":  # old list in (4 B), batch keys in (8 B), new list out (4 B)
@@ -500,16 +626,62 @@ def scale24(T, torch, stream, hbm_gbs, peak_kind):
             "bfs_kernels": {k: v for k, v in bfs_prof.items()},
         }
 
+    def more():
+        """CC, BC (from the BFS source) and TC, with the roofline of the
+        first two: CC 4 m + 12 n (one pass of union-find hooking over every
+        edge), BC 2 * 4 * sum_R deg + 40 n (forward and backward sweep over
+        the reached adjacency); TC is latency-bound and reported as
+        triangles/s.  Then inserts into this graph: three 1e6-pair batches of
+        the same skew (seed stream 1) inserted and then deleted, each timed on
+        the device, with the blocked tier's share of the work."""
+        cc_ms, _ = best(lambda: g.cc(device=True))
+        bc_ms, _ = best(lambda: g.bc(src, device=True), reps=2)
+        tc_ms, tcount = best(lambda: g.tc(), reps=1)
+        lv = g.bfs(src, device=True)[1].cpu().numpy().view(np.uint32)
+        rdeg = int(deg[lv != 0xFFFFFFFF].astype(np.int64).sum())
+        cc_bytes, bc_bytes = 4 * m + 12 * n, 8 * rdeg + 40 * n
+        r = {"cc_ms": cc_ms, "cc_hbm_gbs": cc_bytes / (cc_ms / 1e3) / 1e9,
+             "cc_roofline_frac": cc_bytes / (cc_ms / 1e3) / 1e9 / hbm_gbs,
+             "bc_ms": bc_ms, "bc_hbm_gbs": bc_bytes / (bc_ms / 1e3) / 1e9,
+             "bc_roofline_frac": bc_bytes / (bc_ms / 1e3) / 1e9 / hbm_gbs,
+             "tc_ms": tc_ms, "triangles": tcount, "triangles_per_s": tcount / (tc_ms / 1e3)}
+        ins = []
+        for j in range(3):
+            bs, bd = T.rmat_generate(n, batch_seed(BATCH_STREAM, j), a, b, c, BATCH, device=True)
+            rec = {}
+            for op in ("insert", "delete"):
+                fn = g.add_edge_batch if op == "insert" else g.remove_edge_batch
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                cnt = fn(bs, bd, symmetrize=True, drop_self_loops=True)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                st_ = g.stats()
+                rec[op] = {"ms": ms, "edges": cnt, "edges_per_s": cnt / (ms / 1e3),
+                           **{k: st_[k] for k in st_ if k.startswith("last_")}}
+            ins.append(rec)
+        r["updates_1e6"] = ins
+        r["insert_edges_per_s"] = sum(x["insert"]["edges"] for x in ins) / \
+            (sum(x["insert"]["ms"] for x in ins) / 1e3)
+        r["delete_edges_per_s"] = sum(x["delete"]["edges"] for x in ins) / \
+            (sum(x["delete"]["ms"] for x in ins) / 1e3)
+        return r
+
     default = measure()
     t0 = time.perf_counter()
     tuning = g.autotune(push_pull=True, pagerank=True)
     tuning["seconds"] = time.perf_counter() - t0
     tuned = measure()
+    extra = more()
     st = g.stats()
     g.close()
     out = {"graph": f"rmat{sc} ef{ef} a={a} b={b} c={c}", "n": n, "m": m, "bulk_load_s": load_s,
            "bulk_load_edges_per_s": m / load_s, "peak_gbs": hbm_gbs, "peak_kind": peak_kind}
     out.update(tuned)
+    out.update(extra)
     out["tuning"] = tuning
     out["default_config"] = {k: v for k, v in default.items() if not k.endswith("_kernels")}
     out["tiers"] = {k: st[k] for k in ("inline_edges", "pma_edges", "hub_edges", "num_hubs")}
@@ -683,12 +855,48 @@ def serving(T, torch):
 
 
 # ------------------------------------------------------------ CPU baselines
-def reference_insert_run(steps, warmup, threads, scale=SCALE, sample_note=None, single=0):
+def reference_sweep(R, cur, n):
+    """The reference's update benchmark on the streaming workload
+    (src/graph_bm.cc:316-390), same sizes and batches as sweep_rmat22: per
+    trial, add_edge_batch of the batch's new edges (sorted, deduped,
+    symmetrized: the reference's preconditions, prepared untimed), then the
+    parallel remove_edge loop over the batch's edges (all present then).
+    Returns the per-size rates and the final edge set."""
+    import oracle as O
+    out = []
+    for i, k in enumerate(SWEEP_SIZES):
+        trials = min(sweep_trials(k), 3 if k >= 100000 else 10)
+        ti = td = 0.0
+        ei = ed = 0
+        for ts in range(trials):
+            bs, bd = O.rmat(n, sweep_seed(i, ts), A, B, C, k)
+            bk = O.make_keys(bs, bd, True, True)
+            new = O.key_difference(bk, cur)
+            t0 = time.perf_counter()
+            R.add_keys(new, perm_seed=7 + ts)
+            ti += time.perf_counter() - t0
+            ei += len(new)
+            t0 = time.perf_counter()
+            bad = R.remove_keys(bk)
+            td += time.perf_counter() - t0
+            ed += len(bk) - bad
+            cur = O.key_difference(cur, bk)
+        out.append({"batch_pairs": k, "trials": trials, "insert_edges_per_s": ei / ti,
+                    "insert_pairs_per_s": k * trials / ti, "insert_ms": 1e3 * ti / trials,
+                    "delete_edges_per_s": ed / td, "delete_pairs_per_s": k * trials / td,
+                    "delete_ms": 1e3 * td / trials})
+    return out, cur
+
+
+def reference_insert_run(steps, warmup, threads, scale=SCALE, sample_note=None, single=0,
+                         sweep=False):
     """Reference Terrace (oracle/_ref) on the host: bulk load (untimed), then
     `steps` timed add_edge_batch calls of 1e6-pair batches (sorted, deduped,
     only new edges -- the reference's preconditions, prepared untimed as
     src/graph_bm.cc:343-355 does).  With single > 0, that many further
-    batches are timed on one thread (returned as a fourth value, edges/s)."""
+    batches are timed on one thread (returned as a fourth value, edges/s).
+    With sweep, the update sweep (reference_sweep) follows on all threads and
+    its result is appended to the returned tuple."""
     import oracle as O
     O.ref_lib().ref_set_threads(threads)
     n = 1 << scale
@@ -714,11 +922,17 @@ def reference_insert_run(steps, warmup, threads, scale=SCALE, sample_note=None, 
         elif j >= warmup:
             times.append(dt)
             counts.append(len(new))
-    R.close()
     O.ref_lib().ref_set_threads(threads)
+    sw = None
+    if sweep:
+        sw, cur = reference_sweep(R, cur, n)
+    R.close()
+    res = (sum(counts) / sum(times), sum(times), len(keys))
     if single:
-        return sum(counts) / sum(times), sum(times), len(keys), c1 / t1
-    return sum(counts) / sum(times), sum(times), len(keys)
+        res += (c1 / t1,)
+    if sweep:
+        res += (sw,)
+    return res
 
 
 def run_reference_arm(args, rank, world):
@@ -729,7 +943,7 @@ def run_reference_arm(args, rank, world):
         return {"impl": "reference", "unavailable": "oracle/_ref/libterrace_ref.so not built "
                 "(oracle/build_ref.sh needs the reference sources)"}
     threads = os.cpu_count() or 1
-    val, tsum, m = reference_insert_run(args.steps, args.warmup, threads)
+    val, tsum, m, sw = reference_insert_run(args.steps, args.warmup, threads, sweep=True)
     return {
         "impl": "reference", "metric": "insert edges/s (batch 1e6 pairs, symmetrized)",
         "value": val, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
@@ -743,6 +957,7 @@ def run_reference_arm(args, rank, world):
                          "sample": f"{args.steps} timed add_edge_batch calls of 1e6-pair batches "
                                    "(reference OpenMP build, g++ -Ofast, all host threads)"},
         "e2e": {"value": val, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "sweep_rmat22": sw,
     }
 
 
@@ -763,12 +978,43 @@ def cpu_baseline_for_ours():
         return {"value": len(new) / dt, "unit": "edges/s", "cores": 1, "kind": "port",
                 "sample": "one 1e6-pair batch merged into the scale-22 edge set (oracle set model)"}
     threads = os.cpu_count() or 1
-    val, tsum, m, val1 = reference_insert_run(3, 0, threads, single=1)
+    val, tsum, m, val1, sw = reference_insert_run(3, 0, threads, single=1, sweep=True)
     return {"value": val, "unit": "edges/s", "cores": threads, "kind": "reference",
             "sample": f"3 add_edge_batch calls of 1e6-pair batches into the scale-22 graph "
                       f"({m} edges, bulk load untimed), {tsum:.2f} s timed",
             "single_thread": {"value": val1, "unit": "edges/s", "cores": 1,
-                              "sample": "a fourth 1e6-pair batch into the same graph on one thread"}}
+                              "sample": "a fourth 1e6-pair batch into the same graph on one thread"},
+            "sweep_rmat22": sw}
+
+
+def summary(res):
+    """The headline figures of the whole run in a few hundred bytes."""
+    def r3(x):
+        return None if x is None else float("%.4g" % x)
+    out = {"insert_1e6_edges_per_s": r3(res["value"]), "e2e_edges_per_s": r3(res["e2e"]["value"]),
+           "merge_kernel_frac": r3(res["roofline"].get("frac"))}
+    ref_sw = {x["batch_pairs"]: x for x in (res.get("cpu_baseline") or {}).get("sweep_rmat22") or []}
+    out["sweep_ins_del_vs_ref"] = [
+        [x["batch_pairs"], r3(x["insert_edges_per_s"]), r3(x["delete_edges_per_s"]),
+         r3(ref_sw.get(x["batch_pairs"], {}).get("insert_edges_per_s")),
+         r3(ref_sw.get(x["batch_pairs"], {}).get("delete_edges_per_s"))]
+        for x in res.get("sweep_rmat22") or []]
+    s24 = res.get("analytics_rmat24") or {}
+    if s24:
+        out["rmat24"] = {k: r3(s24.get(k)) for k in (
+            "bfs_ms", "bfs_roofline_frac", "pagerank10_ms", "pagerank_roofline_frac", "cc_ms",
+            "cc_roofline_frac", "bc_ms", "bc_roofline_frac", "tc_ms", "insert_edges_per_s",
+            "delete_edges_per_s")}
+    co = res.get("coalesced_updates_rmat22") or {}
+    if co:
+        out["coalescer_batched_over_fifo"] = r3(co.get("batched_over_fifo"))
+        out["coalescer_same_csr"] = co.get("same_final_csr")
+    sv = res.get("serving") or {}
+    if sv:
+        out["serving_at_equal_p99"] = sv.get("at_equal_p99")
+        out["serving_at_p99_targets"] = [[x["p99_ms"], r3(x["fifo_rps"]), r3(x["batched_rps"])]
+                                         for x in sv.get("at_p99_targets", [])]
+    return out
 
 
 def main():
@@ -779,6 +1025,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-scale24", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
+    ap.add_argument("--skip-sweep", action="store_true")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--serving-only", action="store_true")
@@ -810,6 +1057,7 @@ def main():
     if rank == 0:
         if not args.skip_cpu_baseline:
             res["cpu_baseline"] = cpu_baseline_for_ours()
+        res["summary"] = summary(res)  # last: the headline figures at the end of the line
         print(json.dumps(res), flush=True)
     if world > 1:
         import torch

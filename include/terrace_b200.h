@@ -59,15 +59,16 @@ typedef struct {
                                  0.375: the reference doubles its array when
                                  the root passes 0.75 (double_list,
                                  src/PMA.cc:659-720). */
-  double hub_block_fill;      /* fill of hub blocks after a rewrite.
-                                 Default 0.75. */
+  double hub_block_fill;      /* fill of hub blocks after a rewrite or a
+                                 split.  Default 0.75. */
   uint32_t push_pull_divisor; /* edgeMap goes dense when |F| >= n/divisor;
                                  reference threshold 20 (include/Map.cpp:65-74).
                                  0 = the autotuned value (default 20). */
-  uint32_t hub_stage_limit;   /* largest hub list (elements) merged by the
-                                 shared-memory hub kernel; larger hubs take
-                                 the gather/merge/scatter path.  Default and
-                                 maximum 49152. */
+  uint32_t hub_stage_limit;   /* most batch edges one hub block merges in
+                                 shared memory (capped at 4096); a block
+                                 receiving more sends its hub through a
+                                 whole-list rewrite.  Default 49152 (the
+                                 cap applies). */
   uint32_t cuda_graphs;       /* 1: iteration loops (PageRank) are replayed
                                  from captured CUDA graphs; 0: launched one
                                  by one.  Default 1. */
@@ -97,6 +98,16 @@ trc_status trc_graph_set_stream(trc_graph *g, void *stream);
  * them again.  Useful after a bulk load.  No reference counterpart (the
  * reference frees its temporaries per call). */
 trc_status trc_release_scratch(trc_graph *g);
+
+/* Test hook for the bounded device wait of the batch sort: the radix sort's
+ * scatter passes wait for earlier tiles' counts (decoupled look-back) and
+ * give up after spin_limit polls, failing the call with TRC_ERR_TIMEOUT
+ * before the graph is modified.  withhold_first_tile != 0 makes no tile 0
+ * publish, so every such wait runs out (a flag that nothing sets); 0/0
+ * restores the defaults (spin_limit 0 = 2^22 polls).  No reference
+ * counterpart (the reference has no device waits). */
+trc_status trc_debug_sort_wait(trc_graph *g, uint32_t spin_limit,
+                               int withhold_first_tile);
 
 /* ---- updates: replaces Graph::add_edge_batch (include/graph.h:430-502) and
  *      the per-edge Graph::remove_edge loop of src/graph_bm.cc:375-380 (the
@@ -190,10 +201,9 @@ trc_status trc_tc(trc_graph *g, uint64_t *count);
  *      allocator belongs to another component, or a request path that must
  *      not allocate.  Same results as trc_bfs (levels exact, parents a valid
  *      BFS tree), computed with push steps only.  Its scratch (two frontier
- *      queues and a counter, 8 MiB + 256 B) is a static array every GPU that
- *      loads the library holds until exit; the first call on a device looks
- *      up the array's device address, so make that first call before any
- *      stream capture.  Outputs must be device arrays (TRC_DEVICE_PTR); the
+ *      queues and a counter, 8 MiB + 256 B) is a static device array: it is
+ *      reserved on a GPU, and its device address looked up, when the first
+ *      graph is created there (trc_graph_create), and held until exit.  Outputs must be device arrays (TRC_DEVICE_PTR); the
  *      graph may have at most TRC_NOALLOC_MAX_VERTICES vertices
  *      (TRC_ERR_INVALID otherwise).  All calls share the scratch: calls that
  *      overlap on the GPU race. */
@@ -206,8 +216,11 @@ trc_status trc_bfs_noalloc(trc_graph *g, uint32_t src, int32_t *parents,
  *      reference counterpart (the reference's functors run inside
  *      Graph::map_* on the host, include/graph.h:1287-1613).  Neighbour r of
  *      u: r < min(deg,16): inl[16u + r]; otherwise r' = r - 16 and, when
- *      hub_of[u] < 0, pma[pbeg[u] + r'], else with h = hub_of[u], per =
- *      hub_per[h]: hslot[(hub_blk0[h] + r'/per) * hub_block + r'%per]. */
+ *      hub_of[u] < 0, pma[pbeg[u] + r'], else with h = hub_of[u] and
+ *      e = hub_dir0[h] + i for the largest i < hub_nblk[h] with
+ *      hub_pre[hub_dir0[h] + i] <= r': hslot[hub_dir[e] * hub_block + r' -
+ *      hub_pre[e]].  hub_key[e] is the first neighbour in that block (the
+ *      directory of a hub is sorted by it). */
 typedef struct {
   uint32_t n;
   uint32_t inline_slots; /* 16 */
@@ -217,8 +230,11 @@ typedef struct {
   const uint64_t *pbeg;
   const uint32_t *pma;
   const int32_t *hub_of;
-  const uint64_t *hub_blk0;
-  const uint32_t *hub_per;
+  const uint64_t *hub_dir0;
+  const uint32_t *hub_nblk;
+  const uint32_t *hub_dir;
+  const uint32_t *hub_pre;
+  const uint32_t *hub_key;
   const uint32_t *hslot;
   void *stream; /* the handle's cudaStream_t */
 } trc_device_view;
@@ -355,6 +371,18 @@ typedef struct {
   uint64_t last_written;   /* list elements written (new lists) */
   uint64_t last_windows;   /* PMA windows rebalanced */
   uint64_t last_rebuild;   /* 1 if the PMA was rebuilt */
+  /* the blocked tier (hubs) in the last batch */
+  uint64_t last_hub_touched;        /* hubs with batch edges */
+  uint64_t last_hub_local;          /* of those, updated block by block */
+  uint64_t last_hub_rewritten;      /* of those, rewritten whole */
+  uint64_t last_hub_blocks_written; /* blocks written (splits included) */
+  uint64_t last_hub_read;           /* hub list elements read */
+  uint64_t last_hub_written;        /* hub list elements written */
+  /* the blocked tier since creation */
+  uint64_t hub_splits;              /* blocks added by splits */
+  uint64_t hub_rewrites;            /* whole-hub rewrites */
+  uint64_t hub_blocks_free;         /* pool blocks on the free list */
+  uint64_t hub_absorbs;             /* under-full blocks merged with their successor */
 } trc_stats;
 trc_status trc_get_stats(trc_graph *g, trc_stats *out);
 /* Checks every structural invariant on the device (sorted, duplicate-free

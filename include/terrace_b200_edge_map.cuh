@@ -48,8 +48,15 @@ struct DeviceGraph {
     r -= v.inline_slots;
     int32_t h = v.hub_of[u];
     if (h < 0) return v.pma[v.pbeg[u] + r];
-    uint32_t per = v.hub_per[h];
-    return v.hslot[(v.hub_blk0[h] + r / per) * v.hub_block + r % per];
+    // the hub's directory: the block whose element prefix is the largest <= r
+    const uint64_t e0 = v.hub_dir0[h];
+    uint32_t lo = 0, hi = v.hub_nblk[h];
+    while (hi - lo > 1) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (v.hub_pre[e0 + mid] <= r) lo = mid;
+      else hi = mid;
+    }
+    return v.hslot[(uint64_t)v.hub_dir[e0 + lo] * v.hub_block + (r - v.hub_pre[e0 + lo])];
   }
 };
 

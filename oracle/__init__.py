@@ -77,6 +77,8 @@ def lib():
         L.orc_bc.argtypes = [C.c_uint32, _u64p, _u32p, C.c_uint32, _f64p]
         L.orc_tc.restype = C.c_uint64
         L.orc_tc.argtypes = [C.c_uint32, _u64p, _u32p]
+        L.orc_tc_touching.restype = C.c_uint64
+        L.orc_tc_touching.argtypes = [C.c_uint32, _u64p, _u32p, _u64p, C.c_uint64]
         _lib = L
     return _lib
 
@@ -209,6 +211,26 @@ def tc(off, tgt) -> int:
     n = len(off) - 1
     off, tgt = _csr(off, tgt)
     return int(lib().orc_tc(n, off, tgt))
+
+
+def tc_touching(off, tgt, bkeys) -> int:
+    """Triangles of the graph that contain at least one edge of bkeys (sorted
+    unique directed keys, both directions of every edge): the change of the
+    triangle count when those edges are added to (or removed from) it."""
+    n = len(off) - 1
+    off, tgt = _csr(off, tgt)
+    bk = np.ascontiguousarray(bkeys, np.uint64)
+    if len(bk) == 0:
+        return 0
+    return int(lib().orc_tc_touching(n, off, tgt, bk, len(bk)))
+
+
+def csr_keys(off, tgt):
+    """Sorted directed keys (src<<32|dst) of a CSR."""
+    off = np.asarray(off, np.uint64)
+    n = len(off) - 1
+    src = np.repeat(np.arange(n, dtype=np.uint64), np.diff(off.astype(np.int64)))
+    return (src << np.uint64(32)) | np.asarray(tgt, np.uint64)
 
 
 # ------------------------------------------------------- reference library

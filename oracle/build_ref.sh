@@ -12,9 +12,13 @@
 # -march=x86-64-v3 (AVX2) instead of the Makefile's -march=native: the library
 # travels to other hosts; src/PMA.cc uses AVX2 intrinsics.
 #
-# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+# Usage: oracle/build_ref.sh <reference_root>   (or TERRACE_REF=<reference_root>)
 set -e
-REF=${1:-${TERRACE_REF:-/root/reference}}
+REF=${1:-${TERRACE_REF:-}}
+if [ -z "$REF" ]; then
+  echo "build_ref.sh: give the reference tree as the first argument or in TERRACE_REF" >&2
+  exit 2
+fi
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 if [ ! -f "$REF/include/graph.h" ]; then

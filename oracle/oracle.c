@@ -360,3 +360,49 @@ uint64_t orc_tc(uint32_t n, const uint64_t *off, const uint32_t *tgt) {
   }
   return total;
 }
+
+/* ---------------------------------------------------------------------- */
+/* Triangles that contain at least one edge of a set B, for checking TC   */
+/* after a batch without recounting the whole graph (same triangles as    */
+/* orc_tc above, include/TC.h:51-87): with B as sorted unique directed    */
+/* keys (src<<32|dst) holding both directions of each edge,               */
+/*   T(G + B) = T(G) + orc_tc_touching(G + B, B minus G),                 */
+/*   T(G - B) = T(G) - orc_tc_touching(G, B within G).                    */
+/* A triangle is counted once, at its B edge with the smallest undirected */
+/* key max<<32|min.                                                       */
+/* ---------------------------------------------------------------------- */
+static int key_in(const uint64_t *B, uint64_t nb, uint64_t x) {
+  uint64_t lo = 0, hi = nb;
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) / 2;
+    if (B[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo < nb && B[lo] == x;
+}
+
+static uint64_t ukey(uint32_t a, uint32_t b) {
+  return a > b ? ((uint64_t)a << 32) | b : ((uint64_t)b << 32) | a;
+}
+
+uint64_t orc_tc_touching(uint32_t n, const uint64_t *off, const uint32_t *tgt,
+                         const uint64_t *bk, uint64_t nb) {
+  uint64_t total = 0;
+  for (uint64_t i = 0; i < nb; i++) {
+    uint32_t u = (uint32_t)(bk[i] >> 32), v = (uint32_t)bk[i];
+    if (u <= v || u >= n || v >= n) continue; /* each undirected edge once */
+    uint64_t e = bk[i];
+    uint64_t a = off[u], ae = off[u + 1], b = off[v], be = off[v + 1];
+    while (a < ae && b < be) {
+      uint32_t x = tgt[a], y = tgt[b];
+      if (x < y) { a++; continue; }
+      if (y < x) { b++; continue; }
+      /* common neighbour w = x: triangle {u, v, w} */
+      uint64_t f1 = ukey(u, x), f2 = ukey(v, x);
+      if (!((f1 < e && key_in(bk, nb, f1)) || (f2 < e && key_in(bk, nb, f2)))) total++;
+      a++;
+      b++;
+    }
+  }
+  return total;
+}

@@ -52,7 +52,8 @@ class trc_config(C.Structure):
 class trc_device_view(C.Structure):
     _fields_ = [("n", C.c_uint32), ("inline_slots", C.c_uint32), ("hub_block", C.c_uint32),
                 ("deg", C.c_void_p), ("inl", C.c_void_p), ("pbeg", C.c_void_p), ("pma", C.c_void_p),
-                ("hub_of", C.c_void_p), ("hub_blk0", C.c_void_p), ("hub_per", C.c_void_p),
+                ("hub_of", C.c_void_p), ("hub_dir0", C.c_void_p), ("hub_nblk", C.c_void_p),
+                ("hub_dir", C.c_void_p), ("hub_pre", C.c_void_p), ("hub_key", C.c_void_p),
                 ("hslot", C.c_void_p), ("stream", C.c_void_p)]
 
 
@@ -97,7 +98,17 @@ class trc_stats(C.Structure):
                 ("last_gathered", C.c_uint64),
                 ("last_written", C.c_uint64),
                 ("last_windows", C.c_uint64),
-                ("last_rebuild", C.c_uint64)]
+                ("last_rebuild", C.c_uint64),
+                ("last_hub_touched", C.c_uint64),
+                ("last_hub_local", C.c_uint64),
+                ("last_hub_rewritten", C.c_uint64),
+                ("last_hub_blocks_written", C.c_uint64),
+                ("last_hub_read", C.c_uint64),
+                ("last_hub_written", C.c_uint64),
+                ("hub_splits", C.c_uint64),
+                ("hub_rewrites", C.c_uint64),
+                ("hub_blocks_free", C.c_uint64),
+                ("hub_absorbs", C.c_uint64)]
 
 
 # (name, restype, argtypes) for every symbol the header declares
@@ -111,6 +122,7 @@ SIGNATURES = [
     ("trc_graph_destroy", _int, [_vp]),
     ("trc_graph_set_stream", _int, [_vp, _vp]),
     ("trc_release_scratch", _int, [_vp]),
+    ("trc_debug_sort_wait", _int, [_vp, _u32, _int]),
     ("trc_add_edge_batch", _int, [_vp, _vp, _vp, _u64, _u32, C.POINTER(_u64)]),
     ("trc_remove_edge_batch", _int, [_vp, _vp, _vp, _u64, _u32, C.POINTER(_u64)]),
     ("trc_is_edge", _int, [_vp, _vp, _vp, _u64, _vp, _u32]),

@@ -208,7 +208,8 @@ __global__ void __launch_bounds__(AT) k_pr_M(DevView G, const uint32_t *M, uint6
 // Every load of a step is independent of the others, so a warp keeps 64
 // index loads and 64 gathers in flight instead of one vertex's chain.
 struct FlatWarp {
-  uint32_t u, d, start, total, per;
+  uint32_t u, d, start, total;
+  int32_t hub;  // hub index, or -1
   const uint32_t *seg;
   bool valid;
 };
@@ -222,18 +223,13 @@ __device__ __forceinline__ FlatWarp flat_setup(const DevView &G, const uint32_t 
   f.valid = idx < nV;
   f.u = f.valid ? V[idx] : 0;
   f.d = 0;
-  f.per = 0;
+  f.hub = -1;
   f.seg = G.pma;
   if (f.valid && !op.skip(f.u)) {
     f.d = G.deg[f.u];
     if (f.d > K_INLINE) {
-      int32_t h = G.hub_of[f.u];
-      if (h < 0) {
-        f.seg = G.pma + G.pbeg[f.u];
-      } else {
-        f.seg = G.hslot + G.hub_blk0[h] * HUB_BLOCK;
-        f.per = G.hub_per[h];
-      }
+      f.hub = G.hub_of[f.u];
+      if (f.hub < 0) f.seg = G.pma + G.pbeg[f.u];
     }
   }
   uint32_t incl = warp_incl_scan(f.d);
@@ -258,14 +254,18 @@ __device__ __forceinline__ uint32_t flat_fetch(const DevView &G, const FlatWarp 
                                                uint32_t e, bool act) {
   uint32_t uo = __shfl_sync(0xFFFFFFFFu, f.u, v);
   uint32_t so = __shfl_sync(0xFFFFFFFFu, f.start, v);
-  uint32_t po = __shfl_sync(0xFFFFFFFFu, f.per, v);
+  int32_t ho = __shfl_sync(0xFFFFFFFFu, f.hub, v);
+  uint32_t dh = __shfl_sync(0xFFFFFFFFu, f.d, v);
   const uint32_t *sg = (const uint32_t *)__shfl_sync(0xFFFFFFFFu, (unsigned long long)f.seg, v);
   if (!act) return 0;
   uint32_t r = e - so;
   if (r < K_INLINE) return __ldg(G.inl + (uint64_t)uo * K_INLINE + r);
   r -= K_INLINE;
-  if (po == 0) return __ldg(sg + r);
-  return __ldg(sg + (r / po) * HUB_BLOCK + (r % po));
+  if (ho < 0) return __ldg(sg + r);
+  // a hub: the directory entry of hub rank r
+  const uint64_t e0 = G.hub_dir0[ho];
+  const uint32_t i = hub_entry_of_rank(G.hpre + e0, G.hub_nblk[ho], dh - K_INLINE, r);
+  return __ldg(G.hslot + (uint64_t)G.hdir[e0 + i] * HUB_BLOCK + (r - G.hpre[e0 + i]));
 }
 
 // segmented inclusive sum over lanes (segments = equal owner), tail lanes
@@ -364,12 +364,13 @@ __global__ void __launch_bounds__(AT) k_pr_H(DevView G, const uint32_t *Hv, PRAr
   uint32_t ni = d < K_INLINE ? d : K_INLINE;
   double sum = 0.0;
   if (threadIdx.x < ni) sum = __ldg(a.pc + G.inl[(uint64_t)u * K_INLINE + threadIdx.x]);
-  uint64_t b0 = G.hub_blk0[h];
-  uint32_t nb = G.hub_nblk[h];
+  const uint64_t e0 = G.hub_dir0[h];
+  const uint32_t nb = d > K_INLINE ? G.hub_nblk[h] : 0;
   uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (uint32_t b = warp; b < nb; b += AT / 32) {
-    uint32_t c = G.bcnt[b0 + b];
-    const uint32_t *blk = G.hslot + (b0 + b) * HUB_BLOCK;
+    const uint32_t id = G.hdir[e0 + b];
+    const uint32_t c = G.bcnt[id];
+    const uint32_t *blk = G.hslot + (uint64_t)id * HUB_BLOCK;
     for (uint32_t s = lane; s < c; s += 32) sum += __ldg(a.pc + blk[s]);
   }
   sum = block_sum(sum, sh);

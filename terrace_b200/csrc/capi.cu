@@ -177,6 +177,14 @@ trc_status trc_release_scratch(trc_graph *g) {
   return guard([&] { G(g).release_scratch(); });
 }
 
+trc_status trc_debug_sort_wait(trc_graph *g, uint32_t spin_limit, int withhold_first_tile) {
+  return guard([&] {
+    trc::Graph &gr = G(g);
+    gr.sort_wait.spin_limit = spin_limit ? spin_limit : trc::SortWait{}.spin_limit;
+    gr.sort_wait.withhold_first = withhold_first_tile != 0;
+  });
+}
+
 trc_status trc_add_edge_batch(trc_graph *g, const uint32_t *src, const uint32_t *dst, uint64_t k,
                               uint32_t flags, uint64_t *applied) {
   return guard([&] {
@@ -328,8 +336,11 @@ trc_status trc_get_device_view(trc_graph *g, trc_device_view *out) {
     out->pbeg = v.pbeg;
     out->pma = v.pma;
     out->hub_of = v.hub_of;
-    out->hub_blk0 = v.hub_blk0;
-    out->hub_per = v.hub_per;
+    out->hub_dir0 = v.hub_dir0;
+    out->hub_nblk = v.hub_nblk;
+    out->hub_dir = v.hdir;
+    out->hub_pre = v.hpre;
+    out->hub_key = v.hkey;
     out->hslot = v.hslot;
     out->stream = gr.stream;
   });

@@ -10,6 +10,10 @@ namespace trc {
 
 constexpr uint64_t KEY_INVALID = ~0ull;
 
+// Device address of the no-allocation BFS's static scratch array on the
+// current device (noalloc.cu).
+uint32_t *noalloc_scratch_resolve();
+
 // Lookup of (u, x) in the tiers (used by the update filter and is_edge).
 __device__ __forceinline__ bool has_edge(const DevView &G, uint32_t u, uint32_t x) {
   if (G.deg[u] == 0) return false;
@@ -25,6 +29,26 @@ struct ClassLists {
   uint64_t version = ~0ull;
   DBuf<uint32_t> S, M, Hv, SM, M1, M2, hub_blocks;
   uint64_t nS = 0, nM = 0, nH = 0, nSM = 0, nM1 = 0, nM2 = 0, nHB = 0;
+};
+
+// Tier-3 work of one batch between its two launch phases (hubs.cu).
+struct HubItem {
+  uint64_t i;  // index in the batch's touched-hub records
+  uint32_t h;  // hub index
+};
+struct HubCtx {
+  bool active = false, readback = false, insert = false;
+  uint32_t fill = 192;
+  uint64_t NL = 0, QL = 0, F = 0, fresh0 = 0;
+  std::vector<HubItem> loc, rw;
+  std::vector<uint64_t> lp;
+  uint64_t *d_lp = nullptr;
+  uint32_t *lli = nullptr, *lg = nullptr, *lx = nullptr, *tgq = nullptr, *tgo = nullptr;
+  uint32_t *tgb = nullptr, *hflag = nullptr, *stage = nullptr, *freed = nullptr, *pin = nullptr;
+  int32_t *hnbd = nullptr;
+  const uint32_t *hw_t = nullptr;
+  const uint64_t *bkeys = nullptr, *tpos = nullptr;
+  const std::vector<uint32_t> *hu = nullptr, *hdn = nullptr, *hdo = nullptr;
 };
 
 class Graph {
@@ -45,16 +69,32 @@ class Graph {
   DBuf<uint32_t> deg, inl, c2, pma, err;
   DBuf<uint64_t> pbeg;
   DBuf<int32_t> hub_of;
-  // hub tables (device) and their host mirrors
-  DBuf<uint32_t> hub_vtx, hub_nblk, hub_per;
-  DBuf<uint64_t> hub_blk0;
-  std::vector<uint32_t> h_hub_vtx, h_hub_capb;
-  std::vector<uint64_t> h_hub_blk0;
+  // tier 3 (hubs.cu): hub tables (device) and their host mirrors
+  DBuf<uint32_t> hub_vtx, hub_nblk;
+  DBuf<uint64_t> hub_dir0;
+  std::vector<uint32_t> h_hub_vtx, h_hub_nblk, h_hub_dcap;
+  std::vector<uint64_t> h_hub_dbase;  // the hub's directory region: two halves of dcap entries
+  std::vector<uint8_t> h_hub_dside;   // the half in use
   uint32_t H = 0;
-  // hub block pool
+  // directory pool (entries: block id, elements before the block, first key)
+  DBuf<uint32_t> hdir, hpre, hkey;
+  uint64_t DP = 0, dir_top = 0;
+  // block pool, and the ids of free blocks
   DBuf<uint32_t> hslot, bcnt, bmin, bown;
+  DBuf<uint32_t> bfree, bfreed;
   uint64_t NBP = 0;       // pool capacity in blocks
-  uint64_t pool_top = 0;  // blocks handed out
+  uint64_t pool_top = 0;  // blocks ever handed out
+  uint64_t nfree = 0;     // entries of bfree
+  // per-batch statistics of the blocked tier
+  uint64_t hub_last[6] = {0, 0, 0, 0, 0, 0};  // touched, local, rewritten, blocks written,
+                                              // elements read, elements written
+  uint64_t hub_splits = 0, hub_absorbs = 0, hub_rewrites = 0;
+  // tier-3 scratch
+  DBuf<uint32_t> s_lg, s_lx, s_lli, s_tgq, s_tgo, s_tgb, s_hflag, s_rwstage;
+  DBuf<int32_t> s_hnbd;
+  DBuf<uint64_t> s_hplan, s_hsel;
+  HubCtx hub_ctx_;
+  cudaEvent_t ev_hub = nullptr;  // the block-local group counts are on the host
 
   uint64_t N = 0;          // tier-2 capacity (slots)
   uint64_t m = 0;          // directed edges
@@ -66,6 +106,7 @@ class Graph {
   DBuf<uint64_t> pbeg_alt; // next tier-2 layout while a batch is applied
   uint64_t rebuilds = 0, window_rebalances = 0;
   uint64_t last[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // sizes of the last batch
+  SortWait sort_wait;  // bounded look-back wait of the batch sort (test hook)
 
   // ------------------------------------------------------------- scratch
   DBuf<uint32_t> s_in_src, s_in_dst;
@@ -119,6 +160,7 @@ class Graph {
   void msbc(const uint32_t *sources, uint32_t k, double *out, uint32_t flags);
   // BFS with scratch in a static device array (no allocation), noalloc.cu
   void bfs_noalloc(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags);
+  uint32_t *na_scratch = nullptr;  // that array's device address on this graph's device
   int device = 0;  // device the graph was created on
   void pagerank(uint32_t iters, double damping, double *ranks, uint32_t flags);
   // the iterations on stream s into caller buffers (n each); class lists
@@ -165,6 +207,26 @@ class Graph {
   uint32_t *hub_stage_ = nullptr;
   void grow_pool(uint64_t need_blocks);
   uint64_t *tmp(uint64_t elems) { return s_tmp.ensure(elems); }
+  void grow_dir_pool(uint64_t need);
+  uint32_t *hub_pin_ = nullptr;  // pinned staging of the tier-3 counts
+  uint64_t hub_pin_cap_ = 0;
+  uint32_t *hub_pin(uint64_t words);
+  uint64_t hub_dir_target(uint32_t h, uint32_t nb);
+
+ public:
+  // Tier-3 part of a batch (hubs.cu) on side_stream, in two launch phases
+  // around the small-vertex merge: apply_hubs takes the touched hubs' host
+  // records (vertex, new degree, hub index or -1, old degree), their device
+  // touched indices (hw_t, for each hub's slice of the sorted batch) and
+  // launches the block-local location and counting; apply_hubs_finish reads
+  // those counts, plans, launches the merges and rewrites and makes the
+  // graph's stream wait for them.  The host records must outlive both.
+  void apply_hubs(uint64_t nh, const std::vector<uint32_t> &hu, const std::vector<uint32_t> &hdn,
+                  const std::vector<int32_t> &hh, const std::vector<uint32_t> &hdo,
+                  const uint32_t *hw_t, const uint64_t *bkeys, const uint64_t *tpos, bool insert);
+  void apply_hubs_finish();
+  void hubs_finish();  // after the batch's final synchronisation
+  void hub_init();
 };
 
 // Copies between user buffers and device scratch, honouring TRC_DEVICE_PTR.

@@ -192,6 +192,11 @@ void adj_header(const std::vector<uint8_t> &b, uint64_t &n, uint64_t &m) {
   }
   n = std::stoull(w[1]);
   m = std::stoull(w[2]);
+  // range checks before any sum of the two: vertex ids are 32-bit, and a
+  // file of b bytes holds fewer than b/2 + 1 numbers
+  if (n > 0xFFFFFFFFull) throw_error(TRC_ERR_INVALID, "bad input file: n exceeds 2^32 - 1");
+  if (m > b.size() / 2 + 1)
+    throw_error(TRC_ERR_INVALID, "bad input file: m exceeds the numbers the file can hold");
 }
 
 }  // namespace

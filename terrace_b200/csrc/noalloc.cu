@@ -8,17 +8,19 @@
 // trc_bfs does allocate (level and frontier buffers, per-class vertex lists),
 // so this variant keeps its only scratch -- two frontier queues and a counter
 // -- in the file-scope array below.  It uses push steps only, which need no
-// per-class lists.  Every GPU that loads the library holds the array
-// (NOALLOC_BYTES) until the process exits.
+// per-class lists.
 //
 // The caller passes the outputs (parents and levels, device arrays of n
 // entries).  The array's name in host code is a host-side stand-in, not a
-// device address: the device address is looked up with cudaGetSymbolAddress
-// once per device, with that device current, on the first call on that
-// device.  All calls share the array, so calls that overlap on the GPU (two
-// host threads, two streams, two graphs) race on it.
-#include <mutex>
-
+// device address.  Its device address is looked up with cudaGetSymbolAddress
+// when a graph is created, with the graph's device current, and kept in the
+// graph: that lookup is also what loads this file's module (CUDA loads
+// modules lazily), so the array's NOALLOC_BYTES are reserved on the device
+// when the first graph is created there, not by the no-allocation call, and
+// stay reserved until the process exits.  A graph's copy of the address
+// lives no longer than the graph, which a device reset invalidates anyway.
+// All calls share the array, so calls that overlap on the GPU (two host
+// threads, two streams, two graphs) race on it.
 #include "graph.cuh"
 
 namespace trc {
@@ -30,31 +32,19 @@ constexpr uint64_t NOALLOC_BYTES = NOALLOC_WORDS * 4;  // 8 MiB + 256 B
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_WORDS];
 
-namespace {
-std::mutex g_na_mu;
-constexpr int NA_MAX_DEVICES = 64;
-uint32_t *g_na_ptr[NA_MAX_DEVICES] = {};
-
-// Device address of g_noalloc_scratch on the current device (set-up on the
-// first call per device).
-uint32_t *noalloc_scratch() {
-  int dev = 0;
-  TRC_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= NA_MAX_DEVICES) throw_error(TRC_ERR_STATE, "device index out of range");
-  std::lock_guard<std::mutex> lk(g_na_mu);
-  if (!g_na_ptr[dev]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      cudaGetLastError();
-      throw_error(TRC_ERR_CUDA, std::string("cudaGetSymbolAddress(noalloc scratch) failed: ") +
-                                    cudaGetErrorString(e));
-    }
-    g_na_ptr[dev] = static_cast<uint32_t *>(p);
+// Device address of g_noalloc_scratch on the current device.
+uint32_t *noalloc_scratch_resolve() {
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();
+    throw_error(TRC_ERR_CUDA, std::string("cudaGetSymbolAddress(noalloc scratch) failed: ") +
+                                  cudaGetErrorString(e));
   }
-  return g_na_ptr[dev];
+  return static_cast<uint32_t *>(p);
 }
 
+namespace {
 __device__ __forceinline__ uint32_t na_lanemask_lt() {
   uint32_t m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -114,7 +104,7 @@ void Graph::bfs_noalloc(uint32_t src, int32_t *parents, uint32_t *levels, uint32
   TRC_CUDA(cudaGetDevice(&prev));
   if (prev != device) TRC_CUDA(cudaSetDevice(device));
   try {
-    uint32_t *S = noalloc_scratch();
+    uint32_t *S = na_scratch;  // looked up when the graph was created
     uint32_t *F = S, *Nx = S + NOALLOC_QUEUE, *cnt = S + 2 * NOALLOC_QUEUE;
     TRC_LAUNCH(prof, stream, "na_init", ceil_div(n, 256), 256, 0, k_na_init, levels, parents, n, src,
                F);

@@ -16,14 +16,14 @@ namespace trc {
 // earlier tiles by decoupled look-back over a status word per (tile, digit)
 // (flag in the top bits, running count below; tiles take ids in launch
 // order from an atomic counter, so a tile only waits on tiles that started
-// before it).  The wait is bounded: after OS_SPIN_LIMIT polls the tile sets
-// ERR_TIMEOUT in the error word and proceeds (its output is then garbage and
-// the caller fails the call).
+// before it).  The wait is bounded: after SortWait::spin_limit polls the tile
+// sets ERR_TIMEOUT in the error word and proceeds (its output is then garbage
+// and the caller fails the call; every write stays inside the output, whose
+// digit ranges come from the full histogram).
 
 constexpr uint64_t OS_AGG = 1ull << 62;   // tile count published
 constexpr uint64_t OS_INC = 2ull << 62;   // count of this tile and all before it
 constexpr uint64_t OS_VAL = (1ull << 62) - 1;
-constexpr uint32_t OS_SPIN_LIMIT = 1u << 22;
 constexpr int OS_MAXD = 8;
 
 struct OsShifts {
@@ -59,7 +59,8 @@ __global__ void k_os_prefix(const unsigned long long *ghist, int nd, uint64_t *g
 __global__ void __launch_bounds__(RS_T) k_os_scatter(const uint64_t *in, uint64_t *out, uint64_t n,
                                                      int shift, const uint64_t *goff,
                                                      uint64_t *status, uint32_t *tile_ctr,
-                                                     uint32_t *err) {
+                                                     uint32_t *err, uint32_t spin_limit,
+                                                     uint32_t tile_base) {
   __shared__ uint32_t wh[RS_W][256];
   __shared__ uint64_t tbase[256];    // global start of digit d for this tile, minus its tile start
   __shared__ uint32_t dstart[256];   // start of digit d inside the tile (tile-sorted order)
@@ -67,7 +68,7 @@ __global__ void __launch_bounds__(RS_T) k_os_scatter(const uint64_t *in, uint64_
   __shared__ uint32_t tile_s;
   __shared__ uint32_t ws[RS_W + 1];
   for (int i = threadIdx.x; i < RS_W * 256; i += RS_T) (&wh[0][0])[i] = 0;
-  if (threadIdx.x == 0) tile_s = atomicAdd(tile_ctr, 1u);
+  if (threadIdx.x == 0) tile_s = atomicAdd(tile_ctr, 1u) + tile_base;
   __syncthreads();
   const uint32_t tile = tile_s;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -120,7 +121,7 @@ __global__ void __launch_bounds__(RS_T) k_os_scatter(const uint64_t *in, uint64_
         uint64_t v = st[(uint64_t)t * 256 + d];
         uint64_t f = v & ~OS_VAL;
         if (f == 0) {
-          if (++spins > OS_SPIN_LIMIT) {
+          if (++spins > spin_limit) {
             atomicOr(err, ERR_TIMEOUT);
             break;
           }
@@ -147,7 +148,9 @@ __global__ void __launch_bounds__(RS_T) k_os_scatter(const uint64_t *in, uint64_
     }
   }
   __syncthreads();
-  const uint32_t valid = n - tile0 < (uint64_t)RS_TILE ? (uint32_t)(n - tile0) : (uint32_t)RS_TILE;
+  // (a tile past the end exists only when tile ids start at 1: no keys)
+  const uint32_t valid = tile0 >= n ? 0u
+                         : n - tile0 < (uint64_t)RS_TILE ? (uint32_t)(n - tile0) : (uint32_t)RS_TILE;
   for (uint32_t j = threadIdx.x; j < valid; j += RS_T) {
     uint64_t x = stage[j];
     uint32_t d = (uint32_t)(x >> shift) & 255u;
@@ -157,25 +160,26 @@ __global__ void __launch_bounds__(RS_T) k_os_scatter(const uint64_t *in, uint64_
 
 uint64_t radix_tmp_elems(uint64_t n) {
   uint64_t tiles = ceil_div(n, RS_TILE);
-  // histograms + digit starts (OS_MAXD x 256 each), status (tiles x 256 per
-  // digit position, cleared once per sort), tile counters (one word per
-  // digit position)
-  return 2 * OS_MAXD * 256 + (uint64_t)OS_MAXD * tiles * 256 + OS_MAXD + 2;
+  // histograms + digit starts (OS_MAXD x 256 each), status ((tiles + 1) x
+  // 256 per digit position -- one spare tile for SortWait::withhold_first --
+  // cleared once per sort), tile counters (one word per digit position)
+  return 2 * OS_MAXD * 256 + (uint64_t)OS_MAXD * (tiles + 1) * 256 + OS_MAXD + 2;
 }
 
 uint64_t *radix_sort_u64(uint64_t *keys, uint64_t *alt, uint64_t n, uint32_t vbits,
-                         uint64_t *tmp, cudaStream_t s, Profiler &prof, uint32_t *err) {
+                         uint64_t *tmp, cudaStream_t s, Profiler &prof, uint32_t *err,
+                         const SortWait &wait) {
   // digit shifts: dst bits [0,vbits) and src bits [32,32+vbits)
   int shifts[16];
   int ns = 0;
   for (int sh = 0; sh < (int)vbits; sh += 8) shifts[ns++] = sh;
   for (int sh = 32; sh < 32 + (int)vbits; sh += 8) shifts[ns++] = sh;
-  return radix_sort_u64_shifts(keys, alt, n, shifts, ns, tmp, s, prof, err);
+  return radix_sort_u64_shifts(keys, alt, n, shifts, ns, tmp, s, prof, err, wait);
 }
 
 uint64_t *radix_sort_u64_shifts(uint64_t *keys, uint64_t *alt, uint64_t n, const int *shifts,
                                 int ns, uint64_t *tmp, cudaStream_t s, Profiler &prof,
-                                uint32_t *err) {
+                                uint32_t *err, const SortWait &wait) {
   if (n <= 1 || ns == 0) return keys;
   if (ns > OS_MAXD) throw_error(TRC_ERR_INVALID, "too many radix digits");
   const uint64_t ntiles = ceil_div(n, RS_TILE);
@@ -183,20 +187,22 @@ uint64_t *radix_sort_u64_shifts(uint64_t *keys, uint64_t *alt, uint64_t n, const
   unsigned long long *ghist = (unsigned long long *)tmp;
   uint64_t *goff = tmp + OS_MAXD * 256;
   uint64_t *status = goff + OS_MAXD * 256;
-  uint32_t *ctr = (uint32_t *)(status + (uint64_t)ns * ntiles * 256);
+  const uint64_t sstride = (ntiles + 1) * 256;  // status words per digit pass
+  uint32_t *ctr = (uint32_t *)(status + (uint64_t)ns * sstride);
   OsShifts sh;
   sh.n = ns;
   for (int i = 0; i < OS_MAXD; i++) sh.s[i] = i < ns ? shifts[i] : 0;
   TRC_CUDA(cudaMemsetAsync(ghist, 0, (size_t)OS_MAXD * 256 * 8, s));
   TRC_CUDA(cudaMemsetAsync(ctr, 0, (size_t)OS_MAXD * 4, s));
-  TRC_CUDA(cudaMemsetAsync(status, 0, (size_t)ns * ntiles * 256 * 8, s));
+  TRC_CUDA(cudaMemsetAsync(status, 0, (size_t)ns * sstride * 8, s));
   const unsigned hgrid = (unsigned)std::min<uint64_t>(ceil_div(n, RS_T * 8), (uint64_t)num_sms() * 8);
   TRC_LAUNCH(prof, s, "radix_hist", hgrid, RS_T, 0, k_os_hist, keys, n, sh, ghist);
   TRC_LAUNCH(prof, s, "radix_prefix", 1, RS_T, 0, k_os_prefix, ghist, ns, goff);
   uint64_t *cur = keys, *nxt = alt;
   for (int i = 0; i < ns; i++) {
     TRC_LAUNCH(prof, s, "radix_scatter", ntiles, RS_T, 0, k_os_scatter, cur, nxt, n, shifts[i],
-               goff + i * 256, status + (uint64_t)i * ntiles * 256, ctr + i, err);
+               goff + i * 256, status + (uint64_t)i * sstride, ctr + i, err, wait.spin_limit,
+               wait.withhold_first ? 1u : 0u);
     uint64_t *t = cur;
     cur = nxt;
     nxt = t;

@@ -234,17 +234,28 @@ constexpr int RS_I = 16;
 constexpr int RS_TILE = RS_T * RS_I;  // 4096 keys
 constexpr int RS_W = RS_T / 32;
 
+// The bounded look-back wait of the scatter passes: a tile gives up after
+// spin_limit polls of a predecessor that has not published.  withhold_first
+// (tests of that bound only) starts the tile ids at 1, so no tile 0 ever
+// publishes and every wait runs out; the keys of tile 0 are then not sorted
+// and the call must fail.
+struct SortWait {
+  uint32_t spin_limit = 1u << 22;
+  uint32_t withhold_first = 0;
+};
+
 // Sorts keys[0..n) using alt as the ping-pong buffer; returns the buffer that
 // holds the result (keys or alt).  tmp needs radix_tmp_elems(n) entries.
 // err: device error word; ERR_TIMEOUT is or-ed in if a look-back wait gave
 // up (the caller must then fail the call).
 uint64_t *radix_sort_u64(uint64_t *keys, uint64_t *alt, uint64_t n, uint32_t vbits,
-                         uint64_t *tmp, cudaStream_t s, Profiler &prof, uint32_t *err);
+                         uint64_t *tmp, cudaStream_t s, Profiler &prof, uint32_t *err,
+                         const SortWait &wait = SortWait{});
 // Same, over an explicit list of at most 8 digit shifts (least significant
 // first).
 uint64_t *radix_sort_u64_shifts(uint64_t *keys, uint64_t *alt, uint64_t n, const int *shifts,
                                 int ns, uint64_t *tmp, cudaStream_t s, Profiler &prof,
-                                uint32_t *err);
+                                uint32_t *err, const SortWait &wait = SortWait{});
 uint64_t radix_tmp_elems(uint64_t n);
 
 // ------------------------------------------------------------ merge path

@@ -95,7 +95,9 @@ __global__ void k_dump(DevView G, const uint64_t *off, uint32_t *tgt) {
 // Invariant checker: one warp per vertex, counts violations.
 //  - list strictly increasing, entries < n
 //  - non-hub: c2 == max(deg-16, 0) and segment inside [pbeg[u], pbeg[u+1])
-//  - hub: c2 == 0; blocks used == ceil(rest/per); bcnt/bmin/bown consistent
+//  - hub: c2 == 0; directory entries in key order with 1..256 elements per
+//    block, prefixes and first keys equal to the blocks' counts and first
+//    slots, owner u, the counts summing to deg-16 (no blocks when deg <= 16)
 //  - pbeg non-decreasing, pbeg[n] == N
 __global__ void k_check(DevView G, unsigned long long *bad) {
   uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -113,31 +115,36 @@ __global__ void k_check(DevView G, unsigned long long *bad) {
     if (x >= G.n) nbad++;
     if (j > 0 && L.at(j - 1) >= x) nbad++;
   }
-  if (lane == 0) {
-    int32_t h = G.hub_of[u];
-    uint32_t d = G.deg[u];
-    uint32_t rest = d > K_INLINE ? d - K_INLINE : 0;
-    if (G.pbeg[u] > G.pbeg[u + 1]) nbad++;
-    if (h < 0) {
-      if (G.c2[u] != rest) nbad++;
-      if (G.pbeg[u] + G.c2[u] > G.pbeg[u + 1]) nbad++;
-    } else {
+  const int32_t h = G.hub_of[u];
+  const uint32_t d = G.deg[u];
+  const uint32_t rest = d > K_INLINE ? d - K_INLINE : 0;
+  if (h >= 0) {
+    const uint64_t e0 = G.hub_dir0[h];
+    const uint32_t nb = G.hub_nblk[h];
+    uint32_t sum = 0;  // lane-local part of the element total
+    for (uint32_t i = lane; i < nb; i += 32) {
+      const uint32_t b = G.hdir[e0 + i];
+      const uint32_t c = G.bcnt[b];
+      const uint32_t next = i + 1 < nb ? G.hpre[e0 + i + 1] : rest;
+      if (c == 0 || c > HUB_BLOCK) nbad++;
+      if (next - G.hpre[e0 + i] != c) nbad++;
+      if (G.bown[b] != u) nbad++;
+      if (c && (G.bmin[b] != G.hslot[(uint64_t)b * HUB_BLOCK] || G.hkey[e0 + i] != G.bmin[b])) nbad++;
+      sum += c;
+    }
+    sum = warp_sum(sum);
+    if (lane == 0) {
+      if (sum != rest) nbad++;
+      if (nb && G.hpre[e0] != 0) nbad++;
+      if (rest == 0 && nb != 0) nbad++;
       if (G.c2[u] != 0) nbad++;
       if (G.hub_vtx[h] != u) nbad++;
-      uint32_t per = G.hub_per[h], nb = G.hub_nblk[h];
-      uint32_t want = rest ? (rest + per - 1) / (per ? per : 1) : 0;
-      if (nb != want || (rest && (per == 0 || per > HUB_BLOCK))) nbad++;
-      uint64_t b0 = G.hub_blk0[h];
-      uint32_t sum = 0;
-      for (uint32_t b = 0; b < nb; b++) {
-        uint32_t c = G.bcnt[b0 + b];
-        sum += c;
-        if (G.bown[b0 + b] != u) nbad++;
-        if (c && G.bmin[b0 + b] != G.hslot[(b0 + b) * HUB_BLOCK]) nbad++;
-      }
-      if (sum != rest) nbad++;
     }
+  } else if (lane == 0) {
+    if (G.c2[u] != rest) nbad++;
+    if (G.pbeg[u] + G.c2[u] > G.pbeg[u + 1]) nbad++;
   }
+  if (lane == 0 && G.pbeg[u] > G.pbeg[u + 1]) nbad++;
   nbad = warp_sum(nbad);
   if (lane == 0 && nbad) atomicAdd(bad, (unsigned long long)nbad);
 }
@@ -243,8 +250,8 @@ uint64_t Graph::check() {
 
 uint64_t Graph::size_bytes() const {
   return deg.bytes() + inl.bytes() + c2.bytes() + pbeg.bytes() + hub_of.bytes() + pma.bytes() +
-         hub_vtx.bytes() + hub_nblk.bytes() + hub_per.bytes() + hub_blk0.bytes() + hslot.bytes() +
-         bcnt.bytes() + bmin.bytes() + bown.bytes();
+         hub_vtx.bytes() + hub_nblk.bytes() + hub_dir0.bytes() + hdir.bytes() + hpre.bytes() +
+         hkey.bytes() + hslot.bytes() + bcnt.bytes() + bmin.bytes() + bown.bytes() + bfree.bytes();
 }
 
 void Graph::stats(trc_stats *o) {
@@ -253,7 +260,7 @@ void Graph::stats(trc_stats *o) {
   o->pma_edges = tier2_total;
   o->pma_capacity = N;
   o->num_hubs = H;
-  o->hub_blocks_used = pool_top;
+  o->hub_blocks_used = pool_top - nfree;
   o->device_bytes = budget.used;
   o->pma_rebuilds = rebuilds;
   o->pma_window_rebalances = window_rebalances;
@@ -265,6 +272,16 @@ void Graph::stats(trc_stats *o) {
   o->last_written = last[5];
   o->last_windows = last[6];
   o->last_rebuild = last[7];
+  o->last_hub_touched = hub_last[0];
+  o->last_hub_local = hub_last[1];
+  o->last_hub_rewritten = hub_last[2];
+  o->last_hub_blocks_written = hub_last[3];
+  o->last_hub_read = hub_last[4];
+  o->last_hub_written = hub_last[5];
+  o->hub_splits = hub_splits;
+  o->hub_rewrites = hub_rewrites;
+  o->hub_blocks_free = nfree;
+  o->hub_absorbs = hub_absorbs;
   // inline = sum(min(deg,16)); hub = m - inline - tier2
   uint64_t *t = tmp(scan_tmp_elems(n) + 4);
   uint64_t *off = s_oOff.ensure((uint64_t)n + 1);

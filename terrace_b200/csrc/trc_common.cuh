@@ -25,7 +25,8 @@ namespace trc {
 // separate arrays, so the row holds 16.
 constexpr uint32_t K_INLINE = 16;
 constexpr uint32_t HUB_THRESHOLD_MAX = 12288;  // largest configurable hub threshold
-// Tier 3: hub neighbours are kept in blocks of HUB_BLOCK slots.
+// Tier 3: hub neighbours are kept in blocks of HUB_BLOCK slots, found through
+// a per-hub directory (see DevView).
 constexpr uint32_t HUB_BLOCK = 256;
 constexpr uint32_t NONE32 = 0xFFFFFFFFu;
 
@@ -44,11 +45,22 @@ constexpr uint32_t ERR_TIMEOUT = 4u;
 //                 with slack up to pbeg[u+1]; pbeg[n] = capacity
 //   c2[n]         tier-2 element count (0 for hubs and low-degree vertices)
 //   hub_of[n]     hub index or -1
-//   hub tables    per hub: vertex, first block, blocks used, capacity in
-//                 blocks, elements per block ("per": blocks are filled
-//                 uniformly, so rank r of the hub part is at block r/per,
-//                 slot r%per)
-//   hslot/bcnt/bmin/bown   block pool: slots, count, first key, owner vertex
+//   tier 3, a two-level B-tree per hub (the reference's per-vertex BTree,
+//   include/btree.h:27-826, with one directory level over sorted leaves):
+//     hub_vtx[h], hub_nblk[h]   vertex; blocks in use
+//     hub_dir0[h]               the hub's directory in hdir/hpre/hkey: entry
+//                               i < hub_nblk[h] at hub_dir0[h] + i describes
+//                               the i-th block in key order --
+//     hdir[e]                   its pool block id,
+//     hpre[e]                   the number of hub elements before it (the
+//                               hub part starts at list rank 16), and
+//     hkey[e]                   its first (smallest) element
+//     hslot[b*256 ..], bcnt[b], bmin[b], bown[b]
+//                               block pool: slots (the first bcnt[b] used,
+//                               sorted), count, first key, owner vertex
+//   Rank r >= 16 of a hub is in the block whose hpre is the largest <= r-16;
+//   blocks are filled between 1 and 256 elements, so inserting or removing
+//   an edge rewrites one block (and the directory), not the whole list.
 struct DevView {
   uint32_t n;
   uint32_t hub_T;
@@ -60,9 +72,11 @@ struct DevView {
   uint64_t N;
   int32_t *hub_of;
   uint32_t *hub_vtx;
-  uint64_t *hub_blk0;
+  uint64_t *hub_dir0;
   uint32_t *hub_nblk;
-  uint32_t *hub_per;
+  uint32_t *hdir;
+  uint32_t *hpre;
+  uint32_t *hkey;
   uint32_t *hslot;
   uint32_t *bcnt;
   uint32_t *bmin;
@@ -70,20 +84,61 @@ struct DevView {
   uint32_t *err;  // device error word
 };
 
+// Directory entry of hub-part rank r (0 <= r < rest): the largest i < nb
+// with pre[i] <= r.  Blocks are mostly filled alike, so a proportional guess
+// usually hits; otherwise a binary search on the side it missed.
+__device__ __forceinline__ uint32_t hub_entry_of_rank(const uint32_t *pre, uint32_t nb,
+                                                      uint32_t rest, uint32_t r) {
+  uint32_t i = (uint32_t)(((uint64_t)r * nb) / (rest ? rest : 1));
+  if (i >= nb) i = nb - 1;
+  uint32_t lo, hi;
+  if (pre[i] > r) {
+    lo = 0;
+    hi = i;
+  } else if (i + 1 < nb && pre[i + 1] <= r) {
+    lo = i + 1;
+    hi = nb;
+  } else {
+    return i;
+  }
+  while (hi - lo > 1) {  // invariant: pre[lo] <= r, answer in [lo, hi)
+    uint32_t mid = (lo + hi) >> 1;
+    if (pre[mid] <= r) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Directory entry whose block holds key x if present: the largest i < nb
+// with key[i] <= x, or 0.
+__device__ __forceinline__ uint32_t hub_entry_of_key(const uint32_t *key, uint32_t nb, uint32_t x) {
+  uint32_t lo = 0, hi = nb;  // count of entries with key <= x
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (key[mid] <= x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo ? lo - 1 : 0;
+}
+
 // Read-only accessor for one vertex's sorted neighbour list by rank.
 struct NbrList {
   const uint32_t *inl;   // row
-  const uint32_t *seg;   // tier-2 segment (non-hub) or hub slot base
+  const uint32_t *seg;   // tier-2 segment (non-hub) or the block pool's slots (hub)
+  const uint32_t *dir;   // hub: block ids in key order
+  const uint32_t *pre;   // hub: elements before each block
+  const uint32_t *key;   // hub: first element of each block
   uint32_t ni;           // inline count
   uint32_t rest;         // elements after the inline ones
-  uint32_t per;          // hub: elements per block; 0 = tier-2 segment
+  uint32_t nb;           // hub: blocks; 0 = tier-2 segment (or no hub part)
   uint32_t deg;
 
   __device__ __forceinline__ uint32_t at(uint32_t r) const {
     if (r < ni) return inl[r];
     r -= ni;
-    if (per == 0) return seg[r];
-    return seg[(r / per) * HUB_BLOCK + (r % per)];
+    if (nb == 0) return seg[r];
+    const uint32_t i = hub_entry_of_rank(pre, nb, rest, r);
+    return seg[(uint64_t)dir[i] * HUB_BLOCK + (r - pre[i])];
   }
 };
 
@@ -97,17 +152,39 @@ __device__ __forceinline__ NbrList nbr_list(const DevView &G, uint32_t u) {
   int32_t h = G.hub_of[u];
   if (h < 0) {
     L.seg = G.pma + G.pbeg[u];
-    L.per = 0;
+    L.nb = 0;
+    L.dir = L.pre = L.key = nullptr;
   } else {
-    L.seg = G.hslot + G.hub_blk0[h] * HUB_BLOCK;
-    L.per = G.hub_per[h] ? G.hub_per[h] : 1;
+    const uint64_t e0 = G.hub_dir0[h];
+    L.seg = G.hslot;
+    L.nb = L.rest ? G.hub_nblk[h] : 0;
+    L.dir = G.hdir + e0;
+    L.pre = G.hpre + e0;
+    L.key = G.hkey + e0;
   }
   return L;
 }
 
-// Binary search for x in the neighbour list (lists are sorted, unique).
+// Binary search for x in the neighbour list (lists are sorted, unique); a
+// hub's blocked part is searched through its directory's first keys.
 __device__ __forceinline__ bool list_has(const NbrList &L, uint32_t x) {
   uint32_t lo = 0, hi = L.deg;
+  if (L.nb) {
+    if (L.ni == 0 || x > L.inl[L.ni - 1]) {
+      const uint32_t i = hub_entry_of_key(L.key, L.nb, x);
+      const uint32_t *b = L.seg + (uint64_t)L.dir[i] * HUB_BLOCK;
+      uint32_t blo = 0, bhi = (i + 1 < L.nb ? L.pre[i + 1] : L.rest) - L.pre[i];
+      while (blo < bhi) {
+        uint32_t mid = (blo + bhi) >> 1;
+        uint32_t v = b[mid];
+        if (v < x) blo = mid + 1;
+        else if (v > x) bhi = mid;
+        else return true;
+      }
+      return false;
+    }
+    hi = L.ni;  // x is at most the last inline element
+  }
   while (lo < hi) {
     uint32_t mid = (lo + hi) >> 1;
     uint32_t v = L.at(mid);
@@ -121,6 +198,20 @@ __device__ __forceinline__ bool list_has(const NbrList &L, uint32_t x) {
 // Number of list elements < x.
 __device__ __forceinline__ uint32_t list_lower_bound(const NbrList &L, uint32_t x) {
   uint32_t lo = 0, hi = L.deg;
+  if (L.nb) {
+    if (L.ni == 0 || x > L.inl[L.ni - 1]) {
+      const uint32_t i = hub_entry_of_key(L.key, L.nb, x);
+      const uint32_t *b = L.seg + (uint64_t)L.dir[i] * HUB_BLOCK;
+      uint32_t blo = 0, bhi = (i + 1 < L.nb ? L.pre[i + 1] : L.rest) - L.pre[i];
+      while (blo < bhi) {
+        uint32_t mid = (blo + bhi) >> 1;
+        if (b[mid] < x) blo = mid + 1;
+        else bhi = mid;
+      }
+      return L.ni + L.pre[i] + blo;
+    }
+    hi = L.ni;
+  }
   while (lo < hi) {
     uint32_t mid = (lo + hi) >> 1;
     if (L.at(mid) < x) lo = mid + 1;

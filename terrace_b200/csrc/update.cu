@@ -45,23 +45,27 @@ namespace trc {
 Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_), cfg(cfg_) {
   budget.limit = budget_bytes;
   TRC_CUDA(cudaGetDevice(&device));
+  na_scratch = noalloc_scratch_resolve();
   TRC_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
   TRC_CUDA(cudaStreamCreateWithFlags(&side_stream, cudaStreamNonBlocking));
   TRC_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
   TRC_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+  TRC_CUDA(cudaEventCreateWithFlags(&ev_hub, cudaEventDisableTiming));
   stream = own_stream;
   budget.stream = stream;
   budget.open_pool(device);
   use_graphs = cfg.cuda_graphs != 0;
   if (cfg.push_pull_divisor) tuned.push_pull_divisor = cfg.push_pull_divisor;
-  for (auto *b : {&deg, &inl, &c2, &pma, &err, &hub_vtx, &hub_nblk, &hub_per, &hslot, &bcnt, &bmin,
-                  &bown, &stamp, &s_in_src, &s_in_dst, &s_tu, &s_tdn, &s_tc2, &s_ovl, &s_hw_u,
-                  &s_hw_dn, &s_hw_t, &s_c2n, &s_rlist, &s_pma_next, &lists.S, &lists.M, &lists.Hv,
-                  &lists.SM, &lists.M1, &lists.M2, &lists.hub_blocks})
+  for (auto *b : {&deg, &inl, &c2, &pma, &err, &hub_vtx, &hub_nblk, &hdir, &hpre, &hkey, &hslot,
+                  &bcnt, &bmin, &bown, &bfree, &bfreed, &stamp, &s_in_src, &s_in_dst, &s_tu, &s_tdn,
+                  &s_tc2, &s_ovl, &s_hw_u, &s_hw_dn, &s_hw_t, &s_c2n, &s_rlist, &s_pma_next,
+                  &lists.S, &lists.M, &lists.Hv, &lists.SM, &lists.M1, &lists.M2, &lists.hub_blocks,
+                  &s_lg, &s_lx, &s_lli, &s_tgq, &s_tgo, &s_tgb, &s_hflag, &s_rwstage})
     b->bind(&budget);
-  for (auto *b : {&pbeg, &hub_blk0, &s_A, &s_B, &s_C, &s_tmp, &s_cnt, &s_P, &s_oOff, &s_nOff,
-                  &s_wk, &s_wk2, &s_mw, &s_old, &s_new, &s_hwplan, &s_mrec})
+  for (auto *b : {&pbeg, &hub_dir0, &s_A, &s_B, &s_C, &s_tmp, &s_cnt, &s_P, &s_oOff, &s_nOff,
+                  &s_wk, &s_wk2, &s_mw, &s_old, &s_new, &s_hwplan, &s_mrec, &s_hplan, &s_hsel})
     b->bind(&budget);
+  s_hnbd.bind(&budget);
   hub_of.bind(&budget);
   wstamp.bind(&budget);
   pbeg_alt.bind(&budget);
@@ -91,8 +95,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   TRC_CUDA(cudaMemsetAsync(stamp.get(), 0, nn * 4, stream));
   TRC_CUDA(cudaMemsetAsync(wstamp.get(), 0, nn * 4, stream));
   TRC_CUDA(cudaMemsetAsync(err.get(), 0, 16, stream));
-  grow_hub_tables(64);
-  grow_pool(64);
+  hub_init();
   sync();
   // last, so that nothing after it can throw out of the constructor
   TRC_CUDA(cudaMallocHost(&hub_stage_, 256 + 4 * 4 * HUB_SPEC));  // 32 counters, 4 hub arrays
@@ -108,6 +111,8 @@ Graph::~Graph() {
   // the graph's streams has finished)
   budget.stream = nullptr;
   if (hub_stage_) cudaFreeHost(hub_stage_);
+  if (hub_pin_) cudaFreeHost(hub_pin_);
+  if (ev_hub) cudaEventDestroy(ev_hub);
   if (ev_fork) cudaEventDestroy(ev_fork);
   if (ev_join) cudaEventDestroy(ev_join);
   if (side_stream) cudaStreamDestroy(side_stream);
@@ -126,9 +131,11 @@ DevView Graph::view() const {
   v.N = N;
   v.hub_of = hub_of.get();
   v.hub_vtx = hub_vtx.get();
-  v.hub_blk0 = hub_blk0.get();
+  v.hub_dir0 = hub_dir0.get();
   v.hub_nblk = hub_nblk.get();
-  v.hub_per = hub_per.get();
+  v.hdir = hdir.get();
+  v.hpre = hpre.get();
+  v.hkey = hkey.get();
   v.hslot = hslot.get();
   v.bcnt = bcnt.get();
   v.bmin = bmin.get();
@@ -140,12 +147,14 @@ DevView Graph::view() const {
 void Graph::release_scratch() {
   sync();
   for (auto *b : {&s_in_src, &s_in_dst, &s_tu, &s_tdn, &s_tc2, &s_ovl, &s_hw_u, &s_hw_dn, &s_hw_t,
-                  &s_c2n, &s_rlist, &s_pma_next, &s_tix, &s_hw_do, &s_wbits})
+                  &s_c2n, &s_rlist, &s_pma_next, &s_tix, &s_hw_do, &s_wbits, &s_lg, &s_lx, &s_lli,
+                  &s_tgq, &s_tgo, &s_tgb, &s_hflag, &s_rwstage, &bfreed})
     b->reset();
   for (auto *b : {&s_A, &s_B, &s_C, &s_tmp, &s_P, &s_oOff, &s_nOff, &s_wk, &s_wk2, &s_mw, &s_old,
-                  &s_new, &s_hwplan, &pbeg_alt, &s_mrec})
+                  &s_new, &s_hwplan, &pbeg_alt, &s_mrec, &s_hplan, &s_hsel})
     b->reset();
   s_hw_h.reset();
+  s_hnbd.reset();
   s_flags.reset();
   lists.version = ~0ull;
   for (auto *b : {&lists.S, &lists.M, &lists.Hv, &lists.SM, &lists.M1, &lists.M2, &lists.hub_blocks})
@@ -180,26 +189,6 @@ uint64_t Graph::read_u64(const uint64_t *dptr) {
   TRC_CUDA(cudaMemcpyAsync(&v, dptr, 8, cudaMemcpyDeviceToHost, stream));
   sync();
   return v;
-}
-
-void Graph::grow_hub_tables(uint32_t need) {
-  uint64_t cap = hub_vtx.capacity();
-  if (need <= cap && cap) return;
-  uint64_t nc = std::max<uint64_t>(need, cap * 2);
-  hub_vtx.grow(nc, H, stream);
-  hub_nblk.grow(nc, H, stream);
-  hub_per.grow(nc, H, stream);
-  hub_blk0.grow(nc, H, stream);
-}
-
-void Graph::grow_pool(uint64_t need_blocks) {
-  if (need_blocks <= NBP) return;
-  uint64_t nc = std::max<uint64_t>(need_blocks, NBP * 2);
-  hslot.grow(nc * HUB_BLOCK, pool_top * HUB_BLOCK, stream);
-  bcnt.grow(nc, pool_top, stream);
-  bmin.grow(nc, pool_top, stream);
-  bown.grow(nc, pool_top, stream);
-  NBP = nc;
 }
 
 // ---------------------------------------------------------------------------
@@ -294,10 +283,13 @@ __device__ __forceinline__ uint64_t warp_append64(bool take, unsigned long long 
 __global__ void k_classify(DevView G, const uint64_t *bkeys, const uint64_t *tpos, int insert,
                            uint32_t *tu, uint32_t *tdn, uint32_t *tc2, uint32_t *ovl,
                            uint32_t *hw_u, uint32_t *hw_dn, uint32_t *hw_t, int32_t *hw_h,
-                           uint32_t *hw_do, uint64_t *cnt) {
+                           uint32_t *hw_do, uint64_t *cnt, uint64_t cap) {
   const uint64_t nt = cnt[C_NT], kb = cnt[C_KB];  // on the device: no synchronisation before
   uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  bool valid = t < nt;
+  // t < cap too: cap (the touched tables' size) bounds nt for a sorted batch;
+  // after a failed sort (the call fails at the next synchronisation) the
+  // run count may be anything
+  bool valid = t < nt && t < cap;
   uint32_t u = 0, dn = 0, d = 0;
   int32_t h = -1;
   bool hub = false, over = false;
@@ -337,9 +329,9 @@ __global__ void k_classify(DevView G, const uint64_t *bkeys, const uint64_t *tpo
 }
 
 __global__ void k_scatter_c2(const uint32_t *tu, const uint32_t *tc2, const uint64_t *nt,
-                             uint32_t *c2n) {
+                             uint64_t cap, uint32_t *c2n) {
   uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < *nt) c2n[tu[t]] = tc2[t];
+  if (t < *nt && t < cap) c2n[tu[t]] = tc2[t];
 }
 
 struct LoadC2 {
@@ -509,77 +501,6 @@ struct NewDeg {
     return t != NONE32 ? tdn[t] : deg[u];
   }
 };
-
-// Gather old lists of the rewrite set as sorted 64-bit keys (warp/vertex).
-__global__ void k_gather_old(DevView G, const uint32_t *rlist, uint64_t nr, const uint64_t *oOff,
-                             uint64_t *out) {
-  uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  uint32_t lane = threadIdx.x & 31;
-  if (w >= nr) return;
-  uint32_t u = rlist[w];
-  NbrList L = nbr_list(G, u);
-  uint64_t base = oOff[w];
-  uint64_t hi = (uint64_t)u << 32;
-  for (uint32_t j = lane; j < L.deg; j += 32) out[base + j] = hi | L.at(j);
-}
-
-// Hub table update from the host plan.  plan rows: {h, u, blk0, nb, per, capb}.
-__global__ void k_apply_hub_plan(DevView G, const uint64_t *plan, uint64_t nh) {
-  uint64_t i = blockIdx.x;
-  if (i >= nh) return;
-  const uint64_t *p = plan + 6 * i;
-  uint32_t h = (uint32_t)p[0], u = (uint32_t)p[1];
-  uint64_t blk0 = p[2];
-  uint32_t nb = (uint32_t)p[3], per = (uint32_t)p[4], capb = (uint32_t)p[5];
-  if (threadIdx.x == 0) {
-    G.hub_vtx[h] = u;
-    G.hub_blk0[h] = blk0;
-    G.hub_nblk[h] = nb;
-    G.hub_per[h] = per;
-    G.hub_of[u] = (int32_t)h;
-  }
-  for (uint32_t b = nb + threadIdx.x; b < capb; b += blockDim.x) {
-    G.bcnt[blk0 + b] = 0;
-    G.bown[blk0 + b] = NONE32;
-  }
-}
-
-// Scatter new lists of the rewrite set into the tiers (warp/vertex).
-__global__ void k_scatter_new(DevView G, const uint32_t *rlist, uint64_t nr, const uint64_t *nOff,
-                              const uint64_t *src) {
-  uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  uint32_t lane = threadIdx.x & 31;
-  if (w >= nr) return;
-  uint32_t u = rlist[w];
-  uint64_t base = nOff[w];
-  uint32_t dn = (uint32_t)(nOff[w + 1] - base);
-  uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
-  uint32_t ni = dn < K_INLINE ? dn : K_INLINE;
-  if (lane < ni) row[lane] = (uint32_t)src[base + lane];
-  if (dn > K_INLINE) {
-    uint32_t rest = dn - K_INLINE;
-    int32_t h = G.hub_of[u];
-    if (h < 0) {
-      uint32_t *dst = G.pma + G.pbeg[u];
-      for (uint32_t j = lane; j < rest; j += 32) dst[j] = (uint32_t)src[base + K_INLINE + j];
-    } else {
-      uint64_t blk0 = G.hub_blk0[h];
-      uint32_t per = G.hub_per[h];
-      for (uint32_t j = lane; j < rest; j += 32) {
-        uint32_t b = j / per, s = j - b * per;
-        uint32_t v = (uint32_t)src[base + K_INLINE + j];
-        G.hslot[(blk0 + b) * HUB_BLOCK + s] = v;
-        if (s == 0) {
-          uint32_t c = rest - b * per;
-          G.bcnt[blk0 + b] = c < per ? c : per;
-          G.bmin[blk0 + b] = v;
-          G.bown[blk0 + b] = u;
-        }
-      }
-    }
-  }
-  if (lane == 0) G.deg[u] = dn;
-}
 
 __global__ void k_scatter_c2_final(const uint32_t *tu, const uint32_t *tc2, uint64_t nt,
                                    uint32_t *c2) {
@@ -771,7 +692,8 @@ __device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a,
   L.ni = L.deg < K_INLINE ? L.deg : K_INLINE;
   L.rest = L.deg - L.ni;
   L.seg = G.pma + (r.y >> MR_BITS);
-  L.per = 0;
+  L.nb = 0;
+  L.dir = L.pre = L.key = nullptr;
   const uint32_t d = L.deg;
   const uint64_t *B = a.bkeys + b0;
   uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
@@ -894,109 +816,10 @@ __global__ void k_window_mark2(const uint64_t *mw, uint32_t n, uint32_t *stamp, 
   }
 }
 
-// Fused merge for touched hubs, one CTA per hub: the old list (inline row +
-// blocks, or inline row + PMA segment for a vertex promoted now) is staged in
-// shared memory, output ranks come from binary searches as in k_merge_small,
-// and the new list is written to the hub's region (from the host plan) with
-// uniform block fill; thread 0 then updates the hub tables.
-struct HubMergeArgs {
-  const uint64_t *plan;  // rows {h, u, blk0, nb, per, capb}
-  uint64_t nh;
-  const uint32_t *tix;
-  const uint64_t *tpos;
-  uint64_t nt, kb;
-  const uint64_t *bkeys;
-  int insert;
-};
-
-__global__ void __launch_bounds__(256) k_merge_hub(DevView G, HubMergeArgs a) {
-  extern __shared__ uint32_t A[];
-  const uint64_t *p = a.plan + 6 * (uint64_t)blockIdx.x;
-  const uint32_t h = (uint32_t)p[0], u = (uint32_t)p[1];
-  const uint64_t blk0 = p[2];
-  const uint32_t nbn = (uint32_t)p[3], per = (uint32_t)p[4], capb = (uint32_t)p[5];
-  NbrList L = nbr_list(G, u);  // old tier pointers
-  const uint32_t d = L.deg;
-  for (uint32_t j = threadIdx.x; j < d; j += blockDim.x) A[j] = L.at(j);
-  const uint32_t t = a.tix[u];
-  const uint64_t b0 = a.tpos[t];
-  const uint64_t b1 = t + 1 < a.nt ? a.tpos[t + 1] : a.kb;
-  const uint32_t nb = (uint32_t)(b1 - b0);
-  const uint64_t *B = a.bkeys + b0;
-  const uint32_t dn = a.insert ? d + nb : d - nb;
-  const uint32_t rest = dn > K_INLINE ? dn - K_INLINE : 0;
-  __syncthreads();
-  uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
-  auto put = [&](uint32_t r, uint32_t x) {
-    if (r < K_INLINE) {
-      row[r] = x;
-      return;
-    }
-    uint32_t rr = r - K_INLINE;
-    uint32_t bi = rr / per, si = rr - bi * per;
-    G.hslot[(blk0 + bi) * HUB_BLOCK + si] = x;
-    if (si == 0) {
-      uint32_t c = rest - bi * per;
-      G.bcnt[blk0 + bi] = c < per ? c : per;
-      G.bmin[blk0 + bi] = x;
-      G.bown[blk0 + bi] = u;
-    }
-  };
-  if (a.insert) {
-    for (uint32_t i = threadIdx.x; i < d; i += blockDim.x) {
-      uint32_t x = A[i];
-      put(i + lower_bound_keys(B, nb, x), x);
-    }
-    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
-      uint32_t x = (uint32_t)B[j];
-      put(j + lower_bound_u32(A, d, x), x);
-    }
-  } else {
-    for (uint32_t i = threadIdx.x; i < d; i += blockDim.x) {
-      uint32_t x = A[i];
-      uint32_t c = lower_bound_keys(B, nb, x);
-      if (c < nb && (uint32_t)B[c] == x) continue;
-      put(i - c, x);
-    }
-  }
-  for (uint32_t b = nbn + threadIdx.x; b < capb; b += blockDim.x) {
-    G.bcnt[blk0 + b] = 0;
-    G.bown[blk0 + b] = NONE32;
-  }
-  if (threadIdx.x == 0) {
-    G.hub_vtx[h] = u;
-    G.hub_blk0[h] = blk0;
-    G.hub_nblk[h] = nbn;
-    G.hub_per[h] = per;
-    G.hub_of[u] = (int32_t)h;
-    G.deg[u] = dn;
-  }
-}
-
-// Keys of the batch whose source is in the sorted vertex list V.
-struct KeyInListPred {
-  const uint64_t *keys;
-  const uint32_t *V;
-  uint64_t nv;
-  __device__ bool operator()(uint64_t i) const {
-    uint32_t u = (uint32_t)(keys[i] >> 32);
-    uint64_t lo = 0, hi = nv;
-    while (lo < hi) {
-      uint64_t mid = (lo + hi) >> 1;
-      if (V[mid] < u) lo = mid + 1;
-      else hi = mid;
-    }
-    return lo < nv && V[lo] == u;
-  }
-};
-
 // Batches touching at least this many vertices search PMA windows before
 // the classify counts are read (one synchronisation less; the O(n) prefix of
 // the tier-2 counts is then computed even when no vertex overflows).
 constexpr uint64_t PLAN_SPECULATE = 1u << 16;
-
-// Largest old hub list the fused hub merge stages in shared memory (~192 KB).
-constexpr uint32_t HUB_SMEM_ELEMS = 48 * 1024;
 
 // ---------------------------------------------------------------------------
 // The pipeline
@@ -1005,6 +828,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
                             uint32_t flags, bool insert) {
   if (k == 0) return 0;
   if (!src_in || !dst_in) throw_error(TRC_ERR_INVALID, "null edge array");
+  for (auto &x : hub_last) x = 0;
   const int sym = (flags & TRC_SYMMETRIZE) ? 1 : 0;
   const int drop = (flags & TRC_DROP_SELF_LOOPS) ? 1 : 0;
   phase(nullptr);
@@ -1021,7 +845,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   TRC_LAUNCH(prof, stream, "upd_make_keys", ceil_div(k, 256), 256, 0, k_make_keys, src, dst, k, n,
              sym, drop, A, err.get());
   uint64_t *t = tmp(std::max(radix_tmp_elems(k2), select_tmp_elems(k2)));
-  uint64_t *sorted = radix_sort_u64(A, B, k2, vbits(), t, stream, prof, err.get());
+  uint64_t *sorted = radix_sort_u64(A, B, k2, vbits(), t, stream, prof, err.get(), sort_wait);
   uint64_t *bkeys = sorted == A ? B : A;
   // 3: unique + existence filter (one lookup per key), compacted
   uint8_t *kflags = s_flags.ensure(k2);
@@ -1044,7 +868,8 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   uint32_t *hw_u = s_hw_u.ensure(cap), *hw_dn = s_hw_dn.ensure(cap), *hw_t = s_hw_t.ensure(cap);
   int32_t *hw_h = s_hw_h.ensure(cap);
   TRC_LAUNCH(prof, stream, "upd_classify", ceil_div(cap, 256), 256, 0, k_classify, G, bkeys, tpos,
-             insert ? 1 : 0, tu, tdn, tc2, ovl, hw_u, hw_dn, hw_t, hw_h, s_hw_do.ensure(cap), cnt);
+             insert ? 1 : 0, tu, tdn, tc2, ovl, hw_u, hw_dn, hw_t, hw_h, s_hw_do.ensure(cap), cnt,
+             cap);
   // ---- PMA planning inputs: the new tier-2 counts c2n, their prefix P, and
   // (large batches) the window search on the device-side overflow count,
   // before the synchronisation that reads the counts; a rebuild decided
@@ -1061,7 +886,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     c2n = s_c2n.ensure(n);
     TRC_CUDA(cudaMemcpyAsync(c2n, c2.get(), (uint64_t)n * 4, cudaMemcpyDeviceToDevice, stream));
     TRC_LAUNCH(prof, stream, "upd_scatter_c2", ceil_div(cap, 256), 256, 0, k_scatter_c2, tu, tc2,
-               cnt + C_NT, c2n);
+               cnt + C_NT, cap, c2n);
     P = s_P.ensure((uint64_t)n + 1);
     uint64_t *st = tmp(scan_tmp_elems(n) + 4);
     exclusive_scan(LoadC2{c2n}, n, P, st, stream, prof, "scan_c2");
@@ -1123,13 +948,25 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   const uint64_t t2new = (uint64_t)((int64_t)tier2_total + t2delta);
 
   phase("classify");
-  // ---- hub plan (host): indices for new hubs, regions for grown ones.
-  std::vector<uint64_t> plan;
-  uint32_t hub_max_old = 0;
-  uint64_t hub_old_total = 0, hub_new_total = 0;
+  // ---- tier 3: the touched hubs' records, then the first launch phase of
+  // the hub update on the side stream (block-local groups located and
+  // counted) while the host plans tiers 1-2
+  std::vector<uint32_t> hu, hdn, hdo;
+  std::vector<int32_t> hh;
+  struct HubGuard {  // error path: no hub work may outlive the batch's buffers
+    Graph *g;
+    ~HubGuard() {
+      if (g->hub_ctx_.active || g->hub_ctx_.readback) {
+        g->hub_ctx_.active = g->hub_ctx_.readback = false;
+        cudaStreamSynchronize(g->side_stream);
+      }
+    }
+  } hub_guard{this};
   if (nh) {
-    std::vector<uint32_t> hu(nh), hdn(nh), hdo(nh);
-    std::vector<int32_t> hh(nh);
+    hu.resize(nh);
+    hdn.resize(nh);
+    hdo.resize(nh);
+    hh.resize(nh);
     if (nh <= spec) {
       memcpy(hu.data(), sp, nh * 4);
       memcpy(hdn.data(), sp + HUB_SPEC, nh * 4);
@@ -1142,43 +979,7 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
       TRC_CUDA(cudaMemcpyAsync(hdo.data(), s_hw_do.get(), nh * 4, cudaMemcpyDeviceToHost, stream));
       sync();
     }
-    for (uint64_t i = 0; i < nh; i++) {
-      hub_max_old = std::max(hub_max_old, hdo[i]);
-      hub_old_total += hdo[i];
-      hub_new_total += hdn[i];
-    }
-    plan.resize(6 * nh);
-    const double fill = cfg.hub_block_fill > 0 && cfg.hub_block_fill <= 1 ? cfg.hub_block_fill : 0.75;
-    const uint64_t blk_target = std::max<uint64_t>(1, (uint64_t)(HUB_BLOCK * fill));
-    uint64_t need_top = pool_top;
-    for (uint64_t i = 0; i < nh; i++) {
-      int32_t h = hh[i];
-      if (h < 0) {
-        h = (int32_t)H++;
-        h_hub_vtx.push_back(hu[i]);
-        h_hub_blk0.push_back(0);
-        h_hub_capb.push_back(0);
-      }
-      uint64_t rest = hdn[i] > K_INLINE ? hdn[i] - K_INLINE : 0;
-      uint64_t nb = rest ? ceil_div(rest, blk_target) : 0;
-      uint64_t per = nb ? ceil_div(rest, nb) : 0;
-      if (nb > h_hub_capb[h]) {
-        uint64_t capb = std::max<uint64_t>(nb + nb / 2, 2);
-        h_hub_blk0[h] = need_top;
-        h_hub_capb[h] = (uint32_t)capb;
-        need_top += capb;
-      }
-      uint64_t *p = &plan[6 * i];
-      p[0] = (uint64_t)h;
-      p[1] = hu[i];
-      p[2] = h_hub_blk0[h];
-      p[3] = nb;
-      p[4] = per;
-      p[5] = h_hub_capb[h];
-    }
-    grow_hub_tables(H);
-    grow_pool(need_top);
-    pool_top = need_top;
+    apply_hubs(nh, hu, hdn, hh, hdo, hw_t, bkeys, tpos, insert);
     G = view();
   }
 
@@ -1282,82 +1083,20 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     exclusive_scan(NewDeg{rs, deg.get(), tix, tdn}, nrs, oo, t5, stream, prof);
     SN = read_u64(oo + nrs);
   }
-  uint64_t SOh = 0, SNh = 0;
-  const bool hub_general =
-      nh && hub_max_old > std::min<uint32_t>(HUB_SMEM_ELEMS, cfg.hub_stage_limit);
   {
     MergeArgs ma{rs, 0, tix, tpos, nt, kb, bkeys, insert ? 1 : 0, pbeg_new, dst_pma, mov_pma,
                  nmw ? wstamp.get() : nullptr, epoch, T, dst_pma == pma.get() ? 1 : 0};
     static_assert(HUB_THRESHOLD_MAX <= MR_MASK, "merge record counts");
     ulonglong2 *rec = reinterpret_cast<ulonglong2 *>(s_mrec.ensure(2 * (uint64_t)n));
     TRC_LAUNCH(prof, stream, "upd_merge_prep", pgrid, 256, 0, k_merge_prep, G, ma, nrs_dev, rec);
-    // ---- hub path: fused CTA-per-hub merge (old lists staged in shared
-    // memory) on the side stream, concurrent with the small-vertex merge:
-    // the two touch disjoint vertices (hubs and vertices promoted now versus
-    // the rewrite list), nothing is allocated or freed on the graph's stream
-    // until the join, and window moves land after it.  Hubs too large for
-    // shared memory take the general gather / merge / scatter path below.
-    if (nh && !hub_general) {
-      static bool attr_set = false;
-      if (!attr_set) {
-        TRC_CUDA(cudaFuncSetAttribute(k_merge_hub, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(HUB_SMEM_ELEMS * 4)));
-        attr_set = true;
-      }
-      uint64_t *dplan = s_hwplan.ensure(plan.size());
-      TRC_CUDA(
-          cudaMemcpyAsync(dplan, plan.data(), plan.size() * 8, cudaMemcpyHostToDevice, stream));
-      HubMergeArgs ha{dplan, nh, tix, tpos, nt, kb, bkeys, insert ? 1 : 0};
-      size_t smem = (size_t)std::max<uint32_t>(hub_max_old, 1) * 4;
-      TRC_CUDA(cudaEventRecord(ev_fork, stream));
-      TRC_CUDA(cudaStreamWaitEvent(side_stream, ev_fork, 0));
-      TRC_LAUNCH(prof, side_stream, "upd_merge_hub", nh, 256, smem, k_merge_hub, G, ha);
-      TRC_CUDA(cudaEventRecord(ev_join, side_stream));
-      SOh = hub_old_total;
-      SNh = hub_new_total;
-    }
     TRC_LAUNCH(prof, stream, "upd_merge_small", pgrid, 256, 0, k_merge_small, G, ma, nrs_dev,
                (const ulonglong2 *)rec, (unsigned long long *)(cnt + C_MWORK));
-    if (nh && !hub_general) TRC_CUDA(cudaStreamWaitEvent(stream, ev_join, 0));
   }
-
   phase("merge_small");
-  if (hub_general) {
-    std::vector<uint32_t> rh(nh);
-    for (uint64_t i = 0; i < nh; i++) rh[i] = (uint32_t)plan[6 * i + 1];
-    std::sort(rh.begin(), rh.end());
-    uint32_t *drh = s_hw_t.ensure(nh);
-    TRC_CUDA(cudaMemcpyAsync(drh, rh.data(), nh * 4, cudaMemcpyHostToDevice, stream));
-    uint64_t *bkh = s_wk2.ensure(kb);
-    uint64_t *t6 = tmp(select_tmp_elems(kb) + scan_tmp_elems(nh) + 8);
-    select_if(KeyInListPred{bkeys, drh, nh}, LoadU64Val{bkeys}, kb, bkh, cnt + C_NW, t6, stream,
-              prof);
-    uint64_t *oOff = s_oOff.ensure(nh + 1), *nOff = s_nOff.ensure(nh + 1);
-    exclusive_scan(OldDeg{drh, deg.get()}, nh, oOff, t6, stream, prof);
-    exclusive_scan(NewDeg{drh, deg.get(), tix, tdn}, nh, nOff, t6, stream, prof);
-    uint64_t hcnt[1];
-    TRC_CUDA(cudaMemcpyAsync(&SOh, oOff + nh, 8, cudaMemcpyDeviceToHost, stream));
-    TRC_CUDA(cudaMemcpyAsync(&SNh, nOff + nh, 8, cudaMemcpyDeviceToHost, stream));
-    TRC_CUDA(cudaMemcpyAsync(hcnt, cnt + C_NW, 8, cudaMemcpyDeviceToHost, stream));
-    sync();
-    const uint64_t kbh = hcnt[0];
-    uint64_t *oldk = s_old.ensure(SOh + 1);
-    uint64_t *newk = s_new.ensure((SNh > SOh ? SNh : SOh) + 1);
-    TRC_LAUNCH(prof, stream, "upd_gather", ceil_div(nh * 32, 256), 256, 0, k_gather_old, G, drh, nh,
-               oOff, oldk);
-    if (insert) {
-      merge_u64(oldk, SOh, bkh, kbh, newk, stream, prof);
-    } else {
-      uint8_t *fl = s_flags.ensure(SOh + 1);
-      uint64_t *t7 = tmp(select_tmp_elems(SOh) + 4);
-      difference_u64(oldk, SOh, bkh, kbh, newk, cnt + C_KU, fl, t7, stream, prof);
-    }
-    uint64_t *dplan = s_hwplan.ensure(plan.size());
-    TRC_CUDA(cudaMemcpyAsync(dplan, plan.data(), plan.size() * 8, cudaMemcpyHostToDevice, stream));
-    TRC_LAUNCH(prof, stream, "upd_hub_plan", nh, 128, 0, k_apply_hub_plan, G, dplan, nh);
-    TRC_LAUNCH(prof, stream, "upd_scatter", ceil_div(nh * 32, 256), 256, 0, k_scatter_new, view(),
-               drh, nh, nOff, newk);
-  }
+  // ---- tier 3, second phase (the hubs touch vertices disjoint from the
+  // small-vertex merge's; the graph's stream waits for it before the window
+  // moves)
+  if (nh) apply_hubs_finish();
 
   phase("hub_path");
   // ---- window moves land after every reader of the old segments is done
@@ -1375,11 +1114,12 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
     N = Nn;
   }
   TRC_CUDA(cudaMemcpyAsync(&nrs, nrs_dev, 8, cudaMemcpyDeviceToHost, stream));
-  sync();  // host vectors (plan, rh) outlive their copies
+  sync();  // host vectors (the hub records) outlive their copies
   phase("finish");
+  hubs_finish();
   const uint64_t nr = nrs + nh;
-  SO += SOh;
-  SN += SNh;
+  SO += hub_last[4];
+  SN += hub_last[5];
   m = insert ? m + kb : m - kb;
   tier2_total = rebuild ? Ptot : t2new;
   last[0] = k2;

@@ -2,8 +2,8 @@
 profiling cases so both run the same batches).
 
 Update batch j of seed stream s is rMat(n, hash32(s) ^ j, ...), with the
-reference's hash32 (include/util.h hash32, Thomas Wang's 32-bit integer
-hash as used by graph_bm's batch generation, src/graph_bm.cc:341)."""
+reference's hash32 (include/rmat_util.h:44-52, Thomas Wang's 32-bit integer
+hash; graph_bm draws one rMat generator per batch, src/graph_bm.cc:342)."""
 
 
 def hash32(a: int) -> int:

@@ -107,8 +107,9 @@ def test_rmat_device_generator_bitexact(T):
 @pytest.mark.parametrize("hub_threshold,stage", [(1024, 49152), (64, 49152), (64, 100)])
 def test_update_sequence_matches_reference(T, name, hub_threshold, stage):
     """Bulk load, then every insert/delete batch of the fixture; the sorted
-    adjacency must equal the reference's after each step.  stage=100 sends
-    hubs through the general gather/merge/scatter path."""
+    adjacency must equal the reference's after each step.  stage=100 sends a
+    hub block receiving more than 100 batch edges through the whole-hub
+    rewrite instead of the block-local merge."""
     z = load(name)
     n = int(z["n"])
     g = graph_from_csr(T, z["s0_off"], z["s0_tgt"], hub_threshold=hub_threshold,
@@ -342,3 +343,95 @@ def test_msbc_equals_single_source_bc(T, n_log, k):
         nan = np.isnan(want)
         assert np.array_equal(np.isnan(out[i]), nan), i
         assert rel_close(out[i][~nan], want[~nan]), i
+
+
+@pytest.mark.parametrize("stage", [49152, 100])
+def test_blocked_tier_block_local_updates(T, stage):
+    """A hub of degree 100,000 (blocked tier, the reference's per-vertex
+    B-tree) under small and concentrated batches, every step matching the
+    oracle's set model: deletes that leave every other block under-full merge
+    those blocks with their untouched successors; scattered inserts land in
+    the touched blocks only (elements written scale with the blocks touched,
+    not with the hub's degree); a dense insert into one key range splits
+    blocks; deletes of a run empty whole blocks; deletes of the smallest
+    neighbours refill the inline row from the blocks; the hub shrinks into
+    its inline row and grows back.  stage=100 sends groups of more than 100
+    keys through the whole-hub rewrite instead."""
+    rng = np.random.default_rng(7)
+    n = 1 << 18
+    hub = 7
+    nb = np.sort(rng.choice(np.arange(1000, n, dtype=np.uint32), 100000, replace=False))
+    s, d = T.rmat_generate(n, 3, .5, .1, .1, 4 * n)
+    s, d = s[(s != hub) & (d != hub)], d[(s != hub) & (d != hub)]   # the hub's edges: nb only
+    g = T.Graph(n, hub_stage_limit=stage)
+    g.add_edge_batch(np.concatenate([s, np.full(len(nb), hub, np.uint32)]),
+                     np.concatenate([d, nb]), **SYM)
+    cur = O.key_union(O.make_keys(s, d, True, True),
+                      O.make_keys(np.full(len(nb), hub, np.uint32), nb, True, True))
+    assert g.degree(hub) == len(nb)
+
+    def hub_list():
+        off, tgt = O.csr_from_keys(n, cur)
+        return tgt[off[hub]:off[hub + 1]].copy()
+
+    def step(dst, insert):
+        nonlocal cur
+        src = np.full(len(dst), hub, np.uint32)
+        bk = O.make_keys(src, np.asarray(dst, np.uint32), True, True)
+        if insert:
+            g.add_edge_batch(src, dst, **SYM)
+            cur = O.key_union(cur, bk)
+        else:
+            g.remove_edge_batch(src, dst, **SYM)
+            cur = O.key_difference(cur, bk)
+        off, tgt = O.csr_from_keys(n, cur)
+        assert_same_csr(g, off, tgt)
+        return g.stats(), off, tgt
+
+    # 1. the bulk load filled blocks of `per` elements: empty most of every
+    # other block (30 left), whose untouched successor then joins it
+    rest = len(nb) - 16
+    per = -(-rest // -(-rest // 192))
+    hl = hub_list()
+    ranks = np.concatenate([np.arange(j * per + 10, j * per + per - 20)
+                            for j in range(0, rest // per - 1, 2)]) + 16
+    st, _, _ = step(hl[ranks], False)
+    if stage > 100:
+        assert st["last_hub_local"] == 1 and st["hub_absorbs"] > 100
+    # 2. fifty scattered new neighbours: block-local, few blocks written
+    hl = hub_list()
+    absent = np.setdiff1d(np.arange(1000, n, dtype=np.uint32), hl)
+    new = rng.choice(absent, 50, replace=False).astype(np.uint32)
+    st, _, _ = step(new, True)
+    assert st["last_hub_touched"] >= 1
+    if stage > 100:
+        assert st["last_hub_local"] >= 1
+        assert st["last_hub_written"] < 50 * 300 + 5000   # not the hub's ~75,000
+    # 3. a dense range of 3,000 new neighbours: splits (stage=100: a rewrite)
+    hl = hub_list()
+    lo = int(hl[len(hl) // 2])
+    dense = np.setdiff1d(np.arange(lo, lo + 40000, dtype=np.uint32), hl)[:3000]
+    splits0 = st["hub_splits"]
+    st, _, _ = step(dense, True)
+    if stage > 100:
+        assert st["hub_splits"] > splits0 and st["last_hub_rewritten"] == 0
+    else:
+        assert st["last_hub_rewritten"] >= 1
+    # 4. delete a run of 2,000 consecutive neighbours: whole blocks emptied
+    hl = hub_list()
+    free0 = st["hub_blocks_free"]
+    st, _, _ = step(hl[30000:32000], False)
+    if stage > 100:
+        assert st["hub_blocks_free"] > free0
+    # 5. delete the 300 smallest neighbours: the inline row refills
+    hl = hub_list()
+    st, off, tgt = step(hl[:300], False)
+    assert g.check() == 0
+    check_algorithms(g, off, tgt)
+    # 6. the hub shrinks into its inline row and grows back
+    hl = hub_list()
+    st, _, _ = step(hl[:-10], False)
+    assert g.degree(hub) == 10
+    st, off, tgt = step(hl, True)
+    assert g.check() == 0
+    g.close()

@@ -148,3 +148,29 @@ def test_adj_reader_pinned_to_reference():
                 b"AdjacencyGraph 2 1 1 0 1"):
         with pytest.raises(ValueError):
             O.parse_adj(bad)
+
+
+def test_tc_touching_equals_recount():
+    """The oracle's triangle delta (triangles that hold at least one edge of a
+    batch) against full recounts before and after inserting and removing
+    batches, on a skewed graph whose batches share edges with it and with
+    each other."""
+    n = 1 << 11
+    rng = np.random.default_rng(4)
+    s, d = O.rmat(n, 21, .57, .19, .19, 12 * n)
+    keys = O.make_keys(s, d, True, True)
+    t0 = O.tc(*O.csr_from_keys(n, keys))
+    for j in range(4):
+        bs, bd = O.rmat(n, 100 + j, .57, .19, .19, int(rng.integers(1, 4000)))
+        bk = O.make_keys(bs, bd, True, True)
+        new = O.key_difference(bk, keys)
+        g1 = O.key_union(keys, bk)
+        t1 = O.tc(*O.csr_from_keys(n, g1))
+        assert t1 - t0 == O.tc_touching(*O.csr_from_keys(n, g1), new)
+        h = len(bs) // 2
+        gone = O.key_intersection(g1, O.make_keys(bs[:h], bd[:h], True, True))
+        g2 = O.key_difference(g1, gone)
+        t2 = O.tc(*O.csr_from_keys(n, g2))
+        assert t1 - t2 == O.tc_touching(*O.csr_from_keys(n, g1), gone)
+        keys, t0 = g2, t2
+    assert O.tc_touching(*O.csr_from_keys(n, keys), np.zeros(0, np.uint64)) == 0
