@@ -590,8 +590,30 @@ class Server {
   // smallest BFS group run as one multi-source launch: up to three
   // single-source BFS (direction-optimising, compacted candidates) beat a
   // multi-source launch on RMAT scale 25 (3 sources: 27-30 ms one by one vs
-  // 34-42 ms together); from 4-8 sources the shared traversal wins
+  // 34-42 ms together)
   static constexpr size_t kMinGroup = 4;
+
+  // BFS grouping by measured cost.  The host time of one single-source BFS
+  // and, per group-size class (floor(log2 k)), the time per source of one
+  // multi-source launch are kept as exponentially weighted averages; a group
+  // of k runs as one multi-source launch only when that is estimated at most
+  // 3/4 of k single-source runs, because single runs complete one by one
+  // (each request as soon as its own traversal ends) while a group completes
+  // all its requests at its end.  A class without a measurement is tried
+  // once; until a single run has been timed, groups are not formed.
+  double bfs1_ms_ = 0;
+  double msb_per_ms_[8] = {};
+  static int size_class(size_t k) {
+    int c = 0;
+    while ((size_t)2 << c <= k) c++;
+    return c < 7 ? c : 7;
+  }
+  static void ewma(double &avg, double x) { avg = avg > 0 ? 0.75 * avg + 0.25 * x : x; }
+  bool group_pays(size_t k) const {
+    if (k < kMinGroup || bfs1_ms_ <= 0) return false;
+    const double per = msb_per_ms_[size_class(k)];
+    return per <= 0 || per <= 0.75 * bfs1_ms_;
+  }
 
   void run_bfs(std::vector<Request *> &bfs) {
     const uint32_t n = g_.n;
@@ -610,26 +632,36 @@ class Server {
           if (r->param >= n) r->status = TRC_ERR_INVALID;
           else bfs_one(r, full);
         }
-      } else if (k < kMinGroup) {  // below this, single-source BFS is faster
-        for (Request *r : grp) bfs_one(r, full);
-      } else if (full) {
-        std::vector<uint32_t> lv((uint64_t)k * n);
-        g_.msbfs(src.data(), (uint32_t)k, lv.data(), 0);
-        calls_++;
-        for (size_t j = 0; j < k; j++) {
-          const uint32_t *row = lv.data() + (uint64_t)j * n;
-          grp[j]->out_u32.assign(row, row + n);
-          grp[j]->out_count = n;
+      } else if (cfg_.mode == TRC_SERVE_FIFO || !group_pays(k)) {
+        // one by one, each request completing when its traversal ends
+        for (Request *r : grp) {
+          const double t0 = now_ms();
+          bfs_one(r, full);
+          ewma(bfs1_ms_, now_ms() - t0);
+          std::vector<Request *> one{r};
+          finish(one);
         }
       } else {
-        std::vector<uint64_t> reached(k);
-        std::vector<uint32_t> ecc(k);
-        g_.msbfs_summary(src.data(), (uint32_t)k, reached.data(), ecc.data());
-        calls_++;
-        for (size_t j = 0; j < k; j++) {
-          grp[j]->out_u32 = {(uint32_t)reached[j], ecc[j]};
-          grp[j]->out_count = reached[j];
+        const double t0 = now_ms();
+        if (full) {
+          std::vector<uint32_t> lv((uint64_t)k * n);
+          g_.msbfs(src.data(), (uint32_t)k, lv.data(), 0);
+          for (size_t j = 0; j < k; j++) {
+            const uint32_t *row = lv.data() + (uint64_t)j * n;
+            grp[j]->out_u32.assign(row, row + n);
+            grp[j]->out_count = n;
+          }
+        } else {
+          std::vector<uint64_t> reached(k);
+          std::vector<uint32_t> ecc(k);
+          g_.msbfs_summary(src.data(), (uint32_t)k, reached.data(), ecc.data());
+          for (size_t j = 0; j < k; j++) {
+            grp[j]->out_u32 = {(uint32_t)reached[j], ecc[j]};
+            grp[j]->out_count = reached[j];
+          }
         }
+        calls_++;
+        ewma(msb_per_ms_[size_class(k)], (now_ms() - t0) / (double)k);
       }
       finish(grp);
       i += k;
