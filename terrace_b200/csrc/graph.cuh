@@ -21,15 +21,31 @@ __device__ __forceinline__ bool has_edge(const DevView &G, uint32_t u, uint32_t 
   return list_has(L, x);
 }
 
-// Per-vertex class lists for the analytics kernels, rebuilt when the graph
+// Per-vertex class lists for the traversal kernels, rebuilt when the graph
 // version changes: S = 1..16 neighbours (inline only), M = more than 16 and
-// not a hub (inline + PMA segment), H = hubs.  hub_blocks lists every used
-// hub block (for block-parallel work on the blocked tier).
+// not a hub (inline + PMA segment), H = hubs, SM = S and M.
 struct ClassLists {
   uint64_t version = ~0ull;
-  DBuf<uint32_t> S, M, Hv, SM, M1, M2, hub_blocks;
-  uint64_t nS = 0, nM = 0, nH = 0, nSM = 0, nM1 = 0, nM2 = 0, nHB = 0;
+  DBuf<uint32_t> S, M, Hv, SM;
+  uint64_t nS = 0, nM = 0, nH = 0, nSM = 0;
 };
+
+// PageRank's snapshot of the graph (pagerank.cu), rebuilt when the graph
+// changes: non-isolated vertices relabelled by degree, highest first (perm:
+// new -> old id, inv: old -> new, dsort: degrees in the new order), their
+// lists as one CSR (off, adj: relabelled neighbour ids), and the degree
+// class boundaries of the pull kernels for the lane-group cut `cut`.
+struct PRSnap {
+  uint64_t version = ~0ull;
+  uint64_t na = 0, rb = 0, rw = 0, rg = 0;
+  uint32_t cut = 0;
+  DBuf<uint32_t> perm, inv, dsort, adj;
+  DBuf<uint64_t> off;
+};
+constexpr uint32_t PR_HOT_MAX = 16384;  // rank entries a pull CTA may stage in shared memory
+
+// Raises the pull kernels' dynamic shared memory limit on the current device.
+void pagerank_kernel_attributes();
 
 // Tier-3 work of one batch between its two launch phases (hubs.cu).
 struct HubItem {
@@ -121,6 +137,8 @@ class Graph {
   DBuf<uint32_t> s_wbits;  // per-level PMA window bitmaps (this batch)
   DBuf<uint32_t> s_hw_do;  // old degree of each touched hub
   ClassLists lists;
+  PRSnap prs;
+  void ensure_pr_snapshot();
 
   DevView view() const;
   uint32_t vbits() const;
@@ -196,6 +214,7 @@ class Graph {
     uint32_t pr_group_cut = 64;       // PageRank: degree 17..cut use a lane group
     uint32_t pr_group_lanes = 8;      // ... of this many lanes (4, 8 or 16); above: a warp
     uint32_t pma_leaf_log = 1;        // smallest PMA window: 2^x vertex segments
+    uint32_t pr_hot = 8192;           // PageRank: rank entries staged per CTA (<= PR_HOT_MAX)
   } tuned;
   void autotune(uint32_t what, const uint32_t *src, const uint32_t *dst, uint64_t k,
                 uint32_t flags, double *ms_out);

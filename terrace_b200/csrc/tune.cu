@@ -89,34 +89,46 @@ void Graph::autotune(uint32_t what, const uint32_t *src, const uint32_t *dst, ui
       cudaEvent_t e0, e1;
       TRC_CUDA(cudaEventCreate(&e0));
       TRC_CUDA(cudaEventCreate(&e1));
+      auto time2 = [&]() {  // two iterations, best of two
+        pagerank_launch(1, 0.0, p0, p1, out, stream);  // warm
+        float t = 1e30f;
+        for (int rep = 0; rep < 2; rep++) {
+          TRC_CUDA(cudaEventRecord(e0, stream));
+          pagerank_launch(2, 0.0, p0, p1, out, stream);
+          TRC_CUDA(cudaEventRecord(e1, stream));
+          TRC_CUDA(cudaEventSynchronize(e1));
+          float ms = 0;
+          TRC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          t = std::min(t, ms);
+        }
+        if (t < best) {
+          best = t;
+          best_t = tuned;
+        }
+      };
+      // lane group and cut first, then the staged rank entries
       for (uint32_t cut : {32u, 64u, 128u}) {
         tuned.pr_group_cut = cut;
-        lists.version = ~0ull;  // the class lists depend on the cut
-        ensure_lists();
+        ensure_pr_snapshot();  // class boundaries for the cut
         for (uint32_t lanes : {4u, 8u, 16u}) {
           tuned.pr_group_lanes = lanes;
-          pagerank_launch(1, 0.0, p0, p1, out, stream);  // warm
-          float t = 1e30f;
-          for (int rep = 0; rep < 2; rep++) {
-            TRC_CUDA(cudaEventRecord(e0, stream));
-            pagerank_launch(2, 0.0, p0, p1, out, stream);
-            TRC_CUDA(cudaEventRecord(e1, stream));
-            TRC_CUDA(cudaEventSynchronize(e1));
-            float ms = 0;
-            TRC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            t = std::min(t, ms);
-          }
-          if (t < best) {
-            best = t;
-            best_t = tuned;
-          }
+          time2();
         }
+      }
+      tuned.pr_group_cut = best_t.pr_group_cut;
+      tuned.pr_group_lanes = best_t.pr_group_lanes;
+      ensure_pr_snapshot();
+      for (uint32_t hot : {0u, 4096u, 16384u}) {
+        tuned.pr_hot = hot;
+        time2();
       }
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
       tuned.pr_group_cut = best_t.pr_group_cut;
       tuned.pr_group_lanes = best_t.pr_group_lanes;
+      tuned.pr_hot = best_t.pr_hot;
       lists.version = ~0ull;
+      ensure_pr_snapshot();
       ms_out[1] = best / 2.0;
     }
     // -------------------------------------------------- PMA leaf
