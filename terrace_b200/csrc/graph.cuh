@@ -134,6 +134,7 @@ class Graph {
   DBuf<uint8_t> s_flags;
   DBuf<uint32_t> s_pma_next;
   DBuf<uint32_t> s_tix;  // vertex -> index in the touched list (this batch)
+  DBuf<uint32_t> s_lgroup, s_lwarp;  // rewrite entries merged by a lane group / a warp
   DBuf<uint32_t> s_wbits;  // per-level PMA window bitmaps (this batch)
   DBuf<uint32_t> s_hw_do;  // old degree of each touched hub
   ClassLists lists;

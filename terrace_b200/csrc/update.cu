@@ -60,6 +60,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   for (auto *b : {&deg, &inl, &c2, &pma, &err, &hub_vtx, &hub_nblk, &hdir, &hpre, &hkey, &hslot,
                   &bcnt, &bmin, &bown, &bfree, &bfreed, &stamp, &s_in_src, &s_in_dst, &s_tu, &s_tdn,
                   &s_tc2, &s_ovl, &s_hw_u, &s_hw_dn, &s_hw_t, &s_c2n, &s_rlist, &s_pma_next,
+                  &s_lgroup, &s_lwarp,
                   &lists.S, &lists.M, &lists.Hv, &lists.SM,
                   &s_lg, &s_lx, &s_lli, &s_tgq, &s_tgo, &s_tgb, &s_hflag, &s_rwstage})
     b->bind(&budget);
@@ -151,6 +152,7 @@ void Graph::release_scratch() {
   sync();
   for (auto *b : {&s_in_src, &s_in_dst, &s_tu, &s_tdn, &s_tc2, &s_ovl, &s_hw_u, &s_hw_dn, &s_hw_t,
                   &s_c2n, &s_rlist, &s_pma_next, &s_tix, &s_hw_do, &s_wbits, &s_lg, &s_lx, &s_lli,
+                  &s_lgroup, &s_lwarp,
                   &s_tgq, &s_tgo, &s_tgb, &s_hflag, &s_rwstage, &bfreed})
     b->reset();
   for (auto *b : {&s_A, &s_B, &s_C, &s_tmp, &s_P, &s_oOff, &s_nOff, &s_wk, &s_wk2, &s_mw, &s_old,
@@ -672,18 +674,48 @@ __device__ __forceinline__ void put_rank(uint32_t *row, uint32_t *seg, uint32_t 
 constexpr uint32_t MR_BITS = 24;
 constexpr uint64_t MR_MASK = (1ull << MR_BITS) - 1;
 
-__global__ void k_merge_prep(DevView G, MergeArgs a, const uint64_t *nrs, ulonglong2 *rec) {
+// Rewrite entries whose old list has at most MG_D elements are merged by
+// MG_G lanes each (k_merge_group), the rest by a warp (k_merge_small); the
+// prep kernel sorts them into two index lists (counts in the batch's
+// counters C_NGROUP / C_NWARP).
+constexpr uint32_t MG_G = 8;   // lanes per short list
+constexpr uint32_t MG_R = 8;   // elements per lane: MG_G * MG_R covers a short list
+constexpr uint32_t MG_D = MG_G * MG_R;
+constexpr int C_NGROUP = 21, C_NWARP = 22;
+
+__global__ void k_merge_prep(DevView G, MergeArgs a, const uint64_t *nrs, ulonglong2 *rec,
+                             uint32_t *lgroup, uint32_t *lwarp, unsigned long long *cnt) {
   const uint64_t nw = *nrs;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += stride) {
-    const uint32_t u = a.rs[w];
-    const uint32_t t = a.tix[u];
-    uint64_t b0 = 0, b1 = 0;
-    if (t != NONE32) {
-      b0 = a.tpos[t];
-      b1 = t + 1 < a.nt ? a.tpos[t + 1] : a.kb;
+  // (every thread of a warp runs the same number of iterations)
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < nw; base += stride) {
+    const uint64_t w = base + threadIdx.x;
+    bool ok = w < nw, shortl = false;
+    if (ok) {
+      const uint32_t u = a.rs[w];
+      const uint32_t t = a.tix[u];
+      uint64_t b0 = 0, b1 = 0;
+      if (t != NONE32) {
+        b0 = a.tpos[t];
+        b1 = t + 1 < a.nt ? a.tpos[t + 1] : a.kb;
+      }
+      const uint32_t d = G.deg[u];
+      rec[w] = make_ulonglong2((b0 << MR_BITS) | (b1 - b0), (G.pbeg[u] << MR_BITS) | d);
+      shortl = d <= MG_D;
     }
-    rec[w] = make_ulonglong2((b0 << MR_BITS) | (b1 - b0), (G.pbeg[u] << MR_BITS) | G.deg[u]);
+    const uint32_t mg = __ballot_sync(0xFFFFFFFFu, ok && shortl);
+    const uint32_t mw = __ballot_sync(0xFFFFFFFFu, ok && !shortl);
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t bg = 0, bw = 0;
+    if (lane == 0) {
+      if (mg) bg = (uint32_t)atomicAdd(cnt + C_NGROUP, (unsigned long long)__popc(mg));
+      if (mw) bw = (uint32_t)atomicAdd(cnt + C_NWARP, (unsigned long long)__popc(mw));
+    }
+    bg = __shfl_sync(0xFFFFFFFFu, bg, 0);
+    bw = __shfl_sync(0xFFFFFFFFu, bw, 0);
+    const uint32_t below = (1u << lane) - 1u;
+    if (ok && shortl) lgroup[bg + __popc(mg & below)] = (uint32_t)w;
+    if (ok && !shortl) lwarp[bw + __popc(mw & below)] = (uint32_t)w;
   }
 }
 
@@ -779,18 +811,95 @@ __device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a,
 constexpr uint32_t MS_CHUNK = 8;
 
 __global__ void __launch_bounds__(256, 8) k_merge_small(DevView G, MergeArgs a,
-                                                        const uint64_t *nrs,
+                                                        const uint32_t *lwarp,
+                                                        const unsigned long long *cnt,
                                                         const ulonglong2 *rec,
                                                         unsigned long long *work) {
   const uint32_t lane = threadIdx.x & 31;
-  const uint64_t nw = *nrs;
+  const uint64_t nw = cnt[C_NWARP];
   for (;;) {
     uint64_t w0 = 0;
     if (lane == 0) w0 = atomicAdd(work, (unsigned long long)MS_CHUNK);
     w0 = __shfl_sync(0xFFFFFFFFu, w0, 0);
     if (w0 >= nw) break;
     const uint64_t w1 = w0 + MS_CHUNK < nw ? w0 + MS_CHUNK : nw;
-    for (uint64_t w = w0; w < w1; w++) merge_one(G, a, rec, w, lane);
+    for (uint64_t w = w0; w < w1; w++) merge_one(G, a, rec, lwarp[w], lane);
+  }
+}
+
+// MG_G lanes per short rewrite entry (old list of at most MG_D elements),
+// four entries per warp: the whole old list is loaded into registers (MG_R
+// per lane) before anything is written, so in place needs no ordering; each
+// element goes to its index plus the keys below it (insert: the lane holding
+// element i also writes the keys that land between element i-1 and i) or
+// minus the keys below it (remove), as merge_one does for one chunk.
+__global__ void __launch_bounds__(256, 4) k_merge_group(DevView G, MergeArgs a,
+                                                        const uint32_t *lgroup,
+                                                        const unsigned long long *cnt,
+                                                        const ulonglong2 *rec) {
+  const uint32_t lane = threadIdx.x & 31, g = lane & (MG_G - 1);
+  const unsigned mask = ((1u << MG_G) - 1u) << (lane & ~(MG_G - 1));
+  const uint64_t ng = *(cnt + C_NGROUP);
+  const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / MG_G;
+  for (uint64_t gi = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / MG_G; gi < ng;
+       gi += ngroups) {
+    const uint64_t w = lgroup[gi];
+    const uint32_t u = a.rs[w];
+    const ulonglong2 r = rec[w];
+    const uint64_t b0 = r.x >> MR_BITS;
+    const uint32_t nb = (uint32_t)(r.x & MR_MASK);
+    const uint32_t d = (uint32_t)(r.y & MR_MASK);
+    const uint32_t *oseg = G.pma + (r.y >> MR_BITS);  // old tier-2 elements, rank 16 on
+    uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
+    const uint64_t *B = a.bkeys + b0;
+    const bool moved = a.wstamp && a.wstamp[u] == a.epoch;
+    uint32_t *seg = (moved ? a.mov_pma : a.dst_pma) + a.pbeg_new[u];
+    const bool stay = a.inplace && !moved;
+    uint32_t x[MG_R], c[MG_R];
+#pragma unroll
+    for (uint32_t k = 0; k < MG_R; k++) {
+      const uint32_t i = k * MG_G + g;
+      x[k] = i < d ? (i < K_INLINE ? row[i] : oseg[i - K_INLINE]) : 0u;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < MG_R; k++) {
+      const uint32_t i = k * MG_G + g;
+      c[k] = i < d ? lower_bound_keys(B, nb, x[k]) : 0u;
+    }
+    __syncwarp(mask);
+    if (a.insert) {
+      // keys above every old element: ranks j + d
+      // (c of the last element counts the keys below it; the others are
+      // above it, since inserted keys are absent from the list)
+      uint32_t cl = 0;
+#pragma unroll
+      for (uint32_t k = 0; k < MG_R; k++)
+        if (d && k == (d - 1) / MG_G) cl = c[k];
+      const uint32_t ctop = d ? __shfl_sync(mask, cl, (d - 1) % MG_G, MG_G) : 0u;
+      for (uint32_t j = ctop + g; j < nb; j += MG_G) put_rank(row, seg, j + d, (uint32_t)B[j]);
+#pragma unroll
+      for (uint32_t k = 0; k < MG_R; k++) {
+        const uint32_t i = k * MG_G + g;
+        uint32_t cp = __shfl_up_sync(mask, c[k], 1, MG_G);
+        const uint32_t last = k > 0 ? __shfl_sync(mask, c[k > 0 ? k - 1 : 0], MG_G - 1, MG_G) : 0u;
+        if (g == 0) cp = last;
+        if (i < d) {
+          if (c[k] || !stay) put_rank(row, seg, i + c[k], x[k]);
+          for (uint32_t j = cp; j < c[k]; j++) put_rank(row, seg, j + i, (uint32_t)B[j]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (uint32_t k = 0; k < MG_R; k++) {
+        const uint32_t i = k * MG_G + g;
+        if (i < d) {
+          const uint32_t cc = c[k];
+          if (!(cc < nb && (uint32_t)B[cc] == x[k]) && (cc || !stay)) put_rank(row, seg, i - cc, x[k]);
+        }
+      }
+    }
+    if (g == 0) G.deg[u] = a.insert ? d + nb : d - nb;
+    __syncwarp(mask);
   }
 }
 
@@ -1095,9 +1204,14 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
                  nmw ? wstamp.get() : nullptr, epoch, T, dst_pma == pma.get() ? 1 : 0};
     static_assert(HUB_THRESHOLD_MAX <= MR_MASK, "merge record counts");
     ulonglong2 *rec = reinterpret_cast<ulonglong2 *>(s_mrec.ensure(2 * (uint64_t)n));
-    TRC_LAUNCH(prof, stream, "upd_merge_prep", pgrid, 256, 0, k_merge_prep, G, ma, nrs_dev, rec);
-    TRC_LAUNCH(prof, stream, "upd_merge_small", pgrid, 256, 0, k_merge_small, G, ma, nrs_dev,
-               (const ulonglong2 *)rec, (unsigned long long *)(cnt + C_MWORK));
+    uint32_t *lgroup = s_lgroup.ensure(n), *lwarp = s_lwarp.ensure(n);
+    unsigned long long *ucnt = reinterpret_cast<unsigned long long *>(cnt);
+    TRC_LAUNCH(prof, stream, "upd_merge_prep", pgrid, 256, 0, k_merge_prep, G, ma, nrs_dev, rec,
+               lgroup, lwarp, ucnt);
+    TRC_LAUNCH(prof, stream, "upd_merge_group", (unsigned)num_sms() * 4, 256, 0, k_merge_group, G,
+               ma, lgroup, ucnt, (const ulonglong2 *)rec);
+    TRC_LAUNCH(prof, stream, "upd_merge_small", pgrid, 256, 0, k_merge_small, G, ma, lwarp, ucnt,
+               (const ulonglong2 *)rec, ucnt + C_MWORK);
   }
   phase("merge_small");
   // ---- tier 3, second phase (the hubs touch vertices disjoint from the
