@@ -243,9 +243,8 @@ struct BFSState {
   uint32_t *next;        // next-frontier queue
   uint32_t *next_cnt;
   uint32_t d;            // current level
-  // dense steps: vertices left unvisited by the inline pass that have a
-  // PMA segment (seg), and vertices left unvisited by the step (cand, the
-  // next dense step's candidates); push steps: the frontier's hubs (seg)
+  // push steps: the frontier's hubs (seg); dense steps: the vertices left
+  // unvisited (cand, the next dense step's candidates of the same class)
   uint32_t *seg, *seg_cnt;
   uint32_t *cand, *cand_cnt;
 };
@@ -348,7 +347,8 @@ __global__ void k_level_bits(const uint32_t *lv, uint32_t n, uint32_t d, uint32_
 // is used: list entries, then degree and level, then the row quarters, then
 // the 4 * BP_V frontier-bitmap words.  The first frontier neighbour in
 // sorted order wins (lowest lane of the quad with a hit, then its lowest
-// element).
+// element).  The list holds vertices of at most 16 neighbours; those left
+// unvisited become the next dense step's candidates.
 constexpr uint32_t BP_V = 4;
 
 __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S, uint64_t nS,
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
     ww[i] = act[i] && e + 3 < d[i] ? __ldg(s.bits + (v[i].w >> 5)) : 0u;
   }
   uint32_t wins = 0;  // bit i: this lane claimed vertex i
-  uint32_t tosg = 0, tocand = 0;  // bit i (lane q == 0): vertex i stays unvisited
+  uint32_t tocand = 0;  // bit i (lane q == 0): vertex i stays unvisited
 #pragma unroll
   for (uint32_t i = 0; i < BP_V; i++) {
     const bool uv = d[i] > 0 && s.lv[u[i]] == TRC_UNREACHED;  // cached: loaded above
@@ -401,20 +401,13 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
       s.lv[u[i]] = s.d + 1;
       wins |= 1u << i;
     }
-    if (q == 0 && uv && grp == 0) {
-      if (d[i] > K_INLINE) tosg |= 1u << i;
-      else tocand |= 1u << i;
-    }
+    if (q == 0 && uv && grp == 0) tocand |= 1u << i;
   }
   __shared__ uint32_t sh[AT / 32 + 2];
   uint32_t pos = block_append(__popc(wins), s.next_cnt, sh);
 #pragma unroll
   for (uint32_t i = 0; i < BP_V; i++)
     if ((wins >> i) & 1u) s.next[pos++] = u[i];
-  pos = block_append(__popc(tosg), s.seg_cnt, sh);
-#pragma unroll
-  for (uint32_t i = 0; i < BP_V; i++)
-    if ((tosg >> i) & 1u) s.seg[pos++] = u[i];
   pos = block_append(__popc(tocand), s.cand_cnt, sh);
 #pragma unroll
   for (uint32_t i = 0; i < BP_V; i++)
@@ -523,44 +516,50 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
   uint64_t words = ceil_div(n, 32);
   uint32_t *bm = bits.alloc_exact(words);
   uint32_t *c = cnt.alloc_exact(4);
+  DBuf<uint32_t> hb;
+  hb.bind(&budget);
+  uint32_t *hubl = hb.alloc_exact(H ? H : 1);  // the frontier's hubs of a push step
   TRC_LAUNCH(prof, stream, "bfs_init", ceil_div(n, AT), AT, 0, k_bfs_init, lv, par, n, src, F);
   DevView G = view();
   uint32_t nf = 1, d = 0;
   const uint64_t dense_at = n / push_pull_divisor();
-  // candidates of the dense steps: non-hub vertices not yet visited,
-  // compacted after every dense step
-  DBuf<uint32_t> cbuf[2], segb;  // candidate ping-pong, segment-pass list
-  cbuf[0].bind(&budget);
-  cbuf[1].bind(&budget);
-  segb.bind(&budget);
-  const uint32_t *cand = lists.SM.get();
-  uint64_t ncand = lists.nSM;
+  // candidates of the dense steps, compacted after every dense step: the
+  // unvisited vertices of at most 16 neighbours (their whole list is the
+  // inline row: one pass of four lanes per vertex) and the unvisited non-hub
+  // vertices of more (a warp per vertex, scanning from the largest
+  // neighbour down: on RMAT graphs of the reference's generator the
+  // highest-degree vertices have the largest ids, so a frontier neighbour
+  // is found in the first step, and the inline row -- the smallest
+  // neighbours -- is read only when the rest has none)
+  DBuf<uint32_t> cbS[2], cbM[2];
+  for (auto *b : {&cbS[0], &cbS[1], &cbM[0], &cbM[1]}) b->bind(&budget);
+  const uint32_t *candS = lists.S.get(), *candM = lists.M.get();
+  uint64_t ncS = lists.nS, ncM = lists.nM;
   int cnext = 0;
-  uint32_t *sg = segb.ensure(n);
   const unsigned pgrid = (unsigned)num_sms() * 8;
   while (nf > 0) {
-    TRC_CUDA(cudaMemsetAsync(c, 0, 16, stream));  // next, seg, cand counts
-    BFSState s{lv, par, bm, Nx, c, d, sg, c + 1, nullptr, c + 2};
-    uint32_t hc[3] = {0, 0, 0};
+    TRC_CUDA(cudaMemsetAsync(c, 0, 16, stream));  // next, hubs, S cand, M cand counts
+    BFSState s{lv, par, bm, Nx, c, d, hubl, c + 1, nullptr, c + 2};
+    uint32_t hc[4] = {0, 0, 0, 0};
     if ((uint64_t)nf >= dense_at && dense_at > 0) {
       TRC_LAUNCH(prof, stream, "bfs_bits", ceil_div(n, AT), AT, 0, k_level_bits, lv, n, d, bm);
-      // candidates left for the next dense step (never the list being read)
-      s.cand = cbuf[cnext].ensure(ncand ? ncand : 1);
-      // pass A: the 16 inline neighbours of every unvisited non-hub vertex;
-      // those left unvisited go to the segment list (PMA vertices) or the
-      // next candidates
-      TRC_LAUNCH(prof, stream, "bfs_pull_inline", ceil_div(ncand * 4, (uint64_t)AT * BP_V), AT, 0,
-                 k_bfs_pull_S, G, cand, ncand, s);
-      // pass B: the PMA segments of the segment list (count on the device);
-      // hubs from rank 0
-      TRC_LAUNCH(prof, stream, "bfs_pull_M", pgrid, AT, 0, k_bfs_pull_W, G, sg, 0, c + 1, s,
-                 K_INLINE, 1);
+      // candidates left for the next dense step (never the lists being read)
+      s.cand = cbS[cnext].ensure(ncS ? ncS : 1);
+      BFSState sm = s;
+      sm.cand = cbM[cnext].ensure(ncM ? ncM : 1);
+      sm.cand_cnt = c + 3;
+      TRC_LAUNCH(prof, stream, "bfs_pull_inline", ceil_div(ncS * 4, (uint64_t)AT * BP_V), AT, 0,
+                 k_bfs_pull_S, G, candS, ncS, s);
+      TRC_LAUNCH(prof, stream, "bfs_pull_M", std::min<uint64_t>(pgrid, ceil_div(ncM * 32, AT)), AT,
+                 0, k_bfs_pull_W, G, candM, ncM, (const uint32_t *)nullptr, sm, 0u, 1);
       TRC_LAUNCH(prof, stream, "bfs_pull_H", ceil_div(lists.nH * 32, AT), AT, 0, k_bfs_pull_W, G,
                  lists.Hv.get(), lists.nH, (const uint32_t *)nullptr, s, 0u, 0);
-      TRC_CUDA(cudaMemcpyAsync(hc, c, 12, cudaMemcpyDeviceToHost, stream));
+      TRC_CUDA(cudaMemcpyAsync(hc, c, 16, cudaMemcpyDeviceToHost, stream));
       sync();
-      ncand = hc[2];
-      cand = s.cand;
+      ncS = hc[2];
+      ncM = hc[3];
+      candS = s.cand;
+      candM = sm.cand;
       cnext ^= 1;
     } else {
       TRC_LAUNCH(prof, stream, "bfs_push", ceil_div((uint64_t)nf * 32, AT), AT, 0, k_bfs_push, G, F,
