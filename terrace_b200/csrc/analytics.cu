@@ -15,6 +15,7 @@
 //   H  (hubs, blocked tier): one CTA per hub, warps over its blocks.
 // Direction switching follows the reference rule: dense (pull) when the
 // frontier holds at least n/divisor vertices (include/Map.cpp:65-74).
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -226,7 +227,7 @@ __global__ void __launch_bounds__(AT) k_flat(DevView G, const uint32_t *V, uint6
     flat_seg_add(g2, v2, acc);
     __syncwarp();
   }
-  op.store(f.valid && f.d > 0, f.u, f.d, acc[lane]);
+  op.store(f.valid, f.u, f.d, acc[lane]);  // (d == 0: nothing gathered, sum 0)
 }
 
 // ---------------------------------------------------------------------------
@@ -415,8 +416,8 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
 }
 
 // One warp scans the neighbours of vertex u of rank >= j_first for a
-// frontier member, 64 per step from the largest id down (two independent
-// loads per lane), and returns the smallest frontier neighbour of the first
+// frontier member from the largest id down, 32 in the first step, then 64
+// per step (two independent loads per lane), and returns the smallest frontier neighbour of the first
 // step that has one, or NONE32 (warp-uniform).  Any frontier neighbour is a
 // valid parent (the levels do not depend on the choice); scanning from the
 // top finds one sooner on graphs whose high-degree vertices have large ids
@@ -425,9 +426,11 @@ __device__ __forceinline__ uint32_t warp_any_in_frontier(const NbrList &L, const
                                                          uint32_t j_first) {
   const uint32_t lane = threadIdx.x & 31;
   for (uint32_t e = L.deg; e > j_first;) {
-    const uint32_t s0 = e - j_first > 64 ? e - 64 : j_first;
+    // the first step reads only the 32 largest: most vertices stop there
+    const uint32_t width = e == L.deg ? 32u : 64u;
+    const uint32_t s0 = e - j_first > width ? e - width : j_first;
     const uint32_t ja = s0 + lane, jb = s0 + 32 + lane;
-    const bool va = ja < e, vb = jb < e;
+    const bool va = ja < e, vb = width == 64u && jb < e;
     const uint32_t xa = va ? L.at(ja) : 0u, xb = vb ? L.at(jb) : 0u;
     const bool ha = va && bit_test(bits, xa), hb = vb && bit_test(bits, xb);
     const uint32_t ma = __ballot_sync(0xFFFFFFFFu, ha), mb = __ballot_sync(0xFFFFFFFFu, hb);
@@ -585,9 +588,15 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
 // CC.  The reference propagates labels with writeMin until no label changes
 // (include/Components.h:92-120); on a symmetric graph that fixed point is the
 // smallest vertex id of each component.  The same fixed point is reached here
-// in one pass over the edges with lock-free union-find (a root is always
-// hooked under a smaller root, so the final root of a component is its
-// smallest id), then a pointer-jumping pass.
+// with lock-free union-find (a root is always hooked under a smaller root, so
+// the final root of a component is its smallest id) in the order of the
+// published Afforest algorithm (Sutton, Ben-Nun, Barak, IPDPS 2018): link
+// every vertex to its first two neighbours, compress, take the most frequent
+// root of 1024 sampled vertices as the giant component, then link every
+// edge of every vertex outside it; vertices inside it are skipped (an edge
+// with an endpoint outside is linked from that endpoint, and an edge inside
+// joins vertices already joined).  On power-law graphs the giant component
+// holds almost every edge, so most of the adjacency is never read.
 
 __device__ __forceinline__ uint32_t uf_find(uint32_t *p, uint32_t x) {
   uint32_t px = p[x];
@@ -614,34 +623,55 @@ __device__ __forceinline__ void uf_unite(uint32_t *p, uint32_t a, uint32_t b) {
   }
 }
 
+constexpr uint32_t CC_SAMPLE_NB = 2;   // neighbours linked before the sample
+constexpr uint32_t CC_SAMPLES = 1024;  // vertices sampled for the giant component
+
+// thread per vertex: link to its r-th neighbour (inline: r < 16)
+__global__ void k_cc_link(DevView G, uint32_t *p, uint32_t r) {
+  const uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= G.n || G.deg[u] <= r) return;
+  uf_unite(p, (uint32_t)u, G.inl[u * K_INLINE + r]);
+}
+
+// roots of pseudo-random vertices (hash of the sample index)
+__global__ void k_cc_sample(const uint32_t *p, uint32_t n, uint32_t *out) {
+  const uint32_t i = threadIdx.x + blockIdx.x * blockDim.x;
+  if (i >= CC_SAMPLES) return;
+  uint32_t h = i * 0x9E3779B1u;
+  h ^= h >> 15;
+  h *= 0x2C1B3C6Du;
+  h ^= h >> 12;
+  out[i] = p[h % n];
+}
+
+// the rest of the edges (rank >= CC_SAMPLE_NB) of vertices outside the giant
+// component c: four lanes per vertex of at most 16 neighbours
 __global__ void __launch_bounds__(AT) k_cc_S(DevView G, const uint32_t *S, uint64_t nS,
-                                             uint32_t *p) {
+                                             uint32_t *p, uint32_t c) {
   uint64_t gt = (uint64_t)blockIdx.x * AT + threadIdx.x;
   uint64_t vi = gt >> 2;
   uint32_t q = gt & 3;
   if (vi >= nS) return;
   uint32_t u = S[vi];
   uint32_t d = G.deg[u];
-  if (q * 4 >= d) return;
+  if (q * 4 >= d || d <= CC_SAMPLE_NB || uf_find(p, u) == c) return;
   uint4 v = reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE)[q];
   uint32_t e[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
   for (int i = 0; i < 4; i++)
-    if (q * 4 + i < d && e[i] < u) uf_unite(p, u, e[i]);
+    if (q * 4 + i < d && q * 4 + i >= CC_SAMPLE_NB) uf_unite(p, u, e[i]);
 }
 
+// ... and a warp per vertex of more
 __global__ void __launch_bounds__(AT) k_cc_W(DevView G, const uint32_t *Lst, uint64_t nL,
-                                             uint32_t *p) {
+                                             uint32_t *p, uint32_t c) {
   uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
   uint32_t lane = threadIdx.x & 31;
   if (w >= nL) return;
   uint32_t u = Lst[w];
+  if (uf_find(p, u) == c) return;  // warp-uniform
   NbrList L = nbr_list(G, u);
-  for (uint32_t j = lane; j < L.deg; j += 32) {
-    uint32_t v = L.at(j);
-    if (v >= u) break;  // sorted: the rest are larger
-    uf_unite(p, u, v);
-  }
+  for (uint32_t j = CC_SAMPLE_NB + lane; j < L.deg; j += 32) uf_unite(p, u, L.at(j));
 }
 
 __global__ void k_cc_init(uint32_t *p, uint32_t n) {
@@ -661,17 +691,41 @@ void Graph::cc(uint32_t *labels, uint32_t flags) {
   if (!labels) throw_error(TRC_ERR_INVALID, "null output");
   ensure_lists();
   bool dev = flags & TRC_DEVICE_PTR;
-  DBuf<uint32_t> lb;
+  DBuf<uint32_t> lb, sb;
   lb.bind(&budget);
+  sb.bind(&budget);
   uint32_t *p = dev ? labels : lb.alloc_exact(n);
+  uint32_t *smp = sb.alloc_exact(CC_SAMPLES);
   DevView G = view();
   TRC_LAUNCH(prof, stream, "cc_init", ceil_div(n, AT), AT, 0, k_cc_init, p, n);
+  for (uint32_t r = 0; r < CC_SAMPLE_NB; r++)
+    TRC_LAUNCH(prof, stream, "cc_link", ceil_div(n, AT), AT, 0, k_cc_link, G, p, r);
+  TRC_LAUNCH(prof, stream, "cc_compress", ceil_div(n, AT), AT, 0, k_cc_final, p, n);
+  // the giant component: the most frequent root among the samples
+  uint32_t c = NONE32;
+  if (n) {
+    std::vector<uint32_t> h(CC_SAMPLES);
+    TRC_LAUNCH(prof, stream, "cc_sample", ceil_div(CC_SAMPLES, AT), AT, 0, k_cc_sample, p, n, smp);
+    TRC_CUDA(cudaMemcpyAsync(h.data(), smp, CC_SAMPLES * 4, cudaMemcpyDeviceToHost, stream));
+    sync();
+    std::sort(h.begin(), h.end());
+    uint32_t best = 0;
+    for (size_t i = 0; i < h.size();) {
+      size_t j = i;
+      while (j < h.size() && h[j] == h[i]) j++;
+      if (j - i > best) {
+        best = (uint32_t)(j - i);
+        c = h[i];
+      }
+      i = j;
+    }
+  }
   TRC_LAUNCH(prof, stream, "cc_S", ceil_div(lists.nS * 4, AT), AT, 0, k_cc_S, G, lists.S.get(),
-             lists.nS, p);
+             lists.nS, p, c);
   TRC_LAUNCH(prof, stream, "cc_M", ceil_div(lists.nM * 32, AT), AT, 0, k_cc_W, G, lists.M.get(),
-             lists.nM, p);
+             lists.nM, p, c);
   TRC_LAUNCH(prof, stream, "cc_H", ceil_div(lists.nH * 32, AT), AT, 0, k_cc_W, G, lists.Hv.get(),
-             lists.nH, p);
+             lists.nH, p, c);
   TRC_LAUNCH(prof, stream, "cc_final", ceil_div(n, AT), AT, 0, k_cc_final, p, n);
   if (!dev) TRC_CUDA(cudaMemcpyAsync(labels, p, (uint64_t)n * 4, cudaMemcpyDeviceToHost, stream));
   sync();
@@ -684,6 +738,7 @@ void Graph::cc(uint32_t *labels, uint32_t flags) {
 struct BCFwd {
   uint32_t *lv;
   double *sigma;
+  double *sigma_out;    // pull steps write here (committed after the step)
   uint32_t *order;      // order[base ..] receives the next level
   uint32_t *next_cnt;
   uint32_t d;
@@ -762,13 +817,10 @@ __global__ void __launch_bounds__(AT) k_bc_pull_W(DevView G, const uint32_t *Lst
   if (s.lv[u] == TRC_UNREACHED) {
     NbrList L = nbr_list(G, u);
     double sum = 0.0;
-    for (uint32_t j = lane; j < L.deg; j += 32) {
-      uint32_t v = L.at(j);
-      if (s.lv[v] == s.d) sum += s.sigma[v];
-    }
+    for (uint32_t j = lane; j < L.deg; j += 32) sum += __ldg(s.sigma + L.at(j));
     sum = warp_sum(sum);
     if (sum > 0.0 && lane == 0) {
-      s.sigma[u] = sum;
+      s.sigma_out[u] = sum;
       s.lv[u] = s.d + 1;
       win = true;
     }
@@ -810,16 +862,19 @@ __global__ void __launch_bounds__(AT) k_bc_pull_S(DevView G, const uint32_t *S, 
 
 // Dense forward step with the load-balanced pull: an unvisited vertex sums
 // sigma over its neighbours on level d; a positive sum puts it on level d+1.
+// Dense forward step (pull) for the unvisited vertices: sigma = sum of sigma
+// over the neighbours on level d.  An unvisited vertex has no neighbour above
+// level d (it would have been reached), and every neighbour not on level d
+// is unvisited with sigma 0 (the step writes its results to sigma_out,
+// committed after it), so the gather needs no level test.
 struct BCPullOp {
   BCFwd s;
   __device__ bool skip(uint32_t u) const { return s.lv[u] != TRC_UNREACHED; }
-  __device__ double gather(uint32_t x) const {
-    return __ldg(s.lv + x) == s.d ? __ldg(s.sigma + x) : 0.0;
-  }
+  __device__ double gather(uint32_t x) const { return __ldg(s.sigma + x); }
   __device__ void store(bool ok, uint32_t u, uint32_t, double sum) const {
-    bool win = ok && sum > 0.0;
+    bool win = ok && sum > 0.0;  // (a vertex with no neighbour on level d sums 0)
     if (win) {
-      s.sigma[u] = sum;
+      s.sigma_out[u] = sum;
       s.lv[u] = s.d + 1;
     }
     __shared__ uint32_t sh[AT / 32 + 2];
@@ -830,17 +885,31 @@ struct BCPullOp {
 
 // Backward step with the load-balanced pull over the vertices of level d:
 // dep[v] = sum of dep[w] over neighbours on level d+1, plus 1/sigma[v].
+// Neighbours of a level-d vertex are on levels d-1..d+1; dep holds only the
+// finished levels above d (levels d-1 and d are still 0: this step writes
+// to dep_out, committed after it), so the gather needs no level test.
 struct BCBackOp {
-  const uint32_t *lv;
   const double *inv;
-  double *dep;
-  uint32_t d;
+  const double *dep;
+  double *dep_out;
   __device__ bool skip(uint32_t) const { return false; }
-  __device__ double gather(uint32_t x) const { return __ldg(lv + x) == d + 1 ? dep[x] : 0.0; }
+  __device__ double gather(uint32_t x) const { return __ldg(dep + x); }
   __device__ void store(bool ok, uint32_t u, uint32_t, double sum) const {
-    if (ok) dep[u] = sum + inv[u];
+    if (ok) dep_out[u] = sum + inv[u];  // every vertex of the level, isolated source included
   }
 };
+
+// After a step that wrote to a side array: copy the values of the level's
+// vertices (order[0 .. *cnt or cnt)) into the main array.
+__global__ void k_bc_commit(const uint32_t *order, const uint32_t *cnt_dev, uint64_t cnt,
+                            const double *from, double *to) {
+  const uint64_t nv = cnt_dev ? *cnt_dev : cnt;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = order[i];
+    to[v] = from[v];
+  }
+}
 
 // Backward, one warp per vertex of level d:
 // dep[v] = sum of dep[w] over neighbours on level d+1, plus 1/sigma[v].
@@ -886,9 +955,10 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
   ensure_lists();
   bool dev = flags & TRC_DEVICE_PTR;
   DBuf<uint32_t> lvb, ordb, cntb;
-  DBuf<double> sig, invb, depb, outb;
+  DBuf<double> sig, invb, depb, outb, sideb;
   for (auto *b : {&lvb, &ordb, &cntb}) b->bind(&budget);
-  for (auto *b : {&sig, &invb, &depb, &outb}) b->bind(&budget);
+  for (auto *b : {&sig, &invb, &depb, &outb, &sideb}) b->bind(&budget);
+  double *side = sideb.alloc_exact(n);  // a dense step's results before their commit
   uint32_t *lv = lvb.alloc_exact(n), *order = ordb.alloc_exact(n), *c = cntb.alloc_exact(4);
   DBuf<uint32_t> hubb;
   hubb.bind(&budget);
@@ -906,12 +976,14 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
     uint32_t nf = (uint32_t)(f1 - f0);
     if (nf == 0) break;
     TRC_CUDA(cudaMemsetAsync(c, 0, 8, stream));
-    BCFwd s{lv, sigma, order + f1, c, d, hubl, c + 1};
+    BCFwd s{lv, sigma, side, order + f1, c, d, hubl, c + 1};
     if ((uint64_t)nf >= dense_at && dense_at > 0) {
       TRC_LAUNCH(prof, stream, "bc_pull_flat", ceil_div(lists.nSM, AT), AT, 0, k_flat<BCPullOp>,
                  G, lists.SM.get(), lists.nSM, BCPullOp{s});
       TRC_LAUNCH(prof, stream, "bc_pull_H", ceil_div(lists.nH * 32, AT), AT, 0, k_bc_pull_W, G,
                  lists.Hv.get(), lists.nH, s);
+      TRC_LAUNCH(prof, stream, "bc_commit", (unsigned)num_sms() * 4, AT, 0, k_bc_commit, order + f1,
+                 c, 0, side, sigma);
     } else {
       TRC_LAUNCH(prof, stream, "bc_push", ceil_div((uint64_t)nf * 32, AT), AT, 0, k_bc_push, G,
                  order + f0, nf, s);
@@ -930,7 +1002,9 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
   for (int64_t L = (int64_t)d - 1; L >= 0; L--) {
     uint64_t a = loff[L], b = loff[L + 1];
     TRC_LAUNCH(prof, stream, "bc_back_flat", ceil_div(b - a, AT), AT, 0, k_flat<BCBackOp>, G,
-               order + a, b - a, BCBackOp{lv, inv, dep, (uint32_t)L});
+               order + a, b - a, BCBackOp{inv, dep, side});
+    TRC_LAUNCH(prof, stream, "bc_commit", std::min<uint64_t>(ceil_div(b - a, AT), num_sms() * 4), AT,
+               0, k_bc_commit, order + a, (const uint32_t *)nullptr, b - a, side, dep);
   }
   TRC_LAUNCH(prof, stream, "bc_final", ceil_div(n, AT), AT, 0, k_bc_final, dep, inv, out, n);
   if (!dev) TRC_CUDA(cudaMemcpyAsync(out_user, out, (uint64_t)n * 8, cudaMemcpyDeviceToHost, stream));

@@ -42,10 +42,6 @@ struct PRSnap {
   DBuf<uint32_t> perm, inv, dsort, adj;
   DBuf<uint64_t> off;
 };
-constexpr uint32_t PR_HOT_MAX = 16384;  // rank entries a pull CTA may stage in shared memory
-
-// Raises the pull kernels' dynamic shared memory limit on the current device.
-void pagerank_kernel_attributes();
 
 // Tier-3 work of one batch between its two launch phases (hubs.cu).
 struct HubItem {
@@ -215,7 +211,6 @@ class Graph {
     uint32_t pr_group_cut = 64;       // PageRank: degree 17..cut use a lane group
     uint32_t pr_group_lanes = 8;      // ... of this many lanes (4, 8 or 16); above: a warp
     uint32_t pma_leaf_log = 1;        // smallest PMA window: 2^x vertex segments
-    uint32_t pr_hot = 8192;           // PageRank: rank entries staged per CTA (<= PR_HOT_MAX)
   } tuned;
   void autotune(uint32_t what, const uint32_t *src, const uint32_t *dst, uint64_t k,
                 uint32_t flags, double *ms_out);

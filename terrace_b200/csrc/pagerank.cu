@@ -11,14 +11,13 @@
 // graph, rebuilt when the graph changes: the non-isolated vertices relabelled
 // by degree, highest first, and their lists (neighbour ids relabelled, in the
 // original sorted order) as one CSR.  The most gathered values are then the
-// first entries of the rank vector: each CTA stages the first `hot` of them
-// in shared memory, and the next ones share sectors, stay in L1 and L2.  The
-// lists are read once per iteration with streaming loads, contiguous for
-// every vertex, so vertices of every degree class read with all lanes busy:
-// one CTA per vertex above 4096 neighbours, a warp above the lane-group cut,
-// a lane group (4, 8 or 16) above 16, four lanes below.  Classes are
-// contiguous ranges of the relabelled ids.  Results are scattered back to
-// the original ids on the last iteration.
+// first entries of the rank vector, packed into few sectors that stay in L1
+// and L2.  The lists are read once per iteration with streaming loads,
+// contiguous for every vertex with no tier dispatch, by a lane group sized
+// to the degree class: a CTA per vertex above 4096 neighbours, a warp above
+// the lane-group cut, a lane group (4, 8 or 16) above 16, four lanes below.
+// Classes are contiguous ranges of the relabelled ids.  Results are
+// scattered back to the original ids on the last iteration.
 #include <algorithm>
 #include <cstring>
 
@@ -26,7 +25,7 @@
 
 namespace trc {
 
-constexpr int PRT = 512;               // threads per CTA of the pull kernels
+constexpr int PRT = 256;                 // threads per CTA of the pull kernels
 constexpr uint32_t PR_BLOCK_DEG = 4096;  // above: a CTA per vertex
 
 struct PRSArgs {
@@ -38,7 +37,6 @@ struct PRSArgs {
   double *out;           // final ranks (original order), last iteration
   double damping, base;
   int last;
-  uint32_t nhot;         // entries of pc staged in shared memory
 };
 
 __device__ __forceinline__ void prs_store(const PRSArgs &a, uint64_t r, uint32_t d, double sum) {
@@ -47,66 +45,48 @@ __device__ __forceinline__ void prs_store(const PRSArgs &a, uint64_t r, uint32_t
   if (a.last) a.out[a.perm[r]] = val;
 }
 
-__device__ __forceinline__ void prs_stage_hot(const PRSArgs &a, double *hot) {
-  for (uint32_t i = threadIdx.x; i < a.nhot; i += blockDim.x) hot[i] = a.pc[i];
-  __syncthreads();
-}
-
-__device__ __forceinline__ double prs_gather(const PRSArgs &a, const double *hot, uint32_t x) {
-  return x < a.nhot ? hot[x] : __ldg(a.pc + x);
-}
-
-// GS lanes per vertex over relabelled ids [r0, r1), persistent (grid-stride
-// over vertices); each lane issues U independent list loads, then U gathers.
+// GS lanes per vertex over relabelled ids [r0, r1), one group per vertex;
+// each lane issues U independent list loads, then U gathers.
 template <int GS>
 __global__ void __launch_bounds__(PRT) k_prs_group(PRSArgs a, uint64_t r0, uint64_t r1) {
-  extern __shared__ double hot[];
-  prs_stage_hot(a, hot);
   constexpr int U = 8;
   const uint32_t lg = threadIdx.x & (GS - 1);
   const uint32_t lane = threadIdx.x & 31;
   const unsigned mask = GS == 32 ? 0xFFFFFFFFu : (((1u << GS) - 1u) << (lane & ~(uint32_t)(GS - 1)));
-  const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / GS;
-  for (uint64_t r = r0 + ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / GS; r < r1;
-       r += ngroups) {
-    const uint64_t e0 = a.off[r], e1 = a.off[r + 1];
-    double sum = 0.0;
-    for (uint64_t e = e0 + lg; e < e1; e += (uint64_t)GS * U) {
-      uint32_t x[U];
+  const uint64_t r = r0 + ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / GS;
+  if (r >= r1) return;  // whole groups leave together
+  const uint64_t e0 = a.off[r], e1 = a.off[r + 1];
+  double sum = 0.0;
+  for (uint64_t e = e0 + lg; e < e1; e += (uint64_t)GS * U) {
+    uint32_t x[U];
 #pragma unroll
-      for (int k = 0; k < U; k++) {
-        const uint64_t ee = e + (uint64_t)k * GS;
-        x[k] = ee < e1 ? __ldcs(a.adj + ee) : NONE32;
-      }
-#pragma unroll
-      for (int k = 0; k < U; k++)
-        if (x[k] != NONE32) sum += prs_gather(a, hot, x[k]);
+    for (int k = 0; k < U; k++) {
+      const uint64_t ee = e + (uint64_t)k * GS;
+      x[k] = ee < e1 ? __ldcs(a.adj + ee) : NONE32;
     }
 #pragma unroll
-    for (int o = GS / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(mask, sum, o);
-    if (lg == 0) prs_store(a, r, (uint32_t)(e1 - e0), sum);
+    for (int k = 0; k < U; k++)
+      if (x[k] != NONE32) sum += __ldg(a.pc + x[k]);
   }
+#pragma unroll
+  for (int o = GS / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(mask, sum, o);
+  if (lg == 0) prs_store(a, r, (uint32_t)(e1 - e0), sum);
 }
 
 // A CTA per vertex over [r0, r1) (the largest degrees).
-__global__ void __launch_bounds__(PRT) k_prs_block(PRSArgs a, uint64_t r0, uint64_t r1) {
-  extern __shared__ double hot[];
+__global__ void __launch_bounds__(PRT) k_prs_block(PRSArgs a, uint64_t r0) {
   __shared__ double ws[PRT / 32];
-  prs_stage_hot(a, hot);
-  for (uint64_t r = r0 + blockIdx.x; r < r1; r += gridDim.x) {
-    const uint64_t e0 = a.off[r], e1 = a.off[r + 1];
-    double sum = 0.0;
-    for (uint64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x)
-      sum += prs_gather(a, hot, __ldcs(a.adj + e));
-    sum = warp_sum(sum);
-    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = sum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int w = 0; w < PRT / 32; w++) t += ws[w];
-      prs_store(a, r, (uint32_t)(e1 - e0), t);
-    }
-    __syncthreads();
+  const uint64_t r = r0 + blockIdx.x;
+  const uint64_t e0 = a.off[r], e1 = a.off[r + 1];
+  double sum = 0.0;
+  for (uint64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) sum += __ldg(a.pc + __ldcs(a.adj + e));
+  sum = warp_sum(sum);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < PRT / 32; w++) t += ws[w];
+    prs_store(a, r, (uint32_t)(e1 - e0), t);
   }
 }
 
@@ -220,18 +200,6 @@ void Graph::ensure_pr_snapshot() {
   }
 }
 
-// Dynamic shared memory of the pull kernels (the staged rank entries) may
-// exceed the 48 KB default: the limit is raised per device when a graph is
-// created there (cudaFuncSetAttribute applies to the current device).
-void pagerank_kernel_attributes() {
-  const int bytes = (int)(PR_HOT_MAX * sizeof(double));
-  TRC_CUDA(cudaFuncSetAttribute(k_prs_group<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  TRC_CUDA(cudaFuncSetAttribute(k_prs_group<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  TRC_CUDA(cudaFuncSetAttribute(k_prs_group<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  TRC_CUDA(cudaFuncSetAttribute(k_prs_group<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  TRC_CUDA(cudaFuncSetAttribute(k_prs_block, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-}
-
 // ---------------------------------------------------------------- iterations
 
 void Graph::pagerank(uint32_t iters, double damping, double *ranks, uint32_t flags) {
@@ -267,28 +235,32 @@ void Graph::pr_kernels(uint32_t iters, double damping, double *p0, double *p1, d
   if (S.na == 0) return;
   TRC_LAUNCH(prof, s, "pr_init", ceil_div(S.na, 256), 256, 0, k_prs_init, S.off.get(), S.na,
              one_over_n, p0);
-  const uint32_t nhot = (uint32_t)std::min<uint64_t>(tuned.pr_hot, S.na);
-  const size_t smem = (size_t)nhot * sizeof(double);
-  const unsigned per_sm = smem > 96 * 1024 ? 1u : smem > 48 * 1024 ? 2u : smem ? 3u : 4u;
-  const unsigned grid = (unsigned)num_sms() * per_sm;
   for (uint32_t it = 0; it < iters; it++) {
     PRSArgs a{S.off.get(), S.adj.get(), S.perm.get(), p0, p1, out, damping, base,
-              it + 1 == iters ? 1 : 0, nhot};
-    if (S.rb) TRC_LAUNCH(prof, s, "pr_block", grid, PRT, smem, k_prs_block, a, 0, S.rb);
-    if (S.rw > S.rb) TRC_LAUNCH(prof, s, "pr_warp", grid, PRT, smem, k_prs_group<32>, a, S.rb, S.rw);
+              it + 1 == iters ? 1 : 0};
+    if (S.rb) TRC_LAUNCH(prof, s, "pr_block", S.rb, PRT, 0, k_prs_block, a, 0);
+    if (S.rw > S.rb)
+      TRC_LAUNCH(prof, s, "pr_warp", ceil_div((S.rw - S.rb) * 32, PRT), PRT, 0, k_prs_group<32>, a,
+                 S.rb, S.rw);
     if (S.rg > S.rw) {
+      const uint64_t nv = S.rg - S.rw;
       switch (tuned.pr_group_lanes) {
         case 4:
-          TRC_LAUNCH(prof, s, "pr_group4", grid, PRT, smem, k_prs_group<4>, a, S.rw, S.rg);
+          TRC_LAUNCH(prof, s, "pr_group4", ceil_div(nv * 4, PRT), PRT, 0, k_prs_group<4>, a, S.rw,
+                     S.rg);
           break;
         case 16:
-          TRC_LAUNCH(prof, s, "pr_group16", grid, PRT, smem, k_prs_group<16>, a, S.rw, S.rg);
+          TRC_LAUNCH(prof, s, "pr_group16", ceil_div(nv * 16, PRT), PRT, 0, k_prs_group<16>, a,
+                     S.rw, S.rg);
           break;
         default:
-          TRC_LAUNCH(prof, s, "pr_group8", grid, PRT, smem, k_prs_group<8>, a, S.rw, S.rg);
+          TRC_LAUNCH(prof, s, "pr_group8", ceil_div(nv * 8, PRT), PRT, 0, k_prs_group<8>, a, S.rw,
+                     S.rg);
       }
     }
-    if (S.na > S.rg) TRC_LAUNCH(prof, s, "pr_small", grid, PRT, smem, k_prs_group<4>, a, S.rg, S.na);
+    if (S.na > S.rg)
+      TRC_LAUNCH(prof, s, "pr_small", ceil_div((S.na - S.rg) * 4, PRT), PRT, 0, k_prs_group<4>, a,
+                 S.rg, S.na);
     std::swap(p0, p1);
   }
 }
@@ -311,7 +283,7 @@ void Graph::pagerank_launch(uint32_t iters, double damping, double *p0, double *
   const uint64_t key[PRGraphCache::KEY] = {iters, dbits, (uint64_t)p0, (uint64_t)p1, (uint64_t)out,
                                            prs.version, (uint64_t)prs.adj.get(), prs.na, prs.rb,
                                            prs.rw ^ (prs.rg << 32), (uint64_t)s,
-                                           tuned.pr_group_lanes, tuned.pr_hot};
+                                           tuned.pr_group_lanes, 0};
   bool same = prg.exec != nullptr;
   for (int i = 0; same && i < PRGraphCache::KEY; i++) same = prg.key[i] == key[i];
   if (!same) {

@@ -106,7 +106,7 @@ void Graph::autotune(uint32_t what, const uint32_t *src, const uint32_t *dst, ui
           best_t = tuned;
         }
       };
-      // lane group and cut first, then the staged rank entries
+      // the lane group and the cut between lane groups and warps
       for (uint32_t cut : {32u, 64u, 128u}) {
         tuned.pr_group_cut = cut;
         ensure_pr_snapshot();  // class boundaries for the cut
@@ -115,18 +115,10 @@ void Graph::autotune(uint32_t what, const uint32_t *src, const uint32_t *dst, ui
           time2();
         }
       }
-      tuned.pr_group_cut = best_t.pr_group_cut;
-      tuned.pr_group_lanes = best_t.pr_group_lanes;
-      ensure_pr_snapshot();
-      for (uint32_t hot : {0u, 4096u, 16384u}) {
-        tuned.pr_hot = hot;
-        time2();
-      }
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
       tuned.pr_group_cut = best_t.pr_group_cut;
       tuned.pr_group_lanes = best_t.pr_group_lanes;
-      tuned.pr_hot = best_t.pr_hot;
       lists.version = ~0ull;
       ensure_pr_snapshot();
       ms_out[1] = best / 2.0;

@@ -45,7 +45,6 @@ namespace trc {
 Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_), cfg(cfg_) {
   budget.limit = budget_bytes;
   TRC_CUDA(cudaGetDevice(&device));
-  pagerank_kernel_attributes();
   na_scratch = noalloc_scratch_resolve();
   TRC_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
   TRC_CUDA(cudaStreamCreateWithFlags(&side_stream, cudaStreamNonBlocking));

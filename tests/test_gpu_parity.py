@@ -435,3 +435,23 @@ def test_blocked_tier_block_local_updates(T, stage):
     st, off, tgt = step(hl, True)
     assert g.check() == 0
     g.close()
+
+
+def test_bc_and_bfs_from_isolated_and_leaf_sources(T):
+    """Single-source BC (and BFS) from an isolated vertex and from a vertex of
+    degree one, against the oracle: the reference's backward step adds
+    1/sigma to every vertex of every level, the source included, so an
+    isolated source ends at 0 and every other vertex at NaN."""
+    n = 1 << 12
+    s, d = T.rmat_generate(n, 0, .5, .1, .1, 4 * n)
+    g = T.Graph(n, hub_threshold=64)
+    g.add_edge_batch(s, d, **SYM)
+    off, tgt = g.dump_csr()
+    deg = np.diff(off.astype(np.int64))
+    for src in (int(np.flatnonzero(deg == 0)[0]), int(np.flatnonzero(deg == 1)[0]),
+                int(deg.argmax())):
+        assert rel_close(g.bc(src), O.bc(off, tgt, src)), src
+        par, lv = g.bfs(src)
+        assert np.array_equal(lv, O.bfs_levels(off, tgt, src))
+        assert O.bfs_check_parents(off, tgt, src, lv, par) == 0
+    g.close()
