@@ -273,6 +273,22 @@ __device__ __forceinline__ void bfs_push_chunk(const NbrList &L, uint32_t u, uin
   if (win) s.next[pos] = v;
 }
 
+// The same for a piece of a hub's list (hub_chunk).
+__device__ __forceinline__ void bfs_push_span(const uint32_t *p, uint32_t len, uint32_t u,
+                                              const BFSState &s, uint32_t lane) {
+  bool win = false;
+  uint32_t v = 0;
+  if (lane < len) {
+    v = p[lane];
+    if (s.lv[v] == TRC_UNREACHED && atomicCAS(&s.par[v], -1, (int32_t)u) == -1) {
+      s.lv[v] = s.d + 1;
+      win = true;
+    }
+  }
+  uint32_t pos = warp_append(win, s.next_cnt);
+  if (win) s.next[pos] = v;
+}
+
 // Warp per frontier vertex; hubs are listed for k_bfs_push_hubs.
 __global__ void k_bfs_push(DevView G, const uint32_t *F, uint32_t nf, BFSState s) {
   uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
@@ -301,17 +317,25 @@ __global__ void k_bfs_push_hubs(DevView G, BFSState s) {
   const uint32_t *FH = s.seg;
   const uint64_t nh = *s.seg_cnt;
   const uint64_t nwide = nh < PUSH_WIDE ? nh : PUSH_WIDE;
+  const uint32_t *p;
+  uint32_t len;
   for (uint64_t i = 0; i < nwide; i++) {
     const uint32_t u = FH[i];
     NbrList L = nbr_list(G, u);
-    const uint64_t nch = (L.deg + 31) >> 5;
-    for (uint64_t c = gw; c < nch; c += nwarps) bfs_push_chunk(L, u, (uint32_t)(c << 5), s, lane);
+    const uint64_t nch = hub_chunks(L);
+    for (uint64_t c = gw; c < nch; c += nwarps) {
+      hub_chunk(L, (uint32_t)c, p, len);
+      if (len) bfs_push_span(p, len, u, s, lane);  // (len is warp-uniform)
+    }
   }
   for (uint64_t i = nwide + blockIdx.x; i < nh; i += gridDim.x) {
     const uint32_t u = FH[i];
     NbrList L = nbr_list(G, u);
-    const uint32_t nch = (L.deg + 31) >> 5;
-    for (uint32_t c = wib; c < nch; c += AT / 32) bfs_push_chunk(L, u, c << 5, s, lane);
+    const uint32_t nch = hub_chunks(L);
+    for (uint32_t c = wib; c < nch; c += AT / 32) {
+      hub_chunk(L, c, p, len);
+      if (len) bfs_push_span(p, len, u, s, lane);
+    }
   }
 }
 
@@ -767,6 +791,25 @@ __device__ __forceinline__ void bc_push_chunk(const NbrList &L, double su, uint3
   if (win) s.order[pos] = v;
 }
 
+// The same for a piece of a hub's list (hub_chunk).
+__device__ __forceinline__ void bc_push_span(const uint32_t *p, uint32_t len, double su,
+                                             const BCFwd &s, uint32_t lane) {
+  bool win = false;
+  uint32_t v = 0;
+  if (lane < len) {
+    v = p[lane];
+    uint32_t lvv = s.lv[v];
+    if (lvv == TRC_UNREACHED) {
+      uint32_t old = atomicCAS(&s.lv[v], TRC_UNREACHED, s.d + 1);
+      win = old == TRC_UNREACHED;
+      lvv = win ? s.d + 1 : old;
+    }
+    if (lvv == s.d + 1) atomicAdd(&s.sigma[v], su);
+  }
+  uint32_t pos = warp_append(win, s.next_cnt);
+  if (win) s.order[pos] = v;
+}
+
 // Warp per frontier vertex; hubs are listed for k_bc_push_hubs.
 __global__ void k_bc_push(DevView G, const uint32_t *F, uint32_t nf, BCFwd s) {
   uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
@@ -790,19 +833,27 @@ __global__ void k_bc_push_hubs(DevView G, BCFwd s) {
   const uint64_t nwarps = ((uint64_t)gridDim.x * AT) >> 5;
   const uint64_t nh = *s.hub_cnt;
   const uint64_t nwide = nh < PUSH_WIDE ? nh : PUSH_WIDE;
+  const uint32_t *p;
+  uint32_t len;
   for (uint64_t i = 0; i < nwide; i++) {
     const uint32_t u = s.hubs[i];
     const double su = s.sigma[u];
     NbrList L = nbr_list(G, u);
-    const uint64_t nch = (L.deg + 31) >> 5;
-    for (uint64_t c = gw; c < nch; c += nwarps) bc_push_chunk(L, su, (uint32_t)(c << 5), s, lane);
+    const uint64_t nch = hub_chunks(L);
+    for (uint64_t c = gw; c < nch; c += nwarps) {
+      hub_chunk(L, (uint32_t)c, p, len);
+      if (len) bc_push_span(p, len, su, s, lane);  // (len is warp-uniform)
+    }
   }
   for (uint64_t i = nwide + blockIdx.x; i < nh; i += gridDim.x) {
     const uint32_t u = s.hubs[i];
     const double su = s.sigma[u];
     NbrList L = nbr_list(G, u);
-    const uint32_t nch = (L.deg + 31) >> 5;
-    for (uint32_t c = wib; c < nch; c += AT / 32) bc_push_chunk(L, su, c << 5, s, lane);
+    const uint32_t nch = hub_chunks(L);
+    for (uint32_t c = wib; c < nch; c += AT / 32) {
+      hub_chunk(L, c, p, len);
+      if (len) bc_push_span(p, len, su, s, lane);
+    }
   }
 }
 

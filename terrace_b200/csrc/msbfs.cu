@@ -155,14 +155,16 @@ __global__ void __launch_bounds__(MT) k_ms_pull_W(DevView G, const uint32_t *V, 
 // front[u] after reading it (nothing else reads front in a push level), so
 // that front is all-zero when the level ends.
 // One 32-neighbour chunk of a pushing vertex with source mask m.
+// (p, len): a hub piece (hub_chunk), read directly; otherwise ranks j0 ..
 __device__ __forceinline__ void ms_push_chunk(const NbrList &L, uint64_t m, uint32_t j0,
                                               const uint64_t *seen, unsigned long long *acc,
-                                              uint32_t *T, uint32_t *tcnt, uint32_t lane) {
+                                              uint32_t *T, uint32_t *tcnt, uint32_t lane,
+                                              const uint32_t *p = nullptr, uint32_t len = 0) {
   const uint32_t j = j0 + lane;
   uint32_t x = 0;
   bool first = false;
-  if (j < L.deg) {
-    x = L.at(j);
+  if (p ? lane < len : j < L.deg) {
+    x = p ? p[lane] : L.at(j);
     if ((m & ~seen[x]) != 0) first = atomicOr(acc + x, (unsigned long long)m) == 0;
   }
   const uint32_t b = __ballot_sync(0xFFFFFFFFu, first);
@@ -207,17 +209,23 @@ __global__ void k_ms_push_hubs(DevView G, const uint32_t *hu, const uint64_t *hm
   const uint64_t nwarps = ((uint64_t)gridDim.x * MT) >> 5;
   const uint64_t nh = *hcnt;
   const uint64_t nwide = nh < 64 ? nh : 64;
+  const uint32_t *p;
+  uint32_t len;
   for (uint64_t i = 0; i < nwide; i++) {
     NbrList L = nbr_list(G, hu[i]);
-    const uint64_t nch = (L.deg + 31) >> 5;
-    for (uint64_t c = gw; c < nch; c += nwarps)
-      ms_push_chunk(L, hm[i], (uint32_t)(c << 5), seen, acc, T, tcnt, lane);
+    const uint64_t nch = hub_chunks(L);
+    for (uint64_t c = gw; c < nch; c += nwarps) {
+      hub_chunk(L, (uint32_t)c, p, len);
+      if (len) ms_push_chunk(L, hm[i], 0, seen, acc, T, tcnt, lane, p, len);
+    }
   }
   for (uint64_t i = nwide + blockIdx.x; i < nh; i += gridDim.x) {
     NbrList L = nbr_list(G, hu[i]);
-    const uint32_t nch = (L.deg + 31) >> 5;
-    for (uint32_t c = wib; c < nch; c += MT / 32)
-      ms_push_chunk(L, hm[i], c << 5, seen, acc, T, tcnt, lane);
+    const uint32_t nch = hub_chunks(L);
+    for (uint32_t c = wib; c < nch; c += MT / 32) {
+      hub_chunk(L, c, p, len);
+      if (len) ms_push_chunk(L, hm[i], 0, seen, acc, T, tcnt, lane, p, len);
+    }
   }
 }
 

@@ -165,6 +165,30 @@ __device__ __forceinline__ NbrList nbr_list(const DevView &G, uint32_t u) {
   return L;
 }
 
+// A hub's list in chunks for traversals that need no order: chunk c is the
+// 32-element piece c % 8 of unit c / 8, unit 0 being the inline row and unit
+// 1 + e the block of directory entry e (a block holds at most 256).  Sets the
+// piece's pointer and length (0: an empty piece).  Reads each element from
+// its slot, without a directory search per element.
+__device__ __forceinline__ uint32_t hub_chunks(const NbrList &L) { return (1 + L.nb) * 8; }
+
+__device__ __forceinline__ void hub_chunk(const NbrList &L, uint32_t c, const uint32_t *&p,
+                                          uint32_t &len) {
+  const uint32_t unit = c >> 3, off = (c & 7) * 32;
+  uint32_t ulen;
+  const uint32_t *up;
+  if (unit == 0) {
+    up = L.inl;
+    ulen = L.ni;
+  } else {
+    const uint32_t e = unit - 1;
+    up = L.seg + (uint64_t)L.dir[e] * HUB_BLOCK;
+    ulen = (e + 1 < L.nb ? L.pre[e + 1] : L.rest) - L.pre[e];
+  }
+  p = up + off;
+  len = off < ulen ? (ulen - off < 32 ? ulen - off : 32) : 0;
+}
+
 // Binary search for x in the neighbour list (lists are sorted, unique); a
 // hub's blocked part is searched through its directory's first keys.
 __device__ __forceinline__ bool list_has(const NbrList &L, uint32_t x) {
