@@ -31,13 +31,17 @@ constexpr int AT = 256;  // threads per CTA in the analytics kernels
 struct ClassPred {
   const uint32_t *deg;
   const int32_t *hub_of;
-  int cls;  // 0 = S, 1 = M, 2 = H, 3 = S and M (non-hub, degree >= 1)
+  int cls;  // 0 = S, 1 = M, 2 = H, 3 = S and M (non-hub, degree >= 1),
+            // 4 = M with 17..cut neighbours, 5 = M with more than cut
+  uint32_t cut;
   __device__ bool operator()(uint64_t i) const {
     bool hub = hub_of[i] >= 0;
     uint32_t d = deg[i];
     if (cls == 2) return hub;
     if (hub) return false;
     if (cls == 3) return d >= 1;
+    if (cls == 4) return d > K_INLINE && d <= cut;
+    if (cls == 5) return d > cut;
     return cls == 0 ? (d >= 1 && d <= K_INLINE) : d > K_INLINE;
   }
 };
@@ -50,18 +54,22 @@ void Graph::ensure_lists() {
   if (lists.version == version) return;
   uint64_t *cnt = s_cnt.get() + 24;
   uint64_t *t = tmp(select_tmp_elems(n) + 4);
-  uint32_t *bufs[4] = {lists.S.ensure(n), lists.M.ensure(n), lists.Hv.ensure(H ? H : 1),
-                       lists.SM.ensure(n)};
-  uint64_t lens[4];
-  for (int c = 0; c < 4; c++)
-    select_if(ClassPred{deg.get(), hub_of.get(), c}, IdxVal32{}, n, bufs[c], cnt + c, t, stream,
+  uint32_t *bufs[6] = {lists.S.ensure(n), lists.M.ensure(n), lists.Hv.ensure(H ? H : 1),
+                       lists.SM.ensure(n), lists.M1.ensure(n), lists.M2.ensure(n)};
+  uint64_t lens[6];
+  for (int c = 0; c < 6; c++) {
+    select_if(ClassPred{deg.get(), hub_of.get(), c, tuned.pr_group_cut}, IdxVal32{}, n, bufs[c],
+              cnt + c, t, stream,
               prof);
-  TRC_CUDA(cudaMemcpyAsync(lens, cnt, sizeof(lens), cudaMemcpyDeviceToHost, stream));
+  }
+  TRC_CUDA(cudaMemcpyAsync(lens, cnt, 48, cudaMemcpyDeviceToHost, stream));
   sync();
   lists.nS = lens[0];
   lists.nM = lens[1];
   lists.nH = lens[2];
   lists.nSM = lens[3];
+  lists.nM1 = lens[4];
+  lists.nM2 = lens[5];
   lists.version = version;
 }
 
@@ -117,6 +125,79 @@ __device__ __forceinline__ T block_sum(T v, T *sh) {
   }
   __syncthreads();
   return r;  // valid in thread 0
+}
+
+// ---------------------------------------------------------------------------
+// PageRank: per iteration p_next[u] = sum over N(u) of p[v]/deg(v)
+// (PR_Vertex then the dense PR_F pull).  The kernels read pdiv = p/deg of
+// the previous iteration and write both the new pdiv and, on the last
+// iteration, the undivided value.
+
+// Neighbour ids are read with streaming (evict-first) loads so the list
+// stream does not push the gathered rank vector out of L2.
+struct PRArgs {
+  const double *pc;
+  double *pn;
+  double *out;
+  double damping, base;
+  int last;
+};
+
+__device__ __forceinline__ void pr_range(const PRArgs &, uint32_t, uint32_t d, uint32_t &lo,
+                                         uint32_t &hi) {
+  lo = 0;
+  hi = d;
+}
+
+__device__ __forceinline__ void pr_store(const PRArgs &a, uint32_t u, uint32_t d, double sum) {
+  double val = a.damping > 0.0 ? a.base + a.damping * sum : sum;
+  a.pn[u] = val / (double)d;
+  if (a.last) a.out[u] = val;
+}
+
+__global__ void __launch_bounds__(AT) k_pr_S(DevView G, const uint32_t *S, uint64_t nS, PRArgs a) {
+  uint64_t gt = (uint64_t)blockIdx.x * AT + threadIdx.x;
+  uint64_t vi = gt >> 2;
+  uint32_t q = gt & 3;
+  double sum = 0.0;
+  uint32_t u = 0, d = 0;
+  if (vi < nS) {
+    u = S[vi];
+    d = G.deg[u];
+    uint32_t lo, hi;
+    pr_range(a, u, d, lo, hi);
+    uint32_t e = q * 4;
+    if (e < hi && e + 4 > lo) {
+      uint4 v = __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE) + q);
+      if (e >= lo && e < hi) sum += __ldg(a.pc + v.x);
+      if (e + 1 >= lo && e + 1 < hi) sum += __ldg(a.pc + v.y);
+      if (e + 2 >= lo && e + 2 < hi) sum += __ldg(a.pc + v.z);
+      if (e + 3 >= lo && e + 3 < hi) sum += __ldg(a.pc + v.w);
+    }
+  }
+  sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 1);
+  sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 2);
+  if (vi < nS && q == 0) pr_store(a, u, d, sum);
+}
+
+__global__ void __launch_bounds__(AT) k_pr_M(DevView G, const uint32_t *M, uint64_t nM, PRArgs a) {
+  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (w >= nM) return;
+  uint32_t u = M[w];
+  uint32_t d = G.deg[u];
+  double sum = 0.0;
+  if (lane < K_INLINE) sum = __ldg(a.pc + G.inl[(uint64_t)u * K_INLINE + lane]);
+  const uint32_t *seg = G.pma + G.pbeg[u];
+  uint32_t rest = d - K_INLINE;
+  uint32_t j = lane;
+  for (; j + 96 < rest; j += 128) {
+    uint32_t i0 = seg[j], i1 = seg[j + 32], i2 = seg[j + 64], i3 = seg[j + 96];
+    sum += __ldg(a.pc + i0) + __ldg(a.pc + i1) + __ldg(a.pc + i2) + __ldg(a.pc + i3);
+  }
+  for (; j < rest; j += 32) sum += __ldg(a.pc + seg[j]);
+  sum = warp_sum(sum);
+  if (lane == 0) pr_store(a, u, d, sum);
 }
 
 // Load-balanced pull.  Warp w takes list entries [32w, 32w+32); their
@@ -230,6 +311,198 @@ __global__ void __launch_bounds__(AT) k_flat(DevView G, const uint32_t *V, uint6
   op.store(f.valid, f.u, f.d, acc[lane]);  // (d == 0: nothing gathered, sum 0)
 }
 
+struct PROp {
+  PRArgs a;
+  __device__ bool skip(uint32_t) const { return false; }
+  __device__ double gather(uint32_t x) const { return __ldg(a.pc + x); }
+  __device__ void store(bool ok, uint32_t u, uint32_t d, double sum) const {
+    if (ok) pr_store(a, u, d, sum);
+  }
+};
+
+// Group pull for PMA vertices: GS lanes per vertex (8 for 17..64 neighbours,
+// 32 above), each lane issuing up to 8 independent index loads and then 8
+// gathers before using any of them; a shuffle reduction within the group.
+template <int GS>
+__global__ void __launch_bounds__(AT) k_pr_group(DevView G, const uint32_t *V, uint64_t nV, PRArgs a) {
+  constexpr int U = 8;
+  uint64_t gt = (uint64_t)blockIdx.x * AT + threadIdx.x;
+  uint64_t vi = gt / GS;
+  uint32_t q = gt % GS;
+  double sum = 0.0;
+  uint32_t u = 0, d = 0;
+  if (vi < nV) {
+    u = V[vi];
+    d = G.deg[u];
+    uint32_t lo, hi;
+    pr_range(a, u, d, lo, hi);
+    const uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
+    const uint32_t *seg = G.pma + G.pbeg[u] - K_INLINE;  // index by rank
+    for (uint32_t j0 = lo + q; j0 < hi; j0 += GS * U) {
+      uint32_t x[U];
+#pragma unroll
+      for (int k = 0; k < U; k++) {
+        uint32_t j = j0 + k * GS;
+        x[k] = j < hi ? (j < K_INLINE ? __ldcs(row + j) : __ldcs(seg + j)) : 0u;
+      }
+#pragma unroll
+      for (int k = 0; k < U; k++) {
+        uint32_t j = j0 + k * GS;
+        if (j < hi) sum += __ldg(a.pc + x[k]);
+      }
+    }
+  }
+#pragma unroll
+  for (int o = GS / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+  if (vi < nV && q == 0) pr_store(a, u, d, sum);
+}
+
+__global__ void __launch_bounds__(AT) k_pr_H(DevView G, const uint32_t *Hv, PRArgs a) {
+  __shared__ double sh[AT / 32];
+  uint32_t u = Hv[blockIdx.x];
+  int32_t h = G.hub_of[u];
+  uint32_t d = G.deg[u];
+  uint32_t ni = d < K_INLINE ? d : K_INLINE;
+  double sum = 0.0;
+  if (threadIdx.x < ni) sum = __ldg(a.pc + G.inl[(uint64_t)u * K_INLINE + threadIdx.x]);
+  const uint64_t e0 = G.hub_dir0[h];
+  const uint32_t nb = d > K_INLINE ? G.hub_nblk[h] : 0;
+  uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t b = warp; b < nb; b += AT / 32) {
+    const uint32_t id = G.hdir[e0 + b];
+    const uint32_t c = G.bcnt[id];
+    const uint32_t *blk = G.hslot + (uint64_t)id * HUB_BLOCK;
+    for (uint32_t s = lane; s < c; s += 32) sum += __ldg(a.pc + blk[s]);
+  }
+  sum = block_sum(sum, sh);
+  if (threadIdx.x == 0) pr_store(a, u, d, sum);
+}
+
+__global__ void k_pr_init(const uint32_t *deg, uint32_t n, double p0, double iso, double *pdiv,
+                          double *out) {
+  uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  uint32_t d = deg[u];
+  pdiv[u] = p0 / (double)d;
+  if (d == 0) out[u] = iso;
+}
+
+void Graph::pagerank(uint32_t iters, double damping, double *ranks, uint32_t flags) {
+  if (!ranks) throw_error(TRC_ERR_INVALID, "null output");
+  if (damping < 0.0 || damping >= 1.0) throw_error(TRC_ERR_INVALID, "damping must be in [0,1)");
+  ensure_lists();
+  bool dev = flags & TRC_DEVICE_PTR;
+  DBuf<double> pa, pb, ob;
+  pa.bind(&budget);
+  pb.bind(&budget);
+  ob.bind(&budget);
+  double *p0 = pa.alloc_exact(n), *p1 = pb.alloc_exact(n);
+  double *out = dev ? ranks : ob.alloc_exact(n);
+  if (iters == 0) {
+    // the reference returns the initial vector 1/n (include/Pagerank.h:137-141)
+    std::vector<double> h(n, 1.0 / (double)n);
+    TRC_CUDA(cudaMemcpyAsync(out, h.data(), (uint64_t)n * 8, cudaMemcpyHostToDevice, stream));
+    sync();
+  } else {
+    pagerank_launch(iters, damping, p0, p1, out, stream);
+  }
+  if (!dev) TRC_CUDA(cudaMemcpyAsync(ranks, out, (uint64_t)n * 8, cudaMemcpyDeviceToHost, stream));
+  sync();
+}
+
+void Graph::pr_kernels(uint32_t iters, double damping, double *p0, double *p1, double *out,
+                       cudaStream_t s) {
+  const double one_over_n = 1.0 / (double)n;
+  const double base = (1.0 - damping) / (double)n;
+  TRC_LAUNCH(prof, s, "pr_init", ceil_div(n, AT), AT, 0, k_pr_init, deg.get(), n, one_over_n,
+             damping > 0.0 ? base : 0.0, p0, out);
+  DevView G = view();
+  for (uint32_t it = 0; it < iters; it++) {
+    PRArgs a{p0, p1, out, damping, base, it + 1 == iters};
+    TRC_LAUNCH(prof, s, "pr_S", ceil_div(lists.nS * 4, AT), AT, 0, k_pr_S, G, lists.S.get(),
+               lists.nS, a);
+    switch (tuned.pr_group_lanes) {
+      case 4:
+        TRC_LAUNCH(prof, s, "pr_M4", ceil_div(lists.nM1 * 4, AT), AT, 0, k_pr_group<4>, G,
+                   lists.M1.get(), lists.nM1, a);
+        break;
+      case 16:
+        TRC_LAUNCH(prof, s, "pr_M16", ceil_div(lists.nM1 * 16, AT), AT, 0, k_pr_group<16>, G,
+                   lists.M1.get(), lists.nM1, a);
+        break;
+      default:
+        TRC_LAUNCH(prof, s, "pr_M8", ceil_div(lists.nM1 * 8, AT), AT, 0, k_pr_group<8>, G,
+                   lists.M1.get(), lists.nM1, a);
+    }
+    TRC_LAUNCH(prof, s, "pr_M32", ceil_div(lists.nM2 * 32, AT), AT, 0, k_pr_group<32>, G,
+               lists.M2.get(), lists.nM2, a);
+    TRC_LAUNCH(prof, s, "pr_H", lists.nH, AT, 0, k_pr_H, G, lists.Hv.get(), a);
+    std::swap(p0, p1);
+  }
+}
+
+// The iteration loop (iters x 4 launches) is replayed from a CUDA graph:
+// captured once per (iteration count, buffers, class lists) and patched with
+// cudaGraphExecUpdate when only kernel arguments changed.  With the
+// per-kernel profiler on, kernels are launched directly so that each gets
+// its own events.  Requires the class lists (ensure_lists) and iters >= 1;
+// nothing is allocated or synchronised, so it may run on a second stream.
+void Graph::pagerank_launch(uint32_t iters, double damping, double *p0, double *p1, double *out,
+                            cudaStream_t s) {
+  if (prof.on || !use_graphs || iters < 2) {
+    pr_kernels(iters, damping, p0, p1, out, s);
+    return;
+  }
+  uint64_t dbits;
+  memcpy(&dbits, &damping, 8);
+  const uint64_t key[PRGraphCache::KEY] = {iters, dbits, (uint64_t)p0, (uint64_t)p1, (uint64_t)out,
+                                           lists.version, (uint64_t)lists.S.get(), lists.nS,
+                                           lists.nM1, lists.nM2, lists.nH, (uint64_t)s,
+                                           tuned.pr_group_lanes};
+  bool same = prg.exec != nullptr;
+  for (int i = 0; same && i < PRGraphCache::KEY; i++) same = prg.key[i] == key[i];
+  if (!same) {
+    const uint64_t before = prof.launches;
+    cudaGraph_t gr = nullptr;
+    TRC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      pr_kernels(iters, damping, p0, p1, out, s);
+    } catch (...) {
+      cudaStreamEndCapture(s, &gr);
+      if (gr) cudaGraphDestroy(gr);
+      prof.launches = before;
+      throw;
+    }
+    TRC_CUDA(cudaStreamEndCapture(s, &gr));
+    prg.kernels = prof.launches - before;
+    prof.launches = before;
+    bool updated = false;
+    if (prg.exec) {
+      cudaGraphExecUpdateResultInfo info;
+      updated = cudaGraphExecUpdate(prg.exec, gr, &info) == cudaSuccess;
+      if (!updated) {
+        cudaGetLastError();
+        cudaGraphExecDestroy(prg.exec);
+        prg.exec = nullptr;
+      }
+    }
+    if (!updated) {
+      cudaError_t e = cudaGraphInstantiate(&prg.exec, gr, 0);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(gr);
+        prg.exec = nullptr;
+        TRC_CUDA(e);
+      }
+    }
+    cudaGraphDestroy(gr);
+    memcpy(prg.key, key, sizeof(key));
+    prg.replays_built++;
+  }
+  TRC_CUDA(cudaGraphLaunch(prg.exec, s));
+  prof.launches += prg.kernels;
+  prg.replays++;
+}
+
 // ---------------------------------------------------------------------------
 // BFS (direction-optimising).  Levels are unique; parents follow the
 // reference: push claims a vertex with CAS (any frontier parent, BFS_F::
@@ -244,8 +517,9 @@ struct BFSState {
   uint32_t *next;        // next-frontier queue
   uint32_t *next_cnt;
   uint32_t d;            // current level
-  // push steps: the frontier's hubs (seg); dense steps: the vertices left
-  // unvisited (cand, the next dense step's candidates of the same class)
+  // dense steps: vertices left unvisited by the inline pass that have a
+  // PMA segment (seg), and vertices left unvisited by the step (cand, the
+  // next dense step's candidates); push steps: the frontier's hubs (seg)
   uint32_t *seg, *seg_cnt;
   uint32_t *cand, *cand_cnt;
 };
@@ -372,8 +646,7 @@ __global__ void k_level_bits(const uint32_t *lv, uint32_t n, uint32_t d, uint32_
 // is used: list entries, then degree and level, then the row quarters, then
 // the 4 * BP_V frontier-bitmap words.  The first frontier neighbour in
 // sorted order wins (lowest lane of the quad with a hit, then its lowest
-// element).  The list holds vertices of at most 16 neighbours; those left
-// unvisited become the next dense step's candidates.
+// element).
 constexpr uint32_t BP_V = 4;
 
 __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S, uint64_t nS,
@@ -408,7 +681,7 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
     ww[i] = act[i] && e + 3 < d[i] ? __ldg(s.bits + (v[i].w >> 5)) : 0u;
   }
   uint32_t wins = 0;  // bit i: this lane claimed vertex i
-  uint32_t tocand = 0;  // bit i (lane q == 0): vertex i stays unvisited
+  uint32_t tosg = 0, tocand = 0;  // bit i (lane q == 0): vertex i stays unvisited
 #pragma unroll
   for (uint32_t i = 0; i < BP_V; i++) {
     const bool uv = d[i] > 0 && s.lv[u[i]] == TRC_UNREACHED;  // cached: loaded above
@@ -426,13 +699,20 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
       s.lv[u[i]] = s.d + 1;
       wins |= 1u << i;
     }
-    if (q == 0 && uv && grp == 0) tocand |= 1u << i;
+    if (q == 0 && uv && grp == 0) {
+      if (d[i] > K_INLINE) tosg |= 1u << i;
+      else tocand |= 1u << i;
+    }
   }
   __shared__ uint32_t sh[AT / 32 + 2];
   uint32_t pos = block_append(__popc(wins), s.next_cnt, sh);
 #pragma unroll
   for (uint32_t i = 0; i < BP_V; i++)
     if ((wins >> i) & 1u) s.next[pos++] = u[i];
+  pos = block_append(__popc(tosg), s.seg_cnt, sh);
+#pragma unroll
+  for (uint32_t i = 0; i < BP_V; i++)
+    if ((tosg >> i) & 1u) s.seg[pos++] = u[i];
   pos = block_append(__popc(tocand), s.cand_cnt, sh);
 #pragma unroll
   for (uint32_t i = 0; i < BP_V; i++)
@@ -440,8 +720,8 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
 }
 
 // One warp scans the neighbours of vertex u of rank >= j_first for a
-// frontier member from the largest id down, 32 in the first step, then 64
-// per step (two independent loads per lane), and returns the smallest frontier neighbour of the first
+// frontier member, 64 per step from the largest id down (two independent
+// loads per lane), and returns the smallest frontier neighbour of the first
 // step that has one, or NONE32 (warp-uniform).  Any frontier neighbour is a
 // valid parent (the levels do not depend on the choice); scanning from the
 // top finds one sooner on graphs whose high-degree vertices have large ids
@@ -450,11 +730,9 @@ __device__ __forceinline__ uint32_t warp_any_in_frontier(const NbrList &L, const
                                                          uint32_t j_first) {
   const uint32_t lane = threadIdx.x & 31;
   for (uint32_t e = L.deg; e > j_first;) {
-    // the first step reads only the 32 largest: most vertices stop there
-    const uint32_t width = e == L.deg ? 32u : 64u;
-    const uint32_t s0 = e - j_first > width ? e - width : j_first;
+    const uint32_t s0 = e - j_first > 64 ? e - 64 : j_first;
     const uint32_t ja = s0 + lane, jb = s0 + 32 + lane;
-    const bool va = ja < e, vb = width == 64u && jb < e;
+    const bool va = ja < e, vb = jb < e;
     const uint32_t xa = va ? L.at(ja) : 0u, xb = vb ? L.at(jb) : 0u;
     const bool ha = va && bit_test(bits, xa), hb = vb && bit_test(bits, xb);
     const uint32_t ma = __ballot_sync(0xFFFFFFFFu, ha), mb = __ballot_sync(0xFFFFFFFFu, hb);
@@ -543,50 +821,44 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
   uint64_t words = ceil_div(n, 32);
   uint32_t *bm = bits.alloc_exact(words);
   uint32_t *c = cnt.alloc_exact(4);
-  DBuf<uint32_t> hb;
-  hb.bind(&budget);
-  uint32_t *hubl = hb.alloc_exact(H ? H : 1);  // the frontier's hubs of a push step
   TRC_LAUNCH(prof, stream, "bfs_init", ceil_div(n, AT), AT, 0, k_bfs_init, lv, par, n, src, F);
   DevView G = view();
   uint32_t nf = 1, d = 0;
   const uint64_t dense_at = n / push_pull_divisor();
-  // candidates of the dense steps, compacted after every dense step: the
-  // unvisited vertices of at most 16 neighbours (their whole list is the
-  // inline row: one pass of four lanes per vertex) and the unvisited non-hub
-  // vertices of more (a warp per vertex, scanning from the largest
-  // neighbour down: on RMAT graphs of the reference's generator the
-  // highest-degree vertices have the largest ids, so a frontier neighbour
-  // is found in the first step, and the inline row -- the smallest
-  // neighbours -- is read only when the rest has none)
-  DBuf<uint32_t> cbS[2], cbM[2];
-  for (auto *b : {&cbS[0], &cbS[1], &cbM[0], &cbM[1]}) b->bind(&budget);
-  const uint32_t *candS = lists.S.get(), *candM = lists.M.get();
-  uint64_t ncS = lists.nS, ncM = lists.nM;
+  // candidates of the dense steps: non-hub vertices not yet visited,
+  // compacted after every dense step
+  DBuf<uint32_t> cbuf[2], segb;  // candidate ping-pong, segment-pass list
+  cbuf[0].bind(&budget);
+  cbuf[1].bind(&budget);
+  segb.bind(&budget);
+  const uint32_t *cand = lists.SM.get();
+  uint64_t ncand = lists.nSM;
   int cnext = 0;
+  uint32_t *sg = segb.ensure(n);
   const unsigned pgrid = (unsigned)num_sms() * 8;
   while (nf > 0) {
-    TRC_CUDA(cudaMemsetAsync(c, 0, 16, stream));  // next, hubs, S cand, M cand counts
-    BFSState s{lv, par, bm, Nx, c, d, hubl, c + 1, nullptr, c + 2};
-    uint32_t hc[4] = {0, 0, 0, 0};
+    TRC_CUDA(cudaMemsetAsync(c, 0, 16, stream));  // next, seg, cand counts
+    BFSState s{lv, par, bm, Nx, c, d, sg, c + 1, nullptr, c + 2};
+    uint32_t hc[3] = {0, 0, 0};
     if ((uint64_t)nf >= dense_at && dense_at > 0) {
       TRC_LAUNCH(prof, stream, "bfs_bits", ceil_div(n, AT), AT, 0, k_level_bits, lv, n, d, bm);
-      // candidates left for the next dense step (never the lists being read)
-      s.cand = cbS[cnext].ensure(ncS ? ncS : 1);
-      BFSState sm = s;
-      sm.cand = cbM[cnext].ensure(ncM ? ncM : 1);
-      sm.cand_cnt = c + 3;
-      TRC_LAUNCH(prof, stream, "bfs_pull_inline", ceil_div(ncS * 4, (uint64_t)AT * BP_V), AT, 0,
-                 k_bfs_pull_S, G, candS, ncS, s);
-      TRC_LAUNCH(prof, stream, "bfs_pull_M", std::min<uint64_t>(pgrid, ceil_div(ncM * 32, AT)), AT,
-                 0, k_bfs_pull_W, G, candM, ncM, (const uint32_t *)nullptr, sm, 0u, 1);
+      // candidates left for the next dense step (never the list being read)
+      s.cand = cbuf[cnext].ensure(ncand ? ncand : 1);
+      // pass A: the 16 inline neighbours of every unvisited non-hub vertex;
+      // those left unvisited go to the segment list (PMA vertices) or the
+      // next candidates
+      TRC_LAUNCH(prof, stream, "bfs_pull_inline", ceil_div(ncand * 4, (uint64_t)AT * BP_V), AT, 0,
+                 k_bfs_pull_S, G, cand, ncand, s);
+      // pass B: the PMA segments of the segment list (count on the device);
+      // hubs from rank 0
+      TRC_LAUNCH(prof, stream, "bfs_pull_M", pgrid, AT, 0, k_bfs_pull_W, G, sg, 0, c + 1, s,
+                 K_INLINE, 1);
       TRC_LAUNCH(prof, stream, "bfs_pull_H", ceil_div(lists.nH * 32, AT), AT, 0, k_bfs_pull_W, G,
                  lists.Hv.get(), lists.nH, (const uint32_t *)nullptr, s, 0u, 0);
-      TRC_CUDA(cudaMemcpyAsync(hc, c, 16, cudaMemcpyDeviceToHost, stream));
+      TRC_CUDA(cudaMemcpyAsync(hc, c, 12, cudaMemcpyDeviceToHost, stream));
       sync();
-      ncS = hc[2];
-      ncM = hc[3];
-      candS = s.cand;
-      candM = sm.cand;
+      ncand = hc[2];
+      cand = s.cand;
       cnext ^= 1;
     } else {
       TRC_LAUNCH(prof, stream, "bfs_push", ceil_div((uint64_t)nf * 32, AT), AT, 0, k_bfs_push, G, F,
@@ -686,16 +958,22 @@ __global__ void __launch_bounds__(AT) k_cc_S(DevView G, const uint32_t *S, uint6
     if (q * 4 + i < d && q * 4 + i >= CC_SAMPLE_NB) uf_unite(p, u, e[i]);
 }
 
-// ... and a warp per vertex of more
+// ... and a warp per vertex of more: a warp takes 32 list entries, finds
+// with one test per lane those outside the giant component, and walks their
+// lists one after the other
 __global__ void __launch_bounds__(AT) k_cc_W(DevView G, const uint32_t *Lst, uint64_t nL,
                                              uint32_t *p, uint32_t c) {
-  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
-  uint32_t lane = threadIdx.x & 31;
-  if (w >= nL) return;
-  uint32_t u = Lst[w];
-  if (uf_find(p, u) == c) return;  // warp-uniform
-  NbrList L = nbr_list(G, u);
-  for (uint32_t j = CC_SAMPLE_NB + lane; j < L.deg; j += 32) uf_unite(p, u, L.at(j));
+  const uint64_t i = (uint64_t)blockIdx.x * AT + threadIdx.x;  // 32 entries per warp
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t ul = i < nL ? Lst[i] : 0u;
+  uint32_t todo = __ballot_sync(0xFFFFFFFFu, i < nL && uf_find(p, ul) != c);
+  while (todo) {
+    const uint32_t k = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const uint32_t u = __shfl_sync(0xFFFFFFFFu, ul, k);
+    NbrList L = nbr_list(G, u);
+    for (uint32_t j = CC_SAMPLE_NB + lane; j < L.deg; j += 32) uf_unite(p, u, L.at(j));
+  }
 }
 
 __global__ void k_cc_init(uint32_t *p, uint32_t n) {
@@ -746,9 +1024,9 @@ void Graph::cc(uint32_t *labels, uint32_t flags) {
   }
   TRC_LAUNCH(prof, stream, "cc_S", ceil_div(lists.nS * 4, AT), AT, 0, k_cc_S, G, lists.S.get(),
              lists.nS, p, c);
-  TRC_LAUNCH(prof, stream, "cc_M", ceil_div(lists.nM * 32, AT), AT, 0, k_cc_W, G, lists.M.get(),
+  TRC_LAUNCH(prof, stream, "cc_M", ceil_div(lists.nM, AT), AT, 0, k_cc_W, G, lists.M.get(),
              lists.nM, p, c);
-  TRC_LAUNCH(prof, stream, "cc_H", ceil_div(lists.nH * 32, AT), AT, 0, k_cc_W, G, lists.Hv.get(),
+  TRC_LAUNCH(prof, stream, "cc_H", ceil_div(lists.nH, AT), AT, 0, k_cc_W, G, lists.Hv.get(),
              lists.nH, p, c);
   TRC_LAUNCH(prof, stream, "cc_final", ceil_div(n, AT), AT, 0, k_cc_final, p, n);
   if (!dev) TRC_CUDA(cudaMemcpyAsync(labels, p, (uint64_t)n * 4, cudaMemcpyDeviceToHost, stream));

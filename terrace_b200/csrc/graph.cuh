@@ -21,26 +21,14 @@ __device__ __forceinline__ bool has_edge(const DevView &G, uint32_t u, uint32_t 
   return list_has(L, x);
 }
 
-// Per-vertex class lists for the traversal kernels, rebuilt when the graph
+// Per-vertex class lists for the analytics kernels, rebuilt when the graph
 // version changes: S = 1..16 neighbours (inline only), M = more than 16 and
-// not a hub (inline + PMA segment), H = hubs, SM = S and M.
+// not a hub (inline + PMA segment), H = hubs, SM = S and M; M1 / M2 = M up
+// to / above PageRank's lane-group cut.
 struct ClassLists {
   uint64_t version = ~0ull;
-  DBuf<uint32_t> S, M, Hv, SM;
-  uint64_t nS = 0, nM = 0, nH = 0, nSM = 0;
-};
-
-// PageRank's snapshot of the graph (pagerank.cu), rebuilt when the graph
-// changes: non-isolated vertices relabelled by degree, highest first (perm:
-// new -> old id, inv: old -> new, dsort: degrees in the new order), their
-// lists as one CSR (off, adj: relabelled neighbour ids), and the degree
-// class boundaries of the pull kernels for the lane-group cut `cut`.
-struct PRSnap {
-  uint64_t version = ~0ull;
-  uint64_t na = 0, rb = 0, rw = 0, rg = 0;
-  uint32_t cut = 0;
-  DBuf<uint32_t> perm, inv, dsort, adj;
-  DBuf<uint64_t> off;
+  DBuf<uint32_t> S, M, Hv, SM, M1, M2;
+  uint64_t nS = 0, nM = 0, nH = 0, nSM = 0, nM1 = 0, nM2 = 0;
 };
 
 // Tier-3 work of one batch between its two launch phases (hubs.cu).
@@ -134,8 +122,6 @@ class Graph {
   DBuf<uint32_t> s_wbits;  // per-level PMA window bitmaps (this batch)
   DBuf<uint32_t> s_hw_do;  // old degree of each touched hub
   ClassLists lists;
-  PRSnap prs;
-  void ensure_pr_snapshot();
 
   DevView view() const;
   uint32_t vbits() const;

@@ -699,7 +699,7 @@ class Server {
       return false;
     }
     // async: class lists current, buffers sized, then everything on s2_
-    g_.ensure_pr_snapshot();
+    g_.ensure_lists();
     const unsigned nb = reduce_grid();
     double *p0 = pr0_.ensure(n), *p1 = pr1_.ensure(n), *x = ranks_.ensure(n);
     double *part = pr_part_.ensure(2 * (uint64_t)nb * pr_groups_.size());

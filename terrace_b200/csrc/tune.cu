@@ -89,30 +89,27 @@ void Graph::autotune(uint32_t what, const uint32_t *src, const uint32_t *dst, ui
       cudaEvent_t e0, e1;
       TRC_CUDA(cudaEventCreate(&e0));
       TRC_CUDA(cudaEventCreate(&e1));
-      auto time2 = [&]() {  // two iterations, best of two
-        pagerank_launch(1, 0.0, p0, p1, out, stream);  // warm
-        float t = 1e30f;
-        for (int rep = 0; rep < 2; rep++) {
-          TRC_CUDA(cudaEventRecord(e0, stream));
-          pagerank_launch(2, 0.0, p0, p1, out, stream);
-          TRC_CUDA(cudaEventRecord(e1, stream));
-          TRC_CUDA(cudaEventSynchronize(e1));
-          float ms = 0;
-          TRC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-          t = std::min(t, ms);
-        }
-        if (t < best) {
-          best = t;
-          best_t = tuned;
-        }
-      };
-      // the lane group and the cut between lane groups and warps
       for (uint32_t cut : {32u, 64u, 128u}) {
         tuned.pr_group_cut = cut;
-        ensure_pr_snapshot();  // class boundaries for the cut
+        lists.version = ~0ull;  // the class lists depend on the cut
+        ensure_lists();
         for (uint32_t lanes : {4u, 8u, 16u}) {
           tuned.pr_group_lanes = lanes;
-          time2();
+          pagerank_launch(1, 0.0, p0, p1, out, stream);  // warm
+          float t = 1e30f;
+          for (int rep = 0; rep < 2; rep++) {
+            TRC_CUDA(cudaEventRecord(e0, stream));
+            pagerank_launch(2, 0.0, p0, p1, out, stream);
+            TRC_CUDA(cudaEventRecord(e1, stream));
+            TRC_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            TRC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            t = std::min(t, ms);
+          }
+          if (t < best) {
+            best = t;
+            best_t = tuned;
+          }
         }
       }
       cudaEventDestroy(e0);
@@ -120,7 +117,6 @@ void Graph::autotune(uint32_t what, const uint32_t *src, const uint32_t *dst, ui
       tuned.pr_group_cut = best_t.pr_group_cut;
       tuned.pr_group_lanes = best_t.pr_group_lanes;
       lists.version = ~0ull;
-      ensure_pr_snapshot();
       ms_out[1] = best / 2.0;
     }
     // -------------------------------------------------- PMA leaf

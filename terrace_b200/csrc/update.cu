@@ -60,7 +60,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
                   &bcnt, &bmin, &bown, &bfree, &bfreed, &stamp, &s_in_src, &s_in_dst, &s_tu, &s_tdn,
                   &s_tc2, &s_ovl, &s_hw_u, &s_hw_dn, &s_hw_t, &s_c2n, &s_rlist, &s_pma_next,
                   &s_lgroup, &s_lwarp,
-                  &lists.S, &lists.M, &lists.Hv, &lists.SM,
+                  &lists.S, &lists.M, &lists.Hv, &lists.SM, &lists.M1, &lists.M2,
                   &s_lg, &s_lx, &s_lli, &s_tgq, &s_tgo, &s_tgb, &s_hflag, &s_rwstage})
     b->bind(&budget);
   for (auto *b : {&pbeg, &hub_dir0, &s_A, &s_B, &s_C, &s_tmp, &s_cnt, &s_P, &s_oOff, &s_nOff,
@@ -68,8 +68,6 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
     b->bind(&budget);
   s_hnbd.bind(&budget);
   hub_of.bind(&budget);
-  for (auto *b : {&prs.perm, &prs.inv, &prs.dsort, &prs.adj}) b->bind(&budget);
-  prs.off.bind(&budget);
   wstamp.bind(&budget);
   pbeg_alt.bind(&budget);
   s_tix.bind(&budget);
@@ -161,12 +159,8 @@ void Graph::release_scratch() {
   s_hnbd.reset();
   s_flags.reset();
   lists.version = ~0ull;
-  for (auto *b : {&lists.S, &lists.M, &lists.Hv, &lists.SM})
+  for (auto *b : {&lists.S, &lists.M, &lists.Hv, &lists.SM, &lists.M1, &lists.M2})
     b->reset();
-  prs.version = ~0ull;
-  prs.cut = 0;
-  for (auto *b : {&prs.perm, &prs.inv, &prs.dsort, &prs.adj}) b->reset();
-  prs.off.reset();
   sync();
   budget.trim();
 }
