@@ -39,7 +39,7 @@ struct HubItem {
 struct HubCtx {
   bool active = false, readback = false, insert = false;
   uint32_t fill = 192;
-  uint64_t NL = 0, QL = 0, F = 0, fresh0 = 0;
+  uint64_t NL = 0, QL = 0, F = 0, fresh0 = 0, R = 0;
   std::vector<HubItem> loc, rw;
   std::vector<uint64_t> lp;
   uint64_t *d_lp = nullptr;
@@ -118,7 +118,6 @@ class Graph {
   DBuf<uint8_t> s_flags;
   DBuf<uint32_t> s_pma_next;
   DBuf<uint32_t> s_tix;  // vertex -> index in the touched list (this batch)
-  DBuf<uint32_t> s_lgroup, s_lwarp;  // rewrite entries merged by a lane group / a warp
   DBuf<uint32_t> s_wbits;  // per-level PMA window bitmaps (this batch)
   DBuf<uint32_t> s_hw_do;  // old degree of each touched hub
   ClassLists lists;

@@ -23,11 +23,12 @@
 //   ones replaced by their output blocks.  Bytes moved scale with the blocks
 //   touched, not with the hub's degree.
 //
-//   rewrite (new hubs, hubs without blocks, growth past the old size, a
-//   group with more keys than one merge stages, an inline row that cannot be
-//   refilled from the first two blocks): every old element and every key is
-//   placed at its new rank directly in fresh, uniformly filled blocks; the
-//   old blocks are freed.
+//   rewrite (new hubs, hubs of fewer than HB_LOCAL_MIN neighbours, hubs
+//   without blocks, growth past the old size, a group with more keys than
+//   one merge stages, an inline row that cannot be refilled from the first
+//   two blocks): every old element and every key is placed at its new rank
+//   directly in uniformly filled blocks taken from the free list (then the
+//   pool); the old blocks are freed.
 //
 // Which groups of a block-local hub need the rewrite is known only after the
 // groups are counted, so the host reads those counts once; the small-vertex
@@ -43,6 +44,9 @@ constexpr uint32_t HB_MIN = 64;    // fewer elements after a delete: absorb the 
 constexpr uint32_t HB_OUT = 32;    // most blocks one touched block becomes
 constexpr uint32_t HB_GK = 4096;   // most keys one block merge stages in shared memory
 constexpr uint32_t HB_STAGE = K_INLINE + 2 * HUB_BLOCK;  // old elements of a group, at most
+// Hubs of fewer neighbours than this are rewritten whole: their list is a
+// few KB, less than locating the keys and rebuilding the directory costs.
+constexpr uint32_t HB_LOCAL_MIN = 8192;
 
 // Counter slots in the batch's device counter array (update.cu uses 0..10,
 // the analytics 24..29).
@@ -185,7 +189,8 @@ __global__ void k_hub_count(DevView G, const uint64_t *lp, const uint64_t *cnt, 
 }
 
 // Pool id of the a-th block allocated in this batch: the free list first
-// (from its top), then fresh blocks.
+// (from its top), then fresh blocks.  Indices [0, R) belong to the rewritten
+// hubs (ranges planned on the host), R on to the splits (a device counter).
 __device__ __forceinline__ uint32_t alloc_id(uint64_t a, const uint32_t *bfree, uint64_t F,
                                             uint64_t fresh0) {
   return a < F ? bfree[F - 1 - a] : (uint32_t)(fresh0 + (a - F));
@@ -197,7 +202,7 @@ __global__ void __launch_bounds__(256) k_hub_merge_group(
     DevView G, const uint64_t *lp, const uint64_t *cnt, uint64_t QL, const uint32_t *tgq,
     const uint32_t *lli, const uint32_t *lg, const uint32_t *lx, const uint32_t *tgo,
     const uint32_t *hflag, int insert, const uint32_t *bfree, uint64_t F, uint64_t fresh0,
-    uint32_t *bfreed, uint32_t *tgb, unsigned long long *ctr) {
+    uint64_t R, uint32_t *bfreed, uint32_t *tgb, unsigned long long *ctr) {
   __shared__ uint32_t A[HB_STAGE];
   __shared__ uint32_t O[HB_STAGE + HB_GK];
   __shared__ uint32_t ids[HB_OUT];
@@ -247,7 +252,7 @@ __global__ void __launch_bounds__(256) k_hub_merge_group(
   if (threadIdx.x == 0) {
     const unsigned long long a0 = nout > 1 ? atomicAdd(ctr + H_ALLOC, (unsigned long long)(nout - 1)) : 0ull;
     if (nout > 0) ids[0] = b;
-    for (uint32_t t = 1; t < nout; t++) ids[t] = alloc_id(a0 + t - 1, bfree, F, fresh0);
+    for (uint32_t t = 1; t < nout; t++) ids[t] = alloc_id(R + a0 + t - 1, bfree, F, fresh0);
     if (nout == 0) bfreed[atomicAdd(ctr + H_FREED, 1ull)] = b;
     if (absorb) {
       bfreed[atomicAdd(ctr + H_FREED, 1ull)] = b2;
@@ -374,7 +379,8 @@ __global__ void __launch_bounds__(256) k_hub_dir(DevView G, const uint64_t *lp, 
 // is read through the unchanged tiers.
 __global__ void k_hub_rw_place(DevView G, const uint64_t *rp, uint64_t NR, uint64_t QR,
                                const uint32_t *hw_t, const uint64_t *tpos, const uint64_t *bkeys,
-                               int insert, uint32_t *stage) {
+                               int insert, uint32_t *stage, const uint32_t *bfree, uint64_t F,
+                               uint64_t fresh0) {
   const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= QR) return;
   const uint64_t r = row_of(rp, NR, RP_W, RP_Q0, q);
@@ -403,7 +409,8 @@ __global__ void k_hub_rw_place(DevView G, const uint64_t *rp, uint64_t NR, uint6
     stage[r * K_INLINE + rank] = x;
   } else {
     const uint32_t rr = rank - K_INLINE, per = (uint32_t)row[RP_PER];
-    G.hslot[(row[RP_BLK0] + rr / per) * HUB_BLOCK + rr % per] = x;
+    const uint32_t b = alloc_id(row[RP_BLK0] + rr / per, bfree, F, fresh0);
+    G.hslot[(uint64_t)b * HUB_BLOCK + rr % per] = x;
   }
 }
 
@@ -411,7 +418,8 @@ __global__ void k_hub_rw_place(DevView G, const uint64_t *rp, uint64_t NR, uint6
 // the freed list, the new blocks' counts / first keys / owner, the directory,
 // the hub table entry and the degree.
 __global__ void k_hub_rw_finish(DevView G, const uint64_t *rp, const uint32_t *stage,
-                                uint32_t *bfreed, unsigned long long *ctr) {
+                                uint32_t *bfreed, unsigned long long *ctr, const uint32_t *bfree,
+                                uint64_t F, uint64_t fresh0) {
   const uint64_t r = blockIdx.x;
   const uint64_t *row = rp + r * RP_W;
   const uint32_t h = (uint32_t)row[RP_H], u = (uint32_t)row[RP_U], dn = (uint32_t)row[RP_DN];
@@ -429,13 +437,13 @@ __global__ void k_hub_rw_finish(DevView G, const uint64_t *rp, const uint32_t *s
       bfreed[atomicAdd(ctr + H_FREED, 1ull)] = G.hdir[e0 + i];
   }
   for (uint32_t i = threadIdx.x; i < nbw; i += blockDim.x) {
-    const uint64_t b = blk0 + i;
+    const uint32_t b = alloc_id(blk0 + i, bfree, F, fresh0);
     const uint32_t c = rest - i * per < per ? rest - i * per : per;
-    const uint32_t first = G.hslot[b * HUB_BLOCK];
+    const uint32_t first = G.hslot[(uint64_t)b * HUB_BLOCK];
     G.bcnt[b] = c;
     G.bmin[b] = first;
     G.bown[b] = u;
-    G.hdir[e1 + i] = (uint32_t)b;
+    G.hdir[e1 + i] = b;
     G.hpre[e1 + i] = i * per;
     G.hkey[e1 + i] = first;
   }
@@ -453,9 +461,9 @@ __global__ void k_hub_rw_finish(DevView G, const uint64_t *rp, const uint32_t *s
 
 // The free list after the batch: the entries the splits did not take (its
 // bottom F - min(F, allocated)), then the blocks freed.
-__global__ void k_hub_free_merge(uint32_t *bfree, uint64_t F, const uint32_t *bfreed,
+__global__ void k_hub_free_merge(uint32_t *bfree, uint64_t F, uint64_t R, const uint32_t *bfreed,
                                  const unsigned long long *ctr) {
-  const uint64_t nf = ctr[H_FREED], na = ctr[H_ALLOC];
+  const uint64_t nf = ctr[H_FREED], na = R + ctr[H_ALLOC];
   const uint64_t keep = F - (na < F ? na : F);
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nf;
        i += (uint64_t)gridDim.x * blockDim.x)
@@ -567,7 +575,8 @@ void Graph::apply_hubs(uint64_t nh, const std::vector<uint32_t> &hu,
       const uint32_t rest_old = hdo[i] > K_INLINE ? hdo[i] - K_INLINE : 0;
       const uint32_t rest_new = hdn[i] > K_INLINE ? hdn[i] - K_INLINE : 0;
       const uint32_t k = insert ? hdn[i] - hdo[i] : hdo[i] - hdn[i];
-      rewrite = nbo == 0 || (insert && k > rest_old) || rest_new < 2 * HB_MIN;
+      rewrite = nbo == 0 || hdo[i] < HB_LOCAL_MIN || (insert && k > rest_old) ||
+                rest_new < 2 * HB_MIN;
       freed_bound += nbo;
     }
     (rewrite ? c.rw : c.loc).push_back({i, (uint32_t)h});
@@ -663,12 +672,13 @@ void Graph::apply_hubs_finish() {
     else nloc++;
   }
   const uint64_t NR = rw.size();
-  // ---- blocks: each rewritten hub takes a fresh contiguous range; local
-  // splits take the free list's top first, then fresh blocks after those
-  // ranges (alloc_req bounds them: groups of hubs flagged later allocate
-  // nothing, so the pool top is set from the device's count at the end)
+  // ---- blocks, by allocation index (free list top first, then fresh):
+  // each rewritten hub a planned range of indices, then the splits from a
+  // device counter (alloc_req bounds them: groups of hubs flagged later
+  // allocate nothing, so the pool top is set from the device's count)
   const uint64_t F = nfree;
-  uint64_t top = pool_top;
+  const uint64_t fresh0 = pool_top;
+  uint64_t R = 0;
   std::vector<uint64_t> rp(NR * RP_W, 0);
   uint64_t QR = 0, written_blocks = 0;
   for (uint64_t r = 0; r < NR; r++) {
@@ -683,18 +693,17 @@ void Graph::apply_hubs_finish() {
     row[RP_IHW] = i;
     row[RP_DO] = hdo[i];
     row[RP_DN] = hdn[i];
-    row[RP_BLK0] = top;
+    row[RP_BLK0] = R;
     row[RP_PER] = per;
     row[RP_NB] = nb;
     row[RP_Q0] = QR;
     QR += insert ? hdn[i] : hdo[i];  // old elements (+ keys on insert)
-    top += nb;
+    R += nb;
     written_blocks += nb;
     h_hub_nblk[h] = nb;
     row[RP_E1] = hub_dir_target(h, nb);
   }
-  const uint64_t fresh0 = top;
-  const uint64_t top_bound = top + (alloc_req > F ? alloc_req - F : 0);
+  const uint64_t top_bound = fresh0 + (R + alloc_req > F ? R + alloc_req - F : 0);
   std::vector<uint64_t> e1s(NL, 0);
   for (uint64_t li = 0; li < NL; li++) {
     if (flagged[li]) continue;
@@ -722,27 +731,28 @@ void Graph::apply_hubs_finish() {
   if (NL && ntg) {
     TRC_LAUNCH(prof, z, "hub_merge_group", ntg, 256, 0, k_hub_merge_group, G, c.d_lp, cnt, QL,
                c.tgq, c.lli, c.lg, c.lx, c.tgo, c.hflag, insert ? 1 : 0, bfree.get(), F, fresh0,
-               c.freed, c.tgb, ctr);
+               R, c.freed, c.tgb, ctr);
     TRC_LAUNCH(prof, z, "hub_dir", NL, 256, 0, k_hub_dir, G, c.d_lp, NL, cnt, QL, c.tgq, c.lg,
                c.tgo, c.tgb, c.hflag, d_e1);
   }
   // ---- rewrites
   if (NR) {
     TRC_LAUNCH(prof, z, "hub_rw_place", ceil_div(QR, 256), 256, 0, k_hub_rw_place, G, d_rp, NR,
-               QR, c.hw_t, c.tpos, c.bkeys, insert ? 1 : 0, c.stage);
+               QR, c.hw_t, c.tpos, c.bkeys, insert ? 1 : 0, c.stage, bfree.get(), F, fresh0);
     TRC_LAUNCH(prof, z, "hub_rw_finish", NR, 256, 0, k_hub_rw_finish, G, d_rp, c.stage, c.freed,
-               ctr);
+               ctr, bfree.get(), F, fresh0);
   }
   // ---- the free list: what the splits did not take, then the freed blocks
   // (free ids are distinct pool blocks, so bfree's pool-sized capacity holds
   // them all)
   TRC_LAUNCH(prof, z, "hub_free_merge", (unsigned)num_sms(), 256, 0, k_hub_free_merge, bfree.get(),
-             F, c.freed, ctr);
+             F, R, c.freed, ctr);
   TRC_CUDA(cudaMemcpyAsync(c.pin + 4, cnt + H_ALLOC, 8 * 5, cudaMemcpyDeviceToHost, z));
   TRC_CUDA(cudaEventRecord(ev_join, z));
   TRC_CUDA(cudaStreamWaitEvent(stream, ev_join, 0));
   c.F = F;
   c.fresh0 = fresh0;
+  c.R = R;
   c.readback = true;
   pool_top = top_bound;  // corrected to the blocks taken in hubs_finish
   hub_last[1] = nloc;
@@ -759,9 +769,10 @@ void Graph::hubs_finish() {
   c.readback = false;
   uint64_t v[5];
   memcpy(v, c.pin + 4, sizeof(v));  // H_ALLOC, H_FREED, H_READ, H_WRITE, H_ABSORB
-  const uint64_t from_free = std::min<uint64_t>(c.F, v[0]);
+  const uint64_t allocated = c.R + v[0];
+  const uint64_t from_free = std::min<uint64_t>(c.F, allocated);
   nfree = c.F - from_free + v[1];
-  pool_top = c.fresh0 + (v[0] - from_free);
+  pool_top = c.fresh0 + (allocated - from_free);
   hub_splits += v[0];
   hub_last[3] += v[0];
   hub_last[4] = v[2];

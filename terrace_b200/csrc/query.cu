@@ -285,7 +285,7 @@ void Graph::stats(trc_stats *o) {
   // inline = sum(min(deg,16)); hub = m - inline - tier2
   uint64_t *t = tmp(scan_tmp_elems(n) + 4);
   uint64_t *off = s_oOff.ensure((uint64_t)n + 1);
-  exclusive_scan(LoadMin{deg.get()}, n, off, t, stream, prof);
+  exclusive_scan(LoadMin{deg.get()}, n, off, t, stream, prof, "stats_scan");
   o->inline_edges = read_u64(off + n);
   o->hub_edges = m - o->inline_edges - o->pma_edges;
 }

@@ -59,7 +59,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   for (auto *b : {&deg, &inl, &c2, &pma, &err, &hub_vtx, &hub_nblk, &hdir, &hpre, &hkey, &hslot,
                   &bcnt, &bmin, &bown, &bfree, &bfreed, &stamp, &s_in_src, &s_in_dst, &s_tu, &s_tdn,
                   &s_tc2, &s_ovl, &s_hw_u, &s_hw_dn, &s_hw_t, &s_c2n, &s_rlist, &s_pma_next,
-                  &s_lgroup, &s_lwarp,
+
                   &lists.S, &lists.M, &lists.Hv, &lists.SM, &lists.M1, &lists.M2,
                   &s_lg, &s_lx, &s_lli, &s_tgq, &s_tgo, &s_tgb, &s_hflag, &s_rwstage})
     b->bind(&budget);
@@ -149,7 +149,7 @@ void Graph::release_scratch() {
   sync();
   for (auto *b : {&s_in_src, &s_in_dst, &s_tu, &s_tdn, &s_tc2, &s_ovl, &s_hw_u, &s_hw_dn, &s_hw_t,
                   &s_c2n, &s_rlist, &s_pma_next, &s_tix, &s_hw_do, &s_wbits, &s_lg, &s_lx, &s_lli,
-                  &s_lgroup, &s_lwarp,
+
                   &s_tgq, &s_tgo, &s_tgb, &s_hflag, &s_rwstage, &bfreed})
     b->reset();
   for (auto *b : {&s_A, &s_B, &s_C, &s_tmp, &s_P, &s_oOff, &s_nOff, &s_wk, &s_wk2, &s_mw, &s_old,
@@ -668,47 +668,25 @@ constexpr uint32_t MR_BITS = 24;
 constexpr uint64_t MR_MASK = (1ull << MR_BITS) - 1;
 
 // Rewrite entries whose old list has at most MG_D elements are merged by
-// MG_G lanes each (k_merge_group), the rest by a warp (k_merge_small); the
-// prep kernel sorts them into two index lists (counts in the batch's
-// counters C_NGROUP / C_NWARP).
+// MG_G lanes each (k_merge_group), the rest by a warp (k_merge_small); both
+// kernels walk the whole rewrite list and take their entries by the old
+// degree in the merge record.
 constexpr uint32_t MG_G = 8;   // lanes per short list
 constexpr uint32_t MG_R = 8;   // elements per lane: MG_G * MG_R covers a short list
 constexpr uint32_t MG_D = MG_G * MG_R;
-constexpr int C_NGROUP = 21, C_NWARP = 22;
 
-__global__ void k_merge_prep(DevView G, MergeArgs a, const uint64_t *nrs, ulonglong2 *rec,
-                             uint32_t *lgroup, uint32_t *lwarp, unsigned long long *cnt) {
+__global__ void k_merge_prep(DevView G, MergeArgs a, const uint64_t *nrs, ulonglong2 *rec) {
   const uint64_t nw = *nrs;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  // (every thread of a warp runs the same number of iterations)
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < nw; base += stride) {
-    const uint64_t w = base + threadIdx.x;
-    bool ok = w < nw, shortl = false;
-    if (ok) {
-      const uint32_t u = a.rs[w];
-      const uint32_t t = a.tix[u];
-      uint64_t b0 = 0, b1 = 0;
-      if (t != NONE32) {
-        b0 = a.tpos[t];
-        b1 = t + 1 < a.nt ? a.tpos[t + 1] : a.kb;
-      }
-      const uint32_t d = G.deg[u];
-      rec[w] = make_ulonglong2((b0 << MR_BITS) | (b1 - b0), (G.pbeg[u] << MR_BITS) | d);
-      shortl = d <= MG_D;
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += stride) {
+    const uint32_t u = a.rs[w];
+    const uint32_t t = a.tix[u];
+    uint64_t b0 = 0, b1 = 0;
+    if (t != NONE32) {
+      b0 = a.tpos[t];
+      b1 = t + 1 < a.nt ? a.tpos[t + 1] : a.kb;
     }
-    const uint32_t mg = __ballot_sync(0xFFFFFFFFu, ok && shortl);
-    const uint32_t mw = __ballot_sync(0xFFFFFFFFu, ok && !shortl);
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t bg = 0, bw = 0;
-    if (lane == 0) {
-      if (mg) bg = (uint32_t)atomicAdd(cnt + C_NGROUP, (unsigned long long)__popc(mg));
-      if (mw) bw = (uint32_t)atomicAdd(cnt + C_NWARP, (unsigned long long)__popc(mw));
-    }
-    bg = __shfl_sync(0xFFFFFFFFu, bg, 0);
-    bw = __shfl_sync(0xFFFFFFFFu, bw, 0);
-    const uint32_t below = (1u << lane) - 1u;
-    if (ok && shortl) lgroup[bg + __popc(mg & below)] = (uint32_t)w;
-    if (ok && !shortl) lwarp[bw + __popc(mw & below)] = (uint32_t)w;
+    rec[w] = make_ulonglong2((b0 << MR_BITS) | (b1 - b0), (G.pbeg[u] << MR_BITS) | G.deg[u]);
   }
 }
 
@@ -804,19 +782,19 @@ __device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a,
 constexpr uint32_t MS_CHUNK = 8;
 
 __global__ void __launch_bounds__(256, 8) k_merge_small(DevView G, MergeArgs a,
-                                                        const uint32_t *lwarp,
-                                                        const unsigned long long *cnt,
+                                                        const uint64_t *nrs,
                                                         const ulonglong2 *rec,
                                                         unsigned long long *work) {
   const uint32_t lane = threadIdx.x & 31;
-  const uint64_t nw = cnt[C_NWARP];
+  const uint64_t nw = *nrs;
   for (;;) {
     uint64_t w0 = 0;
     if (lane == 0) w0 = atomicAdd(work, (unsigned long long)MS_CHUNK);
     w0 = __shfl_sync(0xFFFFFFFFu, w0, 0);
     if (w0 >= nw) break;
     const uint64_t w1 = w0 + MS_CHUNK < nw ? w0 + MS_CHUNK : nw;
-    for (uint64_t w = w0; w < w1; w++) merge_one(G, a, rec, lwarp[w], lane);
+    for (uint64_t w = w0; w < w1; w++)
+      if ((rec[w].y & MR_MASK) > MG_D) merge_one(G, a, rec, w, lane);  // (short: k_merge_group)
   }
 }
 
@@ -827,18 +805,17 @@ __global__ void __launch_bounds__(256, 8) k_merge_small(DevView G, MergeArgs a,
 // element i also writes the keys that land between element i-1 and i) or
 // minus the keys below it (remove), as merge_one does for one chunk.
 __global__ void __launch_bounds__(256, 4) k_merge_group(DevView G, MergeArgs a,
-                                                        const uint32_t *lgroup,
-                                                        const unsigned long long *cnt,
+                                                        const uint64_t *nrs,
                                                         const ulonglong2 *rec) {
   const uint32_t lane = threadIdx.x & 31, g = lane & (MG_G - 1);
   const unsigned mask = ((1u << MG_G) - 1u) << (lane & ~(MG_G - 1));
-  const uint64_t ng = *(cnt + C_NGROUP);
+  const uint64_t nw = *nrs;
   const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / MG_G;
-  for (uint64_t gi = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / MG_G; gi < ng;
-       gi += ngroups) {
-    const uint64_t w = lgroup[gi];
-    const uint32_t u = a.rs[w];
+  for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / MG_G; w < nw;
+       w += ngroups) {
     const ulonglong2 r = rec[w];
+    if ((r.y & MR_MASK) > MG_D) continue;  // (long: k_merge_small; group-uniform)
+    const uint32_t u = a.rs[w];
     const uint64_t b0 = r.x >> MR_BITS;
     const uint32_t nb = (uint32_t)(r.x & MR_MASK);
     const uint32_t d = (uint32_t)(r.y & MR_MASK);
@@ -1187,9 +1164,9 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   if (prof.on && nrs) {  // element counts for the profiler's byte accounting
     uint64_t *oo = s_oOff.ensure(nrs + 1);
     uint64_t *t5 = tmp(scan_tmp_elems(nrs) + 4);
-    exclusive_scan(OldDeg{rs, deg.get()}, nrs, oo, t5, stream, prof);
+    exclusive_scan(OldDeg{rs, deg.get()}, nrs, oo, t5, stream, prof, "prof_count");
     SO = read_u64(oo + nrs);
-    exclusive_scan(NewDeg{rs, deg.get(), tix, tdn}, nrs, oo, t5, stream, prof);
+    exclusive_scan(NewDeg{rs, deg.get(), tix, tdn}, nrs, oo, t5, stream, prof, "prof_count");
     SN = read_u64(oo + nrs);
   }
   {
@@ -1197,14 +1174,11 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
                  nmw ? wstamp.get() : nullptr, epoch, T, dst_pma == pma.get() ? 1 : 0};
     static_assert(HUB_THRESHOLD_MAX <= MR_MASK, "merge record counts");
     ulonglong2 *rec = reinterpret_cast<ulonglong2 *>(s_mrec.ensure(2 * (uint64_t)n));
-    uint32_t *lgroup = s_lgroup.ensure(n), *lwarp = s_lwarp.ensure(n);
-    unsigned long long *ucnt = reinterpret_cast<unsigned long long *>(cnt);
-    TRC_LAUNCH(prof, stream, "upd_merge_prep", pgrid, 256, 0, k_merge_prep, G, ma, nrs_dev, rec,
-               lgroup, lwarp, ucnt);
+    TRC_LAUNCH(prof, stream, "upd_merge_prep", pgrid, 256, 0, k_merge_prep, G, ma, nrs_dev, rec);
     TRC_LAUNCH(prof, stream, "upd_merge_group", (unsigned)num_sms() * 4, 256, 0, k_merge_group, G,
-               ma, lgroup, ucnt, (const ulonglong2 *)rec);
-    TRC_LAUNCH(prof, stream, "upd_merge_small", pgrid, 256, 0, k_merge_small, G, ma, lwarp, ucnt,
-               (const ulonglong2 *)rec, ucnt + C_MWORK);
+               ma, nrs_dev, (const ulonglong2 *)rec);
+    TRC_LAUNCH(prof, stream, "upd_merge_small", pgrid, 256, 0, k_merge_small, G, ma, nrs_dev,
+               (const ulonglong2 *)rec, (unsigned long long *)(cnt + C_MWORK));
   }
   phase("merge_small");
   // ---- tier 3, second phase (the hubs touch vertices disjoint from the
