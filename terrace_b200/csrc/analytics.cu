@@ -88,6 +88,36 @@ __device__ __forceinline__ uint32_t warp_append(bool win, uint32_t *counter) {
   return base + __popc(m & lanemask_lt());
 }
 
+// Per-warp staging of list appends from many chunks: the warp's winners of
+// a chunk are written to 32 shared slots and go out with one atomic when
+// the slots fill (and at the end, flush), instead of one atomic per chunk
+// on the list's counter, which every warp of the grid hits.  Calls are
+// warp-uniform.
+struct WarpStage {
+  uint32_t *slot;  // 32 shared words of this warp
+  uint32_t cnt;
+  __device__ void flush(uint32_t *list, uint32_t *counter, uint32_t lane) {
+    __syncwarp();
+    if (cnt) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(counter, cnt);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (lane < cnt) list[base + lane] = slot[lane];
+    }
+    __syncwarp();
+    cnt = 0;
+  }
+  __device__ void add(bool win, uint32_t v, uint32_t *list, uint32_t *counter, uint32_t lane) {
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, win);
+    if (!m) return;
+    const uint32_t k = __popc(m);
+    if (cnt + k > 32) flush(list, counter, lane);
+    if (win) slot[cnt + __popc(m & lanemask_lt())] = v;
+    cnt += k;
+    if (cnt == 32) flush(list, counter, lane);
+  }
+};
+
 // Appends each thread's `cnt` items to a global list with ONE atomic per
 // CTA (a per-level frontier counter is one address: a warp-level atomic per
 // warp serialises there).  Every thread of the CTA must call it; returns the
@@ -532,7 +562,7 @@ __device__ __forceinline__ bool bit_test(const uint32_t *b, uint32_t v) {
 // neighbours by CAS on the parent (any frontier parent, as BFS_F::
 // updateAtomic).
 __device__ __forceinline__ void bfs_push_chunk(const NbrList &L, uint32_t u, uint32_t j0,
-                                               const BFSState &s, uint32_t lane) {
+                                               const BFSState &s, uint32_t lane, WarpStage &st) {
   const uint32_t j = j0 + lane;
   bool win = false;
   uint32_t v = 0;
@@ -543,13 +573,12 @@ __device__ __forceinline__ void bfs_push_chunk(const NbrList &L, uint32_t u, uin
       win = true;
     }
   }
-  uint32_t pos = warp_append(win, s.next_cnt);
-  if (win) s.next[pos] = v;
+  st.add(win, v, s.next, s.next_cnt, lane);
 }
 
 // The same for a piece of a hub's list (hub_chunk).
 __device__ __forceinline__ void bfs_push_span(const uint32_t *p, uint32_t len, uint32_t u,
-                                              const BFSState &s, uint32_t lane) {
+                                              const BFSState &s, uint32_t lane, WarpStage &st) {
   bool win = false;
   uint32_t v = 0;
   if (lane < len) {
@@ -559,8 +588,7 @@ __device__ __forceinline__ void bfs_push_span(const uint32_t *p, uint32_t len, u
       win = true;
     }
   }
-  uint32_t pos = warp_append(win, s.next_cnt);
-  if (win) s.next[pos] = v;
+  st.add(win, v, s.next, s.next_cnt, lane);
 }
 
 // Warp per frontier vertex; hubs are listed for k_bfs_push_hubs.
@@ -573,8 +601,11 @@ __global__ void k_bfs_push(DevView G, const uint32_t *F, uint32_t nf, BFSState s
     if (lane == 0) s.seg[atomicAdd(s.seg_cnt, 1u)] = u;
     return;
   }
+  __shared__ uint32_t stg[AT / 32][32];
+  WarpStage st{stg[(threadIdx.x >> 5)], 0};
   NbrList L = nbr_list(G, u);
-  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) bfs_push_chunk(L, u, j0, s, lane);
+  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) bfs_push_chunk(L, u, j0, s, lane, st);
+  st.flush(s.next, s.next_cnt, lane);
 }
 
 // The frontier's hubs (list and device count from a compaction).  The first
@@ -591,6 +622,8 @@ __global__ void k_bfs_push_hubs(DevView G, BFSState s) {
   const uint32_t *FH = s.seg;
   const uint64_t nh = *s.seg_cnt;
   const uint64_t nwide = nh < PUSH_WIDE ? nh : PUSH_WIDE;
+  __shared__ uint32_t stg[AT / 32][32];
+  WarpStage st{stg[wib], 0};
   const uint32_t *p;
   uint32_t len;
   for (uint64_t i = 0; i < nwide; i++) {
@@ -599,7 +632,7 @@ __global__ void k_bfs_push_hubs(DevView G, BFSState s) {
     const uint64_t nch = hub_chunks(L);
     for (uint64_t c = gw; c < nch; c += nwarps) {
       hub_chunk(L, (uint32_t)c, p, len);
-      if (len) bfs_push_span(p, len, u, s, lane);  // (len is warp-uniform)
+      if (len) bfs_push_span(p, len, u, s, lane, st);  // (len is warp-uniform)
     }
   }
   for (uint64_t i = nwide + blockIdx.x; i < nh; i += gridDim.x) {
@@ -608,9 +641,10 @@ __global__ void k_bfs_push_hubs(DevView G, BFSState s) {
     const uint32_t nch = hub_chunks(L);
     for (uint32_t c = wib; c < nch; c += AT / 32) {
       hub_chunk(L, c, p, len);
-      if (len) bfs_push_span(p, len, u, s, lane);
+      if (len) bfs_push_span(p, len, u, s, lane, st);
     }
   }
+  st.flush(s.next, s.next_cnt, lane);
 }
 
 
@@ -1051,7 +1085,7 @@ struct BCFwd {
 // unvisited neighbours for level d+1 and add su to the path count of every
 // neighbour on level d+1 (BC_F::updateAtomic's CAS-add, include/BC.h:44-58).
 __device__ __forceinline__ void bc_push_chunk(const NbrList &L, double su, uint32_t j0,
-                                              const BCFwd &s, uint32_t lane) {
+                                              const BCFwd &s, uint32_t lane, WarpStage &st) {
   const uint32_t j = j0 + lane;
   bool win = false;
   uint32_t v = 0;
@@ -1065,13 +1099,12 @@ __device__ __forceinline__ void bc_push_chunk(const NbrList &L, double su, uint3
     }
     if (lvv == s.d + 1) atomicAdd(&s.sigma[v], su);
   }
-  uint32_t pos = warp_append(win, s.next_cnt);
-  if (win) s.order[pos] = v;
+  st.add(win, v, s.order, s.next_cnt, lane);
 }
 
 // The same for a piece of a hub's list (hub_chunk).
 __device__ __forceinline__ void bc_push_span(const uint32_t *p, uint32_t len, double su,
-                                             const BCFwd &s, uint32_t lane) {
+                                             const BCFwd &s, uint32_t lane, WarpStage &st) {
   bool win = false;
   uint32_t v = 0;
   if (lane < len) {
@@ -1084,8 +1117,7 @@ __device__ __forceinline__ void bc_push_span(const uint32_t *p, uint32_t len, do
     }
     if (lvv == s.d + 1) atomicAdd(&s.sigma[v], su);
   }
-  uint32_t pos = warp_append(win, s.next_cnt);
-  if (win) s.order[pos] = v;
+  st.add(win, v, s.order, s.next_cnt, lane);
 }
 
 // Warp per frontier vertex; hubs are listed for k_bc_push_hubs.
@@ -1098,9 +1130,12 @@ __global__ void k_bc_push(DevView G, const uint32_t *F, uint32_t nf, BCFwd s) {
     if (lane == 0) s.hubs[atomicAdd(s.hub_cnt, 1u)] = u;
     return;
   }
+  __shared__ uint32_t stg[AT / 32][32];
+  WarpStage st{stg[(threadIdx.x >> 5)], 0};
   double su = s.sigma[u];
   NbrList L = nbr_list(G, u);
-  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) bc_push_chunk(L, su, j0, s, lane);
+  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) bc_push_chunk(L, su, j0, s, lane, st);
+  st.flush(s.order, s.next_cnt, lane);
 }
 
 // The frontier's hubs: the first PUSH_WIDE spread over the grid, the rest a
@@ -1111,6 +1146,8 @@ __global__ void k_bc_push_hubs(DevView G, BCFwd s) {
   const uint64_t nwarps = ((uint64_t)gridDim.x * AT) >> 5;
   const uint64_t nh = *s.hub_cnt;
   const uint64_t nwide = nh < PUSH_WIDE ? nh : PUSH_WIDE;
+  __shared__ uint32_t stg[AT / 32][32];
+  WarpStage st{stg[wib], 0};
   const uint32_t *p;
   uint32_t len;
   for (uint64_t i = 0; i < nwide; i++) {
@@ -1120,7 +1157,7 @@ __global__ void k_bc_push_hubs(DevView G, BCFwd s) {
     const uint64_t nch = hub_chunks(L);
     for (uint64_t c = gw; c < nch; c += nwarps) {
       hub_chunk(L, (uint32_t)c, p, len);
-      if (len) bc_push_span(p, len, su, s, lane);  // (len is warp-uniform)
+      if (len) bc_push_span(p, len, su, s, lane, st);  // (len is warp-uniform)
     }
   }
   for (uint64_t i = nwide + blockIdx.x; i < nh; i += gridDim.x) {
@@ -1130,9 +1167,10 @@ __global__ void k_bc_push_hubs(DevView G, BCFwd s) {
     const uint32_t nch = hub_chunks(L);
     for (uint32_t c = wib; c < nch; c += AT / 32) {
       hub_chunk(L, c, p, len);
-      if (len) bc_push_span(p, len, su, s, lane);
+      if (len) bc_push_span(p, len, su, s, lane, st);
     }
   }
+  st.flush(s.order, s.next_cnt, lane);
 }
 
 // Pull for an unvisited vertex: sigma = sum of sigma over neighbours on level d.
@@ -1227,6 +1265,94 @@ struct BCBackOp {
     if (ok) dep_out[u] = sum + inv[u];  // every vertex of the level, isolated source included
   }
 };
+
+// Backward step over the degree classes instead of the level's list: the
+// class lists are scanned whole and every vertex not on level L skipped (one
+// lv load each), so each vertex of the level is summed by a lane group sized
+// to its degree (four lanes below 17, a group of GS lanes up to the
+// lane-group cut, a warp above, a CTA for a hub), every load of a step issued
+// before any is used, as the PageRank pull does.
+struct BCBackClassOp {
+  const uint32_t *lv;
+  uint32_t L;
+  const double *inv;
+  const double *dep;
+  double *dep_out;
+  __device__ bool skip(uint32_t u) const { return lv[u] != L; }
+  __device__ double gather(uint32_t x) const { return __ldg(dep + x); }
+  __device__ void store(uint32_t u, double sum) const { dep_out[u] = sum + inv[u]; }
+};
+
+template <class Op>
+__global__ void __launch_bounds__(AT) k_cls_S(DevView G, const uint32_t *S, uint64_t nS, Op op) {
+  const uint64_t gt = (uint64_t)blockIdx.x * AT + threadIdx.x;
+  const uint64_t vi = gt >> 2;
+  const uint32_t q = gt & 3;
+  const uint32_t u = vi < nS ? S[vi] : 0u;
+  const bool act = vi < nS && !op.skip(u);
+  double sum = 0.0;
+  if (act) {
+    const uint32_t d = G.deg[u], e = q * 4;
+    if (e < d) {
+      const uint4 v = __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE) + q);
+      sum += op.gather(v.x);
+      if (e + 1 < d) sum += op.gather(v.y);
+      if (e + 2 < d) sum += op.gather(v.z);
+      if (e + 3 < d) sum += op.gather(v.w);
+    }
+  }
+  sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 1);
+  sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 2);
+  if (act && q == 0) op.store(u, sum);
+}
+
+template <int GS, class Op>
+__global__ void __launch_bounds__(AT) k_cls_group(DevView G, const uint32_t *V, uint64_t nV, Op op) {
+  constexpr int U = 8;
+  const uint64_t gt = (uint64_t)blockIdx.x * AT + threadIdx.x;
+  const uint64_t vi = gt / GS;
+  const uint32_t q = gt % GS;
+  const uint32_t u = vi < nV ? V[vi] : 0u;
+  const bool act = vi < nV && !op.skip(u);
+  double sum = 0.0;
+  if (act) {
+    const uint32_t d = G.deg[u];
+    const uint32_t *row = G.inl + (uint64_t)u * K_INLINE;
+    const uint32_t *seg = G.pma + G.pbeg[u] - K_INLINE;  // index by rank
+    for (uint32_t j0 = q; j0 < d; j0 += GS * U) {
+      uint32_t x[U];
+#pragma unroll
+      for (int k = 0; k < U; k++) {
+        const uint32_t j = j0 + k * GS;
+        x[k] = j < d ? (j < K_INLINE ? __ldcs(row + j) : __ldcs(seg + j)) : 0u;
+      }
+#pragma unroll
+      for (int k = 0; k < U; k++)
+        if (j0 + k * GS < d) sum += op.gather(x[k]);
+    }
+  }
+#pragma unroll
+  for (int o = GS / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+  if (act && q == 0) op.store(u, sum);
+}
+
+template <class Op>
+__global__ void __launch_bounds__(AT) k_cls_H(DevView G, const uint32_t *Hv, Op op) {
+  __shared__ double sh[AT / 32];
+  const uint32_t u = Hv[blockIdx.x];
+  if (op.skip(u)) return;  // CTA-uniform
+  NbrList L = nbr_list(G, u);
+  double sum = 0.0;
+  if (threadIdx.x < L.ni) sum = op.gather(L.inl[threadIdx.x]);
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t e = warp; e < L.nb; e += AT / 32) {
+    const uint32_t *blk = L.seg + (uint64_t)L.dir[e] * HUB_BLOCK;
+    const uint32_t c = (e + 1 < L.nb ? L.pre[e + 1] : L.rest) - L.pre[e];
+    for (uint32_t k = lane; k < c; k += 32) sum += op.gather(blk[k]);
+  }
+  sum = block_sum(sum, sh);
+  if (threadIdx.x == 0) op.store(u, sum);
+}
 
 // After a step that wrote to a side array: copy the values of the level's
 // vertices (order[0 .. *cnt or cnt)) into the main array.
@@ -1330,8 +1456,20 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
   TRC_LAUNCH(prof, stream, "bc_inv", ceil_div(n, AT), AT, 0, k_bc_inv, sigma, inv, n);
   for (int64_t L = (int64_t)d - 1; L >= 0; L--) {
     uint64_t a = loff[L], b = loff[L + 1];
-    TRC_LAUNCH(prof, stream, "bc_back_flat", ceil_div(b - a, AT), AT, 0, k_flat<BCBackOp>, G,
-               order + a, b - a, BCBackOp{inv, dep, side});
+    if (b - a < lists.nSM / 64) {  // a small level: its own list, load-balanced
+      TRC_LAUNCH(prof, stream, "bc_back_flat", ceil_div(b - a, AT), AT, 0, k_flat<BCBackOp>, G,
+                 order + a, b - a, BCBackOp{inv, dep, side});
+    } else {  // a large one: the degree classes
+      const BCBackClassOp op{lv, (uint32_t)L, inv, dep, side};
+      TRC_LAUNCH(prof, stream, "bc_back_S", ceil_div(lists.nS * 4, AT), AT, 0, k_cls_S<BCBackClassOp>,
+                 G, lists.S.get(), lists.nS, op);
+      TRC_LAUNCH(prof, stream, "bc_back_M8", ceil_div(lists.nM1 * 8, AT), AT, 0,
+                 (k_cls_group<8, BCBackClassOp>), G, lists.M1.get(), lists.nM1, op);
+      TRC_LAUNCH(prof, stream, "bc_back_M32", ceil_div(lists.nM2 * 32, AT), AT, 0,
+                 (k_cls_group<32, BCBackClassOp>), G, lists.M2.get(), lists.nM2, op);
+      TRC_LAUNCH(prof, stream, "bc_back_H", lists.nH, AT, 0, k_cls_H<BCBackClassOp>, G,
+                 lists.Hv.get(), op);
+    }
     TRC_LAUNCH(prof, stream, "bc_commit", std::min<uint64_t>(ceil_div(b - a, AT), num_sms() * 4), AT,
                0, k_bc_commit, order + a, (const uint32_t *)nullptr, b - a, side, dep);
   }

@@ -455,3 +455,45 @@ def test_bc_and_bfs_from_isolated_and_leaf_sources(T):
         assert np.array_equal(lv, O.bfs_levels(off, tgt, src))
         assert O.bfs_check_parents(off, tgt, src, lv, par) == 0
     g.close()
+
+
+def test_blocked_tier_random_batches(T):
+    """Three hubs of 12,000-40,000 neighbours (block-local path) under forty
+    random insert and delete batches of 1..5,000 edges each, some spread over
+    the whole list and some packed into one key range, compared with the
+    oracle's set model after every batch."""
+    rng = np.random.default_rng(11)
+    n = 1 << 17
+    hubs = np.array([3, 70000, 131000], np.uint32)
+    s, d = T.rmat_generate(n, 9, .5, .1, .1, 2 * n)
+    keep = ~np.isin(s, hubs) & ~np.isin(d, hubs)
+    s, d = s[keep], d[keep]
+    hs = np.concatenate([np.full(k, h, np.uint32) for h, k in zip(hubs, (12000, 25000, 40000))])
+    hd = np.concatenate([rng.choice(n, k, replace=False).astype(np.uint32)
+                         for k in (12000, 25000, 40000)])
+    g = T.Graph(n)
+    g.add_edge_batch(np.concatenate([s, hs]), np.concatenate([d, hd]), **SYM)
+    cur = O.make_keys(np.concatenate([s, hs]), np.concatenate([d, hd]), True, True)
+    local = 0
+    for step in range(40):
+        h = hubs[rng.integers(0, 3)]
+        k = int(rng.integers(1, 5000))
+        if rng.random() < 0.5:
+            dst = rng.integers(0, n, k).astype(np.uint32)
+        else:
+            lo = int(rng.integers(0, n - 4000))
+            dst = rng.integers(lo, lo + 4000, k).astype(np.uint32)
+        src = np.full(k, h, np.uint32)
+        bk = O.make_keys(src, dst, True, True)
+        if step % 2:
+            g.remove_edge_batch(src, dst, **SYM)
+            cur = O.key_difference(cur, bk)
+        else:
+            g.add_edge_batch(src, dst, **SYM)
+            cur = O.key_union(cur, bk)
+        local += g.stats()["last_hub_local"]
+        off, tgt = O.csr_from_keys(n, cur)
+        assert_same_csr(g, off, tgt)
+    assert local > 10
+    check_algorithms(g, off, tgt)
+    g.close()
