@@ -680,7 +680,7 @@ __global__ void k_level_bits(const uint32_t *lv, uint32_t n, uint32_t d, uint32_
 // is used: list entries, then degree and level, then the row quarters, then
 // the 4 * BP_V frontier-bitmap words.  The first frontier neighbour in
 // sorted order wins (lowest lane of the quad with a hit, then its lowest
-// element).
+// element).  S == null: the entries are the vertex ids 0 .. nS-1 themselves.
 constexpr uint32_t BP_V = 4;
 
 __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S, uint64_t nS,
@@ -692,12 +692,14 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
 #pragma unroll
   for (uint32_t i = 0; i < BP_V; i++) {
     const uint64_t vi = wbase + i * 8 + qw;
-    u[i] = vi < nS ? S[vi] : 0u;
+    u[i] = vi < nS ? (S ? S[vi] : (uint32_t)vi) : 0u;
     act[i] = vi < nS;
   }
 #pragma unroll
   for (uint32_t i = 0; i < BP_V; i++) {
     d[i] = act[i] ? G.deg[u[i]] : 0u;
+    // (no list: every vertex id, hubs left to their own pass)
+    if (!S && act[i] && G.hub_of[u[i]] >= 0) d[i] = 0;
     act[i] = act[i] && s.lv[u[i]] == TRC_UNREACHED && q * 4 < d[i];
   }
   uint4 v[BP_V];
@@ -865,8 +867,10 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
   cbuf[0].bind(&budget);
   cbuf[1].bind(&budget);
   segb.bind(&budget);
-  const uint32_t *cand = lists.SM.get();
-  uint64_t ncand = lists.nSM;
+  // (the first dense step reads every vertex id in order, no list: its
+  // candidates are all non-hub vertices, and the loads stay contiguous)
+  const uint32_t *cand = nullptr;
+  uint64_t ncand = n;
   int cnext = 0;
   uint32_t *sg = segb.ensure(n);
   const unsigned pgrid = (unsigned)num_sms() * 8;
