@@ -373,6 +373,97 @@ __global__ void __launch_bounds__(256) k_hub_dir(DevView G, const uint64_t *lp, 
 
 // ---------------------------------------------------------------- rewrite
 
+// A CTA per rewritten hub whose old list fits in shared memory (at most
+// HB_RW_SMEM elements): the old list is staged (inline row, then the blocks
+// or the PMA segment), every old element and key is written at its new rank
+// (ranks below 16 straight to the inline row, whose old contents are
+// staged), then the old blocks go to the freed list, the new blocks get
+// their counts, first keys and owner, and the directory and the hub table
+// entry are written.
+constexpr uint32_t HB_RW_SMEM = 48 * 1024;
+
+__global__ void __launch_bounds__(256) k_hub_rw_cta(DevView G, const uint64_t *rp,
+                                                    const uint32_t *hw_t, const uint64_t *tpos,
+                                                    const uint64_t *bkeys, int insert,
+                                                    const uint32_t *bfree, uint64_t F,
+                                                    uint64_t fresh0, uint32_t *bfreed,
+                                                    unsigned long long *ctr) {
+  extern __shared__ uint32_t A[];
+  __shared__ unsigned long long fbase;
+  const uint64_t *row = rp + (uint64_t)blockIdx.x * RP_W;
+  const uint32_t h = (uint32_t)row[RP_H], u = (uint32_t)row[RP_U];
+  const uint32_t dold = (uint32_t)row[RP_DO], dn = (uint32_t)row[RP_DN];
+  const uint64_t blk0 = row[RP_BLK0], e1 = row[RP_E1];
+  const uint32_t per = (uint32_t)row[RP_PER], nbw = (uint32_t)row[RP_NB];
+  const uint32_t k = insert ? dn - dold : dold - dn;
+  const uint64_t *K = hub_keys(hw_t, tpos, bkeys, row[RP_IHW]);
+  const NbrList L = nbr_list(G, u);  // the old list (tables unchanged until the end)
+  const bool was_hub = G.hub_of[u] >= 0;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  for (uint32_t i = threadIdx.x; i < L.ni; i += blockDim.x) A[i] = L.inl[i];
+  if (L.nb) {
+    for (uint32_t e = warp; e < L.nb; e += nwarp) {
+      const uint32_t *blk = L.seg + (uint64_t)L.dir[e] * HUB_BLOCK;
+      const uint32_t c = (e + 1 < L.nb ? L.pre[e + 1] : L.rest) - L.pre[e];
+      uint32_t *dst = A + L.ni + L.pre[e];
+      for (uint32_t j = lane; j < c; j += 32) dst[j] = blk[j];
+    }
+  } else {
+    for (uint32_t j = threadIdx.x; j < L.rest; j += blockDim.x) A[L.ni + j] = L.seg[j];
+  }
+  __syncthreads();
+  uint32_t *row_inl = G.inl + (uint64_t)u * K_INLINE;
+  auto put = [&](uint32_t r, uint32_t x) {
+    if (r < K_INLINE) {
+      row_inl[r] = x;
+    } else {
+      const uint32_t rr = r - K_INLINE;
+      const uint32_t b = alloc_id(blk0 + rr / per, bfree, F, fresh0);
+      G.hslot[(uint64_t)b * HUB_BLOCK + rr % per] = x;
+    }
+  };
+  if (insert) {
+    for (uint32_t i = threadIdx.x; i < dold; i += blockDim.x) put(i + lb_u64lo(K, k, A[i]), A[i]);
+    for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) {
+      const uint32_t x = (uint32_t)K[j];
+      put(j + lb_u32(A, dold, x), x);
+    }
+  } else {
+    for (uint32_t i = threadIdx.x; i < dold; i += blockDim.x) {
+      const uint32_t x = A[i];
+      const uint32_t c = lb_u64lo(K, k, x);
+      if (!(c < k && (uint32_t)K[c] == x)) put(i - c, x);
+    }
+  }
+  if (threadIdx.x == 0 && was_hub && L.nb)
+    fbase = atomicAdd(ctr + H_FREED, (unsigned long long)L.nb);
+  __syncthreads();
+  if (was_hub)
+    for (uint32_t i = threadIdx.x; i < L.nb; i += blockDim.x) bfreed[fbase + i] = L.dir[i];
+  const uint32_t rest = dn > K_INLINE ? dn - K_INLINE : 0;
+  for (uint32_t i = threadIdx.x; i < nbw; i += blockDim.x) {
+    const uint32_t b = alloc_id(blk0 + i, bfree, F, fresh0);
+    const uint32_t c = rest - i * per < per ? rest - i * per : per;
+    const uint32_t first = G.hslot[(uint64_t)b * HUB_BLOCK];
+    G.bcnt[b] = c;
+    G.bmin[b] = first;
+    G.bown[b] = u;
+    G.hdir[e1 + i] = b;
+    G.hpre[e1 + i] = i * per;
+    G.hkey[e1 + i] = first;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    G.hub_vtx[h] = u;
+    G.hub_dir0[h] = e1;
+    G.hub_nblk[h] = nbw;
+    G.hub_of[u] = (int32_t)h;
+    G.deg[u] = dn;
+    atomicAdd(ctr + H_READ, (unsigned long long)dold);
+    atomicAdd(ctr + H_WRITE, (unsigned long long)dn);
+  }
+}
+
 // One thread per item of a rewritten hub (old elements, then insert keys):
 // its new rank, then its slot -- the inline staging row for ranks < 16, else
 // the hub's fresh blocks, uniformly filled with `per` elements.  The old list
@@ -430,12 +521,13 @@ __global__ void k_hub_rw_finish(DevView G, const uint64_t *rp, const uint32_t *s
   const uint32_t rest = dn - ni;
   for (uint32_t i = threadIdx.x; i < ni; i += blockDim.x)
     G.inl[(uint64_t)u * K_INLINE + i] = stage[r * K_INLINE + i];
-  if (G.hub_of[u] >= 0) {  // an existing hub: its old blocks are free now
-    const uint64_t e0 = G.hub_dir0[h];
-    const uint32_t nb = G.hub_nblk[h];
-    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x)
-      bfreed[atomicAdd(ctr + H_FREED, 1ull)] = G.hdir[e0 + i];
-  }
+  __shared__ unsigned long long fbase;
+  const bool was_hub = G.hub_of[u] >= 0;
+  const uint64_t e0 = was_hub ? G.hub_dir0[h] : 0;
+  const uint32_t nb = was_hub ? G.hub_nblk[h] : 0;
+  if (threadIdx.x == 0 && nb) fbase = atomicAdd(ctr + H_FREED, (unsigned long long)nb);
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) bfreed[fbase + i] = G.hdir[e0 + i];
   for (uint32_t i = threadIdx.x; i < nbw; i += blockDim.x) {
     const uint32_t b = alloc_id(blk0 + i, bfree, F, fresh0);
     const uint32_t c = rest - i * per < per ? rest - i * per : per;
@@ -473,6 +565,10 @@ __global__ void k_hub_free_merge(uint32_t *bfree, uint64_t F, uint64_t R, const 
 // ---------------------------------------------------------------- host side
 
 void Graph::hub_init() {
+  // the staged rewrite may use up to 192 KB of dynamic shared memory; the
+  // limit applies per device (a graph is created with its device current)
+  TRC_CUDA(cudaFuncSetAttribute(k_hub_rw_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(HB_RW_SMEM * sizeof(uint32_t))));
   grow_hub_tables(64);
   grow_pool(64);
   grow_dir_pool(256);
@@ -679,7 +775,14 @@ void Graph::apply_hubs_finish() {
   const uint64_t F = nfree;
   const uint64_t fresh0 = pool_top;
   uint64_t R = 0;
+  // rows: hubs whose old list fits in shared memory (a CTA each, staged)
+  // first, then the others (a thread per element)
   std::vector<uint64_t> rp(NR * RP_W, 0);
+  std::stable_partition(rw.begin(), rw.end(),
+                        [&](const HubItem &x) { return hdo[x.i] <= HB_RW_SMEM; });
+  uint64_t NRC = 0;
+  uint32_t smem_max = 1;
+  while (NRC < NR && hdo[rw[NRC].i] <= HB_RW_SMEM) smem_max = std::max(smem_max, hdo[rw[NRC++].i]);
   uint64_t QR = 0, written_blocks = 0;
   for (uint64_t r = 0; r < NR; r++) {
     const uint64_t i = rw[r].i;
@@ -697,7 +800,7 @@ void Graph::apply_hubs_finish() {
     row[RP_PER] = per;
     row[RP_NB] = nb;
     row[RP_Q0] = QR;
-    QR += insert ? hdn[i] : hdo[i];  // old elements (+ keys on insert)
+    if (r >= NRC) QR += insert ? hdn[i] : hdo[i];  // old elements (+ keys on insert)
     R += nb;
     written_blocks += nb;
     h_hub_nblk[h] = nb;
@@ -736,11 +839,16 @@ void Graph::apply_hubs_finish() {
                c.tgo, c.tgb, c.hflag, d_e1);
   }
   // ---- rewrites
-  if (NR) {
-    TRC_LAUNCH(prof, z, "hub_rw_place", ceil_div(QR, 256), 256, 0, k_hub_rw_place, G, d_rp, NR,
-               QR, c.hw_t, c.tpos, c.bkeys, insert ? 1 : 0, c.stage, bfree.get(), F, fresh0);
-    TRC_LAUNCH(prof, z, "hub_rw_finish", NR, 256, 0, k_hub_rw_finish, G, d_rp, c.stage, c.freed,
-               ctr, bfree.get(), F, fresh0);
+  if (NRC)
+    TRC_LAUNCH(prof, z, "hub_rw_cta", NRC, 256, (size_t)smem_max * 4, k_hub_rw_cta, G, d_rp,
+               c.hw_t, c.tpos, c.bkeys, insert ? 1 : 0, bfree.get(), F, fresh0, c.freed, ctr);
+  if (NR > NRC) {
+    const uint64_t *d_rpe = d_rp + NRC * RP_W;
+    TRC_LAUNCH(prof, z, "hub_rw_place", ceil_div(QR, 256), 256, 0, k_hub_rw_place, G, d_rpe,
+               NR - NRC, QR, c.hw_t, c.tpos, c.bkeys, insert ? 1 : 0, c.stage, bfree.get(), F,
+               fresh0);
+    TRC_LAUNCH(prof, z, "hub_rw_finish", NR - NRC, 256, 0, k_hub_rw_finish, G, d_rpe, c.stage,
+               c.freed, ctr, bfree.get(), F, fresh0);
   }
   // ---- the free list: what the splits did not take, then the freed blocks
   // (free ids are distinct pool blocks, so bfree's pool-sized capacity holds
