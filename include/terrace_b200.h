@@ -109,6 +109,19 @@ trc_status trc_release_scratch(trc_graph *g);
 trc_status trc_debug_sort_wait(trc_graph *g, uint32_t spin_limit,
                                int withhold_first_tile);
 
+/* Test hook for the choice of batch sort.  Batches of 4096 keys or more
+ * (after symmetrizing) sort with a bucket sort (bucket by the source's high
+ * bits, each bucket sorted whole in registers or shared memory); a batch in
+ * which one bucket holds more than 16384 keys is sorted again by the LSD
+ * radix sort before anything is modified (trc_stats.sort_retries counts
+ * these); smaller batches, and all batches while the wait hook above is
+ * set, use the radix sort.  mode 0 restores that choice, 1 forces the radix
+ * sort, 2 tries the bucket sort for every batch.  Results are identical.
+ * No reference counterpart (the reference's driver sorts each batch with
+ * two stable integer sorts, by destination then by source, before the
+ * update call: src/graph_bm.cc:354-355). */
+trc_status trc_debug_sort_mode(trc_graph *g, int mode);
+
 /* ---- updates: replaces Graph::add_edge_batch (include/graph.h:430-502) and
  *      the per-edge Graph::remove_edge loop of src/graph_bm.cc:375-380 (the
  *      reference declares no remove_edge_batch, include/graph.h:143-150).
@@ -383,6 +396,8 @@ typedef struct {
   uint64_t hub_rewrites;            /* whole-hub rewrites */
   uint64_t hub_blocks_free;         /* pool blocks on the free list */
   uint64_t hub_absorbs;             /* under-full blocks merged with their successor */
+  uint64_t sort_retries;            /* batches re-sorted by the radix sort (a source
+                                       with more than 16384 keys in the batch) */
 } trc_stats;
 trc_status trc_get_stats(trc_graph *g, trc_stats *out);
 /* Checks every structural invariant on the device (sorted, duplicate-free

@@ -108,7 +108,7 @@ class trc_stats(C.Structure):
                 ("hub_splits", C.c_uint64),
                 ("hub_rewrites", C.c_uint64),
                 ("hub_blocks_free", C.c_uint64),
-                ("hub_absorbs", C.c_uint64)]
+                ("hub_absorbs", C.c_uint64), ("sort_retries", C.c_uint64)]
 
 
 # (name, restype, argtypes) for every symbol the header declares
@@ -123,6 +123,7 @@ SIGNATURES = [
     ("trc_graph_set_stream", _int, [_vp, _vp]),
     ("trc_release_scratch", _int, [_vp]),
     ("trc_debug_sort_wait", _int, [_vp, _u32, _int]),
+    ("trc_debug_sort_mode", _int, [_vp, _int]),
     ("trc_add_edge_batch", _int, [_vp, _vp, _vp, _u64, _u32, C.POINTER(_u64)]),
     ("trc_remove_edge_batch", _int, [_vp, _vp, _vp, _u64, _u32, C.POINTER(_u64)]),
     ("trc_is_edge", _int, [_vp, _vp, _vp, _u64, _vp, _u32]),

@@ -185,6 +185,13 @@ trc_status trc_debug_sort_wait(trc_graph *g, uint32_t spin_limit, int withhold_f
   });
 }
 
+trc_status trc_debug_sort_mode(trc_graph *g, int mode) {
+  return guard([&] {
+    if (mode < 0 || mode > 2) trc::throw_error(TRC_ERR_INVALID, "sort mode must be 0, 1 or 2");
+    G(g).sort_mode = mode;
+  });
+}
+
 trc_status trc_add_edge_batch(trc_graph *g, const uint32_t *src, const uint32_t *dst, uint64_t k,
                               uint32_t flags, uint64_t *applied) {
   return guard([&] {

@@ -211,6 +211,245 @@ uint64_t *radix_sort_u64_shifts(uint64_t *keys, uint64_t *alt, uint64_t n, const
 }
 
 // ---------------------------------------------------------------------------
+// Bucket sort (see prims.cuh).
+
+namespace {
+
+constexpr uint64_t BK_INVALID = ~0ull;
+constexpr uint32_t BK_MID = 1024;  // buckets of 33..BK_MID keys: a warp in shared memory
+
+struct BucketArgs {
+  uint32_t nb;     // valid buckets; bucket nb holds the invalid keys
+  uint32_t shift;  // bucket = source >> shift
+  __device__ uint32_t of(uint64_t x) const {
+    return x == BK_INVALID ? nb : (uint32_t)(x >> (32 + shift));
+  }
+};
+
+__global__ void k_bucket_hist(const uint64_t *keys, uint64_t k, BucketArgs ba, uint32_t *cnt) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= k) return;
+  atomicAdd(cnt + ba.of(keys[i]), 1u);
+}
+
+struct LoadCnt32 {
+  const uint32_t *c;
+  __device__ uint64_t operator()(uint64_t i) const { return c[i]; }
+};
+
+__global__ void k_bucket_scatter(const uint64_t *keys, uint64_t k, BucketArgs ba,
+                                 const uint64_t *off, uint32_t *fill, uint64_t *out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= k) return;
+  const uint64_t x = keys[i];
+  const uint32_t b = ba.of(x);
+  out[off[b] + atomicAdd(fill + b, 1u)] = x;
+}
+
+// Ascending bitonic network over the 32 lanes of a warp, one value per lane.
+__device__ __forceinline__ uint64_t warp_bitonic32(uint64_t v, uint32_t lane) {
+#pragma unroll
+  for (uint32_t size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+      const uint64_t o = __shfl_xor_sync(0xFFFFFFFFu, v, stride);
+      const bool keep_min = ((lane & size) == 0) == ((lane & stride) == 0);
+      v = keep_min ? (o < v ? o : v) : (o > v ? o : v);
+    }
+  }
+  return v;
+}
+
+// Ascending bitonic sort of P (a power of two) values in shared memory by
+// `nt` threads with index t; `bar` synchronises them.
+template <typename Bar>
+__device__ __forceinline__ void smem_bitonic(uint64_t *v, uint32_t P, uint32_t t, uint32_t nt,
+                                             Bar bar) {
+  for (uint32_t size = 2; size <= P; size <<= 1) {
+    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+      for (uint32_t c = t; c < P / 2; c += nt) {
+        const uint32_t lo = 2 * c - (c & (stride - 1));
+        const uint32_t hi = lo + stride;
+        const uint64_t x = v[lo], y = v[hi];
+        if ((x > y) == ((lo & size) == 0)) {
+          v[lo] = y;
+          v[hi] = x;
+        }
+      }
+      bar();
+    }
+  }
+}
+
+// Ascending bitonic network over N registers of one thread (all indices
+// resolve at compile time, so the values stay in registers).
+template <int N>
+__device__ __forceinline__ void thread_bucket_sort(uint64_t *keys, uint64_t base, uint32_t c) {
+  uint64_t r[N];
+#pragma unroll
+  for (int i = 0; i < N; i++) r[i] = (uint32_t)i < c ? keys[base + i] : BK_INVALID;
+#pragma unroll
+  for (int size = 2; size <= N; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+#pragma unroll
+      for (int i = 0; i < N; i++) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const uint64_t a = r[i], b = r[j];
+          const bool sw = ((i & size) == 0) ? (a > b) : (a < b);
+          r[i] = sw ? b : a;
+          r[j] = sw ? a : b;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < N; i++)
+    if ((uint32_t)i < c) keys[base + i] = r[i];
+}
+
+// A thread per bucket: buckets of 2..16 keys sorted in the thread's
+// registers (network size by the warp's largest such bucket), 17..32 by the
+// whole warp; larger ones listed for the shared-memory kernels (by size);
+// those above BUCKET_SEG_MAX flagged.
+__global__ void k_bucket_sort_small(const uint64_t *off, uint32_t nb, uint64_t *keys,
+                                    uint32_t *mid, uint32_t *big, unsigned long long *nlist,
+                                    uint32_t *err) {
+  const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t base = b < nb ? off[b] : 0;
+  const uint32_t c = b < nb ? (uint32_t)(off[b + 1] - base) : 0u;
+  if (c > 32 && c <= BK_MID) mid[atomicAdd(nlist, 1ull)] = (uint32_t)b;
+  if (c > BK_MID && c <= BUCKET_SEG_MAX) big[atomicAdd(nlist + 1, 1ull)] = (uint32_t)b;
+  if (c > BUCKET_SEG_MAX) atomicOr(err, ERR_BIGSEG);
+  const uint32_t ct = (c >= 2 && c <= 16) ? c : 0u;
+  const uint32_t wmax = __reduce_max_sync(0xFFFFFFFFu, ct);
+  if (ct) {
+    if (wmax <= 4)
+      thread_bucket_sort<4>(keys, base, ct);
+    else if (wmax <= 8)
+      thread_bucket_sort<8>(keys, base, ct);
+    else
+      thread_bucket_sort<16>(keys, base, ct);
+  }
+  uint32_t todo = __ballot_sync(0xFFFFFFFFu, c > 16 && c <= 32);
+  while (todo) {
+    const uint32_t j = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const uint64_t bj = __shfl_sync(0xFFFFFFFFu, base, j);
+    const uint32_t cj = __shfl_sync(0xFFFFFFFFu, c, j);
+    uint64_t v = lane < cj ? keys[bj + lane] : BK_INVALID;
+    v = warp_bitonic32(v, lane);
+    if (lane < cj) keys[bj + lane] = v;
+  }
+}
+
+// A warp per listed bucket of 33..BK_MID keys, sorted in shared memory.
+constexpr uint32_t BK_MID_WARPS = 4;
+__global__ void __launch_bounds__(BK_MID_WARPS * 32)
+    k_bucket_sort_mid(const uint64_t *off, const uint32_t *mid, const unsigned long long *nlist,
+                      uint64_t *keys) {
+  __shared__ uint64_t sv[BK_MID_WARPS][BK_MID];
+  const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t *v = sv[w];
+  const uint64_t nm = nlist[0];
+  for (uint64_t i = (uint64_t)blockIdx.x * BK_MID_WARPS + w; i < nm;
+       i += (uint64_t)gridDim.x * BK_MID_WARPS) {
+    const uint32_t b = mid[i];
+    const uint64_t base = off[b];
+    const uint32_t c = (uint32_t)(off[b + 1] - base);
+    uint32_t P = 64;
+    while (P < c) P <<= 1;
+    for (uint32_t t = lane; t < P; t += 32) v[t] = t < c ? keys[base + t] : BK_INVALID;
+    __syncwarp();
+    smem_bitonic(v, P, lane, 32, [] { __syncwarp(); });
+    for (uint32_t t = lane; t < c; t += 32) keys[base + t] = v[t];
+    __syncwarp();
+  }
+}
+
+// A CTA per listed bucket of BK_MID+1..BUCKET_SEG_MAX keys, sorted in
+// (dynamic) shared memory.
+constexpr uint32_t BK_BIG_T = 1024;
+__global__ void __launch_bounds__(BK_BIG_T)
+    k_bucket_sort_big(const uint64_t *off, const uint32_t *big, const unsigned long long *nlist,
+                      uint64_t *keys) {
+  extern __shared__ uint64_t sbig[];
+  const uint64_t nbg = nlist[1];
+  for (uint64_t i = blockIdx.x; i < nbg; i += gridDim.x) {
+    const uint32_t b = big[i];
+    const uint64_t base = off[b];
+    const uint32_t c = (uint32_t)(off[b + 1] - base);
+    uint32_t P = 2 * BK_MID;
+    while (P < c) P <<= 1;
+    for (uint32_t t = threadIdx.x; t < P; t += blockDim.x) sbig[t] = t < c ? keys[base + t] : BK_INVALID;
+    __syncthreads();
+    smem_bitonic(sbig, P, threadIdx.x, blockDim.x, [] { __syncthreads(); });
+    for (uint32_t t = threadIdx.x; t < c; t += blockDim.x) keys[base + t] = sbig[t];
+    __syncthreads();
+  }
+}
+
+struct BucketLayout {
+  uint32_t nb, shift;
+  uint64_t list_cap;
+  uint64_t cnt_w, off_w, scan_w, list_w;  // words of each part
+  uint64_t total() const { return 2 * cnt_w + off_w + scan_w + 2 * list_w + 2; }
+};
+
+BucketLayout bucket_layout(uint64_t k, uint32_t n) {
+  BucketLayout L{};
+  // about BUCKET_TARGET keys per bucket: bucket = source >> shift
+  constexpr uint64_t BUCKET_TARGET = 4;
+  L.shift = 0;
+  while (L.shift < 31 && ceil_div((uint64_t)n, 1ull << L.shift) * BUCKET_TARGET > k) L.shift++;
+  L.nb = (uint32_t)ceil_div((uint64_t)n, 1ull << L.shift);
+  L.list_cap = std::min<uint64_t>(L.nb, k / 33) + 1;
+  L.cnt_w = ceil_div((uint64_t)L.nb + 1, 2);
+  L.off_w = (uint64_t)L.nb + 1;
+  L.scan_w = scan_tmp_elems((uint64_t)L.nb + 1) + 4;
+  L.list_w = ceil_div(L.list_cap, 2);
+  return L;
+}
+
+}  // namespace
+
+uint64_t bucket_tmp_elems(uint64_t k, uint32_t n) { return bucket_layout(k, n).total(); }
+
+uint64_t *bucket_sort_u64(const uint64_t *keys, uint64_t *alt, uint64_t k, uint32_t n,
+                          uint64_t *tmp, cudaStream_t s, Profiler &prof, uint32_t *err) {
+  if (k == 0) return alt;
+  const BucketLayout L = bucket_layout(k, n);
+  const BucketArgs ba{L.nb, L.shift};
+  uint32_t *cnt = reinterpret_cast<uint32_t *>(tmp);
+  uint32_t *fill = reinterpret_cast<uint32_t *>(tmp + L.cnt_w);
+  uint64_t *off = tmp + 2 * L.cnt_w;
+  uint64_t *st = off + L.off_w;
+  uint32_t *mid = reinterpret_cast<uint32_t *>(st + L.scan_w);
+  uint32_t *big = reinterpret_cast<uint32_t *>(st + L.scan_w + L.list_w);
+  unsigned long long *nlist =
+      reinterpret_cast<unsigned long long *>(st + L.scan_w + 2 * L.list_w);
+  TRC_CUDA(cudaMemsetAsync(tmp, 0, 2 * L.cnt_w * 8, s));  // cnt and fill
+  TRC_CUDA(cudaMemsetAsync(nlist, 0, 16, s));
+  TRC_LAUNCH(prof, s, "bsort_hist", ceil_div(k, 256), 256, 0, k_bucket_hist, keys, k, ba, cnt);
+  exclusive_scan(LoadCnt32{cnt}, (uint64_t)L.nb + 1, off, st, s, prof, "bsort_scan");
+  TRC_LAUNCH(prof, s, "bsort_scatter", ceil_div(k, 256), 256, 0, k_bucket_scatter, keys, k, ba,
+             off, fill, alt);
+  TRC_LAUNCH(prof, s, "bsort_small", ceil_div((uint64_t)L.nb, 256), 256, 0, k_bucket_sort_small,
+             off, L.nb, alt, mid, big, nlist, err);
+  const unsigned sms = (unsigned)num_sms();
+  TRC_LAUNCH(prof, s, "bsort_mid", sms * 8, BK_MID_WARPS * 32, 0, k_bucket_sort_mid, off, mid,
+             nlist, alt);
+  const int big_smem = (int)(BUCKET_SEG_MAX * sizeof(uint64_t));
+  TRC_CUDA(cudaFuncSetAttribute(k_bucket_sort_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                big_smem));
+  TRC_LAUNCH(prof, s, "bsort_big", sms, BK_BIG_T, big_smem, k_bucket_sort_big, off, big, nlist,
+             alt);
+  return alt;
+}
+
+// ---------------------------------------------------------------------------
 // Merge path.  Output tile t covers diagonals [t*MT, (t+1)*MT); its split
 // points are found by binary search, the two input ranges staged in shared
 // memory, and each thread merges MI consecutive outputs.

@@ -282,6 +282,7 @@ void Graph::stats(trc_stats *o) {
   o->hub_rewrites = hub_rewrites;
   o->hub_blocks_free = nfree;
   o->hub_absorbs = hub_absorbs;
+  o->sort_retries = sort_retries;
   // inline = sum(min(deg,16)); hub = m - inline - tier2
   uint64_t *t = tmp(scan_tmp_elems(n) + 4);
   uint64_t *off = s_oOff.ensure((uint64_t)n + 1);

@@ -34,6 +34,7 @@ constexpr uint32_t NONE32 = 0xFFFFFFFFu;
 constexpr uint32_t ERR_BAD_VERTEX = 1u;
 constexpr uint32_t ERR_BOUNDS = 2u;
 constexpr uint32_t ERR_TIMEOUT = 4u;
+constexpr uint32_t ERR_BIGSEG = 8u;  // the bucket sort met a source with too many keys
 
 // ---------------------------------------------------------------------------
 // Device view of the graph, passed to kernels by value.

@@ -907,6 +907,10 @@ __global__ void k_window_mark2(const uint64_t *mw, uint32_t n, uint32_t *stamp, 
 // the tier-2 counts is then computed even when no vertex overflows).
 constexpr uint64_t PLAN_SPECULATE = 1u << 16;
 
+// Batches of at least this many keys sort with the bucket sort (below it
+// both sorts are a handful of launches over a few tiles).
+constexpr uint64_t BUCKET_MIN_KEYS = 1u << 12;
+
 // ---------------------------------------------------------------------------
 // The pipeline
 
@@ -923,6 +927,13 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   const uint64_t k2 = sym ? 2 * k : k;
   DevView G = view();
   uint64_t *cnt = s_cnt.get();
+  // the bucket sort unless the radix sort is asked for (or its wait test
+  // hook is set); a bucket too large for it sends the batch back here, to
+  // the radix sort, before anything is modified
+  bool bucket = sort_mode == 2 ||
+                (sort_mode == 0 && k2 >= BUCKET_MIN_KEYS && !sort_wait.withhold_first &&
+                 sort_wait.spin_limit == SortWait{}.spin_limit);
+retry_sort:
   TRC_CUDA(cudaMemsetAsync(cnt, 0, 32 * 8, stream));
   TRC_CUDA(cudaMemsetAsync(err.get(), 0, 4, stream));
 
@@ -930,8 +941,10 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   uint64_t *A = s_A.ensure(k2), *B = s_B.ensure(k2);
   TRC_LAUNCH(prof, stream, "upd_make_keys", ceil_div(k, 256), 256, 0, k_make_keys, src, dst, k, n,
              sym, drop, A, err.get());
-  uint64_t *t = tmp(std::max(radix_tmp_elems(k2), select_tmp_elems(k2)));
-  uint64_t *sorted = radix_sort_u64(A, B, k2, vbits(), t, stream, prof, err.get(), sort_wait);
+  uint64_t *t = tmp(std::max({radix_tmp_elems(k2), select_tmp_elems(k2),
+                              bucket ? bucket_tmp_elems(k2, n) : (uint64_t)0}));
+  uint64_t *sorted = bucket ? bucket_sort_u64(A, B, k2, n, t, stream, prof, err.get())
+                            : radix_sort_u64(A, B, k2, vbits(), t, stream, prof, err.get(), sort_wait);
   uint64_t *bkeys = sorted == A ? B : A;
   // 3: unique + existence filter (one lookup per key), compacted
   uint8_t *kflags = s_flags.ensure(k2);
@@ -1023,6 +1036,11 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   const uint32_t herr = hub_stage_[60];
   if (herr & ERR_BAD_VERTEX) throw_error(TRC_ERR_INVALID, "vertex id out of range [0, n)");
   if (herr & ERR_TIMEOUT) throw_error(TRC_ERR_TIMEOUT, "radix sort look-back wait gave up");
+  if (herr & ERR_BIGSEG) {
+    bucket = false;
+    sort_retries++;
+    goto retry_sort;
+  }
   const uint64_t kb = hc[C_KB], nt = hc[C_NT];
   if (kb == 0) {
     for (auto &x : last) x = 0;

@@ -247,6 +247,47 @@ def test_random_updates_against_set_model(T):
         assert c == sum(1 for w in na & nb if w < min(a, b))
 
 
+@pytest.mark.parametrize("mode", [1, 2])
+def test_batch_sort_modes_agree_with_oracle(T, mode):
+    """The bucket sort (mode 2: every batch) and the radix sort (mode 1) give
+    the same graph as the oracle's set model over batches of 1..2e5 keys
+    (empty buckets, dropped self loops, buckets of every size tier); a batch
+    with a source of more than 16384 keys goes back to the radix sort before
+    the graph is modified (sort_retries counts it)."""
+    from terrace_b200 import _lib
+    rng = np.random.default_rng(7 + mode)
+    n = 40000
+    g = T.Graph(n, hub_threshold=64)
+    _lib.check(g._L.trc_debug_sort_mode(g._h, mode))
+    cur = np.zeros(0, np.uint64)
+    sizes = [1, 2, 17, 33, 300, 1025, 4096, 20000, 100000]
+    for step, k in enumerate(sizes):
+        s = rng.integers(0, n, k).astype(np.uint32)
+        d = rng.integers(0, n, k).astype(np.uint32)
+        if k >= 300:  # skew: runs of equal sources of every bucket tier
+            s[: k // 4] = rng.integers(0, 8, k // 4).astype(np.uint32)
+            s[k // 4: k // 4 + k // 8] = 12345
+        bk = O.make_keys(s, d, True, True)
+        if step % 4 == 3:
+            g.remove_edge_batch(s, d, **SYM)
+            cur = O.key_difference(cur, bk)
+        else:
+            g.add_edge_batch(s, d, **SYM)
+            cur = O.key_union(cur, bk)
+        assert_same_csr(g, *O.csr_from_keys(n, cur))
+    assert g.stats()["sort_retries"] == 0
+    # one source with 20000 distinct neighbours in one batch: its bucket is
+    # above the bucket sort's limit
+    d = rng.permutation(n)[:20000].astype(np.uint32)
+    s = np.full(20000, 77, np.uint32)
+    g.add_edge_batch(s, d, **SYM)
+    cur = O.key_union(cur, O.make_keys(s, d, True, True))
+    assert_same_csr(g, *O.csr_from_keys(n, cur))
+    assert g.stats()["sort_retries"] == (1 if mode == 2 else 0)
+    assert g.check() == 0
+    g.close()
+
+
 def test_streaming_rmat22_roundtrip_and_parity(T):
     """LiveJournal-shaped RMAT scale 22 ef 16: bulk load and one 1e6-pair
     insert + delete batch.  Parity with the oracle's set model by CSR hash,
