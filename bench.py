@@ -781,16 +781,22 @@ def serving_run(T, g, batched, reqs, gaps, rate, ps, pd):
         else:
             x = srv.stats(code)
             per[k] = {"p50_ms": x["p50_ms"], "p99_ms": x["p99_ms"], "completed": x["completed"]}
+    tr = srv.rounds()
     srv.close()
+    parts = {p: round(sum(r[p + "_ms"] for r in tr), 1)
+             for p in ("lookup", "update", "bfs", "pagerank")}
+    slow = sorted(tr, key=lambda r: -r["ms"])[:3]
+    trace = {"ms_by_part": parts,
+             "bfs_groups": sum(r["bfs_groups"] for r in tr),
+             "bfs_singles": sum(r["bfs_singles"] for r in tr),
+             "slowest_rounds": [{k: (round(v, 2) if isinstance(v, float) else v)
+                                 for k, v in r.items()} for r in slow]}
     return {"offered_rps": len(reqs) / t_sub, "target_rps": rate, "requests": len(reqs),
             "throughput_rps": st["completed"] / st["elapsed_s"], "p50_ms": st["p50_ms"],
             "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
             "rounds": st["rounds"], "device_calls": st["device_calls"],
             "rejected": st["rejected"], "failed": bad, "per_kind": per,
-            "pma_rebuilds": st["pma_rebuilds"],
-            "worst_round": {k: st["worst_" + k] for k in
-                            ("round_ms", "update_ms", "bfs_ms", "pagerank_ms", "round_requests",
-                             "round_rebuilds")}}
+            "pma_rebuilds": st["pma_rebuilds"], "rounds_trace": trace}
 
 
 def serving(T, torch):

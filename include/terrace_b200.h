@@ -360,6 +360,23 @@ trc_status trc_server_reset_stats(trc_server *s);
  * takes every pending request, subject to the admission limits.  Lets a
  * caller gather a burst into one round.  Destroy drains a held server. */
 trc_status trc_server_hold(trc_server *s, int hold);
+/* One record per served round (the last 65536 since creation or reset):
+ * where the round's time went and what it held. */
+typedef struct {
+  double t_start_ms;   /* round start, from the first submit (or reset) */
+  double ms;           /* whole round */
+  double lookup_ms, update_ms, bfs_ms, pagerank_ms; /* its parts (PageRank:
+                          launch + the wait after the BFS part) */
+  uint32_t lookups, updates, bfs, pageranks; /* requests of each kind */
+  uint64_t update_pairs;                      /* pairs over its updates */
+  uint32_t bfs_groups;  /* multi-source BFS launches */
+  uint32_t bfs_singles; /* single-source BFS runs */
+  uint32_t rebuilds;    /* full tier-2 rebuilds */
+  uint32_t pending_after; /* requests left queued when the round started */
+} trc_round_record;
+/* Copies up to cap records, oldest first; *count = records held. */
+trc_status trc_server_rounds(trc_server *s, trc_round_record *out, uint64_t cap,
+                             uint64_t *count);
 
 /* ---- diagnostics (no reference counterpart: the reference has only
  *      lock-ownership checks, src/PMA.cc:29-111). */

@@ -79,6 +79,15 @@ class trc_server_stats(C.Structure):
                 ("worst_round_rebuilds", C.c_uint64), ("pma_rebuilds", C.c_uint64)]
 
 
+class trc_round_record(C.Structure):
+    _fields_ = [("t_start_ms", C.c_double), ("ms", C.c_double), ("lookup_ms", C.c_double),
+                ("update_ms", C.c_double), ("bfs_ms", C.c_double), ("pagerank_ms", C.c_double),
+                ("lookups", C.c_uint32), ("updates", C.c_uint32), ("bfs", C.c_uint32),
+                ("pageranks", C.c_uint32), ("update_pairs", C.c_uint64),
+                ("bfs_groups", C.c_uint32), ("bfs_singles", C.c_uint32),
+                ("rebuilds", C.c_uint32), ("pending_after", C.c_uint32)]
+
+
 class trc_stats(C.Structure):
     _fields_ = [("n", C.c_uint32),
                 ("num_edges", C.c_uint64),
@@ -169,6 +178,7 @@ SIGNATURES = [
     ("trc_server_get_stats", _int, [_vp, _int, C.POINTER(trc_server_stats)]),
     ("trc_server_reset_stats", _int, [_vp]),
     ("trc_server_hold", _int, [_vp, _int]),
+    ("trc_server_rounds", _int, [_vp, C.POINTER(trc_round_record), _u64, C.POINTER(_u64)]),
 ]
 
 _lib = None

@@ -558,25 +558,9 @@ __device__ __forceinline__ bool bit_test(const uint32_t *b, uint32_t v) {
   return (__ldg(b + (v >> 5)) >> (v & 31)) & 1u;
 }
 
-// One 32-neighbour chunk of u's list (ranks j0..j0+31): claim unvisited
+// A piece (list_piece) of frontier vertex u's list: claim its unvisited
 // neighbours by CAS on the parent (any frontier parent, as BFS_F::
 // updateAtomic).
-__device__ __forceinline__ void bfs_push_chunk(const NbrList &L, uint32_t u, uint32_t j0,
-                                               const BFSState &s, uint32_t lane, WarpStage &st) {
-  const uint32_t j = j0 + lane;
-  bool win = false;
-  uint32_t v = 0;
-  if (j < L.deg) {
-    v = L.at(j);
-    if (s.lv[v] == TRC_UNREACHED && atomicCAS(&s.par[v], -1, (int32_t)u) == -1) {
-      s.lv[v] = s.d + 1;
-      win = true;
-    }
-  }
-  st.add(win, v, s.next, s.next_cnt, lane);
-}
-
-// The same for a piece of a hub's list (hub_chunk).
 __device__ __forceinline__ void bfs_push_span(const uint32_t *p, uint32_t len, uint32_t u,
                                               const BFSState &s, uint32_t lane, WarpStage &st) {
   bool win = false;
@@ -591,63 +575,61 @@ __device__ __forceinline__ void bfs_push_span(const uint32_t *p, uint32_t len, u
   st.add(win, v, s.next, s.next_cnt, lane);
 }
 
-// Warp per frontier vertex; hubs are listed for k_bfs_push_hubs.
-__global__ void k_bfs_push(DevView G, const uint32_t *F, uint32_t nf, BFSState s) {
-  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
-  uint32_t lane = threadIdx.x & 31;
-  if (w >= nf) return;
-  uint32_t u = F[w];
-  if (G.hub_of[u] >= 0) {
-    if (lane == 0) s.seg[atomicAdd(s.seg_cnt, 1u)] = u;
-    return;
+// Edge-balanced push (the frontier's lists cut into list_piece()s; off =
+// exclusive prefix of the piece counts, off[nf] = the total T): warp w of W
+// takes pieces [T*w/W, T*(w+1)/W), whatever vertices they belong to, so one
+// long list is spread over many warps and many short lists share one warp.
+struct PushPieces {
+  DevView G;
+  const uint32_t *F;
+  uint64_t nf;
+  __device__ uint64_t operator()(uint64_t i) const {
+    return i < nf ? list_pieces(nbr_list(G, F[i])) : 0;
   }
-  __shared__ uint32_t stg[AT / 32][32];
-  WarpStage st{stg[(threadIdx.x >> 5)], 0};
-  NbrList L = nbr_list(G, u);
-  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) bfs_push_chunk(L, u, j0, s, lane, st);
-  st.flush(s.next, s.next_cnt, lane);
+};
+
+// The frontier vertex of piece t: the i with off[i] <= t < off[i+1] (every
+// list has a piece, so off is strictly increasing).
+__device__ __forceinline__ uint32_t piece_owner(const uint64_t *off, uint32_t nf, uint64_t t) {
+  uint32_t a = 0, b = nf;
+  while (b - a > 1) {
+    const uint32_t m = (a + b) >> 1;
+    if (off[m] <= t) a = m;
+    else b = m;
+  }
+  return a;
 }
 
-// The frontier's hubs (list and device count from a compaction).  The first
-// PUSH_WIDE hubs are spread over the whole grid (every warp takes their
-// 32-neighbour chunks round-robin), so one vertex of 1e5-1e6 neighbours
-// uses the whole GPU; the rest get a CTA each (grid-stride), its warps
-// taking the chunks round-robin.
-constexpr uint64_t PUSH_WIDE = 64;
-
-__global__ void k_bfs_push_hubs(DevView G, BFSState s) {
-  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint64_t gw = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * AT) >> 5;
-  const uint32_t *FH = s.seg;
-  const uint64_t nh = *s.seg_cnt;
-  const uint64_t nwide = nh < PUSH_WIDE ? nh : PUSH_WIDE;
+__global__ void __launch_bounds__(AT) k_bfs_push_lb(DevView G, const uint32_t *F, uint32_t nf,
+                                                    const uint64_t *off, BFSState s) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t W = ((uint64_t)gridDim.x * AT) >> 5;
+  const uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  const uint64_t T = off[nf];
+  const uint64_t lo = T * w / W, hi = T * (w + 1) / W;
   __shared__ uint32_t stg[AT / 32][32];
-  WarpStage st{stg[wib], 0};
-  const uint32_t *p;
-  uint32_t len;
-  for (uint64_t i = 0; i < nwide; i++) {
-    const uint32_t u = FH[i];
+  WarpStage st{stg[threadIdx.x >> 5], 0};
+  if (lo < hi) {
+    uint32_t i = piece_owner(off, nf, lo);
+    uint32_t u = F[i];
     NbrList L = nbr_list(G, u);
-    const uint64_t nch = hub_chunks(L);
-    for (uint64_t c = gw; c < nch; c += nwarps) {
-      hub_chunk(L, (uint32_t)c, p, len);
-      if (len) bfs_push_span(p, len, u, s, lane, st);  // (len is warp-uniform)
-    }
-  }
-  for (uint64_t i = nwide + blockIdx.x; i < nh; i += gridDim.x) {
-    const uint32_t u = FH[i];
-    NbrList L = nbr_list(G, u);
-    const uint32_t nch = hub_chunks(L);
-    for (uint32_t c = wib; c < nch; c += AT / 32) {
-      hub_chunk(L, c, p, len);
-      if (len) bfs_push_span(p, len, u, s, lane, st);
+    uint64_t vbeg = off[i], vend = off[i + 1];
+    for (uint64_t t = lo; t < hi; t++) {
+      while (t >= vend) {  // (t < T = off[nf], so i + 1 < nf here)
+        i++;
+        u = F[i];
+        L = nbr_list(G, u);
+        vbeg = vend;
+        vend = off[i + 1];
+      }
+      const uint32_t *p;
+      uint32_t len;
+      list_piece(L, (uint32_t)(t - vbeg), p, len);
+      if (len) bfs_push_span(p, len, u, s, lane, st);  // (warp-uniform)
     }
   }
   st.flush(s.next, s.next_cnt, lane);
 }
-
-
 
 // List entries that are still unvisited (and have more than min_deg
 // neighbours).
@@ -685,74 +667,66 @@ constexpr uint32_t BP_V = 4;
 
 __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S, uint64_t nS,
                                                    BFSState s) {
-  const uint32_t lane = threadIdx.x & 31, q = lane & 3, qw = lane >> 2;
-  const uint64_t wbase = (((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5) * (8 * BP_V);
-  uint32_t u[BP_V], d[BP_V];
-  bool act[BP_V];
+  const uint32_t lane = threadIdx.x & 31, q = lane & 3, qw = lane >> 2, wib = threadIdx.x >> 5;
+  __shared__ uint32_t stg[3][AT / 32][32];
+  WarpStage sn{stg[0][wib], 0}, ss{stg[1][wib], 0}, sc{stg[2][wib], 0};
+  const uint64_t step = (((uint64_t)gridDim.x * AT) >> 5) * (8 * BP_V);
+  for (uint64_t wbase = (((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5) * (8 * BP_V); wbase < nS;
+       wbase += step) {
+    uint32_t u[BP_V], d[BP_V];
+    bool act[BP_V];
 #pragma unroll
-  for (uint32_t i = 0; i < BP_V; i++) {
-    const uint64_t vi = wbase + i * 8 + qw;
-    u[i] = vi < nS ? (S ? S[vi] : (uint32_t)vi) : 0u;
-    act[i] = vi < nS;
-  }
-#pragma unroll
-  for (uint32_t i = 0; i < BP_V; i++) {
-    d[i] = act[i] ? G.deg[u[i]] : 0u;
-    // (no list: every vertex id, hubs left to their own pass)
-    if (!S && act[i] && G.hub_of[u[i]] >= 0) d[i] = 0;
-    act[i] = act[i] && s.lv[u[i]] == TRC_UNREACHED && q * 4 < d[i];
-  }
-  uint4 v[BP_V];
-#pragma unroll
-  for (uint32_t i = 0; i < BP_V; i++)
-    v[i] = act[i] ? __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u[i] * K_INLINE) + q)
-                  : make_uint4(0, 0, 0, 0);
-  uint32_t wx[BP_V], wy[BP_V], wz[BP_V], ww[BP_V];
-#pragma unroll
-  for (uint32_t i = 0; i < BP_V; i++) {
-    const uint32_t e = q * 4;
-    wx[i] = act[i] ? __ldg(s.bits + (v[i].x >> 5)) : 0u;
-    wy[i] = act[i] && e + 1 < d[i] ? __ldg(s.bits + (v[i].y >> 5)) : 0u;
-    wz[i] = act[i] && e + 2 < d[i] ? __ldg(s.bits + (v[i].z >> 5)) : 0u;
-    ww[i] = act[i] && e + 3 < d[i] ? __ldg(s.bits + (v[i].w >> 5)) : 0u;
-  }
-  uint32_t wins = 0;  // bit i: this lane claimed vertex i
-  uint32_t tosg = 0, tocand = 0;  // bit i (lane q == 0): vertex i stays unvisited
-#pragma unroll
-  for (uint32_t i = 0; i < BP_V; i++) {
-    const bool uv = d[i] > 0 && s.lv[u[i]] == TRC_UNREACHED;  // cached: loaded above
-    uint32_t first = 4;
-    if ((wx[i] >> (v[i].x & 31)) & 1u) first = 0;
-    else if ((wy[i] >> (v[i].y & 31)) & 1u) first = 1;
-    else if ((wz[i] >> (v[i].z & 31)) & 1u) first = 2;
-    else if ((ww[i] >> (v[i].w & 31)) & 1u) first = 3;
-    uint32_t m = __ballot_sync(0xFFFFFFFFu, first < 4);
-    uint32_t grp = (m >> (lane & ~3u)) & 0xFu;
-    bool win = grp && (__ffs(grp) - 1) == (int)q;
-    if (win) {
-      uint32_t p = first == 0 ? v[i].x : first == 1 ? v[i].y : first == 2 ? v[i].z : v[i].w;
-      s.par[u[i]] = (int32_t)p;
-      s.lv[u[i]] = s.d + 1;
-      wins |= 1u << i;
+    for (uint32_t i = 0; i < BP_V; i++) {
+      const uint64_t vi = wbase + i * 8 + qw;
+      u[i] = vi < nS ? (S ? S[vi] : (uint32_t)vi) : 0u;
+      act[i] = vi < nS;
     }
-    if (q == 0 && uv && grp == 0) {
-      if (d[i] > K_INLINE) tosg |= 1u << i;
-      else tocand |= 1u << i;
+#pragma unroll
+    for (uint32_t i = 0; i < BP_V; i++) {
+      d[i] = act[i] ? G.deg[u[i]] : 0u;
+      // (no list: every vertex id, hubs left to their own pass)
+      if (!S && act[i] && G.hub_of[u[i]] >= 0) d[i] = 0;
+      act[i] = act[i] && s.lv[u[i]] == TRC_UNREACHED && q * 4 < d[i];
+    }
+    uint4 v[BP_V];
+#pragma unroll
+    for (uint32_t i = 0; i < BP_V; i++)
+      v[i] = act[i] ? __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u[i] * K_INLINE) + q)
+                    : make_uint4(0, 0, 0, 0);
+    uint32_t wx[BP_V], wy[BP_V], wz[BP_V], ww[BP_V];
+#pragma unroll
+    for (uint32_t i = 0; i < BP_V; i++) {
+      const uint32_t e = q * 4;
+      wx[i] = act[i] ? __ldg(s.bits + (v[i].x >> 5)) : 0u;
+      wy[i] = act[i] && e + 1 < d[i] ? __ldg(s.bits + (v[i].y >> 5)) : 0u;
+      wz[i] = act[i] && e + 2 < d[i] ? __ldg(s.bits + (v[i].z >> 5)) : 0u;
+      ww[i] = act[i] && e + 3 < d[i] ? __ldg(s.bits + (v[i].w >> 5)) : 0u;
+    }
+#pragma unroll
+    for (uint32_t i = 0; i < BP_V; i++) {
+      const bool uv = d[i] > 0 && s.lv[u[i]] == TRC_UNREACHED;  // cached: loaded above
+      uint32_t first = 4;
+      if ((wx[i] >> (v[i].x & 31)) & 1u) first = 0;
+      else if ((wy[i] >> (v[i].y & 31)) & 1u) first = 1;
+      else if ((wz[i] >> (v[i].z & 31)) & 1u) first = 2;
+      else if ((ww[i] >> (v[i].w & 31)) & 1u) first = 3;
+      const uint32_t m = __ballot_sync(0xFFFFFFFFu, first < 4);
+      const uint32_t grp = (m >> (lane & ~3u)) & 0xFu;
+      const bool win = grp && (__ffs(grp) - 1) == (int)q;
+      if (win) {
+        const uint32_t p = first == 0 ? v[i].x : first == 1 ? v[i].y : first == 2 ? v[i].z : v[i].w;
+        s.par[u[i]] = (int32_t)p;
+        s.lv[u[i]] = s.d + 1;
+      }
+      const bool left = q == 0 && uv && grp == 0;
+      sn.add(win, u[i], s.next, s.next_cnt, lane);
+      ss.add(left && d[i] > K_INLINE, u[i], s.seg, s.seg_cnt, lane);
+      sc.add(left && d[i] <= K_INLINE, u[i], s.cand, s.cand_cnt, lane);
     }
   }
-  __shared__ uint32_t sh[AT / 32 + 2];
-  uint32_t pos = block_append(__popc(wins), s.next_cnt, sh);
-#pragma unroll
-  for (uint32_t i = 0; i < BP_V; i++)
-    if ((wins >> i) & 1u) s.next[pos++] = u[i];
-  pos = block_append(__popc(tosg), s.seg_cnt, sh);
-#pragma unroll
-  for (uint32_t i = 0; i < BP_V; i++)
-    if ((tosg >> i) & 1u) s.seg[pos++] = u[i];
-  pos = block_append(__popc(tocand), s.cand_cnt, sh);
-#pragma unroll
-  for (uint32_t i = 0; i < BP_V; i++)
-    if ((tocand >> i) & 1u) s.cand[pos++] = u[i];
+  sn.flush(s.next, s.next_cnt, lane);
+  ss.flush(s.seg, s.seg_cnt, lane);
+  sc.flush(s.cand, s.cand_cnt, lane);
 }
 
 // One warp scans the neighbours of vertex u of rank >= j_first for a
@@ -864,9 +838,12 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
   // candidates of the dense steps: non-hub vertices not yet visited,
   // compacted after every dense step
   DBuf<uint32_t> cbuf[2], segb;  // candidate ping-pong, segment-pass list
+  DBuf<uint64_t> offb, scanb;     // push steps: piece prefix and scan scratch
   cbuf[0].bind(&budget);
   cbuf[1].bind(&budget);
   segb.bind(&budget);
+  offb.bind(&budget);
+  scanb.bind(&budget);
   // (the first dense step reads every vertex id in order, no list: its
   // candidates are all non-hub vertices, and the loads stay contiguous)
   const uint32_t *cand = nullptr;
@@ -885,8 +862,10 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
       // pass A: the 16 inline neighbours of every unvisited non-hub vertex;
       // those left unvisited go to the segment list (PMA vertices) or the
       // next candidates
-      TRC_LAUNCH(prof, stream, "bfs_pull_inline", ceil_div(ncand * 4, (uint64_t)AT * BP_V), AT, 0,
-                 k_bfs_pull_S, G, cand, ncand, s);
+      TRC_LAUNCH(prof, stream, "bfs_pull_inline",
+                 std::min<uint64_t>(ceil_div(ncand * 4, (uint64_t)AT * BP_V),
+                                    resident_grid(k_bfs_pull_S, AT)),
+                 AT, 0, k_bfs_pull_S, G, cand, ncand, s);
       // pass B: the PMA segments of the segment list (count on the device);
       // hubs from rank 0
       TRC_LAUNCH(prof, stream, "bfs_pull_M", pgrid, AT, 0, k_bfs_pull_W, G, sg, 0, c + 1, s,
@@ -899,11 +878,13 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
       cand = s.cand;
       cnext ^= 1;
     } else {
-      TRC_LAUNCH(prof, stream, "bfs_push", ceil_div((uint64_t)nf * 32, AT), AT, 0, k_bfs_push, G, F,
-                 nf, s);
-      // the frontier's hubs (listed by bfs_push), spread over the grid
-      if (H)
-        TRC_LAUNCH(prof, stream, "bfs_push_hubs", pgrid, AT, 0, k_bfs_push_hubs, G, s);
+      // edge-balanced push: piece counts scanned, then every warp of the
+      // grid takes an equal share of the frontier's pieces
+      uint64_t *off = offb.ensure((uint64_t)nf + 1);
+      uint64_t *stmp = scanb.ensure(scan_tmp_elems((uint64_t)nf + 1) + 4);
+      exclusive_scan(PushPieces{G, F, nf}, (uint64_t)nf + 1, off, stmp, stream, prof,
+                     "bfs_push_scan");
+      TRC_LAUNCH(prof, stream, "bfs_push", pgrid, AT, 0, k_bfs_push_lb, G, F, nf, off, s);
       TRC_CUDA(cudaMemcpyAsync(hc, c, 4, cudaMemcpyDeviceToHost, stream));
       sync();
     }
@@ -1082,31 +1063,11 @@ struct BCFwd {
   uint32_t *order;      // order[base ..] receives the next level
   uint32_t *next_cnt;
   uint32_t d;
-  uint32_t *hubs, *hub_cnt;  // push steps: the frontier's hubs
 };
 
-// One 32-neighbour chunk of a frontier vertex u (sigma su): claim
+// A piece (list_piece) of a frontier vertex u's list (sigma su): claim
 // unvisited neighbours for level d+1 and add su to the path count of every
 // neighbour on level d+1 (BC_F::updateAtomic's CAS-add, include/BC.h:44-58).
-__device__ __forceinline__ void bc_push_chunk(const NbrList &L, double su, uint32_t j0,
-                                              const BCFwd &s, uint32_t lane, WarpStage &st) {
-  const uint32_t j = j0 + lane;
-  bool win = false;
-  uint32_t v = 0;
-  if (j < L.deg) {
-    v = L.at(j);
-    uint32_t lvv = s.lv[v];
-    if (lvv == TRC_UNREACHED) {
-      uint32_t old = atomicCAS(&s.lv[v], TRC_UNREACHED, s.d + 1);
-      win = old == TRC_UNREACHED;
-      lvv = win ? s.d + 1 : old;
-    }
-    if (lvv == s.d + 1) atomicAdd(&s.sigma[v], su);
-  }
-  st.add(win, v, s.order, s.next_cnt, lane);
-}
-
-// The same for a piece of a hub's list (hub_chunk).
 __device__ __forceinline__ void bc_push_span(const uint32_t *p, uint32_t len, double su,
                                              const BCFwd &s, uint32_t lane, WarpStage &st) {
   bool win = false;
@@ -1124,53 +1085,34 @@ __device__ __forceinline__ void bc_push_span(const uint32_t *p, uint32_t len, do
   st.add(win, v, s.order, s.next_cnt, lane);
 }
 
-// Warp per frontier vertex; hubs are listed for k_bc_push_hubs.
-__global__ void k_bc_push(DevView G, const uint32_t *F, uint32_t nf, BCFwd s) {
-  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
-  uint32_t lane = threadIdx.x & 31;
-  if (w >= nf) return;
-  uint32_t u = F[w];
-  if (G.hub_of[u] >= 0) {
-    if (lane == 0) s.hubs[atomicAdd(s.hub_cnt, 1u)] = u;
-    return;
-  }
+// Edge-balanced push of a BC level (as k_bfs_push_lb).
+__global__ void __launch_bounds__(AT) k_bc_push_lb(DevView G, const uint32_t *F, uint32_t nf,
+                                                   const uint64_t *off, BCFwd s) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t W = ((uint64_t)gridDim.x * AT) >> 5;
+  const uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  const uint64_t T = off[nf];
+  const uint64_t lo = T * w / W, hi = T * (w + 1) / W;
   __shared__ uint32_t stg[AT / 32][32];
-  WarpStage st{stg[(threadIdx.x >> 5)], 0};
-  double su = s.sigma[u];
-  NbrList L = nbr_list(G, u);
-  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) bc_push_chunk(L, su, j0, s, lane, st);
-  st.flush(s.order, s.next_cnt, lane);
-}
-
-// The frontier's hubs: the first PUSH_WIDE spread over the grid, the rest a
-// CTA each (as k_bfs_push_hubs).
-__global__ void k_bc_push_hubs(DevView G, BCFwd s) {
-  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint64_t gw = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * AT) >> 5;
-  const uint64_t nh = *s.hub_cnt;
-  const uint64_t nwide = nh < PUSH_WIDE ? nh : PUSH_WIDE;
-  __shared__ uint32_t stg[AT / 32][32];
-  WarpStage st{stg[wib], 0};
-  const uint32_t *p;
-  uint32_t len;
-  for (uint64_t i = 0; i < nwide; i++) {
-    const uint32_t u = s.hubs[i];
-    const double su = s.sigma[u];
+  WarpStage st{stg[threadIdx.x >> 5], 0};
+  if (lo < hi) {
+    uint32_t i = piece_owner(off, nf, lo);
+    uint32_t u = F[i];
+    double su = s.sigma[u];
     NbrList L = nbr_list(G, u);
-    const uint64_t nch = hub_chunks(L);
-    for (uint64_t c = gw; c < nch; c += nwarps) {
-      hub_chunk(L, (uint32_t)c, p, len);
-      if (len) bc_push_span(p, len, su, s, lane, st);  // (len is warp-uniform)
-    }
-  }
-  for (uint64_t i = nwide + blockIdx.x; i < nh; i += gridDim.x) {
-    const uint32_t u = s.hubs[i];
-    const double su = s.sigma[u];
-    NbrList L = nbr_list(G, u);
-    const uint32_t nch = hub_chunks(L);
-    for (uint32_t c = wib; c < nch; c += AT / 32) {
-      hub_chunk(L, c, p, len);
+    uint64_t vbeg = off[i], vend = off[i + 1];
+    for (uint64_t t = lo; t < hi; t++) {
+      while (t >= vend) {
+        i++;
+        u = F[i];
+        su = s.sigma[u];
+        L = nbr_list(G, u);
+        vbeg = vend;
+        vend = off[i + 1];
+      }
+      const uint32_t *p;
+      uint32_t len;
+      list_piece(L, (uint32_t)(t - vbeg), p, len);
       if (len) bc_push_span(p, len, su, s, lane, st);
     }
   }
@@ -1419,9 +1361,9 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
   for (auto *b : {&sig, &invb, &depb, &outb, &sideb}) b->bind(&budget);
   double *side = sideb.alloc_exact(n);  // a dense step's results before their commit
   uint32_t *lv = lvb.alloc_exact(n), *order = ordb.alloc_exact(n), *c = cntb.alloc_exact(4);
-  DBuf<uint32_t> hubb;
-  hubb.bind(&budget);
-  uint32_t *hubl = hubb.alloc_exact(H ? H : 1);  // frontier hubs of a push step
+  DBuf<uint64_t> offb, scanb;  // push steps: piece prefix and scan scratch
+  offb.bind(&budget);
+  scanb.bind(&budget);
   double *sigma = sig.alloc_exact(n), *inv = invb.alloc_exact(n), *dep = depb.alloc_exact(n);
   double *out = dev ? out_user : outb.alloc_exact(n);
   TRC_LAUNCH(prof, stream, "bc_init", ceil_div(n, AT), AT, 0, k_bc_init, lv, sigma, dep, n, src,
@@ -1435,7 +1377,7 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
     uint32_t nf = (uint32_t)(f1 - f0);
     if (nf == 0) break;
     TRC_CUDA(cudaMemsetAsync(c, 0, 8, stream));
-    BCFwd s{lv, sigma, side, order + f1, c, d, hubl, c + 1};
+    BCFwd s{lv, sigma, side, order + f1, c, d};
     if ((uint64_t)nf >= dense_at && dense_at > 0) {
       TRC_LAUNCH(prof, stream, "bc_pull_flat", ceil_div(lists.nSM, AT), AT, 0, k_flat<BCPullOp>,
                  G, lists.SM.get(), lists.nSM, BCPullOp{s});
@@ -1444,11 +1386,12 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
       TRC_LAUNCH(prof, stream, "bc_commit", (unsigned)num_sms() * 4, AT, 0, k_bc_commit, order + f1,
                  c, 0, side, sigma);
     } else {
-      TRC_LAUNCH(prof, stream, "bc_push", ceil_div((uint64_t)nf * 32, AT), AT, 0, k_bc_push, G,
-                 order + f0, nf, s);
-      if (H)
-        TRC_LAUNCH(prof, stream, "bc_push_hubs", (unsigned)num_sms() * 8, AT, 0, k_bc_push_hubs, G,
-                   s);
+      uint64_t *off = offb.ensure((uint64_t)nf + 1);
+      uint64_t *stmp = scanb.ensure(scan_tmp_elems((uint64_t)nf + 1) + 4);
+      exclusive_scan(PushPieces{G, order + f0, nf}, (uint64_t)nf + 1, off, stmp, stream, prof,
+                     "bc_push_scan");
+      TRC_LAUNCH(prof, stream, "bc_push", (unsigned)num_sms() * 8, AT, 0, k_bc_push_lb, G,
+                 order + f0, nf, off, s);
     }
     uint32_t nn = 0;
     TRC_CUDA(cudaMemcpyAsync(&nn, c, 4, cudaMemcpyDeviceToHost, stream));

@@ -309,6 +309,16 @@ class Server {
     rounds_ = calls_ = rejected_ = 0;
     worst_ = RoundInfo();
     rebuilds_ = 0;
+    trace_.clear();
+    trace_next_ = 0;
+  }
+
+  uint64_t rounds_trace(trc_round_record *out, uint64_t cap) {
+    std::lock_guard<std::mutex> lk(mu_);
+    const uint64_t held = trace_.size();
+    const uint64_t first = held < kTrace ? 0 : trace_next_ % kTrace;
+    for (uint64_t i = 0; i < held && i < cap; i++) out[i] = trace_[(first + i) % held];
+    return held;
   }
 
  private:
@@ -340,6 +350,11 @@ class Server {
     uint64_t requests = 0, rebuilds = 0;
   } worst_;                    // guarded by mu_
   uint64_t rebuilds_ = 0;      // guarded by mu_
+  static constexpr size_t kTrace = 1u << 16;
+  std::vector<trc_round_record> trace_;  // ring of the last kTrace rounds, guarded by mu_
+  uint64_t trace_next_ = 0;              // guarded by mu_
+  uint32_t round_groups_ = 0, round_singles_ = 0;  // BFS launches of the running round
+  size_t pending_at_start_ = 0;                    // queue length when it was formed
 
   void bind_bufs() {
     if (bufs_bound_) return;
@@ -429,6 +444,7 @@ class Server {
         std::unique_lock<std::mutex> lk(mu_);
         cv_.wait(lk, [&] { return stop_ || (!hold_ && !pending_.empty()); });
         if (pending_.empty() && stop_) break;
+        pending_at_start_ = pending_.size();
         if (cfg_.mode == TRC_SERVE_FIFO) {
           round.push_back(pending_.front());
           pending_.pop_front();
@@ -507,6 +523,14 @@ class Server {
     bind_bufs();
     RoundInfo info;
     info.requests = round.size();
+    round_groups_ = round_singles_ = 0;
+    trc_round_record rec{};
+    rec.lookups = (uint32_t)look.size();
+    rec.updates = (uint32_t)upd.size();
+    rec.bfs = (uint32_t)bfs.size();
+    rec.pageranks = (uint32_t)pr.size();
+    for (Request *r : upd) rec.update_pairs += r->a.size();
+    rec.pending_after = (uint32_t)(pending_at_start_ - std::min(pending_at_start_, round.size()));
     const uint64_t rb0 = g_.rebuilds;
     const double t0 = now_ms();
     guarded(look, [&] { run_lookups(look); });
@@ -542,7 +566,19 @@ class Server {
     info.bfs_ms = t4 - t3;
     info.pr_ms = (t3 - t2) + (t5 - t4);  // synchronous part + wait after the BFS groups
     info.rebuilds = g_.rebuilds - rb0;
+    rec.ms = info.ms;
+    rec.lookup_ms = t1 - t0;
+    rec.update_ms = info.upd_ms;
+    rec.bfs_ms = info.bfs_ms;
+    rec.pagerank_ms = info.pr_ms;
+    rec.bfs_groups = round_groups_;
+    rec.bfs_singles = round_singles_;
+    rec.rebuilds = (uint32_t)info.rebuilds;
     std::lock_guard<std::mutex> lk(mu_);
+    rec.t_start_ms = t0 - t0_;
+    if (trace_.size() < kTrace) trace_.push_back(rec);
+    else trace_[trace_next_ % kTrace] = rec;
+    trace_next_++;
     rebuilds_ += info.rebuilds;
     if (info.ms > worst_.ms) worst_ = info;
   }
@@ -629,14 +665,19 @@ class Server {
       }
       if (bad) {  // the group's valid sources run one by one
         for (Request *r : grp) {
-          if (r->param >= n) r->status = TRC_ERR_INVALID;
-          else bfs_one(r, full);
+          if (r->param >= n) {
+            r->status = TRC_ERR_INVALID;
+          } else {
+            bfs_one(r, full);
+            round_singles_++;
+          }
         }
       } else if (cfg_.mode == TRC_SERVE_FIFO || !group_pays(k)) {
         // one by one, each request completing when its traversal ends
         for (Request *r : grp) {
           const double t0 = now_ms();
           bfs_one(r, full);
+          round_singles_++;
           ewma(bfs1_ms_, now_ms() - t0);
           std::vector<Request *> one{r};
           finish(one);
@@ -661,6 +702,7 @@ class Server {
           }
         }
         calls_++;
+        round_groups_++;
         ewma(msb_per_ms_[size_class(k)], (now_ms() - t0) / (double)k);
       }
       finish(grp);
@@ -959,6 +1001,14 @@ trc_status trc_server_reset_stats(trc_server *s) {
 
 trc_status trc_server_hold(trc_server *s, int hold) {
   return sguard([&] { S(s).hold(hold != 0); });
+}
+
+trc_status trc_server_rounds(trc_server *s, trc_round_record *out, uint64_t cap, uint64_t *count) {
+  return sguard([&] {
+    if (!out && cap) trc::throw_error(TRC_ERR_INVALID, "null output");
+    const uint64_t c = S(s).rounds_trace(out, cap);
+    if (count) *count = c;
+  });
 }
 
 }  // extern "C"

@@ -190,6 +190,28 @@ __device__ __forceinline__ void hub_chunk(const NbrList &L, uint32_t c, const ui
   len = off < ulen ? (ulen - off < 32 ? ulen - off : 32) : 0;
 }
 
+// Any list as pieces of at most 32 elements, for traversals that need no
+// order: a hub's pieces are its hub_chunk()s; a tier-1/2 vertex has piece 0
+// = the inline row, then 32-element pieces of its segment.  Every list has
+// at least one piece (possibly empty).
+__device__ __forceinline__ uint32_t list_pieces(const NbrList &L) {
+  return L.nb ? hub_chunks(L) : 1 + (L.rest + 31) / 32;
+}
+
+__device__ __forceinline__ void list_piece(const NbrList &L, uint32_t c, const uint32_t *&p,
+                                           uint32_t &len) {
+  if (L.nb) {
+    hub_chunk(L, c, p, len);
+  } else if (c == 0) {
+    p = L.inl;
+    len = L.ni;
+  } else {
+    const uint32_t off = (c - 1) * 32;
+    p = L.seg + off;
+    len = L.rest - off < 32 ? L.rest - off : 32;
+  }
+}
+
 // Binary search for x in the neighbour list (lists are sorted, unique); a
 // hub's blocked part is searched through its directory's first keys.
 __device__ __forceinline__ bool list_has(const NbrList &L, uint32_t x) {
@@ -376,5 +398,15 @@ inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
 
 // Number of SMs on the current device (cached).
 int num_sms();
+// CTAs of `threads` threads (and `smem` dynamic shared bytes) of `kernel`
+// that fit on the whole GPU at once: the grid of a grid-stride kernel.
+template <typename K>
+unsigned resident_grid(K kernel, int threads, size_t smem = 0) {
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess ||
+      per < 1)
+    per = 1;
+  return (unsigned)(per * num_sms());
+}
 
 }  // namespace trc

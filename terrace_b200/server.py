@@ -98,6 +98,15 @@ class Server:
         L.check(self._L.trc_server_get_stats(self._h, kind, C.byref(s)))
         return {k: getattr(s, k) for k, _ in L.trc_server_stats._fields_}
 
+    def rounds(self) -> list:
+        """The per-round trace (trc_server_rounds), oldest first, as dicts."""
+        cnt = C.c_uint64()
+        L.check(self._L.trc_server_rounds(self._h, None, 0, C.byref(cnt)))
+        buf = (L.trc_round_record * max(cnt.value, 1))()
+        L.check(self._L.trc_server_rounds(self._h, buf, cnt.value, C.byref(cnt)))
+        return [{k: getattr(r, k) for k, _ in L.trc_round_record._fields_}
+                for r in buf[:cnt.value]]
+
     def reset_stats(self):
         L.check(self._L.trc_server_reset_stats(self._h))
 

@@ -205,6 +205,10 @@ def test_large_round_wide_vertex_ids():
         assert ver == 1  # one round, one net change
         srv.release(rid)
     assert srv.stats()["rounds"] == 1
+    tr = srv.rounds()
+    assert len(tr) == 1 and tr[0]["updates"] == 300 and tr[0]["bfs"] == 0
+    assert tr[0]["update_pairs"] == sum(len(a) for _, a, _ in reqs)
+    assert tr[0]["ms"] >= tr[0]["update_ms"] > 0
     srv.close()
     keys = np.zeros(0, np.uint64)
     for op, a, b in reqs:
