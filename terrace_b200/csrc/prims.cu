@@ -216,7 +216,10 @@ uint64_t *radix_sort_u64_shifts(uint64_t *keys, uint64_t *alt, uint64_t n, const
 namespace {
 
 constexpr uint64_t BK_INVALID = ~0ull;
-constexpr uint32_t BK_MID = 1024;  // buckets of 33..BK_MID keys: a warp in shared memory
+constexpr uint32_t BK_MID = 256;   // 33..BK_MID keys: a warp in shared memory
+constexpr uint32_t BK_BIG = 2048;  // BK_MID+1..BK_BIG: a CTA in static shared memory
+                                   // above: a CTA in dynamic shared memory
+constexpr uint32_t BK_NONE = 0xFFFFFFFFu;
 
 struct BucketArgs {
   uint32_t nb;     // valid buckets; bucket nb holds the invalid keys
@@ -226,10 +229,15 @@ struct BucketArgs {
   }
 };
 
+// Counting and scattering use one atomic per distinct bucket of a warp
+// (match_any), so the skewed sources of RMAT-like batches do not serialise
+// on their counters.
 __global__ void k_bucket_hist(const uint64_t *keys, uint64_t k, BucketArgs ba, uint32_t *cnt) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= k) return;
-  atomicAdd(cnt + ba.of(keys[i]), 1u);
+  const uint32_t b = i < k ? ba.of(keys[i]) : BK_NONE;
+  const uint32_t same = __match_any_sync(0xFFFFFFFFu, b);
+  if (b != BK_NONE && (threadIdx.x & 31) == (uint32_t)(__ffs(same) - 1))
+    atomicAdd(cnt + b, (uint32_t)__popc(same));
 }
 
 struct LoadCnt32 {
@@ -240,10 +248,15 @@ struct LoadCnt32 {
 __global__ void k_bucket_scatter(const uint64_t *keys, uint64_t k, BucketArgs ba,
                                  const uint64_t *off, uint32_t *fill, uint64_t *out) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= k) return;
-  const uint64_t x = keys[i];
-  const uint32_t b = ba.of(x);
-  out[off[b] + atomicAdd(fill + b, 1u)] = x;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t x = i < k ? keys[i] : 0;
+  const uint32_t b = i < k ? ba.of(x) : BK_NONE;
+  const uint32_t same = __match_any_sync(0xFFFFFFFFu, b);
+  const uint32_t leader = __ffs(same) - 1;
+  uint32_t base = 0;
+  if (b != BK_NONE && lane == leader) base = atomicAdd(fill + b, (uint32_t)__popc(same));
+  base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  if (b != BK_NONE) out[off[b] + base + __popc(same & ((1u << lane) - 1))] = x;
 }
 
 // Ascending bitonic network over the 32 lanes of a warp, one value per lane.
@@ -311,18 +324,24 @@ __device__ __forceinline__ void thread_bucket_sort(uint64_t *keys, uint64_t base
 
 // A thread per bucket: buckets of 2..16 keys sorted in the thread's
 // registers (network size by the warp's largest such bucket), 17..32 by the
-// whole warp; larger ones listed for the shared-memory kernels (by size);
-// those above BUCKET_SEG_MAX flagged.
+// whole warp; larger ones listed by size for the shared-memory kernels;
+// those above BUCKET_SEG_MAX flagged.  lists: 3 lists of `cap` entries,
+// nlist their 3 counts.
 __global__ void k_bucket_sort_small(const uint64_t *off, uint32_t nb, uint64_t *keys,
-                                    uint32_t *mid, uint32_t *big, unsigned long long *nlist,
+                                    uint32_t *lists, uint64_t cap, unsigned long long *nlist,
                                     uint32_t *err) {
   const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t base = b < nb ? off[b] : 0;
   const uint32_t c = b < nb ? (uint32_t)(off[b + 1] - base) : 0u;
-  if (c > 32 && c <= BK_MID) mid[atomicAdd(nlist, 1ull)] = (uint32_t)b;
-  if (c > BK_MID && c <= BUCKET_SEG_MAX) big[atomicAdd(nlist + 1, 1ull)] = (uint32_t)b;
-  if (c > BUCKET_SEG_MAX) atomicOr(err, ERR_BIGSEG);
+  if (c > 32) {
+    if (c > BUCKET_SEG_MAX) {
+      atomicOr(err, ERR_BIGSEG);
+    } else {
+      const int t = c <= BK_MID ? 0 : c <= BK_BIG ? 1 : 2;
+      lists[t * cap + atomicAdd(nlist + t, 1ull)] = (uint32_t)b;
+    }
+  }
   const uint32_t ct = (c >= 2 && c <= 16) ? c : 0u;
   const uint32_t wmax = __reduce_max_sync(0xFFFFFFFFu, ct);
   if (ct) {
@@ -346,17 +365,17 @@ __global__ void k_bucket_sort_small(const uint64_t *off, uint32_t nb, uint64_t *
 }
 
 // A warp per listed bucket of 33..BK_MID keys, sorted in shared memory.
-constexpr uint32_t BK_MID_WARPS = 4;
+constexpr uint32_t BK_MID_WARPS = 8;
 __global__ void __launch_bounds__(BK_MID_WARPS * 32)
-    k_bucket_sort_mid(const uint64_t *off, const uint32_t *mid, const unsigned long long *nlist,
+    k_bucket_sort_mid(const uint64_t *off, const uint32_t *list, const unsigned long long *nlist,
                       uint64_t *keys) {
   __shared__ uint64_t sv[BK_MID_WARPS][BK_MID];
   const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint64_t *v = sv[w];
-  const uint64_t nm = nlist[0];
+  const uint64_t nm = *nlist;
   for (uint64_t i = (uint64_t)blockIdx.x * BK_MID_WARPS + w; i < nm;
        i += (uint64_t)gridDim.x * BK_MID_WARPS) {
-    const uint32_t b = mid[i];
+    const uint32_t b = list[i];
     const uint64_t base = off[b];
     const uint32_t c = (uint32_t)(off[b + 1] - base);
     uint32_t P = 64;
@@ -369,24 +388,26 @@ __global__ void __launch_bounds__(BK_MID_WARPS * 32)
   }
 }
 
-// A CTA per listed bucket of BK_MID+1..BUCKET_SEG_MAX keys, sorted in
-// (dynamic) shared memory.
-constexpr uint32_t BK_BIG_T = 1024;
-__global__ void __launch_bounds__(BK_BIG_T)
-    k_bucket_sort_big(const uint64_t *off, const uint32_t *big, const unsigned long long *nlist,
+// A CTA per listed bucket of more than BK_MID keys (at most PMAX), sorted in
+// shared memory: static for PMAX = BK_BIG, dynamic otherwise.
+template <uint32_t PMAX, uint32_t NT>
+__global__ void __launch_bounds__(NT)
+    k_bucket_sort_cta(const uint64_t *off, const uint32_t *list, const unsigned long long *nlist,
                       uint64_t *keys) {
-  extern __shared__ uint64_t sbig[];
-  const uint64_t nbg = nlist[1];
+  __shared__ uint64_t sstat[PMAX <= BK_BIG ? PMAX : 1];
+  extern __shared__ uint64_t sdyn[];
+  uint64_t *v = PMAX <= BK_BIG ? sstat : sdyn;
+  const uint64_t nbg = *nlist;
   for (uint64_t i = blockIdx.x; i < nbg; i += gridDim.x) {
-    const uint32_t b = big[i];
+    const uint32_t b = list[i];
     const uint64_t base = off[b];
     const uint32_t c = (uint32_t)(off[b + 1] - base);
     uint32_t P = 2 * BK_MID;
     while (P < c) P <<= 1;
-    for (uint32_t t = threadIdx.x; t < P; t += blockDim.x) sbig[t] = t < c ? keys[base + t] : BK_INVALID;
+    for (uint32_t t = threadIdx.x; t < P; t += NT) v[t] = t < c ? keys[base + t] : BK_INVALID;
     __syncthreads();
-    smem_bitonic(sbig, P, threadIdx.x, blockDim.x, [] { __syncthreads(); });
-    for (uint32_t t = threadIdx.x; t < c; t += blockDim.x) keys[base + t] = sbig[t];
+    smem_bitonic(v, P, threadIdx.x, NT, [] { __syncthreads(); });
+    for (uint32_t t = threadIdx.x; t < c; t += NT) keys[base + t] = v[t];
     __syncthreads();
   }
 }
@@ -395,21 +416,20 @@ struct BucketLayout {
   uint32_t nb, shift;
   uint64_t list_cap;
   uint64_t cnt_w, off_w, scan_w, list_w;  // words of each part
-  uint64_t total() const { return 2 * cnt_w + off_w + scan_w + 2 * list_w + 2; }
+  uint64_t total() const { return 2 * cnt_w + off_w + scan_w + list_w + 3; }
 };
 
 BucketLayout bucket_layout(uint64_t k, uint32_t n) {
   BucketLayout L{};
-  // about BUCKET_TARGET keys per bucket: bucket = source >> shift
-  constexpr uint64_t BUCKET_TARGET = 4;
+  // at most one bucket per key: bucket = source >> shift
   L.shift = 0;
-  while (L.shift < 31 && ceil_div((uint64_t)n, 1ull << L.shift) * BUCKET_TARGET > k) L.shift++;
+  while (L.shift < 31 && ceil_div((uint64_t)n, 1ull << L.shift) > k) L.shift++;
   L.nb = (uint32_t)ceil_div((uint64_t)n, 1ull << L.shift);
   L.list_cap = std::min<uint64_t>(L.nb, k / 33) + 1;
   L.cnt_w = ceil_div((uint64_t)L.nb + 1, 2);
   L.off_w = (uint64_t)L.nb + 1;
   L.scan_w = scan_tmp_elems((uint64_t)L.nb + 1) + 4;
-  L.list_w = ceil_div(L.list_cap, 2);
+  L.list_w = ceil_div(3 * L.list_cap, 2);
   return L;
 }
 
@@ -426,26 +446,26 @@ uint64_t *bucket_sort_u64(const uint64_t *keys, uint64_t *alt, uint64_t k, uint3
   uint32_t *fill = reinterpret_cast<uint32_t *>(tmp + L.cnt_w);
   uint64_t *off = tmp + 2 * L.cnt_w;
   uint64_t *st = off + L.off_w;
-  uint32_t *mid = reinterpret_cast<uint32_t *>(st + L.scan_w);
-  uint32_t *big = reinterpret_cast<uint32_t *>(st + L.scan_w + L.list_w);
-  unsigned long long *nlist =
-      reinterpret_cast<unsigned long long *>(st + L.scan_w + 2 * L.list_w);
+  uint32_t *lists = reinterpret_cast<uint32_t *>(st + L.scan_w);
+  unsigned long long *nlist = reinterpret_cast<unsigned long long *>(st + L.scan_w + L.list_w);
   TRC_CUDA(cudaMemsetAsync(tmp, 0, 2 * L.cnt_w * 8, s));  // cnt and fill
-  TRC_CUDA(cudaMemsetAsync(nlist, 0, 16, s));
+  TRC_CUDA(cudaMemsetAsync(nlist, 0, 3 * 8, s));
   TRC_LAUNCH(prof, s, "bsort_hist", ceil_div(k, 256), 256, 0, k_bucket_hist, keys, k, ba, cnt);
   exclusive_scan(LoadCnt32{cnt}, (uint64_t)L.nb + 1, off, st, s, prof, "bsort_scan");
   TRC_LAUNCH(prof, s, "bsort_scatter", ceil_div(k, 256), 256, 0, k_bucket_scatter, keys, k, ba,
              off, fill, alt);
   TRC_LAUNCH(prof, s, "bsort_small", ceil_div((uint64_t)L.nb, 256), 256, 0, k_bucket_sort_small,
-             off, L.nb, alt, mid, big, nlist, err);
+             off, L.nb, alt, lists, L.list_cap, nlist, err);
   const unsigned sms = (unsigned)num_sms();
-  TRC_LAUNCH(prof, s, "bsort_mid", sms * 8, BK_MID_WARPS * 32, 0, k_bucket_sort_mid, off, mid,
+  TRC_LAUNCH(prof, s, "bsort_mid", sms * 4, BK_MID_WARPS * 32, 0, k_bucket_sort_mid, off, lists,
              nlist, alt);
-  const int big_smem = (int)(BUCKET_SEG_MAX * sizeof(uint64_t));
-  TRC_CUDA(cudaFuncSetAttribute(k_bucket_sort_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                big_smem));
-  TRC_LAUNCH(prof, s, "bsort_big", sms, BK_BIG_T, big_smem, k_bucket_sort_big, off, big, nlist,
-             alt);
+  TRC_LAUNCH(prof, s, "bsort_big", sms * 4, 256, 0, (k_bucket_sort_cta<BK_BIG, 256>), off,
+             lists + L.list_cap, nlist + 1, alt);
+  const int huge_smem = (int)(BUCKET_SEG_MAX * sizeof(uint64_t));
+  TRC_CUDA(cudaFuncSetAttribute(k_bucket_sort_cta<BUCKET_SEG_MAX, 1024>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, huge_smem));
+  TRC_LAUNCH(prof, s, "bsort_huge", sms, 1024, huge_smem, (k_bucket_sort_cta<BUCKET_SEG_MAX, 1024>),
+             off, lists + 2 * L.list_cap, nlist + 2, alt);
   return alt;
 }
 

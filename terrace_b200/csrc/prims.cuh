@@ -261,15 +261,16 @@ uint64_t radix_tmp_elems(uint64_t n);
 // ------------------------------------------------------------ bucket sort
 // Sorts k keys (src<<32|dst with src < n, or KEY_INVALID = ~0) ascending:
 // keys are bucketed on the source's high bits (bucket = src >> shift, with
-// shift chosen for about four keys per bucket; a count per bucket, a scan,
-// an atomic scatter), then each bucket is sorted whole (up to 32 keys in a
-// warp's registers, up to 1024 in a warp's shared memory, up to
-// BUCKET_SEG_MAX by a CTA).  O(n >> shift + k) traffic in 6-7 launches: for
-// batches of more than a few thousand keys it moves far fewer bytes than the
-// radix sort's passes.  A bucket above BUCKET_SEG_MAX keys is left unsorted
-// and ERR_BIGSEG or-ed into err: the caller must then sort with the radix
-// sort instead.  Writes the sorted keys to alt (keys is left unchanged) and
-// returns alt.  tmp: bucket_tmp_elems(k, n) entries.
+// the smallest shift that leaves at most one bucket per key; a count per
+// bucket, a scan, a scatter, both with one atomic per distinct bucket of a
+// warp), then each bucket is sorted whole (up to 16 keys in a thread's
+// registers, up to 32 across a warp, up to 256 in a warp's shared memory,
+// up to BUCKET_SEG_MAX by a CTA).  O(n >> shift + k) traffic in about 8
+// launches: for batches of more than a few thousand keys it moves far fewer
+// bytes than the radix sort's passes.  A bucket above BUCKET_SEG_MAX keys is
+// left unsorted and ERR_BIGSEG or-ed into err: the caller must then sort
+// with the radix sort instead.  Writes the sorted keys to alt (keys is left
+// unchanged) and returns alt.  tmp: bucket_tmp_elems(k, n) entries.
 constexpr uint32_t BUCKET_SEG_MAX = 16384;
 uint64_t *bucket_sort_u64(const uint64_t *keys, uint64_t *alt, uint64_t k, uint32_t n,
                           uint64_t *tmp, cudaStream_t s, Profiler &prof, uint32_t *err);
