@@ -548,11 +548,16 @@ struct BFSState {
   uint32_t *next_cnt;
   uint32_t d;            // current level
   // dense steps: vertices left unvisited by the inline pass that have a
-  // PMA segment (seg), and vertices left unvisited by the step (cand, the
-  // next dense step's candidates); push steps: the frontier's hubs (seg)
+  // PMA segment (seg: at most BFS_SHORT neighbours, seg2: more), and
+  // vertices left unvisited by the step (cand, the next dense step's
+  // candidates)
   uint32_t *seg, *seg_cnt;
   uint32_t *cand, *cand_cnt;
+  uint32_t *seg2, *seg2_cnt;
 };
+
+// Degree bound of the short segment list (8 lanes per vertex).
+constexpr uint32_t BFS_SHORT = 64;
 
 __device__ __forceinline__ bool bit_test(const uint32_t *b, uint32_t v) {
   return (__ldg(b + (v >> 5)) >> (v & 31)) & 1u;
@@ -668,8 +673,8 @@ constexpr uint32_t BP_V = 4;
 __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S, uint64_t nS,
                                                    BFSState s) {
   const uint32_t lane = threadIdx.x & 31, q = lane & 3, qw = lane >> 2, wib = threadIdx.x >> 5;
-  __shared__ uint32_t stg[3][AT / 32][32];
-  WarpStage sn{stg[0][wib], 0}, ss{stg[1][wib], 0}, sc{stg[2][wib], 0};
+  __shared__ uint32_t stg[4][AT / 32][32];
+  WarpStage sn{stg[0][wib], 0}, ss{stg[1][wib], 0}, sc{stg[2][wib], 0}, sl{stg[3][wib], 0};
   const uint64_t step = (((uint64_t)gridDim.x * AT) >> 5) * (8 * BP_V);
   for (uint64_t wbase = (((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5) * (8 * BP_V); wbase < nS;
        wbase += step) {
@@ -720,12 +725,14 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
       }
       const bool left = q == 0 && uv && grp == 0;
       sn.add(win, u[i], s.next, s.next_cnt, lane);
-      ss.add(left && d[i] > K_INLINE, u[i], s.seg, s.seg_cnt, lane);
+      ss.add(left && d[i] > K_INLINE && d[i] <= BFS_SHORT, u[i], s.seg, s.seg_cnt, lane);
+      sl.add(left && d[i] > BFS_SHORT, u[i], s.seg2, s.seg2_cnt, lane);
       sc.add(left && d[i] <= K_INLINE, u[i], s.cand, s.cand_cnt, lane);
     }
   }
   sn.flush(s.next, s.next_cnt, lane);
   ss.flush(s.seg, s.seg_cnt, lane);
+  sl.flush(s.seg2, s.seg2_cnt, lane);
   sc.flush(s.cand, s.cand_cnt, lane);
 }
 
@@ -808,6 +815,51 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_W(DevView G, const uint32_t *Ls
   if (keep) bl.flush(s.cand, s.cand_cnt, lane);
 }
 
+// Segment pass for the short list (K_INLINE < degree <= BFS_SHORT, no
+// hubs): 8 lanes per vertex, 4 vertices per warp step; lane q checks ranks
+// 16 + q + 8t (t < 6), every segment load and then every bitmap load issued
+// before any is used.  The lowest lane of the group with a frontier
+// neighbour sets the parent; vertices without one join the candidates.
+__global__ void __launch_bounds__(AT) k_bfs_pull_G8(DevView G, const uint32_t *Lst,
+                                                    const uint32_t *nL_dev, BFSState s) {
+  constexpr uint32_t R = (BFS_SHORT - K_INLINE) / 8;
+  const uint32_t lane = threadIdx.x & 31, q = lane & 7, grp = lane >> 3, wib = threadIdx.x >> 5;
+  __shared__ uint32_t stg[2][AT / 32][32];
+  WarpStage sn{stg[0][wib], 0}, sc{stg[1][wib], 0};
+  const uint64_t nL = *nL_dev;
+  const uint64_t step = (((uint64_t)gridDim.x * AT) >> 5) * 4;
+  for (uint64_t base = (((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5) * 4; base < nL;
+       base += step) {
+    const uint64_t vi = base + grp;
+    const bool act = vi < nL;
+    const uint32_t u = act ? Lst[vi] : 0u;
+    const uint32_t d = act ? G.deg[u] : 0u;
+    const uint32_t *seg = G.pma + (act ? G.pbeg[u] : 0) - K_INLINE;  // indexed by rank
+    uint32_t x[R], w[R];
+#pragma unroll
+    for (uint32_t t = 0; t < R; t++) {
+      const uint32_t j = K_INLINE + q + 8 * t;
+      x[t] = j < d ? __ldcs(seg + j) : NONE32;
+    }
+#pragma unroll
+    for (uint32_t t = 0; t < R; t++) w[t] = x[t] != NONE32 ? __ldg(s.bits + (x[t] >> 5)) : 0u;
+    uint32_t p = NONE32;
+#pragma unroll
+    for (uint32_t t = 0; t < R; t++)
+      if (p == NONE32 && x[t] != NONE32 && ((w[t] >> (x[t] & 31)) & 1u)) p = x[t];
+    const uint32_t m = (__ballot_sync(0xFFFFFFFFu, p != NONE32) >> (grp * 8)) & 0xFFu;
+    const bool win = m && (uint32_t)(__ffs(m) - 1) == q;
+    if (win) {
+      s.par[u] = (int32_t)p;
+      s.lv[u] = s.d + 1;
+    }
+    sn.add(win, u, s.next, s.next_cnt, lane);
+    sc.add(act && q == 0 && m == 0, u, s.cand, s.cand_cnt, lane);
+  }
+  sn.flush(s.next, s.next_cnt, lane);
+  sc.flush(s.cand, s.cand_cnt, lane);
+}
+
 __global__ void k_bfs_init(uint32_t *lv, int32_t *par, uint32_t n, uint32_t src, uint32_t *q) {
   uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= n) return;
@@ -837,11 +889,12 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
   const uint64_t dense_at = n / push_pull_divisor();
   // candidates of the dense steps: non-hub vertices not yet visited,
   // compacted after every dense step
-  DBuf<uint32_t> cbuf[2], segb;  // candidate ping-pong, segment-pass list
+  DBuf<uint32_t> cbuf[2], segb, seg2b;  // candidate ping-pong, segment-pass lists
   DBuf<uint64_t> offb, scanb;     // push steps: piece prefix and scan scratch
   cbuf[0].bind(&budget);
   cbuf[1].bind(&budget);
   segb.bind(&budget);
+  seg2b.bind(&budget);
   offb.bind(&budget);
   scanb.bind(&budget);
   // (the first dense step reads every vertex id in order, no list: its
@@ -849,26 +902,29 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
   const uint32_t *cand = nullptr;
   uint64_t ncand = n;
   int cnext = 0;
-  uint32_t *sg = segb.ensure(n);
+  uint32_t *sg = segb.ensure(n), *sg2 = seg2b.ensure(n);
   const unsigned pgrid = (unsigned)num_sms() * 8;
   while (nf > 0) {
     TRC_CUDA(cudaMemsetAsync(c, 0, 16, stream));  // next, seg, cand counts
-    BFSState s{lv, par, bm, Nx, c, d, sg, c + 1, nullptr, c + 2};
+    BFSState s{lv, par, bm, Nx, c, d, sg, c + 1, nullptr, c + 2, sg2, c + 3};
     uint32_t hc[3] = {0, 0, 0};
     if ((uint64_t)nf >= dense_at && dense_at > 0) {
       TRC_LAUNCH(prof, stream, "bfs_bits", ceil_div(n, AT), AT, 0, k_level_bits, lv, n, d, bm);
       // candidates left for the next dense step (never the list being read)
       s.cand = cbuf[cnext].ensure(ncand ? ncand : 1);
       // pass A: the 16 inline neighbours of every unvisited non-hub vertex;
-      // those left unvisited go to the segment list (PMA vertices) or the
-      // next candidates
+      // those left unvisited go to a segment list (PMA vertices: short or
+      // long) or the next candidates
       TRC_LAUNCH(prof, stream, "bfs_pull_inline",
                  std::min<uint64_t>(ceil_div(ncand * 4, (uint64_t)AT * BP_V),
                                     resident_grid(k_bfs_pull_S, AT)),
                  AT, 0, k_bfs_pull_S, G, cand, ncand, s);
-      // pass B: the PMA segments of the segment list (count on the device);
-      // hubs from rank 0
-      TRC_LAUNCH(prof, stream, "bfs_pull_M", pgrid, AT, 0, k_bfs_pull_W, G, sg, 0, c + 1, s,
+      // pass B: the PMA segments of the segment lists (counts on the
+      // device; short lists 8 lanes per vertex, long ones a warp); hubs
+      // from rank 0
+      TRC_LAUNCH(prof, stream, "bfs_pull_M8", resident_grid(k_bfs_pull_G8, AT), AT, 0,
+                 k_bfs_pull_G8, G, sg, c + 1, s);
+      TRC_LAUNCH(prof, stream, "bfs_pull_M", pgrid, AT, 0, k_bfs_pull_W, G, sg2, 0, c + 3, s,
                  K_INLINE, 1);
       TRC_LAUNCH(prof, stream, "bfs_pull_H", ceil_div(lists.nH * 32, AT), AT, 0, k_bfs_pull_W, G,
                  lists.Hv.get(), lists.nH, (const uint32_t *)nullptr, s, 0u, 0);
