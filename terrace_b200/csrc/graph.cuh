@@ -160,6 +160,10 @@ class Graph {
                  uint64_t *reached, uint32_t *ecc);
   // up to 64 BC at once, out[i*n + v] (msbfs.cu)
   void msbc(const uint32_t *sources, uint32_t k, double *out, uint32_t flags);
+  // one edge-balanced push level of msbfs / msbc (msbfs.cu)
+  void ms_push_level(const uint32_t *F, uint32_t nf, const uint64_t *front, const uint64_t *seen,
+                     unsigned long long *acc, uint32_t *T, uint32_t *tcnt, DBuf<uint64_t> &offb,
+                     DBuf<uint64_t> &scanb);
   // BFS with scratch in a static device array (no allocation), noalloc.cu
   void bfs_noalloc(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags);
   uint32_t *na_scratch = nullptr;  // that array's device address on this graph's device

@@ -149,22 +149,20 @@ __global__ void __launch_bounds__(MT) k_ms_pull_W(DevView G, const uint32_t *V, 
 }
 
 // push: every vertex of the active list ORs its front mask into its
-// neighbours' accumulators (warp per active vertex), skipping neighbours
-// that every source in the mask has already seen.  The first OR into an
-// accumulator appends the neighbour to the touched list T.  The warp clears
-// front[u] after reading it (nothing else reads front in a push level), so
-// that front is all-zero when the level ends.
-// One 32-neighbour chunk of a pushing vertex with source mask m.
-// (p, len): a hub piece (hub_chunk), read directly; otherwise ranks j0 ..
-__device__ __forceinline__ void ms_push_chunk(const NbrList &L, uint64_t m, uint32_t j0,
+// neighbours' accumulators, skipping neighbours that every source in the
+// mask has already seen.  The first OR into an accumulator appends the
+// neighbour to the touched list T.  Edge-balanced: the active lists are cut
+// into list_piece()s (off = exclusive prefix of the piece counts) and every
+// warp of the grid takes an equal share of them.  front is left as it is
+// (cleared after the level).
+// One piece (p, len) of a pushing vertex with source mask m.
+__device__ __forceinline__ void ms_push_piece(const uint32_t *p, uint32_t len, uint64_t m,
                                               const uint64_t *seen, unsigned long long *acc,
-                                              uint32_t *T, uint32_t *tcnt, uint32_t lane,
-                                              const uint32_t *p = nullptr, uint32_t len = 0) {
-  const uint32_t j = j0 + lane;
+                                              uint32_t *T, uint32_t *tcnt, uint32_t lane) {
   uint32_t x = 0;
   bool first = false;
-  if (p ? lane < len : j < L.deg) {
-    x = p ? p[lane] : L.at(j);
+  if (lane < len) {
+    x = p[lane];
     if ((m & ~seen[x]) != 0) first = atomicOr(acc + x, (unsigned long long)m) == 0;
   }
   const uint32_t b = __ballot_sync(0xFFFFFFFFu, first);
@@ -176,56 +174,49 @@ __device__ __forceinline__ void ms_push_chunk(const NbrList &L, uint64_t m, uint
   if (first) T[base + __popc(b & lanemask_lt())] = x;
 }
 
-// Warp per active vertex; hubs are listed (with their masks) for
-// k_ms_push_hubs.
-__global__ void k_ms_push(DevView G, const uint32_t *F, uint32_t nf, uint64_t *front,
-                          const uint64_t *seen, unsigned long long *acc, uint32_t *T,
-                          uint32_t *tcnt, uint32_t *hu, uint64_t *hm, uint32_t *hcnt) {
-  uint64_t w = ((uint64_t)blockIdx.x * MT + threadIdx.x) >> 5;
-  uint32_t lane = threadIdx.x & 31;
-  if (w >= nf) return;
-  uint32_t u = F[w];
-  uint64_t m = front[u];
-  __syncwarp();
-  if (lane == 0) front[u] = 0;
-  if (G.hub_of[u] >= 0) {
-    if (lane == 0) {
-      const uint32_t i = atomicAdd(hcnt, 1u);
-      hu[i] = u;
-      hm[i] = m;
-    }
-    return;
+struct MsPieces {
+  DevView G;
+  const uint32_t *F;
+  uint64_t nf;
+  __device__ uint64_t operator()(uint64_t i) const {
+    return i < nf ? list_pieces(nbr_list(G, F[i])) : 0;
   }
-  NbrList L = nbr_list(G, u);
-  for (uint32_t j0 = 0; j0 < L.deg; j0 += 32) ms_push_chunk(L, m, j0, seen, acc, T, tcnt, lane);
-}
+};
 
-// The listed hubs: the first 64 spread over the grid, the rest a CTA each.
-__global__ void k_ms_push_hubs(DevView G, const uint32_t *hu, const uint64_t *hm,
-                               const uint32_t *hcnt, const uint64_t *seen,
-                               unsigned long long *acc, uint32_t *T, uint32_t *tcnt) {
-  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint64_t gw = ((uint64_t)blockIdx.x * MT + threadIdx.x) >> 5;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * MT) >> 5;
-  const uint64_t nh = *hcnt;
-  const uint64_t nwide = nh < 64 ? nh : 64;
-  const uint32_t *p;
-  uint32_t len;
-  for (uint64_t i = 0; i < nwide; i++) {
-    NbrList L = nbr_list(G, hu[i]);
-    const uint64_t nch = hub_chunks(L);
-    for (uint64_t c = gw; c < nch; c += nwarps) {
-      hub_chunk(L, (uint32_t)c, p, len);
-      if (len) ms_push_chunk(L, hm[i], 0, seen, acc, T, tcnt, lane, p, len);
-    }
+__global__ void __launch_bounds__(MT) k_ms_push(DevView G, const uint32_t *F, uint32_t nf,
+                                                const uint64_t *off, const uint64_t *front,
+                                                const uint64_t *seen, unsigned long long *acc,
+                                                uint32_t *T, uint32_t *tcnt) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t W = ((uint64_t)gridDim.x * MT) >> 5;
+  const uint64_t w = ((uint64_t)blockIdx.x * MT + threadIdx.x) >> 5;
+  const uint64_t Tn = off[nf];
+  const uint64_t lo = Tn * w / W, hi = Tn * (w + 1) / W;
+  if (lo >= hi) return;
+  // the vertex of piece lo: the i with off[i] <= lo < off[i+1]
+  uint32_t a = 0, b = nf;
+  while (b - a > 1) {
+    const uint32_t mid = (a + b) >> 1;
+    if (off[mid] <= lo) a = mid;
+    else b = mid;
   }
-  for (uint64_t i = nwide + blockIdx.x; i < nh; i += gridDim.x) {
-    NbrList L = nbr_list(G, hu[i]);
-    const uint32_t nch = hub_chunks(L);
-    for (uint32_t c = wib; c < nch; c += MT / 32) {
-      hub_chunk(L, c, p, len);
-      if (len) ms_push_chunk(L, hm[i], 0, seen, acc, T, tcnt, lane, p, len);
+  uint32_t i = a, u = F[i];
+  uint64_t m = front[u];
+  NbrList L = nbr_list(G, u);
+  uint64_t vbeg = off[i], vend = off[i + 1];
+  for (uint64_t t = lo; t < hi; t++) {
+    while (t >= vend) {  // (t < off[nf], so i + 1 < nf here)
+      i++;
+      u = F[i];
+      m = front[u];
+      L = nbr_list(G, u);
+      vbeg = vend;
+      vend = off[i + 1];
     }
+    const uint32_t *p;
+    uint32_t len;
+    list_piece(L, (uint32_t)(t - vbeg), p, len);
+    if (len) ms_push_piece(p, len, m, seen, acc, T, tcnt, lane);  // (warp-uniform)
   }
 }
 
@@ -461,6 +452,17 @@ __global__ void k_mbc_final(const double *dep, const double *sigma, uint32_t n, 
 }
 }  // namespace
 
+void Graph::ms_push_level(const uint32_t *F, uint32_t nf, const uint64_t *front,
+                          const uint64_t *seen, unsigned long long *acc, uint32_t *T,
+                          uint32_t *tcnt, DBuf<uint64_t> &offb, DBuf<uint64_t> &scanb) {
+  uint64_t *off = offb.ensure((uint64_t)nf + 1);
+  uint64_t *stmp = scanb.ensure(scan_tmp_elems((uint64_t)nf + 1) + 4);
+  const DevView G = view();
+  exclusive_scan(MsPieces{G, F, nf}, (uint64_t)nf + 1, off, stmp, stream, prof, "ms_push_scan");
+  TRC_LAUNCH(prof, stream, "ms_push", (unsigned)num_sms() * 8, MT, 0, k_ms_push, G, F, nf, off,
+             front, seen, acc, T, tcnt);
+}
+
 void Graph::msbfs(const uint32_t *sources, uint32_t k, uint32_t *levels, uint32_t flags) {
   if (!levels) throw_error(TRC_ERR_INVALID, "null pointer");
   msbfs_run(sources, k, levels, flags, nullptr, nullptr);
@@ -510,12 +512,9 @@ void Graph::msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uin
   uint32_t *L[2] = {lst.alloc_exact(n), lst2.alloc_exact(n)};
   uint32_t *T = tl.alloc_exact(n);
   uint32_t *c = cnt.alloc_exact(4);  // [1] next active, [2] touched, [3] pushing hubs
-  DBuf<uint32_t> hub_u;
-  DBuf<uint64_t> hub_m;
-  hub_u.bind(&budget);
-  hub_m.bind(&budget);
-  uint32_t *hu = hub_u.alloc_exact(H ? H : 1);  // hubs of a push level and their masks
-  uint64_t *hm = hub_m.alloc_exact(H ? H : 1);
+  DBuf<uint64_t> offb, scanb;  // push levels: piece prefix and scan scratch
+  offb.bind(&budget);
+  scanb.bind(&budget);
   TRC_CUDA(cudaMemcpyAsync(dsrc, hsrc.data(), k * 4, cudaMemcpyHostToDevice, stream));
   TRC_LAUNCH(prof, stream, "ms_init", ceil_div(n, MT), MT, 0, k_ms_init, n, k, dsrc, seen, front,
              next, lvrow, acc);
@@ -552,13 +551,11 @@ void Graph::msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uin
       TRC_LAUNCH(prof, stream, "ms_clear", ceil_div(nact, MT), MT, 0, k_ms_clear, front, L[cur],
                  nact);
     } else {
-      TRC_LAUNCH(prof, stream, "ms_push", ceil_div((uint64_t)nact * 32, MT), MT, 0, k_ms_push, G,
-                 L[cur], nact, front, seen, acc, T, c + 2, hu, hm, c + 3);
-      if (H)
-        TRC_LAUNCH(prof, stream, "ms_push_hubs", (unsigned)num_sms() * 8, MT, 0, k_ms_push_hubs, G,
-                   hu, hm, c + 3, seen, acc, T, c + 2);
+      ms_push_level(L[cur], nact, front, seen, acc, T, c + 2, offb, scanb);
       TRC_LAUNCH(prof, stream, "ms_commit", commit_grid, MT, 0, k_ms_commit_list, s, T, c + 2,
                  acc, nl, c + 1, any);
+      TRC_LAUNCH(prof, stream, "ms_clear", ceil_div(nact, MT), MT, 0, k_ms_clear, front, L[cur],
+                 nact);
     }
     uint32_t hc[2];
     uint64_t hany = 0;
@@ -657,12 +654,9 @@ void Graph::msbc(const uint32_t *sources, uint32_t k, double *out_user, uint32_t
   uint32_t *L[2] = {lst.alloc_exact(n), lst2.alloc_exact(n)};
   uint32_t *T = tl.alloc_exact(n);
   uint32_t *c = cnt.alloc_exact(4);  // [1] next active, [2] touched, [3] pushing hubs
-  DBuf<uint32_t> hub_u;
-  DBuf<uint64_t> hub_m;
-  hub_u.bind(&budget);
-  hub_m.bind(&budget);
-  uint32_t *hu = hub_u.alloc_exact(H ? H : 1);  // hubs of a push level and their masks
-  uint64_t *hm = hub_m.alloc_exact(H ? H : 1);
+  DBuf<uint64_t> offb, scanb;  // push levels: piece prefix and scan scratch
+  offb.bind(&budget);
+  scanb.bind(&budget);
   DBuf<uint64_t> anyb;
   anyb.bind(&budget);
   unsigned long long *any = (unsigned long long *)anyb.alloc_exact(1);
@@ -710,17 +704,9 @@ void Graph::msbc(const uint32_t *sources, uint32_t k, double *out_user, uint32_t
       TRC_LAUNCH(prof, stream, "ms_collect", ceil_div(n, MT), MT, 0, k_ms_collect, n, next, nl,
                  c + 1, any);
     } else {
-      TRC_LAUNCH(prof, stream, "ms_push", ceil_div((uint64_t)nact * 32, MT), MT, 0, k_ms_push, G,
-                 L[cur], nact, front, seen, acc, T, c + 2, hu, hm, c + 3);
-      if (H)
-        TRC_LAUNCH(prof, stream, "ms_push_hubs", (unsigned)num_sms() * 8, MT, 0, k_ms_push_hubs, G,
-                   hu, hm, c + 3, seen, acc, T, c + 2);
+      ms_push_level(L[cur], nact, front, seen, acc, T, c + 2, offb, scanb);
       TRC_LAUNCH(prof, stream, "ms_commit", pgrid, MT, 0, k_ms_commit_list, s, T, c + 2, acc, nl,
                  c + 1, any);
-      // the push cleared front; restore this level's masks for sigma
-      const uint64_t b0 = loff[loff.size() - 2];
-      TRC_LAUNCH(prof, stream, "mbc_restore", ceil_div(nact, MT), MT, 0, k_mbc_scatter,
-                 lv.o32() + b0, lv.o64() + b0, nact, front);
     }
     TRC_LAUNCH(prof, stream, "mbc_sigma", pgrid, MT, 0, k_mbc_sigma, G, nl, c + 1, front, next,
                sigma, k);
