@@ -219,7 +219,6 @@ constexpr uint64_t BK_INVALID = ~0ull;
 constexpr uint32_t BK_MID = 256;   // 33..BK_MID keys: a warp in shared memory
 constexpr uint32_t BK_BIG = 2048;  // BK_MID+1..BK_BIG: a CTA in static shared memory
                                    // above: a CTA in dynamic shared memory
-constexpr uint32_t BK_NONE = 0xFFFFFFFFu;
 
 struct BucketArgs {
   uint32_t nb;     // valid buckets; bucket nb holds the invalid keys
@@ -229,15 +228,29 @@ struct BucketArgs {
   }
 };
 
-// Counting and scattering use one atomic per distinct bucket of a warp
-// (match_any), so the skewed sources of RMAT-like batches do not serialise
-// on their counters.
-__global__ void k_bucket_hist(const uint64_t *keys, uint64_t k, BucketArgs ba, uint32_t *cnt) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t b = i < k ? ba.of(keys[i]) : BK_NONE;
-  const uint32_t same = __match_any_sync(0xFFFFFFFFu, b);
-  if (b != BK_NONE && (threadIdx.x & 31) == (uint32_t)(__ffs(same) - 1))
-    atomicAdd(cnt + b, (uint32_t)__popc(same));
+// Counting and placing go by tiles of BK_TILE keys, a CTA each, with the
+// tile's bucket counts in shared memory: counts[b * nct + t] = keys of tile
+// t in bucket b (bucket-major, so one exclusive scan gives every (bucket,
+// tile) its output offset), then each tile places its keys at those offsets
+// with shared-memory atomics.  No global atomics: the skewed sources of
+// RMAT-like batches do not serialise anywhere.
+constexpr uint32_t BK_TILE = 16384;
+constexpr uint32_t BK_T = 512;
+constexpr uint32_t BK_MAXB = 8192;  // buckets at most (+1 for the invalid keys)
+
+__global__ void __launch_bounds__(BK_T)
+    k_bucket_count(const uint64_t *keys, uint64_t k, BucketArgs ba, uint32_t nct, uint32_t *counts) {
+  __shared__ uint32_t h[BK_MAXB + 1];
+  for (uint32_t b = threadIdx.x; b <= ba.nb; b += BK_T) h[b] = 0;
+  __syncthreads();
+  const uint64_t base = (uint64_t)blockIdx.x * BK_TILE;
+  for (uint32_t j = threadIdx.x; j < BK_TILE; j += BK_T) {
+    const uint64_t i = base + j;
+    if (i < k) atomicAdd(&h[ba.of(keys[i])], 1u);
+  }
+  __syncthreads();
+  for (uint32_t b = threadIdx.x; b <= ba.nb; b += BK_T)
+    counts[(uint64_t)b * nct + blockIdx.x] = h[b];
 }
 
 struct LoadCnt32 {
@@ -245,19 +258,29 @@ struct LoadCnt32 {
   __device__ uint64_t operator()(uint64_t i) const { return c[i]; }
 };
 
-__global__ void k_bucket_scatter(const uint64_t *keys, uint64_t k, BucketArgs ba,
-                                 const uint64_t *off, uint32_t *fill, uint64_t *out) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t lane = threadIdx.x & 31;
-  const uint64_t x = i < k ? keys[i] : 0;
-  const uint32_t b = i < k ? ba.of(x) : BK_NONE;
-  const uint32_t same = __match_any_sync(0xFFFFFFFFu, b);
-  const uint32_t leader = __ffs(same) - 1;
-  uint32_t base = 0;
-  if (b != BK_NONE && lane == leader) base = atomicAdd(fill + b, (uint32_t)__popc(same));
-  base = __shfl_sync(0xFFFFFFFFu, base, leader);
-  if (b != BK_NONE) out[off[b] + base + __popc(same & ((1u << lane) - 1))] = x;
+__global__ void __launch_bounds__(BK_T)
+    k_bucket_place(const uint64_t *keys, uint64_t k, BucketArgs ba, uint32_t nct,
+                   const uint64_t *offm, uint64_t *out) {
+  __shared__ uint32_t fill[BK_MAXB + 1];
+  for (uint32_t b = threadIdx.x; b <= ba.nb; b += BK_T) fill[b] = 0;
+  __syncthreads();
+  const uint64_t base = (uint64_t)blockIdx.x * BK_TILE;
+  for (uint32_t j = threadIdx.x; j < BK_TILE; j += BK_T) {
+    const uint64_t i = base + j;
+    if (i < k) {
+      const uint64_t x = keys[i];
+      const uint32_t b = ba.of(x);
+      out[offm[(uint64_t)b * nct + blockIdx.x] + atomicAdd(&fill[b], 1u)] = x;
+    }
+  }
 }
+
+// Bucket boundaries: bucket b holds offm[b * stride] .. offm[(b+1) * stride].
+struct BucketOff {
+  const uint64_t *offm;
+  uint32_t stride;
+  __device__ uint64_t operator()(uint64_t b) const { return offm[b * stride]; }
+};
 
 // Ascending bitonic network over the 32 lanes of a warp, one value per lane.
 __device__ __forceinline__ uint64_t warp_bitonic32(uint64_t v, uint32_t lane) {
@@ -327,13 +350,12 @@ __device__ __forceinline__ void thread_bucket_sort(uint64_t *keys, uint64_t base
 // whole warp; larger ones listed by size for the shared-memory kernels;
 // those above BUCKET_SEG_MAX flagged.  lists: 3 lists of `cap` entries,
 // nlist their 3 counts.
-__global__ void k_bucket_sort_small(const uint64_t *off, uint32_t nb, uint64_t *keys,
-                                    uint32_t *lists, uint64_t cap, unsigned long long *nlist,
-                                    uint32_t *err) {
+__global__ void k_bucket_sort_small(BucketOff off, uint32_t nb, uint64_t *keys, uint32_t *lists,
+                                    uint64_t cap, unsigned long long *nlist, uint32_t *err) {
   const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
-  const uint64_t base = b < nb ? off[b] : 0;
-  const uint32_t c = b < nb ? (uint32_t)(off[b + 1] - base) : 0u;
+  const uint64_t base = b < nb ? off(b) : 0;
+  const uint32_t c = b < nb ? (uint32_t)(off(b + 1) - base) : 0u;
   if (c > 32) {
     if (c > BUCKET_SEG_MAX) {
       atomicOr(err, ERR_BIGSEG);
@@ -367,7 +389,7 @@ __global__ void k_bucket_sort_small(const uint64_t *off, uint32_t nb, uint64_t *
 // A warp per listed bucket of 33..BK_MID keys, sorted in shared memory.
 constexpr uint32_t BK_MID_WARPS = 8;
 __global__ void __launch_bounds__(BK_MID_WARPS * 32)
-    k_bucket_sort_mid(const uint64_t *off, const uint32_t *list, const unsigned long long *nlist,
+    k_bucket_sort_mid(BucketOff off, const uint32_t *list, const unsigned long long *nlist,
                       uint64_t *keys) {
   __shared__ uint64_t sv[BK_MID_WARPS][BK_MID];
   const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -376,8 +398,8 @@ __global__ void __launch_bounds__(BK_MID_WARPS * 32)
   for (uint64_t i = (uint64_t)blockIdx.x * BK_MID_WARPS + w; i < nm;
        i += (uint64_t)gridDim.x * BK_MID_WARPS) {
     const uint32_t b = list[i];
-    const uint64_t base = off[b];
-    const uint32_t c = (uint32_t)(off[b + 1] - base);
+    const uint64_t base = off(b);
+    const uint32_t c = (uint32_t)(off(b + 1) - base);
     uint32_t P = 64;
     while (P < c) P <<= 1;
     for (uint32_t t = lane; t < P; t += 32) v[t] = t < c ? keys[base + t] : BK_INVALID;
@@ -392,7 +414,7 @@ __global__ void __launch_bounds__(BK_MID_WARPS * 32)
 // shared memory: static for PMAX = BK_BIG, dynamic otherwise.
 template <uint32_t PMAX, uint32_t NT>
 __global__ void __launch_bounds__(NT)
-    k_bucket_sort_cta(const uint64_t *off, const uint32_t *list, const unsigned long long *nlist,
+    k_bucket_sort_cta(BucketOff off, const uint32_t *list, const unsigned long long *nlist,
                       uint64_t *keys) {
   __shared__ uint64_t sstat[PMAX <= BK_BIG ? PMAX : 1];
   extern __shared__ uint64_t sdyn[];
@@ -400,8 +422,8 @@ __global__ void __launch_bounds__(NT)
   const uint64_t nbg = *nlist;
   for (uint64_t i = blockIdx.x; i < nbg; i += gridDim.x) {
     const uint32_t b = list[i];
-    const uint64_t base = off[b];
-    const uint32_t c = (uint32_t)(off[b + 1] - base);
+    const uint64_t base = off(b);
+    const uint32_t c = (uint32_t)(off(b + 1) - base);
     uint32_t P = 2 * BK_MID;
     while (P < c) P <<= 1;
     for (uint32_t t = threadIdx.x; t < P; t += NT) v[t] = t < c ? keys[base + t] : BK_INVALID;
@@ -413,22 +435,26 @@ __global__ void __launch_bounds__(NT)
 }
 
 struct BucketLayout {
-  uint32_t nb, shift;
+  uint32_t nb, shift, nct;
+  uint64_t cells;  // (nb + 1) * nct
   uint64_t list_cap;
   uint64_t cnt_w, off_w, scan_w, list_w;  // words of each part
-  uint64_t total() const { return 2 * cnt_w + off_w + scan_w + list_w + 3; }
+  uint64_t total() const { return cnt_w + off_w + scan_w + list_w + 3; }
 };
 
 BucketLayout bucket_layout(uint64_t k, uint32_t n) {
   BucketLayout L{};
-  // at most one bucket per key: bucket = source >> shift
+  // about 128 keys per bucket, at most BK_MAXB buckets: bucket = source >> shift
+  const uint64_t target = std::max<uint64_t>(1, std::min<uint64_t>(BK_MAXB, k / 128));
   L.shift = 0;
-  while (L.shift < 31 && ceil_div((uint64_t)n, 1ull << L.shift) > k) L.shift++;
+  while (L.shift < 31 && ceil_div((uint64_t)n, 1ull << L.shift) > target) L.shift++;
   L.nb = (uint32_t)ceil_div((uint64_t)n, 1ull << L.shift);
+  L.nct = (uint32_t)ceil_div(k, BK_TILE);
+  L.cells = ((uint64_t)L.nb + 1) * L.nct;
   L.list_cap = std::min<uint64_t>(L.nb, k / 33) + 1;
-  L.cnt_w = ceil_div((uint64_t)L.nb + 1, 2);
-  L.off_w = (uint64_t)L.nb + 1;
-  L.scan_w = scan_tmp_elems((uint64_t)L.nb + 1) + 4;
+  L.cnt_w = ceil_div(L.cells, 2);
+  L.off_w = L.cells + 1;
+  L.scan_w = scan_tmp_elems(L.cells) + 4;
   L.list_w = ceil_div(3 * L.list_cap, 2);
   return L;
 }
@@ -442,18 +468,17 @@ uint64_t *bucket_sort_u64(const uint64_t *keys, uint64_t *alt, uint64_t k, uint3
   if (k == 0) return alt;
   const BucketLayout L = bucket_layout(k, n);
   const BucketArgs ba{L.nb, L.shift};
-  uint32_t *cnt = reinterpret_cast<uint32_t *>(tmp);
-  uint32_t *fill = reinterpret_cast<uint32_t *>(tmp + L.cnt_w);
-  uint64_t *off = tmp + 2 * L.cnt_w;
-  uint64_t *st = off + L.off_w;
+  uint32_t *counts = reinterpret_cast<uint32_t *>(tmp);
+  uint64_t *offm = tmp + L.cnt_w;
+  uint64_t *st = offm + L.off_w;
   uint32_t *lists = reinterpret_cast<uint32_t *>(st + L.scan_w);
   unsigned long long *nlist = reinterpret_cast<unsigned long long *>(st + L.scan_w + L.list_w);
-  TRC_CUDA(cudaMemsetAsync(tmp, 0, 2 * L.cnt_w * 8, s));  // cnt and fill
   TRC_CUDA(cudaMemsetAsync(nlist, 0, 3 * 8, s));
-  TRC_LAUNCH(prof, s, "bsort_hist", ceil_div(k, 256), 256, 0, k_bucket_hist, keys, k, ba, cnt);
-  exclusive_scan(LoadCnt32{cnt}, (uint64_t)L.nb + 1, off, st, s, prof, "bsort_scan");
-  TRC_LAUNCH(prof, s, "bsort_scatter", ceil_div(k, 256), 256, 0, k_bucket_scatter, keys, k, ba,
-             off, fill, alt);
+  TRC_LAUNCH(prof, s, "bsort_count", L.nct, BK_T, 0, k_bucket_count, keys, k, ba, L.nct, counts);
+  exclusive_scan(LoadCnt32{counts}, L.cells, offm, st, s, prof, "bsort_scan");
+  TRC_LAUNCH(prof, s, "bsort_place", L.nct, BK_T, 0, k_bucket_place, keys, k, ba, L.nct, offm,
+             alt);
+  const BucketOff off{offm, L.nct};
   TRC_LAUNCH(prof, s, "bsort_small", ceil_div((uint64_t)L.nb, 256), 256, 0, k_bucket_sort_small,
              off, L.nb, alt, lists, L.list_cap, nlist, err);
   const unsigned sms = (unsigned)num_sms();

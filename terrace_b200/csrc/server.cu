@@ -341,7 +341,8 @@ class Server {
   DBuf<double> ranks_, pr0_, pr1_, pr_part_;
   DBuf<uint64_t> red_;
   bool bufs_bound_ = false;
-  cudaStream_t s2_ = nullptr;  // PageRank overlapping the BFS groups
+  cudaStream_t s1_ = nullptr;  // the graph's stream while serving (high priority)
+  cudaStream_t s2_ = nullptr;  // PageRank overlapping the BFS groups (low priority)
   double *pin_ = nullptr;      // pinned PageRank partial sums
   unsigned pin_cap_ = 0;
   std::vector<std::pair<size_t, size_t>> pr_groups_;
@@ -437,7 +438,21 @@ class Server {
 
   void loop() {
     cudaSetDevice(g_.device);
-    if (cudaStreamCreateWithFlags(&s2_, cudaStreamNonBlocking) != cudaSuccess) s2_ = nullptr;
+    // the round's own work (lookups, updates, BFS) on a high-priority
+    // stream, PageRank on a low-priority one: a BFS launched while a
+    // PageRank runs gets the SMs as the PageRank's CTAs retire, so the
+    // BFS requests complete one by one instead of at the PageRank's end
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    cudaStream_t user = g_.stream;
+    g_.sync();  // work queued on the graph's stream before the server
+    if (cudaStreamCreateWithPriority(&s1_, cudaStreamNonBlocking, greatest) == cudaSuccess) {
+      g_.stream = s1_;
+      g_.budget.stream = s1_;
+    } else {
+      s1_ = nullptr;
+    }
+    if (cudaStreamCreateWithPriority(&s2_, cudaStreamNonBlocking, least) != cudaSuccess) s2_ = nullptr;
     while (true) {
       std::vector<Request *> round;
       {
@@ -485,6 +500,12 @@ class Server {
     if (s2_) {
       cudaStreamSynchronize(s2_);
       cudaStreamDestroy(s2_);
+    }
+    if (s1_) {
+      cudaStreamSynchronize(s1_);
+      g_.stream = user;
+      g_.budget.stream = user;
+      cudaStreamDestroy(s1_);
     }
     if (pin_) cudaFreeHost(pin_);
   }
@@ -629,26 +650,25 @@ class Server {
   // 34-42 ms together)
   static constexpr size_t kMinGroup = 4;
 
-  // BFS grouping by measured cost.  The host time of one single-source BFS
-  // and, per group-size class (floor(log2 k)), the time per source of one
-  // multi-source launch are kept as exponentially weighted averages; a group
-  // of k runs as one multi-source launch only when that is estimated at most
-  // 3/4 of k single-source runs, because single runs complete one by one
-  // (each request as soon as its own traversal ends) while a group completes
-  // all its requests at its end.  A class without a measurement is tried
-  // once; until a single run has been timed, groups are not formed.
+  // BFS grouping by measured cost.  A multi-source launch costs about the
+  // same whatever its number of sources (its dense levels read every list
+  // once for all of them), so the model is: one single-source BFS takes
+  // bfs1_ms_, one multi-source launch msb_ms_ (host times, exponentially
+  // weighted averages).  k requests run as one launch only when it is
+  // estimated at most 3/4 of k single runs, because single runs complete
+  // one by one (each request as soon as its own traversal ends) while a
+  // group completes all its requests at its end.  Until a launch has been
+  // timed its cost is taken as kMsbPrior single runs, so groups are first
+  // tried only when the queue of BFS requests is long; until a single run
+  // has been timed, groups are not formed.
+  static constexpr double kMsbPrior = 24.0;
   double bfs1_ms_ = 0;
-  double msb_per_ms_[8] = {};
-  static int size_class(size_t k) {
-    int c = 0;
-    while ((size_t)2 << c <= k) c++;
-    return c < 7 ? c : 7;
-  }
+  double msb_ms_ = 0;
   static void ewma(double &avg, double x) { avg = avg > 0 ? 0.75 * avg + 0.25 * x : x; }
   bool group_pays(size_t k) const {
     if (k < kMinGroup || bfs1_ms_ <= 0) return false;
-    const double per = msb_per_ms_[size_class(k)];
-    return per <= 0 || per <= 0.75 * bfs1_ms_;
+    const double launch = msb_ms_ > 0 ? msb_ms_ : kMsbPrior * bfs1_ms_;
+    return launch <= 0.75 * (double)k * bfs1_ms_;
   }
 
   void run_bfs(std::vector<Request *> &bfs) {
@@ -703,7 +723,7 @@ class Server {
         }
         calls_++;
         round_groups_++;
-        ewma(msb_per_ms_[size_class(k)], (now_ms() - t0) / (double)k);
+        ewma(msb_ms_, now_ms() - t0);
       }
       finish(grp);
       i += k;

@@ -907,9 +907,11 @@ __global__ void k_window_mark2(const uint64_t *mw, uint32_t n, uint32_t *stamp, 
 // the tier-2 counts is then computed even when no vertex overflows).
 constexpr uint64_t PLAN_SPECULATE = 1u << 16;
 
-// Batches of at least this many keys sort with the bucket sort (below it
-// both sorts are a handful of launches over a few tiles).
+// Batches of BUCKET_MIN_KEYS .. BUCKET_MAX_KEYS keys sort with the bucket
+// sort (below, both sorts are a handful of launches over a few tiles; above,
+// the buckets of skewed batches outgrow the shared-memory sorts).
 constexpr uint64_t BUCKET_MIN_KEYS = 1u << 12;
+constexpr uint64_t BUCKET_MAX_KEYS = 1u << 24;
 
 // ---------------------------------------------------------------------------
 // The pipeline
@@ -931,7 +933,8 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   // hook is set); a bucket too large for it sends the batch back here, to
   // the radix sort, before anything is modified
   bool bucket = sort_mode == 2 ||
-                (sort_mode == 0 && k2 >= BUCKET_MIN_KEYS && !sort_wait.withhold_first &&
+                (sort_mode == 0 && k2 >= BUCKET_MIN_KEYS && k2 <= BUCKET_MAX_KEYS &&
+                 !sort_wait.withhold_first &&
                  sort_wait.spin_limit == SortWait{}.spin_limit);
 retry_sort:
   TRC_CUDA(cudaMemsetAsync(cnt, 0, 32 * 8, stream));

@@ -265,8 +265,9 @@ def test_batch_sort_modes_agree_with_oracle(T, mode):
         s = rng.integers(0, n, k).astype(np.uint32)
         d = rng.integers(0, n, k).astype(np.uint32)
         if k >= 300:  # skew: runs of equal sources of every bucket tier
-            s[: k // 4] = rng.integers(0, 8, k // 4).astype(np.uint32)
-            s[k // 4: k // 4 + k // 8] = 12345
+            a, b = min(k // 4, 6000), min(k // 8, 12000)
+            s[:a] = rng.integers(0, 8, a).astype(np.uint32)
+            s[a:a + b] = 12345
         bk = O.make_keys(s, d, True, True)
         if step % 4 == 3:
             g.remove_edge_batch(s, d, **SYM)
