@@ -572,7 +572,9 @@ __device__ __forceinline__ void bfs_push_span(const uint32_t *p, uint32_t len, u
   uint32_t v = 0;
   if (lane < len) {
     v = p[lane];
-    if (s.lv[v] == TRC_UNREACHED && atomicCAS(&s.par[v], -1, (int32_t)u) == -1) {
+    // (the parent is claimed before the level is written: a claimed parent
+    // saves a contended CAS on a popular neighbour)
+    if (s.lv[v] == TRC_UNREACHED && s.par[v] == -1 && atomicCAS(&s.par[v], -1, (int32_t)u) == -1) {
       s.lv[v] = s.d + 1;
       win = true;
     }
@@ -584,14 +586,10 @@ __device__ __forceinline__ void bfs_push_span(const uint32_t *p, uint32_t len, u
 // exclusive prefix of the piece counts, off[nf] = the total T): warp w of W
 // takes pieces [T*w/W, T*(w+1)/W), whatever vertices they belong to, so one
 // long list is spread over many warps and many short lists share one warp.
-struct PushPieces {
-  DevView G;
-  const uint32_t *F;
-  uint64_t nf;
-  __device__ uint64_t operator()(uint64_t i) const {
-    return i < nf ? list_pieces(nbr_list(G, F[i])) : 0;
-  }
-};
+__global__ void k_list_pieces(DevView G, const uint32_t *F, uint32_t nf, uint32_t *cnt) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nf) cnt[i] = list_pieces(nbr_list(G, F[i]));
+}
 
 // The frontier vertex of piece t: the i with off[i] <= t < off[i+1] (every
 // list has a piece, so off is strictly increasing).
@@ -653,11 +651,15 @@ struct ListVal {
 };
 
 // frontier bitmap of level d from the levels: one ballot per 32 vertices
-// (no atomics, no clearing pass)
+// (no atomics, no clearing pass); grid-stride, so the grid is what fits on
+// the GPU rather than one tiny CTA per 256 vertices
 __global__ void k_level_bits(const uint32_t *lv, uint32_t n, uint32_t d, uint32_t *bits) {
-  const uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t b = __ballot_sync(0xFFFFFFFFu, v < n && lv[v] == d);
-  if ((threadIdx.x & 31) == 0 && v < n) bits[v >> 5] = b;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v - (threadIdx.x & 31) < n;
+       v += stride) {
+    const uint32_t b = __ballot_sync(0xFFFFFFFFu, v < n && lv[v] == d);
+    if ((threadIdx.x & 31) == 0) bits[v >> 5] = b;
+  }
 }
 
 // Inline pass of a dense step: 4 lanes per vertex (one 128-bit quarter of
@@ -861,11 +863,23 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_G8(DevView G, const uint32_t *L
 }
 
 __global__ void k_bfs_init(uint32_t *lv, int32_t *par, uint32_t n, uint32_t src, uint32_t *q) {
-  uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (u >= n) return;
-  lv[u] = u == src ? 0 : TRC_UNREACHED;
-  par[u] = u == src ? (int32_t)src : -1;
-  if (u == src) q[0] = src;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
+    lv[u] = u == src ? 0 : TRC_UNREACHED;
+    par[u] = u == src ? (int32_t)src : -1;
+    if (u == src) q[0] = src;
+  }
+}
+
+const uint64_t *Graph::piece_offsets(const uint32_t *F, uint32_t nf, PieceBufs &pb,
+                                     const char *tag) {
+  uint32_t *cnt = pb.cnt.ensure(nf);
+  uint64_t *off = pb.off.ensure((uint64_t)nf + 1);
+  uint64_t *st = pb.scan.ensure(scan_tmp_elems(nf) + 4);
+  TRC_LAUNCH(prof, stream, "list_pieces", ceil_div(nf, AT), AT, 0, k_list_pieces, view(), F, nf,
+             cnt);
+  exclusive_scan(LoadU32{cnt}, nf, off, st, stream, prof, tag);  // (off[nf] = the total)
+  return off;
 }
 
 void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags) {
@@ -883,20 +897,19 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
   uint64_t words = ceil_div(n, 32);
   uint32_t *bm = bits.alloc_exact(words);
   uint32_t *c = cnt.alloc_exact(4);
-  TRC_LAUNCH(prof, stream, "bfs_init", ceil_div(n, AT), AT, 0, k_bfs_init, lv, par, n, src, F);
+  TRC_LAUNCH(prof, stream, "bfs_init", std::min<uint64_t>(ceil_div(n, AT), resident_grid(k_bfs_init, AT)),
+             AT, 0, k_bfs_init, lv, par, n, src, F);
   DevView G = view();
   uint32_t nf = 1, d = 0;
   const uint64_t dense_at = n / push_pull_divisor();
   // candidates of the dense steps: non-hub vertices not yet visited,
   // compacted after every dense step
   DBuf<uint32_t> cbuf[2], segb, seg2b;  // candidate ping-pong, segment-pass lists
-  DBuf<uint64_t> offb, scanb;     // push steps: piece prefix and scan scratch
+  PieceBufs pbufs(&budget);  // push steps: piece counts, prefix, scan scratch
   cbuf[0].bind(&budget);
   cbuf[1].bind(&budget);
   segb.bind(&budget);
   seg2b.bind(&budget);
-  offb.bind(&budget);
-  scanb.bind(&budget);
   // (the first dense step reads every vertex id in order, no list: its
   // candidates are all non-hub vertices, and the loads stay contiguous)
   const uint32_t *cand = nullptr;
@@ -909,7 +922,9 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
     BFSState s{lv, par, bm, Nx, c, d, sg, c + 1, nullptr, c + 2, sg2, c + 3};
     uint32_t hc[3] = {0, 0, 0};
     if ((uint64_t)nf >= dense_at && dense_at > 0) {
-      TRC_LAUNCH(prof, stream, "bfs_bits", ceil_div(n, AT), AT, 0, k_level_bits, lv, n, d, bm);
+      TRC_LAUNCH(prof, stream, "bfs_bits",
+                 std::min<uint64_t>(ceil_div(n, AT), resident_grid(k_level_bits, AT)), AT, 0,
+                 k_level_bits, lv, n, d, bm);
       // candidates left for the next dense step (never the list being read)
       s.cand = cbuf[cnext].ensure(ncand ? ncand : 1);
       // pass A: the 16 inline neighbours of every unvisited non-hub vertex;
@@ -936,10 +951,7 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
     } else {
       // edge-balanced push: piece counts scanned, then every warp of the
       // grid takes an equal share of the frontier's pieces
-      uint64_t *off = offb.ensure((uint64_t)nf + 1);
-      uint64_t *stmp = scanb.ensure(scan_tmp_elems((uint64_t)nf + 1) + 4);
-      exclusive_scan(PushPieces{G, F, nf}, (uint64_t)nf + 1, off, stmp, stream, prof,
-                     "bfs_push_scan");
+      const uint64_t *off = piece_offsets(F, nf, pbufs, "bfs_push_scan");
       TRC_LAUNCH(prof, stream, "bfs_push", pgrid, AT, 0, k_bfs_push_lb, G, F, nf, off, s);
       TRC_CUDA(cudaMemcpyAsync(hc, c, 4, cudaMemcpyDeviceToHost, stream));
       sync();
@@ -1417,9 +1429,7 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
   for (auto *b : {&sig, &invb, &depb, &outb, &sideb}) b->bind(&budget);
   double *side = sideb.alloc_exact(n);  // a dense step's results before their commit
   uint32_t *lv = lvb.alloc_exact(n), *order = ordb.alloc_exact(n), *c = cntb.alloc_exact(4);
-  DBuf<uint64_t> offb, scanb;  // push steps: piece prefix and scan scratch
-  offb.bind(&budget);
-  scanb.bind(&budget);
+  PieceBufs pbufs(&budget);  // push steps: piece counts, prefix, scan scratch
   double *sigma = sig.alloc_exact(n), *inv = invb.alloc_exact(n), *dep = depb.alloc_exact(n);
   double *out = dev ? out_user : outb.alloc_exact(n);
   TRC_LAUNCH(prof, stream, "bc_init", ceil_div(n, AT), AT, 0, k_bc_init, lv, sigma, dep, n, src,
@@ -1442,10 +1452,7 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
       TRC_LAUNCH(prof, stream, "bc_commit", (unsigned)num_sms() * 4, AT, 0, k_bc_commit, order + f1,
                  c, 0, side, sigma);
     } else {
-      uint64_t *off = offb.ensure((uint64_t)nf + 1);
-      uint64_t *stmp = scanb.ensure(scan_tmp_elems((uint64_t)nf + 1) + 4);
-      exclusive_scan(PushPieces{G, order + f0, nf}, (uint64_t)nf + 1, off, stmp, stream, prof,
-                     "bc_push_scan");
+      const uint64_t *off = piece_offsets(order + f0, nf, pbufs, "bc_push_scan");
       TRC_LAUNCH(prof, stream, "bc_push", (unsigned)num_sms() * 8, AT, 0, k_bc_push_lb, G,
                  order + f0, nf, off, s);
     }
@@ -1508,10 +1515,6 @@ __global__ void k_tc_count_out(DevView G, uint32_t *outdeg) {
   if (lane == 0) outdeg[u] = c;
 }
 
-struct LoadU32 {
-  const uint32_t *p;
-  __device__ uint64_t operator()(uint64_t i) const { return p[i]; }
-};
 
 __global__ void k_tc_fill(DevView G, const uint64_t *off, uint32_t *adj) {
   uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;

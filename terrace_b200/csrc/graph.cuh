@@ -160,10 +160,22 @@ class Graph {
                  uint64_t *reached, uint32_t *ecc);
   // up to 64 BC at once, out[i*n + v] (msbfs.cu)
   void msbc(const uint32_t *sources, uint32_t k, double *out, uint32_t flags);
+  // Edge-balanced pushes: the frontier F's lists cut into list_piece()s;
+  // returns off[0..nf] = the exclusive prefix of their piece counts (off[nf]
+  // = the total), in pb's buffers (analytics.cu)
+  struct PieceBufs {
+    DBuf<uint32_t> cnt;
+    DBuf<uint64_t> off, scan;
+    explicit PieceBufs(Budget *b) {
+      cnt.bind(b);
+      off.bind(b);
+      scan.bind(b);
+    }
+  };
+  const uint64_t *piece_offsets(const uint32_t *F, uint32_t nf, PieceBufs &pb, const char *tag);
   // one edge-balanced push level of msbfs / msbc (msbfs.cu)
   void ms_push_level(const uint32_t *F, uint32_t nf, const uint64_t *front, const uint64_t *seen,
-                     unsigned long long *acc, uint32_t *T, uint32_t *tcnt, DBuf<uint64_t> &offb,
-                     DBuf<uint64_t> &scanb);
+                     unsigned long long *acc, uint32_t *T, uint32_t *tcnt, PieceBufs &pb);
   // BFS with scratch in a static device array (no allocation), noalloc.cu
   void bfs_noalloc(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags);
   uint32_t *na_scratch = nullptr;  // that array's device address on this graph's device

@@ -174,15 +174,6 @@ __device__ __forceinline__ void ms_push_piece(const uint32_t *p, uint32_t len, u
   if (first) T[base + __popc(b & lanemask_lt())] = x;
 }
 
-struct MsPieces {
-  DevView G;
-  const uint32_t *F;
-  uint64_t nf;
-  __device__ uint64_t operator()(uint64_t i) const {
-    return i < nf ? list_pieces(nbr_list(G, F[i])) : 0;
-  }
-};
-
 __global__ void __launch_bounds__(MT) k_ms_push(DevView G, const uint32_t *F, uint32_t nf,
                                                 const uint64_t *off, const uint64_t *front,
                                                 const uint64_t *seen, unsigned long long *acc,
@@ -454,11 +445,9 @@ __global__ void k_mbc_final(const double *dep, const double *sigma, uint32_t n, 
 
 void Graph::ms_push_level(const uint32_t *F, uint32_t nf, const uint64_t *front,
                           const uint64_t *seen, unsigned long long *acc, uint32_t *T,
-                          uint32_t *tcnt, DBuf<uint64_t> &offb, DBuf<uint64_t> &scanb) {
-  uint64_t *off = offb.ensure((uint64_t)nf + 1);
-  uint64_t *stmp = scanb.ensure(scan_tmp_elems((uint64_t)nf + 1) + 4);
+                          uint32_t *tcnt, PieceBufs &pb) {
+  const uint64_t *off = piece_offsets(F, nf, pb, "ms_push_scan");
   const DevView G = view();
-  exclusive_scan(MsPieces{G, F, nf}, (uint64_t)nf + 1, off, stmp, stream, prof, "ms_push_scan");
   TRC_LAUNCH(prof, stream, "ms_push", (unsigned)num_sms() * 8, MT, 0, k_ms_push, G, F, nf, off,
              front, seen, acc, T, tcnt);
 }
@@ -512,9 +501,7 @@ void Graph::msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uin
   uint32_t *L[2] = {lst.alloc_exact(n), lst2.alloc_exact(n)};
   uint32_t *T = tl.alloc_exact(n);
   uint32_t *c = cnt.alloc_exact(4);  // [1] next active, [2] touched, [3] pushing hubs
-  DBuf<uint64_t> offb, scanb;  // push levels: piece prefix and scan scratch
-  offb.bind(&budget);
-  scanb.bind(&budget);
+  PieceBufs pbufs(&budget);  // push levels: piece counts, prefix, scan scratch
   TRC_CUDA(cudaMemcpyAsync(dsrc, hsrc.data(), k * 4, cudaMemcpyHostToDevice, stream));
   TRC_LAUNCH(prof, stream, "ms_init", ceil_div(n, MT), MT, 0, k_ms_init, n, k, dsrc, seen, front,
              next, lvrow, acc);
@@ -551,7 +538,7 @@ void Graph::msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uin
       TRC_LAUNCH(prof, stream, "ms_clear", ceil_div(nact, MT), MT, 0, k_ms_clear, front, L[cur],
                  nact);
     } else {
-      ms_push_level(L[cur], nact, front, seen, acc, T, c + 2, offb, scanb);
+      ms_push_level(L[cur], nact, front, seen, acc, T, c + 2, pbufs);
       TRC_LAUNCH(prof, stream, "ms_commit", commit_grid, MT, 0, k_ms_commit_list, s, T, c + 2,
                  acc, nl, c + 1, any);
       TRC_LAUNCH(prof, stream, "ms_clear", ceil_div(nact, MT), MT, 0, k_ms_clear, front, L[cur],
@@ -654,9 +641,7 @@ void Graph::msbc(const uint32_t *sources, uint32_t k, double *out_user, uint32_t
   uint32_t *L[2] = {lst.alloc_exact(n), lst2.alloc_exact(n)};
   uint32_t *T = tl.alloc_exact(n);
   uint32_t *c = cnt.alloc_exact(4);  // [1] next active, [2] touched, [3] pushing hubs
-  DBuf<uint64_t> offb, scanb;  // push levels: piece prefix and scan scratch
-  offb.bind(&budget);
-  scanb.bind(&budget);
+  PieceBufs pbufs(&budget);  // push levels: piece counts, prefix, scan scratch
   DBuf<uint64_t> anyb;
   anyb.bind(&budget);
   unsigned long long *any = (unsigned long long *)anyb.alloc_exact(1);
@@ -704,7 +689,7 @@ void Graph::msbc(const uint32_t *sources, uint32_t k, double *out_user, uint32_t
       TRC_LAUNCH(prof, stream, "ms_collect", ceil_div(n, MT), MT, 0, k_ms_collect, n, next, nl,
                  c + 1, any);
     } else {
-      ms_push_level(L[cur], nact, front, seen, acc, T, c + 2, offb, scanb);
+      ms_push_level(L[cur], nact, front, seen, acc, T, c + 2, pbufs);
       TRC_LAUNCH(prof, stream, "ms_commit", pgrid, MT, 0, k_ms_commit_list, s, T, c + 2, acc, nl,
                  c + 1, any);
     }

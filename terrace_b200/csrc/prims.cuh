@@ -124,6 +124,11 @@ struct LoadU64 {
   __device__ uint64_t operator()(uint64_t i) const { return p[i]; }
 };
 
+struct LoadU32 {
+  const uint32_t *p;
+  __device__ uint64_t operator()(uint64_t i) const { return p[i]; }
+};
+
 class Scratch;
 
 // Exclusive scan into out[0..n]; tmp needs scan_tmp_elems(n) entries.
