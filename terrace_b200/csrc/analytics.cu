@@ -654,11 +654,19 @@ struct ListVal {
 // (no atomics, no clearing pass); grid-stride, so the grid is what fits on
 // the GPU rather than one tiny CTA per 256 vertices
 __global__ void k_level_bits(const uint32_t *lv, uint32_t n, uint32_t d, uint32_t *bits) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v - (threadIdx.x & 31) < n;
-       v += stride) {
-    const uint32_t b = __ballot_sync(0xFFFFFFFFu, v < n && lv[v] == d);
-    if ((threadIdx.x & 31) == 0) bits[v >> 5] = b;
+  constexpr uint32_t U = 4;  // level loads in flight per thread
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t W = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v0 - lane < n; v0 += U * W) {
+    uint32_t x[U];
+#pragma unroll
+    for (uint32_t j = 0; j < U; j++) x[j] = v0 + j * W < n ? lv[v0 + j * W] : TRC_UNREACHED;
+#pragma unroll
+    for (uint32_t j = 0; j < U; j++) {
+      const uint64_t v = v0 + j * W;
+      const uint32_t b = __ballot_sync(0xFFFFFFFFu, x[j] == d);
+      if (lane == 0 && v < n) bits[v >> 5] = b;
+    }
   }
 }
 
@@ -862,13 +870,26 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_G8(DevView G, const uint32_t *L
   sc.flush(s.cand, s.cand_cnt, lane);
 }
 
-__global__ void k_bfs_init(uint32_t *lv, int32_t *par, uint32_t n, uint32_t src, uint32_t *q) {
+// (16-byte stores, 4 vertices per thread and step, when both arrays are
+// 16-byte aligned; caller arrays may not be)
+__global__ void k_bfs_init(uint32_t *lv, int32_t *par, uint32_t n, int vec) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
-    lv[u] = u == src ? 0 : TRC_UNREACHED;
-    par[u] = u == src ? (int32_t)src : -1;
-    if (u == src) q[0] = src;
+  const uint64_t n4 = vec ? n / 4 : 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+    reinterpret_cast<uint4 *>(lv)[i] = make_uint4(TRC_UNREACHED, TRC_UNREACHED, TRC_UNREACHED,
+                                                  TRC_UNREACHED);
+    reinterpret_cast<int4 *>(par)[i] = make_int4(-1, -1, -1, -1);
   }
+  for (uint64_t u = n4 * 4 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
+    lv[u] = TRC_UNREACHED;
+    par[u] = -1;
+  }
+}
+
+__global__ void k_bfs_source(uint32_t *lv, int32_t *par, uint32_t src, uint32_t *q) {
+  lv[src] = 0;
+  par[src] = (int32_t)src;
+  q[0] = src;
 }
 
 const uint64_t *Graph::piece_offsets(const uint32_t *F, uint32_t nf, PieceBufs &pb,
@@ -897,8 +918,10 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
   uint64_t words = ceil_div(n, 32);
   uint32_t *bm = bits.alloc_exact(words);
   uint32_t *c = cnt.alloc_exact(4);
-  TRC_LAUNCH(prof, stream, "bfs_init", std::min<uint64_t>(ceil_div(n, AT), resident_grid(k_bfs_init, AT)),
-             AT, 0, k_bfs_init, lv, par, n, src, F);
+  TRC_LAUNCH(prof, stream, "bfs_init",
+             std::min<uint64_t>(ceil_div(n, 4 * AT), resident_grid(k_bfs_init, AT)), AT, 0,
+             k_bfs_init, lv, par, n, (int)((((uintptr_t)lv | (uintptr_t)par) & 15) == 0));
+  TRC_LAUNCH(prof, stream, "bfs_source", 1, 1, 0, k_bfs_source, lv, par, src, F);
   DevView G = view();
   uint32_t nf = 1, d = 0;
   const uint64_t dense_at = n / push_pull_divisor();
