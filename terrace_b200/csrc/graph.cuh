@@ -108,6 +108,8 @@ class Graph {
   uint64_t last[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // sizes of the last batch
   SortWait sort_wait;  // bounded look-back wait of the batch sort (test hook)
   int sort_mode = 0;   // batch sort: 0 by size, 1 radix only, 2 bucket first (test hook)
+  DBuf<uint32_t> bsplits;  // bucket sort: source quantiles of the last large batch
+  bool bsplits_ok = false;
   uint64_t sort_retries = 0;  // batches the bucket sort handed back to the radix sort
 
   // ------------------------------------------------------------- scratch

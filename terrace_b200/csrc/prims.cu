@@ -220,11 +220,24 @@ constexpr uint32_t BK_MID = 256;   // 33..BK_MID keys: a warp in shared memory
 constexpr uint32_t BK_BIG = 2048;  // BK_MID+1..BK_BIG: a CTA in static shared memory
                                    // above: a CTA in dynamic shared memory
 
+// Bucket of a key: with split points (sp, nb + 1 non-decreasing source ids,
+// sp[0] = 0, in shared memory) bucket b holds the sources [sp[b], sp[b+1]);
+// without, bucket = source >> shift.  Bucket nb holds the invalid keys.
 struct BucketArgs {
-  uint32_t nb;     // valid buckets; bucket nb holds the invalid keys
-  uint32_t shift;  // bucket = source >> shift
+  uint32_t nb;
+  uint32_t shift;
+  const uint32_t *sp;  // (shared memory) or null
   __device__ uint32_t of(uint64_t x) const {
-    return x == BK_INVALID ? nb : (uint32_t)(x >> (32 + shift));
+    if (x == BK_INVALID) return nb;
+    const uint32_t src = (uint32_t)(x >> 32);
+    if (!sp) return src >> shift;
+    uint32_t lo = 0, hi = nb;  // the last b with sp[b] <= src
+    while (hi - lo > 1) {
+      const uint32_t m = (lo + hi) >> 1;
+      if (sp[m] <= src) lo = m;
+      else hi = m;
+    }
+    return lo;
   }
 };
 
@@ -236,11 +249,25 @@ struct BucketArgs {
 // RMAT-like batches do not serialise anywhere.
 constexpr uint32_t BK_TILE = 16384;
 constexpr uint32_t BK_T = 512;
-constexpr uint32_t BK_MAXB = 8192;  // buckets at most (+1 for the invalid keys)
+constexpr uint32_t BK_MAXB = BUCKET_SPLITS;  // buckets at most (+1 for the invalid keys)
+
+// splits (global, BK_MAXB + 1 entries) or null; the CTA copies them to
+// shared memory (after its BK_MAXB + 1 counters)
+__device__ __forceinline__ BucketArgs bucket_args_shared(BucketArgs ba, const uint32_t *splits,
+                                                         uint32_t *sp) {
+  if (splits) {
+    for (uint32_t b = threadIdx.x; b <= ba.nb; b += BK_T) sp[b] = splits[b];
+    ba.sp = sp;
+  }
+  return ba;
+}
 
 __global__ void __launch_bounds__(BK_T)
-    k_bucket_count(const uint64_t *keys, uint64_t k, BucketArgs ba, uint32_t nct, uint32_t *counts) {
-  __shared__ uint32_t h[BK_MAXB + 1];
+    k_bucket_count(const uint64_t *keys, uint64_t k, BucketArgs ba0, const uint32_t *splits,
+                   uint32_t nct, uint32_t *counts) {
+  extern __shared__ uint32_t bk_smem[];
+  uint32_t *h = bk_smem;
+  const BucketArgs ba = bucket_args_shared(ba0, splits, bk_smem + BK_MAXB + 1);
   for (uint32_t b = threadIdx.x; b <= ba.nb; b += BK_T) h[b] = 0;
   __syncthreads();
   const uint64_t base = (uint64_t)blockIdx.x * BK_TILE;
@@ -259,9 +286,11 @@ struct LoadCnt32 {
 };
 
 __global__ void __launch_bounds__(BK_T)
-    k_bucket_place(const uint64_t *keys, uint64_t k, BucketArgs ba, uint32_t nct,
-                   const uint64_t *offm, uint64_t *out) {
-  __shared__ uint32_t fill[BK_MAXB + 1];
+    k_bucket_place(const uint64_t *keys, uint64_t k, BucketArgs ba0, const uint32_t *splits,
+                   uint32_t nct, const uint64_t *offm, uint64_t *out) {
+  extern __shared__ uint32_t bk_smem[];
+  uint32_t *fill = bk_smem;
+  const BucketArgs ba = bucket_args_shared(ba0, splits, bk_smem + BK_MAXB + 1);
   for (uint32_t b = threadIdx.x; b <= ba.nb; b += BK_T) fill[b] = 0;
   __syncthreads();
   const uint64_t base = (uint64_t)blockIdx.x * BK_TILE;
@@ -442,13 +471,16 @@ struct BucketLayout {
   uint64_t total() const { return cnt_w + off_w + scan_w + list_w + 3; }
 };
 
-BucketLayout bucket_layout(uint64_t k, uint32_t n) {
+BucketLayout bucket_layout(uint64_t k, uint32_t n, bool splits) {
   BucketLayout L{};
-  // about 128 keys per bucket, at most BK_MAXB buckets: bucket = source >> shift
-  const uint64_t target = std::max<uint64_t>(1, std::min<uint64_t>(BK_MAXB, k / 128));
-  L.shift = 0;
-  while (L.shift < 31 && ceil_div((uint64_t)n, 1ull << L.shift) > target) L.shift++;
-  L.nb = (uint32_t)ceil_div((uint64_t)n, 1ull << L.shift);
+  if (splits) {  // the split points' BK_MAXB buckets
+    L.nb = BK_MAXB;
+  } else {  // about 128 keys per bucket, at most BK_MAXB: bucket = source >> shift
+    const uint64_t target = std::max<uint64_t>(1, std::min<uint64_t>(BK_MAXB, k / 128));
+    L.shift = 0;
+    while (L.shift < 31 && ceil_div((uint64_t)n, 1ull << L.shift) > target) L.shift++;
+    L.nb = (uint32_t)ceil_div((uint64_t)n, 1ull << L.shift);
+  }
   L.nct = (uint32_t)ceil_div(k, BK_TILE);
   L.cells = ((uint64_t)L.nb + 1) * L.nct;
   L.list_cap = std::min<uint64_t>(L.nb, k / 33) + 1;
@@ -459,25 +491,55 @@ BucketLayout bucket_layout(uint64_t k, uint32_t n) {
   return L;
 }
 
+// split j = the source of sorted key j * k / BK_MAXB (sources of invalid
+// keys read as n): BK_MAXB buckets of about equal counts for batches drawn
+// like this one
+__global__ void k_bucket_learn(const uint64_t *sorted, uint64_t k, uint32_t n, uint32_t *splits) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > BK_MAXB) return;
+  uint32_t v = n;
+  if (j == 0) {
+    v = 0;
+  } else if (j < BK_MAXB) {
+    const uint64_t x = sorted[(uint64_t)j * k / BK_MAXB];
+    v = x == BK_INVALID ? n : (uint32_t)(x >> 32);
+  }
+  splits[j] = v;
+}
+
 }  // namespace
 
-uint64_t bucket_tmp_elems(uint64_t k, uint32_t n) { return bucket_layout(k, n).total(); }
+void bucket_learn_splits(const uint64_t *sorted, uint64_t k, uint32_t n, uint32_t *splits,
+                         cudaStream_t s, Profiler &prof) {
+  if (k == 0) return;
+  TRC_LAUNCH(prof, s, "bsort_learn", ceil_div(BUCKET_SPLITS + 1, 256), 256, 0, k_bucket_learn,
+             sorted, k, n, splits);
+}
+
+uint64_t bucket_tmp_elems(uint64_t k, uint32_t n, bool splits) {
+  return bucket_layout(k, n, splits).total();
+}
 
 uint64_t *bucket_sort_u64(const uint64_t *keys, uint64_t *alt, uint64_t k, uint32_t n,
-                          uint64_t *tmp, cudaStream_t s, Profiler &prof, uint32_t *err) {
+                          uint64_t *tmp, cudaStream_t s, Profiler &prof, uint32_t *err,
+                          const uint32_t *splits) {
   if (k == 0) return alt;
-  const BucketLayout L = bucket_layout(k, n);
-  const BucketArgs ba{L.nb, L.shift};
+  const BucketLayout L = bucket_layout(k, n, splits != nullptr);
+  const BucketArgs ba{L.nb, L.shift, nullptr};
   uint32_t *counts = reinterpret_cast<uint32_t *>(tmp);
   uint64_t *offm = tmp + L.cnt_w;
   uint64_t *st = offm + L.off_w;
   uint32_t *lists = reinterpret_cast<uint32_t *>(st + L.scan_w);
   unsigned long long *nlist = reinterpret_cast<unsigned long long *>(st + L.scan_w + L.list_w);
   TRC_CUDA(cudaMemsetAsync(nlist, 0, 3 * 8, s));
-  TRC_LAUNCH(prof, s, "bsort_count", L.nct, BK_T, 0, k_bucket_count, keys, k, ba, L.nct, counts);
+  const int smem = (int)(2 * (BK_MAXB + 1) * sizeof(uint32_t));  // counters + split points
+  TRC_CUDA(cudaFuncSetAttribute(k_bucket_count, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  TRC_CUDA(cudaFuncSetAttribute(k_bucket_place, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  TRC_LAUNCH(prof, s, "bsort_count", L.nct, BK_T, smem, k_bucket_count, keys, k, ba, splits, L.nct,
+             counts);
   exclusive_scan(LoadCnt32{counts}, L.cells, offm, st, s, prof, "bsort_scan");
-  TRC_LAUNCH(prof, s, "bsort_place", L.nct, BK_T, 0, k_bucket_place, keys, k, ba, L.nct, offm,
-             alt);
+  TRC_LAUNCH(prof, s, "bsort_place", L.nct, BK_T, smem, k_bucket_place, keys, k, ba, splits, L.nct,
+             offm, alt);
   const BucketOff off{offm, L.nct};
   TRC_LAUNCH(prof, s, "bsort_small", ceil_div((uint64_t)L.nb, 256), 256, 0, k_bucket_sort_small,
              off, L.nb, alt, lists, L.list_cap, nlist, err);

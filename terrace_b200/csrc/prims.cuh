@@ -264,22 +264,33 @@ uint64_t *radix_sort_u64_shifts(uint64_t *keys, uint64_t *alt, uint64_t n, const
 uint64_t radix_tmp_elems(uint64_t n);
 
 // ------------------------------------------------------------ bucket sort
-// Sorts k keys (src<<32|dst with src < n, or KEY_INVALID = ~0) ascending:
-// keys are bucketed on the source's high bits (bucket = src >> shift, with
-// the smallest shift that leaves at most one bucket per key; a count per
-// bucket, a scan, a scatter, both with one atomic per distinct bucket of a
-// warp), then each bucket is sorted whole (up to 16 keys in a thread's
-// registers, up to 32 across a warp, up to 256 in a warp's shared memory,
-// up to BUCKET_SEG_MAX by a CTA).  O(n >> shift + k) traffic in about 8
-// launches: for batches of more than a few thousand keys it moves far fewer
-// bytes than the radix sort's passes.  A bucket above BUCKET_SEG_MAX keys is
-// left unsorted and ERR_BIGSEG or-ed into err: the caller must then sort
-// with the radix sort instead.  Writes the sorted keys to alt (keys is left
-// unchanged) and returns alt.  tmp: bucket_tmp_elems(k, n) entries.
+// Sorts k keys (src<<32|dst with src < n, or KEY_INVALID = ~0) ascending in
+// one MSD pass plus whole-bucket sorts.  Buckets are source ranges: with
+// `splits` (BUCKET_SPLITS + 1 non-decreasing source ids, splits[0] = 0, as
+// bucket_learn_splits writes them) bucket b holds the sources
+// [splits[b], splits[b+1]), so a batch drawn like the one the splits were
+// learned from fills the buckets about evenly however skewed its sources
+// are; without, bucket = source >> shift (about 128 keys per bucket for
+// uniform sources).  Tiles of 16384 keys count their buckets in shared
+// memory, one scan of the (bucket, tile) counts gives every tile its output
+// offsets, the tiles place their keys, and each bucket is then sorted whole
+// (up to 16 keys in a thread's registers, up to 32 across a warp, up to 256
+// in a warp's shared memory, up to BUCKET_SEG_MAX by a CTA).  No global
+// atomics.  A bucket above BUCKET_SEG_MAX keys is left unsorted and
+// ERR_BIGSEG or-ed into err: the caller must then sort with the radix sort
+// instead.  Writes the sorted keys to alt (keys is left unchanged) and
+// returns alt.  tmp: bucket_tmp_elems(k, n, splits != null) entries.
 constexpr uint32_t BUCKET_SEG_MAX = 16384;
+constexpr uint32_t BUCKET_SPLITS = 8192;
 uint64_t *bucket_sort_u64(const uint64_t *keys, uint64_t *alt, uint64_t k, uint32_t n,
-                          uint64_t *tmp, cudaStream_t s, Profiler &prof, uint32_t *err);
-uint64_t bucket_tmp_elems(uint64_t k, uint32_t n);
+                          uint64_t *tmp, cudaStream_t s, Profiler &prof, uint32_t *err,
+                          const uint32_t *splits);
+uint64_t bucket_tmp_elems(uint64_t k, uint32_t n, bool splits);
+// Split points for the next batches from a sorted batch of k keys: split j =
+// the source of key j * k / BUCKET_SPLITS (n for invalid keys), split 0 = 0,
+// split BUCKET_SPLITS = n.
+void bucket_learn_splits(const uint64_t *sorted, uint64_t k, uint32_t n, uint32_t *splits,
+                         cudaStream_t s, Profiler &prof);
 
 // ------------------------------------------------------------ merge path
 // Merge of two sorted u64 arrays without common elements (A first on ties).

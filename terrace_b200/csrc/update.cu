@@ -944,10 +944,17 @@ retry_sort:
   uint64_t *A = s_A.ensure(k2), *B = s_B.ensure(k2);
   TRC_LAUNCH(prof, stream, "upd_make_keys", ceil_div(k, 256), 256, 0, k_make_keys, src, dst, k, n,
              sym, drop, A, err.get());
+  const uint32_t *splits = bsplits_ok ? bsplits.get() : nullptr;
   uint64_t *t = tmp(std::max({radix_tmp_elems(k2), select_tmp_elems(k2),
-                              bucket ? bucket_tmp_elems(k2, n) : (uint64_t)0}));
-  uint64_t *sorted = bucket ? bucket_sort_u64(A, B, k2, n, t, stream, prof, err.get())
+                              bucket ? bucket_tmp_elems(k2, n, splits != nullptr) : (uint64_t)0}));
+  uint64_t *sorted = bucket ? bucket_sort_u64(A, B, k2, n, t, stream, prof, err.get(), splits)
                             : radix_sort_u64(A, B, k2, vbits(), t, stream, prof, err.get(), sort_wait);
+  // the next batches' bucket boundaries: quantiles of this batch's sources
+  // (a batch large enough to show the distribution)
+  if (k2 >= BUCKET_MIN_KEYS) {
+    bucket_learn_splits(sorted, k2, n, bsplits.ensure(BUCKET_SPLITS + 1), stream, prof);
+    bsplits_ok = true;
+  }
   uint64_t *bkeys = sorted == A ? B : A;
   // 3: unique + existence filter (one lookup per key), compacted
   uint8_t *kflags = s_flags.ensure(k2);
