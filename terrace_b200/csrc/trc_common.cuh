@@ -310,7 +310,7 @@ class DBuf {
     if (count > cap_) {
       reset();
       uint64_t c = count < 16 ? 16 : count;
-      ptr_ = static_cast<T *>(budget_->alloc(c * sizeof(T)));
+      ptr_ = static_cast<T *>(bud().alloc(c * sizeof(T)));
       cap_ = c;
     }
     return ptr_;
@@ -319,7 +319,7 @@ class DBuf {
   T *alloc_exact(uint64_t count) {
     reset();
     uint64_t c = count < 1 ? 1 : count;
-    ptr_ = static_cast<T *>(budget_->alloc(c * sizeof(T)));
+    ptr_ = static_cast<T *>(bud().alloc(c * sizeof(T)));
     cap_ = c;
     return ptr_;
   }
@@ -329,7 +329,7 @@ class DBuf {
     if (count <= cap_) return ptr_;
     if (keep > cap_) keep = cap_;
     uint64_t c = count < 16 ? 16 : count;
-    T *np = static_cast<T *>(budget_->alloc(c * sizeof(T)));
+    T *np = static_cast<T *>(bud().alloc(c * sizeof(T)));
     if (keep) TRC_CUDA(cudaMemcpyAsync(np, ptr_, keep * sizeof(T), cudaMemcpyDeviceToDevice, s));
     TRC_CUDA(cudaStreamSynchronize(s));
     reset();
@@ -355,6 +355,10 @@ class DBuf {
   T *ptr_ = nullptr;
   uint64_t cap_ = 0;
   Budget *budget_ = nullptr;
+  Budget &bud() {
+    if (!budget_) throw_error(TRC_ERR_STATE, "device buffer used before it was bound to a budget");
+    return *budget_;
+  }
 };
 
 // ---------------------------------------------------------------------------

@@ -73,6 +73,7 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   s_tix.bind(&budget);
   s_wbits.bind(&budget);
   s_hw_do.bind(&budget);
+  bsplits.bind(&budget);
   s_hw_h.bind(&budget);
   s_flags.bind(&budget);
 
