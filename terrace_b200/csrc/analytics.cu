@@ -1526,7 +1526,7 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
 // 51-87); both orders count each triangle exactly once, and the degree order
 // bounds the intersection work on skewed graphs.  N+ is materialised once as
 // an oriented CSR snapshot, then one warp per vertex intersects sorted lists
-// (lanes binary-search the shorter list's elements in the longer one).
+// (k_tc_intersect).
 
 __device__ __forceinline__ bool ranked_above(const uint32_t *deg, uint32_t x, uint32_t du,
                                              uint32_t u) {
@@ -1564,32 +1564,70 @@ __global__ void k_tc_fill(DevView G, const uint64_t *off, uint32_t *adj) {
   }
 }
 
-__global__ void k_tc_intersect(uint32_t n, const uint64_t *off, const uint32_t *adj,
-                               unsigned long long *total) {
-  uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
-  uint32_t lane = threadIdx.x & 31;
-  if (w >= n) return;
-  uint32_t u = (uint32_t)w;
-  const uint32_t *A = adj + off[u];
-  uint32_t na = (uint32_t)(off[u + 1] - off[u]);
+// Is x in the sorted list p[0..len)?
+__device__ __forceinline__ bool sorted_has(const uint32_t *p, uint32_t len, uint32_t x) {
+  uint32_t lo = 0, hi = len;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (p[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo < len && p[lo] == x;
+}
+
+// One warp per vertex u (grid-stride).  N+(u) is staged in the warp's
+// shared slice when it fits (TC_STAGE ids); the lanes first load the list
+// offsets of 32 of u's out-neighbours v at once, then for each v either
+// walk N+(v) (coalesced) and look each element up in the staged N+(u) (a
+// shared-memory search), or, when N+(v) is much longer, look N+(u)'s
+// elements up in N+(v) (a global binary search).  Lists longer than the
+// slice take the global search both ways.
+constexpr uint32_t TC_STAGE = 256;
+
+__global__ void __launch_bounds__(AT) k_tc_intersect(uint32_t n, const uint64_t *off,
+                                                     const uint32_t *adj,
+                                                     unsigned long long *total) {
+  __shared__ uint32_t stage[AT / 32][TC_STAGE];
+  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  uint32_t *As = stage[wib];
+  const uint64_t W = ((uint64_t)gridDim.x * AT) >> 5;
   unsigned long long c = 0;
-  for (uint32_t i = 0; i < na; i++) {
-    uint32_t v = A[i];
-    const uint32_t *B = adj + off[v];
-    uint32_t nb = (uint32_t)(off[v + 1] - off[v]);
-    const uint32_t *Sm = na < nb ? A : B;
-    const uint32_t *Lg = na < nb ? B : A;
-    uint32_t ns = na < nb ? na : nb, nl = na < nb ? nb : na;
-    for (uint32_t j = lane; j < ns; j += 32) {
-      uint32_t x = Sm[j];
-      uint32_t lo = 0, hi = nl;
-      while (lo < hi) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (Lg[mid] < x) lo = mid + 1;
-        else hi = mid;
-      }
-      c += (lo < nl && Lg[lo] == x);
+  for (uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5; w < n; w += W) {
+    const uint32_t u = (uint32_t)w;
+    const uint64_t a0 = off[u];
+    const uint32_t na = (uint32_t)(off[u + 1] - a0);
+    if (na < 2) continue;  // (warp-uniform)
+    const uint32_t *A = adj + a0;
+    const bool staged = na <= TC_STAGE;
+    if (staged) {
+      for (uint32_t t = lane; t < na; t += 32) As[t] = A[t];
+      __syncwarp();
     }
+    const uint32_t *Al = staged ? As : A;
+    for (uint32_t i0 = 0; i0 < na; i0 += 32) {
+      const uint32_t iv = i0 + lane;
+      uint64_t b = 0;
+      uint32_t nb = 0;
+      if (iv < na) {
+        const uint32_t v = A[iv];
+        b = off[v];
+        nb = (uint32_t)(off[v + 1] - b);
+      }
+      const uint32_t cnt = na - i0 < 32 ? na - i0 : 32;
+      for (uint32_t j = 0; j < cnt; j++) {
+        const uint64_t bj = __shfl_sync(0xFFFFFFFFu, b, j);
+        const uint32_t nbj = __shfl_sync(0xFFFFFFFFu, nb, j);
+        const uint32_t *B = adj + bj;
+        if (staged && nbj <= 8 * na) {
+          for (uint32_t t = lane; t < nbj; t += 32) c += sorted_has(As, na, B[t]);
+        } else if (na <= nbj) {
+          for (uint32_t t = lane; t < na; t += 32) c += sorted_has(B, nbj, Al[t]);
+        } else {
+          for (uint32_t t = lane; t < nbj; t += 32) c += sorted_has(Al, na, B[t]);
+        }
+      }
+    }
+    __syncwarp();
   }
   c = warp_sum(c);
   if (lane == 0 && c) atomicAdd(total, c);
@@ -1614,8 +1652,9 @@ uint64_t Graph::tc() {
   uint32_t *adj = adjb.alloc_exact(mo ? mo : 1);
   TRC_LAUNCH(prof, stream, "tc_fill", ceil_div((uint64_t)n * 32, AT), AT, 0, k_tc_fill, G, off, adj);
   TRC_CUDA(cudaMemsetAsync(total, 0, 8, stream));
-  TRC_LAUNCH(prof, stream, "tc_intersect", ceil_div((uint64_t)n * 32, AT), AT, 0, k_tc_intersect, n,
-             off, adj, (unsigned long long *)total);
+  TRC_LAUNCH(prof, stream, "tc_intersect",
+             std::min<uint64_t>(ceil_div((uint64_t)n * 32, AT), resident_grid(k_tc_intersect, AT)), AT,
+             0, k_tc_intersect, n, off, adj, (unsigned long long *)total);
   return read_u64(total);
 }
 
