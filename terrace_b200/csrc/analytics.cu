@@ -708,22 +708,14 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
     for (uint32_t i = 0; i < BP_V; i++)
       v[i] = act[i] ? __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u[i] * K_INLINE) + q)
                     : make_uint4(0, 0, 0, 0);
-    // frontier-bitmap probes in two rounds: first ranks 0, 4, 8, 12 (one per
-    // lane of the quad), then the other twelve only for vertices with no
-    // frontier neighbour among those four -- on power-law graphs most
-    // vertices of a dense level have one among their first neighbours, and
-    // the probes, not the row bytes, are what the step is bound by
     uint32_t wx[BP_V], wy[BP_V], wz[BP_V], ww[BP_V];
 #pragma unroll
-    for (uint32_t i = 0; i < BP_V; i++) wx[i] = act[i] ? __ldg(s.bits + (v[i].x >> 5)) : 0u;
-#pragma unroll
     for (uint32_t i = 0; i < BP_V; i++) {
-      const uint32_t m = __ballot_sync(0xFFFFFFFFu, (wx[i] >> (v[i].x & 31)) & 1u);
-      const bool need = act[i] && ((m >> (lane & ~3u)) & 0xFu) == 0;
       const uint32_t e = q * 4;
-      wy[i] = need && e + 1 < d[i] ? __ldg(s.bits + (v[i].y >> 5)) : 0u;
-      wz[i] = need && e + 2 < d[i] ? __ldg(s.bits + (v[i].z >> 5)) : 0u;
-      ww[i] = need && e + 3 < d[i] ? __ldg(s.bits + (v[i].w >> 5)) : 0u;
+      wx[i] = act[i] ? __ldg(s.bits + (v[i].x >> 5)) : 0u;
+      wy[i] = act[i] && e + 1 < d[i] ? __ldg(s.bits + (v[i].y >> 5)) : 0u;
+      wz[i] = act[i] && e + 2 < d[i] ? __ldg(s.bits + (v[i].z >> 5)) : 0u;
+      ww[i] = act[i] && e + 3 < d[i] ? __ldg(s.bits + (v[i].w >> 5)) : 0u;
     }
 #pragma unroll
     for (uint32_t i = 0; i < BP_V; i++) {
