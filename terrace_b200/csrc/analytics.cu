@@ -210,6 +210,75 @@ __global__ void __launch_bounds__(AT) k_pr_S(DevView G, const uint32_t *S, uint6
   if (vi < nS && q == 0) pr_store(a, u, d, sum);
 }
 
+// Load-balanced pull.  Warp w takes list entries [32w, 32w+32); their
+// neighbour lists (inline row, then PMA segment or hub blocks) are flattened
+// and walked 64 elements per step: each lane finds the owner of its element
+// with a shuffle binary search over the lanes' start offsets, loads the
+// neighbour id and applies Op::gather; a segmented warp scan sums per owner
+// and the segment's last lane adds into the owner's slot in shared memory.
+// Every load of a step is independent of the others, so a warp keeps 64
+// index loads and 64 gathers in flight instead of one vertex's chain.
+struct FlatWarp {
+  uint32_t u, d, start, total;
+  int32_t hub;  // hub index, or -1
+  const uint32_t *seg;
+  bool valid;
+};
+
+template <class Op>
+__device__ __forceinline__ FlatWarp flat_setup(const DevView &G, const uint32_t *V, uint64_t nV,
+                                               uint64_t base, const Op &op) {
+  FlatWarp f;
+  uint32_t lane = threadIdx.x & 31;
+  uint64_t idx = base + lane;
+  f.valid = idx < nV;
+  f.u = f.valid ? V[idx] : 0;
+  f.d = 0;
+  f.hub = -1;
+  f.seg = G.pma;
+  if (f.valid && !op.skip(f.u)) {
+    f.d = G.deg[f.u];
+    if (f.d > K_INLINE) {
+      f.hub = G.hub_of[f.u];
+      if (f.hub < 0) f.seg = G.pma + G.pbeg[f.u];
+    }
+  }
+  uint32_t incl = warp_incl_scan(f.d);
+  f.start = incl - f.d;
+  f.total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  return f;
+}
+
+// owner lane of flattened element e (largest lane v with start_v <= e)
+__device__ __forceinline__ int flat_owner(const FlatWarp &f, uint32_t e) {
+  int v = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1) {
+    uint32_t sv = __shfl_sync(0xFFFFFFFFu, f.start, v + step);
+    if (sv <= e) v += step;
+  }
+  return v;
+}
+
+// element of flattened index e (owner v): its rank r = e - start_v
+__device__ __forceinline__ uint32_t flat_fetch(const DevView &G, const FlatWarp &f, int v,
+                                               uint32_t e, bool act) {
+  uint32_t uo = __shfl_sync(0xFFFFFFFFu, f.u, v);
+  uint32_t so = __shfl_sync(0xFFFFFFFFu, f.start, v);
+  int32_t ho = __shfl_sync(0xFFFFFFFFu, f.hub, v);
+  uint32_t dh = __shfl_sync(0xFFFFFFFFu, f.d, v);
+  const uint32_t *sg = (const uint32_t *)__shfl_sync(0xFFFFFFFFu, (unsigned long long)f.seg, v);
+  if (!act) return 0;
+  uint32_t r = e - so;
+  if (r < K_INLINE) return __ldg(G.inl + (uint64_t)uo * K_INLINE + r);
+  r -= K_INLINE;
+  if (ho < 0) return __ldg(sg + r);
+  // a hub: the directory entry of hub rank r
+  const uint64_t e0 = G.hub_dir0[ho];
+  const uint32_t i = hub_entry_of_rank(G.hpre + e0, G.hub_nblk[ho], dh - K_INLINE, r);
+  return __ldg(G.hslot + (uint64_t)G.hdir[e0 + i] * HUB_BLOCK + (r - G.hpre[e0 + i]));
+}
+
 // segmented inclusive sum over lanes (segments = equal owner), tail lanes
 // add the segment total into acc[owner]
 __device__ __forceinline__ void flat_seg_add(double val, int v, double *acc) {
