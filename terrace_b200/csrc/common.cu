@@ -1,5 +1,6 @@
 // common.cu -- error plumbing, budgeted device allocation and the CUDA-event
 // profiler shared by every entry point.
+#include <atomic>
 #include <cstdio>
 #include <string>
 
@@ -123,12 +124,17 @@ Profiler::~Profiler() {
 }
 
 int num_sms() {
-  static int sms = 0;
+  // per device (the current one), cached; a race between threads only
+  // stores the same value twice
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::atomic<int> *slot = dev >= 0 && dev < 64 ? &cache[dev] : nullptr;
+  int sms = slot ? slot->load(std::memory_order_relaxed) : 0;
   if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (sms <= 0) sms = 148;
+    if (slot) slot->store(sms, std::memory_order_relaxed);
   }
   return sms;
 }
