@@ -89,20 +89,22 @@ __device__ __forceinline__ uint32_t warp_append(bool win, uint32_t *counter) {
 }
 
 // Per-warp staging of list appends from many chunks: the warp's winners of
-// a chunk are written to 32 shared slots and go out with one atomic when
-// the slots fill (and at the end, flush), instead of one atomic per chunk
-// on the list's counter, which every warp of the grid hits.  Calls are
-// warp-uniform.
+// a chunk are written to `cap` shared slots (a multiple of 32) and go out
+// with one atomic when the slots fill (and at the end, flush), instead of
+// one atomic per chunk on the list's counter, which every warp of the grid
+// hits.  Calls are warp-uniform.
+constexpr uint32_t WS_BIG = 128;  // slots of the stages of the busiest lists
 struct WarpStage {
-  uint32_t *slot;  // 32 shared words of this warp
+  uint32_t *slot;  // `cap` shared words of this warp
   uint32_t cnt;
+  uint32_t cap = 32;
   __device__ void flush(uint32_t *list, uint32_t *counter, uint32_t lane) {
     __syncwarp();
     if (cnt) {
       uint32_t base = 0;
       if (lane == 0) base = atomicAdd(counter, cnt);
       base = __shfl_sync(0xFFFFFFFFu, base, 0);
-      if (lane < cnt) list[base + lane] = slot[lane];
+      for (uint32_t i = lane; i < cnt; i += 32) list[base + i] = slot[i];
     }
     __syncwarp();
     cnt = 0;
@@ -111,10 +113,10 @@ struct WarpStage {
     const uint32_t m = __ballot_sync(0xFFFFFFFFu, win);
     if (!m) return;
     const uint32_t k = __popc(m);
-    if (cnt + k > 32) flush(list, counter, lane);
+    if (cnt + k > cap) flush(list, counter, lane);
     if (win) slot[cnt + __popc(m & lanemask_lt())] = v;
     cnt += k;
-    if (cnt == 32) flush(list, counter, lane);
+    if (cnt == cap) flush(list, counter, lane);
   }
 };
 
@@ -590,8 +592,8 @@ __global__ void __launch_bounds__(AT) k_bfs_push_lb(DevView G, const uint32_t *F
   const uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
   const uint64_t T = off[nf];
   const uint64_t lo = T * w / W, hi = T * (w + 1) / W;
-  __shared__ uint32_t stg[AT / 32][32];
-  WarpStage st{stg[threadIdx.x >> 5], 0};
+  __shared__ uint32_t stg[AT / 32][WS_BIG];
+  WarpStage st{stg[threadIdx.x >> 5], 0, WS_BIG};
   if (lo < hi) {
     uint32_t i = piece_owner(off, nf, lo);
     uint32_t u = F[i];
@@ -663,8 +665,8 @@ constexpr uint32_t BP_V = 4;
 __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S, uint64_t nS,
                                                    BFSState s) {
   const uint32_t lane = threadIdx.x & 31, q = lane & 3, qw = lane >> 2, wib = threadIdx.x >> 5;
-  __shared__ uint32_t stg[4][AT / 32][32];
-  WarpStage sn{stg[0][wib], 0}, ss{stg[1][wib], 0}, sc{stg[2][wib], 0}, sl{stg[3][wib], 0};
+  __shared__ uint32_t stg[3][AT / 32][32], stn[AT / 32][WS_BIG];
+  WarpStage sn{stn[wib], 0, WS_BIG}, ss{stg[0][wib], 0}, sc{stg[1][wib], 0}, sl{stg[2][wib], 0};
   const uint64_t step = (((uint64_t)gridDim.x * AT) >> 5) * (8 * BP_V);
   for (uint64_t wbase = (((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5) * (8 * BP_V); wbase < nS;
        wbase += step) {
@@ -814,8 +816,8 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_G8(DevView G, const uint32_t *L
                                                     const uint32_t *nL_dev, BFSState s) {
   constexpr uint32_t R = (BFS_SHORT - K_INLINE) / 8;
   const uint32_t lane = threadIdx.x & 31, q = lane & 7, grp = lane >> 3, wib = threadIdx.x >> 5;
-  __shared__ uint32_t stg[2][AT / 32][32];
-  WarpStage sn{stg[0][wib], 0}, sc{stg[1][wib], 0};
+  __shared__ uint32_t stg[AT / 32][32], stn[AT / 32][WS_BIG];
+  WarpStage sn{stn[wib], 0, WS_BIG}, sc{stg[wib], 0};
   const uint64_t nL = *nL_dev;
   const uint64_t step = (((uint64_t)gridDim.x * AT) >> 5) * 4;
   for (uint64_t base = (((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5) * 4; base < nL;
@@ -1164,8 +1166,8 @@ __global__ void __launch_bounds__(AT) k_bc_push_lb(DevView G, const uint32_t *F,
   const uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
   const uint64_t T = off[nf];
   const uint64_t lo = T * w / W, hi = T * (w + 1) / W;
-  __shared__ uint32_t stg[AT / 32][32];
-  WarpStage st{stg[threadIdx.x >> 5], 0};
+  __shared__ uint32_t stg[AT / 32][WS_BIG];
+  WarpStage st{stg[threadIdx.x >> 5], 0, WS_BIG};
   if (lo < hi) {
     uint32_t i = piece_owner(off, nf, lo);
     uint32_t u = F[i];
