@@ -9,7 +9,10 @@ of a round merged into one net change).  Replay: a fresh graph gets the
 same initial edges, then the update requests one by one in arrival order;
 after the updates of version v every query that recorded version v runs
 alone through the plain Graph calls.  BFS levels, degrees and neighbour
-lists must be identical; PageRank within 1e-9 relative (FP64)."""
+lists must be identical; PageRank within 1e-9 relative (FP64).  The replay
+also keeps the oracle's edge set: the first served BFS of every version
+must equal the oracle's levels on it, and the replayed graph must equal it
+at the end."""
 import numpy as np
 import pytest
 
@@ -81,7 +84,8 @@ def _serve(T, server, reqs):
 
 
 def _replay_and_check(T, n, reqs, served, summary=False):
-    g, _ = _initial(T, n)
+    g, (s0, d0) = _initial(T, n)
+    keys = O.make_keys(s0, d0, True, True)  # the oracle's edge set, replayed alongside
     by_version = {}
     for i, (kind, _, _) in enumerate(reqs):
         if kind not in ("ins", "del"):
@@ -96,9 +100,18 @@ def _replay_and_check(T, n, reqs, served, summary=False):
             assert served[upd[ui]][2] == 0
             if kind == "ins":
                 g.add_edge_batch(a, b, symmetrize=True, drop_self_loops=True)
+                keys = O.key_union(keys, O.make_keys(a, b, True, True))
             else:
                 g.remove_edge_batch(a, b, symmetrize=True, drop_self_loops=True)
+                keys = O.key_difference(keys, O.make_keys(a, b, True, True))
             ui += 1
+        # the replayed graph and the served BFS levels pinned to the oracle
+        # too (the first BFS of each version), not only to the library
+        off, tgt = O.csr_from_keys(n, keys)
+        bfs_here = [i for i in by_version.get(v, []) if reqs[i][0] == "bfs"]
+        if bfs_here and not summary:
+            i = bfs_here[0]
+            assert np.array_equal(served[i][0], O.bfs_levels(off, tgt, reqs[i][1])), (i, v)
         for i in by_version.get(v, []):
             kind, a, _ = reqs[i]
             arr, _, st = served[i]
@@ -123,6 +136,9 @@ def _replay_and_check(T, n, reqs, served, summary=False):
                 assert np.allclose(arr, ref, rtol=1e-9, atol=0), (i, v)
             checked += 1
     assert ui == len(upd)
+    off, tgt = O.csr_from_keys(n, keys)
+    goff, gtgt = g.dump_csr()
+    assert np.array_equal(goff, off) and np.array_equal(gtgt, tgt)
     return checked
 
 
