@@ -1549,13 +1549,11 @@ __device__ __forceinline__ bool sorted_has(const uint32_t *p, uint32_t len, uint
   return lo < len && p[lo] == x;
 }
 
-// One warp per vertex u (grid-stride).  N+(u) is staged in the warp's
-// shared slice when it fits (TC_STAGE ids); the lanes first load the list
-// offsets of 32 of u's out-neighbours v at once, then for each v either
-// walk N+(v) (coalesced) and look each element up in the staged N+(u) (a
-// shared-memory search), or, when N+(v) is much longer, look N+(u)'s
-// elements up in N+(v) (a global binary search).  Lists longer than the
-// slice take the global search both ways.
+// One warp per vertex u.  N+(u) is staged in the warp's shared slice when
+// it fits (TC_STAGE ids); the lanes first load the list offsets of 32 of
+// u's out-neighbours v at once, then for each v the lanes walk the shorter
+// of N+(u) and N+(v) and look each element up in the other: in the staged
+// N+(u) by a shared-memory search, in N+(v) by a global binary search.
 constexpr uint32_t TC_STAGE = 256;
 
 __global__ void __launch_bounds__(AT) k_tc_intersect(uint32_t n, const uint64_t *off,
@@ -1564,13 +1562,14 @@ __global__ void __launch_bounds__(AT) k_tc_intersect(uint32_t n, const uint64_t 
   __shared__ uint32_t stage[AT / 32][TC_STAGE];
   const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   uint32_t *As = stage[wib];
-  const uint64_t W = ((uint64_t)gridDim.x * AT) >> 5;
   unsigned long long c = 0;
-  for (uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5; w < n; w += W) {
+  const uint64_t w = ((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5;
+  if (w >= n) return;
+  {
     const uint32_t u = (uint32_t)w;
     const uint64_t a0 = off[u];
     const uint32_t na = (uint32_t)(off[u + 1] - a0);
-    if (na < 2) continue;  // (warp-uniform)
+    if (na < 2) return;  // (warp-uniform)
     const uint32_t *A = adj + a0;
     const bool staged = na <= TC_STAGE;
     if (staged) {
@@ -1592,16 +1591,13 @@ __global__ void __launch_bounds__(AT) k_tc_intersect(uint32_t n, const uint64_t 
         const uint64_t bj = __shfl_sync(0xFFFFFFFFu, b, j);
         const uint32_t nbj = __shfl_sync(0xFFFFFFFFu, nb, j);
         const uint32_t *B = adj + bj;
-        if (staged && nbj <= 8 * na) {
-          for (uint32_t t = lane; t < nbj; t += 32) c += sorted_has(As, na, B[t]);
-        } else if (na <= nbj) {
-          for (uint32_t t = lane; t < na; t += 32) c += sorted_has(B, nbj, Al[t]);
-        } else {
+        if (nbj <= na) {
           for (uint32_t t = lane; t < nbj; t += 32) c += sorted_has(Al, na, B[t]);
+        } else {
+          for (uint32_t t = lane; t < na; t += 32) c += sorted_has(B, nbj, Al[t]);
         }
       }
     }
-    __syncwarp();
   }
   c = warp_sum(c);
   if (lane == 0 && c) atomicAdd(total, c);
@@ -1626,9 +1622,8 @@ uint64_t Graph::tc() {
   uint32_t *adj = adjb.alloc_exact(mo ? mo : 1);
   TRC_LAUNCH(prof, stream, "tc_fill", ceil_div((uint64_t)n * 32, AT), AT, 0, k_tc_fill, G, off, adj);
   TRC_CUDA(cudaMemsetAsync(total, 0, 8, stream));
-  TRC_LAUNCH(prof, stream, "tc_intersect",
-             std::min<uint64_t>(ceil_div((uint64_t)n * 32, AT), resident_grid(k_tc_intersect, AT)), AT,
-             0, k_tc_intersect, n, off, adj, (unsigned long long *)total);
+  TRC_LAUNCH(prof, stream, "tc_intersect", ceil_div((uint64_t)n * 32, AT), AT, 0, k_tc_intersect,
+             n, off, adj, (unsigned long long *)total);
   return read_u64(total);
 }
 
