@@ -652,75 +652,55 @@ __global__ void k_level_bits(const uint32_t *lv, uint32_t n, uint32_t d, uint32_
   }
 }
 
-// Inline pass of a dense step: 4 lanes per vertex (one 128-bit quarter of
-// the 64-byte row each), BP_V vertices per quad.  A quad's vertices are
-// list entries q0 + i * 8 (i < BP_V; the 8 quads of a warp take consecutive
-// entries), and every load of a step is issued for all of them before any
-// is used: list entries, then degree and level, then the row quarters, then
-// the 4 * BP_V frontier-bitmap words.  The first frontier neighbour in
-// sorted order wins (lowest lane of the quad with a hit, then its lowest
-// element).  S == null: the entries are the vertex ids 0 .. nS-1 themselves.
-constexpr uint32_t BP_V = 4;
-
+// Inline pass of a dense step: one thread per vertex (grid-stride; a warp
+// takes 32 consecutive list entries).  Each thread loads its vertex's
+// 64-byte inline row as four 16-byte loads (the warp's rows are one
+// contiguous 2 KB block when the entries are consecutive ids) and then all
+// of its min(deg, 16) frontier-bitmap words, every load issued before any
+// is used; the first frontier neighbour in sorted order is the parent.
+// Vertices left unvisited go to the short or long segment list (PMA
+// vertices) or to the next dense step's candidates.  S == null: the entries
+// are the vertex ids 0 .. nS-1 themselves (hubs left to their own pass).
 __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S, uint64_t nS,
                                                    BFSState s) {
-  const uint32_t lane = threadIdx.x & 31, q = lane & 3, qw = lane >> 2, wib = threadIdx.x >> 5;
+  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   __shared__ uint32_t stg[3][AT / 32][32], stn[AT / 32][WS_BIG];
   WarpStage sn{stn[wib], 0, WS_BIG}, ss{stg[0][wib], 0}, sc{stg[1][wib], 0}, sl{stg[2][wib], 0};
-  const uint64_t step = (((uint64_t)gridDim.x * AT) >> 5) * (8 * BP_V);
-  for (uint64_t wbase = (((uint64_t)blockIdx.x * AT + threadIdx.x) >> 5) * (8 * BP_V); wbase < nS;
-       wbase += step) {
-    uint32_t u[BP_V], d[BP_V];
-    bool act[BP_V];
+  const uint64_t step = (uint64_t)gridDim.x * AT;
+  for (uint64_t base = (uint64_t)blockIdx.x * AT + (threadIdx.x & ~31u); base < nS; base += step) {
+    const uint64_t vi = base + lane;
+    bool act = vi < nS;
+    const uint32_t u = act ? (S ? S[vi] : (uint32_t)vi) : 0u;
+    uint32_t d = act ? G.deg[u] : 0u;
+    if (!S && act && G.hub_of[u] >= 0) d = 0;
+    act = act && d > 0 && s.lv[u] == TRC_UNREACHED;
+    const uint4 *row = reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE);
+    uint32_t x[K_INLINE];
 #pragma unroll
-    for (uint32_t i = 0; i < BP_V; i++) {
-      const uint64_t vi = wbase + i * 8 + qw;
-      u[i] = vi < nS ? (S ? S[vi] : (uint32_t)vi) : 0u;
-      act[i] = vi < nS;
+    for (uint32_t q = 0; q < K_INLINE / 4; q++) {
+      const uint4 t = act && q * 4 < d ? __ldg(row + q) : make_uint4(0, 0, 0, 0);
+      x[4 * q] = t.x;
+      x[4 * q + 1] = t.y;
+      x[4 * q + 2] = t.z;
+      x[4 * q + 3] = t.w;
     }
+    uint32_t wb[K_INLINE];
 #pragma unroll
-    for (uint32_t i = 0; i < BP_V; i++) {
-      d[i] = act[i] ? G.deg[u[i]] : 0u;
-      // (no list: every vertex id, hubs left to their own pass)
-      if (!S && act[i] && G.hub_of[u[i]] >= 0) d[i] = 0;
-      act[i] = act[i] && s.lv[u[i]] == TRC_UNREACHED && q * 4 < d[i];
+    for (uint32_t e = 0; e < K_INLINE; e++) wb[e] = act && e < d ? __ldg(s.bits + (x[e] >> 5)) : 0u;
+    uint32_t p = NONE32;
+#pragma unroll
+    for (int e = K_INLINE - 1; e >= 0; e--)
+      if ((wb[e] >> (x[e] & 31)) & 1u) p = x[e];
+    const bool win = p != NONE32;
+    if (win) {
+      s.par[u] = (int32_t)p;
+      s.lv[u] = s.d + 1;
     }
-    uint4 v[BP_V];
-#pragma unroll
-    for (uint32_t i = 0; i < BP_V; i++)
-      v[i] = act[i] ? __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u[i] * K_INLINE) + q)
-                    : make_uint4(0, 0, 0, 0);
-    uint32_t wx[BP_V], wy[BP_V], wz[BP_V], ww[BP_V];
-#pragma unroll
-    for (uint32_t i = 0; i < BP_V; i++) {
-      const uint32_t e = q * 4;
-      wx[i] = act[i] ? __ldg(s.bits + (v[i].x >> 5)) : 0u;
-      wy[i] = act[i] && e + 1 < d[i] ? __ldg(s.bits + (v[i].y >> 5)) : 0u;
-      wz[i] = act[i] && e + 2 < d[i] ? __ldg(s.bits + (v[i].z >> 5)) : 0u;
-      ww[i] = act[i] && e + 3 < d[i] ? __ldg(s.bits + (v[i].w >> 5)) : 0u;
-    }
-#pragma unroll
-    for (uint32_t i = 0; i < BP_V; i++) {
-      const bool uv = d[i] > 0 && s.lv[u[i]] == TRC_UNREACHED;  // cached: loaded above
-      uint32_t first = 4;
-      if ((wx[i] >> (v[i].x & 31)) & 1u) first = 0;
-      else if ((wy[i] >> (v[i].y & 31)) & 1u) first = 1;
-      else if ((wz[i] >> (v[i].z & 31)) & 1u) first = 2;
-      else if ((ww[i] >> (v[i].w & 31)) & 1u) first = 3;
-      const uint32_t m = __ballot_sync(0xFFFFFFFFu, first < 4);
-      const uint32_t grp = (m >> (lane & ~3u)) & 0xFu;
-      const bool win = grp && (__ffs(grp) - 1) == (int)q;
-      if (win) {
-        const uint32_t p = first == 0 ? v[i].x : first == 1 ? v[i].y : first == 2 ? v[i].z : v[i].w;
-        s.par[u[i]] = (int32_t)p;
-        s.lv[u[i]] = s.d + 1;
-      }
-      const bool left = q == 0 && uv && grp == 0;
-      sn.add(win, u[i], s.next, s.next_cnt, lane);
-      ss.add(left && d[i] > K_INLINE && d[i] <= BFS_SHORT, u[i], s.seg, s.seg_cnt, lane);
-      sl.add(left && d[i] > BFS_SHORT, u[i], s.seg2, s.seg2_cnt, lane);
-      sc.add(left && d[i] <= K_INLINE, u[i], s.cand, s.cand_cnt, lane);
-    }
+    const bool left = act && !win;
+    sn.add(win, u, s.next, s.next_cnt, lane);
+    ss.add(left && d > K_INLINE && d <= BFS_SHORT, u, s.seg, s.seg_cnt, lane);
+    sl.add(left && d > BFS_SHORT, u, s.seg2, s.seg2_cnt, lane);
+    sc.add(left && d <= K_INLINE, u, s.cand, s.cand_cnt, lane);
   }
   sn.flush(s.next, s.next_cnt, lane);
   ss.flush(s.seg, s.seg_cnt, lane);
@@ -936,8 +916,7 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
       // those left unvisited go to a segment list (PMA vertices: short or
       // long) or the next candidates
       TRC_LAUNCH(prof, stream, "bfs_pull_inline",
-                 std::min<uint64_t>(ceil_div(ncand * 4, (uint64_t)AT * BP_V),
-                                    resident_grid(k_bfs_pull_S, AT)),
+                 std::min<uint64_t>(ceil_div(ncand, (uint64_t)AT), resident_grid(k_bfs_pull_S, AT)),
                  AT, 0, k_bfs_pull_S, G, cand, ncand, s);
       // pass B: the PMA segments of the segment lists (counts on the
       // device; short lists 8 lanes per vertex, long ones a warp); hubs
