@@ -554,9 +554,10 @@ __device__ __forceinline__ void bfs_push_span(const uint32_t *p, uint32_t len, u
   uint32_t v = 0;
   if (lane < len) {
     v = p[lane];
-    // (the parent is claimed before the level is written: a claimed parent
-    // saves a contended CAS on a popular neighbour)
-    if (s.lv[v] == TRC_UNREACHED && s.par[v] == -1 && atomicCAS(&s.par[v], -1, (int32_t)u) == -1) {
+    // (every visited vertex has its parent set, and a parent is claimed
+    // before the level is written: one load filters both the visited and
+    // the just-claimed neighbours before a contended CAS)
+    if (s.par[v] == -1 && atomicCAS(&s.par[v], -1, (int32_t)u) == -1) {
       s.lv[v] = s.d + 1;
       win = true;
     }
