@@ -48,7 +48,7 @@ S24 = (24, 32, 0.57, 0.19, 0.19)
 # batches (log-uniform size in [1, 1e6], half inserts, half deletes), 25%
 # single-source BFS, 10% degree / neighbour-list lookups, 5% PageRank (10 it)
 SERVE = dict(scale=25, ef=16, seed=3, rates=(50, 100, 150, 200, 250, 300, 350, 400, 450, 500, 600, 700, 800),
-             seconds=2.5, min_reqs=120, max_reqs=2000, repeats=2, hbm_budget=96 << 30)
+             seconds=2.5, min_reqs=120, max_reqs=2000, repeats=3, hbm_budget=96 << 30)
 
 
 def load_peaks():
