@@ -656,9 +656,10 @@ __global__ void k_level_bits(const uint32_t *lv, uint32_t n, uint32_t d, uint32_
 // Inline pass of a dense step: one thread per vertex (grid-stride; a warp
 // takes 32 consecutive list entries).  Each thread loads its vertex's
 // 64-byte inline row as four 16-byte loads (the warp's rows are one
-// contiguous 2 KB block when the entries are consecutive ids) and then all
-// of its min(deg, 16) frontier-bitmap words, every load issued before any
-// is used; the first frontier neighbour in sorted order is the parent.
+// contiguous 2 KB block when the entries are consecutive ids) and then its
+// frontier-bitmap words (the first four, then the rest on a miss), every
+// load of a round issued before any is used; the first frontier neighbour
+// in sorted order is the parent.
 // Vertices left unvisited go to the short or long segment list (PMA
 // vertices) or to the next dense step's candidates.  S == null: the entries
 // are the vertex ids 0 .. nS-1 themselves (hubs left to their own pass).
@@ -685,13 +686,23 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
       x[4 * q + 2] = t.z;
       x[4 * q + 3] = t.w;
     }
+    // bitmap probes of the first four neighbours, then of the other twelve
+    // only for vertices with no frontier neighbour among those four (on
+    // power-law graphs most have one there; the probes are L2 requests)
     uint32_t wb[K_INLINE];
 #pragma unroll
-    for (uint32_t e = 0; e < K_INLINE; e++) wb[e] = act && e < d ? __ldg(s.bits + (x[e] >> 5)) : 0u;
+    for (uint32_t e = 0; e < 4; e++) wb[e] = act && e < d ? __ldg(s.bits + (x[e] >> 5)) : 0u;
     uint32_t p = NONE32;
 #pragma unroll
-    for (int e = K_INLINE - 1; e >= 0; e--)
+    for (int e = 3; e >= 0; e--)
       if ((wb[e] >> (x[e] & 31)) & 1u) p = x[e];
+    if (act && p == NONE32 && d > 4) {
+#pragma unroll
+      for (uint32_t e = 4; e < K_INLINE; e++) wb[e] = e < d ? __ldg(s.bits + (x[e] >> 5)) : 0u;
+#pragma unroll
+      for (int e = K_INLINE - 1; e >= 4; e--)
+        if ((wb[e] >> (x[e] & 31)) & 1u) p = x[e];
+    }
     const bool win = p != NONE32;
     if (win) {
       s.par[u] = (int32_t)p;
