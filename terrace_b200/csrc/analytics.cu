@@ -536,6 +536,10 @@ struct BFSState {
   uint32_t *seg, *seg_cnt;
   uint32_t *cand, *cand_cnt;
   uint32_t *seg2, *seg2_cnt;
+  // dense steps: the next level's frontier bitmap (zeroed before the step;
+  // every vertex claimed by the step sets its bit), so that a dense step
+  // after a dense step needs no pass over the levels
+  uint32_t *nbits;
 };
 
 // Degree bound of the short segment list (8 lanes per vertex).
@@ -572,6 +576,20 @@ __device__ __forceinline__ void bfs_push_span(const uint32_t *p, uint32_t len, u
 __global__ void k_list_pieces(DevView G, const uint32_t *F, uint32_t nf, uint32_t *cnt) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nf) cnt[i] = list_pieces(nbr_list(G, F[i]));
+}
+
+// The same and the exclusive prefix in one CTA, for frontiers of at most
+// PIECES_ONE_CTA vertices: off[0..nf], off[nf] = the total.
+constexpr uint32_t PIECES_ONE_CTA = 1024;
+__global__ void __launch_bounds__(PIECES_ONE_CTA)
+    k_list_pieces_scan(DevView G, const uint32_t *F, uint32_t nf, uint64_t *off) {
+  __shared__ uint64_t ws[PIECES_ONE_CTA / 32 + 1];
+  const uint32_t i = threadIdx.x;
+  const uint64_t c = i < nf ? list_pieces(nbr_list(G, F[i])) : 0;
+  uint64_t tot;
+  const uint64_t ex = block_excl_scan<uint64_t, PIECES_ONE_CTA>(c, ws, tot);
+  if (i < nf) off[i] = ex;
+  if (i == 0) off[nf] = tot;
 }
 
 // The frontier vertex of piece t: the i with off[i] <= t < off[i+1] (every
@@ -708,6 +726,14 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
       s.par[u] = (int32_t)p;
       s.lv[u] = s.d + 1;
     }
+    if (S) {
+      if (win) atomicOr(s.nbits + (u >> 5), 1u << (u & 31));
+    } else {
+      // (ids in order: the warp's 32 vertices are one bitmap word, and this
+      // pass is the step's first writer)
+      const uint32_t b = __ballot_sync(0xFFFFFFFFu, win);
+      if (lane == 0) s.nbits[base >> 5] = b;
+    }
     const bool left = act && !win;
     sn.add(win, u, s.next, s.next_cnt, lane);
     ss.add(left && d > K_INLINE && d <= BFS_SHORT, u, s.seg, s.seg_cnt, lane);
@@ -790,6 +816,7 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_W(DevView G, const uint32_t *Ls
       if (p != NONE32 && lane == 0) {
         s.par[u] = (int32_t)p;
         s.lv[u] = s.d + 1;
+        atomicOr(s.nbits + (u >> 5), 1u << (u & 31));
       }
     }
     bw.push(unvisited && p != NONE32, u, s.next, s.next_cnt, lane);
@@ -836,6 +863,7 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_G8(DevView G, const uint32_t *L
     if (win) {
       s.par[u] = (int32_t)p;
       s.lv[u] = s.d + 1;
+      atomicOr(s.nbits + (u >> 5), 1u << (u & 31));
     }
     sn.add(win, u, s.next, s.next_cnt, lane);
     sc.add(act && q == 0 && m == 0, u, s.cand, s.cand_cnt, lane);
@@ -868,8 +896,13 @@ __global__ void k_bfs_source(uint32_t *lv, int32_t *par, uint32_t src, uint32_t 
 
 const uint64_t *Graph::piece_offsets(const uint32_t *F, uint32_t nf, PieceBufs &pb,
                                      const char *tag) {
-  uint32_t *cnt = pb.cnt.ensure(nf);
   uint64_t *off = pb.off.ensure((uint64_t)nf + 1);
+  if (nf <= PIECES_ONE_CTA) {
+    TRC_LAUNCH(prof, stream, "list_pieces", 1, PIECES_ONE_CTA, 0, k_list_pieces_scan, view(), F, nf,
+               off);
+    return off;
+  }
+  uint32_t *cnt = pb.cnt.ensure(nf);
   uint64_t *st = pb.scan.ensure(scan_tmp_elems(nf) + 4);
   TRC_LAUNCH(prof, stream, "list_pieces", ceil_div(nf, AT), AT, 0, k_list_pieces, view(), F, nf,
              cnt);
@@ -882,15 +915,16 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
   if (!parents) throw_error(TRC_ERR_INVALID, "null output");
   ensure_lists();
   bool dev = flags & TRC_DEVICE_PTR;
-  DBuf<uint32_t> lvb, qa, qb, bits, cnt;
+  DBuf<uint32_t> lvb, qa, qb, bits, bits2, cnt;
   DBuf<int32_t> parb;
-  for (auto *b : {&lvb, &qa, &qb, &bits, &cnt}) b->bind(&budget);
+  for (auto *b : {&lvb, &qa, &qb, &bits, &bits2, &cnt}) b->bind(&budget);
   parb.bind(&budget);
   uint32_t *lv = (dev && levels) ? levels : lvb.alloc_exact(n);
   int32_t *par = dev ? parents : parb.alloc_exact(n);
   uint32_t *F = qa.alloc_exact(n), *Nx = qb.alloc_exact(n);
   uint64_t words = ceil_div(n, 32);
-  uint32_t *bm = bits.alloc_exact(words);
+  uint32_t *bm = bits.alloc_exact(words), *bm2 = bits2.alloc_exact(words);
+  bool bm_valid = false;  // bm holds level d's frontier (a dense step wrote it)
   uint32_t *c = cnt.alloc_exact(4);
   TRC_LAUNCH(prof, stream, "bfs_init",
              std::min<uint64_t>(ceil_div(n, 4 * AT), resident_grid(k_bfs_init, AT)), AT, 0,
@@ -916,12 +950,14 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
   const unsigned pgrid = (unsigned)num_sms() * 8;
   while (nf > 0) {
     TRC_CUDA(cudaMemsetAsync(c, 0, 16, stream));  // next, seg, cand counts
-    BFSState s{lv, par, bm, Nx, c, d, sg, c + 1, nullptr, c + 2, sg2, c + 3};
+    BFSState s{lv, par, bm, Nx, c, d, sg, c + 1, nullptr, c + 2, sg2, c + 3, bm2};
     uint32_t hc[3] = {0, 0, 0};
     if ((uint64_t)nf >= dense_at && dense_at > 0) {
-      TRC_LAUNCH(prof, stream, "bfs_bits",
-                 std::min<uint64_t>(ceil_div(n, AT), resident_grid(k_level_bits, AT)), AT, 0,
-                 k_level_bits, lv, n, d, bm);
+      if (!bm_valid)
+        TRC_LAUNCH(prof, stream, "bfs_bits",
+                   std::min<uint64_t>(ceil_div(n, AT), resident_grid(k_level_bits, AT)), AT, 0,
+                   k_level_bits, lv, n, d, bm);
+      TRC_CUDA(cudaMemsetAsync(bm2, 0, words * 4, stream));
       // candidates left for the next dense step (never the list being read)
       s.cand = cbuf[cnext].ensure(ncand ? ncand : 1);
       // pass A: the 16 inline neighbours of every unvisited non-hub vertex;
@@ -944,7 +980,10 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
       ncand = hc[2];
       cand = s.cand;
       cnext ^= 1;
+      std::swap(bm, bm2);  // the step's claims: level d+1's frontier
+      bm_valid = true;
     } else {
+      bm_valid = false;
       // edge-balanced push: piece counts scanned, then every warp of the
       // grid takes an equal share of the frontier's pieces
       const uint64_t *off = piece_offsets(F, nf, pbufs, "bfs_push_scan");
