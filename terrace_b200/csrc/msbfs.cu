@@ -92,33 +92,76 @@ __device__ __forceinline__ uint32_t cta_append(bool take, uint32_t *counter, uin
   return pos;
 }
 
-// pull, 4 lanes per inline-only vertex
+// pull, one thread per inline-only vertex: the 64-byte row as four 16-byte
+// loads, then all of its (at most 16) neighbours' front masks in flight
 __global__ void __launch_bounds__(MT) k_ms_pull_S(DevView G, const uint32_t *V, uint64_t nV,
                                                   MSState s) {
-  uint64_t gt = (uint64_t)blockIdx.x * MT + threadIdx.x;
-  uint64_t vi = gt >> 2;
-  uint32_t q = gt & 3;
+  const uint64_t vi = (uint64_t)blockIdx.x * MT + threadIdx.x;
+  if (vi >= nV) return;
+  const uint32_t v = V[vi];
+  if ((s.seen[v] & s.live) == s.live) {
+    s.next[v] = 0;
+    return;
+  }
+  const uint32_t d = G.deg[v];
+  const uint4 *row = reinterpret_cast<const uint4 *>(G.inl + (uint64_t)v * K_INLINE);
+  uint32_t x[K_INLINE];
+#pragma unroll
+  for (uint32_t q = 0; q < K_INLINE / 4; q++) {
+    const uint4 t = q * 4 < d ? __ldg(row + q) : make_uint4(0, 0, 0, 0);
+    x[4 * q] = t.x;
+    x[4 * q + 1] = t.y;
+    x[4 * q + 2] = t.z;
+    x[4 * q + 3] = t.w;
+  }
   uint64_t reach = 0;
-  uint32_t v = 0;
-  bool live = false;
-  if (vi < nV) {
-    v = V[vi];
-    live = (s.seen[v] & s.live) != s.live;
-    uint32_t d = G.deg[v];
-    if (live && q * 4 < d) {
-      uint4 r = __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)v * K_INLINE) + q);
-      reach = s.front[r.x];
-      if (q * 4 + 1 < d) reach |= s.front[r.y];
-      if (q * 4 + 2 < d) reach |= s.front[r.z];
-      if (q * 4 + 3 < d) reach |= s.front[r.w];
+#pragma unroll
+  for (uint32_t e = 0; e < K_INLINE; e++)
+    if (e < d) reach |= s.front[x[e]];
+  ms_commit(s, v, reach);
+}
+
+// pull, 8 lanes per vertex of 17..cut neighbours (inline row, then the PMA
+// segment by rank), 8 ranks per lane per step with every load issued
+// first, stopping once seen | reach covers every live source
+__global__ void __launch_bounds__(MT) k_ms_pull_G8(DevView G, const uint32_t *V, uint64_t nV,
+                                                   MSState s) {
+  constexpr uint32_t U = 8;
+  const uint64_t gt = (uint64_t)blockIdx.x * MT + threadIdx.x;
+  const uint64_t vi = gt >> 3;
+  const uint32_t q = gt & 7;
+  const uint32_t lane = threadIdx.x & 31;
+  const unsigned mask = 0xFFu << (lane & ~7u);
+  if (vi >= nV) return;  // (whole groups: nV groups of 8 lanes)
+  const uint32_t v = V[vi];
+  const uint64_t sv = s.seen[v];
+  if ((sv & s.live) == s.live) {
+    if (q == 0) s.next[v] = 0;
+    return;
+  }
+  const uint32_t d = G.deg[v];
+  const uint32_t *row = G.inl + (uint64_t)v * K_INLINE;
+  const uint32_t *seg = G.pma + G.pbeg[v] - K_INLINE;  // indexed by rank
+  uint64_t reach = 0;
+  for (uint32_t j0 = 0; j0 < d; j0 += 8 * U) {  // (group-uniform trip count)
+    uint32_t x[U];
+#pragma unroll
+    for (uint32_t k = 0; k < U; k++) {
+      const uint32_t j = j0 + q + 8 * k;
+      x[k] = j < d ? (j < K_INLINE ? row[j] : __ldcs(seg + j)) : 0u;
     }
+#pragma unroll
+    for (uint32_t k = 0; k < U; k++)
+      if (j0 + q + 8 * k < d) reach |= s.front[x[k]];
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+      const uint32_t lo = __shfl_xor_sync(mask, (uint32_t)reach, o, 8);
+      const uint32_t hi = __shfl_xor_sync(mask, (uint32_t)(reach >> 32), o, 8);
+      reach |= ((uint64_t)hi << 32) | lo;
+    }
+    if (((reach | sv) & s.live) == s.live) break;  // (group-uniform)
   }
-  reach = shfl_or64(reach, 1);
-  reach = shfl_or64(reach, 2);
-  if (vi < nV && q == 0) {
-    if (live) ms_commit(s, v, reach);
-    else s.next[v] = 0;
-  }
+  if (q == 0) ms_commit(s, v, reach);
 }
 
 // pull, one warp per vertex, stopping once seen | reach covers every live
@@ -526,10 +569,12 @@ void Graph::msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uin
     MSState s{seen, front, next, lvrow, k, live, level};
     uint32_t *nl = L[cur ^ 1];
     if ((uint64_t)nact >= dense_at && dense_at > 0) {
-      TRC_LAUNCH(prof, stream, "ms_pull_S", ceil_div(lists.nS * 4, MT), MT, 0, k_ms_pull_S, G,
+      TRC_LAUNCH(prof, stream, "ms_pull_S", ceil_div(lists.nS, MT), MT, 0, k_ms_pull_S, G,
                  lists.S.get(), lists.nS, s);
-      TRC_LAUNCH(prof, stream, "ms_pull_M", ceil_div(lists.nM * 32, MT), MT, 0, k_ms_pull_W, G,
-                 lists.M.get(), lists.nM, s);
+      TRC_LAUNCH(prof, stream, "ms_pull_M8", ceil_div(lists.nM1 * 8, MT), MT, 0, k_ms_pull_G8, G,
+                 lists.M1.get(), lists.nM1, s);
+      TRC_LAUNCH(prof, stream, "ms_pull_M", ceil_div(lists.nM2 * 32, MT), MT, 0, k_ms_pull_W, G,
+                 lists.M2.get(), lists.nM2, s);
       TRC_LAUNCH(prof, stream, "ms_pull_H", ceil_div(lists.nH * 32, MT), MT, 0, k_ms_pull_W, G,
                  lists.Hv.get(), lists.nH, s);
       // isolated vertices are in no class list; their next mask stays 0
@@ -680,10 +725,12 @@ void Graph::msbc(const uint32_t *sources, uint32_t k, double *out_user, uint32_t
     const uint64_t base = loff.back();
     lv.reserve(base + n, base, stream);
     if ((uint64_t)nact >= dense_at && dense_at > 0) {
-      TRC_LAUNCH(prof, stream, "ms_pull_S", ceil_div(lists.nS * 4, MT), MT, 0, k_ms_pull_S, G,
+      TRC_LAUNCH(prof, stream, "ms_pull_S", ceil_div(lists.nS, MT), MT, 0, k_ms_pull_S, G,
                  lists.S.get(), lists.nS, s);
-      TRC_LAUNCH(prof, stream, "ms_pull_M", ceil_div(lists.nM * 32, MT), MT, 0, k_ms_pull_W, G,
-                 lists.M.get(), lists.nM, s);
+      TRC_LAUNCH(prof, stream, "ms_pull_M8", ceil_div(lists.nM1 * 8, MT), MT, 0, k_ms_pull_G8, G,
+                 lists.M1.get(), lists.nM1, s);
+      TRC_LAUNCH(prof, stream, "ms_pull_M", ceil_div(lists.nM2 * 32, MT), MT, 0, k_ms_pull_W, G,
+                 lists.M2.get(), lists.nM2, s);
       TRC_LAUNCH(prof, stream, "ms_pull_H", ceil_div(lists.nH * 32, MT), MT, 0, k_ms_pull_W, G,
                  lists.Hv.get(), lists.nH, s);
       TRC_LAUNCH(prof, stream, "ms_collect", ceil_div(n, MT), MT, 0, k_ms_collect, n, next, nl,
