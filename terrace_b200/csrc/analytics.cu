@@ -187,29 +187,30 @@ __device__ __forceinline__ void pr_store(const PRArgs &a, uint32_t u, uint32_t d
   if (a.last) a.out[u] = val;
 }
 
+// One thread per vertex of at most 16 neighbours: the 64-byte row as four
+// 16-byte loads, then all of its gathers in flight.
 __global__ void __launch_bounds__(AT) k_pr_S(DevView G, const uint32_t *S, uint64_t nS, PRArgs a) {
-  uint64_t gt = (uint64_t)blockIdx.x * AT + threadIdx.x;
-  uint64_t vi = gt >> 2;
-  uint32_t q = gt & 3;
-  double sum = 0.0;
-  uint32_t u = 0, d = 0;
-  if (vi < nS) {
-    u = S[vi];
-    d = G.deg[u];
-    uint32_t lo, hi;
-    pr_range(a, u, d, lo, hi);
-    uint32_t e = q * 4;
-    if (e < hi && e + 4 > lo) {
-      uint4 v = __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE) + q);
-      if (e >= lo && e < hi) sum += __ldg(a.pc + v.x);
-      if (e + 1 >= lo && e + 1 < hi) sum += __ldg(a.pc + v.y);
-      if (e + 2 >= lo && e + 2 < hi) sum += __ldg(a.pc + v.z);
-      if (e + 3 >= lo && e + 3 < hi) sum += __ldg(a.pc + v.w);
-    }
+  const uint64_t vi = (uint64_t)blockIdx.x * AT + threadIdx.x;
+  if (vi >= nS) return;
+  const uint32_t u = S[vi];
+  const uint32_t d = G.deg[u];
+  const uint4 *row = reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE);
+  uint32_t x[K_INLINE];
+#pragma unroll
+  for (uint32_t q = 0; q < K_INLINE / 4; q++) {
+    const uint4 t = q * 4 < d ? __ldcs(row + q) : make_uint4(0, 0, 0, 0);
+    x[4 * q] = t.x;
+    x[4 * q + 1] = t.y;
+    x[4 * q + 2] = t.z;
+    x[4 * q + 3] = t.w;
   }
-  sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 1);
-  sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 2);
-  if (vi < nS && q == 0) pr_store(a, u, d, sum);
+  double g[K_INLINE];
+#pragma unroll
+  for (uint32_t e = 0; e < K_INLINE; e++) g[e] = e < d ? __ldg(a.pc + x[e]) : 0.0;
+  double sum = 0.0;
+#pragma unroll
+  for (uint32_t e = 0; e < K_INLINE; e++) sum += g[e];
+  pr_store(a, u, d, sum);
 }
 
 // Load-balanced pull.  Warp w takes list entries [32w, 32w+32); their
@@ -431,7 +432,7 @@ void Graph::pr_kernels(uint32_t iters, double damping, double *p0, double *p1, d
   DevView G = view();
   for (uint32_t it = 0; it < iters; it++) {
     PRArgs a{p0, p1, out, damping, base, it + 1 == iters};
-    TRC_LAUNCH(prof, s, "pr_S", ceil_div(lists.nS * 4, AT), AT, 0, k_pr_S, G, lists.S.get(),
+    TRC_LAUNCH(prof, s, "pr_S", ceil_div(lists.nS, AT), AT, 0, k_pr_S, G, lists.S.get(),
                lists.nS, a);
     switch (tuned.pr_group_lanes) {
       case 4:

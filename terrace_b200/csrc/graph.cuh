@@ -175,6 +175,8 @@ class Graph {
     }
   };
   const uint64_t *piece_offsets(const uint32_t *F, uint32_t nf, PieceBufs &pb, const char *tag);
+  void ms_init(uint32_t k, const uint32_t *dsrc, uint64_t *seen, uint64_t *front, uint64_t *next,
+               uint32_t *lvrow, unsigned long long *acc);
   // one edge-balanced push level of msbfs / msbc (msbfs.cu)
   void ms_push_level(const uint32_t *F, uint32_t nf, const uint64_t *front, const uint64_t *seen,
                      unsigned long long *acc, uint32_t *T, uint32_t *tcnt, PieceBufs &pb);

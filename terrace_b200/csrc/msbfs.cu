@@ -329,20 +329,16 @@ __global__ void k_ms_count(uint32_t n, const uint64_t *seen, unsigned long long 
   if (c1) atomicAdd(cnt + 32 + lane, (unsigned long long)c1);
 }
 
-__global__ void k_ms_init(uint32_t n, uint32_t k, const uint32_t *src, uint64_t *seen,
-                          uint64_t *front, uint64_t *next, uint32_t *lvrow,
-                          unsigned long long *acc) {
-  uint64_t v = (uint64_t)blockIdx.x * MT + threadIdx.x;
-  if (v >= n) return;
-  uint64_t m = 0;
-  for (uint32_t i = 0; i < k; i++)
-    if (src[i] == v) m |= 1ull << i;
-  seen[v] = m;
-  front[v] = m;
-  next[v] = 0;
-  acc[v] = 0;
-  if (lvrow)
-    for (uint32_t i = 0; i < k; i++) lvrow[v * k + i] = (m >> i) & 1 ? 0u : TRC_UNREACHED;
+// After the masks were zeroed and the levels filled with TRC_UNREACHED:
+// source i's bit in its vertex's masks, and its level 0.
+__global__ void k_ms_seed(uint32_t k, const uint32_t *src, unsigned long long *seen,
+                          unsigned long long *front, uint32_t *lvrow) {
+  const uint32_t i = threadIdx.x;
+  if (i >= k) return;
+  const uint32_t v = src[i];
+  atomicOr(seen + v, 1ull << i);
+  atomicOr(front + v, 1ull << i);
+  if (lvrow) lvrow[(uint64_t)v * k + i] = 0u;
 }
 
 // levels (vertex-major n x k) -> out (source-major k x n), 32x32 tiles
@@ -486,6 +482,17 @@ __global__ void k_mbc_final(const double *dep, const double *sigma, uint32_t n, 
 }
 }  // namespace
 
+// Initial state of a multi-source traversal: every mask zero, every level
+// TRC_UNREACHED (byte fills), then the sources' bits and levels.
+void Graph::ms_init(uint32_t k, const uint32_t *dsrc, uint64_t *seen, uint64_t *front,
+                    uint64_t *next, uint32_t *lvrow, unsigned long long *acc) {
+  for (void *p : {(void *)seen, (void *)front, (void *)next, (void *)acc})
+    TRC_CUDA(cudaMemsetAsync(p, 0, (uint64_t)n * 8, stream));
+  if (lvrow) TRC_CUDA(cudaMemsetAsync(lvrow, 0xFF, (uint64_t)n * k * 4, stream));
+  TRC_LAUNCH(prof, stream, "ms_init", 1, 64, 0, k_ms_seed, k, dsrc,
+             (unsigned long long *)seen, (unsigned long long *)front, lvrow);
+}
+
 void Graph::ms_push_level(const uint32_t *F, uint32_t nf, const uint64_t *front,
                           const uint64_t *seen, unsigned long long *acc, uint32_t *T,
                           uint32_t *tcnt, PieceBufs &pb) {
@@ -546,8 +553,7 @@ void Graph::msbfs_run(const uint32_t *sources, uint32_t k, uint32_t *levels, uin
   uint32_t *c = cnt.alloc_exact(4);  // [1] next active, [2] touched, [3] pushing hubs
   PieceBufs pbufs(&budget);  // push levels: piece counts, prefix, scan scratch
   TRC_CUDA(cudaMemcpyAsync(dsrc, hsrc.data(), k * 4, cudaMemcpyHostToDevice, stream));
-  TRC_LAUNCH(prof, stream, "ms_init", ceil_div(n, MT), MT, 0, k_ms_init, n, k, dsrc, seen, front,
-             next, lvrow, acc);
+  ms_init(k, dsrc, seen, front, next, lvrow, acc);
   // initial active list = the distinct sources
   std::vector<uint32_t> act(hsrc);
   std::sort(act.begin(), act.end());
@@ -695,8 +701,7 @@ void Graph::msbc(const uint32_t *sources, uint32_t k, double *out_user, uint32_t
   TRC_CUDA(cudaMemcpyAsync(dsrc, hsrc.data(), k * 4, cudaMemcpyHostToDevice, stream));
   TRC_CUDA(cudaMemsetAsync(sigma, 0, (uint64_t)n * k * 8, stream));
   TRC_CUDA(cudaMemsetAsync(dep, 0, (uint64_t)n * k * 8, stream));
-  TRC_LAUNCH(prof, stream, "ms_init", ceil_div(n, MT), MT, 0, k_ms_init, n, k, dsrc, seen, front,
-             next, (uint32_t *)nullptr, acc);
+  ms_init(k, dsrc, seen, front, next, nullptr, acc);
   TRC_LAUNCH(prof, stream, "mbc_seed", 1, 64, 0, k_mbc_seed, dsrc, k, sigma);
   std::vector<uint32_t> act(hsrc);
   std::sort(act.begin(), act.end());
