@@ -1333,27 +1333,32 @@ struct BCBackClassOp {
   __device__ void store(uint32_t u, double sum) const { dep_out[u] = sum + inv[u]; }
 };
 
+// One thread per vertex of at most 16 neighbours: the 64-byte row as four
+// 16-byte loads, then every gather in flight.
 template <class Op>
 __global__ void __launch_bounds__(AT) k_cls_S(DevView G, const uint32_t *S, uint64_t nS, Op op) {
-  const uint64_t gt = (uint64_t)blockIdx.x * AT + threadIdx.x;
-  const uint64_t vi = gt >> 2;
-  const uint32_t q = gt & 3;
-  const uint32_t u = vi < nS ? S[vi] : 0u;
-  const bool act = vi < nS && !op.skip(u);
-  double sum = 0.0;
-  if (act) {
-    const uint32_t d = G.deg[u], e = q * 4;
-    if (e < d) {
-      const uint4 v = __ldcs(reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE) + q);
-      sum += op.gather(v.x);
-      if (e + 1 < d) sum += op.gather(v.y);
-      if (e + 2 < d) sum += op.gather(v.z);
-      if (e + 3 < d) sum += op.gather(v.w);
-    }
+  const uint64_t vi = (uint64_t)blockIdx.x * AT + threadIdx.x;
+  if (vi >= nS) return;
+  const uint32_t u = S[vi];
+  if (op.skip(u)) return;
+  const uint32_t d = G.deg[u];
+  const uint4 *row = reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE);
+  uint32_t x[K_INLINE];
+#pragma unroll
+  for (uint32_t q = 0; q < K_INLINE / 4; q++) {
+    const uint4 t = q * 4 < d ? __ldcs(row + q) : make_uint4(0, 0, 0, 0);
+    x[4 * q] = t.x;
+    x[4 * q + 1] = t.y;
+    x[4 * q + 2] = t.z;
+    x[4 * q + 3] = t.w;
   }
-  sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 1);
-  sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 2);
-  if (act && q == 0) op.store(u, sum);
+  double g[K_INLINE];
+#pragma unroll
+  for (uint32_t e = 0; e < K_INLINE; e++) g[e] = e < d ? op.gather(x[e]) : 0.0;
+  double sum = 0.0;
+#pragma unroll
+  for (uint32_t e = 0; e < K_INLINE; e++) sum += g[e];
+  op.store(u, sum);
 }
 
 template <int GS, class Op>
@@ -1507,7 +1512,7 @@ void Graph::bc(uint32_t src, double *out_user, uint32_t flags) {
                  order + a, b - a, BCBackOp{inv, dep, side});
     } else {  // a large one: the degree classes
       const BCBackClassOp op{lv, (uint32_t)L, inv, dep, side};
-      TRC_LAUNCH(prof, stream, "bc_back_S", ceil_div(lists.nS * 4, AT), AT, 0, k_cls_S<BCBackClassOp>,
+      TRC_LAUNCH(prof, stream, "bc_back_S", ceil_div(lists.nS, AT), AT, 0, k_cls_S<BCBackClassOp>,
                  G, lists.S.get(), lists.nS, op);
       TRC_LAUNCH(prof, stream, "bc_back_M8", ceil_div(lists.nM1 * 8, AT), AT, 0,
                  (k_cls_group<8, BCBackClassOp>), G, lists.M1.get(), lists.nM1, op);
