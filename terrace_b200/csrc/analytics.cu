@@ -674,8 +674,10 @@ __global__ void k_level_bits(const uint32_t *lv, uint32_t n, uint32_t d, uint32_
 
 // Inline pass of a dense step: one thread per vertex (grid-stride; a warp
 // takes 32 consecutive list entries).  Each thread loads its vertex's
-// 64-byte inline row as four 16-byte loads (the warp's rows are one
-// contiguous 2 KB block when the entries are consecutive ids) and then its
+// 64-byte inline row as four 16-byte streaming loads (evict-first, so the
+// rows streaming through L2 do not push the frontier bitmap out; the warp's
+// rows are one contiguous 2 KB block when the entries are consecutive ids)
+// and then its
 // frontier-bitmap words (the first four, then the rest on a miss), every
 // load of a round issued before any is used; the first frontier neighbour
 // in sorted order is the parent.
@@ -699,7 +701,7 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
     uint32_t x[K_INLINE];
 #pragma unroll
     for (uint32_t q = 0; q < K_INLINE / 4; q++) {
-      const uint4 t = act && q * 4 < d ? __ldg(row + q) : make_uint4(0, 0, 0, 0);
+      const uint4 t = act && q * 4 < d ? __ldcs(row + q) : make_uint4(0, 0, 0, 0);
       x[4 * q] = t.x;
       x[4 * q + 1] = t.y;
       x[4 * q + 2] = t.z;
