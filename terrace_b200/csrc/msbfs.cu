@@ -391,14 +391,30 @@ __device__ __forceinline__ void mbc_gather(const DevView &G, uint32_t v, uint64_
     const uint32_t u = j < L.deg ? L.at(j) : 0u;
     const uint64_t mu = j < L.deg ? (mask[u] & want) : 0ull;
     uint32_t ball = __ballot_sync(0xFFFFFFFFu, mu != 0);
+    // up to MBC_BATCH contributing neighbours at a time: their rows loaded
+    // first, then added in neighbour order (the sums stay in the same order)
+    constexpr int MBC_BATCH = 4;
     while (ball) {
-      const int b = __ffs(ball) - 1;
-      ball &= ball - 1;
-      const uint32_t uu = __shfl_sync(0xFFFFFFFFu, u, b);
-      const uint64_t mm = shfl64(mu, b);
-      const double *row = val + (uint64_t)uu * k;
-      if (lane < k && ((mm >> lane) & 1)) a0 += row[lane];
-      if (lane + 32 < k && ((mm >> (lane + 32)) & 1)) a1 += row[lane + 32];
+      double r0[MBC_BATCH], r1[MBC_BATCH];
+#pragma unroll
+      for (int t = 0; t < MBC_BATCH; t++) {
+        r0[t] = 0.0;
+        r1[t] = 0.0;
+        if (ball) {  // (warp-uniform)
+          const int b = __ffs(ball) - 1;
+          ball &= ball - 1;
+          const uint32_t uu = __shfl_sync(0xFFFFFFFFu, u, b);
+          const uint64_t mm = shfl64(mu, b);
+          const double *row = val + (uint64_t)uu * k;
+          if (lane < k && ((mm >> lane) & 1)) r0[t] = row[lane];
+          if (lane + 32 < k && ((mm >> (lane + 32)) & 1)) r1[t] = row[lane + 32];
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < MBC_BATCH; t++) {
+        a0 += r0[t];
+        a1 += r1[t];
+      }
     }
   }
 }
