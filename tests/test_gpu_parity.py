@@ -289,6 +289,33 @@ def test_batch_sort_modes_agree_with_oracle(T, mode):
     g.close()
 
 
+@pytest.mark.parametrize("n", [1, 3, 70])
+def test_batch_sort_tiny_graphs_large_batches(T, n):
+    """Batches of 10,000-60,000 pairs on graphs of 1, 3 and 70 vertices
+    (every bucket holds thousands of duplicates, self loops dropped, one
+    vertex: every key invalid), in every sort mode: the oracle's edge set
+    after each batch."""
+    from terrace_b200 import _lib
+    rng = np.random.default_rng(n)
+    for mode in (0, 1, 2):
+        g = T.Graph(n)
+        _lib.check(g._L.trc_debug_sort_mode(g._h, mode))
+        cur = np.zeros(0, np.uint64)
+        for step, k in enumerate((10000, 60000, 30000)):
+            s = rng.integers(0, n, k).astype(np.uint32)
+            d = rng.integers(0, n, k).astype(np.uint32)
+            bk = O.make_keys(s, d, True, True)
+            if step == 2:
+                g.remove_edge_batch(s[: k // 2], d[: k // 2], **SYM)
+                cur = O.key_difference(cur, O.make_keys(s[: k // 2], d[: k // 2], True, True))
+            else:
+                g.add_edge_batch(s, d, **SYM)
+                cur = O.key_union(cur, bk)
+            assert_same_csr(g, *O.csr_from_keys(n, cur))
+        assert g.check() == 0
+        g.close()
+
+
 def test_streaming_rmat22_roundtrip_and_parity(T):
     """LiveJournal-shaped RMAT scale 22 ef 16: bulk load and one 1e6-pair
     insert + delete batch.  Parity with the oracle's set model by CSR hash,
