@@ -574,27 +574,38 @@ __device__ __forceinline__ void bfs_push_span(const uint32_t *p, uint32_t len, u
 // exclusive prefix of the piece counts, off[nf] = the total T): warp w of W
 // takes pieces [T*w/W, T*(w+1)/W), whatever vertices they belong to, so one
 // long list is spread over many warps and many short lists share one warp.
-__global__ void k_list_pieces(DevView G, const uint32_t *F, uint32_t nf, uint32_t *cnt) {
+// With skip_small, lists of at most K_INLINE elements outside the hub tier
+// count no pieces (their vertices are pushed one thread each by
+// k_bfs_push_small); off may then repeat values, and a piece's owner is the
+// last vertex whose offset is at most the piece's index.
+__device__ __forceinline__ uint32_t push_pieces(const DevView &G, uint32_t u, int skip_small) {
+  const NbrList L = nbr_list(G, u);
+  if (skip_small && L.deg <= K_INLINE && G.hub_of[u] < 0) return 0;
+  return list_pieces(L);
+}
+
+__global__ void k_list_pieces(DevView G, const uint32_t *F, uint32_t nf, uint32_t *cnt,
+                              int skip_small) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nf) cnt[i] = list_pieces(nbr_list(G, F[i]));
+  if (i < nf) cnt[i] = push_pieces(G, F[i], skip_small);
 }
 
 // The same and the exclusive prefix in one CTA, for frontiers of at most
 // PIECES_ONE_CTA vertices: off[0..nf], off[nf] = the total.
 constexpr uint32_t PIECES_ONE_CTA = 1024;
 __global__ void __launch_bounds__(PIECES_ONE_CTA)
-    k_list_pieces_scan(DevView G, const uint32_t *F, uint32_t nf, uint64_t *off) {
+    k_list_pieces_scan(DevView G, const uint32_t *F, uint32_t nf, uint64_t *off, int skip_small) {
   __shared__ uint64_t ws[PIECES_ONE_CTA / 32 + 1];
   const uint32_t i = threadIdx.x;
-  const uint64_t c = i < nf ? list_pieces(nbr_list(G, F[i])) : 0;
+  const uint64_t c = i < nf ? push_pieces(G, F[i], skip_small) : 0;
   uint64_t tot;
   const uint64_t ex = block_excl_scan<uint64_t, PIECES_ONE_CTA>(c, ws, tot);
   if (i < nf) off[i] = ex;
   if (i == 0) off[nf] = tot;
 }
 
-// The frontier vertex of piece t: the i with off[i] <= t < off[i+1] (every
-// list has a piece, so off is strictly increasing).
+// The frontier vertex of piece t: the last i with off[i] <= t (vertices
+// with no pieces share their successor's offset and are passed over).
 __device__ __forceinline__ uint32_t piece_owner(const uint64_t *off, uint32_t nf, uint64_t t) {
   uint32_t a = 0, b = nf;
   while (b - a > 1) {
@@ -603,6 +614,47 @@ __device__ __forceinline__ uint32_t piece_owner(const uint64_t *off, uint32_t nf
     else b = m;
   }
   return a;
+}
+
+// Push of the frontier's short lists (at most K_INLINE elements, outside the
+// hub tier; the edge-balanced push skips them): one thread per frontier
+// vertex, its row as four 16-byte loads and all of its parent probes in
+// flight, then the claims.
+__global__ void __launch_bounds__(AT) k_bfs_push_small(DevView G, const uint32_t *F, uint32_t nf,
+                                                       BFSState s) {
+  const uint32_t lane = threadIdx.x & 31;
+  __shared__ uint32_t stg[AT / 32][WS_BIG];
+  WarpStage st{stg[threadIdx.x >> 5], 0, WS_BIG};
+  const uint64_t i = (uint64_t)blockIdx.x * AT + threadIdx.x;
+  uint32_t u = 0, d = 0;
+  if (i < nf) {
+    u = F[i];
+    d = G.deg[u];
+    if (d > K_INLINE || G.hub_of[u] >= 0) d = 0;  // (an edge-balanced push's)
+  }
+  const uint4 *row = reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE);
+  uint32_t x[K_INLINE];
+#pragma unroll
+  for (uint32_t q = 0; q < K_INLINE / 4; q++) {
+    const uint4 t = q * 4 < d ? __ldcs(row + q) : make_uint4(0, 0, 0, 0);
+    x[4 * q] = t.x;
+    x[4 * q + 1] = t.y;
+    x[4 * q + 2] = t.z;
+    x[4 * q + 3] = t.w;
+  }
+  int32_t pv[K_INLINE];
+#pragma unroll
+  for (uint32_t e = 0; e < K_INLINE; e++) pv[e] = e < d ? s.par[x[e]] : 0;
+#pragma unroll
+  for (uint32_t e = 0; e < K_INLINE; e++) {
+    bool win = false;
+    if (e < d && pv[e] == -1 && atomicCAS(&s.par[x[e]], -1, (int32_t)u) == -1) {
+      s.lv[x[e]] = s.d + 1;
+      win = true;
+    }
+    st.add(win, x[e], s.next, s.next_cnt, lane);
+  }
+  st.flush(s.next, s.next_cnt, lane);
 }
 
 __global__ void __launch_bounds__(AT) k_bfs_push_lb(DevView G, const uint32_t *F, uint32_t nf,
@@ -898,17 +950,17 @@ __global__ void k_bfs_source(uint32_t *lv, int32_t *par, uint32_t src, uint32_t 
 }
 
 const uint64_t *Graph::piece_offsets(const uint32_t *F, uint32_t nf, PieceBufs &pb,
-                                     const char *tag) {
+                                     const char *tag, bool skip_small) {
   uint64_t *off = pb.off.ensure((uint64_t)nf + 1);
   if (nf <= PIECES_ONE_CTA) {
     TRC_LAUNCH(prof, stream, "list_pieces", 1, PIECES_ONE_CTA, 0, k_list_pieces_scan, view(), F, nf,
-               off);
+               off, (int)skip_small);
     return off;
   }
   uint32_t *cnt = pb.cnt.ensure(nf);
   uint64_t *st = pb.scan.ensure(scan_tmp_elems(nf) + 4);
   TRC_LAUNCH(prof, stream, "list_pieces", ceil_div(nf, AT), AT, 0, k_list_pieces, view(), F, nf,
-             cnt);
+             cnt, (int)skip_small);
   exclusive_scan(LoadU32{cnt}, nf, off, st, stream, prof, tag);  // (off[nf] = the total)
   return off;
 }
@@ -989,7 +1041,9 @@ void Graph::bfs(uint32_t src, int32_t *parents, uint32_t *levels, uint32_t flags
       bm_valid = false;
       // edge-balanced push: piece counts scanned, then every warp of the
       // grid takes an equal share of the frontier's pieces
-      const uint64_t *off = piece_offsets(F, nf, pbufs, "bfs_push_scan");
+      const uint64_t *off = piece_offsets(F, nf, pbufs, "bfs_push_scan", true);
+      TRC_LAUNCH(prof, stream, "bfs_push_small", ceil_div(nf, AT), AT, 0, k_bfs_push_small, G, F,
+                 nf, s);
       TRC_LAUNCH(prof, stream, "bfs_push", pgrid, AT, 0, k_bfs_push_lb, G, F, nf, off, s);
       TRC_CUDA(cudaMemcpyAsync(hc, c, 4, cudaMemcpyDeviceToHost, stream));
       sync();

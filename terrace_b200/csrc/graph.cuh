@@ -174,7 +174,8 @@ class Graph {
       scan.bind(b);
     }
   };
-  const uint64_t *piece_offsets(const uint32_t *F, uint32_t nf, PieceBufs &pb, const char *tag);
+  const uint64_t *piece_offsets(const uint32_t *F, uint32_t nf, PieceBufs &pb, const char *tag,
+                                bool skip_small = false);
   void ms_init(uint32_t k, const uint32_t *dsrc, uint64_t *seen, uint64_t *front, uint64_t *next,
                uint32_t *lvrow, unsigned long long *acc);
   // one edge-balanced push level of msbfs / msbc (msbfs.cu)
