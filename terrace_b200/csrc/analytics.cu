@@ -725,11 +725,11 @@ __global__ void k_level_bits(const uint32_t *lv, uint32_t n, uint32_t d, uint32_
 }
 
 // Inline pass of a dense step: one thread per vertex (grid-stride; a warp
-// takes 32 consecutive list entries).  Each thread loads its vertex's
-// 64-byte inline row as four 16-byte streaming loads (evict-first, so the
-// rows streaming through L2 do not push the frontier bitmap out; the warp's
-// rows are one contiguous 2 KB block when the entries are consecutive ids)
-// and then its
+// takes 32 consecutive list entries).  Each thread reads its vertex's
+// 64-byte inline row in 16-byte streaming loads (evict-first, so the rows
+// streaming through L2 do not push the frontier bitmap out; the warp's rows
+// are one contiguous 2 KB block when the entries are consecutive ids), the
+// first one and then the other three only on a miss, and its
 // frontier-bitmap words (the first four, then the rest on a miss), every
 // load of a round issued before any is used; the first frontier neighbour
 // in sorted order is the parent.
@@ -751,17 +751,17 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
     act = act && d > 0 && s.lv[u] == TRC_UNREACHED;
     const uint4 *row = reinterpret_cast<const uint4 *>(G.inl + (uint64_t)u * K_INLINE);
     uint32_t x[K_INLINE];
-#pragma unroll
-    for (uint32_t q = 0; q < K_INLINE / 4; q++) {
-      const uint4 t = act && q * 4 < d ? __ldcs(row + q) : make_uint4(0, 0, 0, 0);
-      x[4 * q] = t.x;
-      x[4 * q + 1] = t.y;
-      x[4 * q + 2] = t.z;
-      x[4 * q + 3] = t.w;
+    // the first four neighbours and their bitmap probes; the rest of the row
+    // and the other twelve probes only for vertices with no frontier
+    // neighbour among those four (on power-law graphs most have one there:
+    // the second half of their row is never read)
+    {
+      const uint4 t = act ? __ldcs(row) : make_uint4(0, 0, 0, 0);
+      x[0] = t.x;
+      x[1] = t.y;
+      x[2] = t.z;
+      x[3] = t.w;
     }
-    // bitmap probes of the first four neighbours, then of the other twelve
-    // only for vertices with no frontier neighbour among those four (on
-    // power-law graphs most have one there; the probes are L2 requests)
     uint32_t wb[K_INLINE];
 #pragma unroll
     for (uint32_t e = 0; e < 4; e++) wb[e] = act && e < d ? __ldg(s.bits + (x[e] >> 5)) : 0u;
@@ -770,6 +770,14 @@ __global__ void __launch_bounds__(AT) k_bfs_pull_S(DevView G, const uint32_t *S,
     for (int e = 3; e >= 0; e--)
       if ((wb[e] >> (x[e] & 31)) & 1u) p = x[e];
     if (act && p == NONE32 && d > 4) {
+#pragma unroll
+      for (uint32_t q = 1; q < K_INLINE / 4; q++) {
+        const uint4 t = q * 4 < d ? __ldcs(row + q) : make_uint4(0, 0, 0, 0);
+        x[4 * q] = t.x;
+        x[4 * q + 1] = t.y;
+        x[4 * q + 2] = t.z;
+        x[4 * q + 3] = t.w;
+      }
 #pragma unroll
       for (uint32_t e = 4; e < K_INLINE; e++) wb[e] = e < d ? __ldg(s.bits + (x[e] >> 5)) : 0u;
 #pragma unroll
