@@ -15,10 +15,45 @@ constexpr uint64_t KEY_INVALID = ~0ull;
 uint32_t *noalloc_scratch_resolve();
 
 // Lookup of (u, x) in the tiers (used by the update filter and is_edge).
+// Is (u, x) an edge?  The inline row is read whole (up to four 16-byte
+// loads issued together) and compared at once; only an x above its last
+// element searches the rest of the list (the PMA segment, or the hub's
+// blocks through the directory).
 __device__ __forceinline__ bool has_edge(const DevView &G, uint32_t u, uint32_t x) {
-  if (G.deg[u] == 0) return false;
-  NbrList L = nbr_list(G, u);
-  return list_has(L, x);
+  const uint32_t d = G.deg[u];
+  if (d == 0) return false;
+  const NbrList L = nbr_list(G, u);
+  const uint4 *row = reinterpret_cast<const uint4 *>(L.inl);
+  uint32_t v[K_INLINE];
+#pragma unroll
+  for (uint32_t q = 0; q < K_INLINE / 4; q++) {
+    const uint4 t = q * 4 < L.ni ? row[q] : make_uint4(0, 0, 0, 0);
+    v[4 * q] = t.x;
+    v[4 * q + 1] = t.y;
+    v[4 * q + 2] = t.z;
+    v[4 * q + 3] = t.w;
+  }
+  bool found = false;
+  uint32_t last = 0;
+#pragma unroll
+  for (uint32_t e = 0; e < K_INLINE; e++) {
+    if (e < L.ni) found |= v[e] == x;
+    if (e + 1 == L.ni) last = v[e];
+  }
+  if (found) return true;
+  if (L.ni == L.deg || x < last) return false;
+  if (L.nb == 0) {  // the PMA segment, rest elements
+    uint32_t lo = 0, hi = L.rest;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      const uint32_t y = L.seg[mid];
+      if (y < x) lo = mid + 1;
+      else if (y > x) hi = mid;
+      else return true;
+    }
+    return false;
+  }
+  return list_has(L, x);  // (a hub: x is above the inline row, so a block search)
 }
 
 // Per-vertex class lists for the analytics kernels, rebuilt when the graph
