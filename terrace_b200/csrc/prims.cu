@@ -248,7 +248,7 @@ struct BucketArgs {
 // with shared-memory atomics.  No global atomics: the skewed sources of
 // RMAT-like batches do not serialise anywhere.
 constexpr uint32_t BK_TILE = 16384;
-constexpr uint32_t BK_T = 512;
+constexpr uint32_t BK_T = 1024;
 constexpr uint32_t BK_MAXB = BUCKET_SPLITS;  // buckets at most (+1 for the invalid keys)
 
 // splits (global, BK_MAXB + 1 entries) or null; the CTA copies them to
