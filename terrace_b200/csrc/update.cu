@@ -779,8 +779,11 @@ __device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a,
 
 // Persistent over the rewrite list, whose length is read on the device;
 // warps take MS_CHUNK entries at a time from a counter, so CTAs that start
-// late (behind the hub merge on the side stream) take fewer.
-constexpr uint32_t MS_CHUNK = 8;
+// late (behind the hub merge on the side stream) take fewer.  (Long lists
+// cluster in the list; per 1e6-pair batch on RMAT-22 the merge took 232 us
+// with 4 entries per grab, 252 with 8, 302 with 2, 516 with 1: the counter
+// contends below 4, the warps' loads unbalance above.)
+constexpr uint32_t MS_CHUNK = 4;
 
 __global__ void __launch_bounds__(256, 8) k_merge_small(DevView G, MergeArgs a,
                                                         const uint64_t *nrs,
