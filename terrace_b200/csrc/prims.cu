@@ -216,7 +216,7 @@ uint64_t *radix_sort_u64_shifts(uint64_t *keys, uint64_t *alt, uint64_t n, const
 namespace {
 
 constexpr uint64_t BK_INVALID = ~0ull;
-constexpr uint32_t BK_MID = 256;   // 33..BK_MID keys: a warp in shared memory
+constexpr uint32_t BK_MID = 256;   // 33..BK_MID keys: a warp in registers
 constexpr uint32_t BK_BIG = 2048;  // BK_MID+1..BK_BIG: a CTA in static shared memory
                                    // above: a CTA in dynamic shared memory
 
@@ -415,27 +415,78 @@ __global__ void k_bucket_sort_small(BucketOff off, uint32_t nb, uint64_t *keys, 
   }
 }
 
-// A warp per listed bucket of 33..BK_MID keys, sorted in shared memory.
+// Ascending bitonic sort of 32 * E values held by a warp in registers, lane
+// l holding positions l * E .. l * E + E - 1 in r[0 .. E-1]: partners less
+// than E apart are in the same lane, the others E * 2^j apart in lane
+// l ^ 2^j (shuffles).  Every index resolves at compile time.
+template <int E>
+__device__ __forceinline__ void warp_regs_bitonic(uint64_t (&r)[E], uint32_t lane) {
+  constexpr int N = 32 * E;
+#pragma unroll
+  for (int size = 2; size <= N; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride < E) {
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          if ((e & stride) == 0) {
+            const int f = e | stride;
+            const uint32_t pos = lane * E + e;  // (pos & size) is the block's direction
+            const bool up = (pos & size) == 0;
+            const uint64_t x = r[e], y = r[f];
+            const bool sw = up ? (x > y) : (x < y);
+            r[e] = sw ? y : x;
+            r[f] = sw ? x : y;
+          }
+        }
+      } else {
+        const int lx = stride / E;  // partner lane offset
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          const uint64_t o = __shfl_xor_sync(0xFFFFFFFFu, r[e], lx);
+          const uint32_t pos = lane * E + e;
+          const bool up = (pos & size) == 0, lower = (pos & stride) == 0;
+          r[e] = (up == lower) ? (o < r[e] ? o : r[e]) : (o > r[e] ? o : r[e]);
+        }
+      }
+    }
+  }
+}
+
+template <int E>
+__device__ __forceinline__ void warp_regs_sort_bucket(uint64_t *keys, uint64_t base, uint32_t c,
+                                                      uint32_t lane) {
+  uint64_t r[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const uint32_t t = lane * E + e;
+    r[e] = t < c ? keys[base + t] : BK_INVALID;
+  }
+  warp_regs_bitonic<E>(r, lane);
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const uint32_t t = lane * E + e;
+    if (t < c) keys[base + t] = r[e];
+  }
+}
+
+// A warp per listed bucket of 33..BK_MID keys, sorted in registers (no
+// shared memory: the 64-bit compare-exchanges in shared memory met bank
+// conflicts at most strides).
 constexpr uint32_t BK_MID_WARPS = 8;
 __global__ void __launch_bounds__(BK_MID_WARPS * 32)
     k_bucket_sort_mid(BucketOff off, const uint32_t *list, const unsigned long long *nlist,
                       uint64_t *keys) {
-  __shared__ uint64_t sv[BK_MID_WARPS][BK_MID];
   const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint64_t *v = sv[w];
   const uint64_t nm = *nlist;
   for (uint64_t i = (uint64_t)blockIdx.x * BK_MID_WARPS + w; i < nm;
        i += (uint64_t)gridDim.x * BK_MID_WARPS) {
     const uint32_t b = list[i];
     const uint64_t base = off(b);
     const uint32_t c = (uint32_t)(off(b + 1) - base);
-    uint32_t P = 64;
-    while (P < c) P <<= 1;
-    for (uint32_t t = lane; t < P; t += 32) v[t] = t < c ? keys[base + t] : BK_INVALID;
-    __syncwarp();
-    smem_bitonic(v, P, lane, 32, [] { __syncwarp(); });
-    for (uint32_t t = lane; t < c; t += 32) keys[base + t] = v[t];
-    __syncwarp();
+    if (c <= 64) warp_regs_sort_bucket<2>(keys, base, c, lane);
+    else if (c <= 128) warp_regs_sort_bucket<4>(keys, base, c, lane);
+    else warp_regs_sort_bucket<8>(keys, base, c, lane);  // (c <= BK_MID = 256)
   }
 }
 
