@@ -109,14 +109,16 @@ trc_status trc_release_scratch(trc_graph *g);
 trc_status trc_debug_sort_wait(trc_graph *g, uint32_t spin_limit,
                                int withhold_first_tile);
 
-/* Test hook for the choice of batch sort.  Batches of 4096 keys or more
- * (after symmetrizing) sort with a bucket sort (bucket by the source's high
- * bits, each bucket sorted whole in registers or shared memory); a batch in
- * which one bucket holds more than 16384 keys is sorted again by the LSD
- * radix sort before anything is modified (trc_stats.sort_retries counts
- * these); smaller batches, and all batches while the wait hook above is
- * set, use the radix sort.  mode 0 restores that choice, 1 forces the radix
- * sort, 2 tries the bucket sort for every batch.  Results are identical.
+/* Test hook for the choice of batch sort.  Batches of 4,096 to 2^24 keys
+ * (after symmetrizing) sort with a bucket sort (buckets are source ranges
+ * whose split points are the source quantiles of the previous large batch,
+ * or source >> shift before there was one; each bucket sorted whole in
+ * registers or shared memory); a batch in which one bucket holds more than
+ * 16384 keys is sorted again by the LSD radix sort before anything is
+ * modified (trc_stats.sort_retries counts these); other batches, and all
+ * batches while the wait hook above is set, use the radix sort.  mode 0
+ * restores that choice, 1 forces the radix sort, 2 tries the bucket sort
+ * for every batch.  Results are identical.
  * No reference counterpart (the reference's driver sorts each batch with
  * two stable integer sorts, by destination then by source, before the
  * update call: src/graph_bm.cc:354-355). */
