@@ -167,7 +167,18 @@ def run_ours(args, rank, world):
     hbm_gbs, peak_kind = load_peaks()
     n = 1 << SCALE
 
-    # ---- setup (untimed): graph and batches resident in HBM
+    # ---- setup (untimed): graph and batches resident in HBM.  A small graph
+    # first takes the process's one-time costs (kernel modules loaded on
+    # first launch, the memory pool's first growth), which would otherwise
+    # land in the bulk-load figure
+    ws_, wd_ = T.rmat_generate(1 << 16, 0, A, B, C, 16 << 16, device=True)
+    gw = T.Graph(1 << 16)
+    gw.add_edge_batch(ws_, wd_, symmetrize=True, drop_self_loops=True)
+    gw.add_edge_batch(ws_[:50000], wd_[:50000], symmetrize=True, drop_self_loops=True)
+    gw.bfs(0, device=True)
+    gw.close()
+    del ws_, wd_
+    torch.cuda.synchronize()
     s, d = T.rmat_generate(n, 0, A, B, C, EF * n, device=True)
     g = T.Graph(n)
     g.set_stream(stream)
