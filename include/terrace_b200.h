@@ -130,7 +130,12 @@ trc_status trc_debug_sort_mode(trc_graph *g, int mode);
  *      Set semantics: duplicates, already-present edges (insert) and absent
  *      edges (remove) are ignored; input need not be sorted and is never
  *      modified.  *applied (may be NULL) receives the number of directed
- *      edges actually inserted / removed. */
+ *      edges actually inserted / removed.
+ *      The call returns once the batch's last kernels (the list merges and
+ *      segment moves) are queued on the handle's stream; src and dst may be
+ *      reused or freed at once.  Every other entry point on the handle first
+ *      waits for those kernels; the next batch call does not, and copies its
+ *      host arrays to the device on a second stream while they run. */
 trc_status trc_add_edge_batch(trc_graph *g, const uint32_t *src,
                               const uint32_t *dst, uint64_t k, uint32_t flags,
                               uint64_t *applied);

@@ -36,9 +36,18 @@ trc_status guard(F &&f) {
   }
 }
 
-trc::Graph &G(trc_graph *g) {
+// The graph behind a handle, for the batch entry points: a batch may leave
+// its last kernels running (the next batch overlaps its input copy with them).
+trc::Graph &G_batch(trc_graph *g) {
   if (!g || !g->g) trc::throw_error(TRC_ERR_INVALID, "null graph handle");
   return *g->g;
+}
+
+// Every other entry point sees the graph with the last batch finished.
+trc::Graph &G(trc_graph *g) {
+  trc::Graph &x = G_batch(g);
+  x.complete_pending();
+  return x;
 }
 }  // namespace
 
@@ -195,7 +204,7 @@ trc_status trc_debug_sort_mode(trc_graph *g, int mode) {
 trc_status trc_add_edge_batch(trc_graph *g, const uint32_t *src, const uint32_t *dst, uint64_t k,
                               uint32_t flags, uint64_t *applied) {
   return guard([&] {
-    uint64_t a = G(g).apply_batch(src, dst, k, flags, true);
+    uint64_t a = G_batch(g).apply_batch(src, dst, k, flags, true, true);
     if (applied) *applied = a;
   });
 }
@@ -203,7 +212,7 @@ trc_status trc_add_edge_batch(trc_graph *g, const uint32_t *src, const uint32_t 
 trc_status trc_remove_edge_batch(trc_graph *g, const uint32_t *src, const uint32_t *dst,
                                  uint64_t k, uint32_t flags, uint64_t *applied) {
   return guard([&] {
-    uint64_t a = G(g).apply_batch(src, dst, k, flags, false);
+    uint64_t a = G_batch(g).apply_batch(src, dst, k, flags, false, true);
     if (applied) *applied = a;
   });
 }

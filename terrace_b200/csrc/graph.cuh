@@ -98,6 +98,10 @@ class Graph {
   cudaStream_t own_stream = nullptr;
   cudaStream_t side_stream = nullptr;  // hub merge, concurrent with the small-vertex merge
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // A host batch's H2D copy, issued while the previous batch's trailing
+  // kernels (merges, window moves) still run on the graph's stream
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_h2d = nullptr;
   Budget budget;
   Profiler prof;
 
@@ -167,8 +171,16 @@ class Graph {
 
   // ------------------------------------------------------------- update
   // Applies a batch; returns the number of directed edges changed.
+  // With defer_tail the call returns after launching the batch's last
+  // kernels: the graph's stream orders every later device use, and
+  // complete_pending() (or the next batch, after its first synchronisation)
+  // does the host bookkeeping that reads their results.
   uint64_t apply_batch(const uint32_t *src, const uint32_t *dst, uint64_t k, uint32_t flags,
-                       bool insert);
+                       bool insert, bool defer_tail = false);
+  // Waits for a deferred batch tail and finishes it (no-op without one).
+  void complete_pending();
+  bool tail_pending = false;
+  uint64_t tail_nh = 0;  // the pending batch's touched hubs (its rewrite count)
 
   // ------------------------------------------------------------- queries
   void is_edge(const uint32_t *src, const uint32_t *dst, uint64_t q, uint8_t *out, uint32_t flags);
@@ -284,6 +296,7 @@ class Graph {
                   const uint32_t *hw_t, const uint64_t *bkeys, const uint64_t *tpos, bool insert);
   void apply_hubs_finish();
   void hubs_finish();  // after the batch's final synchronisation
+  void finish_tail();  // host part of complete_pending, the stream already synchronised
   void hub_init();
 };
 

@@ -51,6 +51,8 @@ Graph::Graph(uint32_t n_, uint64_t budget_bytes, const trc_config &cfg_) : n(n_)
   TRC_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
   TRC_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
   TRC_CUDA(cudaEventCreateWithFlags(&ev_hub, cudaEventDisableTiming));
+  TRC_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+  TRC_CUDA(cudaEventCreateWithFlags(&ev_h2d, cudaEventDisableTiming));
   stream = own_stream;
   budget.stream = stream;
   budget.open_pool(device);
@@ -107,6 +109,7 @@ Graph::~Graph() {
   if (own_stream) cudaStreamSynchronize(own_stream);
   if (stream && stream != own_stream) cudaStreamSynchronize(stream);
   if (side_stream) cudaStreamSynchronize(side_stream);
+  if (copy_stream) cudaStreamSynchronize(copy_stream);
   prof.reset();
   if (prg.exec) cudaGraphExecDestroy(prg.exec);
   // the members free after this body, on the legacy stream (the work on
@@ -117,6 +120,8 @@ Graph::~Graph() {
   if (ev_hub) cudaEventDestroy(ev_hub);
   if (ev_fork) cudaEventDestroy(ev_fork);
   if (ev_join) cudaEventDestroy(ev_join);
+  if (ev_h2d) cudaEventDestroy(ev_h2d);
+  if (copy_stream) cudaStreamDestroy(copy_stream);
   if (side_stream) cudaStreamDestroy(side_stream);
   if (own_stream) cudaStreamDestroy(own_stream);
 }
@@ -920,16 +925,50 @@ constexpr uint64_t BUCKET_MAX_KEYS = 1u << 24;
 // ---------------------------------------------------------------------------
 // The pipeline
 
+void Graph::complete_pending() {
+  if (!tail_pending) return;
+  sync();
+  finish_tail();
+}
+
+// The pending batch's results that only its last kernels produce: the hub
+// pool's free-list size and top (hubs_finish) and the rewrite count.
+void Graph::finish_tail() {
+  if (!tail_pending) return;
+  tail_pending = false;
+  hubs_finish();
+  uint64_t nrs;
+  memcpy(&nrs, hub_stage_ + 62, 8);
+  last[3] = nrs + tail_nh;
+  last[4] += hub_last[4];
+  last[5] += hub_last[5];
+}
+
 uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint64_t k,
-                            uint32_t flags, bool insert) {
+                            uint32_t flags, bool insert, bool defer_tail) {
   if (k == 0) return 0;
   if (!src_in || !dst_in) throw_error(TRC_ERR_INVALID, "null edge array");
-  for (auto &x : hub_last) x = 0;
   const int sym = (flags & TRC_SYMMETRIZE) ? 1 : 0;
   const int drop = (flags & TRC_DROP_SELF_LOOPS) ? 1 : 0;
   phase(nullptr);
-  const uint32_t *src = to_device(*this, src_in, k, flags, s_in_src);
-  const uint32_t *dst = to_device(*this, dst_in, k, flags, s_in_dst);
+  const uint32_t *src, *dst;
+  if (tail_pending && !(flags & TRC_DEVICE_PTR) && s_in_src.capacity() >= k &&
+      s_in_dst.capacity() >= k) {
+    // The previous batch's kernels that still run read neither staging
+    // buffer (its key build, their only reader, finished before its first
+    // synchronisation), so the copy overlaps them on the copy stream; a
+    // buffer that must grow takes the ordered path below instead (its
+    // allocation is ordered on the graph's stream).
+    src = s_in_src.get();
+    dst = s_in_dst.get();
+    TRC_CUDA(cudaMemcpyAsync(s_in_src.get(), src_in, k * 4, cudaMemcpyHostToDevice, copy_stream));
+    TRC_CUDA(cudaMemcpyAsync(s_in_dst.get(), dst_in, k * 4, cudaMemcpyHostToDevice, copy_stream));
+    TRC_CUDA(cudaEventRecord(ev_h2d, copy_stream));
+    TRC_CUDA(cudaStreamWaitEvent(stream, ev_h2d, 0));
+  } else {
+    src = to_device(*this, src_in, k, flags, s_in_src);
+    dst = to_device(*this, dst_in, k, flags, s_in_dst);
+  }
   const uint64_t k2 = sym ? 2 * k : k;
   DevView G = view();
   uint64_t *cnt = s_cnt.get();
@@ -1046,6 +1085,8 @@ retry_sort:
                                  stream));
   }
   sync();
+  finish_tail();  // a deferred previous batch: its kernels ran before this point
+  for (auto &x : hub_last) x = 0;
   memcpy(hc, hub_stage_, sizeof(hc));
   const uint32_t herr = hub_stage_[60];
   if (herr & ERR_BAD_VERTEX) throw_error(TRC_ERR_INVALID, "vertex id out of range [0, n)");
@@ -1073,13 +1114,14 @@ retry_sort:
   std::vector<int32_t> hh;
   struct HubGuard {  // error path: no hub work may outlive the batch's buffers
     Graph *g;
+    bool armed = true;
     ~HubGuard() {
-      if (g->hub_ctx_.active || g->hub_ctx_.readback) {
+      if (armed && (g->hub_ctx_.active || g->hub_ctx_.readback)) {
         g->hub_ctx_.active = g->hub_ctx_.readback = false;
         cudaStreamSynchronize(g->side_stream);
       }
     }
-  } hub_guard{this};
+  } hub_guard{this, true};
   if (nh) {
     hu.resize(nh);
     hdn.resize(nh);
@@ -1233,6 +1275,26 @@ retry_sort:
     s_pma_next.reset();
     N = Nn;
   }
+  m = insert ? m + kb : m - kb;
+  if (defer_tail && !prof.on) {
+    // the rewrite count lands in pinned staging (clear of the counters and
+    // the error word the next batch copies there before reading it)
+    TRC_CUDA(cudaMemcpyAsync(hub_stage_ + 62, nrs_dev, 8, cudaMemcpyDeviceToHost, stream));
+    hub_guard.armed = false;  // apply_hubs_finish ran: only the readback is left
+    tail_pending = true;
+    tail_nh = nh;
+    tier2_total = rebuild ? Ptot : t2new;
+    last[0] = k2;
+    last[1] = kb;
+    last[2] = nt;
+    last[3] = 0;
+    last[4] = SO;
+    last[5] = SN;
+    last[6] = nmw;
+    last[7] = rebuild ? 1 : 0;
+    version++;
+    return kb;
+  }
   TRC_CUDA(cudaMemcpyAsync(&nrs, nrs_dev, 8, cudaMemcpyDeviceToHost, stream));
   sync();  // host vectors (the hub records) outlive their copies
   phase("finish");
@@ -1240,7 +1302,6 @@ retry_sort:
   const uint64_t nr = nrs + nh;
   SO += hub_last[4];
   SN += hub_last[5];
-  m = insert ? m + kb : m - kb;
   tier2_total = rebuild ? Ptot : t2new;
   last[0] = k2;
   last[1] = kb;

@@ -247,6 +247,63 @@ def test_random_updates_against_set_model(T):
         assert c == sum(1 for w in na & nb if w < min(a, b))
 
 
+def test_back_to_back_batches_defer_their_tails(T):
+    """Batch calls return with their last kernels still queued, and a host
+    batch that follows at once copies its input on a second stream while
+    they run.  Graph A takes batches back to back from two reused host
+    arrays (overwritten right after each call returns) and device tensors;
+    graph B takes the same batches with a query after each (every query
+    waits for the tail).  Both must equal the oracle's set model, and their
+    counters (tier-3 free list, splits, the last batch's rewrite counts)
+    must agree."""
+    import torch
+    rng = np.random.default_rng(5)
+    n = 3000
+    kw = dict(hub_threshold=48, hub_stage_limit=400)
+    ga, gb = T.Graph(n, **kw), T.Graph(n, **kw)
+    sizes = [20000, 5000, 19000, 1, 700, 15000, 20000, 300, 12000, 20000, 9000, 4, 18000, 20000]
+    hs = np.zeros(max(sizes), np.uint32)
+    hd = np.zeros(max(sizes), np.uint32)
+    cur = np.zeros(0, np.uint64)
+    for step, k in enumerate(sizes):
+        s = rng.integers(0, n, k).astype(np.uint32)
+        s[: k // 3] = rng.integers(0, 20, k // 3).astype(np.uint32)
+        d = rng.integers(0, n, k).astype(np.uint32)
+        bk = O.make_keys(s, d, True, True)
+        ins = step % 3 != 2
+        hs[:k], hd[:k] = s, d
+        if step % 4 == 3:  # device input
+            ts_, td_ = torch.from_numpy(s.view(np.int32)).cuda(), torch.from_numpy(d.view(np.int32)).cuda()
+            torch.cuda.synchronize()  # the graph's own stream does not wait for torch's
+            ta = ga.add_edge_batch if ins else ga.remove_edge_batch
+            ca = ta(ts_, td_, **SYM)
+        else:
+            ta = ga.add_edge_batch if ins else ga.remove_edge_batch
+            ca = ta(hs[:k], hd[:k], **SYM)
+            hs[:k] = 7  # the caller may reuse its arrays at once
+            hd[:k] = 9
+        tb = gb.add_edge_batch if ins else gb.remove_edge_batch
+        cb = tb(s, d, **SYM)
+        gb.get_num_edges()
+        cur = O.key_union(cur, bk) if ins else O.key_difference(cur, bk)
+        assert ca == cb
+    off, tgt = O.csr_from_keys(n, cur)
+    sa, sb = ga.stats(), gb.stats()
+    sa.pop("device_bytes")
+    sb.pop("device_bytes")
+    assert sa == sb
+    assert sa["num_hubs"] > 0 and sa["last_rewritten"] > 0
+    assert_same_csr(ga, off, tgt)
+    assert_same_csr(gb, off, tgt)
+    # a batch straight after another, then an analytic: the analytic waits
+    ga.add_edge_batch(s, d, **SYM)
+    ga.remove_edge_batch(s, d, **SYM)
+    cur = O.key_difference(cur, bk)
+    off, tgt = O.csr_from_keys(n, cur)
+    assert np.array_equal(ga.bfs(int(s[0]))[1], O.bfs_levels(off, tgt, int(s[0])))
+    assert_same_csr(ga, off, tgt)
+
+
 @pytest.mark.parametrize("mode", [1, 2])
 def test_batch_sort_modes_agree_with_oracle(T, mode):
     """The bucket sort (mode 2: every batch) and the radix sort (mode 1) give
