@@ -726,6 +726,8 @@ __device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a,
     uint32_t ctop = 0;
     if (d > p) ctop = lower_bound_keys(B, nb, L.at(d - 1));
     for (uint32_t j = ctop + lane; j < nb; j += 32) put_rank(row, seg, j + d, (uint32_t)B[j]);
+    // chunks from the top down; kc = keys below the chunk's top element
+    uint32_t kc = ctop;
     for (uint32_t e = d; e > p;) {
       const uint32_t s0 = e - p > MF_CH ? e - MF_CH : p;
       uint32_t x[MF_R], c[MF_R];
@@ -734,14 +736,34 @@ __device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a,
         uint32_t i = s0 + k * 32 + lane;
         x[k] = i < e ? L.at(i) : 0u;
       }
-      // keys below the chunk's first element (from the element under it)
-      uint32_t cbelow = 0;
-      if (s0 > p) cbelow = lower_bound_keys(B, nb, L.at(s0 - 1));
+      // The chunk's keys lie between the element under it and its top
+      // element.  They are walked down from kc, 32 at a time from a
+      // register window, each broadcast to the lanes, which count the keys
+      // above their elements: c = kc - that count (an inserted key never
+      // equals a list element).  Work per chunk: its own keys, not a
+      // search per element.
+      const bool floor = s0 > p;
+      const uint32_t xb = floor ? L.at(s0 - 1) : 0u;
+      uint32_t gt[MF_R];
 #pragma unroll
-      for (uint32_t k = 0; k < MF_R; k++) {
-        uint32_t i = s0 + k * 32 + lane;
-        c[k] = i < e ? lower_bound_keys(B, nb, x[k]) : 0u;
+      for (uint32_t k = 0; k < MF_R; k++) gt[k] = 0;
+      int32_t j = (int32_t)kc - 1;
+      while (j >= 0) {
+        const int32_t jl = j - 31 + (int32_t)lane;
+        const uint32_t bl = jl >= 0 ? (uint32_t)B[jl] : 0u;
+        // keys ascend with the lane: those above xb are the top lanes
+        const uint32_t cnt = __popc(__ballot_sync(0xFFFFFFFFu, jl >= 0 && (!floor || bl > xb)));
+        for (uint32_t t = 0; t < cnt; t++) {
+          const uint32_t bj = __shfl_sync(0xFFFFFFFFu, bl, 31 - t);
+#pragma unroll
+          for (uint32_t k = 0; k < MF_R; k++) gt[k] += bj > x[k] ? 1u : 0u;
+        }
+        j -= (int32_t)cnt;
+        if (cnt < 32) break;
       }
+      const uint32_t cbelow = (uint32_t)(j + 1);  // keys below the element under the chunk
+#pragma unroll
+      for (uint32_t k = 0; k < MF_R; k++) c[k] = kc - gt[k];
       __syncwarp();
 #pragma unroll
       for (uint32_t k = 0; k < MF_R; k++) {
@@ -751,14 +773,19 @@ __device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a,
         if (lane == 0) cp = last;
         if (i < e) {
           if (c[k] || !stay) put_rank(row, seg, i + c[k], x[k]);
-          for (uint32_t j = cp; j < c[k]; j++) put_rank(row, seg, j + i, (uint32_t)B[j]);
+          for (uint32_t j2 = cp; j2 < c[k]; j2++) put_rank(row, seg, j2 + i, (uint32_t)B[j2]);
         }
       }
       __syncwarp();
+      kc = cbelow;
       e = s0;
     }
     // list empty above p (d == p): the keys all went above
   } else {
+    // chunks from the bottom up; kl = keys below the chunk's first element
+    // (0 at p: every key is a list element, and p is the first element
+    // not below the smallest key, or 0)
+    uint32_t kl = 0;
     for (uint32_t s0 = p; s0 < d; s0 += MF_CH) {
       const uint32_t e = d - s0 > MF_CH ? s0 + MF_CH : d;
       uint32_t x[MF_R];
@@ -767,16 +794,41 @@ __device__ __forceinline__ void merge_one(const DevView &G, const MergeArgs &a,
         uint32_t i = s0 + k * 32 + lane;
         x[k] = i < e ? L.at(i) : 0u;
       }
+      // the chunk's keys (up to its top element) walked up from kl, 32 at a
+      // time: each lane counts those below its elements and flags a key
+      // equal to one
+      const uint32_t xt = L.at(e - 1);
+      uint32_t lt[MF_R], eq = 0;
+#pragma unroll
+      for (uint32_t k = 0; k < MF_R; k++) lt[k] = 0;
+      uint32_t j = kl;
+      while (j < nb) {
+        const uint32_t jl = j + lane;
+        const uint32_t bl = jl < nb ? (uint32_t)B[jl] : 0u;
+        // keys ascend with the lane: those up to xt are the bottom lanes
+        const uint32_t cnt = __popc(__ballot_sync(0xFFFFFFFFu, jl < nb && bl <= xt));
+        for (uint32_t t = 0; t < cnt; t++) {
+          const uint32_t bj = __shfl_sync(0xFFFFFFFFu, bl, t);
+#pragma unroll
+          for (uint32_t k = 0; k < MF_R; k++) {
+            lt[k] += bj < x[k] ? 1u : 0u;
+            eq |= bj == x[k] ? 1u << k : 0u;
+          }
+        }
+        j += cnt;
+        if (cnt < 32) break;
+      }
       __syncwarp();
 #pragma unroll
       for (uint32_t k = 0; k < MF_R; k++) {
         uint32_t i = s0 + k * 32 + lane;
         if (i < e) {
-          uint32_t cc = lower_bound_keys(B, nb, x[k]);
-          if (!(cc < nb && (uint32_t)B[cc] == x[k]) && (cc || !stay)) put_rank(row, seg, i - cc, x[k]);
+          const uint32_t cc = kl + lt[k];
+          if (!((eq >> k) & 1u) && (cc || !stay)) put_rank(row, seg, i - cc, x[k]);
         }
       }
       __syncwarp();
+      kl = j;
     }
   }
   if (lane == 0) G.deg[u] = a.insert ? d + nb : d - nb;
