@@ -163,7 +163,10 @@ def run_ours(args, rank, world):
         TB.build()
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    stream = torch.cuda.current_stream()
+    # a stream of its own: torch's default stream has handle 0, which would
+    # leave the graph on its private stream, unordered with events recorded
+    # on torch's (a batch call returns with its last kernels still queued)
+    stream = torch.cuda.Stream(device=dev)
     hbm_gbs, peak_kind = load_peaks()
     n = 1 << SCALE
 

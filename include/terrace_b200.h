@@ -115,8 +115,9 @@ trc_status trc_debug_sort_wait(trc_graph *g, uint32_t spin_limit,
  * or source >> shift before there was one; each bucket sorted whole in
  * registers or shared memory); a batch in which one bucket holds more than
  * 16384 keys is sorted again by the LSD radix sort before anything is
- * modified (trc_stats.sort_retries counts these); other batches, and all
- * batches while the wait hook above is set, use the radix sort.  mode 0
+ * modified (trc_stats.sort_retries counts these); batches of at most 2048
+ * keys sort in one CTA (a bitonic network in shared memory); other batches,
+ * and all batches while the wait hook above is set, use the radix sort.  mode 0
  * restores that choice, 1 forces the radix sort, 2 tries the bucket sort
  * for every batch.  Results are identical.
  * No reference counterpart (the reference's driver sorts each batch with

@@ -514,6 +514,20 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
+constexpr uint32_t SORT_SMALL_T = 512;
+
+__global__ void __launch_bounds__(SORT_SMALL_T) k_sort_small(const uint64_t *in, uint32_t k,
+                                                              uint64_t *out) {
+  __shared__ uint64_t v[SORT_SMALL_MAX];
+  uint32_t P = 2;
+  while (P < k) P <<= 1;
+  // padding with the largest key: the first k sorted values are the keys
+  for (uint32_t t = threadIdx.x; t < P; t += SORT_SMALL_T) v[t] = t < k ? in[t] : BK_INVALID;
+  __syncthreads();
+  smem_bitonic(v, P, threadIdx.x, SORT_SMALL_T, [] { __syncthreads(); });
+  for (uint32_t t = threadIdx.x; t < k; t += SORT_SMALL_T) out[t] = v[t];
+}
+
 struct BucketLayout {
   uint32_t nb, shift, nct;
   uint64_t cells;  // (nb + 1) * nct
@@ -569,6 +583,14 @@ void bucket_learn_splits(const uint64_t *sorted, uint64_t k, uint32_t n, uint32_
 
 uint64_t bucket_tmp_elems(uint64_t k, uint32_t n, bool splits) {
   return bucket_layout(k, n, splits).total();
+}
+
+uint64_t *sort_small_u64(const uint64_t *keys, uint64_t *alt, uint64_t k, cudaStream_t s,
+                         Profiler &prof) {
+  if (k > SORT_SMALL_MAX) throw_error(TRC_ERR_INVALID, "sort_small_u64: more than 2048 keys");
+  if (k == 0) return alt;
+  TRC_LAUNCH(prof, s, "sort_small", 1, SORT_SMALL_T, 0, k_sort_small, keys, (uint32_t)k, alt);
+  return alt;
 }
 
 uint64_t *bucket_sort_u64(const uint64_t *keys, uint64_t *alt, uint64_t k, uint32_t n,

@@ -178,7 +178,7 @@ __global__ void k_select_scatter(P pred, V val, uint64_t n, const uint64_t *tile
                                  uint64_t *count) {
   constexpr int NW = PT / 32;
   static_assert(PI * NW == 64, "one warp scans the tile's (round, warp) counts, two per lane");
-  __shared__ uint32_t wc[PI * NW];
+  __shared__ uint32_t wc[PI * NW + 1];  // + the tile's total
   const uint64_t base = (uint64_t)blockIdx.x * PTILE;
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   uint32_t m[PI];
@@ -191,19 +191,23 @@ __global__ void k_select_scatter(P pred, V val, uint64_t n, const uint64_t *tile
   __syncthreads();
   if (w == 0) {
     const uint32_t a = wc[2 * lane], b = wc[2 * lane + 1];
-    const uint32_t ex = warp_incl_scan(a + b) - (a + b);
+    const uint32_t in = warp_incl_scan(a + b);
+    const uint32_t ex = in - (a + b);
     wc[2 * lane] = ex;
     wc[2 * lane + 1] = ex + a;
+    if (lane == 31) wc[PI * NW] = in;
   }
   __syncthreads();
-  const uint64_t off = tile_off[blockIdx.x];
+  // (tile_off null: a single tile, its own offset 0 and total the count)
+  const uint64_t off = tile_off ? tile_off[blockIdx.x] : 0;
   const uint32_t lt = lanemask_lt();
 #pragma unroll
   for (int i = 0; i < PI; i++) {
     if ((m[i] >> lane) & 1u)
       out[off + wc[i * NW + w] + __popc(m[i] & lt)] = val(base + (uint64_t)i * PT + threadIdx.x);
   }
-  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *count = tile_off[gridDim.x];
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0)
+    *count = tile_off ? tile_off[gridDim.x] : wc[PI * NW];
 }
 
 template <typename P, typename V, typename T>
@@ -215,12 +219,17 @@ void select_if(P pred, V val, uint64_t n, T *out, uint64_t *count, uint64_t *tmp
   }
   const std::string t_cnt = std::string(tag) + ".count", t_sc = std::string(tag) + ".scatter";
   uint64_t tiles = ceil_div(n, PTILE);
+  auto kscatter = k_select_scatter<P, V, T>;
+  if (tiles == 1) {  // one launch: the tile counts, ranks and writes its items
+    TRC_LAUNCH(prof, s, t_sc.c_str(), 1, PT, 0, kscatter, pred, val, n, (const uint64_t *)nullptr,
+               out, count);
+    return;
+  }
   uint64_t *sums = tmp;
   uint64_t *offs = tmp + tiles;
   TRC_LAUNCH(prof, s, t_cnt.c_str(), tiles, PT, 0, k_tile_sum<PredCount<P>>, PredCount<P>{pred}, n,
              sums);
   exclusive_scan(LoadU64{sums}, tiles, offs, offs + tiles + 1, s, prof, "scan_tiles");
-  auto kscatter = k_select_scatter<P, V, T>;
   TRC_LAUNCH(prof, s, t_sc.c_str(), tiles, PT, 0, kscatter, pred, val, n, offs, out, count);
 }
 
@@ -286,6 +295,12 @@ uint64_t *bucket_sort_u64(const uint64_t *keys, uint64_t *alt, uint64_t k, uint3
                           uint64_t *tmp, cudaStream_t s, Profiler &prof, uint32_t *err,
                           const uint32_t *splits);
 uint64_t bucket_tmp_elems(uint64_t k, uint32_t n, bool splits);
+// Sort of at most SORT_SMALL_MAX keys by one CTA (a bitonic network in shared
+// memory): one launch where the radix sort takes eleven operations.  Writes
+// the sorted keys to alt (keys unchanged) and returns alt.
+constexpr uint32_t SORT_SMALL_MAX = 2048;
+uint64_t *sort_small_u64(const uint64_t *keys, uint64_t *alt, uint64_t k, cudaStream_t s,
+                         Profiler &prof);
 // Split points for the next batches from a sorted batch of k keys: split j =
 // the source of key j * k / BUCKET_SPLITS (n for invalid keys), split 0 = 0,
 // split BUCKET_SPLITS = n.

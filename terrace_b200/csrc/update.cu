@@ -1027,10 +1027,11 @@ uint64_t Graph::apply_batch(const uint32_t *src_in, const uint32_t *dst_in, uint
   // the bucket sort unless the radix sort is asked for (or its wait test
   // hook is set); a bucket too large for it sends the batch back here, to
   // the radix sort, before anything is modified
+  const bool hooks = sort_wait.withhold_first || sort_wait.spin_limit != SortWait{}.spin_limit;
   bool bucket = sort_mode == 2 ||
-                (sort_mode == 0 && k2 >= BUCKET_MIN_KEYS && k2 <= BUCKET_MAX_KEYS &&
-                 !sort_wait.withhold_first &&
-                 sort_wait.spin_limit == SortWait{}.spin_limit);
+                (sort_mode == 0 && k2 >= BUCKET_MIN_KEYS && k2 <= BUCKET_MAX_KEYS && !hooks);
+  // small batches: one CTA sorts them all (no radix passes)
+  const bool small = sort_mode == 0 && !hooks && k2 <= SORT_SMALL_MAX;
 retry_sort:
   TRC_CUDA(cudaMemsetAsync(cnt, 0, 32 * 8, stream));
   TRC_CUDA(cudaMemsetAsync(err.get(), 0, 4, stream));
@@ -1042,8 +1043,9 @@ retry_sort:
   const uint32_t *splits = bsplits_ok ? bsplits.get() : nullptr;
   uint64_t *t = tmp(std::max({radix_tmp_elems(k2), select_tmp_elems(k2),
                               bucket ? bucket_tmp_elems(k2, n, splits != nullptr) : (uint64_t)0}));
-  uint64_t *sorted = bucket ? bucket_sort_u64(A, B, k2, n, t, stream, prof, err.get(), splits)
-                            : radix_sort_u64(A, B, k2, vbits(), t, stream, prof, err.get(), sort_wait);
+  uint64_t *sorted = bucket  ? bucket_sort_u64(A, B, k2, n, t, stream, prof, err.get(), splits)
+                     : small ? sort_small_u64(A, B, k2, stream, prof)
+                             : radix_sort_u64(A, B, k2, vbits(), t, stream, prof, err.get(), sort_wait);
   // the next batches' bucket boundaries: quantiles of this batch's sources
   // (a batch large enough to show the distribution)
   if (k2 >= BUCKET_MIN_KEYS) {

@@ -114,7 +114,10 @@ class Graph:
         self.close()
 
     def set_stream(self, stream):
-        """Bind to a CUDA stream (torch.cuda.Stream, raw handle or None)."""
+        """Bind to a CUDA stream (torch.cuda.Stream, raw handle or None).
+        None and handle 0 (torch's default stream) select the graph's own
+        stream; bind a non-default stream to order the graph's work with other
+        work on it (a batch call returns with its last kernels still queued)."""
         ptr = getattr(stream, "cuda_stream", stream)
         L.check(self._L.trc_graph_set_stream(self._h, C.c_void_p(ptr or 0)))
 
