@@ -4,8 +4,10 @@
  * Plain C: opaque handles, plain pointers and sizes, status codes.  No CUDA
  * or torch types appear here; a CUDA stream is passed as `void*`
  * (cudaStream_t).  Every entry point is synchronous: it returns after the
- * device work it launched has finished, so host buffers may be reused at
- * once.  Unless TRC_DEVICE_PTR is set in `flags`, array arguments are HOST
+ * device work it launched has finished, except that a batch update returns
+ * with its last kernels still queued on the handle's stream (every other
+ * entry point waits for them first).  Host buffers may be reused as soon as
+ * any call returns.  Unless TRC_DEVICE_PTR is set in `flags`, array arguments are HOST
  * pointers and the library copies them to and from the device itself.
  *
  * Each declaration names the reference interface it replaces
@@ -87,7 +89,9 @@ const char *trc_last_error(void);
 trc_status trc_graph_create(uint32_t n, uint64_t hbm_budget_bytes,
                             const trc_config *cfg, trc_graph **out);
 trc_status trc_graph_destroy(trc_graph *g);
-/* Bind the handle to a CUDA stream (cudaStream_t); NULL = library stream.
+/* Bind the handle to a CUDA stream (cudaStream_t); NULL = the handle's own
+ * stream (so is handle 0, the legacy default stream: bind another stream to
+ * order the handle's work with work on it).
  * Batch updates also run their hub merge on a second stream owned by the
  * handle, forked from and joined back to the bound stream with events, so
  * every call's work stays ordered after earlier work on the bound stream. */
