@@ -1128,7 +1128,9 @@ retry_sort:
   // take a second copy
   const uint64_t spec = std::min<uint64_t>(cap, HUB_SPEC);
   uint32_t *sp = hub_stage_ + 64;  // after the 32 counters
-  static_assert(C_COUNT <= 32, "counter staging");
+  // staging words: the counters 0 .. 2*C_COUNT-1, the error word 60, a
+  // deferred batch's rewrite count 62-63, the hub records from 64 on
+  static_assert(2 * C_COUNT <= 60, "counter staging");
   TRC_CUDA(cudaMemcpyAsync(hub_stage_, cnt, sizeof(hc), cudaMemcpyDeviceToHost, stream));
   TRC_CUDA(cudaMemcpyAsync(hub_stage_ + 60, err.get(), 4, cudaMemcpyDeviceToHost, stream));
   {
