@@ -312,6 +312,7 @@ def run_ours(args, rank, world):
     roof = roofline_for("upd_merge", (sum(x[0] for x in merge), max(x[1] for x in merge)), sizes,
                         hbm_gbs, peak_kind)
     total_kernel_ms = sum(v[0] for v in kernel_ms.values())
+    step_roof = step_roofline(sizes, ins_ms / args.steps, hbm_gbs, peak_kind)
 
     g.close()
     del batches
@@ -353,6 +354,7 @@ def run_ours(args, rank, world):
         "gpu_launches": launches,
         "clocks": clocks,
         "roofline": roof,
+        "step_roofline": step_roof,
         "host_phase_ms_per_batch": {k: round(v, 3) for k, v in host_ms.items()},
         "kernel_ms_per_batch": round(total_kernel_ms / args.steps, 3),
         "batch_sizes_last": {k: sizes[-1][k] for k in ("last_keys", "last_applied", "last_touched",
@@ -565,6 +567,19 @@ def ncu_traffic(name):
     except OSError:
         pass
     return None, None
+
+
+def step_roofline(sizes, step_ms, hbm_gbs, peak_kind):
+    """The whole insert step against HBM: the bytes a batch has to move at
+    least (its pairs read, its 64-bit keys written and read back once, and
+    the merge's old lists, keys and new lists over all three tiers with ~40 B
+    per rewritten vertex) over the timed device time per step."""
+    per = [8 * BATCH + 16 * sz["last_keys"] + 4 * sz["last_gathered"] + 8 * sz["last_applied"]
+           + 4 * sz["last_written"] + 40 * sz["last_rewritten"] for sz in sizes]
+    b = sum(per) / len(per)
+    achieved = b / (step_ms / 1e3) / 1e9
+    return {"bound": "hbm", "bytes_per_step": b, "step_ms": step_ms, "achieved": achieved,
+            "peak": hbm_gbs, "unit": "GB/s", "frac": achieved / hbm_gbs, "peak_kind": peak_kind}
 
 
 def roofline_for(name, ms_cnt, sizes, hbm_gbs, peak_kind):
